@@ -1,0 +1,239 @@
+"""Synthetic pattern meshes and collider grids for the benchmark workloads.
+
+The reference meshes real pattern files with its own mesher (klon3d-mesh,
+out of scope here). These generators produce the same kind of input the
+scene builder reads — pieces in pattern coordinates (mm), positively oriented
+triangles, a grainline per piece, seam point pairs at equal length fraction
+(crates/klon3d-mesh/src/lib.rs:178-228) and a start position per point —
+from a seed, with numpy only.
+
+Workloads (sizes as named by the benchmark configurations):
+  * ``tube``: closed tube, rest circumference 40 cm, height 20 cm, ~10 mm
+    edges, fitted over an analytic cylinder of radius 8 cm;
+  * ``sheet_over_sphere``: 1.0 x 1.0 m sheet on a 257 x 257 vertex grid with
+    +/-1 mm in-plane jitter, dropped 0.5 m onto a sphere stored as a 128^3
+    signed-distance grid at 1 cm spacing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+
+
+@dataclass
+class Material:
+    """Fabric record (sim/src/material.rs:21-68), SI units."""
+    dehnung_n_m: float
+    kette_n_m: float
+    schub_n_m: float
+    biegung_nm: float
+    biegung_kette_nm: float
+    biegung_schraege_nm: float
+    flaechengewicht_kg_m2: float
+    dicke_m: float
+    reibung: float
+
+    def to_c(self) -> _abi.K3dMaterial:
+        return _abi.K3dMaterial(self.dehnung_n_m, self.kette_n_m, self.schub_n_m, self.biegung_nm,
+                                self.biegung_kette_nm, self.biegung_schraege_nm,
+                                self.flaechengewicht_kg_m2, self.dicke_m, self.reibung)
+
+
+# Fabric profiles shipped with the reference (sim/src/material.rs:73-102).
+RADICAL_RUBBER_04 = Material(348.2741562, 348.2817188, 174.1590469, 2482.2424e-9, 2486.4924e-9,
+                             2486.4924e-9, 0.3489899, 0.4e-3, 0.03)
+RETIFIST_NR_040 = Material(33.333332, 33.333332, 6.6666665, 60.361e-9, 60.361e-9, 60.361e-9,
+                           0.380, 0.4e-3, 0.03)
+
+
+@dataclass
+class Simparameter:
+    """Simparameter (sim/src/szene.rs:96-126), the fields the implicit step reads."""
+    bild_dt: float = 1.0 / 60.0
+    schwerkraft: tuple = (0.0, 0.0, -9.81)
+    daempfung: float = 0.0
+
+    def to_c(self) -> _abi.K3dSimparams:
+        return _abi.K3dSimparams(self.bild_dt, (C.c_double * 3)(*self.schwerkraft), self.daempfung)
+
+
+@dataclass
+class Teil:
+    punkte_mm: np.ndarray            # (n, 2) float64
+    dreiecke: np.ndarray             # (t, 3) uint32
+    fadenlauf: tuple
+    material: Material
+    lage: np.ndarray                 # (n, 3) float64, metres
+    reduktion: float = 0.0
+
+
+@dataclass
+class Teilnaht:
+    teil_a: int
+    teil_b: int
+    paare: np.ndarray                # (k, 2) uint32, local indices on a and b
+
+
+@dataclass
+class Naht:
+    teilnaehte: list
+    laenge_a_mm: float = 0.0
+    laenge_b_mm: float = 0.0
+
+
+@dataclass
+class Muster:
+    """A pattern: pieces, seams and the scene parameters."""
+    teile: list
+    naehte: list = field(default_factory=list)
+    param: Simparameter = field(default_factory=Simparameter)
+    naht_nachgiebigkeit: float = 0.0
+    einhalteweite: bool = False
+
+    def to_c(self):
+        """The k3d_pattern struct plus the objects that keep its memory alive."""
+        keep = []
+        pieces = (_abi.K3dPiece * max(len(self.teile), 1))()
+        for k, t in enumerate(self.teile):
+            pm = np.ascontiguousarray(t.punkte_mm, dtype=np.float64)
+            dr = np.ascontiguousarray(t.dreiecke, dtype=np.uint32)
+            la = np.ascontiguousarray(t.lage, dtype=np.float64)
+            keep += [pm, dr, la]
+            pieces[k] = _abi.K3dPiece(pm.shape[0], _abi.ptr(pm, C.c_double), dr.shape[0],
+                                      _abi.ptr(dr, C.c_uint32),
+                                      (C.c_double * 2)(*t.fadenlauf), t.material.to_c(),
+                                      t.reduktion, _abi.ptr(la, C.c_double))
+        seams = (_abi.K3dSeam * max(len(self.naehte), 1))()
+        for k, n in enumerate(self.naehte):
+            parts = (_abi.K3dSeamPart * max(len(n.teilnaehte), 1))()
+            for q, tn in enumerate(n.teilnaehte):
+                pr = np.ascontiguousarray(tn.paare, dtype=np.uint32)
+                keep.append(pr)
+                parts[q] = _abi.K3dSeamPart(tn.teil_a, tn.teil_b, pr.shape[0], _abi.ptr(pr, C.c_uint32))
+            keep.append(parts)
+            seams[k] = _abi.K3dSeam(len(n.teilnaehte), 0, parts, n.laenge_a_mm, n.laenge_b_mm)
+        keep += [pieces, seams]
+        pat = _abi.K3dPattern(len(self.teile), len(self.naehte), pieces, seams, self.param.to_c(),
+                              self.naht_nachgiebigkeit, 1 if self.einhalteweite else 0, 0)
+        return pat, keep
+
+
+def rechteck_netz(breite_mm: float, hoehe_mm: float, nx: int, ny: int, jitter_mm: float = 0.0,
+                  seed: int = 0):
+    """Regular grid of (nx+1) x (ny+1) points, two positive triangles per cell.
+
+    Point (i, j) has index j*(nx+1) + i. With ``jitter_mm`` every point moves
+    by U(-jitter, jitter) in x and y (seeded)."""
+    xs = np.linspace(0.0, breite_mm, nx + 1)
+    ys = np.linspace(0.0, hoehe_mm, ny + 1)
+    gx, gy = np.meshgrid(xs, ys)
+    p = np.stack([gx.ravel(), gy.ravel()], axis=1)
+    if jitter_mm > 0.0:
+        rng = np.random.default_rng(seed)
+        p = p + rng.uniform(-jitter_mm, jitter_mm, size=p.shape)
+    i = np.arange(nx)
+    j = np.arange(ny)
+    ii, jj = np.meshgrid(i, j)
+    a = (jj * (nx + 1) + ii).ravel()
+    b = a + 1
+    c = a + nx + 2
+    d = a + nx + 1
+    tri = np.empty((2 * a.size, 3), dtype=np.uint32)
+    tri[0::2] = np.stack([a, b, c], axis=1)
+    tri[1::2] = np.stack([a, c, d], axis=1)
+    return p, tri
+
+
+# ------------------------------------------------------------------ tube
+TUBE_MATERIAL = Material(600.0, 600.0, 300.0, 1e-7, 1e-7, 1e-7, 0.5, 0.5e-3, 0.03)
+
+
+def tube(umfang_m: float = 0.40, hoehe_m: float = 0.20, kante_mm: float = 10.0,
+         zylinder_radius_m: float = 0.08, anfangsabstand_m: float = 0.005,
+         material: Material = TUBE_MATERIAL):
+    """Closed tube over a cylinder (the reference's tube acceptance case,
+    sim/src/roehre.rs:197-239, built without the mesher).
+
+    The rectangle's right side is sewn to its left side (roehre.rs:45, B->C
+    against A->D), the two sides keep their own points. Start position: rolled
+    all the way round at radius R + t/2 + ``anfangsabstand_m``, seam closed.
+    Returns (muster, cylinder body dict)."""
+    nx = int(round(umfang_m * 1e3 / kante_mm))
+    ny = int(round(hoehe_m * 1e3 / kante_mm))
+    p, tri = rechteck_netz(umfang_m * 1e3, hoehe_m * 1e3, nx, ny)
+    r0 = zylinder_radius_m + material.dicke_m / 2.0 + anfangsabstand_m
+    je_m = 2.0 * math.pi / umfang_m
+    u = p[:, 0] * 1e-3
+    y = p[:, 1] * 1e-3
+    w = u * je_m
+    lage = np.stack([r0 * np.cos(w), r0 * np.sin(w), -y], axis=1)
+    rechts = np.arange(ny + 1) * (nx + 1) + nx
+    links = np.arange(ny + 1) * (nx + 1)
+    paare = np.stack([rechts, links], axis=1).astype(np.uint32)
+    teil = Teil(p, tri, (1.0, 0.0), material, lage)
+    naht = Naht([Teilnaht(0, 0, paare)], hoehe_m * 1e3, hoehe_m * 1e3)
+    param = Simparameter(bild_dt=1.0 / 60.0, schwerkraft=(0.0, 0.0, 0.0), daempfung=5.0)
+    body = dict(art=_abi.K3D_BODY_CYLINDER, punkt=(0.0, 0.0, 0.0), achse=(0.0, 0.0, 1.0),
+                radius=zylinder_radius_m)
+    return Muster([teil], [naht], param), body
+
+
+# ------------------------------------------------------------------ sheet over a sphere
+SHEET_MATERIAL = Material(dehnung_n_m=1000.0, kette_n_m=2000.0, schub_n_m=50.0, biegung_nm=5e-6,
+                          biegung_kette_nm=5e-6, biegung_schraege_nm=5e-6,
+                          flaechengewicht_kg_m2=0.2, dicke_m=0.5e-3, reibung=0.3)
+
+
+def sphere_sdf_grid(radius_m: float, n: int, spacing_m: float, zentrum=(0.0, 0.0, 0.0)):
+    """Signed distance of a sphere sampled at the nodes of an n^3 grid
+    centred on the sphere. Returns a body dict for a K3D_BODY_SDF_GRID."""
+    half = 0.5 * (n - 1) * spacing_m
+    ax = np.arange(n, dtype=np.float64) * spacing_m - half
+    gz, gy, gx = np.meshgrid(ax, ax, ax, indexing="ij")
+    d = np.sqrt(gx * gx + gy * gy + gz * gz) - radius_m
+    return dict(art=_abi.K3D_BODY_SDF_GRID, punkt=tuple(zentrum), dims=(n, n, n),
+                ursprung=(-half, -half, -half), spacing=spacing_m,
+                sdf=np.ascontiguousarray(d.astype(np.float32)))
+
+
+def sheet_over_sphere(n: int = 257, groesse_m: float = 1.0, jitter_mm: float = 1.0, seed: int = 0,
+                      fall_m: float = 0.5, kugel_radius_m: float = 0.3, sdf_n: int = 128,
+                      sdf_spacing_m: float = 0.01, material: Material = SHEET_MATERIAL,
+                      bild_dt: float = 1.0 / 120.0):
+    """Woven sheet dropped onto a sphere collider.
+
+    n x n vertices over ``groesse_m`` square, in-plane jitter U(-1, 1) mm,
+    grainline angle U[0, pi) from the seed, start plane ``fall_m`` above the
+    sphere top. Returns (muster, sphere SDF body dict)."""
+    rng = np.random.default_rng(seed)
+    winkel = float(rng.uniform(0.0, math.pi))
+    p, tri = rechteck_netz(groesse_m * 1e3, groesse_m * 1e3, n - 1, n - 1, jitter_mm, seed + 1)
+    z0 = kugel_radius_m + fall_m
+    lage = np.stack([p[:, 0] * 1e-3 - 0.5 * groesse_m, p[:, 1] * 1e-3 - 0.5 * groesse_m,
+                     np.full(p.shape[0], z0)], axis=1)
+    teil = Teil(p, tri, (math.cos(winkel), math.sin(winkel)), material, lage)
+    param = Simparameter(bild_dt=bild_dt, schwerkraft=(0.0, 0.0, -9.81), daempfung=0.0)
+    body = sphere_sdf_grid(kugel_radius_m, sdf_n, sdf_spacing_m)
+    return Muster([teil], [], param), body
+
+
+def body_to_c(body: dict) -> _abi.K3dBody:
+    """k3d_body from a body dict; the dict keeps the SDF array alive."""
+    kb = _abi.K3dBody()
+    kb.art = body["art"]
+    for a in range(3):
+        kb.dims[a] = body.get("dims", (0, 0, 0))[a]
+        kb.punkt[a] = body.get("punkt", (0.0, 0.0, 0.0))[a]
+        kb.achse[a] = body.get("achse", (0.0, 0.0, 1.0))[a]
+        kb.geschwindigkeit[a] = body.get("geschwindigkeit", (0.0, 0.0, 0.0))[a]
+        kb.ursprung[a] = body.get("ursprung", (0.0, 0.0, 0.0))[a]
+    kb.radius = body.get("radius", 0.0)
+    kb.spacing = body.get("spacing", 1.0)
+    sdf = body.get("sdf")
+    kb.sdf = _abi.ptr(sdf, C.c_float) if sdf is not None else None
+    return kb

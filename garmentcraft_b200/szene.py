@@ -1,0 +1,137 @@
+"""The scene as the implicit step sees it (Szene, sim/src/szene.rs:198-269).
+
+Host-side numpy arrays in the layout of the k3d_scene C struct. The groups
+(abstand, naht, biegung) are in the scene's colour order, which fixes the
+summation order of the reference CPU solver.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from .synth import Simparameter, body_to_c
+
+_ARRAYS = {
+    # name: (dtype, columns)
+    "x": (np.float64, 3), "v": (np.float64, 3), "masse": (np.float64, 0), "w": (np.float64, 0),
+    "kollisionsabstand": (np.float64, 0), "reibung": (np.float64, 0),
+    "abstand_punkte": (np.uint32, 2), "abstand_ruhe": (np.float64, 0),
+    "abstand_nachgiebigkeit": (np.float64, 0), "membran_kante": (np.uint8, 0),
+    "naht_punkte": (np.uint32, 2), "naht_ruhe": (np.float64, 0),
+    "biegung_punkte": (np.uint32, 4), "biegung_ruhe": (np.float64, 0),
+    "biegung_nachgiebigkeit": (np.float64, 0),
+    "membran_punkte": (np.uint32, 3), "membran_flaeche": (np.float64, 0),
+    "membran_ruhe_inv": (np.float64, 4), "membran_kette": (np.float64, 2),
+    "membran_schuss": (np.float64, 2), "membran_steif": (np.float64, 3),
+    "dreiecke": (np.uint32, 3), "ruhe_inv": (np.float64, 4),
+}
+_COUNT = {
+    "x": "n_punkte", "v": "n_punkte", "masse": "n_punkte", "w": "n_punkte",
+    "kollisionsabstand": "n_punkte", "reibung": "n_punkte",
+    "abstand_punkte": "n_abstand", "abstand_ruhe": "n_abstand", "abstand_nachgiebigkeit": "n_abstand",
+    "membran_kante": "n_abstand", "naht_punkte": "n_naht", "naht_ruhe": "n_naht",
+    "biegung_punkte": "n_biegung", "biegung_ruhe": "n_biegung", "biegung_nachgiebigkeit": "n_biegung",
+    "membran_punkte": "n_membran", "membran_flaeche": "n_membran", "membran_ruhe_inv": "n_membran",
+    "membran_kette": "n_membran", "membran_schuss": "n_membran", "membran_steif": "n_membran",
+    "dreiecke": "n_dreiecke", "ruhe_inv": "n_dreiecke",
+}
+_CTYPE = {np.float64: C.c_double, np.uint32: C.c_uint32, np.uint8: C.c_uint8}
+
+
+@dataclass
+class Szene:
+    x: np.ndarray
+    v: np.ndarray
+    masse: np.ndarray
+    w: np.ndarray
+    kollisionsabstand: np.ndarray
+    reibung: np.ndarray
+    abstand_punkte: np.ndarray
+    abstand_ruhe: np.ndarray
+    abstand_nachgiebigkeit: np.ndarray
+    membran_kante: np.ndarray
+    naht_punkte: np.ndarray
+    naht_ruhe: np.ndarray
+    biegung_punkte: np.ndarray
+    biegung_ruhe: np.ndarray
+    biegung_nachgiebigkeit: np.ndarray
+    membran_punkte: np.ndarray
+    membran_flaeche: np.ndarray
+    membran_ruhe_inv: np.ndarray
+    membran_kette: np.ndarray
+    membran_schuss: np.ndarray
+    membran_steif: np.ndarray
+    dreiecke: np.ndarray
+    ruhe_inv: np.ndarray
+    koerper: list = field(default_factory=list)
+    param: Simparameter = field(default_factory=Simparameter)
+    zeit: float = 0.0
+
+    @property
+    def n(self) -> int:
+        return self.x.shape[0]
+
+    @classmethod
+    def from_view(cls, view: _abi.K3dScene, koerper=None) -> "Szene":
+        """Copies a k3d_scene view into numpy arrays."""
+        kw = {}
+        for name, (dt, cols) in _ARRAYS.items():
+            cnt = getattr(view, _COUNT[name])
+            size = cnt * (cols if cols else 1)
+            p = getattr(view, name)
+            if cnt == 0 or not p:
+                a = np.zeros(size, dtype=dt)
+            else:
+                a = np.ctypeslib.as_array(p, shape=(size,)).astype(dt, copy=True)
+            kw[name] = a.reshape(cnt, cols) if cols else a
+        prm = view.param
+        kw["param"] = Simparameter(prm.bild_dt, tuple(prm.schwerkraft), prm.daempfung)
+        kw["zeit"] = view.zeit
+        kw["koerper"] = list(koerper or [])
+        return cls(**kw)
+
+    def copy(self) -> "Szene":
+        kw = {name: getattr(self, name).copy() for name in _ARRAYS}
+        return Szene(**kw, koerper=list(self.koerper), param=self.param, zeit=self.zeit)
+
+    def to_c(self):
+        """(k3d_scene, keepalive). x and v point at this scene's own arrays, so
+        a call that writes them writes this scene."""
+        for name in _ARRAYS:
+            a = getattr(self, name)
+            if not a.flags["C_CONTIGUOUS"] or a.dtype != _ARRAYS[name][0]:
+                setattr(self, name, np.ascontiguousarray(a, dtype=_ARRAYS[name][0]))
+        s = _abi.K3dScene()
+        s.n_punkte = self.x.shape[0]
+        s.n_abstand = self.abstand_punkte.shape[0]
+        s.n_naht = self.naht_punkte.shape[0]
+        s.n_biegung = self.biegung_punkte.shape[0]
+        s.n_membran = self.membran_punkte.shape[0]
+        s.n_dreiecke = self.dreiecke.shape[0]
+        for name, (dt, _) in _ARRAYS.items():
+            setattr(s, name, _abi.ptr(getattr(self, name), _CTYPE[dt]))
+        bodies = (_abi.K3dBody * max(len(self.koerper), 1))()
+        for k, b in enumerate(self.koerper):
+            bodies[k] = body_to_c(b)
+        s.n_koerper = len(self.koerper)
+        s.koerper = bodies
+        s.param = self.param.to_c()
+        s.zeit = self.zeit
+        return s, [bodies]
+
+    # sim/src/szene.rs:768-774
+    def naht_kuerzen(self, schritt: float) -> None:
+        i, j = self.naht_punkte[:, 0], self.naht_punkte[:, 1]
+        l = np.sqrt(np.sum((self.x[i] - self.x[j]) ** 2, axis=1))
+        self.naht_ruhe = np.maximum(np.minimum(self.naht_ruhe, l) - schritt, 0.0)
+
+    # sim/src/szene.rs:778-782
+    def naht_offen(self) -> None:
+        self.naht_ruhe = np.full_like(self.naht_ruhe, math.inf)
+
+    def gesamtmasse(self) -> float:
+        return float(np.sum(self.masse))

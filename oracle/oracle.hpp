@@ -1,0 +1,257 @@
+// ORACLE — test infrastructure only. A CPU FP64 restatement of klon3d-sim's
+// implicit backward-Euler cloth step (crates/klon3d-sim, viktoschi/GarmentCraft).
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
+// it, and only as the checker or the timed CPU baseline. The product library
+// (garmentcraft_b200) never links or calls it.
+//
+// Parity is pinned by the reference's own known-answer tests, restated in
+// tests/test_oracle_golden.py (bending stiffness values, dihedral gradient vs
+// central differences, membrane acceptance items, 3x3 inverse, seam spring
+// convergence, tube hoop strain). The reference is Rust and cannot be built
+// in this environment, so no reference binary exists to compare against.
+//
+// Every function cites the reference file:line it follows. Paths are relative
+// to the reference project; `sim/` stands for `crates/klon3d-sim/`.
+#pragma once
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <map>
+#include <optional>
+#include <set>
+#include <utility>
+#include <vector>
+
+namespace orc {
+
+using V3 = std::array<double, 3>;
+using V2 = std::array<double, 2>;
+using M3 = std::array<V3, 3>;
+
+// sim/src/koerper.rs:37-54 vector helpers
+inline V3 sub(V3 a, V3 b) { return {a[0] - b[0], a[1] - b[1], a[2] - b[2]}; }
+inline V3 add(V3 a, V3 b) { return {a[0] + b[0], a[1] + b[1], a[2] + b[2]}; }
+inline V3 mul(V3 a, double s) { return {a[0] * s, a[1] * s, a[2] * s}; }
+inline double dot(V3 a, V3 b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline V3 cross(V3 a, V3 b) {
+  return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+}
+inline double norm(V3 a) { return std::sqrt(dot(a, a)); }
+
+// ---------------------------------------------------------------- material
+// sim/src/material.rs:21-68
+struct Material {
+  double dehnung_n_m = 0, kette_n_m = 0, schub_n_m = 0;
+  double biegung_nm = 0, biegung_kette_nm = 0, biegung_schraege_nm = 0;
+  double flaechengewicht_kg_m2 = 0, dicke_m = 0, reibung = 0;
+};
+
+// ---------------------------------------------------------------- membrane
+// sim/src/kontinuum.rs:70-88 (Membran), :117-127 (Hessen)
+struct Membran {
+  double flaeche = 0;
+  std::array<double, 4> ruhe_inv{};
+  V2 kette{}, schuss{};
+  double kette_n_m = 0, dehnung_n_m = 0, schub_n_m = 0;
+};
+struct Hessen {
+  V3 f1{}, f2{}, w{};
+};
+struct MembranElement {
+  std::array<uint32_t, 3> punkte{};
+  Membran element;
+};
+
+std::optional<Membran> membran_bauen(std::array<V2, 3> ruhe, V3 kanten, V2 dir2, V3 material);
+void membran_f(const Membran& m, const std::array<V3, 3>& p, V3& f1, V3& f2);
+V3 membran_dehnung(const Membran& m, const std::array<V3, 3>& p);
+V3 membran_spannung(const Membran& m, const std::array<V3, 3>& p);
+double membran_energie(const Membran& m, const std::array<V3, 3>& p);
+std::array<V3, 3> membran_krafte(const Membran& m, const std::array<V3, 3>& p);
+std::array<V3, 3> membran_krafte_zug(const Membran& m, const std::array<V3, 3>& p);
+Hessen membran_hessen(const Membran& m, const std::array<V3, 3>& p);
+std::array<V3, 3> membran_mal_h_aus(const Membran& m, const Hessen& h, const std::array<V3, 3>& d);
+std::array<M3, 3> membran_diag_bloecke_aus(const Membran& m, const Hessen& h);
+V3 psd2(double a, double b, double c);
+
+// ---------------------------------------------------------------- bending
+// sim/src/biegung.rs:92-173
+double steifigkeit(double weft, double warp, double bias, double theta);
+double steifigkeit_aus(double c2, double s2, double weft, double warp, double bias);
+bool cos2_sin2(V2 e, V2 warp, double& c2, double& s2);
+// sim/src/cpu.rs:279-307
+double winkel_fehler(double theta, double ruhe);
+bool dieder(const std::array<V3, 4>& q, double& theta, std::array<V3, 4>& grad);
+
+// ---------------------------------------------------------------- colouring
+// sim/src/faerbung.rs:11-57
+std::pair<std::vector<uint32_t>, size_t> faerbe(size_t anzahl, size_t npunkte,
+                                                 const std::vector<std::vector<uint32_t>>& punkte);
+std::pair<std::vector<size_t>, std::vector<std::pair<size_t, size_t>>> ordnung(
+    const std::vector<uint32_t>& farbe, size_t zahl);
+
+// ---------------------------------------------------------------- bodies
+// sim/src/koerper.rs:16-35 (Zylinder) plus a sampled signed-distance grid,
+// which has no counterpart in the reference (its mesh body answers exact
+// nearest-triangle queries, sim/src/netzkoerper.rs:503-539).
+struct Kontakt {
+  V3 normale{};
+  double tiefe = 0;
+  V3 geschwindigkeit{};
+};
+struct Koerper {
+  int art = 0;  // 0 = Zylinder, 1 = SDF grid
+  V3 punkt{}, achse{0, 0, 1};
+  double radius = 0;
+  V3 geschwindigkeit{};
+  // grid: node (i,j,k) sits at ursprung + spacing*(i,j,k) + punkt (punkt moves)
+  const float* sdf = nullptr;
+  std::array<int32_t, 3> dims{};
+  V3 ursprung{};
+  double spacing = 1;
+  std::optional<Kontakt> kontakt(V3 x, double abstand) const;
+  Koerper verschoben(double t) const;
+};
+
+// ---------------------------------------------------------------- scene
+// sim/src/szene.rs:96-126
+struct Simparameter {
+  double bild_dt = 1.0 / 60.0;
+  V3 schwerkraft{0, 0, -9.81};
+  double daempfung = 0.0;
+  double naht_nachgiebigkeit = 0.0;
+  bool einhalteweite = false;
+};
+// sim/src/szene.rs:130-179
+template <int N>
+struct Gruppe {
+  std::vector<std::array<uint32_t, N>> punkte;
+  std::vector<double> ruhe, nachgiebigkeit;
+  std::vector<std::pair<size_t, size_t>> farben;
+  size_t size() const { return punkte.size(); }
+};
+// sim/src/szene.rs:198-269 (the fields the implicit step reads)
+struct Szene {
+  std::vector<V3> x, v;
+  std::vector<double> masse, w, kollisionsabstand, reibung;
+  Gruppe<2> abstand, naht;
+  Gruppe<4> biegung;
+  std::vector<std::array<uint32_t, 3>> dreiecke;
+  std::vector<std::array<double, 4>> ruhe_inv;
+  std::vector<uint8_t> membran_kante;
+  std::vector<MembranElement> membran_elemente;
+  std::vector<Koerper> koerper;
+  Simparameter param;
+  double zeit = 0;
+  size_t membran_entartet = 0, naht_biegung_ohne = 0, einhalte_kanten = 0;
+};
+
+// Pattern input of the scene builder: the part of klon3d_mesh::Musternetz
+// (crates/klon3d-mesh/src/lib.rs:91-241) that Szene::bauen reads.
+struct Teil {
+  std::vector<V2> punkte_mm;
+  std::vector<std::array<uint32_t, 3>> dreiecke;
+  V2 fadenlauf{1, 0};
+  Material material;
+  double reduktion = 0;
+  std::vector<V3> lage;  // start position per point (m)
+};
+struct Teilnaht {
+  size_t teil_a = 0, teil_b = 0;
+  std::vector<std::pair<uint32_t, uint32_t>> paare;
+};
+struct Naht {
+  std::vector<Teilnaht> teilnaehte;
+  double laenge_a_mm = 0, laenge_b_mm = 0;
+};
+struct Muster {
+  std::vector<Teil> teile;
+  std::vector<Naht> naehte;
+};
+Szene szene_bauen(const Muster& netz, const std::vector<Koerper>& koerper, Simparameter param);
+void naht_kuerzen(Szene& s, double schritt);
+void naht_offen(Szene& s);
+
+// ---------------------------------------------------------------- implicit
+// sim/src/implizit.rs:79-100
+struct Kante {
+  uint32_t i = 0, j = 0;
+  double k = 0;
+  V3 richtung{};
+  double quer = 0, ruhe = 0;
+};
+struct Biegung {
+  std::array<uint32_t, 4> punkte{};
+  std::array<V3, 4> grad{};
+  double k = 0, ruhe = 0;
+};
+// sim/src/implizit.rs:594-599
+struct Fest {
+  V3 normale{};
+  double vn_soll = 0;
+  V3 v_koerper{};
+};
+// sim/src/implizit.rs:124-172 (without self-collision springs)
+struct System {
+  double h = 0, c = 0;
+  size_t cg_max = 0;
+  double cg_toleranz = 0;
+  const std::vector<double>* masse = nullptr;
+  const std::vector<double>* w = nullptr;
+  const std::vector<V3>* v = nullptr;
+  std::vector<Kante> kanten, naehte;
+  std::vector<Biegung> biegungen;
+  const std::vector<MembranElement>* membran = nullptr;
+  std::vector<Hessen> membran_h;
+  std::vector<V3> rhs, f, last;
+  std::vector<M3> pinv;
+  void mal_h(const std::vector<V3>& p, std::vector<V3>& out) const;
+  void mal_a(const std::vector<V3>& p, std::vector<V3>& out) const;
+  std::vector<M3> diag() const;
+};
+// sim/src/implizit.rs:294-299
+struct CgLauf {
+  size_t iterationen = 0;
+  bool nicht_konvergiert = false;
+  double rest = 0;
+};
+CgLauf cpu_loese(const System& sys, const std::vector<std::optional<Fest>>& fest, std::vector<V3>& dv);
+M3 m3_inv(const M3& m);
+V3 m3_mal(const M3& m, V3 v);
+
+// sim/src/implizit.rs:457-531
+struct ImplizitParameter {
+  size_t schritte_je_bild = 5;
+  size_t cg_max = 50;
+  double cg_toleranz = 1e-5;
+  double naht_k = 500.0;
+  double kontakt_rand = 1e-4;
+  bool normalkraft_aus_last = false;
+  bool durchstoss_pruefen = true;
+};
+// sim/src/implizit.rs:535-561
+struct ImplizitStatistik {
+  size_t cg_iterationen = 0, loesungen = 0, nicht_konvergiert = 0, kontakte = 0, haftend = 0,
+         freigegeben = 0, durchstoesse = 0, koerperpunkte = 0;
+  double rest_max = 0;
+};
+// sim/src/implizit.rs:570-1057
+struct ImplizitCg {
+  ImplizitParameter param;
+  ImplizitStatistik statistik;
+  std::vector<V3> dv_vorher;
+  System system_bauen(Szene& s, double h, std::vector<std::optional<Fest>>& fest);
+  void schritt(Szene& s, double h);
+  void bild(Szene& s);
+  std::vector<V3> op(Szene& s, const std::vector<V3>& p);
+};
+
+// ---------------------------------------------------------------- measurement
+// sim/src/messung.rs:10-116
+double umfang_in_ebene(const Szene& s, V3 punkt, V3 normale);
+std::vector<std::pair<double, double>> dehnung_je_dreieck(const Szene& s);
+double nahtspalt(const Szene& s);
+double mittlere_geschwindigkeit(const Szene& s);
+V3 schwerpunkt(const Szene& s);
+
+}  // namespace orc

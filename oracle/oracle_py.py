@@ -1,0 +1,215 @@
+"""ORACLE (test infrastructure): ctypes access to the FP64 CPU restatement.
+
+Only tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py load
+this module, as the checker or as the timed CPU baseline. The product package
+never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from garmentcraft_b200 import _abi
+from garmentcraft_b200.szene import Szene
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libk3d_oracle.so")
+
+_lib = None
+
+
+def build() -> str:
+    """Compiles the oracle with its Makefile (g++ only, no GPU)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    L.orc_build_scene.argtypes = [C.POINTER(_abi.K3dPattern)]
+    L.orc_build_scene.restype = P
+    L.orc_built_scene_view.argtypes = [P, C.POINTER(_abi.K3dScene)]
+    L.orc_built_scene_counts.argtypes = [P, C.POINTER(C.c_int64)]
+    L.orc_built_scene_free.argtypes = [P]
+    L.orc_sim_create.argtypes = [C.POINTER(_abi.K3dScene), C.POINTER(_abi.K3dParams)]
+    L.orc_sim_create.restype = P
+    L.orc_sim_free.argtypes = [P]
+    L.orc_sim_frames.argtypes = [P, C.c_int32, C.POINTER(_abi.K3dStats)]
+    L.orc_sim_get_state.argtypes = [P, dp, dp]
+    L.orc_sim_set_state.argtypes = [P, dp, dp]
+    L.orc_sim_set_naht_ruhe.argtypes = [P, dp]
+    L.orc_sim_get_naht_ruhe.argtypes = [P, dp]
+    L.orc_sim_naht_kuerzen.argtypes = [P, C.c_double]
+    L.orc_sim_naht_offen.argtypes = [P]
+    L.orc_sim_set_reibung.argtypes = [P, C.c_double]
+    L.orc_sim_get_dv_warm.argtypes = [P, dp]
+    L.orc_sim_operator.argtypes = [P, dp, dp]
+    L.orc_sim_system.argtypes = [P, C.POINTER(_abi.K3dSystemReadback)]
+    L.orc_sim_solve.argtypes = [P, dp, C.POINTER(_abi.K3dCgResult)]
+    L.orc_sim_umfang.argtypes = [P, dp, dp]
+    L.orc_sim_umfang.restype = C.c_double
+    L.orc_sim_nahtspalt.argtypes = [P]
+    L.orc_sim_nahtspalt.restype = C.c_double
+    L.orc_sim_mittlere_geschwindigkeit.argtypes = [P]
+    L.orc_sim_mittlere_geschwindigkeit.restype = C.c_double
+    L.orc_sim_dehnung.argtypes = [P, dp]
+    L.orc_sim_schwerpunkt.argtypes = [P, dp]
+    L.orc_membran_bauen.argtypes = [dp, dp, dp, dp, dp]
+    L.orc_membran_bauen.restype = C.c_int32
+    L.orc_membran_eval.argtypes = [dp, dp, dp, dp, dp, dp, dp, dp]
+    L.orc_membran_mal_h.argtypes = [dp, dp, dp, dp]
+    L.orc_membran_diag.argtypes = [dp, dp, dp]
+    L.orc_psd2.argtypes = [C.c_double, C.c_double, C.c_double, dp]
+    L.orc_steifigkeit.argtypes = [C.c_double] * 4
+    L.orc_steifigkeit.restype = C.c_double
+    L.orc_cos2_sin2.argtypes = [dp, dp, dp]
+    L.orc_cos2_sin2.restype = C.c_int32
+    L.orc_dieder.argtypes = [dp, dp, dp]
+    L.orc_dieder.restype = C.c_int32
+    L.orc_winkel_fehler.argtypes = [C.c_double, C.c_double]
+    L.orc_winkel_fehler.restype = C.c_double
+    L.orc_m3_inv.argtypes = [dp, dp]
+    L.orc_faerbe.argtypes = [C.c_int64, C.c_int32, C.c_int64, C.POINTER(C.c_uint32),
+                             C.POINTER(C.c_uint32), C.POINTER(C.c_int64)]
+    L.orc_faerbe.restype = C.c_int64
+    L.orc_kontakt.argtypes = [C.POINTER(_abi.K3dBody), dp, C.c_double, dp, dp]
+    L.orc_kontakt.restype = C.c_int32
+    _lib = L
+    return L
+
+
+def _d(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def build_scene(muster, koerper=None) -> Szene:
+    """Szene::aus_netz restated (oracle side)."""
+    L = lib()
+    pat, keep = muster.to_c()
+    h = L.orc_build_scene(C.byref(pat))
+    view = _abi.K3dScene()
+    L.orc_built_scene_view(h, C.byref(view))
+    s = Szene.from_view(view, koerper)
+    s.param = muster.param
+    counts = (C.c_int64 * 6)()
+    L.orc_built_scene_counts(h, counts)
+    s.oracle_counts = dict(membran_entartet=counts[0], naht_biegung_ohne=counts[1],
+                           einhalte_kanten=counts[2], farben_abstand=counts[3],
+                           farben_biegung=counts[4], farben_naht=counts[5])
+    L.orc_built_scene_free(h)
+    del keep
+    return s
+
+
+class OracleSim:
+    """ImplizitCg with CpuLoeser over one scene (FP64, single thread)."""
+
+    def __init__(self, szene: Szene, params: _abi.K3dParams):
+        self.L = lib()
+        self.n = szene.n
+        self.n_naht = szene.naht_punkte.shape[0]
+        self.n_tri = szene.dreiecke.shape[0]
+        cs, keep = szene.to_c()
+        self.h = self.L.orc_sim_create(C.byref(cs), C.byref(params))
+        del keep
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.orc_sim_free(self.h)
+            self.h = None
+
+    def frames(self, n: int = 1) -> _abi.K3dStats:
+        st = _abi.K3dStats()
+        self.L.orc_sim_frames(self.h, n, C.byref(st))
+        return st
+
+    def state(self):
+        x = np.zeros((self.n, 3))
+        v = np.zeros((self.n, 3))
+        self.L.orc_sim_get_state(self.h, _d(x), _d(v))
+        return x, v
+
+    def set_state(self, x=None, v=None):
+        xa = f64(x) if x is not None else None
+        va = f64(v) if v is not None else None
+        self.L.orc_sim_set_state(self.h, _d(xa) if xa is not None else None,
+                                 _d(va) if va is not None else None)
+
+    def naht_ruhe(self):
+        r = np.zeros(self.n_naht)
+        self.L.orc_sim_get_naht_ruhe(self.h, _d(r))
+        return r
+
+    def set_naht_ruhe(self, r):
+        r = f64(r)
+        self.L.orc_sim_set_naht_ruhe(self.h, _d(r))
+
+    def naht_kuerzen(self, schritt):
+        self.L.orc_sim_naht_kuerzen(self.h, schritt)
+
+    def naht_offen(self):
+        self.L.orc_sim_naht_offen(self.h)
+
+    def set_reibung(self, mu):
+        self.L.orc_sim_set_reibung(self.h, mu)
+
+    def dv_warm(self):
+        dv = np.zeros((self.n, 3))
+        self.L.orc_sim_get_dv_warm(self.h, _d(dv))
+        return dv
+
+    def operator(self, p):
+        p = f64(p)
+        out = np.zeros((self.n, 3))
+        self.L.orc_sim_operator(self.h, _d(p), _d(out))
+        return out
+
+    def system(self):
+        n = self.n
+        out = dict(rhs=np.zeros((n, 3)), f=np.zeros((n, 3)), last=np.zeros((n, 3)),
+                   pinv=np.zeros((n, 3, 3)), normale=np.zeros((n, 3)), vn_soll=np.zeros(n),
+                   fest=np.zeros(n, dtype=np.uint8))
+        rb = _abi.K3dSystemReadback(_d(out["rhs"]), _d(out["f"]), _d(out["last"]), _d(out["pinv"]),
+                                    _d(out["normale"]), _d(out["vn_soll"]),
+                                    out["fest"].ctypes.data_as(C.POINTER(C.c_uint8)))
+        self.L.orc_sim_system(self.h, C.byref(rb))
+        return out
+
+    def solve(self, dv):
+        dv = f64(dv).copy()
+        res = _abi.K3dCgResult()
+        self.L.orc_sim_solve(self.h, _d(dv), C.byref(res))
+        return dv, res
+
+    def umfang(self, punkt, normale):
+        return self.L.orc_sim_umfang(self.h, _d(f64(punkt)), _d(f64(normale)))
+
+    def nahtspalt(self):
+        return self.L.orc_sim_nahtspalt(self.h)
+
+    def mittlere_geschwindigkeit(self):
+        return self.L.orc_sim_mittlere_geschwindigkeit(self.h)
+
+    def dehnung(self):
+        out = np.zeros((self.n_tri, 2))
+        self.L.orc_sim_dehnung(self.h, _d(out))
+        return out
+
+    def schwerpunkt(self):
+        out = np.zeros(3)
+        self.L.orc_sim_schwerpunkt(self.h, _d(out))
+        return out
