@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""Benchmark of the implicit cloth step: vertex-steps/s.
+
+Workload: a woven sheet of 257 x 257 vertices (66,049 points, 131,072
+membrane triangles, ~196k bending hinges), 1 x 1 m with +/-1 mm jitter,
+warp/weft/shear 2000/1000/50 N/m, dropped 0.5 m onto a sphere of radius
+0.3 m stored as a 128^3 signed-distance grid at 1 cm; friction 0.3,
+dt = 1/120 s, one implicit step per frame, CG cap 50, tolerance 1e-5.
+Synthetic, generated from a seed.
+
+A step is one implicit backward-Euler step (build, PCG with release pass,
+friction, integration) of the whole sheet. ``value`` is measured on the
+device-resident state with CUDA events around the step kernels, L2 flushed
+(256 MiB write) before every timed step; ``e2e`` is the same step through the
+public API (ImplizitCg.bild) with x and v copied from pinned host memory to
+the device and back every step.
+
+Multi-GPU: the step of one drape does not shard (a global Krylov solve), so
+``--gpus N`` runs N independent replicas, one per rank, with no collective on
+the data path; value = total vertex-steps / max over ranks of the time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "vertex-steps/s, mixed vs FP64 GPU at <=1e-4 rel pos err; backward/forward time"
+UNIT = "vertex-steps/s"
+
+
+def args_():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=240)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=257, help="vertices per side of the sheet")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-compare", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(n, s, extra=None):
+    cfg = {
+        "workload": f"sheet over sphere SDF, {n}x{n} vertices",
+        "vertices": int(s.n), "membranes": int(s.membran_punkte.shape[0]),
+        "bends": int(s.biegung_punkte.shape[0]), "springs": int(s.naht_punkte.shape[0]),
+        "sdf": "128^3 at 1 cm", "dt": "1/120", "substeps_per_frame": 1, "cg_max": 50, "cg_tol": 1e-5,
+        "l2": "flushed before every timed step (256 MiB write)", "parallelism": "replicas",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def make_scene(n, pinned=False):
+    from garmentcraft_b200 import synth
+    from garmentcraft_b200.implizit import build_scene
+    m, body = synth.sheet_over_sphere(n=n)
+    s = build_scene(m, [body])
+    if pinned:
+        import torch
+        for name in ("x", "v"):
+            a = getattr(s, name)
+            t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+            t.numpy()[:] = a
+            setattr(s, name, t.numpy())
+    return s
+
+
+def params(prec):
+    from garmentcraft_b200.params import ImplizitParameter
+    return ImplizitParameter(schritte_je_bild=1, cg_max=50, cg_toleranz=1e-5, precision=prec)
+
+
+def algorithmic_bytes(s, sw, steps, iters, solves):
+    """Minimal streamed bytes of the step (each datum once per pass), per
+    unit: per operator application N*10s + T*(12+21s) + B*(16+13s) +
+    S*(8+5s); per CG iteration the vector update N*31s; per step the build
+    and integration 48N + T*(12+21s) + B*(16+13s) + S*(8+5s) + 18s*N + 96N +
+    32N. Operator applications per step = CG iterations + 2 per solve (the
+    start residual and the release test)."""
+    N, T, B = s.n, s.membran_punkte.shape[0], s.biegung_punkte.shape[0]
+    S = s.naht_punkte.shape[0] + int(np.sum(s.membran_kante == 0))
+    elem = T * (12 + 21 * sw) + B * (16 + 13 * sw) + S * (8 + 5 * sw)
+    per_app = N * 10 * sw + elem
+    per_it = N * 31 * sw
+    build = 48 * N + elem + 18 * sw * N + 96 * N + 32 * N
+    return (iters + 2 * solves) * per_app + iters * per_it + steps * build
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id=None):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if bus_id:
+            cmd += ["-i", bus_id]
+        try:
+            self.p = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.split(", ") for l in open(self.f.name).read().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def read_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+def read_traffic():
+    """Per-launch DRAM bytes of the step kernel from the committed ncu summary."""
+    try:
+        txt = open(os.path.join(ROOT, "profiles", "step_kernel_sheet257.md")).read()
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
+        return float(m.group(1)) if m else None
+    except Exception:
+        return None
+
+
+def cpu_leg(n, warmup, seconds):
+    """The FP64 oracle (single thread, the reference's CPU path restated) on
+    the same workload: `warmup` steps, then steps until `seconds` pass."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    from garmentcraft_b200 import _abi
+    s = make_scene(n)
+    sim = oracle_py.OracleSim(s, params(_abi.K3D_FP64).to_c())
+    for _ in range(warmup):
+        sim.frames(1)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        sim.frames(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return {"value": s.n * steps / el, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{steps} steps after {warmup} warm-up steps of the same {n}x{n} drop, {el:.1f} s, "
+                      "FP64 C++ restatement of CpuLoeser/ImplizitCg, one thread"}
+
+
+def dev_timed(n, prec, warmup, steps, flush, torch):
+    """Device-resident steps: returns (ms list, stats sum, launches, scene, cg)."""
+    from garmentcraft_b200.implizit import ImplizitCg
+    s = make_scene(n)
+    cg = ImplizitCg(params(prec), device=torch.cuda.current_device())
+    cg.zustand_hochladen(s)
+    cg.bilder_auf_geraet(warmup)
+    torch.cuda.synchronize()
+    ms, its, solves = [], 0, 0
+    l0 = cg.kernel_starts()
+    for k in range(steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        st = cg.bilder_auf_geraet(1)
+        ms.append(cg.letzte_bild_ms())
+        its += st.cg_iterationen
+        solves += st.loesungen
+    launches = cg.kernel_starts() - l0
+    cg.zustand_lesen(s)
+    return ms, its, solves, launches, s, cg
+
+
+def e2e_timed(n, prec, warmup, steps, flush, torch):
+    from garmentcraft_b200.implizit import ImplizitCg
+    s = make_scene(n, pinned=True)
+    cg = ImplizitCg(params(prec), device=torch.cuda.current_device())
+    for _ in range(warmup):
+        cg.bild(s)
+    torch.cuda.synchronize()
+    tot = 0.0
+    for k in range(steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cg.bild(s)  # H2D x,v (pinned) -> step -> D2H x,v, synchronised
+        tot += time.perf_counter() - t0
+    return tot, s
+
+
+def main():
+    a = args_()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        s = make_scene(a.n)
+        cpu = cpu_leg(a.n, min(a.warmup, 3), max(10.0, min(120.0, a.cpu_seconds * 4)))
+        line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": a.gpus,
+                "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": workload_config(a.n, s, {"precision": "fp64 (CPU)"}),
+                "cpu_baseline": cpu,
+                "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import numpy as np_
+    globals()["np"] = np_
+    import torch
+    import torch.distributed as dist
+    from garmentcraft_b200 import _abi
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
+    bus = None
+    try:
+        pr = torch.cuda.get_device_properties(local)
+        bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+    except Exception:
+        pass
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(bus)
+    ms, its, solves, launches, s_mix, cg = dev_timed(a.n, _abi.K3D_MIXED, a.warmup, a.steps, flush, torch)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t_dev = sum(ms) / 1e3
+    if world > 1:
+        t = torch.tensor([t_dev], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev = float(t.item())
+    nv = s_mix.n
+    value = world * nv * a.steps / t_dev
+
+    # the same steps through the public API with host buffers
+    t_e2e, _ = e2e_timed(a.n, _abi.K3D_MIXED, a.warmup, a.steps, flush, torch)
+    if world > 1:
+        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = {"value": world * nv * a.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 48 * nv,
+           "d2h_bytes_per_step": 48 * nv + 144}
+
+    extra = {}
+    if not a.no_compare:
+        ms64, its64, solves64, _, s64, _ = dev_timed(a.n, _abi.K3D_FP64, a.warmup, a.steps, flush, torch)
+        t64 = sum(ms64) / 1e3
+        extra["fp64"] = {"value": nv * a.steps / t64, "ms_per_step": 1e3 * t64 / a.steps,
+                         "cg_iterations_per_step": its64 / a.steps}
+        # position error of the mixed form after 100 steps of the same drop
+        from garmentcraft_b200.implizit import ImplizitCg
+        sa, sb = make_scene(a.n), make_scene(a.n)
+        ImplizitCg(params(_abi.K3D_FP64)).bilder_resident(sa, 100)
+        ImplizitCg(params(_abi.K3D_MIXED)).bilder_resident(sb, 100)
+        d = float(np.linalg.norm(sa.x.max(0) - sa.x.min(0)))
+        err = float(np.max(np.linalg.norm(sa.x - sb.x, axis=1)) / d)
+        extra["mixed_vs_fp64"] = {"speedup": t64 / t_dev if world == 1 else None,
+                                  "rel_pos_err_after_100_steps": err,
+                                  "definition": "max_i |x_mixed - x_fp64| / bbox diagonal"}
+
+    peaks = read_peaks()
+    alg = algorithmic_bytes(s_mix, 4, a.steps, its, solves)
+    achieved = alg / (sum(ms) / 1e3) / 1e9
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    traffic = read_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": "measured" if peaks else "fallback",
+                "kernel": "k3d::step_kernel<float>",
+                "algorithmic_bytes_per_launch": alg / a.steps}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 * t_dev / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": workload_config(a.n, s_mix, {"precision": "mixed (FP32 operator, FP64 dots/scalars/state)"}),
+            "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
+            "cg_iterations_per_step": its / a.steps, "clocks": clk}
+    line.update(extra)
+    if rank == 0 and world == 1 and not a.no_cpu:
+        line["cpu_baseline"] = cpu_leg(a.n, min(a.warmup, 3), a.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    import numpy as np  # noqa: F401  (used by algorithmic_bytes)
+    main()

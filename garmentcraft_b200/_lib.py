@@ -1,0 +1,86 @@
+"""Loads the in-tree device library and declares the C ABI signatures.
+
+There is no fallback: if libklon3d_b200.so is missing, importing the solver
+raises. Build it with ``python -m garmentcraft_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_native", "libklon3d_b200.so")
+
+# every entry point include/klon3d_step.h declares
+EXPORTS = [
+    "k3d_abi_version", "k3d_params_default", "k3d_simparams_default", "k3d_build_scene",
+    "k3d_built_scene_view", "k3d_built_scene_free", "k3d_solver_create", "k3d_solver_destroy",
+    "k3d_last_error", "k3d_solver_name", "k3d_upload_scene", "k3d_frame", "k3d_frames_resident",
+    "k3d_upload_state", "k3d_download_state", "k3d_operator", "k3d_system_for", "k3d_solve",
+    "k3d_residual", "k3d_read_load", "k3d_last_frame_ms", "k3d_kernel_launches",
+]
+
+_lib = None
+
+
+class K3dError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{_abi.STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing; build it with `python -m garmentcraft_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    st = C.c_int
+    L.k3d_abi_version.restype = C.c_int32
+    L.k3d_params_default.argtypes = [C.POINTER(_abi.K3dParams)]
+    L.k3d_simparams_default.argtypes = [C.POINTER(_abi.K3dSimparams)]
+    L.k3d_build_scene.argtypes = [C.POINTER(_abi.K3dPattern), C.POINTER(P)]
+    L.k3d_build_scene.restype = st
+    L.k3d_built_scene_view.argtypes = [P, C.POINTER(_abi.K3dScene)]
+    L.k3d_built_scene_view.restype = st
+    L.k3d_built_scene_free.argtypes = [P]
+    L.k3d_solver_create.argtypes = [C.POINTER(_abi.K3dParams), C.c_int32]
+    L.k3d_solver_create.restype = P
+    L.k3d_solver_destroy.argtypes = [P]
+    L.k3d_last_error.argtypes = [P]
+    L.k3d_last_error.restype = C.c_char_p
+    L.k3d_solver_name.argtypes = [P]
+    L.k3d_solver_name.restype = C.c_char_p
+    L.k3d_upload_scene.argtypes = [P, C.POINTER(_abi.K3dScene)]
+    L.k3d_upload_scene.restype = st
+    L.k3d_frame.argtypes = [P, C.POINTER(_abi.K3dScene), C.POINTER(_abi.K3dStats)]
+    L.k3d_frame.restype = st
+    L.k3d_frames_resident.argtypes = [P, C.c_int32, C.POINTER(_abi.K3dStats)]
+    L.k3d_frames_resident.restype = st
+    L.k3d_upload_state.argtypes = [P, dp, dp]
+    L.k3d_upload_state.restype = st
+    L.k3d_download_state.argtypes = [P, dp, dp]
+    L.k3d_download_state.restype = st
+    L.k3d_operator.argtypes = [P, dp, dp]
+    L.k3d_operator.restype = st
+    L.k3d_system_for.argtypes = [P, C.POINTER(_abi.K3dSystemReadback)]
+    L.k3d_system_for.restype = st
+    L.k3d_solve.argtypes = [P, dp, C.POINTER(_abi.K3dCgResult)]
+    L.k3d_solve.restype = st
+    L.k3d_residual.argtypes = [P, dp, dp]
+    L.k3d_residual.restype = st
+    L.k3d_read_load.argtypes = [P, dp]
+    L.k3d_read_load.restype = st
+    L.k3d_last_frame_ms.argtypes = [P]
+    L.k3d_last_frame_ms.restype = C.c_double
+    L.k3d_kernel_launches.argtypes = [P]
+    L.k3d_kernel_launches.restype = C.c_int64
+    if L.k3d_abi_version() != 1:
+        raise RuntimeError("libklon3d_b200.so ABI version mismatch")
+    _lib = L
+    return L

@@ -1,0 +1,56 @@
+"""Builds the device library libklon3d_b200.so in-tree with nvcc for sm_100a.
+
+Usage: python -m garmentcraft_b200.build
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "_native")
+LIB = os.path.join(OUT_DIR, "libklon3d_b200.so")
+SOURCES = ["k3d_step.cu", "k3d_host.cpp", "scene_build.cpp"]
+HEADERS = ["k3d_step.h", "k3d_device.cuh", "scene_build.h"]
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
+    "-Xcompiler", "-O3", "-Xcompiler", "-ffp-contract=off", "-cudart", "shared",
+]
+
+
+def _stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps.append(os.path.join(HERE, "..", "include", "klon3d_step.h"))
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not _stale():
+        return LIB
+    os.makedirs(OUT_DIR, exist_ok=True)
+    srcs = []
+    for f in SOURCES:
+        p = os.path.join(CSRC, f)
+        if f.endswith(".cpp"):
+            srcs += ["-x", "cu", p]
+        else:
+            srcs.append(p)
+    cmd = [NVCC, *FLAGS, "-o", LIB + ".tmp", *srcs]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True, cwd=CSRC)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

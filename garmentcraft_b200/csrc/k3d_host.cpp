@@ -1,0 +1,757 @@
+// Host side of the C ABI (include/klon3d_step.h): the solver handle, the
+// device layout of a scene, and the frame loop (Rechenweg::bild,
+// sim/src/implizit.rs:1042-1057) around the persistent step kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/klon3d_step.h"
+#include "k3d_step.h"
+#include "scene_build.h"
+
+using namespace k3d;
+
+namespace {
+
+// One device allocation carved into 256-byte aligned pieces.
+struct Arena {
+  char* base = nullptr;
+  size_t size = 0, used = 0;
+  template <typename T>
+  T* take(size_t count) {
+    size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+    if (bytes == 0) bytes = 256;
+    T* p = reinterpret_cast<T*>(base + used);
+    used += bytes;
+    return p;
+  }
+};
+
+
+}  // namespace
+
+struct k3d_solver {
+  k3d_params p{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err, name;
+  int blocks = 0;
+  size_t rsize = 8;
+  bool uploaded = false, first_step = true;
+  int64_t n = 0, nt = 0, nb = 0, ns = 0;
+  double boden = 0.0;
+  k3d_simparams sim{};
+  std::vector<k3d_body> bodies;         // frame-start bodies as last given
+  std::vector<void*> sdf_dev;           // device copies of SDF grids
+  std::vector<int64_t> seam_slot;       // spring index of each seam, -1 if not streamed
+  std::vector<double2> s_kl_host;
+  int64_t launches = 0;
+  double last_ms = 0.0;
+  Arena arena;
+  StepArgs a{};  // device pointers and constants; per-launch fields are set before each launch
+  double* d_pin = nullptr;  // probe input (3N)
+  double* d_pout = nullptr; // probe output (3N)
+};
+
+static k3d_status fail(k3d_solver* h, k3d_status st, const std::string& msg) {
+  if (h) h->err = msg;
+  return st;
+}
+static k3d_status cuda_fail(k3d_solver* h, cudaError_t e, const char* what) {
+  return fail(h, K3D_DEVICE_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define K3D_CUDA(h, call)                                   \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return cuda_fail((h), e_, #call); \
+  } while (0)
+
+// Writable aliases of the scene constants, for the upload.
+struct Carve {
+  double *masse, *w, *kabst, *reib;
+  uint8_t* frei;
+  uint32_t *off_t, *off_b, *off_s, *ent_t, *ent_b, *ent_s;
+  uint4 *m_idx, *b_idx, *s_idx;
+  double4 *m_r, *m_basis, *m_mat;
+  void *m_rin, *m_kgA;
+  double2 *b_kr, *s_kl;
+};
+
+// Assigns every device array of the handle from the arena (base may be null
+// to measure the size).
+static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t S, size_t et, size_t eb, size_t es,
+                  Carve& cv) {
+  const size_t R = h->rsize;
+  StepArgs& a = h->a;
+  std::memset(&a, 0, sizeof(a));
+  A.used = 0;
+  a.x = A.take<double>(3 * N);
+  a.v = A.take<double>(3 * N);
+  a.dv = A.take<double>(3 * N);
+  a.b = A.take<double>(3 * N);
+  a.vk = A.take<double>(3 * N);
+  a.load = A.take<double>(3 * N);
+  a.nrm_d = A.take<double>(3 * N);
+  h->d_pin = A.take<double>(3 * N);
+  h->d_pout = A.take<double>(3 * N);
+  a.fnk = A.take<double>(N);
+  a.vn_soll = A.take<double>(N);
+  a.masse = cv.masse = A.take<double>(N);
+  a.w = cv.w = A.take<double>(N);
+  a.kabst = cv.kabst = A.take<double>(N);
+  a.reib = cv.reib = A.take<double>(N);
+  a.frei = cv.frei = A.take<uint8_t>(N);
+  a.c = A.take<char>(4 * N * R);
+  a.r = A.take<char>(3 * N * R);
+  a.z = A.take<char>(3 * N * R);
+  a.ap = A.take<char>(3 * N * R);
+  a.nrm = A.take<char>(3 * N * R);
+  a.pinv = A.take<char>(6 * N * R);
+  a.md = A.take<char>(N * R);
+  a.off_t = cv.off_t = A.take<uint32_t>(N + 1);
+  a.off_b = cv.off_b = A.take<uint32_t>(N + 1);
+  a.off_s = cv.off_s = A.take<uint32_t>(N + 1);
+  a.ent_t = cv.ent_t = A.take<uint32_t>(et);
+  a.ent_b = cv.ent_b = A.take<uint32_t>(eb);
+  a.ent_s = cv.ent_s = A.take<uint32_t>(es);
+  a.m_idx = cv.m_idx = A.take<uint4>(T);
+  a.m_r = cv.m_r = A.take<double4>(T);
+  a.m_basis = cv.m_basis = A.take<double4>(T);
+  a.m_mat = cv.m_mat = A.take<double4>(T);
+  a.m_bc = A.take<double4>(3 * T);
+  a.m_lc = A.take<double4>(3 * T);
+  a.m_dc = A.take<double>(24 * T);
+  a.m_f1w = A.take<char>(4 * T * R);
+  a.m_f2w = A.take<char>(4 * T * R);
+  a.m_kgB = A.take<char>(4 * T * R);
+  a.m_rin = cv.m_rin = A.take<char>(4 * T * R);
+  a.m_kgA = cv.m_kgA = A.take<char>(4 * T * R);
+  a.m_out = A.take<char>(12 * T * R);
+  a.b_idx = cv.b_idx = A.take<uint4>(B);
+  a.b_kr = cv.b_kr = A.take<double2>(B);
+  a.b_bc = A.take<double4>(4 * B);
+  a.b_grad = A.take<char>(16 * B * R);
+  a.b_s = A.take<char>(B * R);
+  a.s_idx = cv.s_idx = A.take<uint4>(S);
+  a.s_kl = cv.s_kl = A.take<double2>(S);
+  a.s_bc = A.take<double4>(S);
+  a.s_lc = A.take<double4>(S);
+  a.s_dq = A.take<char>(4 * S * R);
+  a.s_out = A.take<char>(4 * S * R);
+  a.s_k = A.take<char>(S * R);
+  a.sync = A.take<SyncState>(1);
+  a.partials = A.take<double>(size_t(4) * h->blocks);
+  a.stats = A.take<long long>(ST_COUNT);
+  a.stat_rest_max = A.take<double>(2);
+}
+
+extern "C" {
+
+int32_t k3d_abi_version(void) { return K3D_ABI_VERSION; }
+
+void k3d_params_default(k3d_params* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->schritte_je_bild = 5;
+  o->cg_max = 50;
+  o->cg_toleranz = 1e-5;
+  o->naht_k = 500.0;
+  o->kontakt_rand = 1e-4;
+  o->normalkraft_aus_last = 0;
+  o->durchstoss_pruefen = 1;
+  o->selbstkollision = 0;
+  o->precision = K3D_FP64;
+  o->selbst_zusatzdicke = 2.5e-3;
+  o->selbst_steifigkeit = 1e-3;
+}
+
+void k3d_simparams_default(k3d_simparams* o) {
+  if (!o) return;
+  o->bild_dt = 1.0 / 60.0;
+  o->schwerkraft[0] = 0.0;
+  o->schwerkraft[1] = 0.0;
+  o->schwerkraft[2] = -9.81;
+  o->daempfung = 0.0;
+}
+
+// ------------------------------------------------------------ scene builder
+k3d_status k3d_build_scene(const k3d_pattern* pattern, k3d_built_scene** out) {
+  if (!pattern || !out) return K3D_BAD_ARGUMENT;
+  auto* b = new k3d_built_scene;
+  k3d_status st = build_scene_impl(pattern, b->s);
+  if (st != K3D_OK) {
+    delete b;
+    *out = nullptr;
+    return st;
+  }
+  *out = b;
+  return K3D_OK;
+}
+k3d_status k3d_built_scene_view(k3d_built_scene* built, k3d_scene* out) {
+  if (!built || !out) return K3D_BAD_ARGUMENT;
+  built_scene_view(built->s, out);
+  return K3D_OK;
+}
+void k3d_built_scene_free(k3d_built_scene* built) { delete built; }
+
+// ------------------------------------------------------------ solver
+k3d_solver* k3d_solver_create(const k3d_params* params, int32_t device) {
+  auto* h = new k3d_solver;
+  if (params)
+    h->p = *params;
+  else
+    k3d_params_default(&h->p);
+  h->device = device;
+  h->rsize = h->p.precision == K3D_MIXED ? 4 : 8;
+  h->name = h->p.precision == K3D_MIXED ? "B200 (f32/f64)" : "B200 (f64)";
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+    h->err = "no CUDA device available";
+    return h;  // every later call reports K3D_DEVICE_ERROR
+  }
+  h->blocks = step_grid_blocks(h->p.precision == K3D_MIXED ? 1 : 0, device);
+  if (h->blocks <= 0) h->err = "cannot size the cooperative grid";
+  return h;
+}
+
+static void release_device(k3d_solver* h) {
+  if (h->arena.base) cudaFree(h->arena.base);
+  h->arena = Arena{};
+  for (void* p : h->sdf_dev) cudaFree(p);
+  h->sdf_dev.clear();
+  h->uploaded = false;
+}
+
+void k3d_solver_destroy(k3d_solver* h) {
+  if (!h) return;
+  if (h->stream) {
+    cudaStreamSynchronize(h->stream);
+    release_device(h);
+    cudaStreamDestroy(h->stream);
+  }
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  delete h;
+}
+
+const char* k3d_last_error(const k3d_solver* h) { return h ? h->err.c_str() : "null handle"; }
+const char* k3d_solver_name(const k3d_solver* h) { return h ? h->name.c_str() : ""; }
+double k3d_last_frame_ms(const k3d_solver* h) { return h ? h->last_ms : 0.0; }
+int64_t k3d_kernel_launches(const k3d_solver* h) { return h ? h->launches : 0; }
+
+// kg = d2U/dg2 (kontinuum.rs:391-406), symmetric (00, 11, 22, 01, 02, 12)
+static void kg_host(const double* ri, double fl, double kx, double ky, double sx, double sy, double ek, double es,
+                    double g, double kg[6]) {
+  (void)ri;
+  const double a[3] = {kx * kx, ky * ky, kx * ky}, b[3] = {sx * sx, sy * sy, sx * sy},
+               c[3] = {kx * sx, ky * sy, 0.5 * (kx * sy + ky * sx)};
+  const double* v[3] = {a, b, c};
+  const double wt[3] = {0.25 * ek, 0.25 * es, g};
+  for (int q = 0; q < 6; ++q) kg[q] = 0.0;
+  for (int t = 0; t < 3; ++t) {
+    double s = fl * wt[t];
+    kg[0] += s * v[t][0] * v[t][0];
+    kg[1] += s * v[t][1] * v[t][1];
+    kg[2] += s * v[t][2] * v[t][2];
+    kg[3] += s * v[t][0] * v[t][1];
+    kg[4] += s * v[t][0] * v[t][2];
+    kg[5] += s * v[t][1] * v[t][2];
+  }
+}
+
+static k3d_status validate(const k3d_scene* s) {
+  if (!s || s->n_punkte < 0 || s->n_abstand < 0 || s->n_naht < 0 || s->n_biegung < 0 || s->n_membran < 0)
+    return K3D_BAD_ARGUMENT;
+  const int64_t n = s->n_punkte;
+  if (n > 0 && (!s->x || !s->v || !s->masse || !s->w || !s->kollisionsabstand || !s->reibung)) return K3D_BAD_ARGUMENT;
+  if (n >= int64_t(1) << 31) return K3D_BAD_ARGUMENT;
+  auto chk = [&](const uint32_t* p, int64_t cnt) {
+    for (int64_t i = 0; i < cnt; ++i)
+      if (int64_t(p[i]) >= n) return false;
+    return true;
+  };
+  if (s->n_abstand && (!s->abstand_punkte || !s->abstand_ruhe || !s->abstand_nachgiebigkeit ||
+                       !chk(s->abstand_punkte, 2 * s->n_abstand)))
+    return K3D_BAD_ARGUMENT;
+  if (s->n_naht && (!s->naht_punkte || !s->naht_ruhe || !chk(s->naht_punkte, 2 * s->n_naht))) return K3D_BAD_ARGUMENT;
+  if (s->n_biegung && (!s->biegung_punkte || !s->biegung_ruhe || !s->biegung_nachgiebigkeit ||
+                       !chk(s->biegung_punkte, 4 * s->n_biegung)))
+    return K3D_BAD_ARGUMENT;
+  if (s->n_membran && (!s->membran_punkte || !s->membran_flaeche || !s->membran_ruhe_inv || !s->membran_kette ||
+                       !s->membran_schuss || !s->membran_steif || !chk(s->membran_punkte, 3 * s->n_membran)))
+    return K3D_BAD_ARGUMENT;
+  if (s->n_koerper < 0 || s->n_koerper > kMaxBodies || (s->n_koerper && !s->koerper)) return K3D_BAD_ARGUMENT;
+  for (int b = 0; b < s->n_koerper; ++b) {
+    const k3d_body& k = s->koerper[b];
+    if (k.art == K3D_BODY_SDF_GRID) {
+      if (!k.sdf || k.dims[0] < 2 || k.dims[1] < 2 || k.dims[2] < 2 || !(k.spacing > 0.0)) return K3D_BAD_ARGUMENT;
+    } else if (k.art != K3D_BODY_CYLINDER) {
+      return K3D_BAD_ARGUMENT;
+    }
+  }
+  return K3D_OK;
+}
+
+k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
+  if (!h) return K3D_BAD_ARGUMENT;
+  if (!h->stream || h->blocks <= 0) return fail(h, K3D_DEVICE_ERROR, h->err.empty() ? "no device" : h->err);
+  if (validate(s) != K3D_OK) return fail(h, K3D_BAD_ARGUMENT, "invalid scene (null array, index or body)");
+  K3D_CUDA(h, cudaSetDevice(h->device));
+  K3D_CUDA(h, cudaStreamSynchronize(h->stream));
+  release_device(h);
+  const int64_t n = s->n_punkte, nt = s->n_membran, nb = s->n_biegung;
+  const size_t R = h->rsize;
+
+  // springs: pattern edges that carry their own stiffness, then seams (implizit.rs:725-772)
+  std::vector<uint4> s_idx;
+  std::vector<double2> s_kl;
+  for (int64_t e = 0; e < s->n_abstand; ++e) {
+    const bool membran = s->membran_kante && s->membran_kante[e];
+    if (membran) continue;
+    double k = 1.0 / s->abstand_nachgiebigkeit[e];
+    if (k == 0.0) continue;
+    s_idx.push_back(make_uint4(s->abstand_punkte[2 * e], s->abstand_punkte[2 * e + 1], 0u, 0u));
+    s_kl.push_back(make_double2(k, s->abstand_ruhe[e]));
+  }
+  h->seam_slot.assign(size_t(s->n_naht), -1);
+  if (h->p.naht_k != 0.0) {
+    for (int64_t e = 0; e < s->n_naht; ++e) {
+      h->seam_slot[e] = int64_t(s_idx.size());
+      s_idx.push_back(make_uint4(s->naht_punkte[2 * e], s->naht_punkte[2 * e + 1], 1u, 0u));
+      s_kl.push_back(make_double2(h->p.naht_k, s->naht_ruhe[e]));
+    }
+  }
+  const int64_t ns = int64_t(s_idx.size());
+  h->s_kl_host = s_kl;
+
+  // point -> element corner lists, in element order
+  std::vector<uint32_t> off_t(n + 1, 0), off_b(n + 1, 0), off_s(n + 1, 0);
+  for (int64_t t = 0; t < nt; ++t)
+    for (int k = 0; k < 3; ++k) off_t[s->membran_punkte[3 * t + k] + 1]++;
+  for (int64_t b = 0; b < nb; ++b)
+    for (int k = 0; k < 4; ++k) off_b[s->biegung_punkte[4 * b + k] + 1]++;
+  for (int64_t q = 0; q < ns; ++q) {
+    off_s[s_idx[q].x + 1]++;
+    off_s[s_idx[q].y + 1]++;
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    off_t[i + 1] += off_t[i];
+    off_b[i + 1] += off_b[i];
+    off_s[i + 1] += off_s[i];
+  }
+  std::vector<uint32_t> ent_t(off_t[n]), ent_b(off_b[n]), ent_s(off_s[n]);
+  {
+    std::vector<uint32_t> ft(off_t.begin(), off_t.end() - 1), fb(off_b.begin(), off_b.end() - 1),
+        fs(off_s.begin(), off_s.end() - 1);
+    for (int64_t t = 0; t < nt; ++t)
+      for (int k = 0; k < 3; ++k) ent_t[ft[s->membran_punkte[3 * t + k]]++] = uint32_t(3 * t + k);
+    for (int64_t b = 0; b < nb; ++b)
+      for (int k = 0; k < 4; ++k) ent_b[fb[s->biegung_punkte[4 * b + k]]++] = uint32_t(4 * b + k);
+    for (int64_t q = 0; q < ns; ++q) {
+      ent_s[fs[s_idx[q].x]++] = uint32_t(2 * q);
+      ent_s[fs[s_idx[q].y]++] = uint32_t(2 * q + 1);
+    }
+  }
+
+  // element constants
+  std::vector<uint4> m_idx(nt), b_idx(nb);
+  std::vector<double4> m_r(nt), m_basis(nt), m_mat(nt);
+  std::vector<double2> b_kr(nb);
+  std::vector<char> m_rin(size_t(nt) * 4 * R), m_kgA(size_t(nt) * 4 * R);
+  for (int64_t t = 0; t < nt; ++t) {
+    const uint32_t* p = s->membran_punkte + 3 * t;
+    m_idx[t] = make_uint4(p[0], p[1], p[2], 0u);
+    const double* ri = s->membran_ruhe_inv + 4 * t;
+    m_r[t] = make_double4(ri[0], ri[1], ri[2], ri[3]);
+    const double* kt = s->membran_kette + 2 * t;
+    const double* sc = s->membran_schuss + 2 * t;
+    m_basis[t] = make_double4(kt[0], kt[1], sc[0], sc[1]);
+    const double* st = s->membran_steif + 3 * t;
+    m_mat[t] = make_double4(s->membran_flaeche[t], st[0], st[1], st[2]);
+    double kg[6];
+    kg_host(ri, s->membran_flaeche[t], kt[0], kt[1], sc[0], sc[1], st[0], st[1], st[2], kg);
+    const double rin[4] = {ri[0], ri[1], ri[2], ri[3]}, kga[4] = {kg[0], kg[1], kg[2], kg[3]};
+    if (R == 8) {
+      std::memcpy(&m_rin[size_t(t) * 32], rin, 32);
+      std::memcpy(&m_kgA[size_t(t) * 32], kga, 32);
+    } else {
+      float fr[4], fk[4];
+      for (int q = 0; q < 4; ++q) {
+        fr[q] = float(rin[q]);
+        fk[q] = float(kga[q]);
+      }
+      std::memcpy(&m_rin[size_t(t) * 16], fr, 16);
+      std::memcpy(&m_kgA[size_t(t) * 16], fk, 16);
+    }
+  }
+  for (int64_t b = 0; b < nb; ++b) {
+    const uint32_t* p = s->biegung_punkte + 4 * b;
+    b_idx[b] = make_uint4(p[0], p[1], p[2], p[3]);
+    b_kr[b] = make_double2(1.0 / s->biegung_nachgiebigkeit[b], s->biegung_ruhe[b]);
+  }
+  std::vector<uint8_t> frei(n);
+  double msum = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    frei[i] = s->w[i] > 0.0 ? 1 : 0;
+    msum += s->masse[i];
+  }
+  h->boden = msum * 1e-18;
+
+  // one allocation: measure the layout with a null base, then carve it
+  const size_t N = size_t(n), T = size_t(nt), B = size_t(nb), S = size_t(ns);
+  Carve cv;
+  Arena probe;
+  carve(h, probe, N, T, B, S, ent_t.size(), ent_b.size(), ent_s.size(), cv);
+  void* base = nullptr;
+  K3D_CUDA(h, cudaMalloc(&base, probe.used));
+  h->arena.base = static_cast<char*>(base);
+  h->arena.size = probe.used;
+  carve(h, h->arena, N, T, B, S, ent_t.size(), ent_b.size(), ent_s.size(), cv);
+  Arena& A = h->arena;
+  StepArgs& a = h->a;
+  if (A.used > A.size) return fail(h, K3D_DEVICE_ERROR, "arena overflow");
+  K3D_CUDA(h, cudaMemsetAsync(A.base, 0, A.used, h->stream));
+
+  cudaStream_t st = h->stream;
+  auto up = [&](void* dst, const void* src, size_t b) -> cudaError_t {
+    if (b == 0) return cudaSuccess;
+    return cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, st);
+  };
+  K3D_CUDA(h, up(a.x, s->x, 24 * N));
+  K3D_CUDA(h, up(a.v, s->v, 24 * N));
+  K3D_CUDA(h, up(cv.masse, s->masse, 8 * N));
+  K3D_CUDA(h, up(cv.w, s->w, 8 * N));
+  K3D_CUDA(h, up(cv.kabst, s->kollisionsabstand, 8 * N));
+  K3D_CUDA(h, up(cv.reib, s->reibung, 8 * N));
+  K3D_CUDA(h, up(cv.frei, frei.data(), N));
+  K3D_CUDA(h, up(cv.off_t, off_t.data(), 4 * (N + 1)));
+  K3D_CUDA(h, up(cv.off_b, off_b.data(), 4 * (N + 1)));
+  K3D_CUDA(h, up(cv.off_s, off_s.data(), 4 * (N + 1)));
+  K3D_CUDA(h, up(cv.ent_t, ent_t.data(), 4 * ent_t.size()));
+  K3D_CUDA(h, up(cv.ent_b, ent_b.data(), 4 * ent_b.size()));
+  K3D_CUDA(h, up(cv.ent_s, ent_s.data(), 4 * ent_s.size()));
+  K3D_CUDA(h, up(cv.m_idx, m_idx.data(), 16 * T));
+  K3D_CUDA(h, up(cv.m_r, m_r.data(), 32 * T));
+  K3D_CUDA(h, up(cv.m_basis, m_basis.data(), 32 * T));
+  K3D_CUDA(h, up(cv.m_mat, m_mat.data(), 32 * T));
+  K3D_CUDA(h, up(cv.m_rin, m_rin.data(), m_rin.size()));
+  K3D_CUDA(h, up(cv.m_kgA, m_kgA.data(), m_kgA.size()));
+  K3D_CUDA(h, up(cv.b_idx, b_idx.data(), 16 * B));
+  K3D_CUDA(h, up(cv.b_kr, b_kr.data(), 16 * B));
+  K3D_CUDA(h, up(cv.s_idx, s_idx.data(), 16 * S));
+  K3D_CUDA(h, up(cv.s_kl, s_kl.data(), 16 * S));
+
+  // bodies; SDF grids go to the device once here
+  h->bodies.assign(s->koerper, s->koerper + s->n_koerper);
+  for (int b = 0; b < s->n_koerper; ++b) {
+    const k3d_body& k = s->koerper[b];
+    void* d = nullptr;
+    if (k.art == K3D_BODY_SDF_GRID) {
+      size_t cnt = size_t(k.dims[0]) * k.dims[1] * k.dims[2];
+      K3D_CUDA(h, cudaMalloc(&d, 4 * cnt));
+      K3D_CUDA(h, up(d, k.sdf, 4 * cnt));
+    }
+    h->sdf_dev.push_back(d);
+  }
+  K3D_CUDA(h, cudaStreamSynchronize(st));
+
+  a.n = n;
+  a.nt = nt;
+  a.nb = nb;
+  a.ns = ns;
+  h->n = n;
+  h->nt = nt;
+  h->nb = nb;
+  h->ns = ns;
+  h->sim = s->param;
+  h->uploaded = true;
+  h->first_step = true;
+  h->err.clear();
+  return K3D_OK;
+}
+
+}  // extern "C"
+
+// Fills the per-launch fields and launches one step kernel.
+static k3d_status launch(k3d_solver* h, int mode, double t_bodies, bool need_load) {
+  StepArgs& a = h->a;
+  const int sub = std::max(h->p.schritte_je_bild, 1);
+  a.mode = mode;
+  a.h = h->sim.bild_dt / double(sub);
+  a.daempf = h->sim.daempfung;
+  for (int k = 0; k < 3; ++k) a.g[k] = h->sim.schwerkraft[k];
+  a.tol = h->p.cg_toleranz;
+  a.cg_max = h->p.cg_max;
+  a.kontakt_rand = h->p.kontakt_rand;
+  a.boden = h->boden;
+  a.normal_aus_last = h->p.normalkraft_aus_last;
+  a.need_load = (need_load || h->p.normalkraft_aus_last) ? 1 : 0;
+  a.first_step = (mode == MODE_STEP && h->first_step) ? 1 : 0;
+  a.n_bodies = int(h->bodies.size());
+  for (int b = 0; b < a.n_bodies; ++b) {
+    const k3d_body& k = h->bodies[b];
+    Body& d = a.bodies[b];
+    d.art = k.art;
+    for (int q = 0; q < 3; ++q) {
+      d.dims[q] = k.dims[q];
+      d.punkt[q] = k.punkt[q] + k.geschwindigkeit[q] * t_bodies;  // Koerper::verschoben (koerper.rs:122-133)
+      d.achse[q] = k.achse[q];
+      d.vel[q] = k.geschwindigkeit[q];
+      d.ursprung[q] = k.ursprung[q];
+    }
+    d.radius = k.radius;
+    d.spacing = k.spacing;
+    d.sdf = static_cast<const float*>(h->sdf_dev[b]);
+  }
+  cudaError_t e = launch_step(a, h->p.precision == K3D_MIXED ? 1 : 0, h->blocks, h->stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
+  h->launches++;
+  if (mode == MODE_STEP) h->first_step = false;
+  return K3D_OK;
+}
+
+static k3d_status check_sync(k3d_solver* h) {
+  K3D_CUDA(h, cudaStreamSynchronize(h->stream));
+  SyncState ss;
+  K3D_CUDA(h, cudaMemcpy(&ss, h->a.sync, sizeof(ss), cudaMemcpyDeviceToHost));
+  if (ss.error != 0) {
+    cudaMemset(h->a.sync, 0, sizeof(SyncState));
+    return fail(h, K3D_TIMEOUT, "a device barrier wait ran out of time");
+  }
+  return K3D_OK;
+}
+
+static k3d_status read_stats(k3d_solver* h, k3d_stats* out) {
+  long long st[ST_COUNT];
+  double rm[2];
+  K3D_CUDA(h, cudaMemcpy(st, h->a.stats, sizeof(st), cudaMemcpyDeviceToHost));
+  K3D_CUDA(h, cudaMemcpy(rm, h->a.stat_rest_max, sizeof(rm), cudaMemcpyDeviceToHost));
+  if (out) {
+    std::memset(out, 0, sizeof(*out));
+    out->cg_iterationen = st[ST_CG_ITERATIONS];
+    out->loesungen = st[ST_SOLVES];
+    out->nicht_konvergiert = st[ST_UNCONVERGED];
+    out->kontakte = st[ST_CONTACTS];
+    out->haftend = st[ST_STICKING];
+    out->freigegeben = st[ST_RELEASED];
+    out->rest_max = rm[0];
+  }
+  if (st[ST_NONFINITE] > 0) return fail(h, K3D_NON_FINITE, "non-finite position or velocity after the step");
+  return K3D_OK;
+}
+
+static k3d_status reset_stats(k3d_solver* h) {
+  K3D_CUDA(h, cudaMemsetAsync(h->a.stats, 0, sizeof(long long) * ST_COUNT, h->stream));
+  K3D_CUDA(h, cudaMemsetAsync(h->a.stat_rest_max, 0, sizeof(double) * 2, h->stream));
+  return K3D_OK;
+}
+
+static k3d_status ready(k3d_solver* h) {
+  if (!h) return K3D_BAD_ARGUMENT;
+  if (!h->uploaded) return fail(h, K3D_BAD_ARGUMENT, "no scene uploaded");
+  K3D_CUDA(h, cudaSetDevice(h->device));
+  return K3D_OK;
+}
+
+// One frame of substeps on the resident state.
+static k3d_status frame_device(k3d_solver* h) {
+  const int sub = std::max(h->p.schritte_je_bild, 1);
+  const double hs = h->sim.bild_dt / double(sub);
+  for (int k = 0; k < sub; ++k) {
+    k3d_status st = launch(h, MODE_STEP, double(k + 1) * hs, false);
+    if (st != K3D_OK) return st;
+  }
+  // the bodies end the frame moved by v * bild_dt (implizit.rs:1047-1054)
+  for (auto& b : h->bodies)
+    for (int q = 0; q < 3; ++q) b.punkt[q] += b.geschwindigkeit[q] * h->sim.bild_dt;
+  return K3D_OK;
+}
+
+extern "C" {
+
+k3d_status k3d_upload_state(k3d_solver* h, const double* x, const double* v) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if (x) K3D_CUDA(h, cudaMemcpyAsync(h->a.x, x, 24 * size_t(h->n), cudaMemcpyHostToDevice, h->stream));
+  if (v) K3D_CUDA(h, cudaMemcpyAsync(h->a.v, v, 24 * size_t(h->n), cudaMemcpyHostToDevice, h->stream));
+  K3D_CUDA(h, cudaStreamSynchronize(h->stream));
+  return K3D_OK;
+}
+
+k3d_status k3d_download_state(k3d_solver* h, double* x, double* v) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if (x) K3D_CUDA(h, cudaMemcpyAsync(x, h->a.x, 24 * size_t(h->n), cudaMemcpyDeviceToHost, h->stream));
+  if (v) K3D_CUDA(h, cudaMemcpyAsync(v, h->a.v, 24 * size_t(h->n), cudaMemcpyDeviceToHost, h->stream));
+  K3D_CUDA(h, cudaStreamSynchronize(h->stream));
+  return K3D_OK;
+}
+
+k3d_status k3d_frame(k3d_solver* h, k3d_scene* s, k3d_stats* stats) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if (!s || s->n_punkte != h->n || !s->x || !s->v) return fail(h, K3D_BAD_ARGUMENT, "scene does not match the upload");
+  if (s->n_koerper != int32_t(h->bodies.size())) return fail(h, K3D_BAD_ARGUMENT, "body count changed; upload again");
+  // state, seam rest lengths and body positions as the caller holds them now
+  K3D_CUDA(h, cudaMemcpyAsync(h->a.x, s->x, 24 * size_t(h->n), cudaMemcpyHostToDevice, h->stream));
+  K3D_CUDA(h, cudaMemcpyAsync(h->a.v, s->v, 24 * size_t(h->n), cudaMemcpyHostToDevice, h->stream));
+  bool seams = false;
+  for (size_t e = 0; e < h->seam_slot.size() && s->naht_ruhe; ++e)
+    if (h->seam_slot[e] >= 0 && h->s_kl_host[h->seam_slot[e]].y != s->naht_ruhe[e] &&
+        !(std::isnan(s->naht_ruhe[e]))) {
+      h->s_kl_host[h->seam_slot[e]].y = s->naht_ruhe[e];
+      seams = true;
+    }
+  if (seams)
+    K3D_CUDA(h, cudaMemcpyAsync(const_cast<double2*>(h->a.s_kl), h->s_kl_host.data(), 16 * h->s_kl_host.size(),
+                                cudaMemcpyHostToDevice, h->stream));
+  for (int b = 0; b < s->n_koerper; ++b)
+    for (int q = 0; q < 3; ++q) {
+      h->bodies[b].punkt[q] = s->koerper[b].punkt[q];
+      h->bodies[b].geschwindigkeit[q] = s->koerper[b].geschwindigkeit[q];
+    }
+  h->sim = s->param;
+  st = reset_stats(h);
+  if (st != K3D_OK) return st;
+  K3D_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+  st = frame_device(h);
+  if (st != K3D_OK) return st;
+  K3D_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+  K3D_CUDA(h, cudaMemcpyAsync(s->x, h->a.x, 24 * size_t(h->n), cudaMemcpyDeviceToHost, h->stream));
+  K3D_CUDA(h, cudaMemcpyAsync(s->v, h->a.v, 24 * size_t(h->n), cudaMemcpyDeviceToHost, h->stream));
+  st = check_sync(h);
+  if (st != K3D_OK) return st;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  h->last_ms = ms;
+  s->zeit += s->param.bild_dt;
+  return read_stats(h, stats);
+}
+
+k3d_status k3d_frames_resident(k3d_solver* h, int32_t n_frames, k3d_stats* stats) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if (n_frames < 0) return fail(h, K3D_BAD_ARGUMENT, "negative frame count");
+  st = reset_stats(h);
+  if (st != K3D_OK) return st;
+  K3D_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+  for (int f = 0; f < n_frames; ++f) {
+    st = frame_device(h);
+    if (st != K3D_OK) return st;
+  }
+  K3D_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+  st = check_sync(h);
+  if (st != K3D_OK) return st;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  h->last_ms = ms;
+  return read_stats(h, stats);
+}
+
+k3d_status k3d_operator(k3d_solver* h, const double* p, double* out) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if (!p || !out) return fail(h, K3D_BAD_ARGUMENT, "null vector");
+  K3D_CUDA(h, cudaMemcpyAsync(h->d_pin, p, 24 * size_t(h->n), cudaMemcpyHostToDevice, h->stream));
+  h->a.p_in = h->d_pin;
+  h->a.p_out = h->d_pout;
+  st = launch(h, MODE_OPERATOR, 0.0, false);
+  if (st != K3D_OK) return st;
+  K3D_CUDA(h, cudaMemcpyAsync(out, h->d_pout, 24 * size_t(h->n), cudaMemcpyDeviceToHost, h->stream));
+  return check_sync(h);
+}
+
+k3d_status k3d_system_for(k3d_solver* h, k3d_system_readback* rb) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if (!rb) return fail(h, K3D_BAD_ARGUMENT, "null readback");
+  h->a.p_out = rb->f ? h->d_pout : nullptr;
+  st = launch(h, MODE_SYSTEM, 0.0, true);
+  if (st != K3D_OK) return st;
+  st = check_sync(h);
+  if (st != K3D_OK) return st;
+  const size_t N = size_t(h->n);
+  auto down = [&](void* dst, const void* src, size_t b) { return cudaMemcpy(dst, src, b, cudaMemcpyDeviceToHost); };
+  if (rb->rhs) K3D_CUDA(h, down(rb->rhs, h->a.b, 24 * N));
+  if (rb->f) K3D_CUDA(h, down(rb->f, h->d_pout, 24 * N));
+  if (rb->last) K3D_CUDA(h, down(rb->last, h->a.load, 24 * N));
+  std::vector<double> nrm(3 * N);
+  K3D_CUDA(h, down(nrm.data(), h->a.nrm_d, 24 * N));
+  if (rb->normale) std::memcpy(rb->normale, nrm.data(), 24 * N);
+  if (rb->vn_soll) K3D_CUDA(h, down(rb->vn_soll, h->a.vn_soll, 8 * N));
+  if (rb->fest)
+    for (size_t i = 0; i < N; ++i)
+      rb->fest[i] = (nrm[3 * i] != 0.0 || nrm[3 * i + 1] != 0.0 || nrm[3 * i + 2] != 0.0) ? 1 : 0;
+  if (rb->pinv) {
+    std::vector<double> P(6 * N);
+    if (h->rsize == 8) {
+      K3D_CUDA(h, down(P.data(), h->a.pinv, 48 * N));
+    } else {
+      std::vector<float> Pf(6 * N);
+      K3D_CUDA(h, down(Pf.data(), h->a.pinv, 24 * N));
+      for (size_t q = 0; q < 6 * N; ++q) P[q] = Pf[q];
+    }
+    for (size_t i = 0; i < N; ++i) {
+      const double* p = &P[6 * i];
+      double* o = rb->pinv + 9 * i;
+      o[0] = p[0]; o[1] = p[3]; o[2] = p[4];
+      o[3] = p[3]; o[4] = p[1]; o[5] = p[5];
+      o[6] = p[4]; o[7] = p[5]; o[8] = p[2];
+    }
+  }
+  return K3D_OK;
+}
+
+k3d_status k3d_solve(k3d_solver* h, double* dv_inout, k3d_cg_result* out) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if (!dv_inout) return fail(h, K3D_BAD_ARGUMENT, "null dv");
+  K3D_CUDA(h, cudaMemcpyAsync(h->a.dv, dv_inout, 24 * size_t(h->n), cudaMemcpyHostToDevice, h->stream));
+  st = reset_stats(h);
+  if (st != K3D_OK) return st;
+  st = launch(h, MODE_SOLVE, 0.0, false);
+  if (st != K3D_OK) return st;
+  K3D_CUDA(h, cudaMemcpyAsync(dv_inout, h->a.dv, 24 * size_t(h->n), cudaMemcpyDeviceToHost, h->stream));
+  st = check_sync(h);
+  if (st != K3D_OK) return st;
+  long long sv[ST_COUNT];
+  double rm[2];
+  K3D_CUDA(h, cudaMemcpy(sv, h->a.stats, sizeof(sv), cudaMemcpyDeviceToHost));
+  K3D_CUDA(h, cudaMemcpy(rm, h->a.stat_rest_max, sizeof(rm), cudaMemcpyDeviceToHost));
+  if (out) {
+    out->iterationen = sv[ST_LAST_ITERATIONS];
+    out->nicht_konvergiert = sv[ST_UNCONVERGED] ? 1 : 0;
+    out->breakdown = sv[ST_BREAKDOWNS] ? 1 : 0;
+    out->rest = rm[0];
+  }
+  return sv[ST_UNCONVERGED] ? K3D_NOT_CONVERGED : K3D_OK;
+}
+
+k3d_status k3d_residual(k3d_solver* h, const double* dv, double* out) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if (!dv || !out) return fail(h, K3D_BAD_ARGUMENT, "null vector");
+  K3D_CUDA(h, cudaMemcpyAsync(h->d_pin, dv, 24 * size_t(h->n), cudaMemcpyHostToDevice, h->stream));
+  h->a.p_in = h->d_pin;
+  h->a.p_out = h->d_pout;
+  st = launch(h, MODE_RESIDUAL, 0.0, false);
+  if (st != K3D_OK) return st;
+  K3D_CUDA(h, cudaMemcpyAsync(out, h->d_pout, 24 * size_t(h->n), cudaMemcpyDeviceToHost, h->stream));
+  return check_sync(h);
+}
+
+k3d_status k3d_read_load(k3d_solver* h, double* out) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if (!out) return fail(h, K3D_BAD_ARGUMENT, "null vector");
+  K3D_CUDA(h, cudaMemcpy(out, h->a.load, 24 * size_t(h->n), cudaMemcpyDeviceToHost));
+  return K3D_OK;
+}
+
+}  // extern "C"

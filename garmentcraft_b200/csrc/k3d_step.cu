@@ -1,0 +1,850 @@
+// The implicit backward-Euler step on the device: one persistent cooperative
+// kernel per substep.
+//
+//   build (elements)  -> per-corner force/Hv/diag records, operator records
+//   build (points)    -> rhs b, block-Jacobi inverse, contact set
+//   PCG (implizit.rs:370-426), up to two passes with the release test
+//   (implizit.rs:908-943), then friction and integration (:957-1014).
+//
+// Every phase is a grid-stride loop over elements or points, separated by a
+// grid barrier. Sums are deterministic: points gather their incident element
+// corners in a fixed order (no float atomics), and grid reductions add the
+// per-block partials in block order. The barrier waits are bounded by a
+// wall-clock limit; on expiry the kernel records K3D_TIMEOUT and every block
+// returns.
+#include <cfloat>
+#include <cstdint>
+
+#include "k3d_device.cuh"
+#include "k3d_step.h"
+
+namespace k3d {
+
+// ------------------------------------------------------------ barrier + reductions
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_relaxed_i32(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+constexpr uint64_t kBarrierLimitNs = 4000000000ull;  // 4 s per barrier wait
+constexpr int kMaxRed = 4;
+
+struct Shared {
+  double red[kMaxRed][32];
+  double res[kMaxRed];
+  unsigned gen;
+  int last;
+  int err;
+};
+
+// Block sum of NV values, fixed order (warp xor tree, then warps in order).
+// Valid in thread 0 only.
+template <int NV>
+__device__ __forceinline__ void block_sum(Shared& sh, double (&v)[NV]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double x = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) sh.red[k][warp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += sh.red[k][w];
+      v[k] = s;
+    }
+  }
+  __syncthreads();
+}
+
+// Grid barrier with an optional reduction of NV doubles (NV = 0: plain
+// barrier). The last block to arrive adds the block partials in block order
+// and publishes the totals before releasing the others. Returns false if any
+// block recorded an error (every block then leaves the kernel).
+template <int NV>
+__device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV : 1]) {
+  SyncState* s = a.sync;
+  if constexpr (NV > 0) {
+    double loc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) loc[k] = v[k];
+    block_sum<NV>(sh, loc);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < NV; ++k) a.partials[k * gridDim.x + blockIdx.x] = loc[k];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sh.gen = ld_acquire_u32(&s->gen);
+    __threadfence();
+    unsigned prev = atomicAdd(&s->count, 1u);
+    sh.last = (prev == gridDim.x - 1) ? 1 : 0;
+    if (sh.last) __threadfence();
+  }
+  __syncthreads();
+  if (sh.last) {
+    if constexpr (NV > 0) {
+      double loc[NV];
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        double x = 0.0;
+        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) x += __ldcg(&a.partials[k * gridDim.x + b]);
+        loc[k] = x;
+      }
+      block_sum<NV>(sh, loc);
+      if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) s->result[k] = loc[k];
+      }
+    }
+    if (threadIdx.x == 0) {
+      atomicExch(&s->count, 0u);
+      __threadfence();
+      st_release_u32(&s->gen, sh.gen + 1);
+    }
+  } else if (threadIdx.x == 0) {
+    const uint64_t t0 = globaltimer();
+    while (ld_acquire_u32(&s->gen) == sh.gen) {
+      if (ld_relaxed_i32(&s->error) != 0) break;
+      if (globaltimer() - t0 > kBarrierLimitNs) {
+        atomicCAS(&s->error, 0, K3D_STATUS_TIMEOUT);
+        break;
+      }
+      __nanosleep(64);
+    }
+    fence_acq_rel();
+  }
+  if (threadIdx.x == 0) {
+    sh.err = ld_relaxed_i32(&s->error);
+    if constexpr (NV > 0) {
+#pragma unroll
+      for (int k = 0; k < NV; ++k) sh.res[k] = __ldcg(&s->result[k]);
+    }
+  }
+  __syncthreads();
+  if constexpr (NV > 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = sh.res[k];
+  }
+  return sh.err == 0;
+}
+
+__device__ __forceinline__ bool barrier(const StepArgs& a, Shared& sh) {
+  double none[1] = {0.0};
+  return grid_sync<0>(a, sh, none);
+}
+
+#define K3D_FOR(i, n) \
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < (n); i += int64_t(gridDim.x) * blockDim.x)
+
+// ------------------------------------------------------------ typed views
+template <typename R>
+struct View {
+  R4<R>* c;
+  R *r, *z, *ap, *pinv, *nrm, *md;
+  R4<R>*m_f1w, *m_f2w, *m_kgB, *m_out;
+  const R4<R>*m_rin, *m_kgA;
+  R4<R>* b_grad;
+  R* b_s;
+  R4<R>* s_dq;
+  R* s_k;
+  R4<R>* s_out;
+  __device__ explicit View(const StepArgs& a)
+      : c((R4<R>*)a.c), r((R*)a.r), z((R*)a.z), ap((R*)a.ap), pinv((R*)a.pinv), nrm((R*)a.nrm), md((R*)a.md),
+        m_f1w((R4<R>*)a.m_f1w), m_f2w((R4<R>*)a.m_f2w), m_kgB((R4<R>*)a.m_kgB), m_out((R4<R>*)a.m_out),
+        m_rin((const R4<R>*)a.m_rin), m_kgA((const R4<R>*)a.m_kgA), b_grad((R4<R>*)a.b_grad), b_s((R*)a.b_s),
+        s_dq((R4<R>*)a.s_dq), s_k((R*)a.s_k), s_out((R4<R>*)a.s_out) {}
+};
+
+__device__ __forceinline__ double4 ldg4(const double4* p) {
+  const double2 lo = __ldg(reinterpret_cast<const double2*>(p)), hi = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+
+__device__ __forceinline__ MembranC membran_c(const StepArgs& a, int64_t t) {
+  const double4 r = ldg4(&a.m_r[t]), b = ldg4(&a.m_basis[t]), m = ldg4(&a.m_mat[t]);
+  MembranC o;
+  o.r[0] = r.x;
+  o.r[1] = r.y;
+  o.r[2] = r.z;
+  o.r[3] = r.w;
+  o.kx = b.x;
+  o.ky = b.y;
+  o.sx = b.z;
+  o.sy = b.w;
+  o.fl = m.x;
+  o.ek = m.y;
+  o.es = m.z;
+  o.g = m.w;
+  return o;
+}
+
+// ------------------------------------------------------------ build: elements
+// implizit.rs:725-844 and kontinuum.rs, in FP64. Writes, per element corner,
+// the contribution to (f - h H v) and, if asked, to the load, plus the
+// membrane diagonal blocks; and the per-step operator records in precision R.
+template <typename R>
+__device__ void build_elements(const StepArgs& a, const View<R>& vw) {
+  const double h = a.h;
+  K3D_FOR(t, a.nt) {
+    const uint4 id = __ldg(&a.m_idx[t]);
+    const MembranC m = membran_c(a, t);
+    const D3 p0 = ld3(a.x, id.x), p1 = ld3(a.x, id.y), p2 = ld3(a.x, id.z);
+    const D3 e1 = p1 - p0, e2 = p2 - p0;
+    const D3 f1 = e1 * m.r[0] + e2 * m.r[2];
+    const D3 f2 = e1 * m.r[1] + e2 * m.r[3];
+    D3 ba, bb, bc;
+    basis3(m, ba, bb, bc);
+    const D3 g = d3(dot(f1, f1), dot(f2, f2), 2.0 * dot(f1, f2));
+    const D3 e = d3(0.5 * (dot(ba, g) - 1.0), 0.5 * (dot(bb, g) - 1.0), 0.5 * dot(bc, g));
+    const D3 du = du_dg(m, ba, bb, bc, e);
+    D3 F[3];
+    kraefte(m.r, f1, f2, du, F);
+    const D3 dz = du_dg(m, ba, bb, bc, d3(fmax(e.x, 0.0), fmax(e.y, 0.0), e.z));
+    const D3 w = psd2(dz.x, dz.y, dz.z);
+    double kg[6];
+    kg_sym(m, kg);
+    // H v (FP64) with the same record the operator uses
+    R4<double> rf1 = {f1.x, f1.y, f1.z, w.x}, rf2 = {f2.x, f2.y, f2.z, w.y};
+    R4<double> rr = {m.r[0], m.r[1], m.r[2], m.r[3]};
+    R4<double> ka = {kg[0], kg[1], kg[2], kg[3]}, kb = {kg[4], kg[5], w.z, 0.0};
+    R4<double> vv[3], hv[3];
+    const uint32_t ids[3] = {id.x, id.y, id.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      D3 q = ld3(a.v, ids[k]);
+      vv[k] = {q.x, q.y, q.z, 0.0};
+    }
+    membran_hv<double>(rf1, rf2, rr, ka, kb, vv, hv);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      a.m_bc[3 * t + k] = make_double4(F[k].x - hv[k].x * h, F[k].y - hv[k].y * h, F[k].z - hv[k].z * h, 0.0);
+    if (a.need_load) {
+      D3 L[3];
+      kraefte(m.r, f1, f2, dz, L);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a.m_lc[3 * t + k] = make_double4(L[k].x, L[k].y, L[k].z, 0.0);
+    }
+    // diagonal blocks J_k^T kg J_k + s_kk I (kontinuum.rs:675-708)
+    const D3 k1 = coef1(m.r), k2 = coef2(m.r);
+    const double c1[3] = {k1.x, k1.y, k1.z}, c2[3] = {k2.x, k2.y, k2.z};
+    const double K[3][3] = {{kg[0], kg[3], kg[4]}, {kg[3], kg[1], kg[5]}, {kg[4], kg[5], kg[2]}};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const D3 j[3] = {f1 * (2.0 * c1[k]), f2 * (2.0 * c2[k]), f1 * (2.0 * c2[k]) + f2 * (2.0 * c1[k])};
+      D3 u[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) u[i] = j[0] * K[i][0] + j[1] * K[i][1] + j[2] * K[i][2];
+      const double s = 2.0 * (w.x * c1[k] * c1[k] + w.y * c2[k] * c2[k] + 2.0 * w.z * c1[k] * c2[k]);
+      double* dc = a.m_dc + 8 * (3 * t + k);
+      dc[0] = j[0].x * u[0].x + j[1].x * u[1].x + j[2].x * u[2].x + s;
+      dc[1] = j[0].y * u[0].y + j[1].y * u[1].y + j[2].y * u[2].y + s;
+      dc[2] = j[0].z * u[0].z + j[1].z * u[1].z + j[2].z * u[2].z + s;
+      dc[3] = j[0].x * u[0].y + j[1].x * u[1].y + j[2].x * u[2].y;
+      dc[4] = j[0].x * u[0].z + j[1].x * u[1].z + j[2].x * u[2].z;
+      dc[5] = j[0].y * u[0].z + j[1].y * u[1].z + j[2].y * u[2].z;
+    }
+    vw.m_f1w[t] = {R(f1.x), R(f1.y), R(f1.z), R(w.x)};
+    vw.m_f2w[t] = {R(f2.x), R(f2.y), R(f2.z), R(w.y)};
+    vw.m_kgB[t] = {R(kg[4]), R(kg[5]), R(w.z), R(0)};
+  }
+  K3D_FOR(b, a.nb) {
+    const uint4 id = __ldg(&a.b_idx[b]);
+    const double2 kr = __ldg(&a.b_kr[b]);
+    const uint32_t ids[4] = {id.x, id.y, id.z, id.w};
+    D3 gr[4];
+    double theta = 0.0;
+    if (!dieder(ld3(a.x, id.x), ld3(a.x, id.y), ld3(a.x, id.z), ld3(a.x, id.w), theta, gr)) {
+      theta = 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) gr[q] = d3(0, 0, 0);
+    }
+    const double fehler = winkel_fehler(theta, kr.y);
+    double gv = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) gv += dot(gr[q], ld3(a.v, ids[q]));
+    const double sb = -kr.x * fehler - h * (kr.x * gv);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      a.b_bc[4 * b + q] = make_double4(gr[q].x * sb, gr[q].y * sb, gr[q].z * sb, 0.0);
+      vw.b_grad[4 * b + q] = {R(gr[q].x), R(gr[q].y), R(gr[q].z), R(kr.x)};
+    }
+  }
+  K3D_FOR(s, a.ns) {
+    const uint4 id = __ldg(&a.s_idx[s]);
+    const double2 kl = a.s_kl[s];
+    const double k = kl.x;
+    const D3 d = ld3(a.x, id.y) - ld3(a.x, id.x);
+    D3 F, n;
+    double quer;
+    bool zug = false;
+    if (id.z == 0) {  // pattern edge with its own stiffness (implizit.rs:742-752)
+      const double l = fmax(norm(d), 1e-12);
+      n = d * (1.0 / l);
+      F = n * (k * (l - kl.y));
+      quer = fmax(1.0 - kl.y / l, 0.0);
+      zug = l > kl.y;
+    } else {  // seam spring (implizit.rs:763-771)
+      const double l = norm(d);
+      const double l0 = isfinite(kl.y) ? kl.y : l;
+      if (l0 > 0.0 && l > 1e-12) {
+        F = d * (k * (l - l0) / l);
+        n = d * (1.0 / l);
+        quer = fmax(1.0 - l0 / l, 0.0);
+      } else {
+        F = d * k;
+        n = d3(0, 0, 0);
+        quer = 1.0;
+      }
+    }
+    // H v with d = v_i - v_j (implizit.rs:193-197); end i gets +, end j gets -
+    const D3 dv = ld3(a.v, id.x) - ld3(a.v, id.y);
+    const D3 bd = (n * (dot(n, dv) * (1.0 - quer)) + dv * quer) * k;
+    a.s_bc[s] = make_double4(F.x - bd.x * h, F.y - bd.y * h, F.z - bd.z * h, 0.0);
+    if (a.need_load) a.s_lc[s] = zug ? make_double4(F.x, F.y, F.z, 0.0) : make_double4(0, 0, 0, 0);
+    vw.s_dq[s] = {R(n.x), R(n.y), R(n.z), R(quer)};
+    vw.s_k[s] = R(k);
+  }
+}
+
+// ------------------------------------------------------------ build: points
+// implizit.rs:722-723 (gravity, damping), :872-894 (contacts, rhs, pinv).
+template <typename R>
+__device__ void build_points(const StepArgs& a, const View<R>& vw, double& held) {
+  const double h = a.h, h2 = a.h * a.h;
+  held = 0.0;
+  K3D_FOR(i, a.n) {
+    const double m = a.masse[i];
+    const D3 vi = ld3(a.v, uint32_t(i));
+    D3 acc = d3(a.g[0] * m, a.g[1] * m, a.g[2] * m) - vi * (a.daempf * m);
+    D3 load = d3(a.g[0] * m, a.g[1] * m, a.g[2] * m);
+    double D[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t e = __ldg(&a.off_t[i]); e < __ldg(&a.off_t[i + 1]); ++e) {
+      const uint32_t q = __ldg(&a.ent_t[e]);
+      const double4 bc = a.m_bc[q];
+      acc = acc + d3(bc.x, bc.y, bc.z);
+      const double* dc = a.m_dc + 8 * size_t(q);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) D[k] += dc[k];
+      if (a.need_load) {
+        const double4 lc = a.m_lc[q];
+        load = load + d3(lc.x, lc.y, lc.z);
+      }
+    }
+    for (uint32_t e = __ldg(&a.off_b[i]); e < __ldg(&a.off_b[i + 1]); ++e) {
+      const uint32_t q = __ldg(&a.ent_b[e]);
+      const double4 bc = a.b_bc[q];
+      acc = acc + d3(bc.x, bc.y, bc.z);
+      const R4<R> gq = vw.b_grad[q];
+      const double gx = gq.x, gy = gq.y, gz = gq.z, k = gq.w;
+      D[0] += k * gx * gx;
+      D[1] += k * gy * gy;
+      D[2] += k * gz * gz;
+      D[3] += k * gx * gy;
+      D[4] += k * gx * gz;
+      D[5] += k * gy * gz;
+    }
+    for (uint32_t e = __ldg(&a.off_s[i]); e < __ldg(&a.off_s[i + 1]); ++e) {
+      const uint32_t q = __ldg(&a.ent_s[e]);
+      const uint32_t s = q >> 1;
+      const double sg = (q & 1u) ? -1.0 : 1.0;
+      const double4 bc = a.s_bc[s];
+      acc = acc + d3(bc.x, bc.y, bc.z) * sg;
+      if (a.need_load) {
+        const double4 lc = a.s_lc[s];
+        load = load + d3(lc.x, lc.y, lc.z) * sg;
+      }
+      const R4<R> dq = vw.s_dq[s];
+      const double k = vw.s_k[s], nx = dq.x, ny = dq.y, nz = dq.z, qu = dq.w;
+      const double kn = k * (1.0 - qu), kq = k * qu;
+      D[0] += kq + kn * nx * nx;
+      D[1] += kq + kn * ny * ny;
+      D[2] += kq + kn * nz * nz;
+      D[3] += kn * nx * ny;
+      D[4] += kn * nx * nz;
+      D[5] += kn * ny * nz;
+    }
+    st3(a.b, uint32_t(i), acc * h);
+    if (a.need_load) st3(a.load, uint32_t(i), load);
+    const double mdi = m * (1.0 + h * a.daempf);
+    double A[6] = {mdi + h2 * D[0], mdi + h2 * D[1], mdi + h2 * D[2], h2 * D[3], h2 * D[4], h2 * D[5]};
+    double P[6];
+    m3_inv_sym(A, P);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) vw.pinv[6 * i + k] = R(P[k]);
+    vw.md[i] = R(mdi);
+    // contact set: the last body that reports a contact wins (implizit.rs:873-883)
+    D3 nrm = d3(0, 0, 0);
+    double vn_soll = 0.0;
+    D3 vb = d3(0, 0, 0);
+    bool fest = false;
+    if (a.frei[i]) {
+      const D3 xi = ld3(a.x, uint32_t(i));
+      for (int kb = 0; kb < a.n_bodies; ++kb) {
+        D3 nn;
+        double tiefe;
+        if (kontakt(a.bodies[kb], xi, a.kabst[i] + a.kontakt_rand, nn, tiefe)) {
+          const D3 bv = d3(a.bodies[kb].vel[0], a.bodies[kb].vel[1], a.bodies[kb].vel[2]);
+          nrm = nn;
+          vn_soll = (tiefe - a.kontakt_rand) / h + dot(bv, nn);
+          vb = bv;
+          fest = true;
+        }
+      }
+    }
+    st3(a.nrm_d, uint32_t(i), nrm);
+    vw.nrm[3 * i] = R(nrm.x);
+    vw.nrm[3 * i + 1] = R(nrm.y);
+    vw.nrm[3 * i + 2] = R(nrm.z);
+    a.vn_soll[i] = vn_soll;
+    st3(a.vk, uint32_t(i), vb);
+    a.fnk[i] = 0.0;
+    if (fest) held += 1.0;
+    if (a.first_step) st3(a.dv, uint32_t(i), d3(a.g[0] * h, a.g[1] * h, a.g[2] * h));
+  }
+}
+
+// ------------------------------------------------------------ operator A p
+// Per element: the corner products with the direction c (implizit.rs:185-221).
+template <typename R>
+__device__ void apply_elements(const StepArgs& a, const View<R>& vw) {
+  K3D_FOR(t, a.nt) {
+    const uint4 id = __ldg(&a.m_idx[t]);
+    const R4<R> d[3] = {vw.c[id.x], vw.c[id.y], vw.c[id.z]};
+    R4<R> out[3];
+    membran_hv<R>(vw.m_f1w[t], vw.m_f2w[t], vw.m_rin[t], vw.m_kgA[t], vw.m_kgB[t], d, out);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) vw.m_out[3 * t + k] = out[k];
+  }
+  K3D_FOR(b, a.nb) {
+    const uint4 id = __ldg(&a.b_idx[b]);
+    const R4<R> g0 = vw.b_grad[4 * b], g1 = vw.b_grad[4 * b + 1], g2 = vw.b_grad[4 * b + 2], g3 = vw.b_grad[4 * b + 3];
+    const R4<R> c0 = vw.c[id.x], c1 = vw.c[id.y], c2 = vw.c[id.z], c3 = vw.c[id.w];
+    const R gp = g0.x * c0.x + g0.y * c0.y + g0.z * c0.z + g1.x * c1.x + g1.y * c1.y + g1.z * c1.z + g2.x * c2.x +
+                 g2.y * c2.y + g2.z * c2.z + g3.x * c3.x + g3.y * c3.y + g3.z * c3.z;
+    vw.b_s[b] = g0.w * gp;
+  }
+  K3D_FOR(s, a.ns) {
+    const uint4 id = __ldg(&a.s_idx[s]);
+    const R4<R> dq = vw.s_dq[s];
+    const R k = vw.s_k[s];
+    const R4<R> ci = vw.c[id.x], cj = vw.c[id.y];
+    const R dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
+    const R nd = (dq.x * dx + dq.y * dy + dq.z * dz) * (R(1) - dq.w);
+    vw.s_out[s] = {k * (dq.x * nd + dx * dq.w), k * (dq.y * nd + dy * dq.w), k * (dq.z * nd + dz * dq.w), R(0)};
+  }
+}
+
+// H p at point i from the element corner products.
+template <typename R>
+__device__ __forceinline__ void gather_h(const StepArgs& a, const View<R>& vw, int64_t i, R& hx, R& hy, R& hz) {
+  R x = 0, y = 0, z = 0;
+  for (uint32_t e = __ldg(&a.off_t[i]); e < __ldg(&a.off_t[i + 1]); ++e) {
+    const R4<R> o = vw.m_out[__ldg(&a.ent_t[e])];
+    x += o.x;
+    y += o.y;
+    z += o.z;
+  }
+  for (uint32_t e = __ldg(&a.off_b[i]); e < __ldg(&a.off_b[i + 1]); ++e) {
+    const uint32_t q = __ldg(&a.ent_b[e]);
+    const R4<R> g = vw.b_grad[q];
+    const R s = vw.b_s[q >> 2];
+    x += g.x * s;
+    y += g.y * s;
+    z += g.z * s;
+  }
+  for (uint32_t e = __ldg(&a.off_s[i]); e < __ldg(&a.off_s[i + 1]); ++e) {
+    const uint32_t q = __ldg(&a.ent_s[e]);
+    const R4<R> o = vw.s_out[q >> 1];
+    if (q & 1u) {
+      x -= o.x;
+      y -= o.y;
+      z -= o.z;
+    } else {
+      x += o.x;
+      y += o.y;
+      z += o.z;
+    }
+  }
+  hx = x;
+  hy = y;
+  hz = z;
+}
+
+template <typename R>
+__device__ __forceinline__ void filt(const R* nrm, int64_t i, R& x, R& y, R& z) {
+  const R nx = nrm[3 * i], ny = nrm[3 * i + 1], nz = nrm[3 * i + 2];
+  const R d = x * nx + y * ny + z * nz;
+  x -= nx * d;
+  y -= ny * d;
+  z -= nz * d;
+}
+
+template <typename R>
+__device__ __forceinline__ void pmul(const R* P, int64_t i, R x, R y, R z, R& ox, R& oy, R& oz) {
+  const R p0 = P[6 * i], p1 = P[6 * i + 1], p2 = P[6 * i + 2], p3 = P[6 * i + 3], p4 = P[6 * i + 4],
+          p5 = P[6 * i + 5];
+  ox = p0 * x + p3 * y + p4 * z;
+  oy = p3 * x + p1 * y + p5 * z;
+  oz = p4 * x + p5 * y + p2 * z;
+}
+
+// c = (R) dv
+template <typename R>
+__device__ void dv_to_c(const StepArgs& a, const View<R>& vw) {
+  K3D_FOR(i, a.n) {
+    const D3 d = ld3(a.dv, uint32_t(i));
+    vw.c[i] = {R(d.x), R(d.y), R(d.z), R(0)};
+  }
+}
+
+// ------------------------------------------------------------ PCG
+// implizit.rs:370-426. Returns false on a barrier error.
+template <typename R>
+__device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& iters, bool& unconverged,
+                    bool& breakdown, double& rest) {
+  const double h2 = a.h * a.h;
+  // start: pinned points 0, held points get their normal target
+  K3D_FOR(i, a.n) {
+    D3 d = ld3(a.dv, uint32_t(i));
+    if (!a.frei[i]) {
+      d = d3(0, 0, 0);
+    } else {
+      const D3 n = ld3(a.nrm_d, uint32_t(i));
+      if (n.x != 0.0 || n.y != 0.0 || n.z != 0.0) {
+        const double soll = a.vn_soll[i] - dot(ld3(a.v, uint32_t(i)), n);
+        d = (d - n * dot(d, n)) + n * soll;
+      }
+    }
+    st3(a.dv, uint32_t(i), d);
+    vw.c[i] = {R(d.x), R(d.y), R(d.z), R(0)};
+  }
+  if (!barrier(a, sh)) return false;
+  apply_elements<R>(a, vw);
+  if (!barrier(a, sh)) return false;
+  double red[2] = {0.0, 0.0};
+  K3D_FOR(i, a.n) {
+    R hx, hy, hz;
+    gather_h<R>(a, vw, i, hx, hy, hz);
+    const R4<R> ci = vw.c[i];
+    const R m = vw.md[i];
+    R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, cx = 0, cy = 0, cz = 0;
+    if (a.frei[i]) {
+      const R ax = m * ci.x + R(h2) * hx, ay = m * ci.y + R(h2) * hy, az = m * ci.z + R(h2) * hz;
+      const D3 b = ld3(a.b, uint32_t(i));
+      rx = R(b.x - double(ax));
+      ry = R(b.y - double(ay));
+      rz = R(b.z - double(az));
+      filt<R>(vw.nrm, i, rx, ry, rz);
+      R fx = R(b.x), fy = R(b.y), fz = R(b.z);
+      filt<R>(vw.nrm, i, fx, fy, fz);
+      R px, py, pz;
+      pmul<R>(vw.pinv, i, fx, fy, fz, px, py, pz);
+      red[1] += double(fx) * double(px) + double(fy) * double(py) + double(fz) * double(pz);
+      pmul<R>(vw.pinv, i, rx, ry, rz, zx, zy, zz);
+      cx = zx;
+      cy = zy;
+      cz = zz;
+      filt<R>(vw.nrm, i, cx, cy, cz);
+      red[0] += double(rx) * double(cx) + double(ry) * double(cy) + double(rz) * double(cz);
+    }
+    vw.r[3 * i] = rx;
+    vw.r[3 * i + 1] = ry;
+    vw.r[3 * i + 2] = rz;
+    vw.z[3 * i] = zx;
+    vw.z[3 * i + 1] = zy;
+    vw.z[3 * i + 2] = zz;
+    vw.c[i] = {cx, cy, cz, R(0)};
+  }
+  if (!grid_sync<2>(a, sh, red)) return false;
+  double delta = red[0];
+  const double bb = red[1];
+  const double ziel = fmax(a.tol * a.tol * fmax(bb, delta), a.boden);
+  int64_t it = 0;
+  breakdown = false;
+  while (delta > ziel && it < a.cg_max) {
+    apply_elements<R>(a, vw);
+    if (!barrier(a, sh)) return false;
+    double ca[1] = {0.0};
+    K3D_FOR(i, a.n) {
+      R ax = 0, ay = 0, az = 0;
+      const R4<R> ci = vw.c[i];
+      if (a.frei[i]) {
+        R hx, hy, hz;
+        gather_h<R>(a, vw, i, hx, hy, hz);
+        const R m = vw.md[i];
+        ax = m * ci.x + R(h2) * hx;
+        ay = m * ci.y + R(h2) * hy;
+        az = m * ci.z + R(h2) * hz;
+        filt<R>(vw.nrm, i, ax, ay, az);
+      }
+      vw.ap[3 * i] = ax;
+      vw.ap[3 * i + 1] = ay;
+      vw.ap[3 * i + 2] = az;
+      ca[0] += double(ci.x) * double(ax) + double(ci.y) * double(ay) + double(ci.z) * double(az);
+    }
+    if (!grid_sync<1>(a, sh, ca)) return false;
+    if (ca[0] <= DBL_MIN || !isfinite(ca[0])) {
+      breakdown = true;
+      break;
+    }
+    const double alpha = delta / ca[0];
+    double rz[1] = {0.0};
+    K3D_FOR(i, a.n) {
+      const R4<R> ci = vw.c[i];
+      D3 d = ld3(a.dv, uint32_t(i));
+      d = d + d3(double(ci.x), double(ci.y), double(ci.z)) * alpha;
+      st3(a.dv, uint32_t(i), d);
+      const R rx = R(double(vw.r[3 * i]) - alpha * double(vw.ap[3 * i]));
+      const R ry = R(double(vw.r[3 * i + 1]) - alpha * double(vw.ap[3 * i + 1]));
+      const R rzz = R(double(vw.r[3 * i + 2]) - alpha * double(vw.ap[3 * i + 2]));
+      vw.r[3 * i] = rx;
+      vw.r[3 * i + 1] = ry;
+      vw.r[3 * i + 2] = rzz;
+      R zx, zy, zz;
+      pmul<R>(vw.pinv, i, rx, ry, rzz, zx, zy, zz);
+      if (!a.frei[i]) zx = zy = zz = 0;
+      vw.z[3 * i] = zx;
+      vw.z[3 * i + 1] = zy;
+      vw.z[3 * i + 2] = zz;
+      rz[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rzz) * double(zz);
+    }
+    if (!grid_sync<1>(a, sh, rz)) return false;
+    const double beta = rz[0] / delta;
+    delta = rz[0];
+    K3D_FOR(i, a.n) {
+      R cx = 0, cy = 0, cz = 0;
+      if (a.frei[i]) {
+        const R4<R> ci = vw.c[i];
+        cx = R(double(vw.z[3 * i]) + double(ci.x) * beta);
+        cy = R(double(vw.z[3 * i + 1]) + double(ci.y) * beta);
+        cz = R(double(vw.z[3 * i + 2]) + double(ci.z) * beta);
+        filt<R>(vw.nrm, i, cx, cy, cz);
+      }
+      vw.c[i] = {cx, cy, cz, R(0)};
+    }
+    if (!barrier(a, sh)) return false;
+    ++it;
+  }
+  iters = it;
+  unconverged = delta > ziel;
+  rest = sqrt(delta / fmax(bb, a.boden));
+  return true;
+}
+
+// ------------------------------------------------------------ release pass
+// implizit.rs:924-942: normal force from the residual A dv - b along the
+// contact normal; a held point that pulls on the body is released.
+template <typename R>
+__device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double& released) {
+  dv_to_c<R>(a, vw);
+  if (!barrier(a, sh)) return false;
+  apply_elements<R>(a, vw);
+  if (!barrier(a, sh)) return false;
+  const double h2 = a.h * a.h;
+  double cnt[1] = {0.0};
+  K3D_FOR(i, a.n) {
+    const D3 n = ld3(a.nrm_d, uint32_t(i));
+    if (n.x == 0.0 && n.y == 0.0 && n.z == 0.0) continue;
+    R hx, hy, hz;
+    gather_h<R>(a, vw, i, hx, hy, hz);
+    const R4<R> ci = vw.c[i];
+    const R m = vw.md[i];
+    const D3 b = ld3(a.b, uint32_t(i));
+    const D3 rest = d3(double(m * ci.x + R(h2) * hx) - b.x, double(m * ci.y + R(h2) * hy) - b.y,
+                       double(m * ci.z + R(h2) * hz) - b.z);
+    const double fn = dot(rest, n) / a.h;
+    if (fn < 0.0) {
+      st3(a.nrm_d, uint32_t(i), d3(0, 0, 0));
+      vw.nrm[3 * i] = vw.nrm[3 * i + 1] = vw.nrm[3 * i + 2] = R(0);
+      cnt[0] += 1.0;
+    } else {
+      a.fnk[i] = fn;
+    }
+  }
+  if (!grid_sync<1>(a, sh, cnt)) return false;
+  released = cnt[0];
+  return true;
+}
+
+// ------------------------------------------------------------ friction + integration
+// implizit.rs:957-1013 (no mesh bodies: the segment check does not apply).
+__device__ void integrate(const StepArgs& a, double (&cnt)[3]) {
+  const double h = a.h;
+  K3D_FOR(i, a.n) {
+    if (!a.frei[i]) continue;
+    D3 v = ld3(a.v, uint32_t(i)) + ld3(a.dv, uint32_t(i));
+    const D3 n = ld3(a.nrm_d, uint32_t(i));
+    if (n.x != 0.0 || n.y != 0.0 || n.z != 0.0) {
+      cnt[0] += 1.0;
+      const D3 vb = ld3(a.vk, uint32_t(i));
+      const D3 rel = v - vb;
+      const D3 t = rel - n * dot(rel, n);
+      const double lt = norm(t);
+      const double normal = a.normal_aus_last ? fmax(-dot(ld3(a.load, uint32_t(i)), n), 0.0) : a.fnk[i];
+      const double grenze = a.reib[i] * normal * h * a.w[i];
+      if (lt <= grenze) {
+        cnt[1] += 1.0;
+        v = v - t;
+      } else if (lt > 0.0) {
+        v = v - t * (grenze / lt);
+      }
+    }
+    D3 x = ld3(a.x, uint32_t(i)) + v * h;
+    for (int kb = 0; kb < a.n_bodies; ++kb) {
+      D3 nn;
+      double tiefe;
+      if (kontakt(a.bodies[kb], x, a.kabst[i], nn, tiefe)) {
+        x = x + nn * tiefe;
+        const D3 bv = d3(a.bodies[kb].vel[0], a.bodies[kb].vel[1], a.bodies[kb].vel[2]);
+        const double vn = dot(v - bv, nn);
+        if (vn < 0.0) v = v - nn * vn;
+      }
+    }
+    if (!(isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z)))
+      cnt[2] += 1.0;
+    st3(a.x, uint32_t(i), x);
+    st3(a.v, uint32_t(i), v);
+  }
+}
+
+// ------------------------------------------------------------ the kernel
+template <typename R>
+__global__ void __launch_bounds__(kBlock) step_kernel(const __grid_constant__ StepArgs a) {
+  __shared__ Shared sh;
+  const View<R> vw(a);
+  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+
+  build_elements<R>(a, vw);
+  if (!barrier(a, sh)) return;
+  double held[1];
+  build_points<R>(a, vw, held[0]);
+  if (!grid_sync<1>(a, sh, held)) return;
+
+  if (a.mode == MODE_SYSTEM) {
+    if (a.p_out) {  // f = b/h + h H v, for the readback
+      K3D_FOR(i, a.n) {
+        const D3 q = ld3(a.v, uint32_t(i));
+        vw.c[i] = {R(q.x), R(q.y), R(q.z), R(0)};
+      }
+      if (!barrier(a, sh)) return;
+      apply_elements<R>(a, vw);
+      if (!barrier(a, sh)) return;
+      K3D_FOR(i, a.n) {
+        R hx, hy, hz;
+        gather_h<R>(a, vw, i, hx, hy, hz);
+        const D3 b = ld3(a.b, uint32_t(i));
+        st3(a.p_out, uint32_t(i), b * (1.0 / a.h) + d3(double(hx), double(hy), double(hz)) * a.h);
+      }
+    }
+    return;
+  }
+  if (a.mode == MODE_OPERATOR || a.mode == MODE_RESIDUAL) {
+    const double h2 = a.h * a.h;
+    K3D_FOR(i, a.n) {
+      const D3 q = ld3(a.p_in, uint32_t(i));
+      vw.c[i] = {R(q.x), R(q.y), R(q.z), R(0)};
+    }
+    if (!barrier(a, sh)) return;
+    apply_elements<R>(a, vw);
+    if (!barrier(a, sh)) return;
+    K3D_FOR(i, a.n) {
+      R hx, hy, hz;
+      gather_h<R>(a, vw, i, hx, hy, hz);
+      const R4<R> ci = vw.c[i];
+      const R m = vw.md[i];
+      D3 o = d3(double(m * ci.x + R(h2) * hx), double(m * ci.y + R(h2) * hy), double(m * ci.z + R(h2) * hz));
+      if (a.mode == MODE_RESIDUAL) o = o - ld3(a.b, uint32_t(i));
+      st3(a.p_out, uint32_t(i), o);
+    }
+    return;
+  }
+
+  // MODE_SOLVE and MODE_STEP
+  int64_t iters = 0;
+  bool unconv = false, brk = false;
+  double rest = 0.0;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (!pcg<R>(a, vw, sh, iters, unconv, brk, rest)) return;
+    if (lead) {
+      a.stats[ST_CG_ITERATIONS] += iters;
+      a.stats[ST_SOLVES] += 1;
+      if (unconv) a.stats[ST_UNCONVERGED] += 1;
+      if (brk) a.stats[ST_BREAKDOWNS] += 1;
+      a.stat_rest_max[0] = fmax(a.stat_rest_max[0], rest);
+      a.stats[ST_LAST_ITERATIONS] = iters;
+    }
+    if (a.mode == MODE_SOLVE) return;
+    if (held[0] == 0.0) break;
+    double rel = 0.0;
+    if (!release<R>(a, vw, sh, rel)) return;
+    if (lead) a.stats[ST_RELEASED] += int64_t(rel);
+    if (rel == 0.0) break;
+  }
+  double cnt[3] = {0.0, 0.0, 0.0};
+  integrate(a, cnt);
+  if (!grid_sync<3>(a, sh, cnt)) return;
+  if (lead) {
+    a.stats[ST_CONTACTS] += int64_t(cnt[0]);
+    a.stats[ST_STICKING] += int64_t(cnt[1]);
+    a.stats[ST_NONFINITE] += int64_t(cnt[2]);
+  }
+}
+
+template __global__ void step_kernel<double>(const __grid_constant__ StepArgs a);
+template __global__ void step_kernel<float>(const __grid_constant__ StepArgs a);
+
+// ------------------------------------------------------------ launch
+static int g_blocks[2] = {0, 0};
+
+int step_grid_blocks(int precision, int device) {
+  int idx = precision == 0 ? 0 : 1;
+  if (g_blocks[idx] > 0) return g_blocks[idx];
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return -1;
+  int per_sm = 0;
+  cudaError_t e = idx == 0
+                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel<double>, kBlock, 0)
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel<float>, kBlock, 0);
+  if (e != cudaSuccess || per_sm < 1) return -1;
+  g_blocks[idx] = prop.multiProcessorCount * per_sm;
+  return g_blocks[idx];
+}
+
+cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream_t stream) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(kBlock);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (precision == 0) return cudaLaunchKernelEx(&cfg, step_kernel<double>, a);
+  return cudaLaunchKernelEx(&cfg, step_kernel<float>, a);
+}
+
+}  // namespace k3d

@@ -1,0 +1,82 @@
+// Kernel arguments of the persistent step kernel (internal to the library).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "k3d_device.cuh"
+
+namespace k3d {
+
+constexpr int kBlock = 256;
+
+enum Mode : int { MODE_STEP = 0, MODE_SYSTEM = 1, MODE_OPERATOR = 2, MODE_SOLVE = 3, MODE_RESIDUAL = 4 };
+
+// device statistics slots (int64)
+enum StatSlot : int {
+  ST_CG_ITERATIONS = 0,
+  ST_SOLVES = 1,
+  ST_UNCONVERGED = 2,
+  ST_CONTACTS = 3,
+  ST_STICKING = 4,
+  ST_RELEASED = 5,
+  ST_BREAKDOWNS = 6,
+  ST_NONFINITE = 7,
+  ST_LAST_ITERATIONS = 8,
+  ST_COUNT = 16
+};
+
+constexpr int K3D_STATUS_TIMEOUT = 6;
+
+struct SyncState {
+  unsigned count;
+  unsigned gen;
+  int error;
+  int pad;
+  double result[4];
+};
+
+struct StepArgs {
+  int64_t n, nt, nb, ns;
+  int mode, first_step, need_load, normal_aus_last;
+  int cg_max, n_bodies;
+  double h, daempf, g[3], tol, kontakt_rand, boden;
+  Body bodies[kMaxBodies];
+  // points (double)
+  double *x, *v, *dv, *b, *vk, *fnk, *load, *vn_soll, *nrm_d;
+  const double *masse, *w, *kabst, *reib;
+  const uint8_t* frei;
+  // points (operator precision)
+  void *c, *r, *z, *ap, *pinv, *nrm, *md;
+  // point -> element corner lists
+  const uint32_t *off_t, *ent_t, *off_b, *ent_b, *off_s, *ent_s;
+  // membranes
+  const uint4* m_idx;
+  const double4 *m_r, *m_basis, *m_mat;
+  double4 *m_bc, *m_lc;
+  double* m_dc;  // 8 per corner (6 used)
+  void *m_f1w, *m_f2w, *m_kgB, *m_out;
+  const void *m_rin, *m_kgA;
+  // bends
+  const uint4* b_idx;
+  const double2* b_kr;
+  double4* b_bc;
+  void *b_grad, *b_s;
+  // springs
+  const uint4* s_idx;
+  const double2* s_kl;
+  double4 *s_bc, *s_lc;
+  void *s_dq, *s_k, *s_out;
+  // probes
+  const double* p_in;
+  double* p_out;
+  // bookkeeping
+  SyncState* sync;
+  double* partials;  // kMaxRed * blocks
+  long long* stats;
+  double* stat_rest_max;
+};
+
+int step_grid_blocks(int precision, int device);
+cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream_t stream);
+
+}  // namespace k3d

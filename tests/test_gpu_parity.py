@@ -1,0 +1,192 @@
+"""Device step against the FP64 oracle, through the C ABI.
+
+Tolerances: FP64 operator 1e-12 relative (norm), FP64 states after several
+frames 1e-9 of the bounding-box diagonal (summation order differs from the
+oracle's), mixed FP32/FP64 operator 2e-5 relative.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+import oracle_py as O
+from garmentcraft_b200 import _abi, synth
+from garmentcraft_b200.implizit import ImplizitCg, build_scene
+from garmentcraft_b200.params import ImplizitParameter
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def diag(x):
+    return float(np.linalg.norm(x.max(0) - x.min(0)))
+
+
+def tube_scene():
+    m, body = synth.tube()
+    return build_scene(m, [body])
+
+
+def small_sheet(n=33, seed=3):
+    m, body = synth.sheet_over_sphere(n=n, seed=seed, fall_m=0.02)
+    return build_scene(m, [body])
+
+
+def streuung(n):
+    w = np.arange(n)[:, None] * 0.6180339887498949 * np.array([1.0, 2.0, 3.0])
+    return (w % 1.0) - 0.5
+
+
+@pytest.mark.parametrize("prec,tol", [(_abi.K3D_FP64, 1e-12), (_abi.K3D_MIXED, 2e-5)])
+def test_operator_wie_cpu(prec, tol):
+    # sim/tests/gpu.rs:66-110, at the tolerance of each arithmetic
+    s = tube_scene()
+    par = ImplizitParameter()
+    orc = O.OracleSim(s, par.to_c())
+    orc.frames(3)
+    x, v = orc.state()
+    s.x[:], s.v[:] = x, v
+    cg = ImplizitCg(ImplizitParameter(precision=prec))
+    for p in [np.tile([1.0, 0.0, 0.0], (s.n, 1)), streuung(s.n), v.copy()]:
+        a = orc.operator(p)
+        b = cg.operator(s, p)
+        assert rel(b, a) <= tol
+
+
+def test_system_wie_cpu():
+    s = small_sheet()
+    par = ImplizitParameter(schritte_je_bild=1)
+    orc = O.OracleSim(s, par.to_c())
+    orc.frames(8)  # the sheet is on the sphere now: contacts exist
+    x, v = orc.state()
+    s.x[:], s.v[:] = x, v
+    cg = ImplizitCg(par)
+    g, o = cg.system_fuer(s), orc.system()
+    assert np.array_equal(g["fest"], o["fest"])
+    assert g["fest"].sum() > 0
+    assert rel(g["rhs"], o["rhs"]) <= 1e-11
+    assert rel(g["f"], o["f"]) <= 1e-11
+    assert rel(g["last"], o["last"]) <= 1e-11
+    assert np.max(np.abs(g["pinv"] - o["pinv"]) / np.abs(o["pinv"]).max(axis=(1, 2))[:, None, None]) <= 1e-10
+    assert np.max(np.abs(g["normale"] - o["normale"])) <= 1e-12
+    assert np.max(np.abs(g["vn_soll"] - o["vn_soll"])) <= 1e-9 * max(1.0, np.abs(o["vn_soll"]).max())
+
+
+def test_loese_wie_cpu():
+    s = small_sheet()
+    par = ImplizitParameter(schritte_je_bild=1, cg_max=200, cg_toleranz=1e-8)
+    orc = O.OracleSim(s, par.to_c())
+    orc.frames(8)
+    x, v = orc.state()
+    s.x[:], s.v[:] = x, v
+    dv0 = np.tile([0.0, 0.0, -9.81 / 120.0], (s.n, 1))
+    a, la = orc.solve(dv0)
+    b, lb = ImplizitCg(par).loese(s, dv0)
+    assert abs(la.iterationen - lb.iterationen) <= 1
+    assert rel(b, a) <= 1e-9
+    r_o = O.OracleSim(s, par.to_c())
+    assert rel(ImplizitCg(par).rest_geloest(s, a), r_o.operator(a) - r_o.system()["rhs"]) <= 1e-10
+
+
+def test_tube_frames_wie_cpu():
+    s = tube_scene()
+    par = ImplizitParameter(schritte_je_bild=1, cg_max=2000, cg_toleranz=1e-6)
+    orc = O.OracleSim(s, par.to_c())
+    cg = ImplizitCg(par)
+    for _ in range(10):
+        orc.frames(1)
+        cg.bild(s)
+    x, v = orc.state()
+    assert np.max(np.abs(s.x - x)) <= 1e-9 * diag(x)
+    assert cg.statistik.kontakte > 0
+
+
+def test_sheet_frames_wie_cpu():
+    s = small_sheet()
+    par = ImplizitParameter(schritte_je_bild=1)
+    orc = O.OracleSim(s, par.to_c())
+    cg = ImplizitCg(par)
+    st_o = st_g = None
+    for _ in range(20):
+        st_o = orc.frames(1)
+        cg.bild(s)
+    x, _ = orc.state()
+    assert np.max(np.abs(s.x - x)) <= 1e-8 * diag(x)
+    assert cg.statistik.cg_iterationen == st_o.cg_iterationen
+    assert cg.statistik.kontakte == st_o.kontakte
+
+
+def test_naht_mit_ruhelaenge_gpu():
+    # sim/src/implizit.rs:1067-1120 on the device
+    import test_oracle_golden as G
+    s = G.zwei_punkte(0.04)
+    cg = ImplizitCg(ImplizitParameter())
+    for _ in range(60):
+        cg.bild(s)
+    assert abs(np.linalg.norm(s.x[1] - s.x[0]) - 0.04) < 1e-6
+    s = G.zwei_punkte(0.0)
+    s.naht_offen()
+    cg = ImplizitCg(ImplizitParameter())
+    groesster = 0.0
+    for bild in range(1, 121):
+        vorher = np.linalg.norm(s.x[1] - s.x[0])
+        s.naht_kuerzen(1e-3)
+        cg.bild(s)
+        d = np.linalg.norm(s.x[1] - s.x[0])
+        groesster = max(groesster, vorher - d)
+        if bild == 30:
+            assert abs(d - 0.07) < 1e-4
+    assert np.linalg.norm(s.x[1] - s.x[0]) < 1e-6
+    assert groesster < 1.1e-3
+
+
+def test_tube_analytic_gpu():
+    s = tube_scene()
+    cg = ImplizitCg(ImplizitParameter(schritte_je_bild=1, cg_max=2000, cg_toleranz=1e-6))
+    for _ in range(60):
+        cg.bild(s)
+    orc = O.OracleSim(s, ImplizitParameter().to_c())
+    u = orc.umfang([0, 0, -0.10], [0, 0, 1])
+    soll = 2 * math.pi * (0.08 + 0.25e-3) / 0.40 - 1.0
+    assert abs(u / 0.40 - 1.0 - soll) <= 0.005
+    assert orc.nahtspalt() < 1e-3
+
+
+def test_mixed_error_against_fp64():
+    s64 = small_sheet(n=65)
+    s32 = s64.copy()
+    a = ImplizitCg(ImplizitParameter(schritte_je_bild=1))
+    b = ImplizitCg(ImplizitParameter(schritte_je_bild=1, precision=_abi.K3D_MIXED))
+    a.bilder_resident(s64, 100)
+    b.bilder_resident(s32, 100)
+    err = np.max(np.linalg.norm(s32.x - s64.x, axis=1)) / diag(s64.x)
+    assert err <= 1e-4, err
+
+
+def test_deterministic():
+    a, b = small_sheet(), small_sheet()
+    for s in (a, b):
+        ImplizitCg(ImplizitParameter(schritte_je_bild=1)).bilder_resident(s, 10)
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.v, b.v)
+
+
+def test_nonfinite_is_reported():
+    s = small_sheet()
+    s.x[5, 2] = np.nan
+    cg = ImplizitCg(ImplizitParameter(schritte_je_bild=1))
+    with pytest.raises(Exception) as e:
+        cg.bild(s)
+    assert "NON_FINITE" in str(e.value)
+
+
+def test_bad_index_is_rejected():
+    s = small_sheet()
+    s.membran_punkte[0, 0] = s.n + 5
+    cg = ImplizitCg(ImplizitParameter())
+    with pytest.raises(Exception) as e:
+        cg.bild(s)
+    assert "BAD_ARGUMENT" in str(e.value)
