@@ -76,8 +76,9 @@ static k3d_status cuda_fail(k3d_solver* h, cudaError_t e, const char* what) {
 struct Carve {
   double *masse, *w, *kabst, *reib;
   uint8_t* frei;
-  uint32_t *off_t, *off_b, *off_s, *ent_t, *ent_b, *ent_s;
-  uint4 *m_idx, *b_idx, *s_idx;
+  uint32_t *off_t, *off_b, *off_s, *ent_t, *ent_b, *ent_s, *off_v;
+  uint4 *m_idx, *b_idx, *s_idx, *m_pos, *b_pos;
+  uint2* s_pos;
   double4 *m_r, *m_basis, *m_mat;
   void *m_rin, *m_kgA;
   double2 *b_kr, *s_kl;
@@ -87,6 +88,7 @@ struct Carve {
 // to measure the size).
 static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t S, size_t et, size_t eb, size_t es,
                   Carve& cv) {
+  const size_t nslots = 3 * T + 4 * B + 2 * S;
   const size_t R = h->rsize;
   StepArgs& a = h->a;
   std::memset(&a, 0, sizeof(a));
@@ -120,6 +122,11 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.ent_t = cv.ent_t = A.take<uint32_t>(et);
   a.ent_b = cv.ent_b = A.take<uint32_t>(eb);
   a.ent_s = cv.ent_s = A.take<uint32_t>(es);
+  a.off_v = cv.off_v = A.take<uint32_t>(N + 1);
+  a.m_pos = cv.m_pos = A.take<uint4>(T);
+  a.b_pos = cv.b_pos = A.take<uint4>(B);
+  a.s_pos = cv.s_pos = A.take<uint2>(S);
+  a.slot = A.take<char>(4 * nslots * R);
   a.m_idx = cv.m_idx = A.take<uint4>(T);
   a.m_r = cv.m_r = A.take<double4>(T);
   a.m_basis = cv.m_basis = A.take<double4>(T);
@@ -132,18 +139,15 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.m_kgB = A.take<char>(4 * T * R);
   a.m_rin = cv.m_rin = A.take<char>(4 * T * R);
   a.m_kgA = cv.m_kgA = A.take<char>(4 * T * R);
-  a.m_out = A.take<char>(12 * T * R);
   a.b_idx = cv.b_idx = A.take<uint4>(B);
   a.b_kr = cv.b_kr = A.take<double2>(B);
   a.b_bc = A.take<double4>(4 * B);
   a.b_grad = A.take<char>(16 * B * R);
-  a.b_s = A.take<char>(B * R);
   a.s_idx = cv.s_idx = A.take<uint4>(S);
   a.s_kl = cv.s_kl = A.take<double2>(S);
   a.s_bc = A.take<double4>(S);
   a.s_lc = A.take<double4>(S);
   a.s_dq = A.take<char>(4 * S * R);
-  a.s_out = A.take<char>(4 * S * R);
   a.s_k = A.take<char>(S * R);
   a.sync = A.take<SyncState>(1);
   a.partials = A.take<double>(size_t(4) * h->blocks);
@@ -359,6 +363,28 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
     }
   }
 
+  // operator slots: per point its membrane corners, then bend corners, then spring ends
+  std::vector<uint32_t> off_v(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i)
+    off_v[i + 1] = off_v[i] + (off_t[i + 1] - off_t[i]) + (off_b[i + 1] - off_b[i]) + (off_s[i + 1] - off_s[i]);
+  std::vector<uint4> m_pos(nt), b_pos(nb);
+  std::vector<uint2> s_pos(ns);
+  for (int64_t i = 0; i < n; ++i) {
+    uint32_t q = off_v[i];
+    for (uint32_t e = off_t[i]; e < off_t[i + 1]; ++e, ++q) {
+      const uint32_t c = ent_t[e];
+      (&m_pos[c / 3].x)[c % 3] = q;
+    }
+    for (uint32_t e = off_b[i]; e < off_b[i + 1]; ++e, ++q) {
+      const uint32_t c = ent_b[e];
+      (&b_pos[c / 4].x)[c % 4] = q;
+    }
+    for (uint32_t e = off_s[i]; e < off_s[i + 1]; ++e, ++q) {
+      const uint32_t c = ent_s[e];
+      (&s_pos[c / 2].x)[c % 2] = q;
+    }
+  }
+
   // element constants
   std::vector<uint4> m_idx(nt), b_idx(nb);
   std::vector<double4> m_r(nt), m_basis(nt), m_mat(nt);
@@ -436,6 +462,10 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
   K3D_CUDA(h, up(cv.ent_t, ent_t.data(), 4 * ent_t.size()));
   K3D_CUDA(h, up(cv.ent_b, ent_b.data(), 4 * ent_b.size()));
   K3D_CUDA(h, up(cv.ent_s, ent_s.data(), 4 * ent_s.size()));
+  K3D_CUDA(h, up(cv.off_v, off_v.data(), 4 * (N + 1)));
+  K3D_CUDA(h, up(cv.m_pos, m_pos.data(), 16 * T));
+  K3D_CUDA(h, up(cv.b_pos, b_pos.data(), 16 * B));
+  K3D_CUDA(h, up(cv.s_pos, s_pos.data(), 8 * S));
   K3D_CUDA(h, up(cv.m_idx, m_idx.data(), 16 * T));
   K3D_CUDA(h, up(cv.m_r, m_r.data(), 32 * T));
   K3D_CUDA(h, up(cv.m_basis, m_basis.data(), 32 * T));

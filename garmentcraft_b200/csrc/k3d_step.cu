@@ -163,18 +163,17 @@ template <typename R>
 struct View {
   R4<R>* c;
   R *r, *z, *ap, *pinv, *nrm, *md;
-  R4<R>*m_f1w, *m_f2w, *m_kgB, *m_out;
+  R4<R>*m_f1w, *m_f2w, *m_kgB;
   const R4<R>*m_rin, *m_kgA;
   R4<R>* b_grad;
-  R* b_s;
   R4<R>* s_dq;
   R* s_k;
-  R4<R>* s_out;
+  R4<R>* slot;
   __device__ explicit View(const StepArgs& a)
       : c((R4<R>*)a.c), r((R*)a.r), z((R*)a.z), ap((R*)a.ap), pinv((R*)a.pinv), nrm((R*)a.nrm), md((R*)a.md),
-        m_f1w((R4<R>*)a.m_f1w), m_f2w((R4<R>*)a.m_f2w), m_kgB((R4<R>*)a.m_kgB), m_out((R4<R>*)a.m_out),
-        m_rin((const R4<R>*)a.m_rin), m_kgA((const R4<R>*)a.m_kgA), b_grad((R4<R>*)a.b_grad), b_s((R*)a.b_s),
-        s_dq((R4<R>*)a.s_dq), s_k((R*)a.s_k), s_out((R4<R>*)a.s_out) {}
+        m_f1w((R4<R>*)a.m_f1w), m_f2w((R4<R>*)a.m_f2w), m_kgB((R4<R>*)a.m_kgB),
+        m_rin((const R4<R>*)a.m_rin), m_kgA((const R4<R>*)a.m_kgA), b_grad((R4<R>*)a.b_grad),
+        s_dq((R4<R>*)a.s_dq), s_k((R*)a.s_k), slot((R4<R>*)a.slot) {}
 };
 
 __device__ __forceinline__ double4 ldg4(const double4* p) {
@@ -426,66 +425,58 @@ __device__ void build_points(const StepArgs& a, const View<R>& vw, double& held)
 }
 
 // ------------------------------------------------------------ operator A p
-// Per element: the corner products with the direction c (implizit.rs:185-221).
+// Per element: the corner products with the direction c (implizit.rs:185-221),
+// written to the corners' slots.
 template <typename R>
 __device__ void apply_elements(const StepArgs& a, const View<R>& vw) {
   K3D_FOR(t, a.nt) {
     const uint4 id = __ldg(&a.m_idx[t]);
+    const uint4 ps = __ldg(&a.m_pos[t]);
     const R4<R> d[3] = {vw.c[id.x], vw.c[id.y], vw.c[id.z]};
     R4<R> out[3];
     membran_hv<R>(vw.m_f1w[t], vw.m_f2w[t], vw.m_rin[t], vw.m_kgA[t], vw.m_kgB[t], d, out);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) vw.m_out[3 * t + k] = out[k];
+    vw.slot[ps.x] = out[0];
+    vw.slot[ps.y] = out[1];
+    vw.slot[ps.z] = out[2];
   }
   K3D_FOR(b, a.nb) {
     const uint4 id = __ldg(&a.b_idx[b]);
+    const uint4 ps = __ldg(&a.b_pos[b]);
     const R4<R> g0 = vw.b_grad[4 * b], g1 = vw.b_grad[4 * b + 1], g2 = vw.b_grad[4 * b + 2], g3 = vw.b_grad[4 * b + 3];
     const R4<R> c0 = vw.c[id.x], c1 = vw.c[id.y], c2 = vw.c[id.z], c3 = vw.c[id.w];
     const R gp = g0.x * c0.x + g0.y * c0.y + g0.z * c0.z + g1.x * c1.x + g1.y * c1.y + g1.z * c1.z + g2.x * c2.x +
                  g2.y * c2.y + g2.z * c2.z + g3.x * c3.x + g3.y * c3.y + g3.z * c3.z;
-    vw.b_s[b] = g0.w * gp;
+    const R s = g0.w * gp;
+    vw.slot[ps.x] = {g0.x * s, g0.y * s, g0.z * s, R(0)};
+    vw.slot[ps.y] = {g1.x * s, g1.y * s, g1.z * s, R(0)};
+    vw.slot[ps.z] = {g2.x * s, g2.y * s, g2.z * s, R(0)};
+    vw.slot[ps.w] = {g3.x * s, g3.y * s, g3.z * s, R(0)};
   }
   K3D_FOR(s, a.ns) {
     const uint4 id = __ldg(&a.s_idx[s]);
+    const uint2 ps = __ldg(&a.s_pos[s]);
     const R4<R> dq = vw.s_dq[s];
     const R k = vw.s_k[s];
     const R4<R> ci = vw.c[id.x], cj = vw.c[id.y];
     const R dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
     const R nd = (dq.x * dx + dq.y * dy + dq.z * dz) * (R(1) - dq.w);
-    vw.s_out[s] = {k * (dq.x * nd + dx * dq.w), k * (dq.y * nd + dy * dq.w), k * (dq.z * nd + dz * dq.w), R(0)};
+    const R ox = k * (dq.x * nd + dx * dq.w), oy = k * (dq.y * nd + dy * dq.w), oz = k * (dq.z * nd + dz * dq.w);
+    vw.slot[ps.x] = {ox, oy, oz, R(0)};
+    vw.slot[ps.y] = {-ox, -oy, -oz, R(0)};
   }
 }
 
-// H p at point i from the element corner products.
+// H p at point i: the sum of its corner slots.
 template <typename R>
 __device__ __forceinline__ void gather_h(const StepArgs& a, const View<R>& vw, int64_t i, R& hx, R& hy, R& hz) {
   R x = 0, y = 0, z = 0;
-  for (uint32_t e = __ldg(&a.off_t[i]); e < __ldg(&a.off_t[i + 1]); ++e) {
-    const R4<R> o = vw.m_out[__ldg(&a.ent_t[e])];
+  const uint32_t e0 = __ldg(&a.off_v[i]), e1 = __ldg(&a.off_v[i + 1]);
+#pragma unroll 4
+  for (uint32_t e = e0; e < e1; ++e) {
+    const R4<R> o = vw.slot[e];
     x += o.x;
     y += o.y;
     z += o.z;
-  }
-  for (uint32_t e = __ldg(&a.off_b[i]); e < __ldg(&a.off_b[i + 1]); ++e) {
-    const uint32_t q = __ldg(&a.ent_b[e]);
-    const R4<R> g = vw.b_grad[q];
-    const R s = vw.b_s[q >> 2];
-    x += g.x * s;
-    y += g.y * s;
-    z += g.z * s;
-  }
-  for (uint32_t e = __ldg(&a.off_s[i]); e < __ldg(&a.off_s[i + 1]); ++e) {
-    const uint32_t q = __ldg(&a.ent_s[e]);
-    const R4<R> o = vw.s_out[q >> 1];
-    if (q & 1u) {
-      x -= o.x;
-      y -= o.y;
-      z -= o.z;
-    } else {
-      x += o.x;
-      y += o.y;
-      z += o.z;
-    }
   }
   hx = x;
   hy = y;

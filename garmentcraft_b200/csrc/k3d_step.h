@@ -47,25 +47,31 @@ struct StepArgs {
   const uint8_t* frei;
   // points (operator precision)
   void *c, *r, *z, *ap, *pinv, *nrm, *md;
-  // point -> element corner lists
+  // point -> element corner lists (per-step build)
   const uint32_t *off_t, *ent_t, *off_b, *ent_b, *off_s, *ent_s;
+  // operator: every element corner owns a slot in a point-ordered array;
+  // point i sums slots [off_v[i], off_v[i+1])
+  const uint32_t* off_v;
+  const uint4 *m_pos, *b_pos;
+  const uint2* s_pos;
+  void* slot;
   // membranes
   const uint4* m_idx;
   const double4 *m_r, *m_basis, *m_mat;
   double4 *m_bc, *m_lc;
   double* m_dc;  // 8 per corner (6 used)
-  void *m_f1w, *m_f2w, *m_kgB, *m_out;
+  void *m_f1w, *m_f2w, *m_kgB;
   const void *m_rin, *m_kgA;
   // bends
   const uint4* b_idx;
   const double2* b_kr;
   double4* b_bc;
-  void *b_grad, *b_s;
+  void* b_grad;
   // springs
   const uint4* s_idx;
   const double2* s_kl;
   double4 *s_bc, *s_lc;
-  void *s_dq, *s_k, *s_out;
+  void *s_dq, *s_k;
   // probes
   const double* p_in;
   double* p_out;
