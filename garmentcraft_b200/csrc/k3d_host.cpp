@@ -150,7 +150,7 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.s_dq = A.take<char>(4 * S * R);
   a.s_k = A.take<char>(S * R);
   a.sync = A.take<SyncState>(1);
-  a.partials = A.take<double>(size_t(4) * h->blocks);
+  a.partials = A.take<double>(size_t(8) * h->blocks);  // two buffers of 4 sums per block
   a.stats = A.take<long long>(ST_COUNT);
   a.stat_rest_max = A.take<double>(2);
 }
@@ -539,9 +539,10 @@ static k3d_status launch(k3d_solver* h, int mode, double t_bodies, bool need_loa
     d.spacing = k.spacing;
     d.sdf = static_cast<const float*>(h->sdf_dev[b]);
   }
-  cudaError_t e = launch_step(a, h->p.precision == K3D_MIXED ? 1 : 0, h->blocks, h->stream);
+  int launched = 0;
+  cudaError_t e = launch_step(a, h->p.precision == K3D_MIXED ? 1 : 0, h->blocks, h->stream, launched);
+  h->launches += launched;
   if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
-  h->launches++;
   if (mode == MODE_STEP) h->first_step = false;
   return K3D_OK;
 }
@@ -551,7 +552,7 @@ static k3d_status check_sync(k3d_solver* h) {
   SyncState ss;
   K3D_CUDA(h, cudaMemcpy(&ss, h->a.sync, sizeof(ss), cudaMemcpyDeviceToHost));
   if (ss.error != 0) {
-    cudaMemset(h->a.sync, 0, sizeof(SyncState));
+    cudaMemset(&h->a.sync->error, 0, sizeof(int));
     return fail(h, K3D_TIMEOUT, "a device barrier wait ran out of time");
   }
   return K3D_OK;

@@ -47,13 +47,19 @@ constexpr int kMaxRed = 4;
 struct Shared {
   double red[kMaxRed][32];
   double res[kMaxRed];
-  unsigned gen;
-  int last;
+  unsigned epoch;  // barriers passed in this launch
+  unsigned rbuf;   // reductions done in this launch (partials buffer parity)
   int err;
 };
 
-// Block sum of NV values, fixed order (warp xor tree, then warps in order).
-// Valid in thread 0 only.
+__device__ __forceinline__ unsigned atom_add_release(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+// Block sum of NV values in a fixed order (warp xor tree, then the warps in
+// order); the result is in v in every thread.
 template <int NV>
 __device__ __forceinline__ void block_sum(Shared& sh, double (&v)[NV]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -69,21 +75,30 @@ __device__ __forceinline__ void block_sum(Shared& sh, double (&v)[NV]) {
     const int nw = (blockDim.x + 31) >> 5;
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
-      double s = 0.0;
-      for (int w = 0; w < nw; ++w) s += sh.red[k][w];
-      v[k] = s;
+      double t = 0.0;
+      for (int w = 0; w < nw; ++w) t += sh.red[k][w];
+      sh.res[k] = t;
     }
   }
   __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = sh.res[k];
+  __syncthreads();
 }
 
-// Grid barrier with an optional reduction of NV doubles (NV = 0: plain
-// barrier). The last block to arrive adds the block partials in block order
-// and publishes the totals before releasing the others. Returns false if any
-// block recorded an error (every block then leaves the kernel).
+// Grid barrier: every block adds one to a counter that starts at zero in
+// each launch; barrier k of the launch is passed when the counter reaches
+// k * gridDim.x. With NV > 0 it also sums NV doubles over the grid: each
+// block writes its partials before arriving and, once through, adds all
+// blocks' partials in block order itself, so every block holds the same
+// bits. Partials alternate between two buffers (a block can only reuse a
+// buffer after every block has passed the barrier that follows the reads).
+// The wait gives up after kBarrierLimitNs or when another block has recorded
+// an error; the return value is false then and the caller leaves the kernel.
 template <int NV>
 __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV : 1]) {
   SyncState* s = a.sync;
+  const unsigned buf = sh.rbuf & 1u;
   if constexpr (NV > 0) {
     double loc[NV];
 #pragma unroll
@@ -91,63 +106,43 @@ __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV
     block_sum<NV>(sh, loc);
     if (threadIdx.x == 0) {
 #pragma unroll
-      for (int k = 0; k < NV; ++k) a.partials[k * gridDim.x + blockIdx.x] = loc[k];
+      for (int k = 0; k < NV; ++k) a.partials[(buf * kMaxRed + k) * gridDim.x + blockIdx.x] = loc[k];
+      sh.rbuf += 1;  // every thread read the parity at entry, before block_sum's barriers
     }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    sh.gen = ld_acquire_u32(&s->gen);
-    __threadfence();
-    unsigned prev = atomicAdd(&s->count, 1u);
-    sh.last = (prev == gridDim.x - 1) ? 1 : 0;
-    if (sh.last) __threadfence();
-  }
-  __syncthreads();
-  if (sh.last) {
-    if constexpr (NV > 0) {
-      double loc[NV];
-#pragma unroll
-      for (int k = 0; k < NV; ++k) {
-        double x = 0.0;
-        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) x += __ldcg(&a.partials[k * gridDim.x + b]);
-        loc[k] = x;
-      }
-      block_sum<NV>(sh, loc);
-      if (threadIdx.x == 0) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) s->result[k] = loc[k];
-      }
-    }
-    if (threadIdx.x == 0) {
-      atomicExch(&s->count, 0u);
-      __threadfence();
-      st_release_u32(&s->gen, sh.gen + 1);
-    }
-  } else if (threadIdx.x == 0) {
+    const unsigned target = (sh.epoch + 1) * gridDim.x;
+    atom_add_release(&s->count, 1u);
     const uint64_t t0 = globaltimer();
-    while (ld_acquire_u32(&s->gen) == sh.gen) {
-      if (ld_relaxed_i32(&s->error) != 0) break;
+    int err = 0;
+    while (int(ld_acquire_u32(&s->count) - target) < 0) {
+      if ((err = ld_relaxed_i32(&s->error)) != 0) break;
       if (globaltimer() - t0 > kBarrierLimitNs) {
         atomicCAS(&s->error, 0, K3D_STATUS_TIMEOUT);
+        err = K3D_STATUS_TIMEOUT;
         break;
       }
-      __nanosleep(64);
     }
-    fence_acq_rel();
-  }
-  if (threadIdx.x == 0) {
-    sh.err = ld_relaxed_i32(&s->error);
-    if constexpr (NV > 0) {
-#pragma unroll
-      for (int k = 0; k < NV; ++k) sh.res[k] = __ldcg(&s->result[k]);
-    }
+    sh.err = err;
+    sh.epoch += 1;
   }
   __syncthreads();
+  if (sh.err != 0) return false;
   if constexpr (NV > 0) {
+    double loc[NV];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = sh.res[k];
+    for (int k = 0; k < NV; ++k) {
+      double x = 0.0;
+      for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+        x += __ldcg(&a.partials[(buf * kMaxRed + k) * gridDim.x + b]);
+      loc[k] = x;
+    }
+    block_sum<NV>(sh, loc);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = loc[k];
   }
-  return sh.err == 0;
+  return true;
 }
 
 __device__ __forceinline__ bool barrier(const StepArgs& a, Shared& sh) {
@@ -720,59 +715,46 @@ __device__ void integrate(const StepArgs& a, double (&cnt)[3]) {
   }
 }
 
-// ------------------------------------------------------------ the kernel
+// ------------------------------------------------------------ kernels
+// Build (elements): an ordinary grid-stride launch at full occupancy.
 template <typename R>
-__global__ void __launch_bounds__(kBlock) step_kernel(const __grid_constant__ StepArgs a) {
+__global__ void __launch_bounds__(kBlock) build_elements_kernel(const __grid_constant__ StepArgs a) {
+  const View<R> vw(a);
+  build_elements<R>(a, vw);
+}
+
+// Build (points): rhs, preconditioner, contact set; counts held points.
+template <typename R>
+__global__ void __launch_bounds__(kBlock) build_points_kernel(const __grid_constant__ StepArgs a) {
+  __shared__ double red[32];
+  const View<R> vw(a);
+  double held = 0.0;
+  build_points<R>(a, vw, held);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) held += __shfl_xor_sync(0xffffffffu, held, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = held;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) t += red[w];
+    if (t > 0.0) atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[ST_HELD]), (unsigned long long)t);
+  }
+}
+
+// PCG with the release test (persistent, cooperative): MODE_STEP runs up to
+// two solves with a release pass after each, MODE_SOLVE one solve.
+template <typename R>
+__global__ void __launch_bounds__(kSolveBlock) solve_kernel(const __grid_constant__ StepArgs a) {
   __shared__ Shared sh;
+  if (threadIdx.x == 0) {
+    sh.epoch = 0;
+    sh.rbuf = 0;
+    sh.err = 0;
+  }
+  __syncthreads();
   const View<R> vw(a);
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
-
-  build_elements<R>(a, vw);
-  if (!barrier(a, sh)) return;
-  double held[1];
-  build_points<R>(a, vw, held[0]);
-  if (!grid_sync<1>(a, sh, held)) return;
-
-  if (a.mode == MODE_SYSTEM) {
-    if (a.p_out) {  // f = b/h + h H v, for the readback
-      K3D_FOR(i, a.n) {
-        const D3 q = ld3(a.v, uint32_t(i));
-        vw.c[i] = {R(q.x), R(q.y), R(q.z), R(0)};
-      }
-      if (!barrier(a, sh)) return;
-      apply_elements<R>(a, vw);
-      if (!barrier(a, sh)) return;
-      K3D_FOR(i, a.n) {
-        R hx, hy, hz;
-        gather_h<R>(a, vw, i, hx, hy, hz);
-        const D3 b = ld3(a.b, uint32_t(i));
-        st3(a.p_out, uint32_t(i), b * (1.0 / a.h) + d3(double(hx), double(hy), double(hz)) * a.h);
-      }
-    }
-    return;
-  }
-  if (a.mode == MODE_OPERATOR || a.mode == MODE_RESIDUAL) {
-    const double h2 = a.h * a.h;
-    K3D_FOR(i, a.n) {
-      const D3 q = ld3(a.p_in, uint32_t(i));
-      vw.c[i] = {R(q.x), R(q.y), R(q.z), R(0)};
-    }
-    if (!barrier(a, sh)) return;
-    apply_elements<R>(a, vw);
-    if (!barrier(a, sh)) return;
-    K3D_FOR(i, a.n) {
-      R hx, hy, hz;
-      gather_h<R>(a, vw, i, hx, hy, hz);
-      const R4<R> ci = vw.c[i];
-      const R m = vw.md[i];
-      D3 o = d3(double(m * ci.x + R(h2) * hx), double(m * ci.y + R(h2) * hy), double(m * ci.z + R(h2) * hz));
-      if (a.mode == MODE_RESIDUAL) o = o - ld3(a.b, uint32_t(i));
-      st3(a.p_out, uint32_t(i), o);
-    }
-    return;
-  }
-
-  // MODE_SOLVE and MODE_STEP
+  const bool any_held = a.stats[ST_HELD] > 0;
   int64_t iters = 0;
   bool unconv = false, brk = false;
   double rest = 0.0;
@@ -787,55 +769,144 @@ __global__ void __launch_bounds__(kBlock) step_kernel(const __grid_constant__ St
       a.stats[ST_LAST_ITERATIONS] = iters;
     }
     if (a.mode == MODE_SOLVE) return;
-    if (held[0] == 0.0) break;
+    if (!any_held) break;
     double rel = 0.0;
     if (!release<R>(a, vw, sh, rel)) return;
     if (lead) a.stats[ST_RELEASED] += int64_t(rel);
     if (rel == 0.0) break;
   }
+}
+
+// Friction and integration; counts contacts, sticking and non-finite points.
+__global__ void __launch_bounds__(kBlock) integrate_kernel(const __grid_constant__ StepArgs a) {
+  __shared__ double red[3][32];
   double cnt[3] = {0.0, 0.0, 0.0};
   integrate(a, cnt);
-  if (!grid_sync<3>(a, sh, cnt)) return;
-  if (lead) {
-    a.stats[ST_CONTACTS] += int64_t(cnt[0]);
-    a.stats[ST_STICKING] += int64_t(cnt[1]);
-    a.stats[ST_NONFINITE] += int64_t(cnt[2]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double x = cnt[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int slot[3] = {ST_CONTACTS, ST_STICKING, ST_NONFINITE};
+    for (int k = 0; k < 3; ++k) {
+      double t = 0.0;
+      for (int w = 0; w < int(blockDim.x >> 5); ++w) t += red[k][w];
+      if (t > 0.0) atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[slot[k]]), (unsigned long long)t);
+    }
   }
 }
 
-template __global__ void step_kernel<double>(const __grid_constant__ StepArgs a);
-template __global__ void step_kernel<float>(const __grid_constant__ StepArgs a);
-
-// ------------------------------------------------------------ launch
-static int g_blocks[2] = {0, 0};
-
-int step_grid_blocks(int precision, int device) {
-  int idx = precision == 0 ? 0 : 1;
-  if (g_blocks[idx] > 0) return g_blocks[idx];
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return -1;
-  int per_sm = 0;
-  cudaError_t e = idx == 0
-                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel<double>, kBlock, 0)
-                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel<float>, kBlock, 0);
-  if (e != cudaSuccess || per_sm < 1) return -1;
-  g_blocks[idx] = prop.multiProcessorCount * per_sm;
-  return g_blocks[idx];
+// Probes: c = p (or v), then the element products, then per point
+// A c (MODE_OPERATOR), A c - b (MODE_RESIDUAL) or f = b/h + h H v (MODE_SYSTEM).
+template <typename R>
+__global__ void __launch_bounds__(kBlock) probe_load_kernel(const __grid_constant__ StepArgs a) {
+  const View<R> vw(a);
+  const double* src = a.mode == MODE_SYSTEM ? a.v : a.p_in;
+  K3D_FOR(i, a.n) {
+    const D3 q = ld3(src, uint32_t(i));
+    vw.c[i] = {R(q.x), R(q.y), R(q.z), R(0)};
+  }
+}
+template <typename R>
+__global__ void __launch_bounds__(kBlock) apply_kernel(const __grid_constant__ StepArgs a) {
+  const View<R> vw(a);
+  apply_elements<R>(a, vw);
+}
+template <typename R>
+__global__ void __launch_bounds__(kBlock) probe_out_kernel(const __grid_constant__ StepArgs a) {
+  const View<R> vw(a);
+  const double h2 = a.h * a.h;
+  K3D_FOR(i, a.n) {
+    R hx, hy, hz;
+    gather_h<R>(a, vw, i, hx, hy, hz);
+    const D3 b = ld3(a.b, uint32_t(i));
+    if (a.mode == MODE_SYSTEM) {
+      st3(a.p_out, uint32_t(i), b * (1.0 / a.h) + d3(double(hx), double(hy), double(hz)) * a.h);
+      continue;
+    }
+    const R4<R> ci = vw.c[i];
+    const R m = vw.md[i];
+    D3 o = d3(double(m * ci.x + R(h2) * hx), double(m * ci.y + R(h2) * hy), double(m * ci.z + R(h2) * hz));
+    if (a.mode == MODE_RESIDUAL) o = o - b;
+    st3(a.p_out, uint32_t(i), o);
+  }
 }
 
-cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream_t stream) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(blocks);
-  cfg.blockDim = dim3(kBlock);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  if (precision == 0) return cudaLaunchKernelEx(&cfg, step_kernel<double>, a);
-  return cudaLaunchKernelEx(&cfg, step_kernel<float>, a);
+// ------------------------------------------------------------ launch
+template <typename R>
+struct Kernels {
+  static void* be() { return (void*)build_elements_kernel<R>; }
+  static void* bp() { return (void*)build_points_kernel<R>; }
+  static void* sv() { return (void*)solve_kernel<R>; }
+  static void* pl() { return (void*)probe_load_kernel<R>; }
+  static void* ap() { return (void*)apply_kernel<R>; }
+  static void* po() { return (void*)probe_out_kernel<R>; }
+};
+
+static int g_solve_blocks[2] = {0, 0};
+static int g_sms = 0;
+
+int step_grid_blocks(int precision, int device) {
+  const int idx = precision == 0 ? 0 : 1;
+  if (g_solve_blocks[idx] > 0) return g_solve_blocks[idx];
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return -1;
+  g_sms = prop.multiProcessorCount;
+  int per_sm = 0;
+  const void* fn = idx == 0 ? Kernels<double>::sv() : Kernels<float>::sv();
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolveBlock, 0) != cudaSuccess || per_sm < 1)
+    return -1;
+  g_solve_blocks[idx] = prop.multiProcessorCount * per_sm;
+  return g_solve_blocks[idx];
+}
+
+static cudaError_t plain(const void* fn, const StepArgs& a, int64_t work, cudaStream_t st) {
+  int64_t blocks = (work + kBlock - 1) / kBlock;
+  const int64_t cap = int64_t(g_sms > 0 ? g_sms : 148) * 16;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  void* args[] = {(void*)&a};
+  return cudaLaunchKernel(fn, dim3(unsigned(blocks)), dim3(kBlock), args, 0, st);
+}
+
+static cudaError_t cooperative(const void* fn, const StepArgs& a, int blocks, cudaStream_t st) {
+  void* args[] = {(void*)&a};
+  return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kSolveBlock), args, 0, st);
+}
+
+template <typename R>
+static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int& launched) {
+  cudaError_t e;
+  const int64_t elems = a.nt > a.nb ? (a.nt > a.ns ? a.nt : a.ns) : (a.nb > a.ns ? a.nb : a.ns);
+  if ((e = cudaMemsetAsync(&a.sync->count, 0, sizeof(unsigned), st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(&a.stats[ST_HELD], 0, sizeof(long long), st)) != cudaSuccess) return e;
+  if ((e = plain(Kernels<R>::be(), a, elems, st)) != cudaSuccess) return e;
+  if ((e = plain(Kernels<R>::bp(), a, a.n, st)) != cudaSuccess) return e;
+  launched = 2;
+  if (a.mode == MODE_SYSTEM && !a.p_out) return cudaSuccess;
+  if (a.mode == MODE_OPERATOR || a.mode == MODE_RESIDUAL || a.mode == MODE_SYSTEM) {
+    if ((e = plain(Kernels<R>::pl(), a, a.n, st)) != cudaSuccess) return e;
+    if ((e = plain(Kernels<R>::ap(), a, elems, st)) != cudaSuccess) return e;
+    if ((e = plain(Kernels<R>::po(), a, a.n, st)) != cudaSuccess) return e;
+    launched += 3;
+    return cudaSuccess;
+  }
+  if ((e = cooperative(Kernels<R>::sv(), a, blocks, st)) != cudaSuccess) return e;
+  launched += 1;
+  if (a.mode == MODE_STEP) {
+    if ((e = plain((const void*)integrate_kernel, a, a.n, st)) != cudaSuccess) return e;
+    launched += 1;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream_t stream, int& launched) {
+  launched = 0;
+  return precision == 0 ? launch_t<double>(a, blocks, stream, launched) : launch_t<float>(a, blocks, stream, launched);
 }
 
 }  // namespace k3d

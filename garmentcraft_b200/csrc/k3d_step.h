@@ -7,7 +7,8 @@
 
 namespace k3d {
 
-constexpr int kBlock = 256;
+constexpr int kBlock = 256;       // ordinary launches
+constexpr int kSolveBlock = 512;  // the persistent PCG launch
 
 enum Mode : int { MODE_STEP = 0, MODE_SYSTEM = 1, MODE_OPERATOR = 2, MODE_SOLVE = 3, MODE_RESIDUAL = 4 };
 
@@ -22,17 +23,17 @@ enum StatSlot : int {
   ST_BREAKDOWNS = 6,
   ST_NONFINITE = 7,
   ST_LAST_ITERATIONS = 8,
+  ST_HELD = 9,
   ST_COUNT = 16
 };
 
 constexpr int K3D_STATUS_TIMEOUT = 6;
 
 struct SyncState {
-  unsigned count;
-  unsigned gen;
-  int error;
-  int pad;
-  double result[4];
+  unsigned count;  // barrier arrivals in this launch (zeroed before each launch)
+  unsigned pad0[31];
+  int error;       // K3D_STATUS_TIMEOUT after a wait gave up
+  int pad1[31];
 };
 
 struct StepArgs {
@@ -83,6 +84,7 @@ struct StepArgs {
 };
 
 int step_grid_blocks(int precision, int device);
-cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream_t stream);
+// Enqueues one substep (or probe) on `stream`; `launched` = kernels enqueued.
+cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream_t stream, int& launched);
 
 }  // namespace k3d
