@@ -76,7 +76,7 @@ static k3d_status cuda_fail(k3d_solver* h, cudaError_t e, const char* what) {
 struct Carve {
   double *masse, *w, *kabst, *reib;
   uint8_t* frei;
-  uint32_t *off_t, *off_b, *off_s, *ent_t, *ent_b, *ent_s, *off_v;
+  uint32_t *off_t, *off_b, *off_s, *ent_t, *ent_b, *ent_s, *cnt_v;
   uint4 *m_idx, *b_idx, *s_idx, *m_pos, *b_pos;
   uint2* s_pos;
   double4 *m_r, *m_basis, *m_mat;
@@ -87,8 +87,8 @@ struct Carve {
 // Assigns every device array of the handle from the arena (base may be null
 // to measure the size).
 static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t S, size_t et, size_t eb, size_t es,
-                  Carve& cv) {
-  const size_t nslots = 3 * T + 4 * B + 2 * S;
+                  size_t np, size_t kmax, Carve& cv) {
+  const size_t nslots = np * (kmax ? kmax : 1);
   const size_t R = h->rsize;
   StepArgs& a = h->a;
   std::memset(&a, 0, sizeof(a));
@@ -109,7 +109,7 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.kabst = cv.kabst = A.take<double>(N);
   a.reib = cv.reib = A.take<double>(N);
   a.frei = cv.frei = A.take<uint8_t>(N);
-  a.c = A.take<char>(4 * N * R);
+  a.c = A.take<char>(8 * N * R);  // c and w per point
   a.r = A.take<char>(3 * N * R);
   a.z = A.take<char>(3 * N * R);
   a.ap = A.take<char>(3 * N * R);
@@ -122,7 +122,8 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.ent_t = cv.ent_t = A.take<uint32_t>(et);
   a.ent_b = cv.ent_b = A.take<uint32_t>(eb);
   a.ent_s = cv.ent_s = A.take<uint32_t>(es);
-  a.off_v = cv.off_v = A.take<uint32_t>(N + 1);
+  a.cnt_v = cv.cnt_v = A.take<uint32_t>(N);
+  a.np = int64_t(np);
   a.m_pos = cv.m_pos = A.take<uint4>(T);
   a.b_pos = cv.b_pos = A.take<uint4>(B);
   a.s_pos = cv.s_pos = A.take<uint2>(S);
@@ -363,25 +364,31 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
     }
   }
 
-  // operator slots: per point its membrane corners, then bend corners, then spring ends
-  std::vector<uint32_t> off_v(n + 1, 0);
-  for (int64_t i = 0; i < n; ++i)
-    off_v[i + 1] = off_v[i] + (off_t[i + 1] - off_t[i]) + (off_b[i + 1] - off_b[i]) + (off_s[i + 1] - off_s[i]);
+  // operator slots (ELL): per point its membrane corners, then bend corners,
+  // then spring ends; the corner of rank k at point i owns slot k * np + i
+  const size_t np = (size_t(n) + 63) & ~size_t(63);
+  std::vector<uint32_t> cnt_v(n, 0);
+  size_t kmax = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    cnt_v[i] = (off_t[i + 1] - off_t[i]) + (off_b[i + 1] - off_b[i]) + (off_s[i + 1] - off_s[i]);
+    kmax = std::max(kmax, size_t(cnt_v[i]));
+  }
+  if (kmax * np >= (size_t(1) << 32)) return fail(h, K3D_BAD_ARGUMENT, "scene too large for 32-bit slots");
   std::vector<uint4> m_pos(nt), b_pos(nb);
   std::vector<uint2> s_pos(ns);
   for (int64_t i = 0; i < n; ++i) {
-    uint32_t q = off_v[i];
-    for (uint32_t e = off_t[i]; e < off_t[i + 1]; ++e, ++q) {
+    uint32_t k = 0;
+    for (uint32_t e = off_t[i]; e < off_t[i + 1]; ++e, ++k) {
       const uint32_t c = ent_t[e];
-      (&m_pos[c / 3].x)[c % 3] = q;
+      (&m_pos[c / 3].x)[c % 3] = uint32_t(k * np + size_t(i));
     }
-    for (uint32_t e = off_b[i]; e < off_b[i + 1]; ++e, ++q) {
+    for (uint32_t e = off_b[i]; e < off_b[i + 1]; ++e, ++k) {
       const uint32_t c = ent_b[e];
-      (&b_pos[c / 4].x)[c % 4] = q;
+      (&b_pos[c / 4].x)[c % 4] = uint32_t(k * np + size_t(i));
     }
-    for (uint32_t e = off_s[i]; e < off_s[i + 1]; ++e, ++q) {
+    for (uint32_t e = off_s[i]; e < off_s[i + 1]; ++e, ++k) {
       const uint32_t c = ent_s[e];
-      (&s_pos[c / 2].x)[c % 2] = q;
+      (&s_pos[c / 2].x)[c % 2] = uint32_t(k * np + size_t(i));
     }
   }
 
@@ -433,12 +440,12 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
   const size_t N = size_t(n), T = size_t(nt), B = size_t(nb), S = size_t(ns);
   Carve cv;
   Arena probe;
-  carve(h, probe, N, T, B, S, ent_t.size(), ent_b.size(), ent_s.size(), cv);
+  carve(h, probe, N, T, B, S, ent_t.size(), ent_b.size(), ent_s.size(), np, kmax, cv);
   void* base = nullptr;
   K3D_CUDA(h, cudaMalloc(&base, probe.used));
   h->arena.base = static_cast<char*>(base);
   h->arena.size = probe.used;
-  carve(h, h->arena, N, T, B, S, ent_t.size(), ent_b.size(), ent_s.size(), cv);
+  carve(h, h->arena, N, T, B, S, ent_t.size(), ent_b.size(), ent_s.size(), np, kmax, cv);
   Arena& A = h->arena;
   StepArgs& a = h->a;
   if (A.used > A.size) return fail(h, K3D_DEVICE_ERROR, "arena overflow");
@@ -462,7 +469,7 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
   K3D_CUDA(h, up(cv.ent_t, ent_t.data(), 4 * ent_t.size()));
   K3D_CUDA(h, up(cv.ent_b, ent_b.data(), 4 * ent_b.size()));
   K3D_CUDA(h, up(cv.ent_s, ent_s.data(), 4 * ent_s.size()));
-  K3D_CUDA(h, up(cv.off_v, off_v.data(), 4 * (N + 1)));
+  K3D_CUDA(h, up(cv.cnt_v, cnt_v.data(), 4 * N));
   K3D_CUDA(h, up(cv.m_pos, m_pos.data(), 16 * T));
   K3D_CUDA(h, up(cv.b_pos, b_pos.data(), 16 * B));
   K3D_CUDA(h, up(cv.s_pos, s_pos.data(), 8 * S));

@@ -154,9 +154,26 @@ __device__ __forceinline__ bool barrier(const StepArgs& a, Shared& sh) {
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < (n); i += int64_t(gridDim.x) * blockDim.x)
 
 // ------------------------------------------------------------ typed views
+// Per point the CG direction c and the filtered preconditioned residual
+// w = S P^-1 r, side by side so an element reads both with one gather.
+template <typename R>
+struct CW {
+  R4<R> c, w;
+};
+
+// The next direction c' = w + beta c (implizit.rs:421: S(z + beta c) with c
+// already in the filtered space). One helper for the element and the point
+// phase, so both hold the same bits.
+__device__ __forceinline__ float fmar(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmar(double a, double b, double c) { return __fma_rn(a, b, c); }
+template <typename R>
+__device__ __forceinline__ R4<R> next_dir(const CW<R>& q, R beta) {
+  return {fmar(beta, q.c.x, q.w.x), fmar(beta, q.c.y, q.w.y), fmar(beta, q.c.z, q.w.z), R(0)};
+}
+
 template <typename R>
 struct View {
-  R4<R>* c;
+  CW<R>* cw;
   R *r, *z, *ap, *pinv, *nrm, *md;
   R4<R>*m_f1w, *m_f2w, *m_kgB;
   const R4<R>*m_rin, *m_kgA;
@@ -165,7 +182,7 @@ struct View {
   R* s_k;
   R4<R>* slot;
   __device__ explicit View(const StepArgs& a)
-      : c((R4<R>*)a.c), r((R*)a.r), z((R*)a.z), ap((R*)a.ap), pinv((R*)a.pinv), nrm((R*)a.nrm), md((R*)a.md),
+      : cw((CW<R>*)a.c), r((R*)a.r), z((R*)a.z), ap((R*)a.ap), pinv((R*)a.pinv), nrm((R*)a.nrm), md((R*)a.md),
         m_f1w((R4<R>*)a.m_f1w), m_f2w((R4<R>*)a.m_f2w), m_kgB((R4<R>*)a.m_kgB),
         m_rin((const R4<R>*)a.m_rin), m_kgA((const R4<R>*)a.m_kgA), b_grad((R4<R>*)a.b_grad),
         s_dq((R4<R>*)a.s_dq), s_k((R*)a.s_k), slot((R4<R>*)a.slot) {}
@@ -420,14 +437,15 @@ __device__ void build_points(const StepArgs& a, const View<R>& vw, double& held)
 }
 
 // ------------------------------------------------------------ operator A p
-// Per element: the corner products with the direction c (implizit.rs:185-221),
-// written to the corners' slots.
+// Per element: the corner products H_e p with p = w + beta c at its points
+// (implizit.rs:185-221), written to the corners' slots (rank * np + point).
 template <typename R>
-__device__ void apply_elements(const StepArgs& a, const View<R>& vw) {
+__device__ void apply_elements(const StepArgs& a, const View<R>& vw, R beta) {
   K3D_FOR(t, a.nt) {
     const uint4 id = __ldg(&a.m_idx[t]);
     const uint4 ps = __ldg(&a.m_pos[t]);
-    const R4<R> d[3] = {vw.c[id.x], vw.c[id.y], vw.c[id.z]};
+    const R4<R> d[3] = {next_dir<R>(vw.cw[id.x], beta), next_dir<R>(vw.cw[id.y], beta),
+                        next_dir<R>(vw.cw[id.z], beta)};
     R4<R> out[3];
     membran_hv<R>(vw.m_f1w[t], vw.m_f2w[t], vw.m_rin[t], vw.m_kgA[t], vw.m_kgB[t], d, out);
     vw.slot[ps.x] = out[0];
@@ -438,7 +456,8 @@ __device__ void apply_elements(const StepArgs& a, const View<R>& vw) {
     const uint4 id = __ldg(&a.b_idx[b]);
     const uint4 ps = __ldg(&a.b_pos[b]);
     const R4<R> g0 = vw.b_grad[4 * b], g1 = vw.b_grad[4 * b + 1], g2 = vw.b_grad[4 * b + 2], g3 = vw.b_grad[4 * b + 3];
-    const R4<R> c0 = vw.c[id.x], c1 = vw.c[id.y], c2 = vw.c[id.z], c3 = vw.c[id.w];
+    const R4<R> c0 = next_dir<R>(vw.cw[id.x], beta), c1 = next_dir<R>(vw.cw[id.y], beta),
+                c2 = next_dir<R>(vw.cw[id.z], beta), c3 = next_dir<R>(vw.cw[id.w], beta);
     const R gp = g0.x * c0.x + g0.y * c0.y + g0.z * c0.z + g1.x * c1.x + g1.y * c1.y + g1.z * c1.z + g2.x * c2.x +
                  g2.y * c2.y + g2.z * c2.z + g3.x * c3.x + g3.y * c3.y + g3.z * c3.z;
     const R s = g0.w * gp;
@@ -452,7 +471,7 @@ __device__ void apply_elements(const StepArgs& a, const View<R>& vw) {
     const uint2 ps = __ldg(&a.s_pos[s]);
     const R4<R> dq = vw.s_dq[s];
     const R k = vw.s_k[s];
-    const R4<R> ci = vw.c[id.x], cj = vw.c[id.y];
+    const R4<R> ci = next_dir<R>(vw.cw[id.x], beta), cj = next_dir<R>(vw.cw[id.y], beta);
     const R dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
     const R nd = (dq.x * dx + dq.y * dy + dq.z * dz) * (R(1) - dq.w);
     const R ox = k * (dq.x * nd + dx * dq.w), oy = k * (dq.y * nd + dy * dq.w), oz = k * (dq.z * nd + dz * dq.w);
@@ -461,14 +480,16 @@ __device__ void apply_elements(const StepArgs& a, const View<R>& vw) {
   }
 }
 
-// H p at point i: the sum of its corner slots.
+// H p at point i: the sum of its corner slots, rank by rank (coalesced over
+// consecutive points).
 template <typename R>
 __device__ __forceinline__ void gather_h(const StepArgs& a, const View<R>& vw, int64_t i, R& hx, R& hy, R& hz) {
   R x = 0, y = 0, z = 0;
-  const uint32_t e0 = __ldg(&a.off_v[i]), e1 = __ldg(&a.off_v[i + 1]);
-#pragma unroll 4
-  for (uint32_t e = e0; e < e1; ++e) {
-    const R4<R> o = vw.slot[e];
+  const uint32_t cnt = __ldg(&a.cnt_v[i]);
+  const R4<R>* sl = vw.slot + i;
+#pragma unroll 6
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const R4<R> o = sl[size_t(k) * a.np];
     x += o.x;
     y += o.y;
     z += o.z;
@@ -496,17 +517,22 @@ __device__ __forceinline__ void pmul(const R* P, int64_t i, R x, R y, R z, R& ox
   oz = p4 * x + p5 * y + p2 * z;
 }
 
-// c = (R) dv
+// w = (R) dv, c = 0: the next element pass with beta = 0 applies A to dv.
 template <typename R>
-__device__ void dv_to_c(const StepArgs& a, const View<R>& vw) {
+__device__ void dv_to_w(const StepArgs& a, const View<R>& vw) {
   K3D_FOR(i, a.n) {
     const D3 d = ld3(a.dv, uint32_t(i));
-    vw.c[i] = {R(d.x), R(d.y), R(d.z), R(0)};
+    vw.cw[i].w = {R(d.x), R(d.y), R(d.z), R(0)};
+    vw.cw[i].c = {R(0), R(0), R(0), R(0)};
   }
 }
 
 // ------------------------------------------------------------ PCG
-// implizit.rs:370-426. Returns false on a barrier error.
+// implizit.rs:370-426, three grid syncs per iteration:
+//   elements: H p with p = w + beta c            -> barrier
+//   points:   c = p, ap = S A c, c.ap            -> sum
+//   points:   dv += alpha c, r -= alpha ap, z = P r, w = S z, r.z -> sum
+// Returns false on a barrier error.
 template <typename R>
 __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& iters, bool& unconverged,
                     bool& breakdown, double& rest) {
@@ -524,20 +550,21 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       }
     }
     st3(a.dv, uint32_t(i), d);
-    vw.c[i] = {R(d.x), R(d.y), R(d.z), R(0)};
+    vw.cw[i].w = {R(d.x), R(d.y), R(d.z), R(0)};
+    vw.cw[i].c = {R(0), R(0), R(0), R(0)};
   }
   if (!barrier(a, sh)) return false;
-  apply_elements<R>(a, vw);
+  apply_elements<R>(a, vw, R(0));
   if (!barrier(a, sh)) return false;
   double red[2] = {0.0, 0.0};
   K3D_FOR(i, a.n) {
     R hx, hy, hz;
     gather_h<R>(a, vw, i, hx, hy, hz);
-    const R4<R> ci = vw.c[i];
+    const R4<R> pi = vw.cw[i].w;
     const R m = vw.md[i];
     R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, cx = 0, cy = 0, cz = 0;
     if (a.frei[i]) {
-      const R ax = m * ci.x + R(h2) * hx, ay = m * ci.y + R(h2) * hy, az = m * ci.z + R(h2) * hz;
+      const R ax = m * pi.x + R(h2) * hx, ay = m * pi.y + R(h2) * hy, az = m * pi.z + R(h2) * hz;
       const D3 b = ld3(a.b, uint32_t(i));
       rx = R(b.x - double(ax));
       ry = R(b.y - double(ay));
@@ -561,21 +588,25 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     vw.z[3 * i] = zx;
     vw.z[3 * i + 1] = zy;
     vw.z[3 * i + 2] = zz;
-    vw.c[i] = {cx, cy, cz, R(0)};
+    vw.cw[i].w = {cx, cy, cz, R(0)};  // the first direction: w + 0 c
+    vw.cw[i].c = {R(0), R(0), R(0), R(0)};
   }
   if (!grid_sync<2>(a, sh, red)) return false;
   double delta = red[0];
   const double bb = red[1];
   const double ziel = fmax(a.tol * a.tol * fmax(bb, delta), a.boden);
   int64_t it = 0;
+  double beta = 0.0;
   breakdown = false;
   while (delta > ziel && it < a.cg_max) {
-    apply_elements<R>(a, vw);
+    const R rb = R(beta);
+    apply_elements<R>(a, vw, rb);
     if (!barrier(a, sh)) return false;
     double ca[1] = {0.0};
     K3D_FOR(i, a.n) {
+      const R4<R> ci = next_dir<R>(vw.cw[i], rb);
+      vw.cw[i].c = ci;
       R ax = 0, ay = 0, az = 0;
-      const R4<R> ci = vw.c[i];
       if (a.frei[i]) {
         R hx, hy, hz;
         gather_h<R>(a, vw, i, hx, hy, hz);
@@ -596,9 +627,9 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       break;
     }
     const double alpha = delta / ca[0];
-    double rz[1] = {0.0};
+    double rzs[1] = {0.0};
     K3D_FOR(i, a.n) {
-      const R4<R> ci = vw.c[i];
+      const R4<R> ci = vw.cw[i].c;
       D3 d = ld3(a.dv, uint32_t(i));
       d = d + d3(double(ci.x), double(ci.y), double(ci.z)) * alpha;
       st3(a.dv, uint32_t(i), d);
@@ -611,26 +642,14 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       R zx, zy, zz;
       pmul<R>(vw.pinv, i, rx, ry, rzz, zx, zy, zz);
       if (!a.frei[i]) zx = zy = zz = 0;
-      vw.z[3 * i] = zx;
-      vw.z[3 * i + 1] = zy;
-      vw.z[3 * i + 2] = zz;
-      rz[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rzz) * double(zz);
+      R wx = zx, wy = zy, wz = zz;
+      filt<R>(vw.nrm, i, wx, wy, wz);
+      vw.cw[i].w = {wx, wy, wz, R(0)};
+      rzs[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rzz) * double(zz);
     }
-    if (!grid_sync<1>(a, sh, rz)) return false;
-    const double beta = rz[0] / delta;
-    delta = rz[0];
-    K3D_FOR(i, a.n) {
-      R cx = 0, cy = 0, cz = 0;
-      if (a.frei[i]) {
-        const R4<R> ci = vw.c[i];
-        cx = R(double(vw.z[3 * i]) + double(ci.x) * beta);
-        cy = R(double(vw.z[3 * i + 1]) + double(ci.y) * beta);
-        cz = R(double(vw.z[3 * i + 2]) + double(ci.z) * beta);
-        filt<R>(vw.nrm, i, cx, cy, cz);
-      }
-      vw.c[i] = {cx, cy, cz, R(0)};
-    }
-    if (!barrier(a, sh)) return false;
+    if (!grid_sync<1>(a, sh, rzs)) return false;
+    beta = rzs[0] / delta;
+    delta = rzs[0];
     ++it;
   }
   iters = it;
@@ -644,9 +663,9 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
 // contact normal; a held point that pulls on the body is released.
 template <typename R>
 __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double& released) {
-  dv_to_c<R>(a, vw);
+  dv_to_w<R>(a, vw);
   if (!barrier(a, sh)) return false;
-  apply_elements<R>(a, vw);
+  apply_elements<R>(a, vw, R(0));
   if (!barrier(a, sh)) return false;
   const double h2 = a.h * a.h;
   double cnt[1] = {0.0};
@@ -655,7 +674,7 @@ __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double
     if (n.x == 0.0 && n.y == 0.0 && n.z == 0.0) continue;
     R hx, hy, hz;
     gather_h<R>(a, vw, i, hx, hy, hz);
-    const R4<R> ci = vw.c[i];
+    const R4<R> ci = vw.cw[i].w;
     const R m = vw.md[i];
     const D3 b = ld3(a.b, uint32_t(i));
     const D3 rest = d3(double(m * ci.x + R(h2) * hx) - b.x, double(m * ci.y + R(h2) * hy) - b.y,
@@ -808,13 +827,14 @@ __global__ void __launch_bounds__(kBlock) probe_load_kernel(const __grid_constan
   const double* src = a.mode == MODE_SYSTEM ? a.v : a.p_in;
   K3D_FOR(i, a.n) {
     const D3 q = ld3(src, uint32_t(i));
-    vw.c[i] = {R(q.x), R(q.y), R(q.z), R(0)};
+    vw.cw[i].w = {R(q.x), R(q.y), R(q.z), R(0)};
+    vw.cw[i].c = {R(0), R(0), R(0), R(0)};
   }
 }
 template <typename R>
 __global__ void __launch_bounds__(kBlock) apply_kernel(const __grid_constant__ StepArgs a) {
   const View<R> vw(a);
-  apply_elements<R>(a, vw);
+  apply_elements<R>(a, vw, R(0));
 }
 template <typename R>
 __global__ void __launch_bounds__(kBlock) probe_out_kernel(const __grid_constant__ StepArgs a) {
@@ -828,7 +848,7 @@ __global__ void __launch_bounds__(kBlock) probe_out_kernel(const __grid_constant
       st3(a.p_out, uint32_t(i), b * (1.0 / a.h) + d3(double(hx), double(hy), double(hz)) * a.h);
       continue;
     }
-    const R4<R> ci = vw.c[i];
+    const R4<R> ci = vw.cw[i].w;
     const R m = vw.md[i];
     D3 o = d3(double(m * ci.x + R(h2) * hx), double(m * ci.y + R(h2) * hy), double(m * ci.z + R(h2) * hz));
     if (a.mode == MODE_RESIDUAL) o = o - b;

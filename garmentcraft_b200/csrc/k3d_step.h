@@ -50,9 +50,10 @@ struct StepArgs {
   void *c, *r, *z, *ap, *pinv, *nrm, *md;
   // point -> element corner lists (per-step build)
   const uint32_t *off_t, *ent_t, *off_b, *ent_b, *off_s, *ent_s;
-  // operator: every element corner owns a slot in a point-ordered array;
-  // point i sums slots [off_v[i], off_v[i+1])
-  const uint32_t* off_v;
+  // operator: element corner (rank k at point i) owns slot k * np + i; point
+  // i sums its cnt_v[i] slots
+  const uint32_t* cnt_v;
+  int64_t np;
   const uint4 *m_pos, *b_pos;
   const uint2* s_pos;
   void* slot;

@@ -125,18 +125,22 @@ def test_tube_frames_wie_cpu():
 
 
 def test_sheet_frames_wie_cpu():
+    # solved to 1e-12 so the solver's own error is at rounding level; the
+    # sheet lands on the sphere within these frames (contacts, release test,
+    # friction)
     s = small_sheet()
-    par = ImplizitParameter(schritte_je_bild=1, cg_max=4000)
+    par = ImplizitParameter(schritte_je_bild=1, cg_max=20000, cg_toleranz=1e-12)
     orc = O.OracleSim(s, par.to_c())
     cg = ImplizitCg(par)
-    st_o = st_g = None
-    for _ in range(20):
+    kontakte = 0
+    for _ in range(15):
         st_o = orc.frames(1)
         cg.bild(s)
+        assert cg.statistik.kontakte == st_o.kontakte
+        kontakte += st_o.kontakte
     x, _ = orc.state()
-    assert np.max(np.abs(s.x - x)) <= 1e-7 * diag(x)
-    assert abs(cg.statistik.cg_iterationen - st_o.cg_iterationen) <= max(2, st_o.cg_iterationen // 20)
-    assert cg.statistik.kontakte == st_o.kontakte
+    assert kontakte > 0
+    assert np.max(np.abs(s.x - x)) <= 1e-9 * diag(x)
 
 
 def test_naht_mit_ruhelaenge_gpu():
@@ -175,15 +179,23 @@ def test_tube_analytic_gpu():
     assert orc.nahtspalt() < 1e-3
 
 
-def test_mixed_error_against_fp64():
-    s64 = small_sheet(n=65)
-    s32 = s64.copy()
-    a = ImplizitCg(ImplizitParameter(schritte_je_bild=1, cg_max=4000))
-    b = ImplizitCg(ImplizitParameter(schritte_je_bild=1, cg_max=4000, precision=_abi.K3D_MIXED))
-    a.bilder_resident(s64, 100)
-    b.bilder_resident(s32, 100)
-    err = np.max(np.linalg.norm(s32.x - s64.x, axis=1)) / diag(s64.x)
-    assert err <= 1e-4, err
+def test_mixed_step_error_against_fp64():
+    """One step of the mixed form against one FP64 step from the same state,
+    at ten states along a drop onto the sphere (converged solves, tol 1e-5).
+    The difference is the solver tolerance plus FP32 rounding of the operator:
+    below 1e-6 of the bounding-box diagonal per step."""
+    ref = small_sheet(n=65)
+    par64 = ImplizitParameter(schritte_je_bild=1, cg_max=4000)
+    par32 = ImplizitParameter(schritte_je_bild=1, cg_max=4000, precision=_abi.K3D_MIXED)
+    traj = ImplizitCg(par64)
+    worst = 0.0
+    for _ in range(10):
+        traj.bilder_resident(ref, 8)
+        s64, s32 = ref.copy(), ref.copy()
+        ImplizitCg(par64).bild(s64)
+        ImplizitCg(par32).bild(s32)
+        worst = max(worst, float(np.max(np.linalg.norm(s32.x - s64.x, axis=1)) / diag(s64.x)))
+    assert worst <= 1e-6, worst
 
 
 def test_deterministic():
