@@ -169,32 +169,28 @@ __device__ __forceinline__ void kg_sym(const MembranC& m, double kg[6]) {
 
 // Hessian-vector product of one membrane (kontinuum.rs:616-664) in the
 // operator precision R, from the per-step record: f1, f2, w=(w11,w22,w12),
-// rest coefficients r0..r3 and the assembled kg.
+// rest coefficients r0..r3 and the assembled kg. The corner coefficients sum
+// to zero (c1[0] = -(c1[1] + c1[2]), the same for c2), so the product only
+// sees the differences d1 - d0 and d2 - d0: a motion common to the three
+// points cancels before any rounding.
 template <typename R>
 __device__ __forceinline__ void membran_hv(const R4<R>& f1w, const R4<R>& f2w, const R4<R>& rin,
                                            const R4<R>& kgA, const R4<R>& kgB, const R4<R> d[3], R4<R> out[3]) {
   const R c1[3] = {-(rin.x + rin.z), rin.x, rin.z};
   const R c2[3] = {-(rin.y + rin.w), rin.y, rin.w};
-  R q0 = 0, q1 = 0, q2 = 0;
-  R t1x = 0, t1y = 0, t1z = 0, t2x = 0, t2y = 0, t2z = 0;
-#pragma unroll
-  for (int l = 0; l < 3; ++l) {
-    R d1 = f1w.x * d[l].x + f1w.y * d[l].y + f1w.z * d[l].z;
-    R d2 = f2w.x * d[l].x + f2w.y * d[l].y + f2w.z * d[l].z;
-    q0 += R(2) * c1[l] * d1;
-    q1 += R(2) * c2[l] * d2;
-    q2 += R(2) * (c2[l] * d1 + c1[l] * d2);
-    t1x += c1[l] * d[l].x;
-    t1y += c1[l] * d[l].y;
-    t1z += c1[l] * d[l].z;
-    t2x += c2[l] * d[l].x;
-    t2y += c2[l] * d[l].y;
-    t2z += c2[l] * d[l].z;
-  }
+  const R e1x = d[1].x - d[0].x, e1y = d[1].y - d[0].y, e1z = d[1].z - d[0].z;
+  const R e2x = d[2].x - d[0].x, e2y = d[2].y - d[0].y, e2z = d[2].z - d[0].z;
+  const R a1 = f1w.x * e1x + f1w.y * e1y + f1w.z * e1z, b1 = f2w.x * e1x + f2w.y * e1y + f2w.z * e1z;
+  const R a2 = f1w.x * e2x + f1w.y * e2y + f1w.z * e2z, b2 = f2w.x * e2x + f2w.y * e2y + f2w.z * e2z;
+  const R q0 = R(2) * (c1[1] * a1 + c1[2] * a2);
+  const R q1 = R(2) * (c2[1] * b1 + c2[2] * b2);
+  const R q2 = R(2) * (c2[1] * a1 + c1[1] * b1 + c2[2] * a2 + c1[2] * b2);
+  const R t1x = c1[1] * e1x + c1[2] * e2x, t1y = c1[1] * e1y + c1[2] * e2y, t1z = c1[1] * e1z + c1[2] * e2z;
+  const R t2x = c2[1] * e1x + c2[2] * e2x, t2y = c2[1] * e1y + c2[2] * e2y, t2z = c2[1] * e1z + c2[2] * e2z;
   // w = kg q; kgA = (00, 11, 22, 01), kgB = (02, 12, w12, -)
-  R w0 = kgA.x * q0 + kgA.w * q1 + kgB.x * q2;
-  R w1 = kgA.w * q0 + kgA.y * q1 + kgB.y * q2;
-  R w2 = kgB.x * q0 + kgB.y * q1 + kgA.z * q2;
+  const R w0 = kgA.x * q0 + kgA.w * q1 + kgB.x * q2;
+  const R w1 = kgA.w * q0 + kgA.y * q1 + kgB.y * q2;
+  const R w2 = kgB.x * q0 + kgB.y * q1 + kgA.z * q2;
   const R w11 = f1w.w, w22 = f2w.w, w12 = kgB.z;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {

@@ -42,6 +42,10 @@ __device__ __forceinline__ uint64_t globaltimer() {
 }
 
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;  // 4 s per barrier wait
+// The FP32 operator resolves the relative residual (P^-1 norm) to about
+// 1e-6 on stiff cloth; below that the directions lose conjugacy and a solve
+// can diverge. The mixed form never asks for less.
+constexpr double kMixedTolFloor = 1e-6;
 constexpr int kMaxRed = 4;
 
 struct Shared {
@@ -99,19 +103,28 @@ template <int NV>
 __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV : 1]) {
   SyncState* s = a.sync;
   const unsigned buf = sh.rbuf & 1u;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if constexpr (NV > 0) {
-    double loc[NV];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) loc[k] = v[k];
-    block_sum<NV>(sh, loc);
-    if (threadIdx.x == 0) {
+    for (int k = 0; k < NV; ++k) {
+      double x = v[k];
 #pragma unroll
-      for (int k = 0; k < NV; ++k) a.partials[(buf * kMaxRed + k) * gridDim.x + blockIdx.x] = loc[k];
-      sh.rbuf += 1;  // every thread read the parity at entry, before block_sum's barriers
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if (lane == 0) sh.red[k][warp] = x;
     }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    if constexpr (NV > 0) {
+      const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        double t = 0.0;
+        for (int w = 0; w < nw; ++w) t += sh.red[k][w];
+        a.partials[(buf * kMaxRed + k) * gridDim.x + blockIdx.x] = t;
+      }
+      sh.rbuf += 1;  // every thread read the parity at entry, before the barrier above
+    }
     const unsigned target = (sh.epoch + 1) * gridDim.x;
     atom_add_release(&s->count, 1u);
     const uint64_t t0 = globaltimer();
@@ -130,17 +143,21 @@ __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV
   __syncthreads();
   if (sh.err != 0) return false;
   if constexpr (NV > 0) {
-    double loc[NV];
+    // warp 0 adds the block partials in block order (fixed per lane, then a
+    // fixed xor tree): every block gets the same bits
+    if (warp == 0) {
 #pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      double x = 0.0;
-      for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
-        x += __ldcg(&a.partials[(buf * kMaxRed + k) * gridDim.x + b]);
-      loc[k] = x;
+      for (int k = 0; k < NV; ++k) {
+        double x = 0.0;
+        for (unsigned b = lane; b < gridDim.x; b += 32) x += __ldcg(&a.partials[(buf * kMaxRed + k) * gridDim.x + b]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sh.res[k] = x;
+      }
     }
-    block_sum<NV>(sh, loc);
+    __syncthreads();
 #pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = loc[k];
+    for (int k = 0; k < NV; ++k) v[k] = sh.res[k];
   }
   return true;
 }
@@ -458,8 +475,11 @@ __device__ void apply_elements(const StepArgs& a, const View<R>& vw, R beta) {
     const R4<R> g0 = vw.b_grad[4 * b], g1 = vw.b_grad[4 * b + 1], g2 = vw.b_grad[4 * b + 2], g3 = vw.b_grad[4 * b + 3];
     const R4<R> c0 = next_dir<R>(vw.cw[id.x], beta), c1 = next_dir<R>(vw.cw[id.y], beta),
                 c2 = next_dir<R>(vw.cw[id.z], beta), c3 = next_dir<R>(vw.cw[id.w], beta);
-    const R gp = g0.x * c0.x + g0.y * c0.y + g0.z * c0.z + g1.x * c1.x + g1.y * c1.y + g1.z * c1.z + g2.x * c2.x +
-                 g2.y * c2.y + g2.z * c2.z + g3.x * c3.x + g3.y * c3.y + g3.z * c3.z;
+    // the four gradients sum to zero (the angle does not change under a
+    // translation), so only differences to point 0 enter
+    const R gp = g1.x * (c1.x - c0.x) + g1.y * (c1.y - c0.y) + g1.z * (c1.z - c0.z) + g2.x * (c2.x - c0.x) +
+                 g2.y * (c2.y - c0.y) + g2.z * (c2.z - c0.z) + g3.x * (c3.x - c0.x) + g3.y * (c3.y - c0.y) +
+                 g3.z * (c3.z - c0.z);
     const R s = g0.w * gp;
     vw.slot[ps.x] = {g0.x * s, g0.y * s, g0.z * s, R(0)};
     vw.slot[ps.y] = {g1.x * s, g1.y * s, g1.z * s, R(0)};
@@ -594,7 +614,8 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
   if (!grid_sync<2>(a, sh, red)) return false;
   double delta = red[0];
   const double bb = red[1];
-  const double ziel = fmax(a.tol * a.tol * fmax(bb, delta), a.boden);
+  const double tol = sizeof(R) == 4 ? fmax(a.tol, kMixedTolFloor) : a.tol;
+  const double ziel = fmax(tol * tol * fmax(bb, delta), a.boden);
   int64_t it = 0;
   double beta = 0.0;
   breakdown = false;
@@ -763,7 +784,7 @@ __global__ void __launch_bounds__(kBlock) build_points_kernel(const __grid_const
 // PCG with the release test (persistent, cooperative): MODE_STEP runs up to
 // two solves with a release pass after each, MODE_SOLVE one solve.
 template <typename R>
-__global__ void __launch_bounds__(kSolveBlock) solve_kernel(const __grid_constant__ StepArgs a) {
+__global__ void __launch_bounds__(kSolveBlock, sizeof(R) == 4 ? 2 : 1) solve_kernel(const __grid_constant__ StepArgs a) {
   __shared__ Shared sh;
   if (threadIdx.x == 0) {
     sh.epoch = 0;
