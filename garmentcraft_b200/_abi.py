@@ -124,6 +124,8 @@ class K3dStats(C.Structure):
         ("selbst_stoesse", C.c_int64),
         ("durchdringungen", C.c_int64),
         ("durchdringungsgebiete", C.c_int64),
+        ("zusammenbrueche", C.c_int64),
+        ("dv_max", C.c_double),
     ]
 
 

@@ -579,6 +579,8 @@ static k3d_status read_stats(k3d_solver* h, k3d_stats* out) {
     out->haftend = st[ST_STICKING];
     out->freigegeben = st[ST_RELEASED];
     out->rest_max = rm[0];
+    out->zusammenbrueche = st[ST_BREAKDOWNS];
+    out->dv_max = rm[1];
   }
   if (st[ST_NONFINITE] > 0) return fail(h, K3D_NON_FINITE, "non-finite position or velocity after the step");
   return K3D_OK;

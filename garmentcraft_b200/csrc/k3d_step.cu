@@ -162,6 +162,20 @@ __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV
   return true;
 }
 
+// Grid-wide maximum of one non-negative double (bit pattern order equals
+// value order for non-negative doubles, so an integer atomicMax is exact).
+__device__ bool grid_max(const StepArgs& a, Shared& sh, double (&v)[1]) {
+  double x = v[0];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+  if ((threadIdx.x & 31) == 0 && x > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(&a.stat_rest_max[1]), (unsigned long long)__double_as_longlong(x));
+  double none[1] = {0.0};
+  if (!grid_sync<0>(a, sh, none)) return false;
+  v[0] = __longlong_as_double((long long)__ldcg(reinterpret_cast<const unsigned long long*>(&a.stat_rest_max[1])));
+  return true;
+}
+
 __device__ __forceinline__ bool barrier(const StepArgs& a, Shared& sh) {
   double none[1] = {0.0};
   return grid_sync<0>(a, sh, none);
@@ -800,6 +814,12 @@ __global__ void __launch_bounds__(kSolveBlock, sizeof(R) == 4 ? 2 : 1) solve_ker
   double rest = 0.0;
   for (int pass = 0; pass < 2; ++pass) {
     if (!pcg<R>(a, vw, sh, iters, unconv, brk, rest)) return;
+    double dvm[1] = {0.0};
+    K3D_FOR(i, a.n) {
+      const D3 d = ld3(a.dv, uint32_t(i));
+      dvm[0] = fmax(dvm[0], fmax(fabs(d.x), fmax(fabs(d.y), fabs(d.z))));
+    }
+    if (!grid_max(a, sh, dvm)) return;
     if (lead) {
       a.stats[ST_CG_ITERATIONS] += iters;
       a.stats[ST_SOLVES] += 1;

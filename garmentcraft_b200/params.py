@@ -56,6 +56,8 @@ class ImplizitStatistik:
     selbst_stoesse: int = 0
     durchdringungen: int = 0
     durchdringungsgebiete: int = 0
+    zusammenbrueche: int = 0
+    dv_max: float = 0.0
 
     @classmethod
     def from_c(cls, st: _abi.K3dStats) -> "ImplizitStatistik":

@@ -141,6 +141,10 @@ typedef struct k3d_stats {
   int64_t selbst_stoesse;
   int64_t durchdringungen;
   int64_t durchdringungsgebiete;
+  /* not in ImplizitStatistik: solves that stopped on the CG breakdown guard
+   * (implizit.rs:406-408), and the largest |dv| component of the frame's solves */
+  int64_t zusammenbrueche;
+  double dv_max;
 } k3d_stats;
 
 /* CgLauf (sim/src/implizit.rs:294-299). */
