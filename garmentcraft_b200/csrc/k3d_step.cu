@@ -637,7 +637,11 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     const R rb = R(beta);
     apply_elements<R>(a, vw, rb);
     if (!barrier(a, sh)) return false;
-    double ca[1] = {0.0};
+    // ca = c.Ac and, for the FP32 operator, cm = c.M(1+hc)c: the Hessian part
+    // is positive semi-definite, so c.Ac >= cm holds exactly; an FP32 product
+    // that falls far below it has lost the direction and the solve stops
+    // there as at a breakdown (the FP64 form keeps the reference's test only).
+    double ca[2] = {0.0, 0.0};
     K3D_FOR(i, a.n) {
       const R4<R> ci = next_dir<R>(vw.cw[i], rb);
       vw.cw[i].c = ci;
@@ -650,14 +654,23 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
         ay = m * ci.y + R(h2) * hy;
         az = m * ci.z + R(h2) * hz;
         filt<R>(vw.nrm, i, ax, ay, az);
+        if (sizeof(R) == 4)
+          ca[1] += double(m) * (double(ci.x) * double(ci.x) + double(ci.y) * double(ci.y) +
+                                double(ci.z) * double(ci.z));
       }
       vw.ap[3 * i] = ax;
       vw.ap[3 * i + 1] = ay;
       vw.ap[3 * i + 2] = az;
       ca[0] += double(ci.x) * double(ax) + double(ci.y) * double(ay) + double(ci.z) * double(az);
     }
-    if (!grid_sync<1>(a, sh, ca)) return false;
-    if (ca[0] <= DBL_MIN || !isfinite(ca[0])) {
+    if (sizeof(R) == 4) {
+      if (!grid_sync<2>(a, sh, ca)) return false;
+    } else {
+      double c1[1] = {ca[0]};
+      if (!grid_sync<1>(a, sh, c1)) return false;
+      ca[0] = c1[0];
+    }
+    if (ca[0] <= DBL_MIN || !isfinite(ca[0]) || (sizeof(R) == 4 && ca[0] < 0.5 * ca[1])) {
       breakdown = true;
       break;
     }
