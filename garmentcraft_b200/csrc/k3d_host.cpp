@@ -80,7 +80,7 @@ struct Carve {
   uint4 *m_idx, *b_idx, *s_idx, *m_pos, *b_pos;
   uint2* s_pos;
   double4 *m_r, *m_basis, *m_mat;
-  void *m_rin, *m_kgA;
+  void *m_rin, *m_kgA, *m_rin64, *m_kgA64;
   double2 *b_kr, *s_kl;
 };
 
@@ -154,6 +154,18 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.partials = A.take<double>(size_t(8) * h->blocks);  // two buffers of 4 sums per block
   a.stats = A.take<long long>(ST_COUNT);
   a.stat_rest_max = A.take<double>(2);
+  cv.m_rin64 = cv.m_kgA64 = nullptr;
+  if (R == 4) {  // FP64 operator copies for the residuals of the mixed form
+    a.m_f1w64 = A.take<double4>(T);
+    a.m_f2w64 = A.take<double4>(T);
+    a.m_kgB64 = A.take<double4>(T);
+    a.m_rin64 = cv.m_rin64 = A.take<double4>(T);
+    a.m_kgA64 = cv.m_kgA64 = A.take<double4>(T);
+    a.b_grad64 = A.take<double4>(4 * B);
+    a.s_dq64 = A.take<double4>(S);
+    a.s_k64 = A.take<double>(S);
+    a.slot64 = A.take<double4>(nslots);
+  }
 }
 
 extern "C" {
@@ -397,6 +409,7 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
   std::vector<double4> m_r(nt), m_basis(nt), m_mat(nt);
   std::vector<double2> b_kr(nb);
   std::vector<char> m_rin(size_t(nt) * 4 * R), m_kgA(size_t(nt) * 4 * R);
+  std::vector<double4> m_rin64(R == 4 ? nt : 0), m_kgA64(R == 4 ? nt : 0);
   for (int64_t t = 0; t < nt; ++t) {
     const uint32_t* p = s->membran_punkte + 3 * t;
     m_idx[t] = make_uint4(p[0], p[1], p[2], 0u);
@@ -414,6 +427,8 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
       std::memcpy(&m_rin[size_t(t) * 32], rin, 32);
       std::memcpy(&m_kgA[size_t(t) * 32], kga, 32);
     } else {
+      m_rin64[t] = make_double4(rin[0], rin[1], rin[2], rin[3]);
+      m_kgA64[t] = make_double4(kga[0], kga[1], kga[2], kga[3]);
       float fr[4], fk[4];
       for (int q = 0; q < 4; ++q) {
         fr[q] = float(rin[q]);
@@ -479,6 +494,10 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
   K3D_CUDA(h, up(cv.m_mat, m_mat.data(), 32 * T));
   K3D_CUDA(h, up(cv.m_rin, m_rin.data(), m_rin.size()));
   K3D_CUDA(h, up(cv.m_kgA, m_kgA.data(), m_kgA.size()));
+  if (cv.m_rin64) {
+    K3D_CUDA(h, up(cv.m_rin64, m_rin64.data(), 32 * T));
+    K3D_CUDA(h, up(cv.m_kgA64, m_kgA64.data(), 32 * T));
+  }
   K3D_CUDA(h, up(cv.b_idx, b_idx.data(), 16 * B));
   K3D_CUDA(h, up(cv.b_kr, b_kr.data(), 16 * B));
   K3D_CUDA(h, up(cv.s_idx, s_idx.data(), 16 * S));

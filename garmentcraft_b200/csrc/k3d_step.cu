@@ -46,6 +46,11 @@ constexpr uint64_t kBarrierLimitNs = 4000000000ull;  // 4 s per barrier wait
 // 1e-6 on stiff cloth; below that the directions lose conjugacy and a solve
 // can diverge. The mixed form never asks for less.
 constexpr double kMixedTolFloor = 1e-6;
+// Reliable updates of the mixed form: the true residual replaces the
+// recursive one once r.z has fallen by kReliable since the last update, or
+// grown by kGrow (then the direction restarts).
+constexpr double kReliable = 1e-2;
+constexpr double kGrow = 1e2;
 constexpr int kMaxRed = 4;
 
 struct Shared {
@@ -310,6 +315,11 @@ __device__ void build_elements(const StepArgs& a, const View<R>& vw) {
     vw.m_f1w[t] = {R(f1.x), R(f1.y), R(f1.z), R(w.x)};
     vw.m_f2w[t] = {R(f2.x), R(f2.y), R(f2.z), R(w.y)};
     vw.m_kgB[t] = {R(kg[4]), R(kg[5]), R(w.z), R(0)};
+    if (a.m_f1w64) {
+      static_cast<R4<double>*>(a.m_f1w64)[t] = rf1;
+      static_cast<R4<double>*>(a.m_f2w64)[t] = rf2;
+      static_cast<R4<double>*>(a.m_kgB64)[t] = kb;
+    }
   }
   K3D_FOR(b, a.nb) {
     const uint4 id = __ldg(&a.b_idx[b]);
@@ -331,6 +341,7 @@ __device__ void build_elements(const StepArgs& a, const View<R>& vw) {
     for (int q = 0; q < 4; ++q) {
       a.b_bc[4 * b + q] = make_double4(gr[q].x * sb, gr[q].y * sb, gr[q].z * sb, 0.0);
       vw.b_grad[4 * b + q] = {R(gr[q].x), R(gr[q].y), R(gr[q].z), R(kr.x)};
+      if (a.b_grad64) static_cast<R4<double>*>(a.b_grad64)[4 * b + q] = {gr[q].x, gr[q].y, gr[q].z, kr.x};
     }
   }
   K3D_FOR(s, a.ns) {
@@ -367,6 +378,10 @@ __device__ void build_elements(const StepArgs& a, const View<R>& vw) {
     if (a.need_load) a.s_lc[s] = zug ? make_double4(F.x, F.y, F.z, 0.0) : make_double4(0, 0, 0, 0);
     vw.s_dq[s] = {R(n.x), R(n.y), R(n.z), R(quer)};
     vw.s_k[s] = R(k);
+    if (a.s_dq64) {
+      static_cast<R4<double>*>(a.s_dq64)[s] = {n.x, n.y, n.z, quer};
+      static_cast<double*>(a.s_k64)[s] = k;
+    }
   }
 }
 
@@ -514,6 +529,77 @@ __device__ void apply_elements(const StepArgs& a, const View<R>& vw, R beta) {
   }
 }
 
+// The operator in FP64 applied to dv, from the FP64 record copies: the
+// residuals of the mixed form (start, reliable updates, release test).
+__device__ __noinline__ void apply_dv64(const StepArgs& a) {
+  const R4<double>* f1w = static_cast<const R4<double>*>(a.m_f1w64);
+  const R4<double>* f2w = static_cast<const R4<double>*>(a.m_f2w64);
+  const R4<double>* kgB = static_cast<const R4<double>*>(a.m_kgB64);
+  const R4<double>* rin = static_cast<const R4<double>*>(a.m_rin64);
+  const R4<double>* kgA = static_cast<const R4<double>*>(a.m_kgA64);
+  const R4<double>* grad = static_cast<const R4<double>*>(a.b_grad64);
+  const R4<double>* sdq = static_cast<const R4<double>*>(a.s_dq64);
+  const double* sk = static_cast<const double*>(a.s_k64);
+  R4<double>* slot = static_cast<R4<double>*>(a.slot64);
+  auto dvp = [&](uint32_t i) -> R4<double> {
+    const D3 d = ld3(a.dv, i);
+    return {d.x, d.y, d.z, 0.0};
+  };
+  K3D_FOR(t, a.nt) {
+    const uint4 id = __ldg(&a.m_idx[t]);
+    const uint4 ps = __ldg(&a.m_pos[t]);
+    const R4<double> d[3] = {dvp(id.x), dvp(id.y), dvp(id.z)};
+    R4<double> out[3];
+    membran_hv<double>(f1w[t], f2w[t], rin[t], kgA[t], kgB[t], d, out);
+    slot[ps.x] = out[0];
+    slot[ps.y] = out[1];
+    slot[ps.z] = out[2];
+  }
+  K3D_FOR(b, a.nb) {
+    const uint4 id = __ldg(&a.b_idx[b]);
+    const uint4 ps = __ldg(&a.b_pos[b]);
+    const R4<double> g0 = grad[4 * b], g1 = grad[4 * b + 1], g2 = grad[4 * b + 2], g3 = grad[4 * b + 3];
+    const R4<double> c0 = dvp(id.x), c1 = dvp(id.y), c2 = dvp(id.z), c3 = dvp(id.w);
+    const double gp = g1.x * (c1.x - c0.x) + g1.y * (c1.y - c0.y) + g1.z * (c1.z - c0.z) + g2.x * (c2.x - c0.x) +
+                      g2.y * (c2.y - c0.y) + g2.z * (c2.z - c0.z) + g3.x * (c3.x - c0.x) + g3.y * (c3.y - c0.y) +
+                      g3.z * (c3.z - c0.z);
+    const double sc = g0.w * gp;
+    slot[ps.x] = {g0.x * sc, g0.y * sc, g0.z * sc, 0.0};
+    slot[ps.y] = {g1.x * sc, g1.y * sc, g1.z * sc, 0.0};
+    slot[ps.z] = {g2.x * sc, g2.y * sc, g2.z * sc, 0.0};
+    slot[ps.w] = {g3.x * sc, g3.y * sc, g3.z * sc, 0.0};
+  }
+  K3D_FOR(s, a.ns) {
+    const uint4 id = __ldg(&a.s_idx[s]);
+    const uint2 ps = __ldg(&a.s_pos[s]);
+    const R4<double> dq = sdq[s];
+    const double k = sk[s];
+    const R4<double> ci = dvp(id.x), cj = dvp(id.y);
+    const double dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
+    const double nd = (dq.x * dx + dq.y * dy + dq.z * dz) * (1.0 - dq.w);
+    const double ox = k * (dq.x * nd + dx * dq.w), oy = k * (dq.y * nd + dy * dq.w), oz = k * (dq.z * nd + dz * dq.w);
+    slot[ps.x] = {ox, oy, oz, 0.0};
+    slot[ps.y] = {-ox, -oy, -oz, 0.0};
+  }
+}
+
+// (A dv)_i in FP64 from the slots of apply_dv64.
+__device__ __noinline__ D3 a_dv64(const StepArgs& a, int64_t i) {
+  const R4<double>* sl = static_cast<const R4<double>*>(a.slot64) + i;
+  double x = 0, y = 0, z = 0;
+  const uint32_t cnt = __ldg(&a.cnt_v[i]);
+#pragma unroll 6
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const R4<double> o = sl[size_t(k) * a.np];
+    x += o.x;
+    y += o.y;
+    z += o.z;
+  }
+  const double h2 = a.h * a.h, md = a.masse[i] * (1.0 + a.h * a.daempf);
+  const D3 d = ld3(a.dv, uint32_t(i));
+  return d3(md * d.x + h2 * x, md * d.y + h2 * y, md * d.z + h2 * z);
+}
+
 // H p at point i: the sum of its corner slots, rank by rank (coalesced over
 // consecutive points).
 template <typename R>
@@ -588,22 +674,34 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     vw.cw[i].c = {R(0), R(0), R(0), R(0)};
   }
   if (!barrier(a, sh)) return false;
-  apply_elements<R>(a, vw, R(0));
+  // the mixed form takes its residuals from the FP64 operator
+  const bool hi = a.m_f1w64 != nullptr;
+  if (hi)
+    apply_dv64(a);
+  else
+    apply_elements<R>(a, vw, R(0));
   if (!barrier(a, sh)) return false;
   double red[2] = {0.0, 0.0};
   K3D_FOR(i, a.n) {
-    R hx, hy, hz;
-    gather_h<R>(a, vw, i, hx, hy, hz);
-    const R4<R> pi = vw.cw[i].w;
-    const R m = vw.md[i];
     R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, cx = 0, cy = 0, cz = 0;
     if (a.frei[i]) {
-      const R ax = m * pi.x + R(h2) * hx, ay = m * pi.y + R(h2) * hy, az = m * pi.z + R(h2) * hz;
       const D3 b = ld3(a.b, uint32_t(i));
-      rx = R(b.x - double(ax));
-      ry = R(b.y - double(ay));
-      rz = R(b.z - double(az));
-      filt<R>(vw.nrm, i, rx, ry, rz);
+      D3 ad;
+      if (hi) {
+        ad = a_dv64(a, i);
+      } else {
+        R hx, hy, hz;
+        gather_h<R>(a, vw, i, hx, hy, hz);
+        const R4<R> pi = vw.cw[i].w;
+        const R m = vw.md[i];
+        ad = d3(double(m * pi.x + R(h2) * hx), double(m * pi.y + R(h2) * hy), double(m * pi.z + R(h2) * hz));
+      }
+      const D3 n = ld3(a.nrm_d, uint32_t(i));
+      D3 rd = b - ad;
+      rd = rd - n * dot(rd, n);
+      rx = R(rd.x);
+      ry = R(rd.y);
+      rz = R(rd.z);
       R fx = R(b.x), fy = R(b.y), fz = R(b.z);
       filt<R>(vw.nrm, i, fx, fy, fz);
       R px, py, pz;
@@ -631,7 +729,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
   const double tol = sizeof(R) == 4 ? fmax(a.tol, kMixedTolFloor) : a.tol;
   const double ziel = fmax(tol * tol * fmax(bb, delta), a.boden);
   int64_t it = 0;
-  double beta = 0.0;
+  double beta = 0.0, delta_ref = delta;
   breakdown = false;
   while (delta > ziel && it < a.cg_max) {
     const R rb = R(beta);
@@ -696,8 +794,47 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       rzs[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rzz) * double(zz);
     }
     if (!grid_sync<1>(a, sh, rzs)) return false;
-    beta = rzs[0] / delta;
+    double beta_next = rzs[0] / delta;
+    const double delta_prev = delta;
     delta = rzs[0];
+    if (hi && (delta < kReliable * delta_ref || delta > kGrow * delta_ref)) {
+      // reliable update: replace the recursive FP32 residual by the true one,
+      // S (b - A dv) with the FP64 operator; restart the direction if the
+      // residual grew
+      const bool restart = delta > kGrow * delta_ref;
+      apply_dv64(a);
+      if (!barrier(a, sh)) return false;
+      double rz2[1] = {0.0};
+      K3D_FOR(i, a.n) {
+        R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, wx = 0, wy = 0, wz = 0;
+        if (a.frei[i]) {
+          const D3 n = ld3(a.nrm_d, uint32_t(i));
+          D3 rd = ld3(a.b, uint32_t(i)) - a_dv64(a, i);
+          rd = rd - n * dot(rd, n);
+          rx = R(rd.x);
+          ry = R(rd.y);
+          rz = R(rd.z);
+          pmul<R>(vw.pinv, i, rx, ry, rz, zx, zy, zz);
+          wx = zx;
+          wy = zy;
+          wz = zz;
+          filt<R>(vw.nrm, i, wx, wy, wz);
+          rz2[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rz) * double(zz);
+        }
+        vw.r[3 * i] = rx;
+        vw.r[3 * i + 1] = ry;
+        vw.r[3 * i + 2] = rz;
+        vw.z[3 * i] = zx;
+        vw.z[3 * i + 1] = zy;
+        vw.z[3 * i + 2] = zz;
+        vw.cw[i].w = {wx, wy, wz, R(0)};
+      }
+      if (!grid_sync<1>(a, sh, rz2)) return false;
+      delta = rz2[0];
+      beta_next = restart ? 0.0 : delta / delta_prev;
+      delta_ref = delta;
+    }
+    beta = beta_next;
     ++it;
   }
   iters = it;
@@ -711,22 +848,32 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
 // contact normal; a held point that pulls on the body is released.
 template <typename R>
 __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double& released) {
-  dv_to_w<R>(a, vw);
-  if (!barrier(a, sh)) return false;
-  apply_elements<R>(a, vw, R(0));
+  const bool hi = a.m_f1w64 != nullptr;
+  if (hi) {
+    apply_dv64(a);
+  } else {
+    dv_to_w<R>(a, vw);
+    if (!barrier(a, sh)) return false;
+    apply_elements<R>(a, vw, R(0));
+  }
   if (!barrier(a, sh)) return false;
   const double h2 = a.h * a.h;
   double cnt[1] = {0.0};
   K3D_FOR(i, a.n) {
     const D3 n = ld3(a.nrm_d, uint32_t(i));
     if (n.x == 0.0 && n.y == 0.0 && n.z == 0.0) continue;
-    R hx, hy, hz;
-    gather_h<R>(a, vw, i, hx, hy, hz);
-    const R4<R> ci = vw.cw[i].w;
-    const R m = vw.md[i];
     const D3 b = ld3(a.b, uint32_t(i));
-    const D3 rest = d3(double(m * ci.x + R(h2) * hx) - b.x, double(m * ci.y + R(h2) * hy) - b.y,
-                       double(m * ci.z + R(h2) * hz) - b.z);
+    D3 rest;
+    if (hi) {
+      rest = a_dv64(a, i) - b;
+    } else {
+      R hx, hy, hz;
+      gather_h<R>(a, vw, i, hx, hy, hz);
+      const R4<R> ci = vw.cw[i].w;
+      const R m = vw.md[i];
+      rest = d3(double(m * ci.x + R(h2) * hx) - b.x, double(m * ci.y + R(h2) * hy) - b.y,
+                double(m * ci.z + R(h2) * hz) - b.z);
+    }
     const double fn = dot(rest, n) / a.h;
     if (fn < 0.0) {
       st3(a.nrm_d, uint32_t(i), d3(0, 0, 0));

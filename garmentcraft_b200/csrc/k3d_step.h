@@ -74,6 +74,10 @@ struct StepArgs {
   const double2* s_kl;
   double4 *s_bc, *s_lc;
   void *s_dq, *s_k;
+  // FP64 copies of the operator records for the residuals of the mixed form
+  // (start residual, reliable updates, release test); null in the FP64 form
+  void *m_f1w64, *m_f2w64, *m_kgB64, *b_grad64, *s_dq64, *s_k64, *slot64;
+  const void *m_rin64, *m_kgA64;
   // probes
   const double* p_in;
   double* p_out;
