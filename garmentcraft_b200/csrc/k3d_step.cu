@@ -207,28 +207,21 @@ __device__ __forceinline__ R4<R> next_dir(const CW<R>& q, R beta) {
   return {fmar(beta, q.c.x, q.w.x), fmar(beta, q.c.y, q.w.y), fmar(beta, q.c.z, q.w.z), R(0)};
 }
 
-// Typed access to the precision-dependent arrays. The pointers are read from
-// the kernel's constant parameter block on use, so they cost no registers.
 template <typename R>
 struct View {
-  const StepArgs& a;
-  __device__ explicit View(const StepArgs& args) : a(args) {}
-  __device__ __forceinline__ CW<R>* cw() const { return static_cast<CW<R>*>(a.c); }
-  __device__ __forceinline__ R* r() const { return static_cast<R*>(a.r); }
-  __device__ __forceinline__ R* z() const { return static_cast<R*>(a.z); }
-  __device__ __forceinline__ R* ap() const { return static_cast<R*>(a.ap); }
-  __device__ __forceinline__ R* pinv() const { return static_cast<R*>(a.pinv); }
-  __device__ __forceinline__ R* nrm() const { return static_cast<R*>(a.nrm); }
-  __device__ __forceinline__ R* md() const { return static_cast<R*>(a.md); }
-  __device__ __forceinline__ R4<R>* m_f1w() const { return static_cast<R4<R>*>(a.m_f1w); }
-  __device__ __forceinline__ R4<R>* m_f2w() const { return static_cast<R4<R>*>(a.m_f2w); }
-  __device__ __forceinline__ R4<R>* m_kgB() const { return static_cast<R4<R>*>(a.m_kgB); }
-  __device__ __forceinline__ const R4<R>* m_rin() const { return static_cast<const R4<R>*>(a.m_rin); }
-  __device__ __forceinline__ const R4<R>* m_kgA() const { return static_cast<const R4<R>*>(a.m_kgA); }
-  __device__ __forceinline__ R4<R>* b_grad() const { return static_cast<R4<R>*>(a.b_grad); }
-  __device__ __forceinline__ R4<R>* s_dq() const { return static_cast<R4<R>*>(a.s_dq); }
-  __device__ __forceinline__ R* s_k() const { return static_cast<R*>(a.s_k); }
-  __device__ __forceinline__ R4<R>* slot() const { return static_cast<R4<R>*>(a.slot); }
+  CW<R>* cw;
+  R *r, *z, *ap, *pinv, *nrm, *md;
+  R4<R>*m_f1w, *m_f2w, *m_kgB;
+  const R4<R>*m_rin, *m_kgA;
+  R4<R>* b_grad;
+  R4<R>* s_dq;
+  R* s_k;
+  R4<R>* slot;
+  __device__ explicit View(const StepArgs& a)
+      : cw((CW<R>*)a.c), r((R*)a.r), z((R*)a.z), ap((R*)a.ap), pinv((R*)a.pinv), nrm((R*)a.nrm), md((R*)a.md),
+        m_f1w((R4<R>*)a.m_f1w), m_f2w((R4<R>*)a.m_f2w), m_kgB((R4<R>*)a.m_kgB),
+        m_rin((const R4<R>*)a.m_rin), m_kgA((const R4<R>*)a.m_kgA), b_grad((R4<R>*)a.b_grad),
+        s_dq((R4<R>*)a.s_dq), s_k((R*)a.s_k), slot((R4<R>*)a.slot) {}
 };
 
 __device__ __forceinline__ double4 ldg4(const double4* p) {
@@ -319,9 +312,9 @@ __device__ void build_elements(const StepArgs& a, const View<R>& vw) {
       dc[4] = j[0].x * u[0].z + j[1].x * u[1].z + j[2].x * u[2].z;
       dc[5] = j[0].y * u[0].z + j[1].y * u[1].z + j[2].y * u[2].z;
     }
-    vw.m_f1w()[t] = {R(f1.x), R(f1.y), R(f1.z), R(w.x)};
-    vw.m_f2w()[t] = {R(f2.x), R(f2.y), R(f2.z), R(w.y)};
-    vw.m_kgB()[t] = {R(kg[4]), R(kg[5]), R(w.z), R(0)};
+    vw.m_f1w[t] = {R(f1.x), R(f1.y), R(f1.z), R(w.x)};
+    vw.m_f2w[t] = {R(f2.x), R(f2.y), R(f2.z), R(w.y)};
+    vw.m_kgB[t] = {R(kg[4]), R(kg[5]), R(w.z), R(0)};
     if (a.m_f1w64) {
       static_cast<R4<double>*>(a.m_f1w64)[t] = rf1;
       static_cast<R4<double>*>(a.m_f2w64)[t] = rf2;
@@ -347,7 +340,7 @@ __device__ void build_elements(const StepArgs& a, const View<R>& vw) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       a.b_bc[4 * b + q] = make_double4(gr[q].x * sb, gr[q].y * sb, gr[q].z * sb, 0.0);
-      vw.b_grad()[4 * b + q] = {R(gr[q].x), R(gr[q].y), R(gr[q].z), R(kr.x)};
+      vw.b_grad[4 * b + q] = {R(gr[q].x), R(gr[q].y), R(gr[q].z), R(kr.x)};
       if (a.b_grad64) static_cast<R4<double>*>(a.b_grad64)[4 * b + q] = {gr[q].x, gr[q].y, gr[q].z, kr.x};
     }
   }
@@ -383,8 +376,8 @@ __device__ void build_elements(const StepArgs& a, const View<R>& vw) {
     const D3 bd = (n * (dot(n, dv) * (1.0 - quer)) + dv * quer) * k;
     a.s_bc[s] = make_double4(F.x - bd.x * h, F.y - bd.y * h, F.z - bd.z * h, 0.0);
     if (a.need_load) a.s_lc[s] = zug ? make_double4(F.x, F.y, F.z, 0.0) : make_double4(0, 0, 0, 0);
-    vw.s_dq()[s] = {R(n.x), R(n.y), R(n.z), R(quer)};
-    vw.s_k()[s] = R(k);
+    vw.s_dq[s] = {R(n.x), R(n.y), R(n.z), R(quer)};
+    vw.s_k[s] = R(k);
     if (a.s_dq64) {
       static_cast<R4<double>*>(a.s_dq64)[s] = {n.x, n.y, n.z, quer};
       static_cast<double*>(a.s_k64)[s] = k;
@@ -420,7 +413,7 @@ __device__ void build_points(const StepArgs& a, const View<R>& vw, double& held)
       const uint32_t q = __ldg(&a.ent_b[e]);
       const double4 bc = a.b_bc[q];
       acc = acc + d3(bc.x, bc.y, bc.z);
-      const R4<R> gq = vw.b_grad()[q];
+      const R4<R> gq = vw.b_grad[q];
       const double gx = gq.x, gy = gq.y, gz = gq.z, k = gq.w;
       D[0] += k * gx * gx;
       D[1] += k * gy * gy;
@@ -439,8 +432,8 @@ __device__ void build_points(const StepArgs& a, const View<R>& vw, double& held)
         const double4 lc = a.s_lc[s];
         load = load + d3(lc.x, lc.y, lc.z) * sg;
       }
-      const R4<R> dq = vw.s_dq()[s];
-      const double k = vw.s_k()[s], nx = dq.x, ny = dq.y, nz = dq.z, qu = dq.w;
+      const R4<R> dq = vw.s_dq[s];
+      const double k = vw.s_k[s], nx = dq.x, ny = dq.y, nz = dq.z, qu = dq.w;
       const double kn = k * (1.0 - qu), kq = k * qu;
       D[0] += kq + kn * nx * nx;
       D[1] += kq + kn * ny * ny;
@@ -456,8 +449,8 @@ __device__ void build_points(const StepArgs& a, const View<R>& vw, double& held)
     double P[6];
     m3_inv_sym(A, P);
 #pragma unroll
-    for (int k = 0; k < 6; ++k) vw.pinv()[6 * i + k] = R(P[k]);
-    vw.md()[i] = R(mdi);
+    for (int k = 0; k < 6; ++k) vw.pinv[6 * i + k] = R(P[k]);
+    vw.md[i] = R(mdi);
     // contact set: the last body that reports a contact wins (implizit.rs:873-883)
     D3 nrm = d3(0, 0, 0);
     double vn_soll = 0.0;
@@ -478,9 +471,9 @@ __device__ void build_points(const StepArgs& a, const View<R>& vw, double& held)
       }
     }
     st3(a.nrm_d, uint32_t(i), nrm);
-    vw.nrm()[3 * i] = R(nrm.x);
-    vw.nrm()[3 * i + 1] = R(nrm.y);
-    vw.nrm()[3 * i + 2] = R(nrm.z);
+    vw.nrm[3 * i] = R(nrm.x);
+    vw.nrm[3 * i + 1] = R(nrm.y);
+    vw.nrm[3 * i + 2] = R(nrm.z);
     a.vn_soll[i] = vn_soll;
     st3(a.vk, uint32_t(i), vb);
     a.fnk[i] = 0.0;
@@ -497,42 +490,42 @@ __device__ void apply_elements(const StepArgs& a, const View<R>& vw, R beta) {
   K3D_FOR(t, a.nt) {
     const uint4 id = __ldg(&a.m_idx[t]);
     const uint4 ps = __ldg(&a.m_pos[t]);
-    const R4<R> d[3] = {next_dir<R>(vw.cw()[id.x], beta), next_dir<R>(vw.cw()[id.y], beta),
-                        next_dir<R>(vw.cw()[id.z], beta)};
+    const R4<R> d[3] = {next_dir<R>(vw.cw[id.x], beta), next_dir<R>(vw.cw[id.y], beta),
+                        next_dir<R>(vw.cw[id.z], beta)};
     R4<R> out[3];
-    membran_hv<R>(vw.m_f1w()[t], vw.m_f2w()[t], vw.m_rin()[t], vw.m_kgA()[t], vw.m_kgB()[t], d, out);
-    vw.slot()[ps.x] = out[0];
-    vw.slot()[ps.y] = out[1];
-    vw.slot()[ps.z] = out[2];
+    membran_hv<R>(vw.m_f1w[t], vw.m_f2w[t], vw.m_rin[t], vw.m_kgA[t], vw.m_kgB[t], d, out);
+    vw.slot[ps.x] = out[0];
+    vw.slot[ps.y] = out[1];
+    vw.slot[ps.z] = out[2];
   }
   K3D_FOR(b, a.nb) {
     const uint4 id = __ldg(&a.b_idx[b]);
     const uint4 ps = __ldg(&a.b_pos[b]);
-    const R4<R> g0 = vw.b_grad()[4 * b], g1 = vw.b_grad()[4 * b + 1], g2 = vw.b_grad()[4 * b + 2], g3 = vw.b_grad()[4 * b + 3];
-    const R4<R> c0 = next_dir<R>(vw.cw()[id.x], beta), c1 = next_dir<R>(vw.cw()[id.y], beta),
-                c2 = next_dir<R>(vw.cw()[id.z], beta), c3 = next_dir<R>(vw.cw()[id.w], beta);
+    const R4<R> g0 = vw.b_grad[4 * b], g1 = vw.b_grad[4 * b + 1], g2 = vw.b_grad[4 * b + 2], g3 = vw.b_grad[4 * b + 3];
+    const R4<R> c0 = next_dir<R>(vw.cw[id.x], beta), c1 = next_dir<R>(vw.cw[id.y], beta),
+                c2 = next_dir<R>(vw.cw[id.z], beta), c3 = next_dir<R>(vw.cw[id.w], beta);
     // the four gradients sum to zero (the angle does not change under a
     // translation), so only differences to point 0 enter
     const R gp = g1.x * (c1.x - c0.x) + g1.y * (c1.y - c0.y) + g1.z * (c1.z - c0.z) + g2.x * (c2.x - c0.x) +
                  g2.y * (c2.y - c0.y) + g2.z * (c2.z - c0.z) + g3.x * (c3.x - c0.x) + g3.y * (c3.y - c0.y) +
                  g3.z * (c3.z - c0.z);
     const R s = g0.w * gp;
-    vw.slot()[ps.x] = {g0.x * s, g0.y * s, g0.z * s, R(0)};
-    vw.slot()[ps.y] = {g1.x * s, g1.y * s, g1.z * s, R(0)};
-    vw.slot()[ps.z] = {g2.x * s, g2.y * s, g2.z * s, R(0)};
-    vw.slot()[ps.w] = {g3.x * s, g3.y * s, g3.z * s, R(0)};
+    vw.slot[ps.x] = {g0.x * s, g0.y * s, g0.z * s, R(0)};
+    vw.slot[ps.y] = {g1.x * s, g1.y * s, g1.z * s, R(0)};
+    vw.slot[ps.z] = {g2.x * s, g2.y * s, g2.z * s, R(0)};
+    vw.slot[ps.w] = {g3.x * s, g3.y * s, g3.z * s, R(0)};
   }
   K3D_FOR(s, a.ns) {
     const uint4 id = __ldg(&a.s_idx[s]);
     const uint2 ps = __ldg(&a.s_pos[s]);
-    const R4<R> dq = vw.s_dq()[s];
-    const R k = vw.s_k()[s];
-    const R4<R> ci = next_dir<R>(vw.cw()[id.x], beta), cj = next_dir<R>(vw.cw()[id.y], beta);
+    const R4<R> dq = vw.s_dq[s];
+    const R k = vw.s_k[s];
+    const R4<R> ci = next_dir<R>(vw.cw[id.x], beta), cj = next_dir<R>(vw.cw[id.y], beta);
     const R dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
     const R nd = (dq.x * dx + dq.y * dy + dq.z * dz) * (R(1) - dq.w);
     const R ox = k * (dq.x * nd + dx * dq.w), oy = k * (dq.y * nd + dy * dq.w), oz = k * (dq.z * nd + dz * dq.w);
-    vw.slot()[ps.x] = {ox, oy, oz, R(0)};
-    vw.slot()[ps.y] = {-ox, -oy, -oz, R(0)};
+    vw.slot[ps.x] = {ox, oy, oz, R(0)};
+    vw.slot[ps.y] = {-ox, -oy, -oz, R(0)};
   }
 }
 
@@ -613,7 +606,7 @@ template <typename R>
 __device__ __forceinline__ void gather_h(const StepArgs& a, const View<R>& vw, int64_t i, R& hx, R& hy, R& hz) {
   R x = 0, y = 0, z = 0;
   const uint32_t cnt = __ldg(&a.cnt_v[i]);
-  const R4<R>* sl = vw.slot() + i;
+  const R4<R>* sl = vw.slot + i;
 #pragma unroll 6
   for (uint32_t k = 0; k < cnt; ++k) {
     const R4<R> o = sl[size_t(k) * a.np];
@@ -649,182 +642,9 @@ template <typename R>
 __device__ void dv_to_w(const StepArgs& a, const View<R>& vw) {
   K3D_FOR(i, a.n) {
     const D3 d = ld3(a.dv, uint32_t(i));
-    vw.cw()[i].w = {R(d.x), R(d.y), R(d.z), R(0)};
-    vw.cw()[i].c = {R(0), R(0), R(0), R(0)};
+    vw.cw[i].w = {R(d.x), R(d.y), R(d.z), R(0)};
+    vw.cw[i].c = {R(0), R(0), R(0), R(0)};
   }
-}
-
-// The CG phases, out of line so that each loads its own array pointers and
-// the iteration loop keeps only its scalars live.
-template <typename R>
-__device__ __noinline__ void cg_apply(const StepArgs& a, R beta) {
-  const View<R> vw(a);
-  apply_elements<R>(a, vw, beta);
-}
-
-// c = w + beta c, ap = S A c for free points; out = (c.ap, c.M(1+hc)c).
-template <typename R>
-__device__ __noinline__ void cg_point_ap(const StepArgs& a, R rb, double* out) {
-  const View<R> vw(a);
-  const double h2 = a.h * a.h;
-  double ca[2] = {0.0, 0.0};
-    K3D_FOR(i, a.n) {
-      const R4<R> ci = next_dir<R>(vw.cw()[i], rb);
-      vw.cw()[i].c = ci;
-      R ax = 0, ay = 0, az = 0;
-      if (a.frei[i]) {
-        R hx, hy, hz;
-        gather_h<R>(a, vw, i, hx, hy, hz);
-        const R m = vw.md()[i];
-        ax = m * ci.x + R(h2) * hx;
-        ay = m * ci.y + R(h2) * hy;
-        az = m * ci.z + R(h2) * hz;
-        filt<R>(vw.nrm(), i, ax, ay, az);
-        if (sizeof(R) == 4)
-          ca[1] += double(m) * (double(ci.x) * double(ci.x) + double(ci.y) * double(ci.y) +
-                                double(ci.z) * double(ci.z));
-      }
-      vw.ap()[3 * i] = ax;
-      vw.ap()[3 * i + 1] = ay;
-      vw.ap()[3 * i + 2] = az;
-      ca[0] += double(ci.x) * double(ax) + double(ci.y) * double(ay) + double(ci.z) * double(az);
-    }
-  out[0] = ca[0];
-  out[1] = ca[1];
-}
-
-// dv += alpha c, r -= alpha ap, z = P r, w = S z; returns the partial r.z.
-template <typename R>
-__device__ __noinline__ double cg_point_update(const StepArgs& a, double alpha) {
-  const View<R> vw(a);
-  double rzs[1] = {0.0};
-    K3D_FOR(i, a.n) {
-      const R4<R> ci = vw.cw()[i].c;
-      D3 d = ld3(a.dv, uint32_t(i));
-      d = d + d3(double(ci.x), double(ci.y), double(ci.z)) * alpha;
-      st3(a.dv, uint32_t(i), d);
-      const R rx = R(double(vw.r()[3 * i]) - alpha * double(vw.ap()[3 * i]));
-      const R ry = R(double(vw.r()[3 * i + 1]) - alpha * double(vw.ap()[3 * i + 1]));
-      const R rzz = R(double(vw.r()[3 * i + 2]) - alpha * double(vw.ap()[3 * i + 2]));
-      vw.r()[3 * i] = rx;
-      vw.r()[3 * i + 1] = ry;
-      vw.r()[3 * i + 2] = rzz;
-      R zx, zy, zz;
-      pmul<R>(vw.pinv(), i, rx, ry, rzz, zx, zy, zz);
-      if (!a.frei[i]) zx = zy = zz = 0;
-      R wx = zx, wy = zy, wz = zz;
-      filt<R>(vw.nrm(), i, wx, wy, wz);
-      vw.cw()[i].w = {wx, wy, wz, R(0)};
-      rzs[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rzz) * double(zz);
-    }
-  return rzs[0];
-}
-
-// r = S (b - A dv) with the FP64 operator, z = P r, w = S z; returns the
-// partial r.z (reliable update of the mixed form).
-template <typename R>
-__device__ __noinline__ double cg_point_true_residual(const StepArgs& a) {
-  const View<R> vw(a);
-  double rz2[1] = {0.0};
-      K3D_FOR(i, a.n) {
-        R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, wx = 0, wy = 0, wz = 0;
-        if (a.frei[i]) {
-          const D3 n = ld3(a.nrm_d, uint32_t(i));
-          D3 rd = ld3(a.b, uint32_t(i)) - a_dv64(a, i);
-          rd = rd - n * dot(rd, n);
-          rx = R(rd.x);
-          ry = R(rd.y);
-          rz = R(rd.z);
-          pmul<R>(vw.pinv(), i, rx, ry, rz, zx, zy, zz);
-          wx = zx;
-          wy = zy;
-          wz = zz;
-          filt<R>(vw.nrm(), i, wx, wy, wz);
-          rz2[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rz) * double(zz);
-        }
-        vw.r()[3 * i] = rx;
-        vw.r()[3 * i + 1] = ry;
-        vw.r()[3 * i + 2] = rz;
-        vw.z()[3 * i] = zx;
-        vw.z()[3 * i + 1] = zy;
-        vw.z()[3 * i + 2] = zz;
-        vw.cw()[i].w = {wx, wy, wz, R(0)};
-      }
-  return rz2[0];
-}
-
-// Start values: pinned points 0, held points get their normal target
-// (implizit.rs:375-384); w = dv, c = 0 for the start product.
-template <typename R>
-__device__ __noinline__ void cg_point_dv_start(const StepArgs& a) {
-  const View<R> vw(a);
-  K3D_FOR(i, a.n) {
-    D3 d = ld3(a.dv, uint32_t(i));
-    if (!a.frei[i]) {
-      d = d3(0, 0, 0);
-    } else {
-      const D3 n = ld3(a.nrm_d, uint32_t(i));
-      if (n.x != 0.0 || n.y != 0.0 || n.z != 0.0) {
-        const double soll = a.vn_soll[i] - dot(ld3(a.v, uint32_t(i)), n);
-        d = (d - n * dot(d, n)) + n * soll;
-      }
-    }
-    st3(a.dv, uint32_t(i), d);
-    vw.cw()[i].w = {R(d.x), R(d.y), R(d.z), R(0)};
-    vw.cw()[i].c = {R(0), R(0), R(0), R(0)};
-  }
-}
-
-// r = S (b - A dv), z = P r, first direction w = S z (implizit.rs:385-391);
-// red = (r.w, (S b).P (S b)) partials.
-template <typename R>
-__device__ __noinline__ void cg_point_start(const StepArgs& a, bool hi, double* red_out) {
-  const View<R> vw(a);
-  const double h2 = a.h * a.h;
-  double red[2] = {0.0, 0.0};
-  K3D_FOR(i, a.n) {
-    R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, cx = 0, cy = 0, cz = 0;
-    if (a.frei[i]) {
-      const D3 b = ld3(a.b, uint32_t(i));
-      D3 ad;
-      if (hi) {
-        ad = a_dv64(a, i);
-      } else {
-        R hx, hy, hz;
-        gather_h<R>(a, vw, i, hx, hy, hz);
-        const R4<R> pi = vw.cw()[i].w;
-        const R m = vw.md()[i];
-        ad = d3(double(m * pi.x + R(h2) * hx), double(m * pi.y + R(h2) * hy), double(m * pi.z + R(h2) * hz));
-      }
-      const D3 n = ld3(a.nrm_d, uint32_t(i));
-      D3 rd = b - ad;
-      rd = rd - n * dot(rd, n);
-      rx = R(rd.x);
-      ry = R(rd.y);
-      rz = R(rd.z);
-      R fx = R(b.x), fy = R(b.y), fz = R(b.z);
-      filt<R>(vw.nrm(), i, fx, fy, fz);
-      R px, py, pz;
-      pmul<R>(vw.pinv(), i, fx, fy, fz, px, py, pz);
-      red[1] += double(fx) * double(px) + double(fy) * double(py) + double(fz) * double(pz);
-      pmul<R>(vw.pinv(), i, rx, ry, rz, zx, zy, zz);
-      cx = zx;
-      cy = zy;
-      cz = zz;
-      filt<R>(vw.nrm(), i, cx, cy, cz);
-      red[0] += double(rx) * double(cx) + double(ry) * double(cy) + double(rz) * double(cz);
-    }
-    vw.r()[3 * i] = rx;
-    vw.r()[3 * i + 1] = ry;
-    vw.r()[3 * i + 2] = rz;
-    vw.z()[3 * i] = zx;
-    vw.z()[3 * i + 1] = zy;
-    vw.z()[3 * i + 2] = zz;
-    vw.cw()[i].w = {cx, cy, cz, R(0)};  // the first direction: w + 0 c
-    vw.cw()[i].c = {R(0), R(0), R(0), R(0)};
-  }
-  red_out[0] = red[0];
-  red_out[1] = red[1];
 }
 
 // ------------------------------------------------------------ PCG
@@ -837,17 +657,72 @@ template <typename R>
 __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& iters, bool& unconverged,
                     bool& breakdown, double& rest) {
   const double h2 = a.h * a.h;
-  cg_point_dv_start<R>(a);
+  // start: pinned points 0, held points get their normal target
+  K3D_FOR(i, a.n) {
+    D3 d = ld3(a.dv, uint32_t(i));
+    if (!a.frei[i]) {
+      d = d3(0, 0, 0);
+    } else {
+      const D3 n = ld3(a.nrm_d, uint32_t(i));
+      if (n.x != 0.0 || n.y != 0.0 || n.z != 0.0) {
+        const double soll = a.vn_soll[i] - dot(ld3(a.v, uint32_t(i)), n);
+        d = (d - n * dot(d, n)) + n * soll;
+      }
+    }
+    st3(a.dv, uint32_t(i), d);
+    vw.cw[i].w = {R(d.x), R(d.y), R(d.z), R(0)};
+    vw.cw[i].c = {R(0), R(0), R(0), R(0)};
+  }
   if (!barrier(a, sh)) return false;
   // the mixed form takes its residuals from the FP64 operator
   const bool hi = a.m_f1w64 != nullptr;
   if (hi)
     apply_dv64(a);
   else
-    cg_apply<R>(a, R(0));
+    apply_elements<R>(a, vw, R(0));
   if (!barrier(a, sh)) return false;
   double red[2] = {0.0, 0.0};
-  cg_point_start<R>(a, hi, red);
+  K3D_FOR(i, a.n) {
+    R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, cx = 0, cy = 0, cz = 0;
+    if (a.frei[i]) {
+      const D3 b = ld3(a.b, uint32_t(i));
+      D3 ad;
+      if (hi) {
+        ad = a_dv64(a, i);
+      } else {
+        R hx, hy, hz;
+        gather_h<R>(a, vw, i, hx, hy, hz);
+        const R4<R> pi = vw.cw[i].w;
+        const R m = vw.md[i];
+        ad = d3(double(m * pi.x + R(h2) * hx), double(m * pi.y + R(h2) * hy), double(m * pi.z + R(h2) * hz));
+      }
+      const D3 n = ld3(a.nrm_d, uint32_t(i));
+      D3 rd = b - ad;
+      rd = rd - n * dot(rd, n);
+      rx = R(rd.x);
+      ry = R(rd.y);
+      rz = R(rd.z);
+      R fx = R(b.x), fy = R(b.y), fz = R(b.z);
+      filt<R>(vw.nrm, i, fx, fy, fz);
+      R px, py, pz;
+      pmul<R>(vw.pinv, i, fx, fy, fz, px, py, pz);
+      red[1] += double(fx) * double(px) + double(fy) * double(py) + double(fz) * double(pz);
+      pmul<R>(vw.pinv, i, rx, ry, rz, zx, zy, zz);
+      cx = zx;
+      cy = zy;
+      cz = zz;
+      filt<R>(vw.nrm, i, cx, cy, cz);
+      red[0] += double(rx) * double(cx) + double(ry) * double(cy) + double(rz) * double(cz);
+    }
+    vw.r[3 * i] = rx;
+    vw.r[3 * i + 1] = ry;
+    vw.r[3 * i + 2] = rz;
+    vw.z[3 * i] = zx;
+    vw.z[3 * i + 1] = zy;
+    vw.z[3 * i + 2] = zz;
+    vw.cw[i].w = {cx, cy, cz, R(0)};  // the first direction: w + 0 c
+    vw.cw[i].c = {R(0), R(0), R(0), R(0)};
+  }
   if (!grid_sync<2>(a, sh, red)) return false;
   double delta = red[0];
   const double bb = red[1];
@@ -858,14 +733,34 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
   breakdown = false;
   while (delta > ziel && it < a.cg_max) {
     const R rb = R(beta);
-    cg_apply<R>(a, rb);
+    apply_elements<R>(a, vw, rb);
     if (!barrier(a, sh)) return false;
     // ca = c.Ac and, for the FP32 operator, cm = c.M(1+hc)c: the Hessian part
     // is positive semi-definite, so c.Ac >= cm holds exactly; an FP32 product
     // that falls far below it has lost the direction and the solve stops
     // there as at a breakdown (the FP64 form keeps the reference's test only).
     double ca[2] = {0.0, 0.0};
-    cg_point_ap<R>(a, rb, ca);
+    K3D_FOR(i, a.n) {
+      const R4<R> ci = next_dir<R>(vw.cw[i], rb);
+      vw.cw[i].c = ci;
+      R ax = 0, ay = 0, az = 0;
+      if (a.frei[i]) {
+        R hx, hy, hz;
+        gather_h<R>(a, vw, i, hx, hy, hz);
+        const R m = vw.md[i];
+        ax = m * ci.x + R(h2) * hx;
+        ay = m * ci.y + R(h2) * hy;
+        az = m * ci.z + R(h2) * hz;
+        filt<R>(vw.nrm, i, ax, ay, az);
+        if (sizeof(R) == 4)
+          ca[1] += double(m) * (double(ci.x) * double(ci.x) + double(ci.y) * double(ci.y) +
+                                double(ci.z) * double(ci.z));
+      }
+      vw.ap[3 * i] = ax;
+      vw.ap[3 * i + 1] = ay;
+      vw.ap[3 * i + 2] = az;
+      ca[0] += double(ci.x) * double(ax) + double(ci.y) * double(ay) + double(ci.z) * double(az);
+    }
     if (sizeof(R) == 4) {
       if (!grid_sync<2>(a, sh, ca)) return false;
     } else {
@@ -878,7 +773,26 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       break;
     }
     const double alpha = delta / ca[0];
-    double rzs[1] = {cg_point_update<R>(a, alpha)};
+    double rzs[1] = {0.0};
+    K3D_FOR(i, a.n) {
+      const R4<R> ci = vw.cw[i].c;
+      D3 d = ld3(a.dv, uint32_t(i));
+      d = d + d3(double(ci.x), double(ci.y), double(ci.z)) * alpha;
+      st3(a.dv, uint32_t(i), d);
+      const R rx = R(double(vw.r[3 * i]) - alpha * double(vw.ap[3 * i]));
+      const R ry = R(double(vw.r[3 * i + 1]) - alpha * double(vw.ap[3 * i + 1]));
+      const R rzz = R(double(vw.r[3 * i + 2]) - alpha * double(vw.ap[3 * i + 2]));
+      vw.r[3 * i] = rx;
+      vw.r[3 * i + 1] = ry;
+      vw.r[3 * i + 2] = rzz;
+      R zx, zy, zz;
+      pmul<R>(vw.pinv, i, rx, ry, rzz, zx, zy, zz);
+      if (!a.frei[i]) zx = zy = zz = 0;
+      R wx = zx, wy = zy, wz = zz;
+      filt<R>(vw.nrm, i, wx, wy, wz);
+      vw.cw[i].w = {wx, wy, wz, R(0)};
+      rzs[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rzz) * double(zz);
+    }
     if (!grid_sync<1>(a, sh, rzs)) return false;
     double beta_next = rzs[0] / delta;
     const double delta_prev = delta;
@@ -890,7 +804,31 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       const bool restart = delta > kGrow * delta_ref;
       apply_dv64(a);
       if (!barrier(a, sh)) return false;
-      double rz2[1] = {cg_point_true_residual<R>(a)};
+      double rz2[1] = {0.0};
+      K3D_FOR(i, a.n) {
+        R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, wx = 0, wy = 0, wz = 0;
+        if (a.frei[i]) {
+          const D3 n = ld3(a.nrm_d, uint32_t(i));
+          D3 rd = ld3(a.b, uint32_t(i)) - a_dv64(a, i);
+          rd = rd - n * dot(rd, n);
+          rx = R(rd.x);
+          ry = R(rd.y);
+          rz = R(rd.z);
+          pmul<R>(vw.pinv, i, rx, ry, rz, zx, zy, zz);
+          wx = zx;
+          wy = zy;
+          wz = zz;
+          filt<R>(vw.nrm, i, wx, wy, wz);
+          rz2[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rz) * double(zz);
+        }
+        vw.r[3 * i] = rx;
+        vw.r[3 * i + 1] = ry;
+        vw.r[3 * i + 2] = rz;
+        vw.z[3 * i] = zx;
+        vw.z[3 * i + 1] = zy;
+        vw.z[3 * i + 2] = zz;
+        vw.cw[i].w = {wx, wy, wz, R(0)};
+      }
       if (!grid_sync<1>(a, sh, rz2)) return false;
       delta = rz2[0];
       beta_next = restart ? 0.0 : delta / delta_prev;
@@ -909,7 +847,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
 // implizit.rs:924-942: normal force from the residual A dv - b along the
 // contact normal; a held point that pulls on the body is released.
 template <typename R>
-__device__ __noinline__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double& released) {
+__device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double& released) {
   const bool hi = a.m_f1w64 != nullptr;
   if (hi) {
     apply_dv64(a);
@@ -931,15 +869,15 @@ __device__ __noinline__ bool release(const StepArgs& a, const View<R>& vw, Share
     } else {
       R hx, hy, hz;
       gather_h<R>(a, vw, i, hx, hy, hz);
-      const R4<R> ci = vw.cw()[i].w;
-      const R m = vw.md()[i];
+      const R4<R> ci = vw.cw[i].w;
+      const R m = vw.md[i];
       rest = d3(double(m * ci.x + R(h2) * hx) - b.x, double(m * ci.y + R(h2) * hy) - b.y,
                 double(m * ci.z + R(h2) * hz) - b.z);
     }
     const double fn = dot(rest, n) / a.h;
     if (fn < 0.0) {
       st3(a.nrm_d, uint32_t(i), d3(0, 0, 0));
-      vw.nrm()[3 * i] = vw.nrm()[3 * i + 1] = vw.nrm()[3 * i + 2] = R(0);
+      vw.nrm[3 * i] = vw.nrm[3 * i + 1] = vw.nrm[3 * i + 2] = R(0);
       cnt[0] += 1.0;
     } else {
       a.fnk[i] = fn;
@@ -1090,8 +1028,8 @@ __global__ void __launch_bounds__(kBlock) probe_load_kernel(const __grid_constan
   const double* src = a.mode == MODE_SYSTEM ? a.v : a.p_in;
   K3D_FOR(i, a.n) {
     const D3 q = ld3(src, uint32_t(i));
-    vw.cw()[i].w = {R(q.x), R(q.y), R(q.z), R(0)};
-    vw.cw()[i].c = {R(0), R(0), R(0), R(0)};
+    vw.cw[i].w = {R(q.x), R(q.y), R(q.z), R(0)};
+    vw.cw[i].c = {R(0), R(0), R(0), R(0)};
   }
 }
 template <typename R>
@@ -1111,8 +1049,8 @@ __global__ void __launch_bounds__(kBlock) probe_out_kernel(const __grid_constant
       st3(a.p_out, uint32_t(i), b * (1.0 / a.h) + d3(double(hx), double(hy), double(hz)) * a.h);
       continue;
     }
-    const R4<R> ci = vw.cw()[i].w;
-    const R m = vw.md()[i];
+    const R4<R> ci = vw.cw[i].w;
+    const R m = vw.md[i];
     D3 o = d3(double(m * ci.x + R(h2) * hx), double(m * ci.y + R(h2) * hy), double(m * ci.z + R(h2) * hz));
     if (a.mode == MODE_RESIDUAL) o = o - b;
     st3(a.p_out, uint32_t(i), o);
