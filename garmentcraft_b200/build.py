@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_native")
 LIB = os.path.join(OUT_DIR, "libklon3d_b200.so")
-SOURCES = ["k3d_step.cu", "k3d_host.cpp", "scene_build.cpp"]
+SOURCES = ["k3d_step.cu", "k3d_host.cpp", "scene_build.cpp", "k3d_noalloc.cu"]
 HEADERS = ["k3d_step.h", "k3d_device.cuh", "scene_build.h"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -278,6 +278,28 @@ double k3d_last_frame_ms(const k3d_solver* h);
 /* Number of device kernels the handle launched since creation. */
 int64_t k3d_kernel_launches(const k3d_solver* h);
 
+/* ---------------------------------------------------------------- no allocation
+ * k3d_operator_noalloc has no counterpart in the reference. It is A p as
+ * k3d_operator computes it (FP64, the scene's positions s->x), for a caller
+ * that must not allocate device memory: code that runs while a CUDA graph is
+ * being captured, a host application or framework that owns the whole device
+ * memory budget through its own pool and forbids cudaMalloc/cudaFree behind
+ * its back, or a real-time loop that must never block in the driver's
+ * allocator. No handle is needed and nothing is allocated: every pointer in
+ * `s` (x, masse and the constraint arrays; v, w, bodies are not read) and `p`,
+ * `out` (3 doubles per point) are DEVICE pointers owned by the caller, and the
+ * only scratch is a static array of 3 MiB inside the library, present on every
+ * GPU that loads it until the process exits. Limits: s->n_punkte <= 131072
+ * (K3D_BAD_ARGUMENT beyond), at most 8192 element corners per point. The
+ * first call on a device looks the scratch up for that device; make that
+ * first call before any stream capture. Calls share the scratch, so calls
+ * that overlap on the GPU (other streams, other host threads) race; the call
+ * clears what it needs and synchronises `stream` (a cudaStream_t, null = the
+ * legacy default stream) before it returns. An element that names a point
+ * out of range is skipped and reported as K3D_BAD_ARGUMENT. */
+k3d_status k3d_operator_noalloc(const k3d_params* params, const k3d_scene* s, const double* p, double* out,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif
