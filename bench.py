@@ -68,6 +68,9 @@ def args_():
     p.add_argument("--cpu-seconds", type=float, default=25.0)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-compare", action="store_true")
+    p.add_argument("--capture", type=int, default=0,
+                   help="profiling case: run this many mixed-form steps of the drop on cuda:0 and exit")
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="form used by --capture")
     return p.parse_args()
 
 
@@ -103,6 +106,16 @@ def make_scene(n, pinned=False):
 def params(prec):
     from garmentcraft_b200.params import ImplizitParameter
     return ImplizitParameter(schritte_je_bild=1, cg_max=CG_MAX, cg_toleranz=1e-5, precision=prec)
+
+
+def algorithmic_solve_bytes(s, sw, iters, solves):
+    """Algorithmic bytes of the PCG launches alone (the dominant kernel):
+    operator applications (CG iterations + 2 per solve) and the per-iteration
+    vector update, with the per-unit figures of algorithmic_bytes."""
+    N, T, B = s.n, s.membran_punkte.shape[0], s.biegung_punkte.shape[0]
+    S = s.naht_punkte.shape[0] + int(np.sum(s.membran_kante == 0))
+    per_app = N * 10 * sw + T * (12 + 21 * sw) + B * (16 + 13 * sw) + S * (8 + 5 * sw)
+    return (iters + 2 * solves) * per_app + iters * N * 31 * sw
 
 
 def algorithmic_bytes(s, sw, steps, iters, solves):
@@ -168,10 +181,12 @@ def read_peaks():
 
 
 def read_traffic():
-    """Per-launch DRAM bytes of the step kernel from the committed ncu summary."""
+    """DRAM bytes per CG iteration of solve_kernel<float>, from the committed
+    ncu summary (dram__bytes_read.sum + dram__bytes_write.sum of one captured
+    launch divided by its iterations)."""
     try:
-        txt = open(os.path.join(ROOT, "profiles", "step_kernel_sheet257.md")).read()
-        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
+        txt = open(os.path.join(ROOT, "profiles", "solve_kernel_sheet257.md")).read()
+        m = re.search(r"traffic_bytes_per_iteration:\s*([0-9.eE+]+)", txt)
         return float(m.group(1)) if m else None
     except Exception:
         return None
@@ -210,17 +225,19 @@ def dev_timed(n, prec, warmup, steps, flush, torch):
     pre, wu = window(warmup)
     cg.bilder_auf_geraet(pre + wu)
     torch.cuda.synchronize()
-    ms, its, solves = [], 0, 0
+    ms, its, solves, solve_ms = [], 0, 0, 0.0
     l0 = cg.kernel_starts()
     for k in range(steps):
         flush.fill_(float(k))
         torch.cuda.synchronize()
         st = cg.bilder_auf_geraet(1)
         ms.append(cg.letzte_bild_ms())
+        solve_ms += cg.letzte_loesung_ms()
         its += st.cg_iterationen
         solves += st.loesungen
     launches = cg.kernel_starts() - l0
     cg.zustand_lesen(s)
+    cg.solve_ms_total = solve_ms
     return ms, its, solves, launches, s, cg
 
 
@@ -248,6 +265,20 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if a.capture:
+        # a fixed case for ncu: the same drop, no timing, no flush
+        from garmentcraft_b200 import _abi
+        from garmentcraft_b200.implizit import ImplizitCg
+        prec = _abi.K3D_MIXED if a.precision == "mixed" else _abi.K3D_FP64
+        s = make_scene(a.n)
+        cg = ImplizitCg(params(prec))
+        cg.zustand_hochladen(s)
+        st = cg.bilder_auf_geraet(a.capture - 1)
+        st = cg.bilder_auf_geraet(1)
+        print(json.dumps({"capture_steps": a.capture, "last_step_cg_iterations": st.cg_iterationen,
+                          "last_step_ms": cg.letzte_bild_ms()}))
+        return
 
     if a.impl == "reference":
         if rank != 0:
@@ -323,14 +354,16 @@ def main():
                                   "definition": "max_i |x_mixed - x_fp64| / bbox diagonal"}
 
     peaks = read_peaks()
-    alg = algorithmic_bytes(s_mix, 4, a.steps, its, solves)
-    achieved = alg / (sum(ms) / 1e3) / 1e9
+    alg = algorithmic_solve_bytes(s_mix, 4, its, solves)
+    achieved = alg / (cg.solve_ms_total / 1e3) / 1e9
     peak = peaks["hbm_gbs"] if peaks else 6650.0
-    traffic = read_traffic()
+    tpi = read_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_source": "measured" if peaks else "fallback",
-                "kernel": "k3d::step_kernel<float>",
-                "algorithmic_bytes_per_launch": alg / a.steps}
+                "traffic": tpi * its / a.steps if tpi else None,
+                "peak_source": "measured" if peaks else "fallback", "kernel": "k3d::solve_kernel<float>",
+                "algorithmic_bytes_per_launch": alg / a.steps,
+                "kernel_share_of_step": cg.solve_ms_total / sum(ms),
+                "note": "working set is L2-resident; traffic = ncu DRAM bytes per iteration x iterations per launch"}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1e3 * t_dev / a.steps, "higher_is_better": True,

@@ -52,7 +52,8 @@ struct k3d_solver {
   std::vector<int64_t> seam_slot;       // spring index of each seam, -1 if not streamed
   std::vector<double2> s_kl_host;
   int64_t launches = 0;
-  double last_ms = 0.0;
+  double last_ms = 0.0, solve_ms = 0.0;
+  std::vector<cudaEvent_t> sev;  // one pair per substep of a frame
   Arena arena;
   StepArgs a{};  // device pointers and constants; per-launch fields are set before each launch
   double* d_pin = nullptr;  // probe input (3N)
@@ -254,12 +255,14 @@ void k3d_solver_destroy(k3d_solver* h) {
   }
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  for (cudaEvent_t e : h->sev) cudaEventDestroy(e);
   delete h;
 }
 
 const char* k3d_last_error(const k3d_solver* h) { return h ? h->err.c_str() : "null handle"; }
 const char* k3d_solver_name(const k3d_solver* h) { return h ? h->name.c_str() : ""; }
 double k3d_last_frame_ms(const k3d_solver* h) { return h ? h->last_ms : 0.0; }
+double k3d_last_solve_ms(const k3d_solver* h) { return h ? h->solve_ms : 0.0; }
 int64_t k3d_kernel_launches(const k3d_solver* h) { return h ? h->launches : 0; }
 
 // kg = d2U/dg2 (kontinuum.rs:391-406), symmetric (00, 11, 22, 01, 02, 12)
@@ -573,6 +576,16 @@ static k3d_status launch(k3d_solver* h, int mode, double t_bodies, bool need_loa
   return K3D_OK;
 }
 
+// Sum of the PCG launch times recorded by the last frame(s).
+static void sum_solve_ms(k3d_solver* h, size_t ev_used) {
+  double t = 0.0;
+  for (size_t q = 0; q + 1 < ev_used; q += 2) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, h->sev[q], h->sev[q + 1]) == cudaSuccess) t += ms;
+  }
+  h->solve_ms = t;
+}
+
 static k3d_status check_sync(k3d_solver* h) {
   K3D_CUDA(h, cudaStreamSynchronize(h->stream));
   SyncState ss;
@@ -619,11 +632,20 @@ static k3d_status ready(k3d_solver* h) {
 }
 
 // One frame of substeps on the resident state.
-static k3d_status frame_device(k3d_solver* h) {
+static k3d_status frame_device(k3d_solver* h, size_t& ev_used) {
   const int sub = std::max(h->p.schritte_je_bild, 1);
   const double hs = h->sim.bild_dt / double(sub);
   for (int k = 0; k < sub; ++k) {
+    while (h->sev.size() < ev_used + 2) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return fail(h, K3D_DEVICE_ERROR, "event create");
+      h->sev.push_back(e);
+    }
+    h->a.ev_solve0 = h->sev[ev_used];
+    h->a.ev_solve1 = h->sev[ev_used + 1];
+    ev_used += 2;
     k3d_status st = launch(h, MODE_STEP, double(k + 1) * hs, false);
+    h->a.ev_solve0 = h->a.ev_solve1 = nullptr;
     if (st != K3D_OK) return st;
   }
   // the bodies end the frame moved by v * bild_dt (implizit.rs:1047-1054)
@@ -679,7 +701,8 @@ k3d_status k3d_frame(k3d_solver* h, k3d_scene* s, k3d_stats* stats) {
   st = reset_stats(h);
   if (st != K3D_OK) return st;
   K3D_CUDA(h, cudaEventRecord(h->ev0, h->stream));
-  st = frame_device(h);
+  size_t ev_used = 0;
+  st = frame_device(h, ev_used);
   if (st != K3D_OK) return st;
   K3D_CUDA(h, cudaEventRecord(h->ev1, h->stream));
   K3D_CUDA(h, cudaMemcpyAsync(s->x, h->a.x, 24 * size_t(h->n), cudaMemcpyDeviceToHost, h->stream));
@@ -689,6 +712,7 @@ k3d_status k3d_frame(k3d_solver* h, k3d_scene* s, k3d_stats* stats) {
   float ms = 0.f;
   cudaEventElapsedTime(&ms, h->ev0, h->ev1);
   h->last_ms = ms;
+  sum_solve_ms(h, ev_used);
   s->zeit += s->param.bild_dt;
   return read_stats(h, stats);
 }
@@ -700,8 +724,9 @@ k3d_status k3d_frames_resident(k3d_solver* h, int32_t n_frames, k3d_stats* stats
   st = reset_stats(h);
   if (st != K3D_OK) return st;
   K3D_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+  size_t ev_used = 0;
   for (int f = 0; f < n_frames; ++f) {
-    st = frame_device(h);
+    st = frame_device(h, ev_used);
     if (st != K3D_OK) return st;
   }
   K3D_CUDA(h, cudaEventRecord(h->ev1, h->stream));
@@ -710,6 +735,7 @@ k3d_status k3d_frames_resident(k3d_solver* h, int32_t n_frames, k3d_stats* stats
   float ms = 0.f;
   cudaEventElapsedTime(&ms, h->ev0, h->ev1);
   h->last_ms = ms;
+  sum_solve_ms(h, ev_used);
   return read_stats(h, stats);
 }
 

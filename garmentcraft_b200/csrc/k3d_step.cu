@@ -1116,7 +1116,9 @@ static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int&
     launched += 3;
     return cudaSuccess;
   }
+  if (a.ev_solve0 && (e = cudaEventRecord(a.ev_solve0, st)) != cudaSuccess) return e;
   if ((e = cooperative(Kernels<R>::sv(), a, blocks, st)) != cudaSuccess) return e;
+  if (a.ev_solve1 && (e = cudaEventRecord(a.ev_solve1, st)) != cudaSuccess) return e;
   launched += 1;
   if (a.mode == MODE_STEP) {
     if ((e = plain((const void*)integrate_kernel, a, a.n, st)) != cudaSuccess) return e;

@@ -82,6 +82,7 @@ struct StepArgs {
   const double* p_in;
   double* p_out;
   // bookkeeping
+  cudaEvent_t ev_solve0, ev_solve1;  // around the PCG launch (host-side handles)
   SyncState* sync;
   double* partials;  // kMaxRed * blocks
   long long* stats;

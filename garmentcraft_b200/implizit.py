@@ -186,5 +186,9 @@ class ImplizitCg:
     def letzte_bild_ms(self) -> float:
         return self._L.k3d_last_frame_ms(self._h)
 
+    def letzte_loesung_ms(self) -> float:
+        """Device time of the PCG launches of the last frame call (ms)."""
+        return self._L.k3d_last_solve_ms(self._h)
+
     def kernel_starts(self) -> int:
         return self._L.k3d_kernel_launches(self._h)

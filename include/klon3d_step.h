@@ -275,6 +275,10 @@ k3d_status k3d_read_load(k3d_solver* h, double* out);
  * handle's stream (the figure GpuLoeser::zeiten reports, gpu.rs:1225-1227). */
 double k3d_last_frame_ms(const k3d_solver* h);
 
+/* Time of the PCG launches (solve and release test) of the last frame call,
+ * in ms, CUDA events on the handle's stream around each of them. */
+double k3d_last_solve_ms(const k3d_solver* h);
+
 /* Number of device kernels the handle launched since creation. */
 int64_t k3d_kernel_launches(const k3d_solver* h);
 
