@@ -73,6 +73,72 @@ static k3d_status cuda_fail(k3d_solver* h, cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail((h), e_, #call); \
   } while (0)
 
+// Block pattern of A (3x3 blocks): per point its sorted columns, ELL layout
+// with block (rank k, row i) at k * np + i; per block the element
+// contributions in a fixed order (membranes, then bends, then springs, each in
+// element order, then by corner pair). Code: type << 30 | a << 28 | b << 26 | id.
+struct Pattern {
+  std::vector<uint32_t> cnt, col, ctr_off, ctr;
+  size_t kmax = 0;
+};
+
+static bool build_pattern(size_t n, size_t np, const uint32_t* m_p, size_t nt, const uint32_t* b_p, size_t nb,
+                          const std::vector<uint4>& s_idx, Pattern& P) {
+  if (nt >= (size_t(1) << 26) || nb >= (size_t(1) << 26) || s_idx.size() >= (size_t(1) << 26)) return false;
+  std::vector<std::vector<uint32_t>> cols(n);
+  for (size_t i = 0; i < n; ++i) cols[i].push_back(uint32_t(i));
+  auto link = [&](const uint32_t* q, int k) {
+    for (int a = 0; a < k; ++a)
+      for (int b = 0; b < k; ++b) cols[q[a]].push_back(q[b]);
+  };
+  for (size_t t = 0; t < nt; ++t) link(m_p + 3 * t, 3);
+  for (size_t b = 0; b < nb; ++b) link(b_p + 4 * b, 4);
+  for (const uint4& q : s_idx) {
+    const uint32_t ij[2] = {q.x, q.y};
+    link(ij, 2);
+  }
+  P.cnt.assign(n, 0);
+  P.kmax = 0;
+  for (size_t i = 0; i < n; ++i) {
+    std::sort(cols[i].begin(), cols[i].end());
+    cols[i].erase(std::unique(cols[i].begin(), cols[i].end()), cols[i].end());
+    P.cnt[i] = uint32_t(cols[i].size());
+    P.kmax = std::max(P.kmax, cols[i].size());
+  }
+  if (P.kmax * np >= (size_t(1) << 32)) return false;
+  const size_t ns = P.kmax * np;
+  P.col.assign(ns, 0);
+  for (size_t i = 0; i < n; ++i)
+    for (size_t k = 0; k < cols[i].size(); ++k) P.col[k * np + i] = cols[i][k];
+  auto slot = [&](uint32_t i, uint32_t j) -> size_t {
+    const auto& c = cols[i];
+    return size_t(std::lower_bound(c.begin(), c.end(), j) - c.begin()) * np + i;
+  };
+  // count, then fill (stable: element order within a block)
+  P.ctr_off.assign(ns + 1, 0);
+  auto each = [&](auto&& f) {
+    for (size_t t = 0; t < nt; ++t)
+      for (uint32_t a = 0; a < 3; ++a)
+        for (uint32_t b = 0; b < 3; ++b)
+          f(slot(m_p[3 * t + a], m_p[3 * t + b]), (0u << 30) | (a << 28) | (b << 26) | uint32_t(t));
+    for (size_t e = 0; e < nb; ++e)
+      for (uint32_t a = 0; a < 4; ++a)
+        for (uint32_t b = 0; b < 4; ++b)
+          f(slot(b_p[4 * e + a], b_p[4 * e + b]), (1u << 30) | (a << 28) | (b << 26) | uint32_t(e));
+    for (size_t q = 0; q < s_idx.size(); ++q) {
+      const uint32_t ij[2] = {s_idx[q].x, s_idx[q].y};
+      for (uint32_t a = 0; a < 2; ++a)
+        for (uint32_t b = 0; b < 2; ++b) f(slot(ij[a], ij[b]), (2u << 30) | (a << 28) | (b << 26) | uint32_t(q));
+    }
+  };
+  each([&](size_t sl, uint32_t) { P.ctr_off[sl + 1]++; });
+  for (size_t q = 0; q < ns; ++q) P.ctr_off[q + 1] += P.ctr_off[q];
+  P.ctr.assign(P.ctr_off[ns], 0);
+  std::vector<uint32_t> fill(P.ctr_off.begin(), P.ctr_off.end() - 1);
+  each([&](size_t sl, uint32_t code) { P.ctr[fill[sl]++] = code; });
+  return true;
+}
+
 // Writable aliases of the scene constants, for the upload.
 struct Carve {
   double *masse, *w, *kabst, *reib;
@@ -83,12 +149,13 @@ struct Carve {
   double4 *m_r, *m_basis, *m_mat;
   void *m_rin, *m_kgA, *m_rin64, *m_kgA64;
   double2 *b_kr, *s_kl;
+  uint32_t *row_cnt, *col, *ctr_off, *ctr;
 };
 
 // Assigns every device array of the handle from the arena (base may be null
 // to measure the size).
 static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t S, size_t et, size_t eb, size_t es,
-                  size_t np, size_t kmax, Carve& cv) {
+                  size_t np, size_t kmax, const Pattern& P, Carve& cv) {
   const size_t nslots = np * (kmax ? kmax : 1);
   const size_t R = h->rsize;
   StepArgs& a = h->a;
@@ -155,6 +222,15 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.partials = A.take<double>(size_t(8) * h->blocks);  // two buffers of 4 sums per block
   a.stats = A.take<long long>(ST_COUNT);
   a.stat_rest_max = A.take<double>(2);
+  // assembled A (BSR, ELL by rank) and its contribution lists
+  const size_t nbs = P.kmax * np;
+  a.bplane = int64_t(nbs);
+  a.row_cnt = cv.row_cnt = A.take<uint32_t>(N);
+  a.col = cv.col = A.take<uint32_t>(nbs);
+  a.bmat = A.take<char>(9 * nbs * R);
+  a.ctr_off = cv.ctr_off = A.take<uint32_t>(nbs + 1);
+  a.ctr = cv.ctr = A.take<uint32_t>(P.ctr.size());
+  a.cw2 = A.take<char>(8 * N * R);  // the second buffer of (c, w)
   cv.m_rin64 = cv.m_kgA64 = nullptr;
   if (R == 4) {  // FP64 operator copies for the residuals of the mixed form
     a.m_f1w64 = A.take<double4>(T);
@@ -407,6 +483,10 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
     }
   }
 
+  Pattern pat;
+  if (!build_pattern(size_t(n), np, s->membran_punkte, size_t(nt), s->biegung_punkte, size_t(nb), s_idx, pat))
+    return fail(h, K3D_BAD_ARGUMENT, "scene too large for the block pattern");
+
   // element constants
   std::vector<uint4> m_idx(nt), b_idx(nb);
   std::vector<double4> m_r(nt), m_basis(nt), m_mat(nt);
@@ -458,12 +538,12 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
   const size_t N = size_t(n), T = size_t(nt), B = size_t(nb), S = size_t(ns);
   Carve cv;
   Arena probe;
-  carve(h, probe, N, T, B, S, ent_t.size(), ent_b.size(), ent_s.size(), np, kmax, cv);
+  carve(h, probe, N, T, B, S, ent_t.size(), ent_b.size(), ent_s.size(), np, kmax, pat, cv);
   void* base = nullptr;
   K3D_CUDA(h, cudaMalloc(&base, probe.used));
   h->arena.base = static_cast<char*>(base);
   h->arena.size = probe.used;
-  carve(h, h->arena, N, T, B, S, ent_t.size(), ent_b.size(), ent_s.size(), np, kmax, cv);
+  carve(h, h->arena, N, T, B, S, ent_t.size(), ent_b.size(), ent_s.size(), np, kmax, pat, cv);
   Arena& A = h->arena;
   StepArgs& a = h->a;
   if (A.used > A.size) return fail(h, K3D_DEVICE_ERROR, "arena overflow");
@@ -488,6 +568,10 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
   K3D_CUDA(h, up(cv.ent_b, ent_b.data(), 4 * ent_b.size()));
   K3D_CUDA(h, up(cv.ent_s, ent_s.data(), 4 * ent_s.size()));
   K3D_CUDA(h, up(cv.cnt_v, cnt_v.data(), 4 * N));
+  K3D_CUDA(h, up(cv.row_cnt, pat.cnt.data(), 4 * N));
+  K3D_CUDA(h, up(cv.col, pat.col.data(), 4 * pat.col.size()));
+  K3D_CUDA(h, up(cv.ctr_off, pat.ctr_off.data(), 4 * pat.ctr_off.size()));
+  K3D_CUDA(h, up(cv.ctr, pat.ctr.data(), 4 * pat.ctr.size()));
   K3D_CUDA(h, up(cv.m_pos, m_pos.data(), 16 * T));
   K3D_CUDA(h, up(cv.b_pos, b_pos.data(), 16 * B));
   K3D_CUDA(h, up(cv.s_pos, s_pos.data(), 8 * S));

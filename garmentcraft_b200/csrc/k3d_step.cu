@@ -647,16 +647,128 @@ __device__ void dv_to_w(const StepArgs& a, const View<R>& vw) {
   }
 }
 
+// ------------------------------------------------------------ assembled A
+// A = M(1+hc) + h^2 H as 3x3 blocks (implizit.rs:185-229 written out per
+// point pair), from the FP64 records of this step. Each block adds its
+// contributions in the fixed order of its list, so the assembly is
+// deterministic. Membrane block (a, b): J_a^T kg J_b + s_ab I with the rows
+// of J_k = (2 c1_k f1, 2 c2_k f2, 2 c2_k f1 + 2 c1_k f2) and s_ab the
+// geometric term (kontinuum.rs:616-708); bend block: k g_a g_b^T; spring
+// block: +-k (n n^T (1 - q) + q I).
+template <typename R>
+__global__ void __launch_bounds__(kBlock) assemble_kernel(const __grid_constant__ StepArgs a) {
+  const bool own = sizeof(R) == 8;
+  const R4<double>* f1w = static_cast<const R4<double>*>(own ? a.m_f1w : a.m_f1w64);
+  const R4<double>* f2w = static_cast<const R4<double>*>(own ? a.m_f2w : a.m_f2w64);
+  const R4<double>* kgB = static_cast<const R4<double>*>(own ? a.m_kgB : a.m_kgB64);
+  const R4<double>* rin = static_cast<const R4<double>*>(own ? a.m_rin : a.m_rin64);
+  const R4<double>* kgA = static_cast<const R4<double>*>(own ? a.m_kgA : a.m_kgA64);
+  const R4<double>* grad = static_cast<const R4<double>*>(own ? a.b_grad : a.b_grad64);
+  const R4<double>* sdq = static_cast<const R4<double>*>(own ? a.s_dq : a.s_dq64);
+  const double* sk = static_cast<const double*>(own ? a.s_k : a.s_k64);
+  R* bm = static_cast<R*>(a.bmat);
+  const double h2 = a.h * a.h;
+  K3D_FOR(sid, a.bplane) {
+    const int64_t i = sid % a.np, k = sid / a.np;
+    if (i >= a.n || k >= int64_t(__ldg(&a.row_cnt[i]))) continue;
+    double B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t e = __ldg(&a.ctr_off[sid]); e < __ldg(&a.ctr_off[sid + 1]); ++e) {
+      const uint32_t code = __ldg(&a.ctr[e]);
+      const uint32_t ty = code >> 30, ca = (code >> 28) & 3u, cb = (code >> 26) & 3u, id = code & 0x3ffffffu;
+      if (ty == 0) {
+        const R4<double> F1 = f1w[id], F2 = f2w[id], KB = kgB[id], RI = rin[id], KA = kgA[id];
+        const double c1[3] = {-(RI.x + RI.z), RI.x, RI.z}, c2[3] = {-(RI.y + RI.w), RI.y, RI.w};
+        const D3 f1 = d3(F1.x, F1.y, F1.z), f2 = d3(F2.x, F2.y, F2.z);
+        const D3 ja[3] = {f1 * (2.0 * c1[ca]), f2 * (2.0 * c2[ca]), f1 * (2.0 * c2[ca]) + f2 * (2.0 * c1[ca])};
+        const D3 jb[3] = {f1 * (2.0 * c1[cb]), f2 * (2.0 * c2[cb]), f1 * (2.0 * c2[cb]) + f2 * (2.0 * c1[cb])};
+        const double K[3][3] = {{KA.x, KA.w, KB.x}, {KA.w, KA.y, KB.y}, {KB.x, KB.y, KA.z}};
+        D3 u[3];  // u_p = sum_q K[p][q] jb_q
+#pragma unroll
+        for (int pp = 0; pp < 3; ++pp) u[pp] = jb[0] * K[pp][0] + jb[1] * K[pp][1] + jb[2] * K[pp][2];
+        const double sab =
+            2.0 * (F1.w * c1[ca] * c1[cb] + F2.w * c2[ca] * c2[cb] + KB.z * (c1[ca] * c2[cb] + c2[ca] * c1[cb]));
+        double H[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int pp = 0; pp < 3; ++pp) {
+          H[0] += ja[pp].x * u[pp].x;
+          H[1] += ja[pp].x * u[pp].y;
+          H[2] += ja[pp].x * u[pp].z;
+          H[3] += ja[pp].y * u[pp].x;
+          H[4] += ja[pp].y * u[pp].y;
+          H[5] += ja[pp].y * u[pp].z;
+          H[6] += ja[pp].z * u[pp].x;
+          H[7] += ja[pp].z * u[pp].y;
+          H[8] += ja[pp].z * u[pp].z;
+        }
+        H[0] += sab;
+        H[4] += sab;
+        H[8] += sab;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) B[q] += h2 * H[q];
+      } else if (ty == 1) {
+        const R4<double> ga = grad[4 * size_t(id) + ca], gb = grad[4 * size_t(id) + cb];
+        const double kk = h2 * ga.w;
+        const double gav[3] = {ga.x, ga.y, ga.z}, gbv[3] = {gb.x, gb.y, gb.z};
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) B[3 * r + c] += kk * gav[r] * gbv[c];
+      } else {
+        const R4<double> dq = sdq[id];
+        const double kk = h2 * sk[id] * (ca == cb ? 1.0 : -1.0);
+        const double nv[3] = {dq.x, dq.y, dq.z};
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) B[3 * r + c] += kk * (nv[r] * nv[c] * (1.0 - dq.w) + (r == c ? dq.w : 0.0));
+      }
+    }
+    if (int64_t(__ldg(&a.col[sid])) == i) {
+      const double md = a.masse[i] * (1.0 + a.h * a.daempf);
+      B[0] += md;
+      B[4] += md;
+      B[8] += md;
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) bm[q * a.bplane + sid] = R(B[q]);
+  }
+}
+
+// (A p)_i = sum over the row's blocks of B p_col, p = w + beta c from `buf`.
+template <typename R>
+__device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<R>* buf, int64_t i, R beta, R& ox, R& oy,
+                                        R& oz) {
+  const R* bm = static_cast<const R*>(a.bmat);
+  const int64_t P = a.bplane;
+  R x = 0, y = 0, z = 0;
+  const uint32_t cnt = __ldg(&a.row_cnt[i]);
+#pragma unroll 2
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const int64_t sid = int64_t(k) * a.np + i;
+    const uint32_t j = __ldg(&a.col[sid]);
+    const R4<R> pj = next_dir<R>(buf[j], beta);
+    x += bm[sid] * pj.x + bm[P + sid] * pj.y + bm[2 * P + sid] * pj.z;
+    y += bm[3 * P + sid] * pj.x + bm[4 * P + sid] * pj.y + bm[5 * P + sid] * pj.z;
+    z += bm[6 * P + sid] * pj.x + bm[7 * P + sid] * pj.y + bm[8 * P + sid] * pj.z;
+  }
+  ox = x;
+  oy = y;
+  oz = z;
+}
+
 // ------------------------------------------------------------ PCG
-// implizit.rs:370-426, three grid syncs per iteration:
-//   elements: H p with p = w + beta c            -> barrier
-//   points:   c = p, ap = S A c, c.ap            -> sum
-//   points:   dv += alpha c, r -= alpha ap, z = P r, w = S z, r.z -> sum
-// Returns false on a barrier error.
+// implizit.rs:370-426 with the assembled A, two grid syncs per iteration:
+//   points: c = w + beta c (neighbours' from one (c, w) buffer, own written to
+//           the other), ap = S A c, c.ap                            -> sum
+//   points: dv += alpha c, r -= alpha ap, z = P r, w = S z, r.z       -> sum
+// The mixed form takes its residuals (start, reliable updates) from the FP64
+// operator. Returns false on a barrier error.
 template <typename R>
 __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& iters, bool& unconverged,
                     bool& breakdown, double& rest) {
-  const double h2 = a.h * a.h;
+  CW<R>* cur = static_cast<CW<R>*>(a.c);
+  CW<R>* nxt = static_cast<CW<R>*>(a.cw2);
+  const bool hi = a.m_f1w64 != nullptr;
   // start: pinned points 0, held points get their normal target
   K3D_FOR(i, a.n) {
     D3 d = ld3(a.dv, uint32_t(i));
@@ -670,17 +782,14 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       }
     }
     st3(a.dv, uint32_t(i), d);
-    vw.cw[i].w = {R(d.x), R(d.y), R(d.z), R(0)};
-    vw.cw[i].c = {R(0), R(0), R(0), R(0)};
+    cur[i].w = {R(d.x), R(d.y), R(d.z), R(0)};
+    cur[i].c = {R(0), R(0), R(0), R(0)};
   }
   if (!barrier(a, sh)) return false;
-  // the mixed form takes its residuals from the FP64 operator
-  const bool hi = a.m_f1w64 != nullptr;
-  if (hi)
+  if (hi) {
     apply_dv64(a);
-  else
-    apply_elements<R>(a, vw, R(0));
-  if (!barrier(a, sh)) return false;
+    if (!barrier(a, sh)) return false;
+  }
   double red[2] = {0.0, 0.0};
   K3D_FOR(i, a.n) {
     R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, cx = 0, cy = 0, cz = 0;
@@ -691,10 +800,8 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
         ad = a_dv64(a, i);
       } else {
         R hx, hy, hz;
-        gather_h<R>(a, vw, i, hx, hy, hz);
-        const R4<R> pi = vw.cw[i].w;
-        const R m = vw.md[i];
-        ad = d3(double(m * pi.x + R(h2) * hx), double(m * pi.y + R(h2) * hy), double(m * pi.z + R(h2) * hz));
+        bsr_row<R>(a, cur, i, R(0), hx, hy, hz);
+        ad = d3(double(hx), double(hy), double(hz));
       }
       const D3 n = ld3(a.nrm_d, uint32_t(i));
       D3 rd = b - ad;
@@ -717,13 +824,15 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     vw.r[3 * i] = rx;
     vw.r[3 * i + 1] = ry;
     vw.r[3 * i + 2] = rz;
-    vw.z[3 * i] = zx;
-    vw.z[3 * i + 1] = zy;
-    vw.z[3 * i + 2] = zz;
-    vw.cw[i].w = {cx, cy, cz, R(0)};  // the first direction: w + 0 c
-    vw.cw[i].c = {R(0), R(0), R(0), R(0)};
+    nxt[i].w = {cx, cy, cz, R(0)};  // the first direction: w + 0 c
+    nxt[i].c = {R(0), R(0), R(0), R(0)};
   }
   if (!grid_sync<2>(a, sh, red)) return false;
+  {
+    CW<R>* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
   double delta = red[0];
   const double bb = red[1];
   const double tol = sizeof(R) == 4 ? fmax(a.tol, kMixedTolFloor) : a.tol;
@@ -733,28 +842,22 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
   breakdown = false;
   while (delta > ziel && it < a.cg_max) {
     const R rb = R(beta);
-    apply_elements<R>(a, vw, rb);
-    if (!barrier(a, sh)) return false;
     // ca = c.Ac and, for the FP32 operator, cm = c.M(1+hc)c: the Hessian part
     // is positive semi-definite, so c.Ac >= cm holds exactly; an FP32 product
     // that falls far below it has lost the direction and the solve stops
     // there as at a breakdown (the FP64 form keeps the reference's test only).
     double ca[2] = {0.0, 0.0};
     K3D_FOR(i, a.n) {
-      const R4<R> ci = next_dir<R>(vw.cw[i], rb);
-      vw.cw[i].c = ci;
+      const R4<R> ci = next_dir<R>(cur[i], rb);
+      nxt[i].c = ci;
       R ax = 0, ay = 0, az = 0;
       if (a.frei[i]) {
-        R hx, hy, hz;
-        gather_h<R>(a, vw, i, hx, hy, hz);
-        const R m = vw.md[i];
-        ax = m * ci.x + R(h2) * hx;
-        ay = m * ci.y + R(h2) * hy;
-        az = m * ci.z + R(h2) * hz;
+        bsr_row<R>(a, cur, i, rb, ax, ay, az);
         filt<R>(vw.nrm, i, ax, ay, az);
-        if (sizeof(R) == 4)
-          ca[1] += double(m) * (double(ci.x) * double(ci.x) + double(ci.y) * double(ci.y) +
-                                double(ci.z) * double(ci.z));
+        if (sizeof(R) == 4) {
+          const double m = double(vw.md[i]);
+          ca[1] += m * (double(ci.x) * double(ci.x) + double(ci.y) * double(ci.y) + double(ci.z) * double(ci.z));
+        }
       }
       vw.ap[3 * i] = ax;
       vw.ap[3 * i + 1] = ay;
@@ -775,7 +878,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     const double alpha = delta / ca[0];
     double rzs[1] = {0.0};
     K3D_FOR(i, a.n) {
-      const R4<R> ci = vw.cw[i].c;
+      const R4<R> ci = nxt[i].c;
       D3 d = ld3(a.dv, uint32_t(i));
       d = d + d3(double(ci.x), double(ci.y), double(ci.z)) * alpha;
       st3(a.dv, uint32_t(i), d);
@@ -790,7 +893,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       if (!a.frei[i]) zx = zy = zz = 0;
       R wx = zx, wy = zy, wz = zz;
       filt<R>(vw.nrm, i, wx, wy, wz);
-      vw.cw[i].w = {wx, wy, wz, R(0)};
+      nxt[i].w = {wx, wy, wz, R(0)};
       rzs[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rzz) * double(zz);
     }
     if (!grid_sync<1>(a, sh, rzs)) return false;
@@ -824,10 +927,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
         vw.r[3 * i] = rx;
         vw.r[3 * i + 1] = ry;
         vw.r[3 * i + 2] = rz;
-        vw.z[3 * i] = zx;
-        vw.z[3 * i + 1] = zy;
-        vw.z[3 * i + 2] = zz;
-        vw.cw[i].w = {wx, wy, wz, R(0)};
+        nxt[i].w = {wx, wy, wz, R(0)};
       }
       if (!grid_sync<1>(a, sh, rz2)) return false;
       delta = rz2[0];
@@ -835,6 +935,11 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       delta_ref = delta;
     }
     beta = beta_next;
+    {
+      CW<R>* t = cur;
+      cur = nxt;
+      nxt = t;
+    }
     ++it;
   }
   iters = it;
@@ -849,15 +954,11 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
 template <typename R>
 __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double& released) {
   const bool hi = a.m_f1w64 != nullptr;
-  if (hi) {
+  if (hi)
     apply_dv64(a);
-  } else {
+  else
     dv_to_w<R>(a, vw);
-    if (!barrier(a, sh)) return false;
-    apply_elements<R>(a, vw, R(0));
-  }
   if (!barrier(a, sh)) return false;
-  const double h2 = a.h * a.h;
   double cnt[1] = {0.0};
   K3D_FOR(i, a.n) {
     const D3 n = ld3(a.nrm_d, uint32_t(i));
@@ -868,11 +969,8 @@ __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double
       rest = a_dv64(a, i) - b;
     } else {
       R hx, hy, hz;
-      gather_h<R>(a, vw, i, hx, hy, hz);
-      const R4<R> ci = vw.cw[i].w;
-      const R m = vw.md[i];
-      rest = d3(double(m * ci.x + R(h2) * hx) - b.x, double(m * ci.y + R(h2) * hy) - b.y,
-                double(m * ci.z + R(h2) * hz) - b.z);
+      bsr_row<R>(a, vw.cw, i, R(0), hx, hy, hz);
+      rest = d3(double(hx), double(hy), double(hz)) - b;
     }
     const double fn = dot(rest, n) / a.h;
     if (fn < 0.0) {
@@ -1066,6 +1164,7 @@ struct Kernels {
   static void* pl() { return (void*)probe_load_kernel<R>; }
   static void* ap() { return (void*)apply_kernel<R>; }
   static void* po() { return (void*)probe_out_kernel<R>; }
+  static void* as() { return (void*)assemble_kernel<R>; }
 };
 
 static int g_solve_blocks[2] = {0, 0};
@@ -1117,6 +1216,8 @@ static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int&
     return cudaSuccess;
   }
   if (a.ev_solve0 && (e = cudaEventRecord(a.ev_solve0, st)) != cudaSuccess) return e;
+  if ((e = plain(Kernels<R>::as(), a, a.bplane, st)) != cudaSuccess) return e;
+  launched += 1;
   if ((e = cooperative(Kernels<R>::sv(), a, blocks, st)) != cudaSuccess) return e;
   if (a.ev_solve1 && (e = cudaEventRecord(a.ev_solve1, st)) != cudaSuccess) return e;
   launched += 1;

@@ -74,6 +74,12 @@ struct StepArgs {
   const double2* s_kl;
   double4 *s_bc, *s_lc;
   void *s_dq, *s_k;
+  // assembled A: block (rank k, row i) at k * np + i of `bplane` blocks, 9
+  // planes of R (row-major 3x3); per block the contribution list ctr_off/ctr
+  const uint32_t *row_cnt, *col, *ctr_off, *ctr;
+  void* bmat;
+  int64_t bplane;
+  void* cw2;  // second (c, w) buffer: the row product reads one, writes the other
   // FP64 copies of the operator records for the residuals of the mixed form
   // (start residual, reliable updates, release test); null in the FP64 form
   void *m_f1w64, *m_f2w64, *m_kgB64, *b_grad64, *s_dq64, *s_k64, *slot64;
