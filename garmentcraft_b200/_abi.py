@@ -10,6 +10,8 @@ c_u32_p = C.POINTER(C.c_uint32)
 c_u8_p = C.POINTER(C.c_uint8)
 c_f32_p = C.POINTER(C.c_float)
 
+K3D_ABI_VERSION = 2
+
 K3D_OK = 0
 K3D_NOT_CONVERGED = 1
 K3D_BREAKDOWN = 2
@@ -105,6 +107,10 @@ class K3dScene(C.Structure):
         ("koerper", C.POINTER(K3dBody)),
         ("param", K3dSimparams),
         ("zeit", C.c_double),
+        ("n_teile", C.c_int64),
+        ("teil_bereiche", C.POINTER(C.c_int64)),
+        ("teil_dehnung", c_f64_p),
+        ("teil_band_von", C.POINTER(C.c_int32)),
     ]
 
 

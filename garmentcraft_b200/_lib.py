@@ -86,7 +86,7 @@ def lib():
     L.k3d_operator_noalloc.argtypes = [C.POINTER(_abi.K3dParams), C.POINTER(_abi.K3dScene), C.c_void_p,
                                        C.c_void_p, C.c_void_p]
     L.k3d_operator_noalloc.restype = st
-    if L.k3d_abi_version() != 1:
+    if L.k3d_abi_version() != _abi.K3D_ABI_VERSION:
         raise RuntimeError("libklon3d_b200.so ABI version mismatch")
     _lib = L
     return L

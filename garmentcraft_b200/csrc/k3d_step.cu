@@ -1054,9 +1054,12 @@ __global__ void __launch_bounds__(kBlock) build_points_kernel(const __grid_const
 }
 
 // PCG with the release test (persistent, cooperative): MODE_STEP runs up to
-// two solves with a release pass after each, MODE_SOLVE one solve.
+// two solves with a release pass after each, MODE_SOLVE one solve. One block
+// of 512 threads per SM in both precisions: the iteration is bound by the two
+// grid barriers, whose cost grows with the number of arriving blocks, and the
+// 128 registers a thread gets at this shape keep the FP32 form free of spills.
 template <typename R>
-__global__ void __launch_bounds__(kSolveBlock, sizeof(R) == 4 ? 2 : 1) solve_kernel(const __grid_constant__ StepArgs a) {
+__global__ void __launch_bounds__(kSolveBlock, 1) solve_kernel(const __grid_constant__ StepArgs a) {
   __shared__ Shared sh;
   if (threadIdx.x == 0) {
     sh.epoch = 0;

@@ -176,6 +176,12 @@ k3d_status build_scene_impl(const k3d_pattern* pat, BuiltScene& S) {
     const double skala = 1.0 - t.reduktion;
     const uint32_t off = uint32_t(S.masse.size());
     versatz[ti] = off;
+    // Teilinfo (szene.rs:483-489): point and triangle ranges, stretch stiffness
+    S.teil_bereiche.insert(S.teil_bereiche.end(), {int64_t(off), int64_t(off) + t.n_punkte,
+                                                   int64_t(S.dreiecke.size() / 3),
+                                                   int64_t(S.dreiecke.size() / 3) + t.n_dreiecke});
+    S.teil_dehnung.push_back(t.material.dehnung_n_m);
+    S.teil_band_von.push_back(-1);
     std::vector<double>& pm = pts_m[ti];
     pm.resize(2 * size_t(t.n_punkte));
     for (int64_t i = 0; i < t.n_punkte; ++i) {
@@ -434,6 +440,10 @@ void built_scene_view(BuiltScene& S, k3d_scene* o) {
   o->dreiecke = S.dreiecke.data();
   o->ruhe_inv = S.ruhe_inv.data();
   o->param = S.param;
+  o->n_teile = int64_t(S.teil_dehnung.size());
+  o->teil_bereiche = S.teil_bereiche.data();
+  o->teil_dehnung = S.teil_dehnung.data();
+  o->teil_band_von = S.teil_band_von.data();
 }
 
 }  // namespace k3d

@@ -14,6 +14,9 @@ struct BuiltScene {
   std::vector<double> a_r, a_a, n_r, b_r, b_a;
   std::vector<uint8_t> mkante;
   std::vector<double> m_flaeche, m_ruhe_inv, m_kette, m_schuss, m_steif, ruhe_inv;
+  std::vector<int64_t> teil_bereiche;  // 4 per piece
+  std::vector<double> teil_dehnung;
+  std::vector<int32_t> teil_band_von;
   k3d_simparams param{};
   size_t membran_entartet = 0, naht_biegung_ohne = 0, einhalte_kanten = 0;
   size_t farben[3] = {0, 0, 0};

@@ -28,6 +28,7 @@ _ARRAYS = {
     "membran_ruhe_inv": (np.float64, 4), "membran_kette": (np.float64, 2),
     "membran_schuss": (np.float64, 2), "membran_steif": (np.float64, 3),
     "dreiecke": (np.uint32, 3), "ruhe_inv": (np.float64, 4),
+    "teil_bereiche": (np.int64, 4), "teil_dehnung": (np.float64, 0), "teil_band_von": (np.int32, 0),
 }
 _COUNT = {
     "x": "n_punkte", "v": "n_punkte", "masse": "n_punkte", "w": "n_punkte",
@@ -38,8 +39,10 @@ _COUNT = {
     "membran_punkte": "n_membran", "membran_flaeche": "n_membran", "membran_ruhe_inv": "n_membran",
     "membran_kette": "n_membran", "membran_schuss": "n_membran", "membran_steif": "n_membran",
     "dreiecke": "n_dreiecke", "ruhe_inv": "n_dreiecke",
+    "teil_bereiche": "n_teile", "teil_dehnung": "n_teile", "teil_band_von": "n_teile",
 }
-_CTYPE = {np.float64: C.c_double, np.uint32: C.c_uint32, np.uint8: C.c_uint8}
+_CTYPE = {np.float64: C.c_double, np.uint32: C.c_uint32, np.uint8: C.c_uint8, np.int64: C.c_int64,
+          np.int32: C.c_int32}
 
 
 @dataclass
@@ -67,6 +70,11 @@ class Szene:
     membran_steif: np.ndarray
     dreiecke: np.ndarray
     ruhe_inv: np.ndarray
+    # Teilinfo (szene.rs:181-194): per part its point and triangle ranges
+    # (start, end, start, end), stretch stiffness and folded-band carrier (-1)
+    teil_bereiche: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), dtype=np.int64))
+    teil_dehnung: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    teil_band_von: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int32))
     koerper: list = field(default_factory=list)
     param: Simparameter = field(default_factory=Simparameter)
     zeit: float = 0.0
@@ -112,6 +120,7 @@ class Szene:
         s.n_biegung = self.biegung_punkte.shape[0]
         s.n_membran = self.membran_punkte.shape[0]
         s.n_dreiecke = self.dreiecke.shape[0]
+        s.n_teile = self.teil_dehnung.shape[0]
         for name, (dt, _) in _ARRAYS.items():
             setattr(s, name, _abi.ptr(getattr(self, name), _CTYPE[dt]))
         bodies = (_abi.K3dBody * max(len(self.koerper), 1))()

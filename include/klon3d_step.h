@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define K3D_ABI_VERSION 1
+#define K3D_ABI_VERSION 2
 
 /* Status of a call. Unconverged CG is data (k3d_cg_result), not an error,
  * as in CgLauf (sim/src/implizit.rs:294-299). */
@@ -123,6 +123,13 @@ typedef struct k3d_scene {
   const k3d_body* koerper;
   k3d_simparams param;
   double zeit;
+  /* Teilinfo (sim/src/szene.rs:181-194), read by self-collision only
+   * (selbstkollision.rs:623-688). n_teile = 0 with null arrays: no parts
+   * (every point and triangle gets stretch stiffness 0, no folded bands). */
+  int64_t n_teile;
+  const int64_t* teil_bereiche;  /* 4 per part: first point, end point, first triangle, end triangle */
+  const double* teil_dehnung;    /* per part: the material's dehnung_n_m, N/m */
+  const int32_t* teil_band_von;  /* per part: carrier part of a folded allowance band, -1 = none; may be null */
 } k3d_scene;
 
 /* ImplizitStatistik (sim/src/implizit.rs:535-561), field for field. */

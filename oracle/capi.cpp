@@ -102,7 +102,15 @@ struct Gebaut {
     }
     for (auto& d : s.dreiecke) dr.insert(dr.end(), d.begin(), d.end());
     for (auto& r : s.ruhe_inv) ri.insert(ri.end(), r.begin(), r.end());
+    for (auto& t : s.teile) {
+      tb.insert(tb.end(), {int64_t(t.p0), int64_t(t.p1), int64_t(t.d0), int64_t(t.d1)});
+      te.push_back(t.dehnung_n_m);
+      tv.push_back(int32_t(t.band_von));
+    }
   }
+  std::vector<int64_t> tb;
+  std::vector<double> te;
+  std::vector<int32_t> tv;
 };
 
 Szene szene_aus(const k3d_scene* k, Koerperdaten& kd) {
@@ -154,6 +162,16 @@ Szene szene_aus(const k3d_scene* k, Koerperdaten& kd) {
     s.dreiecke.push_back({k->dreiecke[3 * t], k->dreiecke[3 * t + 1], k->dreiecke[3 * t + 2]});
     s.ruhe_inv.push_back({k->ruhe_inv[4 * t], k->ruhe_inv[4 * t + 1], k->ruhe_inv[4 * t + 2], k->ruhe_inv[4 * t + 3]});
   }
+  for (int64_t t = 0; t < k->n_teile; ++t) {
+    Teilinfo ti;
+    ti.p0 = size_t(k->teil_bereiche[4 * t]);
+    ti.p1 = size_t(k->teil_bereiche[4 * t + 1]);
+    ti.d0 = size_t(k->teil_bereiche[4 * t + 2]);
+    ti.d1 = size_t(k->teil_bereiche[4 * t + 3]);
+    ti.dehnung_n_m = k->teil_dehnung[t];
+    ti.band_von = k->teil_band_von ? k->teil_band_von[t] : -1;
+    s.teile.push_back(ti);
+  }
   kd = koerper_aus(k->koerper, k->n_koerper);
   s.koerper = kd.koerper;
   s.param = sim_aus(k->param);
@@ -170,6 +188,9 @@ ImplizitParameter param_aus(const k3d_params* p) {
   o.kontakt_rand = p->kontakt_rand;
   o.normalkraft_aus_last = p->normalkraft_aus_last != 0;
   o.durchstoss_pruefen = p->durchstoss_pruefen != 0;
+  o.selbstkollision = p->selbstkollision != 0;
+  o.selbst_zusatzdicke = p->selbst_zusatzdicke;
+  o.selbst_steifigkeit = p->selbst_steifigkeit;
   return o;
 }
 
@@ -191,6 +212,8 @@ void stats_aus(const ImplizitStatistik& st, k3d_stats* out) {
   out->durchstoesse = int64_t(st.durchstoesse);
   out->koerperpunkte = int64_t(st.koerperpunkte);
   out->rest_max = st.rest_max;
+  out->naehe_punkt_dreieck = int64_t(st.naehe_punkt_dreieck);
+  out->naehe_kante_kante = int64_t(st.naehe_kante_kante);
 }
 
 }  // namespace
@@ -273,6 +296,10 @@ void orc_built_scene_view(void* h, k3d_scene* out) {
   out->param.bild_dt = g->s.param.bild_dt;
   for (int a = 0; a < 3; ++a) out->param.schwerkraft[a] = g->s.param.schwerkraft[a];
   out->param.daempfung = g->s.param.daempfung;
+  out->n_teile = int64_t(g->s.teile.size());
+  out->teil_bereiche = g->tb.data();
+  out->teil_dehnung = g->te.data();
+  out->teil_band_von = g->tv.data();
 }
 
 int64_t orc_built_scene_counts(void* h, int64_t* out6) {
@@ -310,6 +337,8 @@ void orc_sim_frames(void* h, int32_t n, k3d_stats* st) {
     summe.haftend += b.haftend;
     summe.freigegeben += b.freigegeben;
     summe.rest_max = std::max(summe.rest_max, b.rest_max);
+    summe.naehe_punkt_dreieck += b.naehe_punkt_dreieck;
+    summe.naehe_kante_kante += b.naehe_kante_kante;
   }
   stats_aus(summe, st);
 }
@@ -536,6 +565,127 @@ int32_t orc_kontakt(const k3d_body* kb, const double* x, double abstand, double*
   for (int a = 0; a < 3; ++a) normale3[a] = k->normale[a];
   *tiefe = k->tiefe;
   return 1;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ self-collision probes
+namespace {
+std::vector<V3> v3_aus(const double* p, size_t n) {
+  std::vector<V3> o(n);
+  for (size_t i = 0; i < n; ++i) o[i] = {p[3 * i], p[3 * i + 1], p[3 * i + 2]};
+  return o;
+}
+int64_t naehe_aus(const std::vector<Naehe>& nh, int64_t cap, int32_t* art, uint32_t* punkte4, double* gewichte4,
+                  double* normale3, double* abstand, double* ruhe) {
+  const int64_t n = int64_t(nh.size());
+  for (int64_t q = 0; q < std::min(n, cap); ++q) {
+    const Naehe& p = nh[size_t(q)];
+    if (art) art[q] = int32_t(p.art);
+    for (int k = 0; k < 4; ++k) {
+      if (punkte4) punkte4[4 * q + k] = p.punkte[k];
+      if (gewichte4) gewichte4[4 * q + k] = p.gewichte[k];
+    }
+    for (int k = 0; k < 3; ++k)
+      if (normale3) normale3[3 * q + k] = p.normale[k];
+    if (abstand) abstand[q] = p.abstand;
+    if (ruhe) ruhe[q] = p.ruhe;
+  }
+  return n;
+}
+std::pair<Stoffnetz, Stoffwerte> netz_von(Sim* sim) {
+  return aus_szene(sim->s, sim->cg.param.selbst_zusatzdicke);
+}
+}  // namespace
+
+extern "C" {
+
+int64_t orc_zellindex(double x, double zelle) { return zellindex(x, zelle); }
+uint64_t orc_streue(int64_t i, int64_t j, int64_t k, uint64_t n) { return uint64_t(streue(i, j, k, size_t(n))); }
+
+// Stoffnetz::neu on raw triangles and radii, then finde (the reference's
+// own unit tests build the mesh this way, selbstkollision.rs:1352-1396)
+int64_t orc_finde_roh(int64_t n, const double* x, const double* w, int64_t nt, const uint32_t* dreiecke,
+                      const double* r_punkt, int32_t pd, int32_t kk, int64_t cap, int32_t* art, uint32_t* punkte4,
+                      double* gewichte4, double* normale3, double* abstand, double* ruhe) {
+  std::vector<std::array<uint32_t, 3>> d(static_cast<size_t>(nt));
+  for (int64_t t = 0; t < nt; ++t) d[size_t(t)] = {dreiecke[3 * t], dreiecke[3 * t + 1], dreiecke[3 * t + 2]};
+  Stoffnetz netz = stoffnetz_neu(d, std::vector<double>(r_punkt, r_punkt + n));
+  std::vector<double> wv(w, w + n);
+  return naehe_aus(finde(netz, v3_aus(x, size_t(n)), wv, pd != 0, kk != 0), cap, art, punkte4, gewichte4, normale3,
+                   abstand, ruhe);
+}
+
+// Proximity pairs of the simulation's scene at positions x (its own w).
+int64_t orc_selbst_finde(void* h, const double* x, int32_t pd, int32_t kk, int64_t cap, int32_t* art,
+                         uint32_t* punkte4, double* gewichte4, double* normale3, double* abstand, double* ruhe) {
+  auto* sim = static_cast<Sim*>(h);
+  auto nw = netz_von(sim);
+  return naehe_aus(finde(nw.first, v3_aus(x, sim->s.x.size()), sim->s.w, pd != 0, kk != 0), cap, art, punkte4,
+                   gewichte4, normale3, abstand, ruhe);
+}
+
+// Edge list of the scene's self-collision mesh (Stoffnetz::neu order),
+// 2 per edge, and the hash cell size; returns the edge count.
+int64_t orc_selbst_kanten(void* h, int64_t cap, uint32_t* kanten2, double* zelle) {
+  auto* sim = static_cast<Sim*>(h);
+  auto nw = netz_von(sim);
+  const auto& k = nw.first.kanten;
+  for (size_t e = 0; e < std::min(k.size(), size_t(cap)); ++e) {
+    kanten2[2 * e] = k[e][0];
+    kanten2[2 * e + 1] = k[e][1];
+  }
+  if (zelle) *zelle = hash_zelle(nw.first);
+  return int64_t(k.size());
+}
+
+// Hashgitter::neu of the point boxes (kanten = 0) or the edge boxes
+// (kanten = 1) at positions x: bucket starts (eimer + 1) and entries.
+// Returns the bucket count; *n_eintraege = entry count.
+int64_t orc_selbst_hash(void* h, const double* x, int32_t kanten, int64_t cap_anfang, uint32_t* anfang,
+                        int64_t cap_eintraege, uint32_t* eintraege, int64_t* n_eintraege) {
+  auto* sim = static_cast<Sim*>(h);
+  auto nw = netz_von(sim);
+  const Stoffnetz& netz = nw.first;
+  std::vector<V3> xv = v3_aus(x, sim->s.x.size());
+  std::vector<Quader> q;
+  if (kanten) {
+    for (size_t e = 0; e < netz.kanten.size(); ++e)
+      q.push_back(kanten_quader(xv[netz.kanten[e][0]], xv[netz.kanten[e][1]], netz.r_kante[e] + ZUSCHLAG_QUADER));
+  } else {
+    for (size_t v = 0; v < xv.size(); ++v) q.push_back(quader_punkte(&xv[v], 1, netz.r_punkt[v] + ZUSCHLAG_QUADER));
+  }
+  Hashgitter g = hashgitter_neu(q, hash_zelle(netz));
+  for (size_t b = 0; b < std::min(g.anfang.size(), size_t(cap_anfang)); ++b) anfang[b] = g.anfang[b];
+  for (size_t e = 0; e < std::min(g.eintraege.size(), size_t(cap_eintraege)); ++e) eintraege[e] = g.eintraege[e];
+  if (n_eintraege) *n_eintraege = int64_t(g.eintraege.size());
+  return int64_t(g.eimer);
+}
+
+// finde + federn on the simulation's scene at (x, v): springs (5 points and
+// weights, force, 3x3 block) and the damped velocities in v_inout.
+int64_t orc_selbst_federn(void* h, const double* x, double* v_inout, int64_t cap, uint32_t* punkte5,
+                          double* gewichte5, double* kraft3, double* block9) {
+  auto* sim = static_cast<Sim*>(h);
+  auto nw = netz_von(sim);
+  const size_t n = sim->s.x.size();
+  std::vector<V3> xv = v3_aus(x, n), vv = v3_aus(v_inout, n);
+  auto nh = finde(nw.first, xv, sim->s.w, true, true);
+  auto fe = federn(nw.first, nw.second, nh, sim->cg.param.selbst_steifigkeit, sim->s.masse, sim->s.w,
+                   sim->s.naht.ruhe, vv);
+  for (size_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) v_inout[3 * i + a] = vv[i][a];
+  for (size_t q = 0; q < std::min(fe.size(), size_t(cap)); ++q) {
+    for (int k = 0; k < 5; ++k) {
+      punkte5[5 * q + k] = fe[q].punkte[k];
+      gewichte5[5 * q + k] = fe[q].gewichte[k];
+    }
+    for (int a = 0; a < 3; ++a) {
+      kraft3[3 * q + a] = fe[q].kraft[a];
+      for (int b = 0; b < 3; ++b) block9[9 * q + 3 * a + b] = fe[q].block[a][b];
+    }
+  }
+  return int64_t(fe.size());
 }
 
 }  // extern "C"

@@ -1,7 +1,8 @@
 // ORACLE (test infrastructure). Restatement of the implicit CG step
 // (sim/src/implizit.rs) in FP64, same loops and summation order: System::mal_h,
 // mal_a, diag, CpuLoeser::loese, ImplizitCg::system_bauen / schritt / bild.
-// Glue zones and self-collision springs are not part of this restatement.
+// Glue zones, and the penetration and impact stages of self-collision, are
+// not part of this restatement; its proximity springs are (selbst.cpp).
 #include <algorithm>
 #include <cfloat>
 #include <limits>
@@ -34,6 +35,16 @@ M3 m3_inv(const M3& m) {
           V3{(d * h - e * g) * s, (b * g - a * h) * s, (a * e - b * d) * s}};
 }
 
+// implizit.rs:63-70: the (first side, second side, |g_q g_r|) pairs of a spring
+template <typename F>
+static void feder_paare(const Feder& fe, F&& f) {
+  for (int q = 0; q < 5; ++q)
+    for (int r = 0; r < 5; ++r) {
+      double gq = fe.gewichte[q], gr = fe.gewichte[r];
+      if (gq > 0.0 && gr < 0.0) f(size_t(fe.punkte[q]), size_t(fe.punkte[r]), -gq * gr);
+    }
+}
+
 // implizit.rs:185-221
 void System::mal_h(const std::vector<V3>& p, std::vector<V3>& out) const {
   for (auto& o : out) o = {0, 0, 0};
@@ -59,6 +70,12 @@ void System::mal_h(const std::vector<V3>& p, std::vector<V3>& out) const {
     auto hu = membran_mal_h_aus(m.element, membran_h[t], d3);
     for (int k = 0; k < 3; ++k) out[m.punkte[k]] = add(out[m.punkte[k]], hu[k]);
   }
+  for (const auto& fe : this->federn)
+    feder_paare(fe, [&](size_t q, size_t r, double om) {
+      V3 t = mul(m3_mal(fe.block, sub(p[q], p[r])), om);
+      out[q] = add(out[q], t);
+      out[r] = sub(out[r], t);
+    });
 }
 // implizit.rs:224-229
 void System::mal_a(const std::vector<V3>& p, std::vector<V3>& out) const {
@@ -94,6 +111,12 @@ std::vector<M3> System::diag() const {
       for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) dg[m.punkte[k]][a][b] += h2 * bl[k][a][b];
   }
+  for (const auto& fe : this->federn)
+    feder_paare(fe, [&](size_t q, size_t r, double om) {
+      for (size_t pt : {q, r})
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) dg[pt][a][b] += h2 * om * fe.block[a][b];
+    });
   return dg;
 }
 
@@ -158,6 +181,22 @@ System ImplizitCg::system_bauen(Szene& s, double h, std::vector<std::optional<Fe
   const size_t n = s.x.size();
   const V3 g = s.param.schwerkraft;
   const double c = s.param.daempfung;
+  // implizit.rs:668-691: proximity pairs and springs; their approach damping
+  // acts on v before every other force
+  std::vector<Feder> fed;
+  if (param.selbstkollision) {
+    if (!selbst || selbst->first.r_punkt.size() != n) selbst = aus_szene(s, param.selbst_zusatzdicke);
+    const auto& netz = selbst->first;
+    const auto& werte = selbst->second;
+    std::vector<Naehe> naehe = finde(netz, s.x, s.w, true, true);
+    for (const auto& p : naehe) {
+      if (p.art == Art::PunktDreieck)
+        statistik.naehe_punkt_dreieck += 1;
+      else
+        statistik.naehe_kante_kante += 1;
+    }
+    fed = federn(netz, werte, naehe, param.selbst_steifigkeit, s.masse, s.w, s.naht.ruhe, s.v);
+  }
   std::vector<V3> f(n), last(n);
   for (size_t i = 0; i < n; ++i) {
     f[i] = sub(mul(g, s.masse[i]), mul(s.v[i], c * s.masse[i]));
@@ -214,6 +253,10 @@ System ImplizitCg::system_bauen(Szene& s, double h, std::vector<std::optional<Fe
     for (int m = 0; m < 4; ++m) f[idx[m]] = sub(f[idx[m]], mul(gr[m], k * fehler));
     sys.biegungen.push_back({idx, gr, k, ruhe});
   }
+  // implizit.rs:798-805
+  for (const auto& fe : fed)
+    for (int q = 0; q < 5; ++q) f[fe.punkte[q]] = add(f[fe.punkte[q]], mul(fe.kraft, fe.gewichte[q]));
+  sys.federn = std::move(fed);
   for (const auto& m : s.membran_elemente) {
     std::array<V3, 3> p3 = {s.x[m.punkte[0]], s.x[m.punkte[1]], s.x[m.punkte[2]]};
     auto fe = membran_krafte(m.element, p3);

@@ -130,6 +130,13 @@ struct Gruppe {
   std::vector<std::pair<size_t, size_t>> farben;
   size_t size() const { return punkte.size(); }
 };
+// sim/src/szene.rs:181-194 (Teilinfo: the fields self-collision reads)
+struct Teilinfo {
+  size_t p0 = 0, p1 = 0;  // point range
+  size_t d0 = 0, d1 = 0;  // triangle range
+  double dehnung_n_m = 0;
+  int64_t band_von = -1;  // carrier part of a folded allowance band, -1 = none
+};
 // sim/src/szene.rs:198-269 (the fields the implicit step reads)
 struct Szene {
   std::vector<V3> x, v;
@@ -141,6 +148,7 @@ struct Szene {
   std::vector<uint8_t> membran_kante;
   std::vector<MembranElement> membran_elemente;
   std::vector<Koerper> koerper;
+  std::vector<Teilinfo> teile;
   Simparameter param;
   double zeit = 0;
   size_t membran_entartet = 0, naht_biegung_ohne = 0, einhalte_kanten = 0;
@@ -185,13 +193,79 @@ struct Biegung {
   std::array<V3, 4> grad{};
   double k = 0, ruhe = 0;
 };
+// ---------------------------------------------------------------- self-collision
+// sim/src/selbstkollision.rs:41-588 (proximity stage: search and springs)
+constexpr double ZUSCHLAG_QUADER = 2e-5;
+constexpr double ZUSCHLAG_PAAR = 4e-5;
+constexpr double KANTE_MIN = 1e-4;
+constexpr double AUSLENKUNG_MAX = 2.5e-3;
+constexpr double ANNAEHERUNG_ANTEIL = 1.0 / 32.0;
+constexpr uint32_t KEIN = 0xffffffffu;
+using Quader = std::pair<V3, V3>;
+enum class Art { PunktDreieck = 0, KanteKante = 1 };
+struct Naehe {
+  Art art = Art::PunktDreieck;
+  std::array<uint32_t, 4> punkte{};
+  std::array<double, 4> gewichte{};
+  V3 normale{};
+  double abstand = 0, ruhe = 0;
+};
+struct Stoffnetz {
+  std::vector<std::array<uint32_t, 3>> dreiecke;
+  std::vector<std::array<uint32_t, 2>> kanten, kanten_dreiecke;
+  std::vector<std::array<uint32_t, 3>> dreieck_kanten;
+  std::vector<double> r_punkt, r_kante, r_dreieck;
+  std::map<std::pair<uint32_t, uint32_t>, uint32_t> kanten_index;
+  std::vector<std::vector<uint32_t>> naht_partner;
+  std::vector<uint32_t> teil_von, band_von;
+  std::vector<double> dicke;
+  bool band_und_traeger(uint32_t a, uint32_t b) const;
+  std::optional<double> band_abstand(uint32_t a, const uint32_t* andere, int n) const;
+  bool gleich_oder_partner(uint32_t a, uint32_t b) const;
+};
+Stoffnetz stoffnetz_neu(const std::vector<std::array<uint32_t, 3>>& dreiecke, std::vector<double> r_punkt);
+struct Normalen {
+  std::vector<V3> dreieck, punkt, kantenebene;
+};
+Normalen normalen_neu(const Stoffnetz& netz, const std::vector<V3>& x);
+int64_t zellindex(double x, double zelle);
+size_t streue(int64_t i, int64_t j, int64_t k, size_t n);
+struct Hashgitter {
+  double zelle = 0;
+  size_t eimer = 0;
+  std::vector<uint32_t> anfang, eintraege;
+};
+Hashgitter hashgitter_neu(const std::vector<Quader>& quader, double zelle);
+Quader quader_punkte(const V3* p, int n, double m);
+Quader kanten_quader(V3 a, V3 b, double m);
+std::array<double, 3> naechster_dreieck(V3 p0, V3 p1, V3 p2, V3 x);
+// the hash cell size of both searches (selbstkollision.rs:402,514)
+double hash_zelle(const Stoffnetz& netz);
+std::vector<Naehe> finde(const Stoffnetz& netz, const std::vector<V3>& x, const std::vector<double>& w, bool pd,
+                         bool kk);
+struct Stoffwerte {
+  std::vector<double> e_punkt, a_punkt, e_kante, a_kante, e_dreieck, a_dreieck, mu_punkt;
+  std::vector<std::vector<std::pair<uint32_t, uint32_t>>> naht_partner;
+};
+std::pair<Stoffnetz, Stoffwerte> aus_szene(const Szene& s, double zusatzdicke);
+// sim/src/selbstkollision.rs:691-697
+struct Feder {
+  std::array<uint32_t, 5> punkte{};
+  std::array<double, 5> gewichte{};
+  V3 kraft{};
+  M3 block{};
+};
+std::vector<Feder> federn(const Stoffnetz& netz, const Stoffwerte& werte, const std::vector<Naehe>& naehe,
+                          double steifigkeit, const std::vector<double>& masse, const std::vector<double>& w,
+                          const std::vector<double>& naht_ruhe, std::vector<V3>& v);
+
 // sim/src/implizit.rs:594-599
 struct Fest {
   V3 normale{};
   double vn_soll = 0;
   V3 v_koerper{};
 };
-// sim/src/implizit.rs:124-172 (without self-collision springs)
+// sim/src/implizit.rs:124-172
 struct System {
   double h = 0, c = 0;
   size_t cg_max = 0;
@@ -203,6 +277,7 @@ struct System {
   std::vector<Biegung> biegungen;
   const std::vector<MembranElement>* membran = nullptr;
   std::vector<Hessen> membran_h;
+  std::vector<Feder> federn;
   std::vector<V3> rhs, f, last;
   std::vector<M3> pinv;
   void mal_h(const std::vector<V3>& p, std::vector<V3>& out) const;
@@ -228,11 +303,14 @@ struct ImplizitParameter {
   double kontakt_rand = 1e-4;
   bool normalkraft_aus_last = false;
   bool durchstoss_pruefen = true;
+  bool selbstkollision = false;  // proximity stage only (selbstkollision.rs:387-788)
+  double selbst_zusatzdicke = 2.5e-3;
+  double selbst_steifigkeit = 1e-3;
 };
 // sim/src/implizit.rs:535-561
 struct ImplizitStatistik {
   size_t cg_iterationen = 0, loesungen = 0, nicht_konvergiert = 0, kontakte = 0, haftend = 0,
-         freigegeben = 0, durchstoesse = 0, koerperpunkte = 0;
+         freigegeben = 0, durchstoesse = 0, koerperpunkte = 0, naehe_punkt_dreieck = 0, naehe_kante_kante = 0;
   double rest_max = 0;
 };
 // sim/src/implizit.rs:570-1057
@@ -240,6 +318,7 @@ struct ImplizitCg {
   ImplizitParameter param;
   ImplizitStatistik statistik;
   std::vector<V3> dv_vorher;
+  std::optional<std::pair<Stoffnetz, Stoffwerte>> selbst;
   System system_bauen(Szene& s, double h, std::vector<std::optional<Fest>>& fest);
   void schritt(Szene& s, double h);
   void bild(Szene& s);

@@ -63,6 +63,7 @@ Szene szene_bauen(const Muster& netz, const std::vector<Koerper>& koerper, Simpa
     double skala = 1.0 - t.reduktion;
     uint32_t off = uint32_t(s.x.size());
     versatz.push_back(off);
+    const size_t d_anfang = s.dreiecke.size();
     std::vector<V2> p_m;
     for (const auto& p : t.punkte_mm) p_m.push_back({p[0] * 1e-3, p[1] * 1e-3});
     V2 dir2 = t.fadenlauf;
@@ -132,6 +133,8 @@ Szene szene_bauen(const Muster& netz, const std::vector<Koerper>& koerper, Simpa
     skala_je_teil.push_back(skala);
     kanten_index_je_teil.push_back(kanten_e);
     biegesteif.push_back(mat.biegung_nm);
+    // szene.rs:483-489
+    s.teile.push_back({off, s.x.size(), d_anfang, s.dreiecke.size(), mat.dehnung_n_m, -1});
   }
 
   // szene.rs:492-529 bending across seams
