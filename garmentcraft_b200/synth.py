@@ -222,6 +222,38 @@ def sheet_over_sphere(n: int = 257, groesse_m: float = 1.0, jitter_mm: float = 1
     return Muster([teil], [], param), body
 
 
+# ------------------------------------------------------------------ two layers
+def zwei_lagen(groesse_m: float = 0.2, kante_mm: float = 10.0, abstand_m: float = 0.01,
+               material: Material = RADICAL_RUBBER_04, neigung: float = 0.0, z_unten: float = 0.0,
+               oben_groesse_m: float | None = None, versatz_m=(0.0, 0.0)):
+    """Two square pieces, the upper one ``abstand_m`` above the lower (the
+    reference's self-collision scene, sim/tests/selbstkollision.rs:15-32,
+    meshed as a regular grid instead of by the mesher). The upper piece has
+    side ``oben_groesse_m`` (default: the same) and is shifted by
+    ``versatz_m`` in x and y. With ``neigung`` it is tilted:
+    z = z_unten + abstand_m + neigung * x. Frame 1/30 s, air damping 1. Pin
+    the lower piece's points (w = 0) with ``pin_teil(szene, 0)``. Returns the
+    pattern."""
+    nk = int(round(groesse_m * 1e3 / kante_mm))
+    p, tri = rechteck_netz(groesse_m * 1e3, groesse_m * 1e3, nk, nk)
+    xm, ym = p[:, 0] * 1e-3, p[:, 1] * 1e-3
+    unten = np.stack([xm, ym, np.full(xm.shape, z_unten)], axis=1)
+    go = groesse_m if oben_groesse_m is None else oben_groesse_m
+    no = int(round(go * 1e3 / kante_mm))
+    q, tq = rechteck_netz(go * 1e3, go * 1e3, no, no)
+    xo, yo = q[:, 0] * 1e-3 + versatz_m[0], q[:, 1] * 1e-3 + versatz_m[1]
+    oben = np.stack([xo, yo, z_unten + abstand_m + neigung * xo], axis=1)
+    teile = [Teil(p, tri, (1.0, 0.0), material, unten), Teil(q, tq, (1.0, 0.0), material, oben)]
+    param = Simparameter(bild_dt=1.0 / 30.0, schwerkraft=(0.0, 0.0, -9.81), daempfung=1.0)
+    return Muster(teile, [], param)
+
+
+def pin_teil(szene, teil: int) -> None:
+    """Holds every point of one piece (w = 0), as the reference's tests do."""
+    a, b = int(szene.teil_bereiche[teil, 0]), int(szene.teil_bereiche[teil, 1])
+    szene.w[a:b] = 0.0
+
+
 def body_to_c(body: dict) -> _abi.K3dBody:
     """k3d_body from a body dict; the dict keeps the SDF array alive."""
     kb = _abi.K3dBody()

@@ -84,6 +84,24 @@ def lib():
     L.orc_faerbe.restype = C.c_int64
     L.orc_kontakt.argtypes = [C.POINTER(_abi.K3dBody), dp, C.c_double, dp, dp]
     L.orc_kontakt.restype = C.c_int32
+    u32p = C.POINTER(C.c_uint32)
+    i32p = C.POINTER(C.c_int32)
+    i64p = C.POINTER(C.c_int64)
+    L.orc_zellindex.argtypes = [C.c_double, C.c_double]
+    L.orc_zellindex.restype = C.c_int64
+    L.orc_streue.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_uint64]
+    L.orc_streue.restype = C.c_uint64
+    L.orc_finde_roh.argtypes = [C.c_int64, dp, dp, C.c_int64, u32p, dp, C.c_int32, C.c_int32, C.c_int64,
+                                i32p, u32p, dp, dp, dp, dp]
+    L.orc_finde_roh.restype = C.c_int64
+    L.orc_selbst_finde.argtypes = [P, dp, C.c_int32, C.c_int32, C.c_int64, i32p, u32p, dp, dp, dp, dp]
+    L.orc_selbst_finde.restype = C.c_int64
+    L.orc_selbst_kanten.argtypes = [P, C.c_int64, u32p, dp]
+    L.orc_selbst_kanten.restype = C.c_int64
+    L.orc_selbst_hash.argtypes = [P, dp, C.c_int32, C.c_int64, u32p, C.c_int64, u32p, i64p]
+    L.orc_selbst_hash.restype = C.c_int64
+    L.orc_selbst_federn.argtypes = [P, dp, dp, C.c_int64, u32p, dp, dp, dp]
+    L.orc_selbst_federn.restype = C.c_int64
     _lib = L
     return L
 
@@ -213,3 +231,71 @@ class OracleSim:
         out = np.zeros(3)
         self.L.orc_sim_schwerpunkt(self.h, _d(out))
         return out
+
+
+def _naehe(call, cap=0):
+    """Runs a pair query twice (count, then fill) and returns the pairs as arrays."""
+    n = call(0, None, None, None, None, None, None)
+    art = np.zeros(max(n, 1), dtype=np.int32)
+    pk = np.zeros((max(n, 1), 4), dtype=np.uint32)
+    gw = np.zeros((max(n, 1), 4))
+    nr = np.zeros((max(n, 1), 3))
+    ab = np.zeros(max(n, 1))
+    ru = np.zeros(max(n, 1))
+    call(n, art.ctypes.data_as(C.POINTER(C.c_int32)), pk.ctypes.data_as(C.POINTER(C.c_uint32)), _d(gw), _d(nr),
+         _d(ab), _d(ru))
+    return dict(art=art[:n], punkte=pk[:n], gewichte=gw[:n], normale=nr[:n], abstand=ab[:n], ruhe=ru[:n])
+
+
+def finde_roh(x, w, dreiecke, r_punkt, punkt_dreieck=True, kante_kante=True):
+    """Stoffnetz::neu + finde (selbstkollision.rs:159-187, 387-398) on a bare mesh."""
+    L = lib()
+    x, w, r = f64(x), f64(w), f64(r_punkt)
+    d = np.ascontiguousarray(dreiecke, dtype=np.uint32)
+    return _naehe(lambda cap, *o: L.orc_finde_roh(x.shape[0], _d(x), _d(w), d.shape[0],
+                                                  d.ctypes.data_as(C.POINTER(C.c_uint32)), _d(r),
+                                                  int(punkt_dreieck), int(kante_kante), cap, *o))
+
+
+class SelbstProbe:
+    """Self-collision probes on an OracleSim's scene (aus_szene with its params)."""
+
+    def __init__(self, sim: "OracleSim"):
+        self.sim = sim
+        self.L = sim.L
+
+    def finde(self, x, punkt_dreieck=True, kante_kante=True):
+        x = f64(x)
+        return _naehe(lambda cap, *o: self.L.orc_selbst_finde(self.sim.h, _d(x), int(punkt_dreieck),
+                                                              int(kante_kante), cap, *o))
+
+    def kanten(self):
+        z = C.c_double()
+        n = self.L.orc_selbst_kanten(self.sim.h, 0, None, C.byref(z))
+        k = np.zeros((max(n, 1), 2), dtype=np.uint32)
+        self.L.orc_selbst_kanten(self.sim.h, n, k.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(z))
+        return k[:n], z.value
+
+    def hash(self, x, kanten: bool):
+        """(anfang, eintraege) of Hashgitter::neu over the point or edge boxes."""
+        x = f64(x)
+        ne = C.c_int64()
+        eimer = self.L.orc_selbst_hash(self.sim.h, _d(x), int(kanten), 0, None, 0, None, C.byref(ne))
+        anf = np.zeros(eimer + 1, dtype=np.uint32)
+        ein = np.zeros(max(ne.value, 1), dtype=np.uint32)
+        self.L.orc_selbst_hash(self.sim.h, _d(x), int(kanten), eimer + 1, anf.ctypes.data_as(C.POINTER(C.c_uint32)),
+                               ne.value, ein.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(ne))
+        return anf, ein[:ne.value]
+
+    def federn(self, x, v):
+        """Springs and the damped velocities (selbstkollision.rs:713-787)."""
+        x = f64(x)
+        vv = f64(v).copy()
+        n = self.L.orc_selbst_federn(self.sim.h, _d(x), _d(vv.copy()), 0, None, None, None, None)
+        pk = np.zeros((max(n, 1), 5), dtype=np.uint32)
+        gw = np.zeros((max(n, 1), 5))
+        kr = np.zeros((max(n, 1), 3))
+        bl = np.zeros((max(n, 1), 3, 3))
+        self.L.orc_selbst_federn(self.sim.h, _d(x), _d(vv), n, pk.ctypes.data_as(C.POINTER(C.c_uint32)), _d(gw),
+                                 _d(kr), _d(bl))
+        return dict(punkte=pk[:n], gewichte=gw[:n], kraft=kr[:n], block=bl[:n]), vv

@@ -1,0 +1,146 @@
+"""The oracle's self-collision proximity stage against the reference's own tests.
+
+Known answers from sim/src/selbstkollision.rs:1352-1396 (two layers in range,
+crossed edges) and sim/tests/selbstkollision.rs:34-64 (the upper layer comes to
+rest on the pinned lower one). The reference meshes its 20 x 20 cm squares with
+its own mesher; these tests use a regular 10 mm grid.
+"""
+import math
+
+import numpy as np
+
+import oracle_py as O
+from garmentcraft_b200 import synth
+from garmentcraft_b200.params import ImplizitParameter
+
+
+def _quadrat(z):
+    return [[0.0, 0.0, z], [0.01, 0.0, z], [0.01, 0.01, z], [0.0, 0.01, z]]
+
+
+def test_zwei_lagen_in_naehe():
+    """selbstkollision.rs:1352-1372: all eight points in range at r = 1.45 mm,
+    distance 2 mm, rest 2.9 mm; none at r = 0.5 mm."""
+    x = np.array(_quadrat(0.0) + _quadrat(0.002))
+    d = [[0, 1, 2], [0, 2, 3], [4, 5, 6], [4, 6, 7]]
+    w = np.ones(8)
+    n = O.finde_roh(x, w, d, np.full(8, 1.45e-3), True, False)
+    assert sorted(set(int(p) for p in n["punkte"][:, 0])) == list(range(8))
+    assert np.all(np.abs(n["abstand"] - 0.002) < 1e-12)
+    assert np.all(np.abs(n["ruhe"] - 2.9e-3) < 1e-12)
+    assert np.all(n["art"] == 0)
+    n = O.finde_roh(x, w, d, np.full(8, 0.5e-3), True, True)
+    assert n["punkte"].shape[0] == 0
+
+
+def test_gekreuzte_kanten():
+    """selbstkollision.rs:1376-1396: one edge-edge pair, normal from the
+    second edge to the first, weights exactly (0.5, 0.5, -0.5, -0.5)."""
+    x = np.array([[-0.01, 0.0, 0.001], [0.01, 0.0, 0.001], [0.0, -0.01, 0.0], [0.0, 0.01, 0.0], [0.02, 0.0, 0.0],
+                  [0.0, 0.02, 0.001]])
+    d = [[0, 1, 5], [2, 3, 4]]
+    n = O.finde_roh(x, np.ones(6), d, np.full(6, 1e-3), False, True)
+    kk = [q for q in range(n["punkte"].shape[0]) if list(n["punkte"][q, :2]) == [0, 1]]
+    assert len(kk) == 1
+    q = kk[0]
+    assert abs(n["abstand"][q] - 0.001) < 1e-12
+    assert abs(n["normale"][q, 2] - 1.0) < 1e-12
+    assert list(n["gewichte"][q]) == [0.5, 0.5, -0.5, -0.5]
+    assert n["art"][q] == 1
+
+
+def test_zellindex_und_streue():
+    """selbstkollision.rs:263-278: floor division, saturating cast, Ericson's
+    primes on the wrapped 32-bit cell coordinates, unsigned remainder."""
+    L = O.lib()
+    assert L.orc_zellindex(0.0059, 0.0059) == 1
+    assert L.orc_zellindex(-1e-9, 0.0059) == -1
+    assert L.orc_zellindex(float("nan"), 1.0) == 0
+    assert L.orc_zellindex(1e300, 1e-3) == 2**63 - 1
+    assert L.orc_zellindex(-1e300, 1e-3) == -(2**63)
+    for i, j, k, n in [(0, 0, 0, 64), (1, -2, 3, 1000), (-7, 11, -13, 4097), (2**40 + 5, -(2**35), 9, 12345)]:
+        h = (((i & 0xffffffff) * 0x8DA6B343) & 0xffffffff) ^ (((j & 0xffffffff) * 0xD8163841) & 0xffffffff) ^ \
+            (((k & 0xffffffff) * 0xCB1AB31F) & 0xffffffff)
+        assert L.orc_streue(i, j, k, n) == h % n
+
+
+# The upper piece is inset (18 cm, shifted by 7.3 / 4.1 mm) so that every
+# upper point lies over the interior of a lower triangle. Two identical
+# regular grids stack their boundary points exactly; rounding then moves an
+# upper corner outside the lower piece by ~1e-12 m, it fails the prism test of
+# every lower triangle, and only the reference's impact stage (not restated)
+# would catch it.
+INSET = dict(oben_groesse_m=0.18, versatz_m=(0.0073, 0.0041))
+
+
+def _zwei_lagen_sim(selbst: bool, abstand_m=0.01, neigung=0.0):
+    m = synth.zwei_lagen(abstand_m=abstand_m, neigung=neigung, **INSET)
+    s = O.build_scene(m)
+    synth.pin_teil(s, 0)
+    p = ImplizitParameter(selbstkollision=selbst)
+    return s, O.OracleSim(s, p.to_c())
+
+
+def test_hash_buckets():
+    """Hashgitter::neu (selbstkollision.rs:281-324): max(2n, 64) buckets, the
+    bucket starts are the prefix sum of per-box distinct buckets, entries
+    ascend inside a bucket, and every box sits in each of its cells' buckets."""
+    s, sim = _zwei_lagen_sim(True, abstand_m=0.002)
+    probe = O.SelbstProbe(sim)
+    kanten, zelle = probe.kanten()
+    r = s.kollisionsabstand + 2.5e-3 / 2.0
+    assert abs(zelle - max(2.0 * r.max() + 4e-5, 1e-4) * 2.0) == 0.0
+    for which in (False, True):
+        anf, ein = probe.hash(s.x, which)
+        n_box = kanten.shape[0] if which else s.n
+        assert anf.shape[0] == max(2 * n_box, 64) + 1
+        assert anf[0] == 0 and anf[-1] == ein.shape[0] and np.all(np.diff(anf.astype(np.int64)) >= 0)
+        for b in range(anf.shape[0] - 1):
+            seg = ein[anf[b]:anf[b + 1]]
+            assert np.all(np.diff(seg.astype(np.int64)) > 0)
+        assert np.bincount(ein, minlength=n_box).min() >= 1
+
+
+def test_obere_lage_bleibt_liegen():
+    """sim/tests/selbstkollision.rs:34-64: without self-collision the upper
+    layer falls through the pinned lower one; with it, it comes to rest
+    2.0-3.2 mm above (rest distance r1 + r2 = 2.9 mm) and pairs are found.
+    Here it rests at 2.899-2.900 mm (the reference measured 2.66-2.90 mm
+    with its mesh)."""
+    s, sim = _zwei_lagen_sim(False)
+    sim.frames(30)
+    x, _ = sim.state()
+    oben = slice(int(s.teil_bereiche[1, 0]), int(s.teil_bereiche[1, 1]))
+    assert x[oben, 2].min() < -0.05
+    s, sim = _zwei_lagen_sim(True)
+    paare = 0
+    for _ in range(60):
+        st = sim.frames(1)
+        paare = st.naehe_punkt_dreieck + st.naehe_kante_kante
+    x, _ = sim.state()
+    z, hoechster = x[oben, 2].min(), x[oben, 2].max()
+    assert paare > 0
+    assert z > 2.0e-3 and hoechster < 3.2e-3, (z, hoechster)
+
+
+def test_federn_impuls():
+    """selbstkollision.rs:760-778: the approach damping conserves momentum
+    when every point is free, and touches nothing that separates."""
+    s, sim = _zwei_lagen_sim(True, abstand_m=0.002)
+    s.w[:] = 1.0 / np.maximum(s.masse, 1e-30)
+    sim = O.OracleSim(s, ImplizitParameter(selbstkollision=True).to_c())
+    probe = O.SelbstProbe(sim)
+    v = np.zeros((s.n, 3))
+    oben = slice(int(s.teil_bereiche[1, 0]), int(s.teil_bereiche[1, 1]))
+    v[oben, 2] = -0.3
+    fe, vd = probe.federn(s.x, v)
+    assert fe["punkte"].shape[0] > 0
+    p0 = (s.masse[:, None] * v).sum(axis=0)
+    p1 = (s.masse[:, None] * vd).sum(axis=0)
+    assert np.max(np.abs(p1 - p0)) < 1e-12 * np.abs(p0).max()
+    assert np.max(vd[oben, 2]) > -0.3
+    fe2, vs = probe.federn(s.x, -v)
+    assert np.array_equal(vs, -v)
+    # force along the normal, k (mu I + (1 - mu) n n^T) blocks are symmetric
+    assert np.allclose(fe["block"], np.transpose(fe["block"], (0, 2, 1)), rtol=0, atol=0)
+    assert np.all(fe["gewichte"][:, 4] == 0.0) and np.array_equal(fe["punkte"][:, 4], fe["punkte"][:, 0])
