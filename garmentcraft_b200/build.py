@@ -12,14 +12,18 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_native")
 LIB = os.path.join(OUT_DIR, "libklon3d_b200.so")
-SOURCES = ["k3d_step.cu", "k3d_host.cpp", "scene_build.cpp", "k3d_noalloc.cu"]
-HEADERS = ["k3d_step.h", "k3d_device.cuh", "scene_build.h"]
+SOURCES = ["k3d_step.cu", "k3d_build.cu", "k3d_host.cpp", "scene_build.cpp", "k3d_noalloc.cu"]
+HEADERS = ["k3d_step.h", "k3d_device.cuh", "k3d_step_common.cuh", "scene_build.h"]
+# Per-file flags. The build of the system rounds every product and sum on its
+# own (no fused multiply-add), as the reference's arithmetic does: see the
+# header of k3d_build.cu for the element term that needs it.
+EXTRA = {"k3d_build.cu": ["-fmad=false"]}
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
-    "-Xcompiler", "-O3", "-Xcompiler", "-ffp-contract=off", "-cudart", "shared",
+    "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+    "-Xcompiler", "-O3", "-Xcompiler", "-ffp-contract=off",
 ]
 
 
@@ -35,19 +39,22 @@ def _stale() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
-    os.makedirs(OUT_DIR, exist_ok=True)
-    srcs = []
+    obj_dir = os.path.join(OUT_DIR, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    objs = []
     for f in SOURCES:
         p = os.path.join(CSRC, f)
-        if f.endswith(".cpp"):
-            srcs += ["-x", "cu", p]
-        else:
-            srcs.append(p)
-    cmd = [NVCC, *FLAGS, "-o", LIB + ".tmp", *srcs]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True, cwd=CSRC)
+        o = os.path.join(obj_dir, f + ".o")
+        lang = ["-x", "cu"] if f.endswith(".cpp") else []
+        cmd = [NVCC, *FLAGS, *EXTRA.get(f, []), "-c", *lang, p, "-o", o]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True, cwd=CSRC)
+        objs.append(o)
+    link = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "--shared", "-cudart", "shared",
+            "-o", LIB + ".tmp", *objs]
+    subprocess.run(link, check=True, cwd=CSRC)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -95,6 +95,12 @@ struct StepArgs {
   double* stat_rest_max;
 };
 
+// The build, probe and integration kernels (compiled apart from the PCG).
+struct BuildKernels {
+  const void *elements, *points, *assemble, *probe_load, *probe_apply, *probe_out, *integrate;
+};
+BuildKernels build_kernels(int precision);
+
 int step_grid_blocks(int precision, int device);
 // Enqueues one substep (or probe) on `stream`; `launched` = kernels enqueued.
 cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream_t stream, int& launched);

@@ -57,6 +57,30 @@ def test_operator_wie_cpu(prec, tol):
         assert rel(b, a) <= tol
 
 
+@pytest.mark.parametrize("prec,tol", [(_abi.K3D_FP64, 1e-12), (_abi.K3D_MIXED, 2e-5)])
+def test_operator_gescherter_zustand(prec, tol):
+    # In-plane distortion with shear stiffness: elements whose warp strain is
+    # clamped and whose shear is small sit where the PSD projection of the
+    # geometric stress (kontinuum.rs:158-177) cancels; the device's build has
+    # to round exactly like the reference there.
+    p, tri = synth.rechteck_netz(200.0, 200.0, 20, 20)
+    lage = np.stack([p[:, 0] * 1e-3, p[:, 1] * 1e-3, np.zeros(p.shape[0])], axis=1)
+    m = synth.Muster([synth.Teil(p, tri, (1.0, 0.0), synth.RADICAL_RUBBER_04, lage)], [],
+                     synth.Simparameter(bild_dt=1.0 / 30.0, daempfung=1.0))
+    s = build_scene(m)
+    rng = np.random.default_rng(5)
+    s.x[:, :2] += rng.uniform(-2e-4, 2e-4, size=(s.n, 2))
+    s.x[:, 2] += rng.uniform(-1e-4, 1e-4, size=s.n)
+    orc = O.OracleSim(s, ImplizitParameter().to_c())
+    cg = ImplizitCg(ImplizitParameter(precision=prec))
+    for q in [rng.normal(size=(s.n, 3)), streuung(s.n)]:
+        assert rel(cg.operator(s, q), orc.operator(q)) <= tol
+    if prec == _abi.K3D_FP64:
+        g, o = cg.system_fuer(s), orc.system()
+        assert rel(g["rhs"], o["rhs"]) <= 1e-11
+        assert np.max(np.abs(g["pinv"] - o["pinv"]) / np.abs(o["pinv"]).max(axis=(1, 2))[:, None, None]) <= 1e-10
+
+
 def test_system_wie_cpu():
     s = small_sheet()
     par = ImplizitParameter(schritte_je_bild=1)

@@ -39,7 +39,8 @@ def device_scene(s, torch):
     cs.n_biegung = s.biegung_punkte.shape[0]
     cs.n_membran = s.membran_punkte.shape[0]
     cs.n_dreiecke = s.dreiecke.shape[0]
-    ctype = {np.float64: C.c_double, np.uint32: C.c_uint32, np.uint8: C.c_uint8}
+    ctype = {np.float64: C.c_double, np.uint32: C.c_uint32, np.uint8: C.c_uint8, np.int64: C.c_int64,
+             np.int32: C.c_int32}
     for name, (dt, _) in _ARRAYS.items():
         a = np.ascontiguousarray(getattr(s, name), dtype=dt)
         raw = np.frombuffer(a.tobytes(), dtype=np.uint8).copy() if a.size else np.zeros(8, np.uint8)
