@@ -20,7 +20,7 @@ EXPORTS = [
     "k3d_last_error", "k3d_solver_name", "k3d_upload_scene", "k3d_frame", "k3d_frames_resident",
     "k3d_upload_state", "k3d_download_state", "k3d_operator", "k3d_system_for", "k3d_solve",
     "k3d_residual", "k3d_read_load", "k3d_last_frame_ms", "k3d_last_solve_ms", "k3d_kernel_launches",
-    "k3d_operator_noalloc",
+    "k3d_operator_noalloc", "k3d_selfcollision_pairs", "k3d_selfcollision_hash", "k3d_selfcollision_springs",
 ]
 
 _lib = None
@@ -86,6 +86,13 @@ def lib():
     L.k3d_operator_noalloc.argtypes = [C.POINTER(_abi.K3dParams), C.POINTER(_abi.K3dScene), C.c_void_p,
                                        C.c_void_p, C.c_void_p]
     L.k3d_operator_noalloc.restype = st
+    u32p = C.POINTER(C.c_uint32)
+    L.k3d_selfcollision_pairs.argtypes = [P, C.c_int64, C.POINTER(C.c_int32), u32p, dp, dp, dp, dp]
+    L.k3d_selfcollision_pairs.restype = C.c_int64
+    L.k3d_selfcollision_hash.argtypes = [P, C.c_int32, C.c_int64, u32p, C.c_int64, u32p, C.POINTER(C.c_int64)]
+    L.k3d_selfcollision_hash.restype = C.c_int64
+    L.k3d_selfcollision_springs.argtypes = [P, C.c_int64, dp, dp]
+    L.k3d_selfcollision_springs.restype = C.c_int64
     if L.k3d_abi_version() != _abi.K3D_ABI_VERSION:
         raise RuntimeError("libklon3d_b200.so ABI version mismatch")
     _lib = L

@@ -213,6 +213,18 @@ __device__ void build_points(const StepArgs& a, const View<R>& vw, double& held)
       D[4] += kn * nx * nz;
       D[5] += kn * ny * nz;
     }
+    if (a.sc_off) {  // proximity springs: force, -h H v, diagonal (implizit.rs:798-805, 887-894)
+      for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
+        const uint32_t ent = a.sc_ent[e];
+        const double4 kf = a.sc_kf[ent >> 2];
+        const double4 g4 = a.sc_w[ent >> 2];
+        const uint32_t k = ent & 3u;
+        const double g = k == 0 ? g4.x : k == 1 ? g4.y : k == 2 ? g4.z : g4.w;
+        acc = acc + d3(kf.x, kf.y, kf.z) * g;
+      }
+      const D3 hv = feder_hp64(a, i, [&](uint32_t j) { return ld3(a.v, j); }, D);
+      acc = acc - hv * h;
+    }
     st3(a.b, uint32_t(i), acc * h);
     if (a.need_load) st3(a.load, uint32_t(i), load);
     const double mdi = m * (1.0 + h * a.daempf);
@@ -514,6 +526,18 @@ __global__ void __launch_bounds__(kBlock) probe_out_kernel(const __grid_constant
   K3D_FOR(i, a.n) {
     R hx, hy, hz;
     gather_h<R>(a, vw, i, hx, hy, hz);
+    if (a.sc_off) {
+      const D3 sp = feder_hp64(
+          a, i,
+          [&](uint32_t j) {
+            const R4<R> c = vw.cw[j].w;
+            return d3(double(c.x), double(c.y), double(c.z));
+          },
+          nullptr);
+      hx += R(sp.x);
+      hy += R(sp.y);
+      hz += R(sp.z);
+    }
     const D3 b = ld3(a.b, uint32_t(i));
     if (a.mode == MODE_SYSTEM) {
       st3(a.p_out, uint32_t(i), b * (1.0 / a.h) + d3(double(hx), double(hy), double(hz)) * a.h);

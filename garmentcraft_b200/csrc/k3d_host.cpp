@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/klon3d_step.h"
+#include "k3d_selbst_host.h"
 #include "k3d_step.h"
 #include "scene_build.h"
 
@@ -58,6 +59,7 @@ struct k3d_solver {
   StepArgs a{};  // device pointers and constants; per-launch fields are set before each launch
   double* d_pin = nullptr;  // probe input (3N)
   double* d_pout = nullptr; // probe output (3N)
+  SelbstHost sc;            // self-collision proximity stage (when enabled)
 };
 
 static k3d_status fail(k3d_solver* h, k3d_status st, const std::string& msg) {
@@ -315,6 +317,7 @@ k3d_solver* k3d_solver_create(const k3d_params* params, int32_t device) {
 }
 
 static void release_device(k3d_solver* h) {
+  selbst_free(h->sc);
   if (h->arena.base) cudaFree(h->arena.base);
   h->arena = Arena{};
   for (void* p : h->sdf_dev) cudaFree(p);
@@ -382,6 +385,10 @@ static k3d_status validate(const k3d_scene* s) {
   if (s->n_membran && (!s->membran_punkte || !s->membran_flaeche || !s->membran_ruhe_inv || !s->membran_kette ||
                        !s->membran_schuss || !s->membran_steif || !chk(s->membran_punkte, 3 * s->n_membran)))
     return K3D_BAD_ARGUMENT;
+  if (s->n_dreiecke < 0 ||
+      (s->n_dreiecke && (!s->dreiecke || !s->ruhe_inv || !chk(s->dreiecke, 3 * s->n_dreiecke))))
+    return K3D_BAD_ARGUMENT;
+  if (s->n_teile < 0 || (s->n_teile && (!s->teil_bereiche || !s->teil_dehnung))) return K3D_BAD_ARGUMENT;
   if (s->n_koerper < 0 || s->n_koerper > kMaxBodies || (s->n_koerper && !s->koerper)) return K3D_BAD_ARGUMENT;
   for (int b = 0; b < s->n_koerper; ++b) {
     const k3d_body& k = s->koerper[b];
@@ -603,6 +610,12 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
     h->sdf_dev.push_back(d);
   }
   K3D_CUDA(h, cudaStreamSynchronize(st));
+  if (h->p.selbstkollision) {
+    if (n >= (int64_t(1) << 30) || s->n_dreiecke >= (int64_t(1) << 31))
+      return fail(h, K3D_BAD_ARGUMENT, "scene too large for the self-collision stage");
+    K3D_CUDA(h, selbst_upload(h->sc, s, h->p.selbst_zusatzdicke, h->p.selbst_steifigkeit, int(R), a.x, a.v, cv.masse,
+                              cv.w, cv.reib, st));
+  }
 
   a.n = n;
   a.nt = nt;
@@ -653,6 +666,11 @@ static k3d_status launch(k3d_solver* h, int mode, double t_bodies, bool need_loa
     d.sdf = static_cast<const float*>(h->sdf_dev[b]);
   }
   int launched = 0;
+  if (h->sc.on) {  // proximity pairs and springs before the system (implizit.rs:668-691)
+    cudaError_t es = selbst_run(h->sc, a.h, h->stream, launched);
+    if (es != cudaSuccess) return cuda_fail(h, es, "self-collision stage");
+  }
+  selbst_step_args(h->sc, a);
   cudaError_t e = launch_step(a, h->p.precision == K3D_MIXED ? 1 : 0, h->blocks, h->stream, launched);
   h->launches += launched;
   if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
@@ -697,12 +715,15 @@ static k3d_status read_stats(k3d_solver* h, k3d_stats* out) {
     out->rest_max = rm[0];
     out->zusammenbrueche = st[ST_BREAKDOWNS];
     out->dv_max = rm[1];
+    out->naehe_punkt_dreieck = int64_t(h->sc.naehe_pt);
+    out->naehe_kante_kante = int64_t(h->sc.naehe_kk);
   }
   if (st[ST_NONFINITE] > 0) return fail(h, K3D_NON_FINITE, "non-finite position or velocity after the step");
   return K3D_OK;
 }
 
 static k3d_status reset_stats(k3d_solver* h) {
+  h->sc.naehe_pt = h->sc.naehe_kk = 0;
   K3D_CUDA(h, cudaMemsetAsync(h->a.stats, 0, sizeof(long long) * ST_COUNT, h->stream));
   K3D_CUDA(h, cudaMemsetAsync(h->a.stat_rest_max, 0, sizeof(double) * 2, h->stream));
   return K3D_OK;
@@ -776,6 +797,7 @@ k3d_status k3d_frame(k3d_solver* h, k3d_scene* s, k3d_stats* stats) {
   if (seams)
     K3D_CUDA(h, cudaMemcpyAsync(const_cast<double2*>(h->a.s_kl), h->s_kl_host.data(), 16 * h->s_kl_host.size(),
                                 cudaMemcpyHostToDevice, h->stream));
+  K3D_CUDA(h, selbst_set_naht_ruhe(h->sc, s->naht_ruhe, s->n_naht, h->stream));
   for (int b = 0; b < s->n_koerper; ++b)
     for (int q = 0; q < 3; ++q) {
       h->bodies[b].punkt[q] = s->koerper[b].punkt[q];
@@ -921,6 +943,102 @@ k3d_status k3d_read_load(k3d_solver* h, double* out) {
   if (!out) return fail(h, K3D_BAD_ARGUMENT, "null vector");
   K3D_CUDA(h, cudaMemcpy(out, h->a.load, 24 * size_t(h->n), cudaMemcpyDeviceToHost));
   return K3D_OK;
+}
+
+// ------------------------------------------------------------ self-collision probes
+static bool selbst_ready(k3d_solver* h) {
+  if (ready(h) != K3D_OK) return false;
+  if (!h->sc.on || !h->sc.ran) {
+    fail(h, K3D_BAD_ARGUMENT, "self-collision is off or has not run");
+    return false;
+  }
+  return cudaStreamSynchronize(h->stream) == cudaSuccess;
+}
+
+int64_t k3d_selfcollision_pairs(k3d_solver* h, int64_t cap, int32_t* art, uint32_t* punkte, double* gewichte,
+                                double* normale, double* abstand, double* ruhe) {
+  if (!selbst_ready(h)) return -1;
+  const SelbstArgs& s = h->sc.s;
+  const int64_t np = int64_t(h->sc.n_pt) + h->sc.n_kk;
+  const int64_t m = std::min(np, cap);
+  if (m <= 0) return np;
+  std::vector<uint4> idx(m);
+  std::vector<double4> w(m), nab(m);
+  std::vector<double> ru(m);
+  if (cudaMemcpy(idx.data(), s.pr_idx, 16 * m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(w.data(), s.pr_w, 32 * m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(nab.data(), s.pr_nab, 32 * m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(ru.data(), s.pr_ruhe, 8 * m, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  for (int64_t q = 0; q < m; ++q) {
+    if (art) art[q] = q < int64_t(h->sc.n_pt) ? 0 : 1;
+    if (punkte) {
+      punkte[4 * q] = idx[q].x;
+      punkte[4 * q + 1] = idx[q].y;
+      punkte[4 * q + 2] = idx[q].z;
+      punkte[4 * q + 3] = idx[q].w;
+    }
+    if (gewichte) {
+      gewichte[4 * q] = w[q].x;
+      gewichte[4 * q + 1] = w[q].y;
+      gewichte[4 * q + 2] = w[q].z;
+      gewichte[4 * q + 3] = w[q].w;
+    }
+    if (normale) {
+      normale[3 * q] = nab[q].x;
+      normale[3 * q + 1] = nab[q].y;
+      normale[3 * q + 2] = nab[q].z;
+    }
+    if (abstand) abstand[q] = nab[q].w;
+    if (ruhe) ruhe[q] = ru[q];
+  }
+  return np;
+}
+
+int64_t k3d_selfcollision_hash(k3d_solver* h, int32_t kanten, int64_t cap_anfang, uint32_t* anfang,
+                               int64_t cap_eintraege, uint32_t* eintraege, int64_t* n_eintraege) {
+  if (!selbst_ready(h)) return -1;
+  const SelbstArgs& s = h->sc.s;
+  const uint32_t eimer = kanten ? s.eimer_k : s.eimer_p;
+  const uint32_t* anf = kanten ? s.anf_k : s.anf_p;
+  const uint32_t* ein = kanten ? s.ein_k : s.ein_p;
+  uint32_t total = 0;
+  if (cudaMemcpy(&total, anf + eimer, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  if (n_eintraege) *n_eintraege = total;
+  if (anfang && cap_anfang > 0 &&
+      cudaMemcpy(anfang, anf, 4 * size_t(std::min<int64_t>(cap_anfang, int64_t(eimer) + 1)),
+                 cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  if (eintraege && cap_eintraege > 0 && total > 0 &&
+      cudaMemcpy(eintraege, ein, 4 * size_t(std::min<int64_t>(cap_eintraege, total)), cudaMemcpyDeviceToHost) !=
+          cudaSuccess)
+    return -1;
+  return int64_t(eimer);
+}
+
+int64_t k3d_selfcollision_springs(k3d_solver* h, int64_t cap, double* kraft, double* block) {
+  if (!selbst_ready(h)) return -1;
+  const SelbstArgs& s = h->sc.s;
+  const int64_t np = int64_t(h->sc.n_pt) + h->sc.n_kk;
+  const int64_t m = std::min(np, cap);
+  if (m <= 0) return np;
+  std::vector<double4> kf(m), b0(m), b1(m);
+  if (cudaMemcpy(kf.data(), s.pr_kf, 32 * m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(b0.data(), s.pr_b0, 32 * m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(b1.data(), s.pr_b1, 32 * m, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  for (int64_t q = 0; q < m; ++q) {
+    if (kraft) {
+      kraft[3 * q] = kf[q].x;
+      kraft[3 * q + 1] = kf[q].y;
+      kraft[3 * q + 2] = kf[q].z;
+    }
+    if (block) {
+      const double B[9] = {b0[q].x, b0[q].w, b1[q].x, b0[q].w, b0[q].y, b1[q].y, b1[q].x, b1[q].y, b0[q].z};
+      for (int k = 0; k < 9; ++k) block[9 * q + k] = B[k];
+    }
+  }
+  return np;
 }
 
 }  // extern "C"

@@ -239,6 +239,7 @@ __device__ __noinline__ void apply_dv64(const StepArgs& a) {
 }
 
 // (A dv)_i in FP64 from the slots of apply_dv64.
+template <bool SC>
 __device__ __noinline__ D3 a_dv64(const StepArgs& a, int64_t i) {
   const R4<double>* sl = static_cast<const R4<double>*>(a.slot64) + i;
   double x = 0, y = 0, z = 0;
@@ -249,6 +250,12 @@ __device__ __noinline__ D3 a_dv64(const StepArgs& a, int64_t i) {
     x += o.x;
     y += o.y;
     z += o.z;
+  }
+  if (SC) {
+    const D3 sp = feder_hp64(a, i, [&](uint32_t j) { return ld3(a.dv, j); }, nullptr);
+    x += sp.x;
+    y += sp.y;
+    z += sp.z;
   }
   const double h2 = a.h * a.h, md = a.masse[i] * (1.0 + a.h * a.daempf);
   const D3 d = ld3(a.dv, uint32_t(i));
@@ -268,7 +275,7 @@ __device__ void dv_to_w(const StepArgs& a, const View<R>& vw) {
 }
 
 
-template <typename R>
+template <typename R, bool SC>
 __device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<R>* buf, int64_t i, R beta, R& ox, R& oy,
                                         R& oz) {
   const R* bm = static_cast<const R*>(a.bmat);
@@ -284,6 +291,33 @@ __device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<R>* buf, int
     y += bm[3 * P + sid] * pj.x + bm[4 * P + sid] * pj.y + bm[5 * P + sid] * pj.z;
     z += bm[6 * P + sid] * pj.x + bm[7 * P + sid] * pj.y + bm[8 * P + sid] * pj.z;
   }
+  if (SC) {  // proximity springs, matrix-free (h^2 is in their blocks)
+    const R4<R>* bR = static_cast<const R4<R>*>(a.sc_bR);
+    const R4<R>* wR = static_cast<const R4<R>*>(a.sc_wR);
+    const R4<R> pi = next_dir<R>(buf[i], beta);
+    for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
+      const uint32_t ent = a.sc_ent[e], q = ent >> 2, k = ent & 3u;
+      const uint4 id = a.sc_idx[q];
+      const R4<R> w4 = wR[q];
+      const R g[4] = {w4.x, w4.y, w4.z, w4.w};
+      const uint32_t ix[4] = {id.x, id.y, id.z, id.w};
+      const R gk = g[k];
+      R sx = 0, sy = 0, sz = 0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if ((gk > R(0) && g[r] < R(0)) || (gk < R(0) && g[r] > R(0))) {
+          const R om = -gk * g[r];
+          const R4<R> pr = next_dir<R>(buf[ix[r]], beta);
+          sx += om * (pi.x - pr.x);
+          sy += om * (pi.y - pr.y);
+          sz += om * (pi.z - pr.z);
+        }
+      const R4<R> b0 = bR[2 * q], b1 = bR[2 * q + 1];
+      x += b0.x * sx + b0.w * sy + b1.x * sz;
+      y += b0.w * sx + b0.y * sy + b1.y * sz;
+      z += b1.x * sx + b1.y * sy + b0.z * sz;
+    }
+  }
   ox = x;
   oy = y;
   oz = z;
@@ -296,7 +330,7 @@ __device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<R>* buf, int
 //   points: dv += alpha c, r -= alpha ap, z = P r, w = S z, r.z       -> sum
 // The mixed form takes its residuals (start, reliable updates) from the FP64
 // operator. Returns false on a barrier error.
-template <typename R>
+template <typename R, bool SC>
 __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& iters, bool& unconverged,
                     bool& breakdown, double& rest) {
   CW<R>* cur = static_cast<CW<R>*>(a.c);
@@ -330,10 +364,10 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       const D3 b = ld3(a.b, uint32_t(i));
       D3 ad;
       if (hi) {
-        ad = a_dv64(a, i);
+        ad = a_dv64<SC>(a, i);
       } else {
         R hx, hy, hz;
-        bsr_row<R>(a, cur, i, R(0), hx, hy, hz);
+        bsr_row<R, SC>(a, cur, i, R(0), hx, hy, hz);
         ad = d3(double(hx), double(hy), double(hz));
       }
       const D3 n = ld3(a.nrm_d, uint32_t(i));
@@ -385,7 +419,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       nxt[i].c = ci;
       R ax = 0, ay = 0, az = 0;
       if (a.frei[i]) {
-        bsr_row<R>(a, cur, i, rb, ax, ay, az);
+        bsr_row<R, SC>(a, cur, i, rb, ax, ay, az);
         filt<R>(vw.nrm, i, ax, ay, az);
         if (sizeof(R) == 4) {
           const double m = double(vw.md[i]);
@@ -445,7 +479,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
         R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, wx = 0, wy = 0, wz = 0;
         if (a.frei[i]) {
           const D3 n = ld3(a.nrm_d, uint32_t(i));
-          D3 rd = ld3(a.b, uint32_t(i)) - a_dv64(a, i);
+          D3 rd = ld3(a.b, uint32_t(i)) - a_dv64<SC>(a, i);
           rd = rd - n * dot(rd, n);
           rx = R(rd.x);
           ry = R(rd.y);
@@ -484,7 +518,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
 // ------------------------------------------------------------ release pass
 // implizit.rs:924-942: normal force from the residual A dv - b along the
 // contact normal; a held point that pulls on the body is released.
-template <typename R>
+template <typename R, bool SC>
 __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double& released) {
   const bool hi = a.m_f1w64 != nullptr;
   if (hi)
@@ -499,10 +533,10 @@ __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double
     const D3 b = ld3(a.b, uint32_t(i));
     D3 rest;
     if (hi) {
-      rest = a_dv64(a, i) - b;
+      rest = a_dv64<SC>(a, i) - b;
     } else {
       R hx, hy, hz;
-      bsr_row<R>(a, vw.cw, i, R(0), hx, hy, hz);
+      bsr_row<R, SC>(a, vw.cw, i, R(0), hx, hy, hz);
       rest = d3(double(hx), double(hy), double(hz)) - b;
     }
     const double fn = dot(rest, n) / a.h;
@@ -520,7 +554,7 @@ __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double
 }
 
 
-template <typename R>
+template <typename R, bool SC>
 __global__ void __launch_bounds__(kSolveBlock, 1) solve_kernel(const __grid_constant__ StepArgs a) {
   __shared__ Shared sh;
   if (threadIdx.x == 0) {
@@ -536,7 +570,7 @@ __global__ void __launch_bounds__(kSolveBlock, 1) solve_kernel(const __grid_cons
   bool unconv = false, brk = false;
   double rest = 0.0;
   for (int pass = 0; pass < 2; ++pass) {
-    if (!pcg<R>(a, vw, sh, iters, unconv, brk, rest)) return;
+    if (!pcg<R, SC>(a, vw, sh, iters, unconv, brk, rest)) return;
     double dvm[1] = {0.0};
     K3D_FOR(i, a.n) {
       const D3 d = ld3(a.dv, uint32_t(i));
@@ -554,7 +588,7 @@ __global__ void __launch_bounds__(kSolveBlock, 1) solve_kernel(const __grid_cons
     if (a.mode == MODE_SOLVE) return;
     if (!any_held) break;
     double rel = 0.0;
-    if (!release<R>(a, vw, sh, rel)) return;
+    if (!release<R, SC>(a, vw, sh, rel)) return;
     if (lead) a.stats[ST_RELEASED] += int64_t(rel);
     if (rel == 0.0) break;
   }
@@ -565,7 +599,8 @@ __global__ void __launch_bounds__(kSolveBlock, 1) solve_kernel(const __grid_cons
 // ------------------------------------------------------------ launch
 template <typename R>
 struct Kernels {
-  static void* sv() { return (void*)solve_kernel<R>; }
+  static void* sv() { return (void*)solve_kernel<R, false>; }
+  static void* svf() { return (void*)solve_kernel<R, true>; }
 };
 
 static int g_solve_blocks[2] = {0, 0};
@@ -620,7 +655,7 @@ static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int&
   if (a.ev_solve0 && (e = cudaEventRecord(a.ev_solve0, st)) != cudaSuccess) return e;
   if ((e = plain(K.assemble, a, a.bplane, st)) != cudaSuccess) return e;
   launched += 1;
-  if ((e = cooperative(Kernels<R>::sv(), a, blocks, st)) != cudaSuccess) return e;
+  if ((e = cooperative(a.sc_off ? Kernels<R>::svf() : Kernels<R>::sv(), a, blocks, st)) != cudaSuccess) return e;
   if (a.ev_solve1 && (e = cudaEventRecord(a.ev_solve1, st)) != cudaSuccess) return e;
   launched += 1;
   if (a.mode == MODE_STEP) {

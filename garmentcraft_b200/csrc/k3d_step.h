@@ -84,6 +84,14 @@ struct StepArgs {
   // (start residual, reliable updates, release test); null in the FP64 form
   void *m_f1w64, *m_f2w64, *m_kgB64, *b_grad64, *s_dq64, *s_k64, *slot64;
   const void *m_rin64, *m_kgA64;
+  // proximity springs of cloth self-collision (the stage's last run), null
+  // when off: per point its (pair << 2 | slot) entries; per pair its points,
+  // weights, force and k, block k[(1-mu) n n^T + mu I] as (xx, yy, zz, xy),
+  // (xz, yz, mu, 0), and the operator copies (h^2 block as 2 R4, weights R4)
+  const uint32_t *sc_off, *sc_ent;
+  const uint4* sc_idx;
+  const double4 *sc_w, *sc_kf, *sc_b0, *sc_b1;
+  const void *sc_bR, *sc_wR;
   // probes
   const double* p_in;
   double* p_out;

@@ -183,6 +183,52 @@ class ImplizitCg:
         self._check(self._L.k3d_read_load(self._h, _d(out)), "load")
         return out
 
+    # ---- self-collision probes: the proximity stage's last run
+    def _selbst_check(self, n: int, what: str) -> int:
+        if n < 0:
+            raise K3dError(_abi.K3D_BAD_ARGUMENT, f"{what}: {self._L.k3d_last_error(self._h).decode()}")
+        return n
+
+    def selbst_paare(self) -> dict:
+        """selbstkollision::finde (selbstkollision.rs:387-398) of the last run:
+        art (0 point-triangle, 1 edge-edge), punkte, gewichte, normale,
+        abstand, ruhe, in the reference's order."""
+        L = self._L
+        n = self._selbst_check(L.k3d_selfcollision_pairs(self._h, 0, None, None, None, None, None, None), "pairs")
+        m = max(n, 1)
+        art = np.zeros(m, dtype=np.int32)
+        pk = np.zeros((m, 4), dtype=np.uint32)
+        gw = np.zeros((m, 4))
+        nr = np.zeros((m, 3))
+        ab = np.zeros(m)
+        ru = np.zeros(m)
+        L.k3d_selfcollision_pairs(self._h, n, art.ctypes.data_as(C.POINTER(C.c_int32)),
+                                  pk.ctypes.data_as(C.POINTER(C.c_uint32)), _d(gw), _d(nr), _d(ab), _d(ru))
+        return dict(art=art[:n], punkte=pk[:n], gewichte=gw[:n], normale=nr[:n], abstand=ab[:n], ruhe=ru[:n])
+
+    def selbst_hash(self, kanten: bool):
+        """Hashgitter (selbstkollision.rs:256-345) of the last run's point or
+        edge boxes: (bucket starts, entries)."""
+        L = self._L
+        ne = C.c_int64()
+        eimer = self._selbst_check(L.k3d_selfcollision_hash(self._h, int(kanten), 0, None, 0, None, C.byref(ne)),
+                                   "hash")
+        anf = np.zeros(eimer + 1, dtype=np.uint32)
+        ein = np.zeros(max(ne.value, 1), dtype=np.uint32)
+        L.k3d_selfcollision_hash(self._h, int(kanten), eimer + 1, anf.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                 ne.value, ein.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(ne))
+        return anf, ein[:ne.value]
+
+    def selbst_federn(self) -> dict:
+        """selbstkollision::federn (selbstkollision.rs:713-787) of the last run:
+        force on the first side and the 3x3 block per pair."""
+        L = self._L
+        n = self._selbst_check(L.k3d_selfcollision_springs(self._h, 0, None, None), "springs")
+        kr = np.zeros((max(n, 1), 3))
+        bl = np.zeros((max(n, 1), 3, 3))
+        L.k3d_selfcollision_springs(self._h, n, _d(kr), _d(bl))
+        return dict(kraft=kr[:n], block=bl[:n])
+
     def letzte_bild_ms(self) -> float:
         return self._L.k3d_last_frame_ms(self._h)
 

@@ -52,7 +52,7 @@ typedef struct k3d_params {
   double kontakt_rand;          /* contact margin m, default 1e-4 */
   int32_t normalkraft_aus_last; /* friction normal force from the load, default 0 */
   int32_t durchstoss_pruefen;   /* segment-through-skin check (mesh bodies only), default 1 */
-  int32_t selbstkollision;      /* cloth-cloth proximity springs, default 0 */
+  int32_t selbstkollision;      /* cloth-cloth proximity springs (selbstkollision.rs:387-788), default 0 */
   int32_t precision;            /* k3d_precision, default K3D_FP64 */
   double selbst_zusatzdicke;    /* default 2.5e-3 m */
   double selbst_steifigkeit;    /* default 1e-3 */
@@ -310,6 +310,32 @@ int64_t k3d_kernel_launches(const k3d_solver* h);
  * out of range is skipped and reported as K3D_BAD_ARGUMENT. */
 k3d_status k3d_operator_noalloc(const k3d_params* params, const k3d_scene* s, const double* p, double* out,
                                 void* stream);
+
+/* ---- self-collision probes (proximity stage, sim/src/selbstkollision.rs)
+ * Readbacks of the stage's last run, which every frame, operator, system,
+ * solve and residual call makes first when k3d_params.selbstkollision is set
+ * (the penetration and impact stages of the reference are not part of it).
+ * Each returns -1 when self-collision is off or has not run (k3d_last_error
+ * says which); otherwise the full count, filling at most `cap` entries of
+ * every non-null array. */
+
+/* selbstkollision::finde (:387-398): the proximity pairs in the reference's
+ * order (point-triangle pairs by triangle, then edge-edge pairs by edge).
+ * art: 0 point-triangle, 1 edge-edge; punkte and gewichte 4 per pair (the
+ * weighted sum of the points is the gap vector from the second side to the
+ * first); normale 3 per pair; abstand; ruhe (the rest distance as found). */
+int64_t k3d_selfcollision_pairs(k3d_solver* h, int64_t cap, int32_t* art, uint32_t* punkte, double* gewichte,
+                                double* normale, double* abstand, double* ruhe);
+
+/* Hashgitter (:256-345) of the point boxes (kanten = 0) or the edge boxes
+ * (kanten = 1): returns the bucket count; anfang receives the bucket starts
+ * (bucket count + 1 values), eintraege the entries, *n_eintraege their count. */
+int64_t k3d_selfcollision_hash(k3d_solver* h, int32_t kanten, int64_t cap_anfang, uint32_t* anfang,
+                               int64_t cap_eintraege, uint32_t* eintraege, int64_t* n_eintraege);
+
+/* selbstkollision::federn (:713-787): per pair the force on the first side
+ * (3 values) and the 3x3 block k[(1 - mu) n n^T + mu I] (9 values, row-major). */
+int64_t k3d_selfcollision_springs(k3d_solver* h, int64_t cap, double* kraft, double* block);
 
 #ifdef __cplusplus
 }
