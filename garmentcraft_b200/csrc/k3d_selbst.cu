@@ -578,51 +578,171 @@ __global__ void __launch_bounds__(kT) federn_kernel(const __grid_constant__ Selb
     const D3 n = d3(nab.x, nab.y, nab.z);
     const double kc = k * c;
     s.pr_kf[q] = make_double4(n.x * kc, n.y * kc, n.z * kc, k);
-    const double m1 = 1.0 - mu;
-    const double bxx = k * (m1 * n.x * n.x + mu), byy = k * (m1 * n.y * n.y + mu), bzz = k * (m1 * n.z * n.z + mu);
-    const double bxy = k * (m1 * n.x * n.y + 0.0), bxz = k * (m1 * n.x * n.z + 0.0), byz = k * (m1 * n.y * n.z + 0.0);
+    const double om = 1.0 - mu;
+    const double bxx = k * (om * n.x * n.x + mu), byy = k * (om * n.y * n.y + mu), bzz = k * (om * n.z * n.z + mu);
+    const double bxy = k * (om * n.x * n.y + 0.0), bxz = k * (om * n.x * n.z + 0.0), byz = k * (om * n.y * n.z + 0.0);
+    // the damping's mass shares (selbstkollision.rs:759-777), in the reference's order
+    double m1 = 0.0, m2 = 0.0;
+    for (int kq = 0; kq < 4; ++kq) {
+      if (gw[kq] > 0.0)
+        m1 += gw[kq] * s.masse[idx[kq]];
+      else
+        m2 -= gw[kq] * s.masse[idx[kq]];
+    }
+    double ga[4];
+    for (int kq = 0; kq < 4; ++kq) ga[kq] = gw[kq] * (gw[kq] > 0.0 ? m2 / (m1 + m2) : m1 / (m1 + m2));
     s.pr_b0[q] = make_double4(bxx, byy, bzz, bxy);
-    s.pr_b1[q] = make_double4(bxz, byz, mu, 0.0);
+    s.pr_b1[q] = make_double4(bxz, byz, mu, m1 + m2 > 0.0 ? 1.0 : 0.0);
+    s.pr_ga[q] = make_double4(ga[0], ga[1], ga[2], ga[3]);
     bR[2 * q] = {R(h2 * bxx), R(h2 * byy), R(h2 * bzz), R(h2 * bxy)};
     bR[2 * q + 1] = {R(h2 * bxz), R(h2 * byz), R(0), R(0)};
     wR[q] = {R(gw[0]), R(gw[1]), R(gw[2]), R(gw[3])};
   }
 }
 
-// The approach damping (selbstkollision.rs:753-778) in pair order: each pair
-// reads the velocities its predecessors left, as in the reference. Pairs that
-// share a free point are chained, and in the reference's order (triangle by
-// triangle) the chain runs through nearly every pair, so this runs as one
-// thread.
-__global__ void daempfung_kernel(const __grid_constant__ SelbstArgs s) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+// The approach damping (selbstkollision.rs:753-778). The reference applies
+// it pair by pair: each pair reads the velocities its predecessors left.
+// Here one block takes the pairs in batches of kDB. The batch's free points
+// get shared-memory slots; one thread gives each pair a level, one more than
+// the highest level of the earlier pairs in the batch that share a free
+// point with it; then the levels run one after another, all pairs of a level
+// at once. Pairs of one level share no free point, and every pair runs after
+// all earlier pairs it shares a free point with, so every pair reads exactly
+// the velocities the sequential order gives it. Points that are held (w <= 0)
+// are never written and are read from global memory.
+constexpr int kDB = 512;
+constexpr int kDSlots = 4 * kDB;
+constexpr uint16_t kFest = 0xffffu;
+constexpr size_t kDampSmem = size_t(kDSlots) * (3 * sizeof(double) + sizeof(uint32_t) + sizeof(uint16_t)) +
+                             size_t(kDB) * (4 + 1) * sizeof(uint16_t) + 64;
+
+__global__ void __launch_bounds__(kDB, 1) daempfung_kernel(const __grid_constant__ SelbstArgs s) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  double* vx = reinterpret_cast<double*>(dsm);
+  double* vy = vx + kDSlots;
+  double* vz = vy + kDSlots;
+  uint32_t* slot_pt = reinterpret_cast<uint32_t*>(vz + kDSlots);
+  uint16_t* last = reinterpret_cast<uint16_t*>(slot_pt + kDSlots);
+  uint16_t* pslot = last + kDSlots;  // 4 per pair
+  uint16_t* level = pslot + 4 * kDB;
+  __shared__ uint32_t nslots, maxlevel;
   const uint32_t P = paare(s);
-  for (uint32_t q = 0; q < P; ++q) {
-    const uint4 id = s.pr_idx[q];
-    const double4 g4 = s.pr_w[q];
-    const double4 nab = s.pr_nab[q];
-    const double mu = s.pr_b1[q].z;
-    const uint32_t idx[4] = {id.x, id.y, id.z, id.w};
-    const double gw[4] = {g4.x, g4.y, g4.z, g4.w};
-    const D3 n = d3(nab.x, nab.y, nab.z);
-    double m1 = 0.0, m2 = 0.0;
-    D3 dv = d3(0.0, 0.0, 0.0);
-    for (int k = 0; k < 4; ++k) {
-      dv = dv + ld3(s.v, idx[k]) * gw[k];
-      if (gw[k] > 0.0)
-        m1 += gw[k] * s.masse[idx[k]];
-      else
-        m2 -= gw[k] * s.masse[idx[k]];
+  const int tid = threadIdx.x;
+  for (uint32_t b0 = 0; b0 < P; b0 += kDB) {
+    const uint32_t nb = P - b0 < uint32_t(kDB) ? P - b0 : uint32_t(kDB);
+    if (tid == 0) {
+      nslots = 0;
+      maxlevel = 0;
     }
-    const double an = dot(dv, n) * kAnnaeherung;
-    if (an < 0.0 && m1 + m2 > 0.0) {
-      const D3 u = n * an + (dv - n * an) * mu;
+    __syncthreads();
+    // 1. the pair's data into registers; slots for its free points (first
+    //    come, first served); held points' velocities are constant
+    const bool mine = uint32_t(tid) < nb;
+    double gw[4] = {0, 0, 0, 0}, ga[4] = {0, 0, 0, 0}, mu = 0.0, flag = 0.0;
+    D3 n = d3(0, 0, 0), vk[4];
+    uint16_t sl[4] = {kFest, kFest, kFest, kFest};
+    if (mine) {
+      const uint32_t q = b0 + tid;
+      const uint4 id = s.pr_idx[q];
+      const double4 g4 = s.pr_w[q], nab = s.pr_nab[q], b1 = s.pr_b1[q], ga4 = s.pr_ga[q];
+      const uint32_t pts[4] = {id.x, id.y, id.z, id.w};
+      gw[0] = g4.x, gw[1] = g4.y, gw[2] = g4.z, gw[3] = g4.w;
+      ga[0] = ga4.x, ga[1] = ga4.y, ga[2] = ga4.z, ga[3] = ga4.w;
+      n = d3(nab.x, nab.y, nab.z);
+      mu = b1.z;
+      flag = b1.w;
+#pragma unroll
       for (int k = 0; k < 4; ++k) {
-        if (s.w[idx[k]] <= 0.0) continue;
-        const double anteil = gw[k] > 0.0 ? m2 / (m1 + m2) : m1 / (m1 + m2);
-        st3(s.v, idx[k], ld3(s.v, idx[k]) - u * (gw[k] * anteil));
+        if (s.w[pts[k]] > 0.0) {
+          int32_t cur = atomicAdd(&s.slot_of[pts[k]], 0);
+          if (cur < 0) {
+            const uint32_t me = atomicAdd(&nslots, 1u);
+            const int32_t old = atomicCAS(&s.slot_of[pts[k]], -1, int32_t(me));
+            slot_pt[me] = old < 0 ? pts[k] : kKein;
+            cur = old < 0 ? int32_t(me) : old;
+          }
+          sl[k] = uint16_t(cur);
+          vk[k] = d3(0, 0, 0);
+        } else {
+          vk[k] = ld3(s.v, pts[k]);
+        }
+        pslot[4 * tid + k] = sl[k];
       }
     }
+    __syncthreads();
+    // 2. the slots' velocities
+    for (uint32_t q = tid; q < nslots; q += kDB) {
+      const uint32_t pt = slot_pt[q];
+      if (pt != kKein) {
+        const D3 v = ld3(s.v, pt);
+        vx[q] = v.x;
+        vy[q] = v.y;
+        vz[q] = v.z;
+      }
+      last[q] = 0;
+    }
+    __syncthreads();
+    // 3. levels, in pair order (pairs without a free point write nothing: level 0)
+    if (tid == 0) {
+      uint32_t mx = 0;
+      for (uint32_t q = 0; q < nb; ++q) {
+        const uint16_t s0 = pslot[4 * q], s1 = pslot[4 * q + 1], s2 = pslot[4 * q + 2], s3 = pslot[4 * q + 3];
+        uint32_t l = 0;
+        bool frei = false;
+        if (s0 != kFest) { l = last[s0] > l ? last[s0] : l; frei = true; }
+        if (s1 != kFest) { l = last[s1] > l ? last[s1] : l; frei = true; }
+        if (s2 != kFest) { l = last[s2] > l ? last[s2] : l; frei = true; }
+        if (s3 != kFest) { l = last[s3] > l ? last[s3] : l; frei = true; }
+        if (!frei) {
+          level[q] = 0;
+          continue;
+        }
+        ++l;
+        level[q] = uint16_t(l);
+        if (s0 != kFest) last[s0] = uint16_t(l);
+        if (s1 != kFest) last[s1] = uint16_t(l);
+        if (s2 != kFest) last[s2] = uint16_t(l);
+        if (s3 != kFest) last[s3] = uint16_t(l);
+        mx = l > mx ? l : mx;
+      }
+      maxlevel = mx;
+    }
+    __syncthreads();
+    // 4. the levels one after another
+    const uint32_t L = maxlevel;
+    const uint32_t my = mine ? level[tid] : 0u;
+    for (uint32_t lv = 1; lv <= L; ++lv) {
+      if (my == lv) {
+        D3 cur[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cur[k] = sl[k] != kFest ? d3(vx[sl[k]], vy[sl[k]], vz[sl[k]]) : vk[k];
+        D3 dv = d3(0.0, 0.0, 0.0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dv = dv + cur[k] * gw[k];
+        const double an = dot(dv, n) * kAnnaeherung;
+        if (an < 0.0 && flag != 0.0) {
+          const D3 u = n * an + (dv - n * an) * mu;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            if (sl[k] == kFest) continue;
+            const D3 nv = cur[k] - u * ga[k];
+            vx[sl[k]] = nv.x;
+            vy[sl[k]] = nv.y;
+            vz[sl[k]] = nv.z;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // 5. back to global memory; the slots are free again
+    for (uint32_t q = tid; q < nslots; q += kDB) {
+      const uint32_t pt = slot_pt[q];
+      if (pt != kKein) {
+        st3(s.v, pt, d3(vx[q], vy[q], vz[q]));
+        s.slot_of[pt] = -1;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -784,7 +904,14 @@ cudaError_t selbst_paare_und_federn(const SelbstArgs& s, cudaStream_t st) {
     federn_kernel<float><<<grid_for(pmax), kT, 0, st>>>(s);
   else
     federn_kernel<double><<<grid_for(pmax), kT, 0, st>>>(s);
-  daempfung_kernel<<<1, 32, 0, st>>>(s);
+  static bool smem_set = false;
+  if (!smem_set) {
+    if ((e = cudaFuncSetAttribute(daempfung_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kDampSmem))) !=
+        cudaSuccess)
+      return e;
+    smem_set = true;
+  }
+  daempfung_kernel<<<1, kDB, kDampSmem, st>>>(s);
   inc_count_kernel<<<grid_for(pmax), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = scan(s.inc_off, s.n + 1, s.scan_tmp, &s.zahl[SZ_INZIDENZ], st)) != cudaSuccess) return e;

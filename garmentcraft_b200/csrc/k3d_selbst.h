@@ -61,12 +61,14 @@ struct SelbstArgs {
   double4* pr_nab;         // normal, distance
   double* pr_ruhe;         // rest distance as found
   double4* pr_kf;          // force on the first side, k
-  double4 *pr_b0, *pr_b1;  // block k[(1-mu) n n^T + mu I]: (xx, yy, zz, xy), (xz, yz, mu, 0)
+  double4 *pr_b0, *pr_b1;  // block k[(1-mu) n n^T + mu I]: (xx, yy, zz, xy), (xz, yz, mu, m1 + m2 > 0)
+  double4* pr_ga;          // per slot g * (mass share of the other side), the damping's update factor
   void* pr_bR;             // h^2 * block in operator precision, 2 R4 per pair
   void* pr_wR;             // weights in operator precision, R4 per pair
   uint32_t *inc_off, *inc_cur, *inc_ent;  // per point: (pair << 2 | slot)
   uint32_t cap_inc;
-  uint32_t* zahl;  // SZ_COUNT counters
+  int32_t* slot_of;  // damping scratch per point: its shared-memory slot, -1 between batches
+  uint32_t* zahl;    // SZ_COUNT counters
   uint32_t* scan_tmp;
 };
 

@@ -260,6 +260,9 @@ cudaError_t selbst_upload(SelbstHost& H, const k3d_scene* sc, double zusatzdicke
   if ((e = alloc(s.inc_off, size_t(n) + 1, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.inc_cur, size_t(n), H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.zahl, size_t(SZ_COUNT), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.slot_of, size_t(n), H.fest)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(s.slot_of, 0xff, sizeof(int32_t) * std::max<size_t>(size_t(n), 1), st)) != cudaSuccess)
+    return e;
   const int64_t longest = std::max({int64_t(s.eimer_p) + 1, int64_t(s.eimer_k) + 1, nd + 1, ne + 1, n + 1});
   if ((e = alloc(s.scan_tmp, selbst_scan_tmp_words(longest), H.fest)) != cudaSuccess) return e;
   if ((e = selbst_grow_edge_hash(H, uint32_t(std::min<int64_t>(27 * std::max<int64_t>(ne, 1), 0x7fffffff)))) !=
@@ -292,6 +295,7 @@ cudaError_t selbst_grow_pairs(SelbstHost& H, uint32_t cap) {
   if ((e = alloc(s.pr_kf, cap, H.pairs)) != cudaSuccess) return e;
   if ((e = alloc(s.pr_b0, cap, H.pairs)) != cudaSuccess) return e;
   if ((e = alloc(s.pr_b1, cap, H.pairs)) != cudaSuccess) return e;
+  if ((e = alloc(s.pr_ga, cap, H.pairs)) != cudaSuccess) return e;
   char* bR = nullptr;
   if ((e = alloc(bR, size_t(cap) * 8 * size_t(s.rsize), H.pairs)) != cudaSuccess) return e;
   s.pr_bR = bR;
