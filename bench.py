@@ -88,10 +88,10 @@ def workload_config(n, s, extra=None):
     return cfg
 
 
-def make_scene(n, pinned=False):
+def make_scene(n, pinned=False, jitter_mm=1.0):
     from garmentcraft_b200 import synth
     from garmentcraft_b200.implizit import build_scene
-    m, body = synth.sheet_over_sphere(n=n)
+    m, body = synth.sheet_over_sphere(n=n, jitter_mm=jitter_mm)
     s = build_scene(m, [body])
     if pinned:
         import torch
