@@ -10,7 +10,7 @@ c_u32_p = C.POINTER(C.c_uint32)
 c_u8_p = C.POINTER(C.c_uint8)
 c_f32_p = C.POINTER(C.c_float)
 
-K3D_ABI_VERSION = 2
+K3D_ABI_VERSION = 3
 
 K3D_OK = 0
 K3D_NOT_CONVERGED = 1
@@ -68,6 +68,8 @@ class K3dBody(C.Structure):
         ("ursprung", C.c_double * 3),
         ("spacing", C.c_double),
         ("sdf", c_f32_p),
+        ("instanz", C.c_int32),
+        ("pad", C.c_int32),
     ]
 
 
@@ -111,6 +113,8 @@ class K3dScene(C.Structure):
         ("teil_bereiche", C.POINTER(C.c_int64)),
         ("teil_dehnung", c_f64_p),
         ("teil_band_von", C.POINTER(C.c_int32)),
+        ("n_instanzen", C.c_int64),
+        ("instanz_punkte", C.POINTER(C.c_int64)),
     ]
 
 

@@ -241,7 +241,9 @@ __device__ void build_points(const StepArgs& a, const View<R>& vw, double& held)
     bool fest = false;
     if (a.frei[i]) {
       const D3 xi = ld3(a.x, uint32_t(i));
+      const int inst = a.pinst ? int(a.pinst[i]) : 0;
       for (int kb = 0; kb < a.n_bodies; ++kb) {
+        if (a.bodies[kb].inst >= 0 && a.bodies[kb].inst != inst) continue;
         D3 nn;
         double tiefe;
         if (kontakt(a.bodies[kb], xi, a.kabst[i] + a.kontakt_rand, nn, tiefe)) {
@@ -429,7 +431,9 @@ __device__ void integrate(const StepArgs& a, double (&cnt)[3]) {
       }
     }
     D3 x = ld3(a.x, uint32_t(i)) + v * h;
+    const int inst = a.pinst ? int(a.pinst[i]) : 0;
     for (int kb = 0; kb < a.n_bodies; ++kb) {
+      if (a.bodies[kb].inst >= 0 && a.bodies[kb].inst != inst) continue;
       D3 nn;
       double tiefe;
       if (kontakt(a.bodies[kb], x, a.kabst[i], nn, tiefe)) {

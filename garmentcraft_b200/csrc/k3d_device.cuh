@@ -48,8 +48,9 @@ struct Body {
   int dims[3];
   double punkt[3], achse[3], radius, vel[3], ursprung[3], spacing;
   const float* sdf;  // device copy of the grid
+  int inst;          // the instance (independent drape) it acts on, -1 = every instance
 };
-constexpr int kMaxBodies = 8;
+constexpr int kMaxBodies = 64;
 
 // Contact query, sim/src/koerper.rs:69-91 for the cylinder; the SDF grid is a
 // trilinear interpolant of node values (value and gradient), no contact

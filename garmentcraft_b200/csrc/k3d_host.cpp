@@ -60,6 +60,7 @@ struct k3d_solver {
   double* d_pin = nullptr;  // probe input (3N)
   double* d_pout = nullptr; // probe output (3N)
   SelbstHost sc;            // self-collision proximity stage (when enabled)
+  int n_grp = 1;            // instances (independent drapes) of the uploaded scene
 };
 
 static k3d_status fail(k3d_solver* h, k3d_status st, const std::string& msg) {
@@ -152,6 +153,8 @@ struct Carve {
   void *m_rin, *m_kgA, *m_rin64, *m_kgA64;
   double2 *b_kr, *s_kl;
   uint32_t *row_cnt, *col, *ctr_off, *ctr;
+  Grp* grp;
+  uint32_t *blk_grp, *pinst;
 };
 
 // Assigns every device array of the handle from the arena (base may be null
@@ -222,6 +225,11 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.s_k = A.take<char>(S * R);
   a.sync = A.take<SyncState>(1);
   a.partials = A.take<double>(size_t(8) * h->blocks);  // two buffers of 4 sums per block
+  a.n_grp = h->n_grp;
+  a.grp = cv.grp = A.take<Grp>(size_t(h->n_grp));
+  a.blk_grp = cv.blk_grp = A.take<uint32_t>(size_t(h->blocks));
+  a.grp_cnt = A.take<unsigned>(size_t(32) * size_t(h->n_grp));
+  a.pinst = cv.pinst = h->n_grp > 1 ? A.take<uint32_t>(N) : nullptr;
   a.stats = A.take<long long>(ST_COUNT);
   a.stat_rest_max = A.take<double>(2);
   // assembled A (BSR, ELL by rank) and its contribution lists
@@ -389,9 +397,17 @@ static k3d_status validate(const k3d_scene* s) {
       (s->n_dreiecke && (!s->dreiecke || !s->ruhe_inv || !chk(s->dreiecke, 3 * s->n_dreiecke))))
     return K3D_BAD_ARGUMENT;
   if (s->n_teile < 0 || (s->n_teile && (!s->teil_bereiche || !s->teil_dehnung))) return K3D_BAD_ARGUMENT;
+  if (s->n_instanzen < 0 || (s->n_instanzen > 1 && !s->instanz_punkte)) return K3D_BAD_ARGUMENT;
+  if (s->n_instanzen > 1) {
+    const int64_t* o = s->instanz_punkte;
+    if (o[0] != 0 || o[s->n_instanzen] != n) return K3D_BAD_ARGUMENT;
+    for (int64_t k = 0; k < s->n_instanzen; ++k)
+      if (o[k + 1] <= o[k]) return K3D_BAD_ARGUMENT;
+  }
   if (s->n_koerper < 0 || s->n_koerper > kMaxBodies || (s->n_koerper && !s->koerper)) return K3D_BAD_ARGUMENT;
   for (int b = 0; b < s->n_koerper; ++b) {
     const k3d_body& k = s->koerper[b];
+    if (k.instanz < -1 || (s->n_instanzen > 1 && k.instanz >= s->n_instanzen)) return K3D_BAD_ARGUMENT;
     if (k.art == K3D_BODY_SDF_GRID) {
       if (!k.sdf || k.dims[0] < 2 || k.dims[1] < 2 || k.dims[2] < 2 || !(k.spacing > 0.0)) return K3D_BAD_ARGUMENT;
     } else if (k.art != K3D_BODY_CYLINDER) {
@@ -411,26 +427,71 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
   const int64_t n = s->n_punkte, nt = s->n_membran, nb = s->n_biegung;
   const size_t R = h->rsize;
 
-  // springs: pattern edges that carry their own stiffness, then seams (implizit.rs:725-772)
+  // instances (independent drapes of a batch): point offsets, and every
+  // element group's range per instance (the groups list instance by instance)
+  const int ng = s->n_instanzen > 1 ? int(s->n_instanzen) : 1;
+  if (ng > h->blocks) return fail(h, K3D_BAD_ARGUMENT, "more instances than blocks of the PCG launch");
+  if (ng > 1 && h->p.selbstkollision)
+    return fail(h, K3D_BAD_ARGUMENT, "self-collision is not supported in a batch scene");
+  std::vector<int64_t> io(ng + 1, 0);
+  for (int k = 0; k <= ng; ++k) io[k] = ng > 1 ? s->instanz_punkte[k] : (k == 0 ? 0 : n);
+  std::vector<uint32_t> pinst(ng > 1 ? n : 0);
+  for (int k = 0; k < ng && ng > 1; ++k)
+    for (int64_t i = io[k]; i < io[k + 1]; ++i) pinst[i] = uint32_t(k);
+  auto inst_of = [&](uint32_t p) -> int { return ng > 1 ? int(pinst[p]) : 0; };
+  // element ranges: [lo, hi) per instance; false if an element spans two
+  // instances or the group is not ordered by instance
+  auto ranges = [&](const uint32_t* pts, int64_t cnt, int w, std::vector<int64_t>& lo, std::vector<int64_t>& hi) {
+    lo.assign(ng, 0);
+    hi.assign(ng, 0);
+    int prev = 0;
+    for (int64_t e = 0; e < cnt; ++e) {
+      const int k = inst_of(pts[w * e]);
+      for (int q = 1; q < w; ++q)
+        if (inst_of(pts[w * e + q]) != k) return false;
+      if (k < prev) return false;
+      prev = k;
+    }
+    int64_t e = 0;
+    for (int k = 0; k < ng; ++k) {
+      lo[k] = e;
+      while (e < cnt && inst_of(pts[w * e]) == k) ++e;
+      hi[k] = e;
+    }
+    return true;
+  };
+  std::vector<int64_t> t_lo, t_hi, b_lo, b_hi, a_lo, a_hi, n_lo, n_hi;
+  if (!ranges(s->membran_punkte, nt, 3, t_lo, t_hi) || !ranges(s->biegung_punkte, nb, 4, b_lo, b_hi) ||
+      !ranges(s->abstand_punkte, s->n_abstand, 2, a_lo, a_hi) || !ranges(s->naht_punkte, s->n_naht, 2, n_lo, n_hi))
+    return fail(h, K3D_BAD_ARGUMENT, "an element spans two instances, or a group is not ordered by instance");
+
+  // springs: pattern edges that carry their own stiffness, then seams
+  // (implizit.rs:725-772), instance by instance
   std::vector<uint4> s_idx;
   std::vector<double2> s_kl;
-  for (int64_t e = 0; e < s->n_abstand; ++e) {
-    const bool membran = s->membran_kante && s->membran_kante[e];
-    if (membran) continue;
-    double k = 1.0 / s->abstand_nachgiebigkeit[e];
-    if (k == 0.0) continue;
-    s_idx.push_back(make_uint4(s->abstand_punkte[2 * e], s->abstand_punkte[2 * e + 1], 0u, 0u));
-    s_kl.push_back(make_double2(k, s->abstand_ruhe[e]));
-  }
+  std::vector<int64_t> s_lo(ng), s_hi(ng);
   h->seam_slot.assign(size_t(s->n_naht), -1);
-  if (h->p.naht_k != 0.0) {
-    for (int64_t e = 0; e < s->n_naht; ++e) {
-      h->seam_slot[e] = int64_t(s_idx.size());
-      s_idx.push_back(make_uint4(s->naht_punkte[2 * e], s->naht_punkte[2 * e + 1], 1u, 0u));
-      s_kl.push_back(make_double2(h->p.naht_k, s->naht_ruhe[e]));
+  for (int k = 0; k < ng; ++k) {
+    s_lo[k] = int64_t(s_idx.size());
+    for (int64_t e = a_lo[k]; e < a_hi[k]; ++e) {
+      const bool membran = s->membran_kante && s->membran_kante[e];
+      if (membran) continue;
+      double kk = 1.0 / s->abstand_nachgiebigkeit[e];
+      if (kk == 0.0) continue;
+      s_idx.push_back(make_uint4(s->abstand_punkte[2 * e], s->abstand_punkte[2 * e + 1], 0u, 0u));
+      s_kl.push_back(make_double2(kk, s->abstand_ruhe[e]));
     }
+    if (h->p.naht_k != 0.0) {
+      for (int64_t e = n_lo[k]; e < n_hi[k]; ++e) {
+        h->seam_slot[e] = int64_t(s_idx.size());
+        s_idx.push_back(make_uint4(s->naht_punkte[2 * e], s->naht_punkte[2 * e + 1], 1u, 0u));
+        s_kl.push_back(make_double2(h->p.naht_k, s->naht_ruhe[e]));
+      }
+    }
+    s_hi[k] = int64_t(s_idx.size());
   }
   const int64_t ns = int64_t(s_idx.size());
+  h->n_grp = ng;
   h->s_kl_host = s_kl;
 
   // point -> element corner lists, in element order
@@ -597,11 +658,57 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
   K3D_CUDA(h, up(cv.s_idx, s_idx.data(), 16 * S));
   K3D_CUDA(h, up(cv.s_kl, s_kl.data(), 16 * S));
 
+  // groups of the PCG launch: blocks in proportion to the instances' points
+  // (at least one each, largest remainders), points and elements per group
+  {
+    const int B = h->blocks;
+    std::vector<int> nbk(ng, 1);
+    int left = B - ng;
+    std::vector<std::pair<double, int>> rem;
+    for (int k = 0; k < ng; ++k) {
+      const double share = double(left) * double(io[k + 1] - io[k]) / double(std::max<int64_t>(n, 1));
+      const int whole = int(share);
+      nbk[k] += whole;
+      rem.push_back({share - double(whole), k});
+    }
+    int used = 0;
+    for (int k = 0; k < ng; ++k) used += nbk[k];
+    std::sort(rem.begin(), rem.end(), [](const auto& x, const auto& y) { return x.first > y.first || (x.first == y.first && x.second < y.second); });
+    for (size_t q = 0; used < B; ++q, ++used) nbk[rem[q % rem.size()].second] += 1;
+    std::vector<Grp> grp(ng);
+    std::vector<uint32_t> blk(B);
+    unsigned first = 0;
+    for (int k = 0; k < ng; ++k) {
+      Grp& g = grp[k];
+      g.r0 = io[k];
+      g.r1 = io[k + 1];
+      g.t0 = t_lo[k];
+      g.t1 = t_hi[k];
+      g.b0 = b_lo[k];
+      g.b1 = b_hi[k];
+      g.s0 = s_lo[k];
+      g.s1 = s_hi[k];
+      g.first_blk = first;
+      g.nblk = unsigned(nbk[k]);
+      double msum = 0.0;
+      for (int64_t i = io[k]; i < io[k + 1]; ++i) msum += s->masse[i];
+      g.boden = msum * 1e-18;
+      g.count = a.grp_cnt + 32 * size_t(k);
+      g.partials = a.partials + 8 * size_t(first);
+      for (int q = 0; q < nbk[k]; ++q) blk[first + q] = uint32_t(k);
+      first += unsigned(nbk[k]);
+    }
+    K3D_CUDA(h, up(cv.grp, grp.data(), sizeof(Grp) * grp.size()));
+    K3D_CUDA(h, up(cv.blk_grp, blk.data(), 4 * blk.size()));
+    if (cv.pinst) K3D_CUDA(h, up(cv.pinst, pinst.data(), 4 * pinst.size()));
+  }
+
   // bodies; SDF grids go to the device once here
   h->bodies.assign(s->koerper, s->koerper + s->n_koerper);
   for (int b = 0; b < s->n_koerper; ++b) {
     const k3d_body& k = s->koerper[b];
     void* d = nullptr;
+    if (k.instanz < -1 || (s->n_instanzen > 1 && k.instanz >= s->n_instanzen)) return K3D_BAD_ARGUMENT;
     if (k.art == K3D_BODY_SDF_GRID) {
       size_t cnt = size_t(k.dims[0]) * k.dims[1] * k.dims[2];
       K3D_CUDA(h, cudaMalloc(&d, 4 * cnt));
@@ -664,6 +771,7 @@ static k3d_status launch(k3d_solver* h, int mode, double t_bodies, bool need_loa
     d.radius = k.radius;
     d.spacing = k.spacing;
     d.sdf = static_cast<const float*>(h->sdf_dev[b]);
+    d.inst = h->n_grp > 1 ? k.instanz : -1;
   }
   int launched = 0;
   if (h->sc.on) {  // proximity pairs and springs before the system (implizit.rs:668-691)

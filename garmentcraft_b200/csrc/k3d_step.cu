@@ -58,7 +58,15 @@ struct Shared {
   unsigned epoch;  // barriers passed in this launch
   unsigned rbuf;   // reductions done in this launch (partials buffer parity)
   int err;
+  Grp g;           // this block's group (instance)
+  unsigned bidx;   // this block's index within the group
 };
+
+// Loops of the PCG over the group's points and element ranges, strided over
+// the group's blocks (for a scene of one drape: the whole grid).
+#define GRP_FOR(i, lo, hi)                                                                         \
+  for (int64_t i = (lo) + int64_t(sh.bidx) * blockDim.x + threadIdx.x; i < (hi); \
+       i += int64_t(sh.g.nblk) * blockDim.x)
 
 __device__ __forceinline__ unsigned atom_add_release(unsigned* p, unsigned v) {
   unsigned old;
@@ -107,6 +115,7 @@ template <int NV>
 __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV : 1]) {
   SyncState* s = a.sync;
   const unsigned buf = sh.rbuf & 1u;
+  const unsigned nb = sh.g.nblk;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if constexpr (NV > 0) {
 #pragma unroll
@@ -125,15 +134,15 @@ __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV
       for (int k = 0; k < NV; ++k) {
         double t = 0.0;
         for (int w = 0; w < nw; ++w) t += sh.red[k][w];
-        a.partials[(buf * kMaxRed + k) * gridDim.x + blockIdx.x] = t;
+        sh.g.partials[(buf * kMaxRed + k) * nb + sh.bidx] = t;
       }
       sh.rbuf += 1;  // every thread read the parity at entry, before the barrier above
     }
-    const unsigned target = (sh.epoch + 1) * gridDim.x;
-    atom_add_release(&s->count, 1u);
+    const unsigned target = (sh.epoch + 1) * nb;
+    atom_add_release(sh.g.count, 1u);
     const uint64_t t0 = globaltimer();
     int err = 0;
-    while (int(ld_acquire_u32(&s->count) - target) < 0) {
+    while (int(ld_acquire_u32(sh.g.count) - target) < 0) {
       if ((err = ld_relaxed_i32(&s->error)) != 0) break;
       if (globaltimer() - t0 > kBarrierLimitNs) {
         atomicCAS(&s->error, 0, K3D_STATUS_TIMEOUT);
@@ -153,7 +162,7 @@ __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV
 #pragma unroll
       for (int k = 0; k < NV; ++k) {
         double x = 0.0;
-        for (unsigned b = lane; b < gridDim.x; b += 32) x += __ldcg(&a.partials[(buf * kMaxRed + k) * gridDim.x + b]);
+        for (unsigned b = lane; b < nb; b += 32) x += __ldcg(&sh.g.partials[(buf * kMaxRed + k) * nb + b]);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
         if (lane == 0) sh.res[k] = x;
@@ -166,27 +175,13 @@ __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV
   return true;
 }
 
-// Grid-wide maximum of one non-negative double (bit pattern order equals
-// value order for non-negative doubles, so an integer atomicMax is exact).
-__device__ bool grid_max(const StepArgs& a, Shared& sh, double (&v)[1]) {
-  double x = v[0];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
-  if ((threadIdx.x & 31) == 0 && x > 0.0)
-    atomicMax(reinterpret_cast<unsigned long long*>(&a.stat_rest_max[1]), (unsigned long long)__double_as_longlong(x));
-  double none[1] = {0.0};
-  if (!grid_sync<0>(a, sh, none)) return false;
-  v[0] = __longlong_as_double((long long)__ldcg(reinterpret_cast<const unsigned long long*>(&a.stat_rest_max[1])));
-  return true;
-}
-
 __device__ __forceinline__ bool barrier(const StepArgs& a, Shared& sh) {
   double none[1] = {0.0};
   return grid_sync<0>(a, sh, none);
 }
 
 
-__device__ __noinline__ void apply_dv64(const StepArgs& a) {
+__device__ __noinline__ void apply_dv64(const StepArgs& a, const Shared& sh) {
   const R4<double>* f1w = static_cast<const R4<double>*>(a.m_f1w64);
   const R4<double>* f2w = static_cast<const R4<double>*>(a.m_f2w64);
   const R4<double>* kgB = static_cast<const R4<double>*>(a.m_kgB64);
@@ -200,7 +195,7 @@ __device__ __noinline__ void apply_dv64(const StepArgs& a) {
     const D3 d = ld3(a.dv, i);
     return {d.x, d.y, d.z, 0.0};
   };
-  K3D_FOR(t, a.nt) {
+  GRP_FOR(t, sh.g.t0, sh.g.t1) {
     const uint4 id = __ldg(&a.m_idx[t]);
     const uint4 ps = __ldg(&a.m_pos[t]);
     const R4<double> d[3] = {dvp(id.x), dvp(id.y), dvp(id.z)};
@@ -210,7 +205,7 @@ __device__ __noinline__ void apply_dv64(const StepArgs& a) {
     slot[ps.y] = out[1];
     slot[ps.z] = out[2];
   }
-  K3D_FOR(b, a.nb) {
+  GRP_FOR(b, sh.g.b0, sh.g.b1) {
     const uint4 id = __ldg(&a.b_idx[b]);
     const uint4 ps = __ldg(&a.b_pos[b]);
     const R4<double> g0 = grad[4 * b], g1 = grad[4 * b + 1], g2 = grad[4 * b + 2], g3 = grad[4 * b + 3];
@@ -224,7 +219,7 @@ __device__ __noinline__ void apply_dv64(const StepArgs& a) {
     slot[ps.z] = {g2.x * sc, g2.y * sc, g2.z * sc, 0.0};
     slot[ps.w] = {g3.x * sc, g3.y * sc, g3.z * sc, 0.0};
   }
-  K3D_FOR(s, a.ns) {
+  GRP_FOR(s, sh.g.s0, sh.g.s1) {
     const uint4 id = __ldg(&a.s_idx[s]);
     const uint2 ps = __ldg(&a.s_pos[s]);
     const R4<double> dq = sdq[s];
@@ -266,8 +261,8 @@ __device__ __noinline__ D3 a_dv64(const StepArgs& a, int64_t i) {
 // consecutive points).
 
 template <typename R>
-__device__ void dv_to_w(const StepArgs& a, const View<R>& vw) {
-  K3D_FOR(i, a.n) {
+__device__ void dv_to_w(const StepArgs& a, const View<R>& vw, const Shared& sh) {
+  GRP_FOR(i, sh.g.r0, sh.g.r1) {
     const D3 d = ld3(a.dv, uint32_t(i));
     vw.cw[i].w = {R(d.x), R(d.y), R(d.z), R(0)};
     vw.cw[i].c = {R(0), R(0), R(0), R(0)};
@@ -337,7 +332,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
   CW<R>* nxt = static_cast<CW<R>*>(a.cw2);
   const bool hi = a.m_f1w64 != nullptr;
   // start: pinned points 0, held points get their normal target
-  K3D_FOR(i, a.n) {
+  GRP_FOR(i, sh.g.r0, sh.g.r1) {
     D3 d = ld3(a.dv, uint32_t(i));
     if (!a.frei[i]) {
       d = d3(0, 0, 0);
@@ -354,11 +349,11 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
   }
   if (!barrier(a, sh)) return false;
   if (hi) {
-    apply_dv64(a);
+    apply_dv64(a, sh);
     if (!barrier(a, sh)) return false;
   }
   double red[2] = {0.0, 0.0};
-  K3D_FOR(i, a.n) {
+  GRP_FOR(i, sh.g.r0, sh.g.r1) {
     R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, cx = 0, cy = 0, cz = 0;
     if (a.frei[i]) {
       const D3 b = ld3(a.b, uint32_t(i));
@@ -403,7 +398,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
   double delta = red[0];
   const double bb = red[1];
   const double tol = sizeof(R) == 4 ? fmax(a.tol, kMixedTolFloor) : a.tol;
-  const double ziel = fmax(tol * tol * fmax(bb, delta), a.boden);
+  const double ziel = fmax(tol * tol * fmax(bb, delta), sh.g.boden);
   int64_t it = 0;
   double beta = 0.0, delta_ref = delta;
   breakdown = false;
@@ -414,7 +409,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     // that falls far below it has lost the direction and the solve stops
     // there as at a breakdown (the FP64 form keeps the reference's test only).
     double ca[2] = {0.0, 0.0};
-    K3D_FOR(i, a.n) {
+    GRP_FOR(i, sh.g.r0, sh.g.r1) {
       const R4<R> ci = next_dir<R>(cur[i], rb);
       nxt[i].c = ci;
       R ax = 0, ay = 0, az = 0;
@@ -444,7 +439,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     }
     const double alpha = delta / ca[0];
     double rzs[1] = {0.0};
-    K3D_FOR(i, a.n) {
+    GRP_FOR(i, sh.g.r0, sh.g.r1) {
       const R4<R> ci = nxt[i].c;
       D3 d = ld3(a.dv, uint32_t(i));
       d = d + d3(double(ci.x), double(ci.y), double(ci.z)) * alpha;
@@ -472,10 +467,10 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       // S (b - A dv) with the FP64 operator; restart the direction if the
       // residual grew
       const bool restart = delta > kGrow * delta_ref;
-      apply_dv64(a);
+      apply_dv64(a, sh);
       if (!barrier(a, sh)) return false;
       double rz2[1] = {0.0};
-      K3D_FOR(i, a.n) {
+      GRP_FOR(i, sh.g.r0, sh.g.r1) {
         R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, wx = 0, wy = 0, wz = 0;
         if (a.frei[i]) {
           const D3 n = ld3(a.nrm_d, uint32_t(i));
@@ -511,7 +506,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
   }
   iters = it;
   unconverged = delta > ziel;
-  rest = sqrt(delta / fmax(bb, a.boden));
+  rest = sqrt(delta / fmax(bb, sh.g.boden));
   return true;
 }
 
@@ -522,12 +517,12 @@ template <typename R, bool SC>
 __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double& released) {
   const bool hi = a.m_f1w64 != nullptr;
   if (hi)
-    apply_dv64(a);
+    apply_dv64(a, sh);
   else
-    dv_to_w<R>(a, vw);
+    dv_to_w<R>(a, vw, sh);
   if (!barrier(a, sh)) return false;
   double cnt[1] = {0.0};
-  K3D_FOR(i, a.n) {
+  GRP_FOR(i, sh.g.r0, sh.g.r1) {
     const D3 n = ld3(a.nrm_d, uint32_t(i));
     if (n.x == 0.0 && n.y == 0.0 && n.z == 0.0) continue;
     const D3 b = ld3(a.b, uint32_t(i));
@@ -561,10 +556,12 @@ __global__ void __launch_bounds__(kSolveBlock, 1) solve_kernel(const __grid_cons
     sh.epoch = 0;
     sh.rbuf = 0;
     sh.err = 0;
+    sh.g = a.grp[a.blk_grp[blockIdx.x]];
+    sh.bidx = blockIdx.x - sh.g.first_blk;
   }
   __syncthreads();
   const View<R> vw(a);
-  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  const bool lead = sh.bidx == 0 && threadIdx.x == 0;  // one thread per group
   const bool any_held = a.stats[ST_HELD] > 0;
   int64_t iters = 0;
   bool unconv = false, brk = false;
@@ -572,24 +569,33 @@ __global__ void __launch_bounds__(kSolveBlock, 1) solve_kernel(const __grid_cons
   for (int pass = 0; pass < 2; ++pass) {
     if (!pcg<R, SC>(a, vw, sh, iters, unconv, brk, rest)) return;
     double dvm[1] = {0.0};
-    K3D_FOR(i, a.n) {
+    GRP_FOR(i, sh.g.r0, sh.g.r1) {
       const D3 d = ld3(a.dv, uint32_t(i));
       dvm[0] = fmax(dvm[0], fmax(fabs(d.x), fmax(fabs(d.y), fabs(d.z))));
     }
-    if (!grid_max(a, sh, dvm)) return;
+    // |dv| maximum and the counters go to the statistics by atomics (the
+    // groups of a batch finish at different times)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dvm[0] = fmax(dvm[0], __shfl_xor_sync(0xffffffffu, dvm[0], o));
+    if ((threadIdx.x & 31) == 0 && dvm[0] > 0.0)
+      atomicMax(reinterpret_cast<unsigned long long*>(&a.stat_rest_max[1]),
+                (unsigned long long)__double_as_longlong(dvm[0]));
     if (lead) {
-      a.stats[ST_CG_ITERATIONS] += iters;
-      a.stats[ST_SOLVES] += 1;
-      if (unconv) a.stats[ST_UNCONVERGED] += 1;
-      if (brk) a.stats[ST_BREAKDOWNS] += 1;
-      a.stat_rest_max[0] = fmax(a.stat_rest_max[0], rest);
-      a.stats[ST_LAST_ITERATIONS] = iters;
+      atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[ST_CG_ITERATIONS]), (unsigned long long)iters);
+      atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[ST_SOLVES]), 1ull);
+      if (unconv) atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[ST_UNCONVERGED]), 1ull);
+      if (brk) atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[ST_BREAKDOWNS]), 1ull);
+      if (rest > 0.0)
+        atomicMax(reinterpret_cast<unsigned long long*>(&a.stat_rest_max[0]),
+                  (unsigned long long)__double_as_longlong(rest));
+      if (sh.g.first_blk == 0) a.stats[ST_LAST_ITERATIONS] = iters;
     }
     if (a.mode == MODE_SOLVE) return;
     if (!any_held) break;
     double rel = 0.0;
     if (!release<R, SC>(a, vw, sh, rel)) return;
-    if (lead) a.stats[ST_RELEASED] += int64_t(rel);
+    if (lead && rel > 0.0)
+      atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[ST_RELEASED]), (unsigned long long)rel);
     if (rel == 0.0) break;
   }
 }
@@ -639,7 +645,7 @@ static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int&
   cudaError_t e;
   const BuildKernels K = build_kernels(sizeof(R) == 8 ? 0 : 1);
   const int64_t elems = a.nt > a.nb ? (a.nt > a.ns ? a.nt : a.ns) : (a.nb > a.ns ? a.nb : a.ns);
-  if ((e = cudaMemsetAsync(&a.sync->count, 0, sizeof(unsigned), st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(a.grp_cnt, 0, sizeof(unsigned) * 32 * size_t(a.n_grp), st)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(&a.stats[ST_HELD], 0, sizeof(long long), st)) != cudaSuccess) return e;
   if ((e = plain(K.elements, a, elems, st)) != cudaSuccess) return e;
   if ((e = plain(K.points, a, a.n, st)) != cudaSuccess) return e;

@@ -36,6 +36,18 @@ struct SyncState {
   int pad1[31];
 };
 
+// One instance of a batch (an independent drape) and the group of blocks of
+// the PCG launch that solves it: its points, elements, barrier counter and
+// reduction partials. A scene of one drape is one group over all blocks.
+struct Grp {
+  int64_t r0, r1;                  // points
+  int64_t t0, t1, b0, b1, s0, s1;  // membranes, bends, springs
+  unsigned first_blk, nblk;
+  double boden;       // convergence floor: 1e-18 of the instance's mass (implizit.rs:390-391)
+  unsigned* count;    // barrier arrivals (zeroed before each launch)
+  double* partials;   // 2 * kMaxRed per block of the group
+};
+
 struct StepArgs {
   int64_t n, nt, nb, ns;
   int mode, first_step, need_load, normal_aus_last;
@@ -95,6 +107,13 @@ struct StepArgs {
   // probes
   const double* p_in;
   double* p_out;
+  // instances (independent drapes): per point its instance (null for one),
+  // the groups of the PCG launch and each block's group
+  const uint32_t* pinst;
+  const Grp* grp;
+  const uint32_t* blk_grp;
+  unsigned* grp_cnt;  // the groups' counters, 32 words apart
+  int n_grp;
   // bookkeeping
   cudaEvent_t ev_solve0, ev_solve1;  // around the PCG launch (host-side handles)
   SyncState* sync;

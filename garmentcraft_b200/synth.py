@@ -266,6 +266,7 @@ def body_to_c(body: dict) -> _abi.K3dBody:
         kb.ursprung[a] = body.get("ursprung", (0.0, 0.0, 0.0))[a]
     kb.radius = body.get("radius", 0.0)
     kb.spacing = body.get("spacing", 1.0)
+    kb.instanz = int(body.get("instanz", -1))
     sdf = body.get("sdf")
     kb.sdf = _abi.ptr(sdf, C.c_float) if sdf is not None else None
     return kb

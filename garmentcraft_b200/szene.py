@@ -75,6 +75,8 @@ class Szene:
     teil_bereiche: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), dtype=np.int64))
     teil_dehnung: np.ndarray = field(default_factory=lambda: np.zeros(0))
     teil_band_von: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int32))
+    # batch of independent drapes: n_instanzen + 1 point offsets (empty: one drape)
+    instanz_punkte: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int64))
     koerper: list = field(default_factory=list)
     param: Simparameter = field(default_factory=Simparameter)
     zeit: float = 0.0
@@ -104,7 +106,46 @@ class Szene:
 
     def copy(self) -> "Szene":
         kw = {name: getattr(self, name).copy() for name in _ARRAYS}
-        return Szene(**kw, koerper=list(self.koerper), param=self.param, zeit=self.zeit)
+        return Szene(**kw, instanz_punkte=self.instanz_punkte.copy(), koerper=list(self.koerper),
+                     param=self.param, zeit=self.zeit)
+
+    @classmethod
+    def verbinden(cls, szenen: list) -> "Szene":
+        """A batch scene of independent drapes: the scenes' points, elements and
+        parts one after another (each element group instance by instance),
+        bodies tagged with their instance. All scenes share one frame length
+        and substep count; the first scene's Simparameter apply."""
+        off = 0
+        tri_off = 0
+        parts = {name: [] for name in _ARRAYS}
+        koerper = []
+        io = [0]
+        for k, s in enumerate(szenen):
+            for name, (dt, cols) in _ARRAYS.items():
+                a = np.asarray(getattr(s, name))
+                if name in ("abstand_punkte", "naht_punkte", "biegung_punkte", "membran_punkte", "dreiecke"):
+                    a = a.astype(np.uint32) + np.uint32(off)
+                elif name == "teil_bereiche":
+                    a = a.astype(np.int64) + np.array([off, off, tri_off, tri_off], dtype=np.int64)
+                parts[name].append(a)
+            for b in s.koerper:
+                d = dict(b)
+                d["instanz"] = k
+                koerper.append(d)
+            off += s.n
+            tri_off += s.dreiecke.shape[0]
+            io.append(off)
+        kw = {}
+        for name, (dt, cols) in _ARRAYS.items():
+            kw[name] = np.ascontiguousarray(np.concatenate(parts[name], axis=0), dtype=dt)
+        return cls(**kw, instanz_punkte=np.array(io, dtype=np.int64), koerper=koerper,
+                   param=szenen[0].param, zeit=szenen[0].zeit)
+
+    def instanz(self, k: int):
+        """Point slice of instance k of a batch scene."""
+        if self.instanz_punkte.shape[0] == 0:
+            return slice(0, self.n)
+        return slice(int(self.instanz_punkte[k]), int(self.instanz_punkte[k + 1]))
 
     def to_c(self):
         """(k3d_scene, keepalive). x and v point at this scene's own arrays, so
@@ -121,6 +162,9 @@ class Szene:
         s.n_membran = self.membran_punkte.shape[0]
         s.n_dreiecke = self.dreiecke.shape[0]
         s.n_teile = self.teil_dehnung.shape[0]
+        self.instanz_punkte = np.ascontiguousarray(self.instanz_punkte, dtype=np.int64)
+        s.n_instanzen = max(self.instanz_punkte.shape[0] - 1, 0)
+        s.instanz_punkte = _abi.ptr(self.instanz_punkte, C.c_int64) if s.n_instanzen > 0 else None
         for name, (dt, _) in _ARRAYS.items():
             setattr(s, name, _abi.ptr(getattr(self, name), _CTYPE[dt]))
         bodies = (_abi.K3dBody * max(len(self.koerper), 1))()

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define K3D_ABI_VERSION 2
+#define K3D_ABI_VERSION 3
 
 /* Status of a call. Unconverged CG is data (k3d_cg_result), not an error,
  * as in CgLauf (sim/src/implizit.rs:294-299). */
@@ -82,6 +82,8 @@ typedef struct k3d_body {
   double ursprung[3];       /* grid: position of node (0,0,0) relative to punkt */
   double spacing;           /* grid: node spacing m */
   const float* sdf;         /* grid: dims[0]*dims[1]*dims[2] values, x fastest (host) */
+  int32_t instanz;          /* the instance it acts on in a batch scene, -1 = every instance */
+  int32_t pad;
 } k3d_body;
 
 /* Szene (sim/src/szene.rs:198-269): the arrays the implicit step reads or
@@ -130,6 +132,15 @@ typedef struct k3d_scene {
   const int64_t* teil_bereiche;  /* 4 per part: first point, end point, first triangle, end triangle */
   const double* teil_dehnung;    /* per part: the material's dehnung_n_m, N/m */
   const int32_t* teil_band_von;  /* per part: carrier part of a folded allowance band, -1 = none; may be null */
+  /* Batch of independent drapes (no counterpart in the reference, which steps
+   * one scene at a time). n_instanzen <= 1: one drape. Otherwise instance k
+   * owns points [instanz_punkte[k], instanz_punkte[k + 1]); every element
+   * lies within one instance, and each element group (abstand, naht, biegung,
+   * membran) lists its elements instance by instance. The instances share one
+   * PCG launch, each with its own blocks, reductions and convergence; bodies
+   * act on the instance named in k3d_body.instanz. */
+  int64_t n_instanzen;
+  const int64_t* instanz_punkte;  /* n_instanzen + 1 point offsets, ascending from 0 to n_punkte */
 } k3d_scene;
 
 /* ImplizitStatistik (sim/src/implizit.rs:535-561), field for field. */
