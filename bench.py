@@ -71,7 +71,64 @@ def args_():
     p.add_argument("--capture", type=int, default=0,
                    help="profiling case: run this many mixed-form steps of the drop on cuda:0 and exit")
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="form used by --capture")
+    p.add_argument("--no-batch", action="store_true", help="skip the batched-drape comparison")
+    p.add_argument("--batch-steps", type=int, default=5)
     return p.parse_args()
+
+
+BATCH_PRE = 15  # free-fall steps of the batched drapes (0.1 m drop) before the timed window
+
+
+def batch_leg(steps, flush, torch):
+    """Batched drapes: 64 sheets of 2k-60k vertices (log-uniform), aspect
+    1:1 to 1:3, per-instance materials, each over its own sphere or capsule
+    SDF (64^3). The same window (steps BATCH_PRE .. BATCH_PRE + steps) timed
+    as one batch scene (one launch per kernel for all 64) and as 64 solvers
+    run one after another (the per-instance launches), mixed form; the batch
+    also in FP64. Device time per step with CUDA events, L2 flushed first."""
+    from garmentcraft_b200 import _abi, synth
+    from garmentcraft_b200.implizit import ImplizitCg, build_scene
+    from garmentcraft_b200.params import ImplizitParameter
+    from garmentcraft_b200.szene import Szene
+    scenes = [build_scene(m, [b]) for m, b in synth.drape_batch(64)]
+    nv = sum(s.n for s in scenes)
+
+    def timed(cg, k):
+        ms, its = 0.0, 0
+        for _ in range(k):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            st = cg.bilder_auf_geraet(1)
+            ms += cg.letzte_bild_ms()
+            its += st.cg_iterationen
+        return ms, its
+
+    out = {"workload": "64 sheets, 2k-60k vertices log-uniform, aspect U(1,3), sphere or capsule SDF 64^3 each",
+           "vertices": nv, "instances": len(scenes), "window": f"steps {BATCH_PRE}-{BATCH_PRE + steps} of the drop"}
+    for prec, name in ((_abi.K3D_MIXED, "mixed"), (_abi.K3D_FP64, "fp64")):
+        par = ImplizitParameter(schritte_je_bild=1, cg_max=CG_MAX, precision=prec)
+        cg = ImplizitCg(par)
+        cg.zustand_hochladen(Szene.verbinden([s.copy() for s in scenes]))
+        cg.bilder_auf_geraet(BATCH_PRE)
+        ms, its = timed(cg, steps)
+        out[f"batched_{name}"] = {"value": nv * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+                                  "cg_iterations_per_step": its / steps}
+        del cg
+    par = ImplizitParameter(schritte_je_bild=1, cg_max=CG_MAX, precision=_abi.K3D_MIXED)
+    ms_all, its_all = 0.0, 0
+    for s in scenes:
+        c = ImplizitCg(par)
+        c.zustand_hochladen(s.copy())
+        c.bilder_auf_geraet(BATCH_PRE)
+        ms, its = timed(c, steps)
+        ms_all += ms
+        its_all += its
+        del c
+    out["per_instance_mixed"] = {"value": nv * steps / (ms_all * 1e-3), "ms_per_step": ms_all / steps,
+                                 "cg_iterations_per_step": its_all / steps}
+    out["batched_vs_per_instance"] = out["batched_mixed"]["value"] / out["per_instance_mixed"]["value"]
+    out["unit"] = UNIT
+    return out
 
 
 def workload_config(n, s, extra=None):
@@ -372,6 +429,8 @@ def main():
             "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
             "cg_iterations_per_step": its / a.steps, "clocks": clk}
     line.update(extra)
+    if world == 1 and not a.no_batch:
+        line["batched"] = batch_leg(a.batch_steps, flush, torch)
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_leg(a.n, a.warmup, a.cpu_seconds)
     if rank == 0:

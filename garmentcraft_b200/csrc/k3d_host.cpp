@@ -658,15 +658,26 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
   K3D_CUDA(h, up(cv.s_idx, s_idx.data(), 16 * S));
   K3D_CUDA(h, up(cv.s_kl, s_kl.data(), 16 * S));
 
-  // groups of the PCG launch: blocks in proportion to the instances' points
-  // (at least one each, largest remainders), points and elements per group
+  // groups of the PCG launch: blocks in proportion to the instances' work
+  // (at least one each, largest remainders), points and elements per group.
+  // An instance's PCG work per step grows as its points times its iteration
+  // count, and the iteration count of a 2D mesh grows as the square root of
+  // its points (the condition number grows as the mesh width squared), so
+  // the weight is points^1.5.
   {
     const int B = h->blocks;
     std::vector<int> nbk(ng, 1);
     int left = B - ng;
     std::vector<std::pair<double, int>> rem;
+    std::vector<double> wk(ng);
+    double wsum = 0.0;
     for (int k = 0; k < ng; ++k) {
-      const double share = double(left) * double(io[k + 1] - io[k]) / double(std::max<int64_t>(n, 1));
+      const double pts = double(io[k + 1] - io[k]);
+      wk[k] = pts * std::sqrt(pts);
+      wsum += wk[k];
+    }
+    for (int k = 0; k < ng; ++k) {
+      const double share = double(left) * wk[k] / std::max(wsum, 1e-300);
       const int whole = int(share);
       nbk[k] += whole;
       rem.push_back({share - double(whole), k});

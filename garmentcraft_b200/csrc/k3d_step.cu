@@ -409,6 +409,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     // that falls far below it has lost the direction and the solve stops
     // there as at a breakdown (the FP64 form keeps the reference's test only).
     double ca[2] = {0.0, 0.0};
+#pragma unroll 2
     GRP_FOR(i, sh.g.r0, sh.g.r1) {
       const R4<R> ci = next_dir<R>(cur[i], rb);
       nxt[i].c = ci;
@@ -439,6 +440,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     }
     const double alpha = delta / ca[0];
     double rzs[1] = {0.0};
+#pragma unroll 2
     GRP_FOR(i, sh.g.r0, sh.g.r1) {
       const R4<R> ci = nxt[i].c;
       D3 d = ld3(a.dv, uint32_t(i));

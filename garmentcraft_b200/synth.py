@@ -222,6 +222,70 @@ def sheet_over_sphere(n: int = 257, groesse_m: float = 1.0, jitter_mm: float = 1
     return Muster([teil], [], param), body
 
 
+# ------------------------------------------------------------------ batched drapes
+def capsule_sdf_grid(radius_m: float, halbe_laenge_m: float, n: int, zentrum=(0.0, 0.0, 0.0)):
+    """Signed distance of a capsule (segment along x of half length
+    ``halbe_laenge_m``, radius ``radius_m``) sampled on an n^3 grid that holds
+    it with a margin. Returns a body dict for a K3D_BODY_SDF_GRID."""
+    ausdehnung = 2.0 * (halbe_laenge_m + radius_m) * 1.2
+    spacing = ausdehnung / (n - 1)
+    half = 0.5 * (n - 1) * spacing
+    ax = np.arange(n, dtype=np.float64) * spacing - half
+    gz, gy, gx = np.meshgrid(ax, ax, ax, indexing="ij")
+    px = np.clip(gx, -halbe_laenge_m, halbe_laenge_m)
+    d = np.sqrt((gx - px) ** 2 + gy * gy + gz * gz) - radius_m
+    return dict(art=_abi.K3D_BODY_SDF_GRID, punkt=tuple(zentrum), dims=(n, n, n),
+                ursprung=(-half, -half, -half), spacing=spacing, sdf=np.ascontiguousarray(d.astype(np.float32)))
+
+
+def drape(nx: int, ny: int, kante_m: float, material: Material, winkel: float, body: dict, fall_m: float,
+          koerper_oben_m: float, seed: int, jitter_frac: float = 0.25, bild_dt: float = 1.0 / 120.0):
+    """A rectangular sheet of (nx + 1) x (ny + 1) vertices at spacing
+    ``kante_m``, centred over the body, ``fall_m`` above the body's top, with
+    in-plane jitter of ``jitter_frac`` of the spacing. Returns (muster, body)."""
+    rng_j = jitter_frac * kante_m * 1e3
+    p, tri = rechteck_netz(nx * kante_m * 1e3, ny * kante_m * 1e3, nx, ny, rng_j, seed)
+    z0 = koerper_oben_m + fall_m
+    lage = np.stack([p[:, 0] * 1e-3 - 0.5 * nx * kante_m, p[:, 1] * 1e-3 - 0.5 * ny * kante_m,
+                     np.full(p.shape[0], z0)], axis=1)
+    teil = Teil(p, tri, (math.cos(winkel), math.sin(winkel)), material, lage)
+    param = Simparameter(bild_dt=bild_dt, schwerkraft=(0.0, 0.0, -9.81), daempfung=0.0)
+    return Muster([teil], [], param), body
+
+
+def drape_batch(anzahl: int = 64, seed: int = 0, n_min: int = 2000, n_max: int = 60000, kante_m: float = 1.0 / 256,
+                fall_m: float = 0.1):
+    """The batched-drape workload: ``anzahl`` sheets with vertex counts
+    log-uniform in [n_min, n_max], aspect ratio U(1, 3), the C2 sheet's
+    spacing and areal density, warp U(1000, 2000), weft U(500, 1000), shear
+    U(25, 50) N/m, bending U(2.5e-6, 5e-6) N m, grain angle U[0, pi), each
+    falling onto its own sphere or capsule sampled on a 64^3 grid. Returns a
+    list of (muster, body)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(anzahl):
+        nv = float(np.exp(rng.uniform(math.log(n_min), math.log(n_max))))
+        asp = float(rng.uniform(1.0, 3.0))
+        ny = max(int(round(math.sqrt(nv / asp))) - 1, 2)
+        nx = max(int(round(asp * (ny + 1))) - 1, 2)
+        bend = float(rng.uniform(2.5e-6, 5e-6))
+        mat = Material(dehnung_n_m=float(rng.uniform(500.0, 1000.0)), kette_n_m=float(rng.uniform(1000.0, 2000.0)),
+                       schub_n_m=float(rng.uniform(25.0, 50.0)), biegung_nm=bend, biegung_kette_nm=bend,
+                       biegung_schraege_nm=bend, flaechengewicht_kg_m2=0.2, dicke_m=0.5e-3, reibung=0.3)
+        winkel = float(rng.uniform(0.0, math.pi))
+        laenge = max(nx, ny) * kante_m
+        if rng.uniform() < 0.5:
+            r = 0.3 * laenge
+            body = sphere_sdf_grid(r, 64, 2.4 * r / 63)
+            oben = r
+        else:
+            r = 0.15 * laenge
+            body = capsule_sdf_grid(r, 0.3 * nx * kante_m, 64)
+            oben = r
+        out.append(drape(nx, ny, kante_m, mat, winkel, body, fall_m, oben, seed * 1000 + k))
+    return out
+
+
 # ------------------------------------------------------------------ two layers
 def zwei_lagen(groesse_m: float = 0.2, kante_mm: float = 10.0, abstand_m: float = 0.01,
                material: Material = RADICAL_RUBBER_04, neigung: float = 0.0, z_unten: float = 0.0,
