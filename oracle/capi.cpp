@@ -324,6 +324,41 @@ void* orc_sim_create(const k3d_scene* s, const k3d_params* p) {
 }
 void orc_sim_free(void* h) { delete static_cast<Sim*>(h); }
 
+// Adjoint of n frames (adjoint.cpp): runs the frames from the current state,
+// recording every substep, then goes back through them. gx, gv: cotangents of
+// the final x, v (3 per point); out: those of the initial x, v, and per
+// membrane (E_warp, E_weft, G, grain rotation) and per hinge (k) the
+// parameter cotangents. iters: adjoint CG iterations (may be null).
+void orc_sim_adjoint(void* h, int32_t n, const double* gx, const double* gv, double* gx0, double* gv0,
+                     double* g_membran, double* g_biegung, double toleranz, int64_t* iters) {
+  auto* sim = static_cast<Sim*>(h);
+  std::vector<Aufnahme> auf;
+  for (int32_t f = 0; f < n; ++f) sim->cg.bild(sim->s, &auf);
+  const size_t np = sim->s.x.size();
+  std::vector<V3> xq(np), vq(np), lam;
+  for (size_t i = 0; i < np; ++i)
+    for (int a = 0; a < 3; ++a) {
+      xq[i][a] = gx[3 * i + a];
+      vq[i][a] = gv[3 * i + a];
+    }
+  AdjGrad g;
+  g.membran.assign(sim->s.membran_elemente.size(), {0, 0, 0, 0});
+  g.biegung.assign(sim->s.biegung.size(), 0.0);
+  AdjStat st;
+  Szene s = sim->s;
+  ImplizitCg cg = sim->cg;
+  for (size_t k = auf.size(); k-- > 0;) cg.adjoint_schritt(s, auf[k], xq, vq, g, lam, st, toleranz);
+  for (size_t i = 0; i < np; ++i)
+    for (int a = 0; a < 3; ++a) {
+      gx0[3 * i + a] = xq[i][a];
+      gv0[3 * i + a] = vq[i][a];
+    }
+  for (size_t t = 0; t < g.membran.size(); ++t)
+    for (int q = 0; q < 4; ++q) g_membran[4 * t + q] = g.membran[t][q];
+  for (size_t b = 0; b < g.biegung.size(); ++b) g_biegung[b] = g.biegung[b];
+  if (iters) *iters = int64_t(st.cg_iterationen);
+}
+
 void orc_sim_frames(void* h, int32_t n, k3d_stats* st) {
   auto* sim = static_cast<Sim*>(h);
   ImplizitStatistik summe;

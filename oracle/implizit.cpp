@@ -302,9 +302,17 @@ System ImplizitCg::system_bauen(Szene& s, double h, std::vector<std::optional<Fe
 
 // implizit.rs:899-1038 (no self-collision, no body-point passes; durchstoss
 // only applies to mesh bodies, which this restatement does not carry)
-void ImplizitCg::schritt(Szene& s, double h) {
+void ImplizitCg::schritt(Szene& s, double h, Aufnahme* auf) {
   const size_t n = s.x.size();
   const V3 g = s.param.schwerkraft;
+  if (auf) {
+    auf->h = h;
+    auf->x = s.x;
+    auf->v = s.v;
+    auf->koerper = s.koerper;
+    auf->reib.assign(n, 0);
+    auf->stoss.assign(n, 0);
+  }
   std::vector<std::optional<Fest>> fest;
   System sys = system_bauen(s, h, fest);
   std::vector<V3> dv = dv_vorher.size() == n ? dv_vorher : std::vector<V3>(n, mul(g, h));
@@ -336,6 +344,11 @@ void ImplizitCg::schritt(Szene& s, double h) {
     if (!frei) break;
   }
   dv_vorher = dv;
+  if (auf) {
+    auf->dv = dv;
+    auf->fest = fest;
+    auf->fn = fn_kraft;
+  }
   const std::vector<V3>& last = sys.last;
   for (size_t i = 0; i < n; ++i) {
     if (s.w[i] <= 0.0) continue;
@@ -351,25 +364,28 @@ void ImplizitCg::schritt(Szene& s, double h) {
       if (lt <= grenze) {
         statistik.haftend += 1;
         v = sub(v, t);
+        if (auf) auf->reib[i] = 1;
       } else if (lt > 0.0) {
         v = sub(v, mul(t, grenze / lt));
+        if (auf) auf->reib[i] = 2;
       }
     }
     s.v[i] = v;
     s.x[i] = add(s.x[i], mul(v, h));
-    for (const auto& kb : s.koerper) {
-      auto kt = kb.kontakt(s.x[i], s.kollisionsabstand[i]);
+    for (size_t kb = 0; kb < s.koerper.size(); ++kb) {
+      auto kt = s.koerper[kb].kontakt(s.x[i], s.kollisionsabstand[i]);
       if (kt) {
         s.x[i] = add(s.x[i], mul(kt->normale, kt->tiefe));
         double vn = dot(sub(s.v[i], kt->geschwindigkeit), kt->normale);
         if (vn < 0.0) s.v[i] = sub(s.v[i], mul(kt->normale, vn));
+        if (auf) auf->stoss[i] |= (1u << (2 * kb)) | (vn < 0.0 ? 1u << (2 * kb + 1) : 0u);
       }
     }
   }
 }
 
 // implizit.rs:1042-1057
-void ImplizitCg::bild(Szene& s) {
+void ImplizitCg::bild(Szene& s, std::vector<Aufnahme>* auf) {
   size_t n = std::max<size_t>(param.schritte_je_bild, 1);
   double h = s.param.bild_dt / double(n);
   statistik = ImplizitStatistik{};
@@ -377,7 +393,12 @@ void ImplizitCg::bild(Szene& s) {
   for (size_t k = 0; k < n; ++k) {
     double weg = double(k + 1) * h;
     for (size_t b = 0; b < s.koerper.size(); ++b) s.koerper[b] = anfang[b].verschoben(weg);
-    schritt(s, h);
+    if (auf) {
+      auf->emplace_back();
+      schritt(s, h, &auf->back());
+    } else {
+      schritt(s, h);
+    }
   }
   s.zeit += s.param.bild_dt;
 }

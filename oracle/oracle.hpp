@@ -313,6 +313,29 @@ struct ImplizitStatistik {
          freigegeben = 0, durchstoesse = 0, koerperpunkte = 0, naehe_punkt_dreieck = 0, naehe_kante_kante = 0;
   double rest_max = 0;
 };
+// Forward record of one substep, for the adjoint (no reference counterpart):
+// the state at the start, the final solution, the contact set after the
+// release pass, each held point's normal force and friction case, and per
+// point which bodies pushed it out after the move.
+struct Aufnahme {
+  double h = 0;
+  std::vector<V3> x, v, dv;
+  std::vector<std::optional<Fest>> fest;
+  std::vector<double> fn;
+  std::vector<uint8_t> reib;    // held points: 1 stick, 2 slip
+  std::vector<uint32_t> stoss;  // body b: bit 2b pushed out, bit 2b+1 inward normal velocity removed
+  std::vector<Koerper> koerper; // the bodies as placed for this substep
+};
+// Parameter cotangents per element, summed over the substeps of a backward
+// pass: membranes (E_warp, E_weft, G, rotation of the grain basis), hinges k.
+struct AdjGrad {
+  std::vector<std::array<double, 4>> membran;
+  std::vector<double> biegung;
+};
+struct AdjStat {
+  size_t cg_iterationen = 0, loesungen = 0, nicht_konvergiert = 0;
+};
+
 // sim/src/implizit.rs:570-1057
 struct ImplizitCg {
   ImplizitParameter param;
@@ -320,9 +343,14 @@ struct ImplizitCg {
   std::vector<V3> dv_vorher;
   std::optional<std::pair<Stoffnetz, Stoffwerte>> selbst;
   System system_bauen(Szene& s, double h, std::vector<std::optional<Fest>>& fest);
-  void schritt(Szene& s, double h);
-  void bild(Szene& s);
+  void schritt(Szene& s, double h, Aufnahme* auf = nullptr);
+  void bild(Szene& s, std::vector<Aufnahme>* auf = nullptr);
   std::vector<V3> op(Szene& s, const std::vector<V3>& p);
+  // Adjoint of one recorded substep (adjoint.cpp): xq, vq enter as the
+  // cotangents of the substep's output x, v and leave as those of its input;
+  // lam is the adjoint solve's warm start and result.
+  void adjoint_schritt(Szene& s, const Aufnahme& a, std::vector<V3>& xq, std::vector<V3>& vq, AdjGrad& g,
+                       std::vector<V3>& lam, AdjStat& st, double adj_toleranz);
 };
 
 // ---------------------------------------------------------------- measurement

@@ -45,6 +45,7 @@ def lib():
     L.orc_sim_create.restype = P
     L.orc_sim_free.argtypes = [P]
     L.orc_sim_frames.argtypes = [P, C.c_int32, C.POINTER(_abi.K3dStats)]
+    L.orc_sim_adjoint.argtypes = [P, C.c_int32, dp, dp, dp, dp, dp, dp, C.c_double, C.POINTER(C.c_int64)]
     L.orc_sim_get_state.argtypes = [P, dp, dp]
     L.orc_sim_set_state.argtypes = [P, dp, dp]
     L.orc_sim_set_naht_ruhe.argtypes = [P, dp]
@@ -141,6 +142,8 @@ class OracleSim:
         self.n = szene.n
         self.n_naht = szene.naht_punkte.shape[0]
         self.n_tri = szene.dreiecke.shape[0]
+        self.n_membran = szene.membran_punkte.shape[0]
+        self.n_biegung = szene.biegung_punkte.shape[0]
         cs, keep = szene.to_c()
         self.h = self.L.orc_sim_create(C.byref(cs), C.byref(params))
         del keep
@@ -154,6 +157,21 @@ class OracleSim:
         st = _abi.K3dStats()
         self.L.orc_sim_frames(self.h, n, C.byref(st))
         return st
+
+    def adjoint(self, n: int, gx, gv, toleranz: float = 1e-12) -> dict:
+        """``n`` frames from the current state, then the adjoint back through
+        them: cotangents of the initial x, v and of the element parameters
+        (per membrane E_warp, E_weft, G, grain rotation; per hinge k) for the
+        cotangents ``gx``, ``gv`` of the final x, v."""
+        gx = f64(gx)
+        gv = f64(gv)
+        ox = np.zeros((self.n, 3))
+        ov = np.zeros((self.n, 3))
+        gm = np.zeros((self.n_membran, 4))
+        gb = np.zeros(self.n_biegung)
+        it = C.c_int64(0)
+        self.L.orc_sim_adjoint(self.h, n, _d(gx), _d(gv), _d(ox), _d(ov), _d(gm), _d(gb), toleranz, C.byref(it))
+        return dict(x=ox, v=ov, membran=gm, biegung=gb, iterationen=int(it.value))
 
     def state(self):
         x = np.zeros((self.n, 3))
