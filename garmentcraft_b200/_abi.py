@@ -139,6 +139,18 @@ class K3dStats(C.Structure):
     ]
 
 
+class K3dAdjointStats(C.Structure):
+    _fields_ = [
+        ("cg_iterationen", C.c_int64),
+        ("loesungen", C.c_int64),
+        ("nicht_konvergiert", C.c_int64),
+        ("zusammenbrueche", C.c_int64),
+        ("ms_vorwaerts", C.c_double),
+        ("ms_rueckwaerts", C.c_double),
+        ("ms_neuberechnung", C.c_double),
+    ]
+
+
 class K3dCgResult(C.Structure):
     _fields_ = [
         ("iterationen", C.c_int64),

@@ -21,6 +21,7 @@ EXPORTS = [
     "k3d_upload_state", "k3d_download_state", "k3d_operator", "k3d_system_for", "k3d_solve",
     "k3d_residual", "k3d_read_load", "k3d_last_frame_ms", "k3d_last_solve_ms", "k3d_kernel_launches",
     "k3d_operator_noalloc", "k3d_selfcollision_pairs", "k3d_selfcollision_hash", "k3d_selfcollision_springs",
+    "k3d_adjoint_forward", "k3d_adjoint_backward",
 ]
 
 _lib = None
@@ -63,6 +64,10 @@ def lib():
     L.k3d_frame.restype = st
     L.k3d_frames_resident.argtypes = [P, C.c_int32, C.POINTER(_abi.K3dStats)]
     L.k3d_frames_resident.restype = st
+    L.k3d_adjoint_forward.argtypes = [P, C.c_int32, C.c_int32, C.POINTER(_abi.K3dStats)]
+    L.k3d_adjoint_forward.restype = st
+    L.k3d_adjoint_backward.argtypes = [P, dp, dp, dp, dp, dp, dp, C.POINTER(_abi.K3dAdjointStats)]
+    L.k3d_adjoint_backward.restype = st
     L.k3d_upload_state.argtypes = [P, dp, dp]
     L.k3d_upload_state.restype = st
     L.k3d_download_state.argtypes = [P, dp, dp]

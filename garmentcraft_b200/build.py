@@ -13,14 +13,15 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_native")
 LIB = os.path.join(OUT_DIR, "libklon3d_b200.so")
 SOURCES = ["k3d_step.cu", "k3d_build.cu", "k3d_host.cpp", "scene_build.cpp", "k3d_noalloc.cu", "k3d_selbst.cu",
-           "k3d_selbst_host.cpp"]
+           "k3d_selbst_host.cpp", "k3d_adjoint.cu"]
 HEADERS = ["k3d_step.h", "k3d_device.cuh", "k3d_step_common.cuh", "scene_build.h", "k3d_selbst.h",
-           "k3d_selbst_host.h"]
+           "k3d_selbst_host.h", "k3d_adjoint.h"]
 # Per-file flags. The build of the system and the self-collision stage round
 # every product and sum on their own (no fused multiply-add), as the
 # reference's arithmetic does: the element term of k3d_build.cu needs it, and
-# the self-collision cell indices, buckets and pairs come out bit-exact.
-EXTRA = {"k3d_build.cu": ["-fmad=false"], "k3d_selbst.cu": ["-fmad=false"]}
+# the self-collision cell indices, buckets and pairs come out bit-exact. The
+# adjoint replays the forward's contact queries and rounds the same way.
+EXTRA = {"k3d_build.cu": ["-fmad=false"], "k3d_selbst.cu": ["-fmad=false"], "k3d_adjoint.cu": ["-fmad=false"]}
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [

@@ -412,10 +412,15 @@ __global__ void __launch_bounds__(kBlock) assemble_kernel(const __grid_constant_
 __device__ void integrate(const StepArgs& a, double (&cnt)[3]) {
   const double h = a.h;
   K3D_FOR(i, a.n) {
-    if (!a.frei[i]) continue;
+    if (!a.frei[i]) {
+      if (a.rec_flags) a.rec_flags[i] = 0u;
+      continue;
+    }
+    uint32_t fl = 0u;
     D3 v = ld3(a.v, uint32_t(i)) + ld3(a.dv, uint32_t(i));
     const D3 n = ld3(a.nrm_d, uint32_t(i));
     if (n.x != 0.0 || n.y != 0.0 || n.z != 0.0) {
+      fl |= 1u;
       cnt[0] += 1.0;
       const D3 vb = ld3(a.vk, uint32_t(i));
       const D3 rel = v - vb;
@@ -426,8 +431,10 @@ __device__ void integrate(const StepArgs& a, double (&cnt)[3]) {
       if (lt <= grenze) {
         cnt[1] += 1.0;
         v = v - t;
+        fl |= 2u;
       } else if (lt > 0.0) {
         v = v - t * (grenze / lt);
+        fl |= 4u;
       }
     }
     D3 x = ld3(a.x, uint32_t(i)) + v * h;
@@ -441,8 +448,10 @@ __device__ void integrate(const StepArgs& a, double (&cnt)[3]) {
         const D3 bv = d3(a.bodies[kb].vel[0], a.bodies[kb].vel[1], a.bodies[kb].vel[2]);
         const double vn = dot(v - bv, nn);
         if (vn < 0.0) v = v - nn * vn;
+        if (kb < kMaxAdjointBodies) fl |= (1u << (4 + 2 * kb)) | (vn < 0.0 ? 1u << (5 + 2 * kb) : 0u);
       }
     }
+    if (a.rec_flags) a.rec_flags[i] = fl | (a.rec_flags[i] & 8u);
     if (!(isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z)))
       cnt[2] += 1.0;
     st3(a.x, uint32_t(i), x);

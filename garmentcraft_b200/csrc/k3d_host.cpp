@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/klon3d_step.h"
+#include "k3d_adjoint.h"
 #include "k3d_selbst_host.h"
 #include "k3d_step.h"
 #include "scene_build.h"
@@ -61,6 +62,19 @@ struct k3d_solver {
   double* d_pout = nullptr; // probe output (3N)
   SelbstHost sc;            // self-collision proximity stage (when enabled)
   int n_grp = 1;            // instances (independent drapes) of the uploaded scene
+  // adjoint: the last k3d_adjoint_forward's checkpoints (x, v, dv every k
+  // substeps) and the bodies at the start of each of its frames; one segment
+  // of substep records; the backward's vectors
+  struct Adj {
+    bool valid = false;
+    int k = 0, sub = 1;
+    int64_t steps = 0;
+    double ms_fwd = 0.0;
+    std::vector<uint8_t> first;                 // first_step at each checkpoint
+    std::vector<std::vector<k3d_body>> bodies;  // per frame
+    void *ck = nullptr, *rec = nullptr, *work = nullptr;
+    size_t ck_bytes = 0, rec_bytes = 0, work_bytes = 0;
+  } adj;
 };
 
 static k3d_status fail(k3d_solver* h, k3d_status st, const std::string& msg) {
@@ -326,6 +340,9 @@ k3d_solver* k3d_solver_create(const k3d_params* params, int32_t device) {
 
 static void release_device(k3d_solver* h) {
   selbst_free(h->sc);
+  for (void* q : {h->adj.ck, h->adj.rec, h->adj.work})
+    if (q) cudaFree(q);
+  h->adj = k3d_solver::Adj{};
   if (h->arena.base) cudaFree(h->arena.base);
   h->arena = Arena{};
   for (void* p : h->sdf_dev) cudaFree(p);
@@ -753,7 +770,9 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
 }  // extern "C"
 
 // Fills the per-launch fields and launches one step kernel.
-static k3d_status launch(k3d_solver* h, int mode, double t_bodies, bool need_load) {
+// The per-launch fields of the handle's StepArgs: step constants and the
+// bodies moved by t_bodies from their frame-start positions.
+static void step_args(k3d_solver* h, int mode, double t_bodies, bool need_load) {
   StepArgs& a = h->a;
   const int sub = std::max(h->p.schritte_je_bild, 1);
   a.mode = mode;
@@ -784,6 +803,11 @@ static k3d_status launch(k3d_solver* h, int mode, double t_bodies, bool need_loa
     d.sdf = static_cast<const float*>(h->sdf_dev[b]);
     d.inst = h->n_grp > 1 ? k.instanz : -1;
   }
+}
+
+static k3d_status launch(k3d_solver* h, int mode, double t_bodies, bool need_load) {
+  StepArgs& a = h->a;
+  step_args(h, mode, t_bodies, need_load);
   int launched = 0;
   if (h->sc.on) {  // proximity pairs and springs before the system (implizit.rs:668-691)
     cudaError_t es = selbst_run(h->sc, a.h, h->stream, launched);
@@ -1158,6 +1182,215 @@ int64_t k3d_selfcollision_springs(k3d_solver* h, int64_t cap, double* kraft, dou
     }
   }
   return np;
+}
+
+
+// ------------------------------------------------------------ adjoint
+static k3d_status adj_check(k3d_solver* h) {
+  if (h->p.precision != K3D_FP64) return fail(h, K3D_BAD_ARGUMENT, "the adjoint needs K3D_FP64");
+  if (h->p.selbstkollision) return fail(h, K3D_BAD_ARGUMENT, "the adjoint needs self-collision off");
+  if (h->p.normalkraft_aus_last) return fail(h, K3D_BAD_ARGUMENT, "the adjoint needs normalkraft_aus_last off");
+  if (h->bodies.size() > size_t(kMaxAdjointBodies))
+    return fail(h, K3D_BAD_ARGUMENT, "the adjoint takes at most 14 bodies");
+  return K3D_OK;
+}
+
+static bool grow(void*& p, size_t& have, size_t need) {
+  if (need <= have) return true;
+  if (p) cudaFree(p);
+  p = nullptr;
+  have = 0;
+  if (cudaMalloc(&p, need) != cudaSuccess) return false;
+  have = need;
+  return true;
+}
+
+k3d_status k3d_adjoint_forward(k3d_solver* h, int32_t n_frames, int32_t k, k3d_stats* stats) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if ((st = adj_check(h)) != K3D_OK) return st;
+  if (n_frames < 1 || k < 1) return fail(h, K3D_BAD_ARGUMENT, "frames and checkpoint spacing must be positive");
+  auto& A = h->adj;
+  const int sub = std::max(h->p.schritte_je_bild, 1);
+  const int64_t steps = int64_t(n_frames) * sub, nck = (steps + k - 1) / k;
+  const size_t N3 = 3 * size_t(h->n);
+  if (!grow(A.ck, A.ck_bytes, size_t(nck) * 3 * N3 * sizeof(double)))
+    return fail(h, K3D_DEVICE_ERROR, "out of device memory for the adjoint checkpoints");
+  A.valid = false;
+  A.k = k;
+  A.sub = sub;
+  A.steps = steps;
+  A.first.assign(size_t(nck), 0);
+  A.bodies.clear();
+  st = reset_stats(h);
+  if (st != K3D_OK) return st;
+  const double hs = h->sim.bild_dt / double(sub);
+  double* ck = static_cast<double*>(A.ck);
+  K3D_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+  for (int f = 0; f < n_frames; ++f) {
+    A.bodies.push_back(h->bodies);
+    for (int q = 0; q < sub; ++q) {
+      const int64_t j = int64_t(f) * sub + q;
+      if (j % k == 0) {
+        double* c = ck + size_t(j / k) * 3 * N3;
+        K3D_CUDA(h, cudaMemcpyAsync(c, h->a.x, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+        K3D_CUDA(h, cudaMemcpyAsync(c + N3, h->a.v, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+        K3D_CUDA(h, cudaMemcpyAsync(c + 2 * N3, h->a.dv, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+        A.first[size_t(j / k)] = h->first_step ? 1 : 0;
+      }
+      st = launch(h, MODE_STEP, double(q + 1) * hs, false);
+      if (st != K3D_OK) return st;
+    }
+    for (auto& b : h->bodies)
+      for (int q = 0; q < 3; ++q) b.punkt[q] += b.geschwindigkeit[q] * h->sim.bild_dt;
+  }
+  K3D_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+  st = check_sync(h);
+  if (st != K3D_OK) return st;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  h->last_ms = ms;
+  A.ms_fwd = ms;
+  st = read_stats(h, stats);
+  if (st == K3D_OK) A.valid = true;
+  return st;
+}
+
+k3d_status k3d_adjoint_backward(k3d_solver* h, const double* gx, const double* gv, double* gx0, double* gv0,
+                                double* g_membran, double* g_biegung, k3d_adjoint_stats* out) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if ((st = adj_check(h)) != K3D_OK) return st;
+  auto& A = h->adj;
+  if (!A.valid) return fail(h, K3D_BAD_ARGUMENT, "no adjoint forward to go back through");
+  if (!gx || !gv) return fail(h, K3D_BAD_ARGUMENT, "null cotangent");
+  const size_t N = size_t(h->n), N3 = 3 * N, T = size_t(h->nt), B = size_t(h->nb), S = size_t(h->ns);
+  const size_t k = size_t(A.k);
+  // one record: x, v, dv (3N each), fn (N) in doubles, then flags (N)
+  const size_t rec_d = 10 * N, rec_stride = ((rec_d * 8 + 4 * N) + 255) & ~size_t(255);
+  if (!grow(A.rec, A.rec_bytes, k * rec_stride)) return fail(h, K3D_DEVICE_ERROR, "out of device memory (records)");
+  const size_t n_vec = 16;  // final state (3) and the backward's 13 vectors
+  const size_t work_d = n_vec * N3 + 10 * T + 13 * B + 6 * S + 4 * T + B + 2 + ST_COUNT;
+  if (!grow(A.work, A.work_bytes, work_d * 8)) return fail(h, K3D_DEVICE_ERROR, "out of device memory (adjoint)");
+  double* w = static_cast<double*>(A.work);
+  double* fin = w;
+  double* vec = w + 3 * N3;
+  AdjArgs J{};
+  double** vs[13] = {&J.xq, &J.vq, &J.adv, &J.gq, &J.rq, &J.nq, &J.xa, &J.va, &J.gg, &J.arq, &J.lam, &J.alam, &J.mu};
+  for (int q = 0; q < 13; ++q) *vs[q] = vec + size_t(q) * N3;
+  double* tail = w + n_vec * N3;
+  J.om = tail;
+  J.ob = J.om + 10 * T;
+  J.os = J.ob + 13 * B;
+  J.acc_m = J.os + 6 * S;
+  J.acc_b = J.acc_m + 4 * T;
+  J.rest = J.acc_b + B;
+  J.stats = reinterpret_cast<long long*>(J.rest + 2);
+  // keep the forward's final state; the segments overwrite the resident one
+  K3D_CUDA(h, cudaMemcpyAsync(fin, h->a.x, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+  K3D_CUDA(h, cudaMemcpyAsync(fin + N3, h->a.v, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+  K3D_CUDA(h, cudaMemcpyAsync(fin + 2 * N3, h->a.dv, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+  const std::vector<k3d_body> bodies_end = h->bodies;
+  const bool first_end = h->first_step;
+  K3D_CUDA(h, cudaMemcpyAsync(J.xq, gx, N3 * 8, cudaMemcpyHostToDevice, h->stream));
+  K3D_CUDA(h, cudaMemcpyAsync(J.vq, gv, N3 * 8, cudaMemcpyHostToDevice, h->stream));
+  K3D_CUDA(h, cudaMemsetAsync(J.lam, 0, N3 * 8, h->stream));
+  K3D_CUDA(h, cudaMemsetAsync(J.acc_m, 0, (4 * T + B + 2 + ST_COUNT) * 8, h->stream));
+  const double hs = h->sim.bild_dt / double(A.sub);
+  const double* ck = static_cast<const double*>(A.ck);
+  char* rec = static_cast<char*>(A.rec);
+  const int64_t nck = (A.steps + A.k - 1) / A.k;
+  cudaEvent_t e_r0 = nullptr, e_r1 = nullptr;
+  K3D_CUDA(h, cudaEventCreate(&e_r0));
+  K3D_CUDA(h, cudaEventCreate(&e_r1));
+  double ms_re = 0.0;
+  K3D_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+  for (int64_t seg = nck - 1; seg >= 0 && st == K3D_OK; --seg) {
+    const int64_t j0 = seg * A.k, j1 = std::min<int64_t>(j0 + A.k, A.steps);
+    const double* c = ck + size_t(seg) * 3 * N3;
+    K3D_CUDA(h, cudaEventRecord(e_r0, h->stream));
+    K3D_CUDA(h, cudaMemcpyAsync(h->a.x, c, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+    K3D_CUDA(h, cudaMemcpyAsync(h->a.v, c + N3, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+    K3D_CUDA(h, cudaMemcpyAsync(h->a.dv, c + 2 * N3, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+    h->first_step = A.first[size_t(seg)] != 0;
+    // the segment again, recording each substep
+    for (int64_t j = j0; j < j1 && st == K3D_OK; ++j) {
+      double* r = reinterpret_cast<double*>(rec + size_t(j - j0) * rec_stride);
+      h->bodies = A.bodies[size_t(j / A.sub)];
+      K3D_CUDA(h, cudaMemcpyAsync(r, h->a.x, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+      K3D_CUDA(h, cudaMemcpyAsync(r + N3, h->a.v, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+      h->a.rec_flags = reinterpret_cast<uint32_t*>(r + rec_d);
+      K3D_CUDA(h, cudaMemsetAsync(h->a.rec_flags, 0, N * sizeof(uint32_t), h->stream));
+      st = launch(h, MODE_STEP, double(j % A.sub + 1) * hs, false);
+      h->a.rec_flags = nullptr;
+      if (st != K3D_OK) break;
+      K3D_CUDA(h, cudaMemcpyAsync(r + 2 * N3, h->a.dv, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+      K3D_CUDA(h, cudaMemcpyAsync(r + 3 * N3, h->a.fnk, N * 8, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    if (st != K3D_OK) break;
+    K3D_CUDA(h, cudaEventRecord(e_r1, h->stream));
+    // back through it
+    for (int64_t j = j1 - 1; j >= j0; --j) {
+      const double* r = reinterpret_cast<const double*>(rec + size_t(j - j0) * rec_stride);
+      h->bodies = A.bodies[size_t(j / A.sub)];
+      step_args(h, MODE_STEP, double(j % A.sub + 1) * hs, false);
+      StepArgs a = h->a;
+      a.x = const_cast<double*>(r);
+      a.v = const_cast<double*>(r + N3);
+      J.x = r;
+      J.v = r + N3;
+      J.dv = r + 2 * N3;
+      J.fn = r + 3 * N3;
+      J.flags = reinterpret_cast<const uint32_t*>(r + rec_d);
+      int launched = 0;
+      cudaError_t e = launch_adjoint_step(a, J, h->blocks, h->stream, launched);
+      h->launches += launched;
+      if (e != cudaSuccess) {
+        st = cuda_fail(h, e, "adjoint step launch");
+        break;
+      }
+    }
+    K3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e_r0, e_r1);
+    ms_re += ms;
+  }
+  K3D_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+  cudaEventDestroy(e_r0);
+  cudaEventDestroy(e_r1);
+  // the forward's final state again
+  K3D_CUDA(h, cudaMemcpyAsync(h->a.x, fin, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+  K3D_CUDA(h, cudaMemcpyAsync(h->a.v, fin + N3, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+  K3D_CUDA(h, cudaMemcpyAsync(h->a.dv, fin + 2 * N3, N3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+  h->bodies = bodies_end;
+  h->first_step = first_end;
+  k3d_status sy = check_sync(h);
+  if (st != K3D_OK) return st;
+  if (sy != K3D_OK) return sy;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  if (gx0) K3D_CUDA(h, cudaMemcpy(gx0, J.xq, N3 * 8, cudaMemcpyDeviceToHost));
+  if (gv0) K3D_CUDA(h, cudaMemcpy(gv0, J.vq, N3 * 8, cudaMemcpyDeviceToHost));
+  if (g_membran && T > 0) {
+    std::vector<double> gm(4 * T);
+    K3D_CUDA(h, cudaMemcpy(gm.data(), J.acc_m, 4 * T * 8, cudaMemcpyDeviceToHost));
+    for (size_t t = 0; t < T; ++t)
+      for (size_t q = 0; q < 4; ++q) g_membran[4 * t + q] = gm[q * T + t];
+  }
+  if (g_biegung && B > 0) K3D_CUDA(h, cudaMemcpy(g_biegung, J.acc_b, B * 8, cudaMemcpyDeviceToHost));
+  long long sts[ST_COUNT];
+  K3D_CUDA(h, cudaMemcpy(sts, J.stats, sizeof(sts), cudaMemcpyDeviceToHost));
+  if (out) {
+    std::memset(out, 0, sizeof(*out));
+    out->cg_iterationen = sts[ST_CG_ITERATIONS];
+    out->loesungen = sts[ST_SOLVES];
+    out->nicht_konvergiert = sts[ST_UNCONVERGED];
+    out->zusammenbrueche = sts[ST_BREAKDOWNS];
+    out->ms_vorwaerts = A.ms_fwd;
+    out->ms_rueckwaerts = ms;
+    out->ms_neuberechnung = ms_re;
+  }
+  return K3D_OK;
 }
 
 }  // extern "C"

@@ -339,7 +339,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     } else {
       const D3 n = ld3(a.nrm_d, uint32_t(i));
       if (n.x != 0.0 || n.y != 0.0 || n.z != 0.0) {
-        const double soll = a.vn_soll[i] - dot(ld3(a.v, uint32_t(i)), n);
+        const double soll = a.adjoint ? 0.0 : a.vn_soll[i] - dot(ld3(a.v, uint32_t(i)), n);
         d = (d - n * dot(d, n)) + n * soll;
       }
     }
@@ -516,7 +516,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
 // implizit.rs:924-942: normal force from the residual A dv - b along the
 // contact normal; a held point that pulls on the body is released.
 template <typename R, bool SC>
-__device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double& released) {
+__device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double& released, bool last) {
   const bool hi = a.m_f1w64 != nullptr;
   if (hi)
     apply_dv64(a, sh);
@@ -541,6 +541,8 @@ __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double
       st3(a.nrm_d, uint32_t(i), d3(0, 0, 0));
       vw.nrm[3 * i] = vw.nrm[3 * i + 1] = vw.nrm[3 * i + 2] = R(0);
       cnt[0] += 1.0;
+      // released after the last solve: held in dv's constraint, free in friction
+      if (last && a.rec_flags) a.rec_flags[i] |= 8u;
     } else {
       a.fnk[i] = fn;
     }
@@ -595,7 +597,7 @@ __global__ void __launch_bounds__(kSolveBlock, 1) solve_kernel(const __grid_cons
     if (a.mode == MODE_SOLVE) return;
     if (!any_held) break;
     double rel = 0.0;
-    if (!release<R, SC>(a, vw, sh, rel)) return;
+    if (!release<R, SC>(a, vw, sh, rel, pass == 1)) return;
     if (lead && rel > 0.0)
       atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[ST_RELEASED]), (unsigned long long)rel);
     if (rel == 0.0) break;
@@ -671,6 +673,14 @@ static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int&
     launched += 1;
   }
   return cudaSuccess;
+}
+
+cudaError_t launch_pcg64(const StepArgs& a, int blocks, cudaStream_t stream) {
+  StepArgs s = a;
+  s.mode = MODE_SOLVE;
+  cudaError_t e = cudaMemsetAsync(s.grp_cnt, 0, sizeof(unsigned) * 32 * size_t(s.n_grp), stream);
+  if (e != cudaSuccess) return e;
+  return cooperative(Kernels<double>::sv(), s, blocks, stream);
 }
 
 cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream_t stream, int& launched) {

@@ -114,6 +114,14 @@ struct StepArgs {
   const uint32_t* blk_grp;
   unsigned* grp_cnt;  // the groups' counters, 32 words apart
   int n_grp;
+  // adjoint: the PCG solves S A S lam = S b with a zero target on held points
+  // (adjoint != 0); the step records each point's branches in rec_flags
+  // (null: no record; zeroed before the step): bit 0 held after the release
+  // pass, bit 1 stick, bit 2 slip, bit 3 released after the last solve (the
+  // second release pass), body k: bit 4 + 2k pushed out, bit 5 + 2k inward
+  // normal velocity removed
+  int adjoint;
+  uint32_t* rec_flags;
   // bookkeeping
   cudaEvent_t ev_solve0, ev_solve1;  // around the PCG launch (host-side handles)
   SyncState* sync;
@@ -131,5 +139,9 @@ BuildKernels build_kernels(int precision);
 int step_grid_blocks(int precision, int device);
 // Enqueues one substep (or probe) on `stream`; `launched` = kernels enqueued.
 cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream_t stream, int& launched);
+// The FP64 PCG launch alone on the system built before (one pass, no release
+// test): dv (start and result), b, normals and the assembled A as in `a`.
+cudaError_t launch_pcg64(const StepArgs& a, int blocks, cudaStream_t stream);
+constexpr int kMaxAdjointBodies = 14;  // bodies whose push-outs fit in rec_flags
 
 }  // namespace k3d

@@ -229,6 +229,37 @@ class ImplizitCg:
         L.k3d_selfcollision_springs(self._h, n, _d(kr), _d(bl))
         return dict(kraft=kr[:n], block=bl[:n])
 
+    def adjoint_vorwaerts(self, n: int, k: int = 10) -> ImplizitStatistik:
+        """``n`` frames on the device-resident state (as ``bilder_auf_geraet``)
+        that keep x, v and the warm start every ``k`` substeps for
+        ``adjoint_rueckwaerts``."""
+        st = _abi.K3dStats()
+        self._check(self._L.k3d_adjoint_forward(self._h, n, k, C.byref(st)), "adjoint forward")
+        return ImplizitStatistik.from_c(st)
+
+    def adjoint_rueckwaerts(self, gx: np.ndarray, gv: np.ndarray) -> dict:
+        """The adjoint of the last ``adjoint_vorwaerts``: for the cotangents
+        ``gx``, ``gv`` of the final x, v, those of the initial x, v, per
+        membrane of (E_warp, E_weft, G, grain rotation) and per hinge of k,
+        with the adjoint solve's statistics and device times."""
+        sz = self._szene
+        if sz is None:
+            raise K3dError(_abi.K3D_BAD_ARGUMENT, "no scene uploaded")
+        n, nt, nb = sz.n, sz.membran_punkte.shape[0], sz.biegung_punkte.shape[0]
+        gx = np.ascontiguousarray(gx, dtype=np.float64).reshape(n, 3)
+        gv = np.ascontiguousarray(gv, dtype=np.float64).reshape(n, 3)
+        ox = np.zeros((n, 3))
+        ov = np.zeros((n, 3))
+        gm = np.zeros((max(nt, 1), 4))
+        gb = np.zeros(max(nb, 1))
+        st = _abi.K3dAdjointStats()
+        self._check(self._L.k3d_adjoint_backward(self._h, _d(gx), _d(gv), _d(ox), _d(ov), _d(gm), _d(gb),
+                                                 C.byref(st)), "adjoint backward")
+        return dict(x=ox, v=ov, membran=gm[:nt], biegung=gb[:nb], iterationen=st.cg_iterationen,
+                    loesungen=st.loesungen, nicht_konvergiert=st.nicht_konvergiert,
+                    zusammenbrueche=st.zusammenbrueche, ms_vorwaerts=st.ms_vorwaerts,
+                    ms_rueckwaerts=st.ms_rueckwaerts, ms_neuberechnung=st.ms_neuberechnung)
+
     def letzte_bild_ms(self) -> float:
         return self._L.k3d_last_frame_ms(self._h)
 

@@ -204,14 +204,15 @@ def sphere_sdf_grid(radius_m: float, n: int, spacing_m: float, zentrum=(0.0, 0.0
 def sheet_over_sphere(n: int = 257, groesse_m: float = 1.0, jitter_mm: float = 1.0, seed: int = 0,
                       fall_m: float = 0.5, kugel_radius_m: float = 0.3, sdf_n: int = 128,
                       sdf_spacing_m: float = 0.01, material: Material = SHEET_MATERIAL,
-                      bild_dt: float = 1.0 / 120.0):
+                      bild_dt: float = 1.0 / 120.0, winkel: float | None = None):
     """Woven sheet dropped onto a sphere collider.
 
     n x n vertices over ``groesse_m`` square, in-plane jitter U(-1, 1) mm,
-    grainline angle U[0, pi) from the seed, start plane ``fall_m`` above the
-    sphere top. Returns (muster, sphere SDF body dict)."""
+    grainline angle U[0, pi) from the seed (or ``winkel``), start plane
+    ``fall_m`` above the sphere top. Returns (muster, sphere SDF body dict)."""
     rng = np.random.default_rng(seed)
-    winkel = float(rng.uniform(0.0, math.pi))
+    w0 = float(rng.uniform(0.0, math.pi))
+    winkel = w0 if winkel is None else float(winkel)
     p, tri = rechteck_netz(groesse_m * 1e3, groesse_m * 1e3, n - 1, n - 1, jitter_mm, seed + 1)
     z0 = kugel_radius_m + fall_m
     lage = np.stack([p[:, 0] * 1e-3 - 0.5 * groesse_m, p[:, 1] * 1e-3 - 0.5 * groesse_m,
@@ -220,6 +221,28 @@ def sheet_over_sphere(n: int = 257, groesse_m: float = 1.0, jitter_mm: float = 1
     param = Simparameter(bild_dt=bild_dt, schwerkraft=(0.0, 0.0, -9.81), daempfung=0.0)
     body = sphere_sdf_grid(kugel_radius_m, sdf_n, sdf_spacing_m)
     return Muster([teil], [], param), body
+
+
+# ------------------------------------------------------------------ material fit
+def materialfit(n: int = 129, seed: int = 0):
+    """The material-fit workload: an n x n sheet (1 x 1 m) dropped onto the
+    sphere of the sheet workload (R 0.3 m, 128^3 SDF at 1 cm). Hidden
+    parameters from the seed, uniform in warp 1000-2000, weft 500-1000, shear
+    25-50 N/m, bending 2.5e-6-5e-6 N m (all three directions), grain angle
+    [0, pi); the fit starts from them scaled by U(0.5, 2) each. Returns
+    (szene at the hidden parameters, hidden (warp, weft, shear, bend, grain),
+    start parameters)."""
+    from .implizit import build_scene
+    rng = np.random.default_rng(seed + 7919)
+    verdeckt = np.array([rng.uniform(1000.0, 2000.0), rng.uniform(500.0, 1000.0), rng.uniform(25.0, 50.0),
+                         rng.uniform(2.5e-6, 5e-6), rng.uniform(0.0, math.pi)])
+    start = verdeckt * rng.uniform(0.5, 2.0, size=5)
+    b = float(verdeckt[3])
+    mat = Material(dehnung_n_m=float(verdeckt[1]), kette_n_m=float(verdeckt[0]), schub_n_m=float(verdeckt[2]),
+                   biegung_nm=b, biegung_kette_nm=b, biegung_schraege_nm=b, flaechengewicht_kg_m2=0.2,
+                   dicke_m=0.5e-3, reibung=0.3)
+    m, body = sheet_over_sphere(n=n, seed=seed, material=mat, winkel=float(verdeckt[4]))
+    return build_scene(m, [body]), verdeckt, start
 
 
 # ------------------------------------------------------------------ batched drapes

@@ -300,6 +300,38 @@ double k3d_last_solve_ms(const k3d_solver* h);
 /* Number of device kernels the handle launched since creation. */
 int64_t k3d_kernel_launches(const k3d_solver* h);
 
+/* ---------------------------------------------------------------- adjoint
+ * The reference has no differentiation; these have no counterpart in it.
+ * They differentiate the step k3d_frames_resident takes, with its discrete
+ * decisions as the forward took them (the contact set after the release
+ * pass, stick or slip, which bodies pushed a point out). They need
+ * K3D_FP64, self-collision off, normalkraft_aus_last off and at most 14
+ * bodies (K3D_BAD_ARGUMENT otherwise). */
+typedef struct k3d_adjoint_stats {
+  int64_t cg_iterationen;    /* adjoint PCG iterations, all substeps */
+  int64_t loesungen;
+  int64_t nicht_konvergiert;
+  int64_t zusammenbrueche;
+  double ms_vorwaerts;       /* device time of the last k3d_adjoint_forward */
+  double ms_rueckwaerts;     /* device time of k3d_adjoint_backward, recomputation included */
+  double ms_neuberechnung;   /* the recomputation of the segments within it */
+} k3d_adjoint_stats;
+
+/* n_frames frames on the device-resident state, as k3d_frames_resident, that
+ * keep x, v and the warm start on the device every k substeps. */
+k3d_status k3d_adjoint_forward(k3d_solver* h, int32_t n_frames, int32_t k, k3d_stats* stats);
+
+/* The adjoint of the frames of the last k3d_adjoint_forward. gx, gv: the
+ * cotangents of the final x, v (host, 3 per point). Writes, where the
+ * pointer is not null, the cotangents of the initial x and v (3 per point),
+ * per membrane those of (E_warp, E_weft, G, a rotation of its grain basis in
+ * the rest plane) (4 per membrane, the scene's membrane order) and per hinge
+ * that of its stiffness k = 1/biegung_nachgiebigkeit, summed over the
+ * substeps. Each segment of k substeps is computed again from its checkpoint;
+ * afterwards the resident state is the forward's final state. */
+k3d_status k3d_adjoint_backward(k3d_solver* h, const double* gx, const double* gv, double* gx0, double* gv0,
+                                double* g_membran, double* g_biegung, k3d_adjoint_stats* stats);
+
 /* ---------------------------------------------------------------- no allocation
  * k3d_operator_noalloc has no counterpart in the reference. It is A p as
  * k3d_operator computes it (FP64, the scene's positions s->x), for a caller

@@ -2,8 +2,10 @@
 // (ImplizitCg::schritt, implizit.rs:899-1038), the check for the device
 // adjoint. The reference has no adjoint; this is derived from the forward
 // restatement in implizit.cpp with every discrete decision of the recorded
-// substep frozen: the contact set after the release pass, stick or slip, and
-// which bodies pushed a point out. Element and contact derivatives are taken
+// substep frozen: the contact set of the last solve and after the release
+// pass (a second release pass ends the loop, so points it releases keep
+// their constraint in dv but get no friction), stick or slip, and which
+// bodies pushed a point out. Element and contact derivatives are taken
 // by central differences of this oracle's own element and contact functions
 // (local to one element or point, so they are well conditioned), which keeps
 // the check independent of the device's forward-mode derivatives.
@@ -137,6 +139,7 @@ void ImplizitCg::adjoint_schritt(Szene& s, const Aufnahme& a, std::vector<V3>& x
   std::vector<std::optional<Fest>> fest0;
   System sys = system_bauen(s, h, fest0);
   const auto& fest = a.fest;
+  const auto& loes = a.fest_loes;
   // rho = A dv - b
   std::vector<V3> adv(n), rho(n);
   sys.mal_a(a.dv, adv);
@@ -222,7 +225,7 @@ void ImplizitCg::adjoint_schritt(Szene& s, const Aufnahme& a, std::vector<V3>& x
   adj.rhs = gg;
   adj.cg_toleranz = adj_toleranz;
   adj.cg_max = 100000;
-  std::vector<std::optional<Fest>> fa = fest;
+  std::vector<std::optional<Fest>> fa = loes;
   for (size_t i = 0; i < n; ++i)
     if (fa[i]) fa[i]->vn_soll = dot(a.v[i], fa[i]->normale);  // zero target
   if (lam.size() != n) lam.assign(n, V3{0, 0, 0});
@@ -242,14 +245,14 @@ void ImplizitCg::adjoint_schritt(Szene& s, const Aufnahme& a, std::vector<V3>& x
   for (size_t i = 0; i < n; ++i) {
     xo[i] = xa[i];
     vo[i] = add(va[i], sub(mul(mu[i], s.masse[i]), amu[i]));
-    if (!fest[i] || s.w[i] <= 0.0) continue;
-    const V3 nn = fest[i]->normale;
+    if (!loes[i] || s.w[i] <= 0.0) continue;
+    const V3 nn = loes[i]->normale;
     const double zeta = dot(nn, sub(gg[i], alam[i]));
     vo[i] = sub(vo[i], mul(nn, zeta));
     V3 nbar = nq[i];
     nbar = add(nbar, mul(lam[i], dot(nn, rho[i])));
     nbar = sub(nbar, mul(a.dv[i], zeta));
-    nbar = add(nbar, mul(sub(fest[i]->v_koerper, a.v[i]), zeta));
+    nbar = add(nbar, mul(sub(loes[i]->v_koerper, a.v[i]), zeta));
     // the build's contact: the last body in contact at x
     KontaktAbl ka, kl;
     bool hat = false;

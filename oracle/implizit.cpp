@@ -319,6 +319,7 @@ void ImplizitCg::schritt(Szene& s, double h, Aufnahme* auf) {
   std::vector<double> fn_kraft(n, 0.0);
   for (int durchgang = 0; durchgang < 2; ++durchgang) {
     CgLauf lauf = cpu_loese(sys, fest, dv);
+    if (auf) auf->fest_loes = fest;
     statistik.loesungen += 1;
     statistik.cg_iterationen += lauf.iterationen;
     statistik.rest_max = std::max(statistik.rest_max, lauf.rest);

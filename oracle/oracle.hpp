@@ -314,13 +314,14 @@ struct ImplizitStatistik {
   double rest_max = 0;
 };
 // Forward record of one substep, for the adjoint (no reference counterpart):
-// the state at the start, the final solution, the contact set after the
-// release pass, each held point's normal force and friction case, and per
-// point which bodies pushed it out after the move.
+// the state at the start, the final solution, the contact set of the last
+// solve and after the release pass, each held point's normal force and
+// friction case, and per point which bodies pushed it out after the move.
 struct Aufnahme {
   double h = 0;
   std::vector<V3> x, v, dv;
-  std::vector<std::optional<Fest>> fest;
+  std::vector<std::optional<Fest>> fest;       // after the release pass (friction)
+  std::vector<std::optional<Fest>> fest_loes;  // in the last solve (a second release pass ends the loop)
   std::vector<double> fn;
   std::vector<uint8_t> reib;    // held points: 1 stick, 2 slip
   std::vector<uint32_t> stoss;  // body b: bit 2b pushed out, bit 2b+1 inward normal velocity removed
