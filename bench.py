@@ -23,6 +23,9 @@ device-resident state with CUDA events around the step kernels, L2 flushed
 public API (ImplizitCg.bild) with x and v copied from pinned host memory to
 the device and back every step.
 
+``adjoint`` is the backward/forward time of the step's adjoint on the
+material-fit workload (see adjoint_leg), with its gradient check.
+
 Multi-GPU: the step of one drape does not shard (a global Krylov solve), so
 ``--gpus N`` runs N independent replicas, one per rank, with no collective on
 the data path; value = total vertex-steps / max over ranks of the time.
@@ -72,11 +75,84 @@ def args_():
                    help="profiling case: run this many mixed-form steps of the drop on cuda:0 and exit")
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="form used by --capture")
     p.add_argument("--no-batch", action="store_true", help="skip the batched-drape comparison")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (material-fit) leg")
     p.add_argument("--batch-steps", type=int, default=5)
     return p.parse_args()
 
 
 BATCH_PRE = 15  # free-fall steps of the batched drapes (0.1 m drop) before the timed window
+
+
+ADJ_N = 129        # material-fit sheet: 129 x 129 points
+ADJ_FRAMES = 120
+ADJ_K = 10         # checkpoint spacing (substeps)
+ADJ_FD_FRAMES = 40  # horizon of the gradient check: through first impact
+
+
+def adjoint_leg(torch):
+    """Backward/forward time of the adjoint on the material-fit workload:
+    a 129 x 129 sheet (16,641 points) dropped onto the sheet workload's
+    sphere (128^3 SDF at 1 cm), 120 frames, FP64 (the adjoint's form), PCG
+    tolerance 1e-5 as the main workload, checkpoints every 10 substeps.
+    Hidden parameters (warp, weft, shear, bend, grain) from the seed, the
+    target is the drop at them, the loss sum |x - x*|^2 at the start
+    parameters (hidden x U(0.5, 2)). backward = device time of
+    k3d_adjoint_backward, recomputation of the segments included; forward =
+    that of k3d_adjoint_forward (the frames with checkpoints).
+
+    Gradient check: the five parameter gradients against central differences
+    of the device forward (relative steps 1e-3 and 1e-4, PCG tolerance 1e-8)
+    over the first 40 frames, through first impact. Over the whole drop the
+    central differences do not converge as the step shrinks (contact and
+    friction decisions make the drop chaotic after impact), so the check
+    uses the horizon where they do."""
+    import numpy as np
+    from garmentcraft_b200 import _abi, synth
+    from garmentcraft_b200.adjoint import NAMEN, Drapierung, Stoff
+    from garmentcraft_b200.params import ImplizitParameter
+    s, hid, start = synth.materialfit(n=ADJ_N)
+    bs = Stoff.von(hid)
+    par = ImplizitParameter(schritte_je_bild=1, cg_max=CG_MAX, cg_toleranz=1e-5, precision=_abi.K3D_FP64)
+    d = Drapierung(s, bs, frames=ADJ_FRAMES, k=ADJ_K, param=par)
+    ziel, _ = d.vorwaerts(hid)
+    x, _ = d.vorwaerts(start)  # warm-up pass
+    d.rueckwaerts(2.0 * (x - ziel))
+    x, _ = d.vorwaerts(start)
+    fst = d.letzte["vorwaerts"]
+    g = d.rueckwaerts(2.0 * (x - ziel))
+    r = g["roh"]
+    out = {"workload": f"material fit: {ADJ_N}x{ADJ_N} sheet ({s.n} points) onto the sphere SDF, "
+                       f"{ADJ_FRAMES} frames, FP64, tol 1e-5",
+           "frames": ADJ_FRAMES, "checkpoint_every": ADJ_K, "forward_ms": r["ms_vorwaerts"],
+           "backward_ms": r["ms_rueckwaerts"], "recompute_ms": r["ms_neuberechnung"],
+           "backward_forward": r["ms_rueckwaerts"] / r["ms_vorwaerts"],
+           "forward_cg_iterations": fst.cg_iterationen, "adjoint_cg_iterations": r["iterationen"],
+           "adjoint_unconverged_solves": r["nicht_konvergiert"],
+           "definition": "device time of the backward (recomputation included) / device time of the forward"}
+    par2 = ImplizitParameter(schritte_je_bild=1, cg_max=20000, cg_toleranz=1e-8, precision=_abi.K3D_FP64)
+    d2 = Drapierung(s, bs, frames=ADJ_FD_FRAMES, k=ADJ_K, param=par2)
+    ziel2, _ = d2.vorwaerts(hid)
+
+    def loss(p):
+        xx, _ = d2.vorwaerts(p)
+        return float(np.sum((xx - ziel2) ** 2))
+
+    x2, _ = d2.vorwaerts(start)
+    g2 = d2.rueckwaerts(2.0 * (x2 - ziel2))["stoff"]
+    chk = {}
+    for q, name in enumerate(NAMEN):
+        fd = {}
+        for rel in (1e-3, 1e-4):
+            h = rel * abs(start[q])
+            pp, pm = start.copy(), start.copy()
+            pp[q] += h
+            pm[q] -= h
+            fd[f"{rel:g}"] = (loss(pp) - loss(pm)) / (2.0 * h)
+        errs = {k: abs(v - g2[q]) / abs(v) for k, v in fd.items()}
+        chk[name] = {"adjoint": float(g2[q]), "fd": fd, "rel_err": errs, "best_rel_err": min(errs.values())}
+    out["gradient_check"] = {"frames": ADJ_FD_FRAMES, "tol": 1e-8, "params": chk,
+                             "max_best_rel_err": max(c["best_rel_err"] for c in chk.values())}
+    return out
 
 
 def batch_leg(steps, flush, torch):
@@ -431,6 +507,8 @@ def main():
     line.update(extra)
     if world == 1 and not a.no_batch:
         line["batched"] = batch_leg(a.batch_steps, flush, torch)
+    if world == 1 and not a.no_adjoint:
+        line["adjoint"] = adjoint_leg(torch)
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_leg(a.n, a.warmup, a.cpu_seconds)
     if rank == 0:
