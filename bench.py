@@ -25,6 +25,8 @@ the device and back every step.
 
 ``adjoint`` is the backward/forward time of the step's adjoint on the
 material-fit workload (see adjoint_leg), with its gradient check.
+``garment`` is the same step on the ~205k-point sewn garment with the
+self-collision proximity stage on and off (see garment_leg).
 
 Multi-GPU: the step of one drape does not shard (a global Krylov solve), so
 ``--gpus N`` runs N independent replicas, one per rank, with no collective on
@@ -76,6 +78,7 @@ def args_():
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="form used by --capture")
     p.add_argument("--no-batch", action="store_true", help="skip the batched-drape comparison")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (material-fit) leg")
+    p.add_argument("--no-garment", action="store_true", help="skip the sewn-garment leg")
     p.add_argument("--batch-steps", type=int, default=5)
     return p.parse_args()
 
@@ -152,6 +155,49 @@ def adjoint_leg(torch):
         chk[name] = {"adjoint": float(g2[q]), "fd": fd, "rel_err": errs, "best_rel_err": min(errs.values())}
     out["gradient_check"] = {"frames": ADJ_FD_FRAMES, "tol": 1e-8, "params": chk,
                              "max_best_rel_err": max(c["best_rel_err"] for c in chk.values())}
+    return out
+
+
+GARMENT_PRE = 10    # untimed frames of the garment before its window
+GARMENT_STEPS = 5
+
+
+def garment_leg(flush, torch):
+    """The sewn-garment workload (synth.garment_szene: 28 panels, ~205k
+    points, 15-capsule body SDF 256x256x384 at 5 mm, latex, 2 mm collision
+    thickness, dt 1/120): frames GARMENT_PRE .. GARMENT_PRE + GARMENT_STEPS of
+    the drop, device-resident, L2 flushed before every timed frame, mixed
+    and FP64, with the self-collision proximity stage on (the workload) and
+    off (the step alone)."""
+    import numpy as np
+    from garmentcraft_b200 import _abi, synth
+    from garmentcraft_b200.implizit import ImplizitCg
+    from garmentcraft_b200.params import ImplizitParameter
+    s0, _ = synth.garment_szene()
+    out = {"workload": f"sewn garment: 28 panels, {s0.n} points, {s0.membran_punkte.shape[0]} membranes, "
+                       f"{s0.naht_punkte.shape[0]} seam pairs, 15-capsule SDF 256x256x384 at 5 mm",
+           "window": f"frames {GARMENT_PRE}-{GARMENT_PRE + GARMENT_STEPS}", "unit": UNIT}
+    for selbst in (True, False):
+        for prec, name in ((_abi.K3D_MIXED, "mixed"), (_abi.K3D_FP64, "fp64")):
+            s = s0.copy()
+            par = ImplizitParameter(schritte_je_bild=1, cg_max=CG_MAX, cg_toleranz=1e-5, precision=prec,
+                                    selbstkollision=selbst)
+            cg = ImplizitCg(par, device=torch.cuda.current_device())
+            cg.zustand_hochladen(s)
+            cg.bilder_auf_geraet(GARMENT_PRE)
+            ms, its, pairs = [], 0, 0
+            for k in range(GARMENT_STEPS):
+                flush.fill_(float(k))
+                torch.cuda.synchronize()
+                st = cg.bilder_auf_geraet(1)
+                ms.append(cg.letzte_bild_ms())
+                its += st.cg_iterationen
+                pairs += st.naehe_punkt_dreieck + st.naehe_kante_kante
+            key = f"{'selfcollision' if selbst else 'no_selfcollision'}_{name}"
+            out[key] = {"value": s.n * GARMENT_STEPS / (sum(ms) * 1e-3), "ms_per_step": float(np.mean(ms)),
+                        "cg_iterations_per_step": its / GARMENT_STEPS, "proximity_pairs_per_step": pairs / GARMENT_STEPS}
+    for tag in ("selfcollision", "no_selfcollision"):
+        out[f"{tag}_mixed_vs_fp64"] = out[f"{tag}_mixed"]["value"] / out[f"{tag}_fp64"]["value"]
     return out
 
 
@@ -509,6 +555,8 @@ def main():
         line["batched"] = batch_leg(a.batch_steps, flush, torch)
     if world == 1 and not a.no_adjoint:
         line["adjoint"] = adjoint_leg(torch)
+    if world == 1 and not a.no_garment:
+        line["garment"] = garment_leg(flush, torch)
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_leg(a.n, a.warmup, a.cpu_seconds)
     if rank == 0:

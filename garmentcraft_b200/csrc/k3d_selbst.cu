@@ -775,6 +775,12 @@ __global__ void __launch_bounds__(kT) inc_fill_kernel(const __grid_constant__ Se
 __global__ void __launch_bounds__(kT) inc_sort_kernel(const __grid_constant__ SelbstArgs s) {
   SC_FOR(i, s.n) sort_range(s.inc_ent, s.inc_off[i], s.inc_off[i + 1]);
 }
+// The inverse of the lists: each nonzero slot's entry index (the PCG writes a
+// pair's slot products there and sums them per point in list order).
+__global__ void __launch_bounds__(kT) inc_pos_kernel(const __grid_constant__ SelbstArgs s) {
+  const uint32_t E = s.inc_off[s.n] < s.cap_inc ? s.inc_off[s.n] : s.cap_inc;
+  SC_FOR(e, E) s.inc_pos[s.inc_ent[e]] = uint32_t(e);
+}
 
 // ------------------------------------------------------------ exclusive scan
 // Exclusive prefix sum of n uint32 in place, 1024 per block; block totals in
@@ -869,7 +875,7 @@ unsigned grid_for(int64_t work) {
 size_t selbst_scan_tmp_words(int64_t n) { return size_t((n + kScanChunk - 1) / kScanChunk) + 1; }
 // normals, boxes; 2 scans, fill, sort, count, 2 scans; fill, springs, damping,
 // count, scan, fill, sort
-int selbst_launches_per_run() { return 2 + (6 + 3 + 6) + (4 + 3 + 2); }
+int selbst_launches_per_run() { return 2 + (6 + 3 + 6) + (4 + 3 + 3); }
 
 // Part 1: normals, planes, boxes, bucket counts. The host has zeroed the
 // bucket-count arrays (anf_p, anf_k: eimer + 1 each) and the counters.
@@ -917,6 +923,7 @@ cudaError_t selbst_paare_und_federn(const SelbstArgs& s, cudaStream_t st) {
   if ((e = scan(s.inc_off, s.n + 1, s.scan_tmp, &s.zahl[SZ_INZIDENZ], st)) != cudaSuccess) return e;
   inc_fill_kernel<<<grid_for(pmax), kT, 0, st>>>(s);
   inc_sort_kernel<<<grid_for(s.n), kT, 0, st>>>(s);
+  inc_pos_kernel<<<grid_for(int64_t(s.cap_inc)), kT, 0, st>>>(s);
   return cudaGetLastError();
 }
 

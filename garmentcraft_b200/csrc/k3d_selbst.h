@@ -67,6 +67,8 @@ struct SelbstArgs {
   void* pr_wR;             // weights in operator precision, R4 per pair
   uint32_t *inc_off, *inc_cur, *inc_ent;  // per point: (pair << 2 | slot)
   uint32_t cap_inc;
+  uint32_t* inc_pos;  // per (pair << 2 | slot): its entry index, all ones for a zero weight
+  void* inc_out;      // per entry: the PCG's spring product of that slot, R4
   int32_t* slot_of;  // damping scratch per point: its shared-memory slot, -1 between batches
   uint32_t* zahl;    // SZ_COUNT counters
   uint32_t* scan_tmp;

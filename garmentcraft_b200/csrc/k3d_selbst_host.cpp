@@ -302,6 +302,10 @@ cudaError_t selbst_grow_pairs(SelbstHost& H, uint32_t cap) {
   char* wR = nullptr;
   if ((e = alloc(wR, size_t(cap) * 4 * size_t(s.rsize), H.pairs)) != cudaSuccess) return e;
   s.pr_wR = wR;
+  if ((e = alloc(s.inc_pos, size_t(s.cap_inc), H.pairs)) != cudaSuccess) return e;
+  char* out = nullptr;
+  if ((e = alloc(out, size_t(s.cap_inc) * 4 * size_t(s.rsize), H.pairs)) != cudaSuccess) return e;
+  s.inc_out = out;
   return alloc(s.inc_ent, size_t(s.cap_inc), H.pairs);
 }
 
@@ -342,6 +346,8 @@ cudaError_t selbst_run(SelbstHost& H, double h, cudaStream_t st, int& launches) 
   }
   if ((e = cudaMemsetAsync(s.inc_off, 0, sizeof(uint32_t) * (size_t(s.n) + 1), st)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(s.inc_cur, 0, sizeof(uint32_t) * size_t(s.n), st)) != cudaSuccess) return e;
+  if (paare > 0 && (e = cudaMemsetAsync(s.inc_pos, 0xff, sizeof(uint32_t) * 4 * size_t(paare), st)) != cudaSuccess)
+    return e;
   if ((e = selbst_paare_und_federn(s, st)) != cudaSuccess) return e;
   H.n_pt = z[SZ_PAARE_PT];
   H.n_kk = z[SZ_PAARE_KK];
@@ -354,10 +360,12 @@ cudaError_t selbst_run(SelbstHost& H, double h, cudaStream_t st, int& launches) 
 
 void selbst_step_args(const SelbstHost& H, StepArgs& a) {
   if (!H.on) {
-    a.sc_off = a.sc_ent = nullptr;
+    a.sc_off = a.sc_ent = a.sc_pos = nullptr;
     a.sc_idx = nullptr;
     a.sc_w = a.sc_kf = a.sc_b0 = a.sc_b1 = nullptr;
     a.sc_bR = a.sc_wR = nullptr;
+    a.sc_out = nullptr;
+    a.sc_np = 0;
     return;
   }
   const SelbstArgs& s = H.s;
@@ -370,6 +378,9 @@ void selbst_step_args(const SelbstHost& H, StepArgs& a) {
   a.sc_b1 = s.pr_b1;
   a.sc_bR = s.pr_bR;
   a.sc_wR = s.pr_wR;
+  a.sc_pos = s.inc_pos;
+  a.sc_out = s.inc_out;
+  a.sc_np = std::min<uint32_t>(H.n_pt + H.n_kk, s.cap_pairs);
 }
 
 }  // namespace k3d

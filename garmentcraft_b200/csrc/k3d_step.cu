@@ -415,7 +415,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       nxt[i].c = ci;
       R ax = 0, ay = 0, az = 0;
       if (a.frei[i]) {
-        bsr_row<R, SC>(a, cur, i, rb, ax, ay, az);
+        bsr_row<R, false>(a, cur, i, rb, ax, ay, az);
         filt<R>(vw.nrm, i, ax, ay, az);
         if (sizeof(R) == 4) {
           const double m = double(vw.md[i]);
@@ -426,6 +426,45 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       vw.ap[3 * i + 1] = ay;
       vw.ap[3 * i + 2] = az;
       ca[0] += double(ci.x) * double(ax) + double(ci.y) * double(ay) + double(ci.z) * double(az);
+    }
+    if (SC) {
+      // proximity springs pair by pair (implizit.rs:214-220): each nonzero
+      // slot's product goes to its entry; the update phase sums a point's
+      // entries in list order. c is filtered (pinned points hold 0), so the
+      // slot's share of c.A c is c_k.t_k.
+      const R4<R>* bR = static_cast<const R4<R>*>(a.sc_bR);
+      const R4<R>* wR = static_cast<const R4<R>*>(a.sc_wR);
+      R4<R>* out = static_cast<R4<R>*>(a.sc_out);
+      const int64_t nth = int64_t(sh.g.nblk) * blockDim.x;
+      for (int64_t q = int64_t(sh.bidx) * blockDim.x + threadIdx.x; q < int64_t(a.sc_np); q += nth) {
+        const uint4 id = a.sc_idx[q];
+        const R4<R> w4 = wR[q];
+        const R g[4] = {w4.x, w4.y, w4.z, w4.w};
+        const uint32_t ix[4] = {id.x, id.y, id.z, id.w};
+        R4<R> c[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) c[r] = next_dir<R>(cur[ix[r]], rb);
+        const R4<R> b0 = bR[2 * q], b1 = bR[2 * q + 1];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const uint32_t e = a.sc_pos[4 * q + k];
+          if (e == 0xffffffffu) continue;
+          R sx = 0, sy = 0, sz = 0;
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            if ((g[k] > R(0) && g[r] < R(0)) || (g[k] < R(0) && g[r] > R(0))) {
+              const R om = -g[k] * g[r];
+              sx += om * (c[k].x - c[r].x);
+              sy += om * (c[k].y - c[r].y);
+              sz += om * (c[k].z - c[r].z);
+            }
+          const R tx = b0.x * sx + b0.w * sy + b1.x * sz;
+          const R ty = b0.w * sx + b0.y * sy + b1.y * sz;
+          const R tz = b1.x * sx + b1.y * sy + b0.z * sz;
+          out[e] = {tx, ty, tz, R(0)};
+          ca[0] += double(c[k].x) * double(tx) + double(c[k].y) * double(ty) + double(c[k].z) * double(tz);
+        }
+      }
     }
     if (sizeof(R) == 4) {
       if (!grid_sync<2>(a, sh, ca)) return false;
@@ -446,9 +485,24 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       D3 d = ld3(a.dv, uint32_t(i));
       d = d + d3(double(ci.x), double(ci.y), double(ci.z)) * alpha;
       st3(a.dv, uint32_t(i), d);
-      const R rx = R(double(vw.r[3 * i]) - alpha * double(vw.ap[3 * i]));
-      const R ry = R(double(vw.r[3 * i + 1]) - alpha * double(vw.ap[3 * i + 1]));
-      const R rzz = R(double(vw.r[3 * i + 2]) - alpha * double(vw.ap[3 * i + 2]));
+      R apx = vw.ap[3 * i], apy = vw.ap[3 * i + 1], apz = vw.ap[3 * i + 2];
+      if (SC && a.frei[i]) {  // the point's proximity-spring entries, in list order
+        const R4<R>* out = static_cast<const R4<R>*>(a.sc_out);
+        R sx = 0, sy = 0, sz = 0;
+        for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
+          const R4<R> t = out[e];
+          sx += t.x;
+          sy += t.y;
+          sz += t.z;
+        }
+        filt<R>(vw.nrm, i, sx, sy, sz);
+        apx += sx;
+        apy += sy;
+        apz += sz;
+      }
+      const R rx = R(double(vw.r[3 * i]) - alpha * double(apx));
+      const R ry = R(double(vw.r[3 * i + 1]) - alpha * double(apy));
+      const R rzz = R(double(vw.r[3 * i + 2]) - alpha * double(apz));
       vw.r[3 * i] = rx;
       vw.r[3 * i + 1] = ry;
       vw.r[3 * i + 2] = rzz;

@@ -104,6 +104,12 @@ struct StepArgs {
   const uint4* sc_idx;
   const double4 *sc_w, *sc_kf, *sc_b0, *sc_b1;
   const void *sc_bR, *sc_wR;
+  // the PCG iteration's spring product pair by pair: each nonzero slot's
+  // entry index (sc_pos, per pair << 2 | slot) and the per-entry products
+  // (sc_out, R4), summed per point in list order; sc_np pairs
+  const uint32_t* sc_pos;
+  void* sc_out;
+  uint32_t sc_np;
   // probes
   const double* p_in;
   double* p_out;

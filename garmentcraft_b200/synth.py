@@ -223,6 +223,160 @@ def sheet_over_sphere(n: int = 257, groesse_m: float = 1.0, jitter_mm: float = 1
     return Muster([teil], [], param), body
 
 
+# ------------------------------------------------------------------ sewn garment
+def kapsel_sdf(segmente, dims, spacing_m: float, ursprung, band_m: float = 0.06):
+    """Signed distance of a union of capsules (segments (a, b, radius)) at the
+    nodes of a grid (x fastest), in float32: exact within ``band_m`` of each
+    capsule, ``band_m`` beyond (contact queries only read the values near the
+    surface). Returns a body dict."""
+    nx, ny, nz = dims
+    o = np.asarray(ursprung, dtype=np.float64)
+    out = np.full((nz, ny, nx), band_m, dtype=np.float32)
+    for a, b, r in segmente:
+        a = np.asarray(a, dtype=np.float64)
+        b = np.asarray(b, dtype=np.float64)
+        lo = np.floor((np.minimum(a, b) - r - band_m - o) / spacing_m).astype(int)
+        hi = np.ceil((np.maximum(a, b) + r + band_m - o) / spacing_m).astype(int) + 1
+        lo = np.maximum(lo, 0)
+        hi = np.minimum(hi, [nx, ny, nz])
+        if np.any(hi <= lo):
+            continue
+        zs = o[2] + spacing_m * np.arange(lo[2], hi[2])
+        ys = o[1] + spacing_m * np.arange(lo[1], hi[1])
+        xs = o[0] + spacing_m * np.arange(lo[0], hi[0])
+        gz, gy, gx = np.meshgrid(zs, ys, xs, indexing="ij")
+        p = np.stack([gx, gy, gz], axis=-1)
+        ab = b - a
+        t = np.clip(((p - a) @ ab) / float(ab @ ab), 0.0, 1.0)
+        d = np.linalg.norm(p - (a + t[..., None] * ab), axis=-1) - r
+        sub = out[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]]
+        np.minimum(sub, np.minimum(d, band_m).astype(np.float32), out=sub)
+    return dict(art=_abi.K3D_BODY_SDF_GRID, punkt=(0.0, 0.0, 0.0), dims=(nx, ny, nz), ursprung=tuple(ursprung),
+                spacing=spacing_m, sdf=np.ascontiguousarray(out.ravel()))
+
+
+# Body proxy: 15 capsules (a, b, radius), metres, z up, A-pose.
+KOERPER_KAPSELN = [
+    ((0.0, 0.0, 0.95), (0.0, 0.0, 1.08), 0.150),    # hips
+    ((0.0, 0.0, 1.08), (0.0, 0.0, 1.24), 0.125),    # waist
+    ((0.0, 0.0, 1.24), (0.0, 0.0, 1.40), 0.150),    # chest
+    ((0.0, 0.0, 1.44), (0.0, 0.0, 1.58), 0.055),    # neck
+    ((0.0, 0.0, 0.88), (0.0, 0.0, 0.95), 0.140),    # pelvis
+    ((0.09, 0.0, 0.86), (0.11, 0.0, 0.45), 0.075),  # thighs
+    ((-0.09, 0.0, 0.86), (-0.11, 0.0, 0.45), 0.075),
+    ((0.12, 0.0, 1.42), (0.22, 0.0, 1.40), 0.060),  # shoulders
+    ((-0.12, 0.0, 1.42), (-0.22, 0.0, 1.40), 0.060),
+    ((0.22, 0.0, 1.40), (0.38, 0.0, 1.16), 0.050),  # upper arms
+    ((-0.22, 0.0, 1.40), (-0.38, 0.0, 1.16), 0.050),
+    ((0.38, 0.0, 1.16), (0.50, 0.0, 0.92), 0.040),  # forearms
+    ((-0.38, 0.0, 1.16), (-0.50, 0.0, 0.92), 0.040),
+    ((0.50, 0.0, 0.92), (0.54, 0.0, 0.84), 0.035),  # hands
+    ((-0.50, 0.0, 0.92), (-0.54, 0.0, 0.84), 0.035),
+]
+
+
+def garment(seed: int = 0, ziel_punkte: int = 200_000, sdf: bool = True):
+    """The sewn-garment workload: 28 panels (rectangles or trapezoids, sides
+    10-60 cm) rolled on cylinders around a body proxy of 15 capsules, voxelised
+    into a 256 x 256 x 384 SDF at 5 mm. Tubes: 8 panels round the torso, 4
+    round each upper arm and each forearm, 4 round the neck; neighbouring
+    panels of a tube are sewn side to side (points paired at equal length
+    fractions), each upper sleeve to its forearm sleeve. Latex: E U(1.0, 1.5)
+    MPa per panel, G = E/2, 0.5 mm, 1000 kg/m^3, friction 0.4, collision
+    thickness 2 mm (the scene's kollisionsabstand), dt 1/120 s. The mesh
+    spacing is chosen so that the garment has about ``ziel_punkte`` points.
+    Returns (muster, body dict or None)."""
+    rng = np.random.default_rng(seed)
+    # tubes: (centre of the axis start, axis end, radius of the cloth, panels, height)
+    k = KOERPER_KAPSELN
+
+    def aermel(kap, ab):  # sleeve tube along a capsule, starting a fraction `ab` down it
+        a, b, r = np.asarray(kap[0]), np.asarray(kap[1]), kap[2]
+        return (a + ab * (b - a), b, r + 0.025, 4)
+
+    rohre = [((0.0, 0.0, 0.98), (0.0, 0.0, 1.30), 0.180, 8),                  # torso
+             aermel(k[9], 0.3), aermel(k[10], 0.3), aermel(k[11], 0.0), aermel(k[12], 0.0),
+             ((0.0, 0.0, 1.54), (0.0, 0.0, 1.62), 0.085, 4)]                   # collar
+    flaeche = 0.0
+    geo = []
+    for a, b, r, np_ in rohre:
+        a = np.asarray(a, dtype=np.float64)
+        b = np.asarray(b, dtype=np.float64)
+        hoehe = float(np.linalg.norm(b - a))
+        breite = 2.0 * math.pi * r / np_
+        # trapezoid: the panels of a tube share their height; the top edge
+        # is narrower or wider by up to 15 % (the tube becomes a cone)
+        konus = float(rng.uniform(-0.15, 0.15))
+        geo.append((a, b, r, np_, hoehe, breite, konus))
+        flaeche += np_ * hoehe * breite * (1.0 + 0.5 * konus)
+    h_mm = 1e3 * math.sqrt(flaeche / ziel_punkte)
+    teile, naehte = [], []
+    for ri, (a, b, r, np_, hoehe, breite, konus) in enumerate(geo):
+        achse = (b - a) / hoehe
+        e1 = np.cross(achse, [0.0, 1.0, 0.0])
+        if np.linalg.norm(e1) < 1e-6:
+            e1 = np.cross(achse, [1.0, 0.0, 0.0])
+        e1 /= np.linalg.norm(e1)
+        e2 = np.cross(achse, e1)
+        nx = max(int(round(breite * 1e3 / h_mm)), 2)
+        ny = max(int(round(hoehe * 1e3 / h_mm)), 2)
+        erst = len(teile)
+        for q in range(np_):
+            p, tri = rechteck_netz(breite * 1e3, hoehe * 1e3, nx, ny)
+            # trapezoid in the pattern plane: width scales with the height
+            sk = 1.0 + konus * p[:, 1] / (hoehe * 1e3)
+            p2 = np.stack([(p[:, 0] - 0.5 * breite * 1e3) * sk + 0.5 * breite * 1e3, p[:, 1]], axis=1)
+            E = float(rng.uniform(1.0e6, 1.5e6)) * 0.5e-3
+            mat = Material(dehnung_n_m=E, kette_n_m=E, schub_n_m=0.5 * E, biegung_nm=1e-7, biegung_kette_nm=1e-7,
+                           biegung_schraege_nm=1e-7, flaechengewicht_kg_m2=0.5, dicke_m=0.5e-3, reibung=0.4)
+            # roll onto the tube: the panel's u runs round the axis
+            u = p2[:, 0] * 1e-3 + q * breite
+            v = p2[:, 1] * 1e-3
+            rr = r * (1.0 + konus * v / hoehe)
+            w = u / r
+            lage = a + np.outer(v, achse) + (rr * np.cos(w))[:, None] * e1 + (rr * np.sin(w))[:, None] * e2
+            teile.append(Teil(p2, tri, (1.0, 0.0), mat, lage))
+        links = np.arange(ny + 1) * (nx + 1)
+        rechts = links + nx
+        for q in range(np_):
+            ta, tb = erst + q, erst + (q + 1) % np_
+            paare = np.stack([rechts, links], axis=1).astype(np.uint32)
+            naehte.append(Naht([Teilnaht(ta, tb, paare)], hoehe * 1e3, hoehe * 1e3))
+        geo[ri] = geo[ri] + (erst, nx, ny)
+    # each upper sleeve's far end (its top row) to the forearm sleeve's near
+    # end (bottom row), panel by panel; the shorter edge's points pair with
+    # the points at the same length fraction of the longer one
+    for ob, un in ((1, 3), (2, 4)):
+        _, _, _, np_a, _, _, _, ea, nxa, nya = geo[ob]
+        _, _, _, np_b, _, _, _, eb, nxb, nyb = geo[un]
+        oben = nya * (nxa + 1) + np.arange(nxa + 1)
+        unten = np.arange(nxb + 1)
+        if nxa <= nxb:
+            ib = np.rint(np.arange(nxa + 1) * (nxb / nxa)).astype(np.int64)
+            paare = np.stack([oben, unten[ib]], axis=1)
+        else:
+            ia = np.rint(np.arange(nxb + 1) * (nxa / nxb)).astype(np.int64)
+            paare = np.stack([oben[ia], unten], axis=1)
+        for q in range(min(np_a, np_b)):
+            naehte.append(Naht([Teilnaht(ea + q, eb + q, paare.astype(np.uint32))], 1.0, 1.0))
+    param = Simparameter(bild_dt=1.0 / 120.0, schwerkraft=(0.0, 0.0, -9.81), daempfung=0.0)
+    body = None
+    if sdf:
+        body = kapsel_sdf(KOERPER_KAPSELN, (256, 256, 384), 0.005, (-0.6375, -0.6375, 0.0))
+    return Muster(teile, naehte, param), body
+
+
+def garment_szene(seed: int = 0, ziel_punkte: int = 200_000, sdf: bool = True):
+    """The garment workload as a scene: ``garment`` built with the library's
+    scene builder, collision thickness 2 mm on every point. Returns (szene,
+    body dict or None)."""
+    from .implizit import build_scene
+    m, body = garment(seed, ziel_punkte, sdf)
+    s = build_scene(m, [body] if body is not None else [])
+    s.kollisionsabstand[:] = 2e-3
+    return s, body
+
+
 # ------------------------------------------------------------------ material fit
 def materialfit(n: int = 129, seed: int = 0):
     """The material-fit workload: an n x n sheet (1 x 1 m) dropped onto the
