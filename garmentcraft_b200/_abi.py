@@ -45,7 +45,9 @@ class K3dParams(C.Structure):
         ("precision", C.c_int32),
         ("selbst_zusatzdicke", C.c_double),
         ("selbst_steifigkeit", C.c_double),
-        ("reserved", C.c_int32 * 8),
+        ("selbst_stoss_iterationen", C.c_int32),
+        ("selbst_schnitte_an_naehten", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 

@@ -287,6 +287,8 @@ void k3d_params_default(k3d_params* o) {
   o->precision = K3D_FP64;
   o->selbst_zusatzdicke = 2.5e-3;
   o->selbst_steifigkeit = 1e-3;
+  o->selbst_stoss_iterationen = 1;
+  o->selbst_schnitte_an_naehten = 0;
 }
 
 void k3d_simparams_default(k3d_simparams* o) {

@@ -21,6 +21,8 @@ class ImplizitParameter:
     selbstkollision: bool = False
     selbst_zusatzdicke: float = 2.5e-3
     selbst_steifigkeit: float = 1e-3
+    selbst_stoss_iterationen: int = 1
+    selbst_schnitte_an_naehten: bool = False
     precision: int = _abi.K3D_FP64
 
     def to_c(self) -> _abi.K3dParams:
@@ -36,6 +38,8 @@ class ImplizitParameter:
         p.precision = self.precision
         p.selbst_zusatzdicke = self.selbst_zusatzdicke
         p.selbst_steifigkeit = self.selbst_steifigkeit
+        p.selbst_stoss_iterationen = self.selbst_stoss_iterationen
+        p.selbst_schnitte_an_naehten = int(self.selbst_schnitte_an_naehten)
         return p
 
 

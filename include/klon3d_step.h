@@ -56,7 +56,9 @@ typedef struct k3d_params {
   int32_t precision;            /* k3d_precision, default K3D_FP64 */
   double selbst_zusatzdicke;    /* default 2.5e-3 m */
   double selbst_steifigkeit;    /* default 1e-3 */
-  int32_t reserved[8];
+  int32_t selbst_stoss_iterationen;   /* impact response passes (implizit.rs:491), default 1 */
+  int32_t selbst_schnitte_an_naehten; /* edges through their seam partners' triangles count (:494), default 0 */
+  int32_t reserved[6];
 } k3d_params;
 
 /* Simparameter (sim/src/szene.rs:96-126), the part the implicit step reads. */

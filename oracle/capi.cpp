@@ -2,6 +2,7 @@
 // restatement, for tests/ and the CPU-baseline leg of bench.py (ctypes). The
 // scene and parameter structs reuse the public ABI layouts of
 // include/klon3d_step.h so both sides read the same inputs.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -191,6 +192,8 @@ ImplizitParameter param_aus(const k3d_params* p) {
   o.selbstkollision = p->selbstkollision != 0;
   o.selbst_zusatzdicke = p->selbst_zusatzdicke;
   o.selbst_steifigkeit = p->selbst_steifigkeit;
+  o.selbst_stoss_iterationen = size_t(std::max(p->selbst_stoss_iterationen, 0));
+  o.selbst_schnitte_an_naehten = p->selbst_schnitte_an_naehten != 0;
   return o;
 }
 
@@ -214,6 +217,9 @@ void stats_aus(const ImplizitStatistik& st, k3d_stats* out) {
   out->rest_max = st.rest_max;
   out->naehe_punkt_dreieck = int64_t(st.naehe_punkt_dreieck);
   out->naehe_kante_kante = int64_t(st.naehe_kante_kante);
+  out->selbst_stoesse = int64_t(st.selbst_stoesse);
+  out->durchdringungen = int64_t(st.durchdringungen);
+  out->durchdringungsgebiete = int64_t(st.durchdringungsgebiete);
 }
 
 }  // namespace
@@ -324,6 +330,50 @@ void* orc_sim_create(const k3d_scene* s, const k3d_params* p) {
 }
 void orc_sim_free(void* h) { delete static_cast<Sim*>(h); }
 
+// Impacts on the way x0 -> x1 of a small mesh (triangles, or with nt == 0
+// the edges alone) and their response (selbstkollision.rs:1196-1343); x1 is
+// updated. Writes per impact (art, zeit, seite) up to cap; returns the number
+// of impacts, *antworten the response's count.
+int64_t orc_stoesse(int64_t np, const double* x0, double* x1, const double* w, const double* masse, int64_t nt,
+                    const uint32_t* tris, int64_t ne, const uint32_t* kanten, int32_t pd, int32_t kk,
+                    int32_t iterationen, double* out3, int64_t cap, int64_t* antworten) {
+  std::vector<std::array<uint32_t, 3>> d(static_cast<size_t>(nt));
+  for (int64_t t = 0; t < nt; ++t) d[size_t(t)] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+  Stoffnetz netz = stoffnetz_neu(d, std::vector<double>(static_cast<size_t>(np), 1e-3));
+  if (nt == 0)
+    for (int64_t e = 0; e < ne; ++e) netz.kanten.push_back({kanten[2 * e], kanten[2 * e + 1]});
+  std::vector<V3> a(static_cast<size_t>(np)), b(static_cast<size_t>(np));
+  std::vector<double> wv(w, w + np), mv(masse, masse + np);
+  for (int64_t i = 0; i < np; ++i)
+    for (int k = 0; k < 3; ++k) {
+      a[size_t(i)][k] = x0[3 * i + k];
+      b[size_t(i)][k] = x1[3 * i + k];
+    }
+  std::vector<Stoss> st = finde_stoesse(netz, a, b, wv, pd != 0, kk != 0);
+  for (size_t q = 0; q < st.size() && int64_t(q) < cap; ++q) {
+    out3[3 * q] = st[q].art == Art::PunktDreieck ? 0.0 : 1.0;
+    out3[3 * q + 1] = st[q].zeit;
+    out3[3 * q + 2] = st[q].seite;
+  }
+  size_t z = stossantwort(st, b, mv, wv, size_t(std::max(iterationen, 0)));
+  for (int64_t i = 0; i < np; ++i)
+    for (int k = 0; k < 3; ++k) x1[3 * i + k] = b[size_t(i)][k];
+  if (antworten) *antworten = int64_t(z);
+  return int64_t(st.size());
+}
+
+// finde_schnitte (selbstkollision.rs:858) at the simulation's current state,
+// with the scene's cloth tables (aus_szene, zusatzdicke 2.5 mm); writes the
+// region roots (gebiete) up to cap; returns the number of intersections.
+int64_t orc_sim_schnitte(void* h, int32_t an_naehten, int64_t cap, int64_t* wurzeln) {
+  auto* sim = static_cast<Sim*>(h);
+  auto nw = aus_szene(sim->s, 2.5e-3);
+  std::vector<Schnitt> schn = finde_schnitte(nw.first, sim->s.x, an_naehten != 0);
+  std::vector<size_t> r = gebiete(nw.first, schn);
+  for (size_t q = 0; q < r.size() && int64_t(q) < cap; ++q) wurzeln[q] = int64_t(r[q]);
+  return int64_t(schn.size());
+}
+
 // Adjoint of n frames (adjoint.cpp): runs the frames from the current state,
 // recording every substep, then goes back through them. gx, gv: cotangents of
 // the final x, v (3 per point); out: those of the initial x, v, and per
@@ -374,6 +424,9 @@ void orc_sim_frames(void* h, int32_t n, k3d_stats* st) {
     summe.rest_max = std::max(summe.rest_max, b.rest_max);
     summe.naehe_punkt_dreieck += b.naehe_punkt_dreieck;
     summe.naehe_kante_kante += b.naehe_kante_kante;
+    summe.selbst_stoesse += b.selbst_stoesse;
+    summe.durchdringungen += b.durchdringungen;
+    summe.durchdringungsgebiete += b.durchdringungsgebiete;
   }
   stats_aus(summe, st);
 }

@@ -196,6 +196,35 @@ System ImplizitCg::system_bauen(Szene& s, double h, std::vector<std::optional<Fe
         statistik.naehe_kante_kante += 1;
     }
     fed = federn(netz, werte, naehe, param.selbst_steifigkeit, s.masse, s.w, s.naht.ruhe, s.v);
+    // implizit.rs:692-707: edges through triangles, their regions, push
+    // springs; a region is switched off where the body holds the edge side and
+    // the triangle side from opposite directions
+    std::vector<Schnitt> schn = finde_schnitte(netz, s.x, param.selbst_schnitte_an_naehten);
+    std::vector<size_t> wurzeln = gebiete(netz, schn);
+    statistik.durchdringungen += schn.size();
+    for (size_t i = 0; i < wurzeln.size(); ++i)
+      if (wurzeln[i] == i) statistik.durchdringungsgebiete += 1;
+    const double rand = param.kontakt_rand;
+    auto normale = [&](uint32_t i) -> std::optional<V3> {
+      for (const auto& kb : s.koerper) {
+        auto kt = kb.kontakt(s.x[i], s.kollisionsabstand[i] + rand);
+        if (kt) return kt->normale;
+      }
+      return std::nullopt;
+    };
+    auto eingeklemmt = [&](std::array<uint32_t, 2> kp, std::array<uint32_t, 3> dp) {
+      V3 summe{0, 0, 0};
+      for (uint32_t i : dp)
+        if (auto nk = normale(i)) summe = add(summe, *nk);
+      if (!(norm(summe) > 0.0)) return false;
+      for (uint32_t i : kp)
+        if (auto nk = normale(i))
+          if (dot(*nk, summe) < 0.0) return true;
+      return false;
+    };
+    std::vector<Feder> schub = schubfedern(netz, werte, schn, wurzeln, param.selbst_steifigkeit, folge, eingeklemmt);
+    fed.insert(fed.end(), schub.begin(), schub.end());
+    schnitte = std::move(schn);
   }
   std::vector<V3> f(n), last(n);
   for (size_t i = 0; i < n; ++i) {
@@ -305,6 +334,7 @@ System ImplizitCg::system_bauen(Szene& s, double h, std::vector<std::optional<Fe
 void ImplizitCg::schritt(Szene& s, double h, Aufnahme* auf) {
   const size_t n = s.x.size();
   const V3 g = s.param.schwerkraft;
+  const std::vector<V3> x_anfang = param.selbstkollision ? s.x : std::vector<V3>();
   if (auf) {
     auf->h = h;
     auf->x = s.x;
@@ -381,6 +411,19 @@ void ImplizitCg::schritt(Szene& s, double h, Aufnahme* auf) {
         if (vn < 0.0) s.v[i] = sub(s.v[i], mul(kt->normale, vn));
         if (auf) auf->stoss[i] |= (1u << (2 * kb)) | (vn < 0.0 ? 1u << (2 * kb + 1) : 0u);
       }
+    }
+  }
+  // implizit.rs:1027-1037: the way x_anfang -> x, impacts between parts that
+  // do not already interpenetrate, position response; held points count as
+  // heavy (x 1e9)
+  if (param.selbstkollision && selbst) {
+    const Stoffnetz& netz = selbst->first;
+    std::vector<Stoss> st = finde_stoesse(netz, x_anfang, s.x, s.w, true, true);
+    st = ohne_durchdrungene(netz, std::move(st), schnitte);
+    if (!st.empty()) {
+      std::vector<double> m_eff(n);
+      for (size_t i = 0; i < n; ++i) m_eff[i] = fest[i] ? s.masse[i] * 1e9 : s.masse[i];
+      statistik.selbst_stoesse += stossantwort(st, s.x, m_eff, s.w, param.selbst_stoss_iterationen);
     }
   }
 }

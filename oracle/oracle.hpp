@@ -16,6 +16,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <optional>
 #include <set>
@@ -255,6 +256,34 @@ struct Feder {
   V3 kraft{};
   M3 block{};
 };
+// selbstkollision.rs:810-826, 1092-1114: an edge through a triangle; an impact
+struct Schnitt {
+  uint32_t kante = 0, dreieck = 0;
+  double t = 0;
+  std::array<double, 3> w{};
+  V3 richtung{};
+  double gewicht = 0;
+};
+struct Stoss {
+  Art art = Art::PunktDreieck;
+  std::array<uint32_t, 4> punkte{};
+  std::array<double, 2> lage{};
+  double zeit = 0, seite = 0;
+  V3 normale{};
+};
+constexpr double STOSS_ABSTAND = 1e-4, STOSS_KANTE_MIN = 1e-4, SCHUB_HEBEL = 1e-3;
+constexpr uint32_t FOLGE_MAX = 5;
+std::vector<Schnitt> finde_schnitte(const Stoffnetz& netz, const std::vector<V3>& x, bool an_naehten);
+std::vector<size_t> gebiete(const Stoffnetz& netz, std::vector<Schnitt>& schnitte);
+std::vector<Stoss> finde_stoesse(const Stoffnetz& netz, const std::vector<V3>& x0, const std::vector<V3>& x1,
+                                 const std::vector<double>& w, bool pd, bool kk);
+std::vector<Stoss> ohne_durchdrungene(const Stoffnetz& netz, std::vector<Stoss> stoesse,
+                                      const std::vector<Schnitt>& schnitte);
+size_t stossantwort(const std::vector<Stoss>& stoesse, std::vector<V3>& x, const std::vector<double>& masse,
+                    const std::vector<double>& w, size_t iterationen);
+std::vector<Feder> schubfedern(const Stoffnetz& netz, const Stoffwerte& werte, const std::vector<Schnitt>& schnitte,
+                               const std::vector<size_t>& wurzeln, double steifigkeit, std::vector<uint32_t>& folge,
+                               const std::function<bool(std::array<uint32_t, 2>, std::array<uint32_t, 3>)>& eingeklemmt);
 std::vector<Feder> federn(const Stoffnetz& netz, const Stoffwerte& werte, const std::vector<Naehe>& naehe,
                           double steifigkeit, const std::vector<double>& masse, const std::vector<double>& w,
                           const std::vector<double>& naht_ruhe, std::vector<V3>& v);
@@ -306,9 +335,12 @@ struct ImplizitParameter {
   bool selbstkollision = false;  // proximity stage only (selbstkollision.rs:387-788)
   double selbst_zusatzdicke = 2.5e-3;
   double selbst_steifigkeit = 1e-3;
+  size_t selbst_stoss_iterationen = 1;      // implizit.rs:491, 525
+  bool selbst_schnitte_an_naehten = false;  // implizit.rs:494, 526
 };
 // sim/src/implizit.rs:535-561
 struct ImplizitStatistik {
+  size_t selbst_stoesse = 0, durchdringungen = 0, durchdringungsgebiete = 0;
   size_t cg_iterationen = 0, loesungen = 0, nicht_konvergiert = 0, kontakte = 0, haftend = 0,
          freigegeben = 0, durchstoesse = 0, koerperpunkte = 0, naehe_punkt_dreieck = 0, naehe_kante_kante = 0;
   double rest_max = 0;
@@ -343,6 +375,8 @@ struct ImplizitCg {
   ImplizitStatistik statistik;
   std::vector<V3> dv_vorher;
   std::optional<std::pair<Stoffnetz, Stoffwerte>> selbst;
+  std::vector<uint32_t> folge;     // per triangle: steps in a row with an edge through it
+  std::vector<Schnitt> schnitte;   // of the last system build
   System system_bauen(Szene& s, double h, std::vector<std::optional<Fest>>& fest);
   void schritt(Szene& s, double h, Aufnahme* auf = nullptr);
   void bild(Szene& s, std::vector<Aufnahme>* auf = nullptr);

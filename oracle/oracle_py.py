@@ -46,6 +46,12 @@ def lib():
     L.orc_sim_free.argtypes = [P]
     L.orc_sim_frames.argtypes = [P, C.c_int32, C.POINTER(_abi.K3dStats)]
     L.orc_sim_adjoint.argtypes = [P, C.c_int32, dp, dp, dp, dp, dp, dp, C.c_double, C.POINTER(C.c_int64)]
+    up = C.POINTER(C.c_uint32)
+    L.orc_stoesse.argtypes = [C.c_int64, dp, dp, dp, dp, C.c_int64, up, C.c_int64, up, C.c_int32, C.c_int32,
+                              C.c_int32, dp, C.c_int64, C.POINTER(C.c_int64)]
+    L.orc_stoesse.restype = C.c_int64
+    L.orc_sim_schnitte.argtypes = [P, C.c_int32, C.c_int64, C.POINTER(C.c_int64)]
+    L.orc_sim_schnitte.restype = C.c_int64
     L.orc_sim_get_state.argtypes = [P, dp, dp]
     L.orc_sim_set_state.argtypes = [P, dp, dp]
     L.orc_sim_set_naht_ruhe.argtypes = [P, dp]
@@ -172,6 +178,15 @@ class OracleSim:
         it = C.c_int64(0)
         self.L.orc_sim_adjoint(self.h, n, _d(gx), _d(gv), _d(ox), _d(ov), _d(gm), _d(gb), toleranz, C.byref(it))
         return dict(x=ox, v=ov, membran=gm, biegung=gb, iterationen=int(it.value))
+
+    def schnitte(self, an_naehten: bool = True):
+        """finde_schnitte and gebiete at the current state: the region root of
+        each intersection (selbstkollision.rs:858-1009)."""
+        cap = 1 << 20
+        r = np.zeros(cap, dtype=np.int64)
+        n = self.L.orc_sim_schnitte(self.h, int(an_naehten), cap,
+                                    r.ctypes.data_as(C.POINTER(C.c_int64)))
+        return r[:n]
 
     def state(self):
         x = np.zeros((self.n, 3))
@@ -317,3 +332,21 @@ class SelbstProbe:
         self.L.orc_selbst_federn(self.sim.h, _d(x), _d(vv), n, pk.ctypes.data_as(C.POINTER(C.c_uint32)), _d(gw),
                                  _d(kr), _d(bl))
         return dict(punkte=pk[:n], gewichte=gw[:n], kraft=kr[:n], block=bl[:n]), vv
+
+
+def stoesse(x0, x1, w, masse, dreiecke=None, kanten=None, pd=True, kk=True, iterationen=1):
+    """finde_stoesse and stossantwort on a small mesh (oracle): returns
+    (impacts as rows (art, zeit, seite), responses, x1 after the response)."""
+    L = lib()
+    x0 = f64(x0)
+    x1 = f64(x1).copy()
+    w = f64(w)
+    m = f64(masse)
+    tri = np.ascontiguousarray(np.zeros((0, 3)) if dreiecke is None else dreiecke, dtype=np.uint32)
+    ka = np.ascontiguousarray(np.zeros((0, 2)) if kanten is None else kanten, dtype=np.uint32)
+    out = np.zeros((64, 3))
+    z = C.c_int64(0)
+    up = C.POINTER(C.c_uint32)
+    n = L.orc_stoesse(x0.shape[0], _d(x0), _d(x1), _d(w), _d(m), tri.shape[0], tri.ctypes.data_as(up),
+                      ka.shape[0], ka.ctypes.data_as(up), int(pd), int(kk), iterationen, _d(out), 64, C.byref(z))
+    return out[:n], int(z.value), x1

@@ -6,6 +6,7 @@
 // order with the reference's bits. The penetration regions and the impact
 // stage (selbstkollision.rs:813-1343) are not restated.
 #include <algorithm>
+#include <cfloat>
 #include <limits>
 
 #include "oracle.hpp"
@@ -581,6 +582,427 @@ std::vector<Feder> federn(const Stoffnetz& netz, const Stoffwerte& werte, const 
     aus.push_back(fe);
   }
   return aus;
+}
+
+// ============================================================ response stages
+// selbstkollision.rs:810-1350: edges through triangles, their regions and
+// push springs; impacts on the way x0 -> x1 and their position response.
+namespace {
+// selbstkollision.rs:1116-1122
+double ebenenabstand(V3 a, V3 b, V3 c, V3 p) { return dot(sub(p, a), einheit(cross(sub(b, a), sub(c, a)))); }
+V3 lerp(V3 a, V3 b, double t) { return add(mul(a, 1.0 - t), mul(b, t)); }
+// selbstkollision.rs:1156-1171
+std::optional<std::array<double, 2>> im_dreieck(V3 a, V3 b, V3 c, V3 p) {
+  V3 e1 = sub(b, a), e2 = sub(c, a), r = sub(p, a);
+  double d11 = dot(e1, e1), d12 = dot(e1, e2), d22 = dot(e2, e2);
+  double det = d11 * d22 - d12 * d12;
+  if (det <= 1e-4 * d11 * d22) return std::nullopt;
+  double r1 = dot(r, e1), r2 = dot(r, e2);
+  double u = (d22 * r1 - d12 * r2) / det;
+  double v = (d11 * r2 - d12 * r1) / det;
+  if (u < 0.0 || v < 0.0 || u + v > 1.0) return std::nullopt;
+  return std::array<double, 2>{u, v};
+}
+// selbstkollision.rs:830-846
+std::optional<std::pair<double, std::array<double, 3>>> kante_durch_dreieck(V3 a, V3 b, const std::array<V3, 3>& v,
+                                                                             V3 n) {
+  double d0 = dot(n, sub(a, v[0])), d1 = dot(n, sub(b, v[0]));
+  if ((d0 > 0.0 && d1 > 0.0) || (d0 < 0.0 && d1 < 0.0) || std::abs(d1 - d0) < 1e-12) return std::nullopt;
+  double t = -d0 / (d1 - d0);
+  if (std::abs(t) < 1e-5 || std::abs(t - 1.0) < 1e-5) return std::nullopt;
+  V3 p = lerp(a, b, t);
+  V3 e1 = sub(v[1], v[0]), e2 = sub(v[2], v[0]);
+  if (norm(e1) < STOSS_KANTE_MIN || norm(e2) < STOSS_KANTE_MIN) return std::nullopt;
+  auto uv = im_dreieck(v[0], v[1], v[2], p);
+  if (!uv) return std::nullopt;
+  return std::make_pair(t, std::array<double, 3>{1.0 - (*uv)[0] - (*uv)[1], (*uv)[0], (*uv)[1]});
+}
+// selbstkollision.rs:1128-1153 (regula falsi on the plane distance)
+std::optional<double> koplanar_zeit(const std::array<V3, 4>& x0, const std::array<V3, 4>& x1, double tol) {
+  auto f = [&](double t) {
+    std::array<V3, 4> q;
+    for (int k = 0; k < 4; ++k) q[k] = lerp(x0[k], x1[k], t);
+    return ebenenabstand(q[0], q[1], q[2], q[3]);
+  };
+  double t0 = 0.0, t1 = 1.0, d0 = f(0.0), d1 = f(1.0);
+  for (int it = 0; it < 16; ++it) {
+    if (d0 * d1 > 0.0) return std::nullopt;
+    double tau = t0 + (t1 - t0) * std::abs(d0) / std::max(std::abs(d0) + std::abs(d1), DBL_MIN);
+    double d = f(tau);
+    if (std::abs(d) < tol || t1 - t0 < 1e-4) return tau;
+    if (d0 * d > 0.0) {
+      t0 = tau;
+      d0 = d;
+    } else {
+      t1 = tau;
+      d1 = d;
+    }
+  }
+  return std::nullopt;
+}
+// selbstkollision.rs:1173-1193
+std::optional<std::array<double, 2>> kanten_kreuzen(V3 a, V3 b, V3 c, V3 d) {
+  V3 e1 = sub(b, a), e2 = sub(d, c);
+  double l1 = norm(e1), l2 = norm(e2);
+  if (l1 < STOSS_KANTE_MIN || l2 < STOSS_KANTE_MIN) return std::nullopt;
+  V3 u1 = mul(e1, 1.0 / l1), u2 = mul(e2, 1.0 / l2);
+  double g = dot(u1, u2);
+  if (std::abs(g) > 0.99999) return std::nullopt;
+  V3 q = sub(c, a);
+  double nen = 1.0 - g * g;
+  double s = (dot(q, u1) - g * dot(q, u2)) / nen;
+  double w = (g * dot(q, u1) - dot(q, u2)) / nen;
+  if (s <= 0.0 || s >= l1 || w <= 0.0 || w >= l2) return std::nullopt;
+  return std::array<double, 2>{s / l1, w / l2};
+}
+// selbstkollision.rs:910-925 (union-find with path halving; root = the smallest index)
+size_t wurzel(std::vector<size_t>& eltern, size_t i) {
+  while (eltern[i] != i) {
+    eltern[i] = eltern[eltern[i]];
+    i = eltern[i];
+  }
+  return i;
+}
+void vereinige(std::vector<size_t>& eltern, size_t a, size_t b) {
+  size_t ra = wurzel(eltern, a), rb = wurzel(eltern, b);
+  if (ra != rb) eltern[std::max(ra, rb)] = std::min(ra, rb);
+}
+}  // namespace
+
+// selbstkollision.rs:858-907
+std::vector<Schnitt> finde_schnitte(const Stoffnetz& netz, const std::vector<V3>& x, bool an_naehten) {
+  Normalen nrm = normalen_neu(netz, x);
+  std::vector<Quader> qt(netz.dreiecke.size());
+  for (size_t t = 0; t < qt.size(); ++t) {
+    V3 p[3] = {x[netz.dreiecke[t][0]], x[netz.dreiecke[t][1]], x[netz.dreiecke[t][2]]};
+    qt[t] = quader_punkte(p, 3, ZUSCHLAG_QUADER);
+  }
+  double laenge = 0.0;
+  for (const auto& k : netz.kanten) laenge = std::fmax(laenge, norm(sub(x[k[0]], x[k[1]])));
+  Hashgitter gitter = hashgitter_neu(qt, std::fmax(laenge, 1e-3));
+  std::vector<Schnitt> aus;
+  for (size_t e = 0; e < netz.kanten.size(); ++e) {
+    uint32_t a0 = netz.kanten[e][0], a1 = netz.kanten[e][1];
+    const auto& kd = netz.kanten_dreiecke[e];
+    if (a0 == a1 || kd[0] == KEIN) continue;
+    V3 pa = x[a0], pb = x[a1];
+    V3 pe[2] = {pa, pb};
+    Quader qe = quader_punkte(pe, 2, ZUSCHLAG_QUADER);
+    V3 ehat = einheit(sub(pb, pa));
+    je_eintrag(gitter, qe, [&](uint32_t t, std::array<int64_t, 3> c) {
+      const auto& d = netz.dreiecke[t];
+      bool nachbar = false;
+      for (uint32_t i : d)
+        nachbar = nachbar || (an_naehten ? (i == a0 || i == a1)
+                                         : (netz.gleich_oder_partner(a0, i) || netz.gleich_oder_partner(a1, i)));
+      if (nachbar || !ueberlappt(qt[t], qe) || !erste_zelle(qe, qt[t], gitter.zelle, c)) return;
+      V3 n = nrm.dreieck[t];
+      auto kd_t = kante_durch_dreieck(pa, pb, {x[d[0]], x[d[1]], x[d[2]]}, n);
+      if (!kd_t) return;
+      double cn = dot(n, ehat);
+      if (std::abs(cn) < 1e-6) return;
+      V3 p = lerp(pa, pb, kd_t->first);
+      V3 g{0, 0, 0};
+      for (uint32_t k : kd) {
+        if (k == KEIN) continue;
+        const auto& dk = netz.dreiecke[k];
+        uint32_t o = KEIN;
+        for (uint32_t i : dk)
+          if (i != a0 && i != a1) {
+            o = i;
+            break;
+          }
+        if (o == KEIN) continue;
+        V3 m = einheit(cross(n, nrm.dreieck[k]));
+        V3 r = sub(x[o], p);
+        V3 r_quer = sub(r, mul(ehat, dot(ehat, r)));
+        if (dot(m, r_quer) < 0.0) m = mul(m, -1.0);
+        g = add(g, sub(m, mul(n, dot(ehat, m) / cn)));
+      }
+      double lg = norm(g);
+      aus.push_back(Schnitt{uint32_t(e), t, kd_t->first, kd_t->second, einheit(g), lg / std::sqrt(lg * lg + 2.25)});
+    });
+  }
+  return aus;
+}
+
+// selbstkollision.rs:931-1009
+std::vector<size_t> gebiete(const Stoffnetz& netz, std::vector<Schnitt>& schnitte) {
+  const size_t n = schnitte.size();
+  std::map<std::pair<uint32_t, uint32_t>, size_t> index;
+  for (size_t i = 0; i < n; ++i) index.emplace(std::make_pair(schnitte[i].kante, schnitte[i].dreieck), i);
+  auto finde = [&](uint32_t e, uint32_t t, std::vector<size_t>& out) {
+    auto it = index.find({e, t});
+    if (it != index.end()) out.push_back(it->second);
+  };
+  auto nachbardreiecke = [&](uint32_t t) {
+    std::vector<uint32_t> v;
+    for (uint32_t k : netz.dreieck_kanten[t])
+      for (uint32_t u : netz.kanten_dreiecke[k])
+        if (u != KEIN && u != t) v.push_back(u);
+    return v;
+  };
+  std::vector<size_t> eltern(n);
+  for (size_t i = 0; i < n; ++i) eltern[i] = i;
+  std::vector<std::pair<size_t, size_t>> tausch;
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t e = schnitte[i].kante, t = schnitte[i].dreieck;
+    std::vector<uint32_t> kde;
+    for (uint32_t k : netz.kanten_dreiecke[e])
+      if (k != KEIN) kde.push_back(k);
+    std::vector<uint32_t> andere;
+    for (uint32_t k : kde)
+      for (uint32_t f : netz.dreieck_kanten[k])
+        if (f != e) andere.push_back(f);
+    std::vector<uint32_t> tn = nachbardreiecke(t);
+    std::vector<size_t> gleich;
+    for (uint32_t f : andere) finde(f, t, gleich);
+    for (uint32_t u : tn) {
+      finde(e, u, gleich);
+      for (uint32_t f : andere) finde(f, u, gleich);
+    }
+    for (size_t j : gleich) vereinige(eltern, i, j);
+    for (uint32_t f : netz.dreieck_kanten[t])
+      for (uint32_t k : kde) {
+        std::vector<size_t> j;
+        finde(f, k, j);
+        if (!j.empty()) tausch.push_back({i, j[0]});
+      }
+  }
+  for (int runde = 0; runde < 2; ++runde) {
+    std::vector<size_t> partner(n, SIZE_MAX);
+    for (auto [i, j] : tausch) {
+      size_t ri = wurzel(eltern, i), rj = wurzel(eltern, j);
+      partner[ri] = std::min(partner[ri], rj);
+      partner[rj] = std::min(partner[rj], ri);
+    }
+    for (auto [i, j] : tausch) {
+      size_t rj = wurzel(eltern, j);
+      if (partner[rj] != SIZE_MAX) vereinige(eltern, i, partner[rj]);
+    }
+  }
+  std::vector<size_t> wurzeln(n);
+  for (size_t i = 0; i < n; ++i) wurzeln[i] = wurzel(eltern, i);
+  std::vector<V3> summe(n, V3{0, 0, 0});
+  for (size_t i = 0; i < n; ++i) summe[wurzeln[i]] = add(summe[wurzeln[i]], mul(schnitte[i].richtung, schnitte[i].gewicht));
+  for (size_t i = 0; i < n; ++i) schnitte[i].richtung = einheit(summe[wurzeln[i]]);
+  return wurzeln;
+}
+
+// selbstkollision.rs:1014-1058
+std::vector<Feder> schubfedern(const Stoffnetz& netz, const Stoffwerte& werte, const std::vector<Schnitt>& schnitte,
+                               const std::vector<size_t>& wurzeln, double steifigkeit, std::vector<uint32_t>& folge,
+                               const std::function<bool(std::array<uint32_t, 2>, std::array<uint32_t, 3>)>& eingeklemmt) {
+  if (folge.size() != netz.dreiecke.size()) folge.assign(netz.dreiecke.size(), 1u);
+  std::vector<uint8_t> hat(netz.dreiecke.size(), 0), klemm(schnitte.size(), 0);
+  for (size_t i = 0; i < schnitte.size(); ++i) {
+    hat[schnitte[i].dreieck] = 1;
+    if (eingeklemmt(netz.kanten[schnitte[i].kante], netz.dreiecke[schnitte[i].dreieck])) klemm[wurzeln[i]] = 1;
+  }
+  for (size_t t = 0; t < folge.size(); ++t) folge[t] = hat[t] ? folge[t] + 1 : 1u;
+  std::vector<Feder> aus;
+  for (size_t i = 0; i < schnitte.size(); ++i) {
+    if (klemm[wurzeln[i]]) continue;
+    const Schnitt& s = schnitte[i];
+    size_t e = s.kante, t = s.dreieck;
+    double k = 2.0 * steifigkeit * (werte.e_kante[e] + werte.e_dreieck[t]) * (werte.a_kante[e] + werte.a_dreieck[t]) / 1e-6;
+    V3 g = s.richtung;
+    Feder f;
+    f.kraft = mul(g, k * double(std::min(folge[t], FOLGE_MAX)) * SCHUB_HEBEL);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) f.block[a][b] = k * g[a] * g[b];
+    f.punkte = {netz.kanten[e][0], netz.kanten[e][1], netz.dreiecke[t][0], netz.dreiecke[t][1], netz.dreiecke[t][2]};
+    f.gewichte = {1.0 - s.t, s.t, -s.w[0], -s.w[1], -s.w[2]};
+    aus.push_back(f);
+  }
+  return aus;
+}
+
+// selbstkollision.rs:1063-1084
+std::vector<Stoss> ohne_durchdrungene(const Stoffnetz& netz, std::vector<Stoss> stoesse,
+                                      const std::vector<Schnitt>& schnitte) {
+  if (schnitte.empty()) return stoesse;
+  std::set<std::pair<uint32_t, uint32_t>> paare;
+  for (const auto& s : schnitte) paare.insert({s.kante, s.dreieck});
+  std::vector<Stoss> aus;
+  for (const auto& st : stoesse) {
+    bool weg = false;
+    if (st.art == Art::PunktDreieck) {
+      uint32_t t = uint32_t(dreieck_von(netz, &st.punkte[1]));
+      for (const auto& s : schnitte)
+        if (s.dreieck == t && (netz.kanten[s.kante][0] == st.punkte[0] || netz.kanten[s.kante][1] == st.punkte[0]))
+          weg = true;
+    } else {
+      size_t i = kante_von(netz, st.punkte[0], st.punkte[1]), j = kante_von(netz, st.punkte[2], st.punkte[3]);
+      auto trifft = [&](size_t a, size_t b) {
+        for (uint32_t t : netz.kanten_dreiecke[b]) {
+          if (t == KEIN) continue;
+          const auto& dk = netz.dreieck_kanten[t];
+          if (paare.count({uint32_t(a), t}) && (dk[0] == b || dk[1] == b || dk[2] == b)) return true;
+        }
+        return false;
+      };
+      weg = trifft(i, j) || trifft(j, i);
+    }
+    if (!weg) aus.push_back(st);
+  }
+  return aus;
+}
+
+// selbstkollision.rs:1196-1285
+std::vector<Stoss> finde_stoesse(const Stoffnetz& netz, const std::vector<V3>& x0, const std::vector<V3>& x1,
+                                 const std::vector<double>& w, bool pd, bool kk) {
+  std::vector<Stoss> aus;
+  auto weg = [&](const uint32_t* idx, int m) {
+    V3 p[8];
+    for (int k = 0; k < m; ++k) {
+      p[k] = x0[idx[k]];
+      p[m + k] = x1[idx[k]];
+    }
+    return quader_punkte(p, 2 * m, 1e-8);
+  };
+  double laenge = 0.0;
+  for (const auto& k : netz.kanten) laenge = std::fmax(laenge, norm(sub(x1[k[0]], x1[k[1]])));
+  const double zelle = std::fmax(laenge, 1e-3);
+  auto bew = [](const std::array<V3, 4>& a0, const std::array<V3, 4>& a1, int k) { return sub(a1[k], a0[k]); };
+  if (pd) {
+    std::vector<Quader> qp(x0.size());
+    for (uint32_t v = 0; v < qp.size(); ++v) qp[v] = weg(&v, 1);
+    Hashgitter gitter = hashgitter_neu(qp, zelle);
+    for (const auto& d : netz.dreiecke) {
+      if (d[0] == d[1] || d[1] == d[2] || d[0] == d[2]) continue;
+      Quader qt = weg(d.data(), 3);
+      std::optional<Stoss> best;
+      je_eintrag(gitter, qt, [&](uint32_t v, std::array<int64_t, 3> c) {
+        bool nb = false;
+        for (uint32_t i : d) nb = nb || netz.gleich_oder_partner(v, i);
+        if (nb || !ueberlappt(qp[v], qt) || !erste_zelle(qt, qp[v], zelle, c)) return;
+        std::array<uint32_t, 4> idx = {d[0], d[1], d[2], v};
+        bool alle_fest = true;
+        for (uint32_t i : idx) alle_fest = alle_fest && w[i] <= 0.0;
+        if (alle_fest) return;
+        std::array<V3, 4> a0, a1;
+        for (int k = 0; k < 4; ++k) {
+          a0[k] = x0[idx[k]];
+          a1[k] = x1[idx[k]];
+        }
+        auto zeit = koplanar_zeit(a0, a1, STOSS_ABSTAND * 0.1);
+        if (!zeit) return;
+        if (best && best->zeit <= *zeit) return;
+        std::array<V3, 4> q;
+        for (int k = 0; k < 4; ++k) q[k] = lerp(a0[k], a1[k], *zeit);
+        auto uv = im_dreieck(q[0], q[1], q[2], q[3]);
+        if (!uv) return;
+        V3 n = einheit(cross(sub(q[1], q[0]), sub(q[2], q[0])));
+        double g[3] = {1.0 - (*uv)[0] - (*uv)[1], (*uv)[0], (*uv)[1]};
+        V3 rel = sub(bew(a0, a1, 3), add(add(mul(bew(a0, a1, 0), g[0]), mul(bew(a0, a1, 1), g[1])), mul(bew(a0, a1, 2), g[2])));
+        double seite = dot(rel, n) <= 0.0 ? 1.0 : -1.0;
+        best = Stoss{Art::PunktDreieck, {v, d[0], d[1], d[2]}, *uv, *zeit, seite, mul(n, seite)};
+      });
+      if (best) aus.push_back(*best);
+    }
+  }
+  if (kk) {
+    std::vector<Quader> qk(netz.kanten.size());
+    for (size_t e = 0; e < qk.size(); ++e) qk[e] = weg(netz.kanten[e].data(), 2);
+    Hashgitter gitter = hashgitter_neu(qk, zelle);
+    for (size_t i = 0; i < netz.kanten.size(); ++i) {
+      uint32_t i0 = netz.kanten[i][0], i1 = netz.kanten[i][1];
+      if (i0 == i1) continue;
+      std::optional<Stoss> best;
+      je_eintrag(gitter, qk[i], [&](uint32_t jj, std::array<int64_t, 3> c) {
+        size_t j = jj;
+        if (j <= i || !ueberlappt(qk[i], qk[j]) || !erste_zelle(qk[i], qk[j], zelle, c)) return;
+        uint32_t j0 = netz.kanten[j][0], j1 = netz.kanten[j][1];
+        for (uint32_t q : {j0, j1})
+          if (netz.gleich_oder_partner(q, i0) || netz.gleich_oder_partner(q, i1)) return;
+        std::array<uint32_t, 4> idx = {i1, j0, j1, i0};
+        bool alle_fest = true;
+        for (uint32_t k : idx) alle_fest = alle_fest && w[k] <= 0.0;
+        if (alle_fest) return;
+        std::array<V3, 4> a0, a1;
+        for (int k = 0; k < 4; ++k) {
+          a0[k] = x0[idx[k]];
+          a1[k] = x1[idx[k]];
+        }
+        auto zeit = koplanar_zeit(a0, a1, STOSS_ABSTAND * 0.1);
+        if (!zeit) return;
+        if (best && best->zeit <= *zeit) return;
+        std::array<V3, 4> q;
+        for (int k = 0; k < 4; ++k) q[k] = lerp(a0[k], a1[k], *zeit);
+        auto sw = kanten_kreuzen(q[3], q[0], q[1], q[2]);
+        if (!sw) return;
+        V3 n = einheit(cross(sub(q[0], q[3]), sub(q[2], q[1])));
+        V3 auf_i = add(mul(bew(a0, a1, 3), 1.0 - (*sw)[0]), mul(bew(a0, a1, 0), (*sw)[0]));
+        V3 auf_j = add(mul(bew(a0, a1, 1), 1.0 - (*sw)[1]), mul(bew(a0, a1, 2), (*sw)[1]));
+        double seite = dot(sub(auf_i, auf_j), n) <= 0.0 ? 1.0 : -1.0;
+        best = Stoss{Art::KanteKante, {i0, i1, j0, j1}, *sw, *zeit, seite, mul(n, seite)};
+      });
+      if (best) aus.push_back(*best);
+    }
+  }
+  return aus;
+}
+
+// selbstkollision.rs:1288-1343
+size_t stossantwort(const std::vector<Stoss>& stoesse, std::vector<V3>& x, const std::vector<double>& masse,
+                    const std::vector<double>& w, size_t iterationen) {
+  size_t zahl = 0;
+  for (size_t it = 0; it < iterationen; ++it) {
+    std::vector<V3> dx(x.size(), V3{0, 0, 0});
+    std::vector<uint32_t> cnt(x.size(), 0);
+    for (const auto& s : stoesse) {
+      size_t p0 = s.punkte[0], p1 = s.punkte[1], p2 = s.punkte[2], p3 = s.punkte[3];
+      std::vector<std::pair<size_t, double>> erste, zweite;
+      V3 n;
+      double d;
+      if (s.art == Art::PunktDreieck) {
+        n = mul(einheit(cross(sub(x[p2], x[p1]), sub(x[p3], x[p1]))), s.seite);
+        double g0 = 1.0 - s.lage[0] - s.lage[1];
+        erste = {{p0, 1.0}};
+        zweite = {{p1, g0}, {p2, s.lage[0]}, {p3, s.lage[1]}};
+        d = dot(n, sub(x[p0], x[p1]));
+      } else {
+        n = s.normale;
+        V3 a = lerp(x[p0], x[p1], s.lage[0]), b = lerp(x[p2], x[p3], s.lage[1]);
+        erste = {{p0, 1.0 - s.lage[0]}, {p1, s.lage[0]}};
+        zweite = {{p2, 1.0 - s.lage[1]}, {p3, s.lage[1]}};
+        d = dot(n, sub(a, b));
+      }
+      double tief = STOSS_ABSTAND - d;
+      if (tief <= 0.0) continue;
+      double m1 = 0.0, m2 = 0.0;
+      bool fest1 = true, fest2 = true;
+      for (auto [i, g] : erste) {
+        m1 += g * masse[i];
+        fest1 = fest1 && w[i] <= 0.0;
+      }
+      for (auto [i, g] : zweite) {
+        m2 += g * masse[i];
+        fest2 = fest2 && w[i] <= 0.0;
+      }
+      double alpha = fest2 ? 1.0 : (fest1 ? 0.0 : m2 / (m1 + m2));
+      for (auto [i, g] : erste)
+        if (w[i] > 0.0) {
+          dx[i] = add(dx[i], mul(n, tief * alpha));
+          cnt[i] += 1;
+        }
+      for (auto [i, g] : zweite)
+        if (w[i] > 0.0) {
+          dx[i] = sub(dx[i], mul(n, tief * (1.0 - alpha)));
+          cnt[i] += 1;
+        }
+      zahl += 1;
+    }
+    bool bewegt = false;
+    for (size_t i = 0; i < x.size(); ++i)
+      if (cnt[i] > 0) {
+        x[i] = add(x[i], mul(dx[i], 1.0 / double(cnt[i])));
+        bewegt = true;
+      }
+    if (!bewegt) break;
+  }
+  return zahl;
 }
 
 }  // namespace orc

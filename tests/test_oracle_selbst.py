@@ -11,6 +11,7 @@ import numpy as np
 
 import oracle_py as O
 from garmentcraft_b200 import synth
+from garmentcraft_b200.implizit import build_scene
 from garmentcraft_b200.params import ImplizitParameter
 
 
@@ -144,3 +145,49 @@ def test_federn_impuls():
     # force along the normal, k (mu I + (1 - mu) n n^T) blocks are symmetric
     assert np.allclose(fe["block"], np.transpose(fe["block"], (0, 2, 1)), rtol=0, atol=0)
     assert np.all(fe["gewichte"][:, 4] == 0.0) and np.array_equal(fe["punkte"][:, 4], fe["punkte"][:, 0])
+
+
+# ---------------------------------------------------------------- response stages
+def test_punkt_durch_dreieck():
+    """selbstkollision.rs:1400-1416: a point falls 4 mm through a level,
+    held triangle in one step: one impact at time 0.5 from above; the
+    response sets it 0.1 mm above the plane and leaves the triangle."""
+    x0 = np.array([[0.0, 0.0, 0.0], [0.02, 0.0, 0.0], [0.0, 0.02, 0.0], [0.005, 0.005, 0.002]])
+    x1 = x0.copy()
+    x1[3, 2] = -0.002
+    st, n, x = O.stoesse(x0, x1, [0.0, 0.0, 0.0, 1.0], [1e-5] * 4, dreiecke=[[0, 1, 2]])
+    assert st.shape[0] == 1
+    assert abs(st[0, 1] - 0.5) < 1e-6 and st[0, 2] == 1.0
+    assert n == 1
+    assert abs(x[3, 2] - 1e-4) < 1e-12
+    assert np.array_equal(x[0], x0[0])
+
+
+def test_kante_durch_kante():
+    """selbstkollision.rs:1418-1430: two edges cross in one step; the moving
+    edge comes back to 0.1 mm in front of the held one."""
+    x0 = np.array([[-0.01, 0.0, 0.001], [0.01, 0.0, 0.001], [0.0, -0.01, 0.0], [0.0, 0.01, 0.0]])
+    x1 = x0.copy()
+    x1[0, 2] = -0.001
+    x1[1, 2] = -0.001
+    st, n, x = O.stoesse(x0, x1, [1.0, 1.0, 0.0, 0.0], [1e-5] * 4, kanten=[[0, 1], [2, 3]], pd=False, kk=True)
+    assert st.shape[0] == 1
+    assert abs(x[0, 2] - 1e-4) < 1e-12 and abs(x[1, 2] - 1e-4) < 1e-12
+
+
+def test_schraege_lage_loest_sich():
+    """sim/tests/selbstkollision.rs:69-95: the upper layer starts tilted
+    through the lower one (z from -5 mm to +15 mm over 20 cm); more than 10
+    edges pierce the other layer at the start, none after 3 s (90 frames at
+    1/30 s, default parameters with self-collision). Regular 10 mm grids stand
+    in for the mesher; the upper piece is inset and shifted so that the line
+    where it crosses the lower one does not run along its grid points (an
+    edge with an end in the other layer's plane does not count as piercing)."""
+    m = synth.zwei_lagen(abstand_m=-0.005, neigung=0.1, **INSET)
+    s = build_scene(m)
+    synth.pin_teil(s, 0)
+    o = O.OracleSim(s, ImplizitParameter(selbstkollision=True).to_c())
+    anfang = o.schnitte(an_naehten=True)
+    assert anfang.shape[0] > 10
+    o.frames(90)
+    assert o.schnitte(an_naehten=True).shape[0] == 0
