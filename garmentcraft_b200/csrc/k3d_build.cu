@@ -216,10 +216,10 @@ __device__ void build_points(const StepArgs& a, const View<R>& vw, double& held)
     if (a.sc_off) {  // proximity springs: force, -h H v, diagonal (implizit.rs:798-805, 887-894)
       for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
         const uint32_t ent = a.sc_ent[e];
-        const double4 kf = a.sc_kf[ent >> 2];
-        const double4 g4 = a.sc_w[ent >> 2];
-        const uint32_t k = ent & 3u;
-        const double g = k == 0 ? g4.x : k == 1 ? g4.y : k == 2 ? g4.z : g4.w;
+        const double4 kf = a.sc_kf[ent >> 3];
+        const double4 g4 = a.sc_w[ent >> 3];
+        const uint32_t k = ent & 7u;
+        const double g = k == 0 ? g4.x : k == 1 ? g4.y : k == 2 ? g4.z : k == 3 ? g4.w : a.sc_g5[ent >> 3];
         acc = acc + d3(kf.x, kf.y, kf.z) * g;
       }
       const D3 hv = feder_hp64(a, i, [&](uint32_t j) { return ld3(a.v, j); }, D);

@@ -811,7 +811,17 @@ static k3d_status launch(k3d_solver* h, int mode, double t_bodies, bool need_loa
   StepArgs& a = h->a;
   step_args(h, mode, t_bodies, need_load);
   int launched = 0;
-  if (h->sc.on) {  // proximity pairs and springs before the system (implizit.rs:668-691)
+  if (h->sc.on) {  // proximity pairs, regions and springs before the system (implizit.rs:668-707)
+    SelbstArgs& ss = h->sc.s;
+    ss.n_bodies = a.n_bodies;
+    ss.kabst = a.kabst;
+    ss.rand = a.kontakt_rand;
+    ss.an_naehten = h->p.selbst_schnitte_an_naehten;
+    if (a.n_bodies > 0)
+      K3D_CUDA(h, cudaMemcpyAsync(h->sc.bodies_dev, a.bodies, sizeof(Body) * size_t(a.n_bodies),
+                                  cudaMemcpyHostToDevice, h->stream));
+    if (mode == MODE_STEP)  // the way the impact stage checks starts here (implizit.rs:903)
+      K3D_CUDA(h, cudaMemcpyAsync(h->sc.x0, a.x, 24 * size_t(h->n), cudaMemcpyDeviceToDevice, h->stream));
     cudaError_t es = selbst_run(h->sc, a.h, h->stream, launched);
     if (es != cudaSuccess) return cuda_fail(h, es, "self-collision stage");
   }
@@ -819,6 +829,12 @@ static k3d_status launch(k3d_solver* h, int mode, double t_bodies, bool need_loa
   cudaError_t e = launch_step(a, h->p.precision == K3D_MIXED ? 1 : 0, h->blocks, h->stream, launched);
   h->launches += launched;
   if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
+  if (h->sc.on && mode == MODE_STEP) {  // cloth against cloth on the way (implizit.rs:1027-1037)
+    int ls = 0;
+    cudaError_t es = selbst_stoss_run(h->sc, a.x, a.nrm_d, std::max(h->p.selbst_stoss_iterationen, 0), h->stream, ls);
+    h->launches += ls;
+    if (es != cudaSuccess) return cuda_fail(h, es, "self-collision impact stage");
+  }
   if (mode == MODE_STEP) h->first_step = false;
   return K3D_OK;
 }
@@ -862,6 +878,13 @@ static k3d_status read_stats(k3d_solver* h, k3d_stats* out) {
     out->dv_max = rm[1];
     out->naehe_punkt_dreieck = int64_t(h->sc.naehe_pt);
     out->naehe_kante_kante = int64_t(h->sc.naehe_kk);
+    if (h->sc.on) {
+      unsigned long long acc[3];
+      K3D_CUDA(h, cudaMemcpy(acc, h->sc.acc, sizeof(acc), cudaMemcpyDeviceToHost));
+      out->selbst_stoesse = int64_t(acc[0]);
+      out->durchdringungen = int64_t(acc[1]);
+      out->durchdringungsgebiete = int64_t(acc[2]);
+    }
   }
   if (st[ST_NONFINITE] > 0) return fail(h, K3D_NON_FINITE, "non-finite position or velocity after the step");
   return K3D_OK;
@@ -869,6 +892,7 @@ static k3d_status read_stats(k3d_solver* h, k3d_stats* out) {
 
 static k3d_status reset_stats(k3d_solver* h) {
   h->sc.naehe_pt = h->sc.naehe_kk = 0;
+  if (h->sc.on) K3D_CUDA(h, cudaMemsetAsync(h->sc.acc, 0, 3 * sizeof(unsigned long long), h->stream));
   K3D_CUDA(h, cudaMemsetAsync(h->a.stats, 0, sizeof(long long) * ST_COUNT, h->stream));
   K3D_CUDA(h, cudaMemsetAsync(h->a.stat_rest_max, 0, sizeof(double) * 2, h->stream));
   return K3D_OK;

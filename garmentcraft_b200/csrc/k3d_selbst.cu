@@ -13,6 +13,7 @@
 //   triangle (point-triangle) and per edge (edge-edge)    -> host reads sizes
 //   pairs written in the reference's order; springs per pair; the approach
 //   damping in pair order; per-point incidence lists (pair, slot)
+#include <cfloat>
 #include <cstdint>
 
 #include "k3d_device.cuh"
@@ -515,6 +516,12 @@ __device__ __forceinline__ uint32_t paare(const SelbstArgs& s) {
   const uint64_t p = uint64_t(s.zahl[SZ_PAARE_PT]) + s.zahl[SZ_PAARE_KK];
   return p < s.cap_pairs ? uint32_t(p) : s.cap_pairs;
 }
+// all springs: the proximity pairs, then the push springs
+__device__ __forceinline__ uint32_t federn_alle(const SelbstArgs& s) {
+  const uint32_t ns = s.zahl[SZ_SCHNITTE] < s.cap_s ? s.zahl[SZ_SCHNITTE] : s.cap_s;
+  const uint64_t p = uint64_t(s.zahl[SZ_PAARE_PT]) + s.zahl[SZ_PAARE_KK] + ns;
+  return p < s.cap_pairs ? uint32_t(p) : s.cap_pairs;
+}
 
 // Spring of each pair (selbstkollision.rs:715-752, 779-785) without the
 // approach damping: stiffness, rest (seam override), force, block; and the
@@ -597,6 +604,9 @@ __global__ void __launch_bounds__(kT) federn_kernel(const __grid_constant__ Selb
     bR[2 * q] = {R(h2 * bxx), R(h2 * byy), R(h2 * bzz), R(h2 * bxy)};
     bR[2 * q + 1] = {R(h2 * bxz), R(h2 * byz), R(0), R(0)};
     wR[q] = {R(gw[0]), R(gw[1]), R(gw[2]), R(gw[3])};
+    s.pr_x5[q] = kKein;
+    s.pr_g5[q] = 0.0;
+    static_cast<R*>(s.pr_g5R)[q] = R(0);
   }
 }
 
@@ -746,9 +756,9 @@ __global__ void __launch_bounds__(kDB, 1) daempfung_kernel(const __grid_constant
   }
 }
 
-// Per-point incidence lists of the pairs' nonzero slots, ascending.
+// Per-point incidence lists of the springs' nonzero slots, ascending.
 __global__ void __launch_bounds__(kT) inc_count_kernel(const __grid_constant__ SelbstArgs s) {
-  const uint32_t P = paare(s);
+  const uint32_t P = federn_alle(s);
   SC_FOR(q, P) {
     const uint4 id = s.pr_idx[q];
     const double4 g = s.pr_w[q];
@@ -756,19 +766,20 @@ __global__ void __launch_bounds__(kT) inc_count_kernel(const __grid_constant__ S
     if (g.y != 0.0) atomicAdd(&s.inc_off[id.y], 1u);
     if (g.z != 0.0) atomicAdd(&s.inc_off[id.z], 1u);
     if (g.w != 0.0) atomicAdd(&s.inc_off[id.w], 1u);
+    if (s.pr_g5[q] != 0.0) atomicAdd(&s.inc_off[s.pr_x5[q]], 1u);
   }
 }
 __global__ void __launch_bounds__(kT) inc_fill_kernel(const __grid_constant__ SelbstArgs s) {
-  const uint32_t P = paare(s);
+  const uint32_t P = federn_alle(s);
   SC_FOR(q, P) {
     const uint4 id = s.pr_idx[q];
     const double4 g = s.pr_w[q];
-    const uint32_t pts[4] = {id.x, id.y, id.z, id.w};
-    const double gw[4] = {g.x, g.y, g.z, g.w};
-    for (int k = 0; k < 4; ++k) {
+    const uint32_t pts[5] = {id.x, id.y, id.z, id.w, s.pr_x5[q]};
+    const double gw[5] = {g.x, g.y, g.z, g.w, s.pr_g5[q]};
+    for (int k = 0; k < 5; ++k) {
       if (gw[k] == 0.0) continue;
       const uint32_t pos = s.inc_off[pts[k]] + atomicAdd(&s.inc_cur[pts[k]], 1u);
-      if (pos < s.cap_inc) s.inc_ent[pos] = (uint32_t(q) << 2) | uint32_t(k);
+      if (pos < s.cap_inc) s.inc_ent[pos] = (uint32_t(q) << 3) | uint32_t(k);
     }
   }
 }
@@ -776,7 +787,7 @@ __global__ void __launch_bounds__(kT) inc_sort_kernel(const __grid_constant__ Se
   SC_FOR(i, s.n) sort_range(s.inc_ent, s.inc_off[i], s.inc_off[i + 1]);
 }
 // The inverse of the lists: each nonzero slot's entry index (the PCG writes a
-// pair's slot products there and sums them per point in list order).
+// spring's slot products there and sums them per point in list order).
 __global__ void __launch_bounds__(kT) inc_pos_kernel(const __grid_constant__ SelbstArgs s) {
   const uint32_t E = s.inc_off[s.n] < s.cap_inc ? s.inc_off[s.n] : s.cap_inc;
   SC_FOR(e, E) s.inc_pos[s.inc_ent[e]] = uint32_t(e);
@@ -870,12 +881,753 @@ unsigned grid_for(int64_t work) {
   return unsigned(b);
 }
 
+
+// ============================================================ penetration regions
+// selbstkollision.rs:810-1058: edges through triangles (a hash of triangle
+// boxes with the longest edge as cell), their regions (the reference's
+// union-find, one thread), the push springs after the proximity pairs.
+
+// the longest edge at positions x (atomicMax on the bits of a non-negative double)
+__global__ void __launch_bounds__(kT) kante_max_kernel(const __grid_constant__ SelbstArgs s, const double* x,
+                                                       unsigned long long* out) {
+  double m = 0.0;
+  SC_FOR(e, s.ne) {
+    const uint2 k = s.k_idx[e];
+    m = fmax(m, norm(ld3(x, k.x) - ld3(x, k.y)));
+  }
+  if (m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+__device__ __forceinline__ double zelle_aus(const unsigned long long* lm) {
+  return fmax(__longlong_as_double((long long)*lm), 1e-3);
+}
+
+// Hashgitter::neu over the boxes of g with the cell in *lm (selbstkollision.rs:281-322):
+// distinct buckets per box counted, then (after a scan) filled, then sorted.
+__global__ void __launch_bounds__(kT) hg_count_kernel(const HashG g, const unsigned long long* lm, uint32_t* zahl) {
+  const double z = zelle_aus(lm);
+  SC_FOR(b, g.m) {
+    const Box q = box_of(g.lo, g.hi, b);
+    uint32_t c = 0;
+    je_eimer(q, z, g.eimer, [&](uint32_t h) {
+      atomicAdd(&g.anf[h], 1u);
+      ++c;
+    });
+    if (c) atomicAdd(zahl, c);
+  }
+}
+__global__ void __launch_bounds__(kT) hg_fill_kernel(const HashG g, const unsigned long long* lm) {
+  const double z = zelle_aus(lm);
+  SC_FOR(b, g.m) {
+    const Box q = box_of(g.lo, g.hi, b);
+    je_eimer(q, z, g.eimer, [&](uint32_t h) {
+      const uint32_t pos = g.anf[h] + atomicAdd(&g.cur[h], 1u);
+      if (pos < g.cap) g.ein[pos] = uint32_t(b);
+    });
+  }
+}
+__global__ void __launch_bounds__(kT) hg_sort_kernel(const HashG g) {
+  SC_FOR(b, g.eimer) sort_range(g.ein, g.anf[b], g.anf[b + 1]);
+}
+
+// triangle boxes of the intersection search (selbstkollision.rs:860)
+__global__ void __launch_bounds__(kT) schnitt_boxen_kernel(const __grid_constant__ SelbstArgs s) {
+  SC_FOR(t, s.nd) {
+    const uint4 d = s.d_idx[t];
+    const D3 p[3] = {ld3(s.x, d.x), ld3(s.x, d.y), ld3(s.x, d.z)};
+    const Box b = quader_punkte(p, 3, kZuschlagQuader);
+    s.hs.lo[t] = make_double4(b.lo.x, b.lo.y, b.lo.z, 0.0);
+    s.hs.hi[t] = make_double4(b.hi.x, b.hi.y, b.hi.z, 0.0);
+  }
+}
+
+__device__ __forceinline__ D3 lerp3(D3 a, D3 b, double t) { return a * (1.0 - t) + b * t; }
+// selbstkollision.rs:1156-1171
+__device__ bool im_dreieck(D3 a, D3 b, D3 c, D3 p, double& u, double& v) {
+  const D3 e1 = b - a, e2 = c - a, r = p - a;
+  const double d11 = dot(e1, e1), d12 = dot(e1, e2), d22 = dot(e2, e2);
+  const double det = d11 * d22 - d12 * d12;
+  if (det <= 1e-4 * d11 * d22) return false;
+  const double r1 = dot(r, e1), r2 = dot(r, e2);
+  u = (d22 * r1 - d12 * r2) / det;
+  v = (d11 * r2 - d12 * r1) / det;
+  return !(u < 0.0 || v < 0.0 || u + v > 1.0);
+}
+// selbstkollision.rs:830-846
+__device__ bool kante_durch_dreieck(D3 a, D3 b, D3 v0, D3 v1, D3 v2, D3 n, double& t, double w[3]) {
+  const double d0 = dot(n, a - v0), d1 = dot(n, b - v0);
+  if ((d0 > 0.0 && d1 > 0.0) || (d0 < 0.0 && d1 < 0.0) || fabs(d1 - d0) < 1e-12) return false;
+  t = -d0 / (d1 - d0);
+  if (fabs(t) < 1e-5 || fabs(t - 1.0) < 1e-5) return false;
+  const D3 p = lerp3(a, b, t);
+  if (norm(v1 - v0) < kKanteMin || norm(v2 - v0) < kKanteMin) return false;
+  double u, v;
+  if (!im_dreieck(v0, v1, v2, p, u, v)) return false;
+  w[0] = 1.0 - u - v;
+  w[1] = u;
+  w[2] = v;
+  return true;
+}
+
+// The intersections of edge e (selbstkollision.rs:866-903), counted or
+// written from `pos` on in the reference's order.
+template <bool FILL>
+__device__ uint32_t kante_schnitte(const SelbstArgs& s, int64_t e, uint32_t pos, double zelle) {
+  const uint2 ka = s.k_idx[e];
+  const uint2 kd = s.k_dr[e];
+  const uint32_t a0 = ka.x, a1 = ka.y;
+  if (a0 == a1 || kd.x == kKein) return 0;
+  const D3 pa = ld3(s.x, a0), pb = ld3(s.x, a1);
+  const D3 pe[2] = {pa, pb};
+  const Box qe = quader_punkte(pe, 2, kZuschlagQuader);
+  const D3 ehat = einheit(pb - pa);
+  uint32_t cnt = 0;
+  je_eintrag(qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, [&](uint32_t t, int64_t ci, int64_t cj, int64_t ck) {
+    const uint4 d = s.d_idx[t];
+    const uint32_t dd[3] = {d.x, d.y, d.z};
+    bool nachbar = false;
+    for (int k = 0; k < 3; ++k)
+      nachbar = nachbar || (s.an_naehten ? (dd[k] == a0 || dd[k] == a1)
+                                         : (gleich_oder_partner(s, a0, dd[k]) || gleich_oder_partner(s, a1, dd[k])));
+    const Box qt = box_of(s.hs.lo, s.hs.hi, t);
+    if (nachbar || !ueberlappt(qt, qe) || !erste_zelle(qe, qt, zelle, ci, cj, ck)) return;
+    const double4 n4 = s.nrm_t[t];
+    const D3 n = d3(n4.x, n4.y, n4.z);
+    double tk, w[3];
+    if (!kante_durch_dreieck(pa, pb, ld3(s.x, d.x), ld3(s.x, d.y), ld3(s.x, d.z), n, tk, w)) return;
+    const double cn = dot(n, ehat);
+    if (fabs(cn) < 1e-6) return;
+    if (FILL) {
+      const D3 p = lerp3(pa, pb, tk);
+      D3 g = d3(0, 0, 0);
+      const uint32_t kk[2] = {kd.x, kd.y};
+      for (int q = 0; q < 2; ++q) {
+        if (kk[q] == kKein) continue;
+        const uint4 dk = s.d_idx[kk[q]];
+        const uint32_t dkk[3] = {dk.x, dk.y, dk.z};
+        uint32_t o = kKein;
+        for (int a = 0; a < 3; ++a)
+          if (dkk[a] != a0 && dkk[a] != a1) {
+            o = dkk[a];
+            break;
+          }
+        if (o == kKein) continue;
+        const double4 m4 = s.nrm_t[kk[q]];
+        D3 m = einheit(cross(n, d3(m4.x, m4.y, m4.z)));
+        const D3 r = ld3(s.x, o) - p;
+        const D3 r_quer = r - ehat * dot(ehat, r);
+        if (dot(m, r_quer) < 0.0) m = m * -1.0;
+        g = g + (m - n * (dot(ehat, m) / cn));
+      }
+      const double lg = norm(g);
+      const uint32_t q = pos + cnt;
+      if (q < s.cap_s) {
+        const D3 gh = einheit(g);
+        s.sn_ke[q] = make_uint2(uint32_t(e), t);
+        s.sn_t[q] = tk;
+        s.sn_w[q] = make_double4(w[0], w[1], w[2], 0.0);
+        s.sn_g[q] = make_double4(gh.x, gh.y, gh.z, lg / sqrt(lg * lg + 2.25));
+      }
+    }
+    ++cnt;
+  });
+  return cnt;
+}
+__global__ void __launch_bounds__(kT) schnitt_count_kernel(const __grid_constant__ SelbstArgs s) {
+  const double z = zelle_aus(&s.lmax[0]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) s.off_s[s.ne] = 0u;
+  SC_FOR(e, s.ne) s.off_s[e] = kante_schnitte<false>(s, e, 0, z);
+}
+__global__ void __launch_bounds__(kT) schnitt_fill_kernel(const __grid_constant__ SelbstArgs s) {
+  const double z = zelle_aus(&s.lmax[0]);
+  SC_FOR(e, s.ne) kante_schnitte<true>(s, e, s.off_s[e], z);
+}
+
+// finde(e, t): the intersection of edge e with triangle t (the list is edge by edge)
+__device__ __forceinline__ uint32_t finde_schnitt(const SelbstArgs& s, uint32_t e, uint32_t t) {
+  const uint32_t a = s.off_s[e], b = s.off_s[e + 1];
+  for (uint32_t q = a; q < b; ++q)
+    if (s.sn_ke[q].y == t) return q;
+  return kKein;
+}
+__device__ __forceinline__ uint32_t wurzel(uint32_t* el, uint32_t i) {
+  while (el[i] != i) {
+    el[i] = el[el[i]];
+    i = el[i];
+  }
+  return i;
+}
+__device__ __forceinline__ void vereinige(uint32_t* el, uint32_t a, uint32_t b) {
+  const uint32_t ra = wurzel(el, a), rb = wurzel(el, b);
+  if (ra != rb) el[ra > rb ? ra : rb] = ra < rb ? ra : rb;
+}
+// gebiete (selbstkollision.rs:931-1009) as the reference runs it, on one
+// thread: the unions depend on their order.
+__global__ void gebiete_kernel(const __grid_constant__ SelbstArgs s) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const uint32_t n = s.zahl[SZ_SCHNITTE] < s.cap_s ? s.zahl[SZ_SCHNITTE] : s.cap_s;
+  uint32_t* el = s.sn_eltern;
+  for (uint32_t i = 0; i < n; ++i) el[i] = i;
+  uint32_t nt = 0;
+  const uint32_t cap_t = 6u * s.cap_s;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint2 et = s.sn_ke[i];
+    const uint32_t e = et.x, t = et.y;
+    const uint2 kd2 = s.k_dr[e];
+    uint32_t kde[2], nk = 0;
+    if (kd2.x != kKein) kde[nk++] = kd2.x;
+    if (kd2.y != kKein) kde[nk++] = kd2.y;
+    uint32_t andere[6], na = 0;
+    for (uint32_t q = 0; q < nk; ++q) {
+      const uint4 dk = s.d_kan[kde[q]];
+      const uint32_t f3[3] = {dk.x, dk.y, dk.z};
+      for (int a = 0; a < 3; ++a)
+        if (f3[a] != e) andere[na++] = f3[a];
+    }
+    uint32_t tn[6], ntn = 0;  // nachbardreiecke(t)
+    {
+      const uint4 dk = s.d_kan[t];
+      const uint32_t f3[3] = {dk.x, dk.y, dk.z};
+      for (int a = 0; a < 3; ++a) {
+        const uint2 u2 = s.k_dr[f3[a]];
+        if (u2.x != kKein && u2.x != t) tn[ntn++] = u2.x;
+        if (u2.y != kKein && u2.y != t) tn[ntn++] = u2.y;
+      }
+    }
+    for (uint32_t a = 0; a < na; ++a) {
+      const uint32_t j = finde_schnitt(s, andere[a], t);
+      if (j != kKein) vereinige(el, i, j);
+    }
+    for (uint32_t u = 0; u < ntn; ++u) {
+      uint32_t j = finde_schnitt(s, e, tn[u]);
+      if (j != kKein) vereinige(el, i, j);
+      for (uint32_t a = 0; a < na; ++a) {
+        j = finde_schnitt(s, andere[a], tn[u]);
+        if (j != kKein) vereinige(el, i, j);
+      }
+    }
+    const uint4 dt = s.d_kan[t];
+    const uint32_t ft[3] = {dt.x, dt.y, dt.z};
+    for (int a = 0; a < 3; ++a)
+      for (uint32_t q = 0; q < nk; ++q) {
+        const uint32_t j = finde_schnitt(s, ft[a], kde[q]);
+        if (j != kKein && nt < cap_t) s.sn_tausch[nt++] = make_uint2(i, j);
+      }
+  }
+  for (int runde = 0; runde < 2; ++runde) {
+    for (uint32_t i = 0; i < n; ++i) s.sn_partner[i] = kKein;
+    for (uint32_t q = 0; q < nt; ++q) {
+      const uint2 ij = s.sn_tausch[q];
+      const uint32_t ri = wurzel(el, ij.x), rj = wurzel(el, ij.y);
+      if (rj < s.sn_partner[ri]) s.sn_partner[ri] = rj;
+      if (ri < s.sn_partner[rj]) s.sn_partner[rj] = ri;
+    }
+    for (uint32_t q = 0; q < nt; ++q) {
+      const uint2 ij = s.sn_tausch[q];
+      const uint32_t rj = wurzel(el, ij.y);
+      if (s.sn_partner[rj] != kKein) vereinige(el, ij.x, s.sn_partner[rj]);
+    }
+  }
+  uint32_t gebiete = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    s.sn_wurzel[i] = wurzel(el, i);
+    s.sn_summe[i] = make_double4(0, 0, 0, 0);
+    if (s.sn_wurzel[i] == i) ++gebiete;
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    const double4 g = s.sn_g[i];
+    double4& m = s.sn_summe[s.sn_wurzel[i]];
+    m.x += g.x * g.w;
+    m.y += g.y * g.w;
+    m.z += g.z * g.w;
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    const double4 m = s.sn_summe[s.sn_wurzel[i]];
+    const D3 r = einheit(d3(m.x, m.y, m.z));
+    s.sn_g[i] = make_double4(r.x, r.y, r.z, s.sn_g[i].w);
+  }
+  s.zahl[SZ_GEBIETE] = gebiete;
+}
+
+// the first body in contact at point i (implizit.rs:700)
+__device__ bool erste_normale(const SelbstArgs& s, uint32_t i, D3& n) {
+  const D3 x = ld3(s.x, i);
+  for (int kb = 0; kb < s.n_bodies; ++kb) {
+    double ti;
+    if (kontakt(s.bodies[kb], x, s.kabst[i] + s.rand, n, ti)) return true;
+  }
+  return false;
+}
+// hat per triangle; pinched regions (implizit.rs:701-704)
+__global__ void __launch_bounds__(kT) klemm_kernel(const __grid_constant__ SelbstArgs s) {
+  const uint32_t n = s.zahl[SZ_SCHNITTE] < s.cap_s ? s.zahl[SZ_SCHNITTE] : s.cap_s;
+  SC_FOR(i, n) {
+    const uint2 et = s.sn_ke[i];
+    s.hat[et.y] = 1;
+    if (s.n_bodies == 0) continue;
+    const uint2 kp = s.k_idx[et.x];
+    const uint4 dp = s.d_idx[et.y];
+    const uint32_t dd[3] = {dp.x, dp.y, dp.z};
+    D3 summe = d3(0, 0, 0), nk;
+    for (int a = 0; a < 3; ++a)
+      if (erste_normale(s, dd[a], nk)) summe = summe + nk;
+    if (!(norm(summe) > 0.0)) continue;
+    bool k = false;
+    if (erste_normale(s, kp.x, nk) && dot(nk, summe) < 0.0) k = true;
+    if (!k && erste_normale(s, kp.y, nk) && dot(nk, summe) < 0.0) k = true;
+    if (k) s.klemm[s.sn_wurzel[i]] = 1;
+  }
+}
+__global__ void __launch_bounds__(kT) folge_kernel(const __grid_constant__ SelbstArgs s) {
+  SC_FOR(t, s.nd) s.folge[t] = s.hat[t] ? s.folge[t] + 1u : 1u;
+}
+// schubfedern (selbstkollision.rs:1014-1058) after the proximity pairs
+template <typename R>
+__global__ void __launch_bounds__(kT) schub_kernel(const __grid_constant__ SelbstArgs s) {
+  const uint32_t n = s.zahl[SZ_SCHNITTE] < s.cap_s ? s.zahl[SZ_SCHNITTE] : s.cap_s;
+  const uint32_t P = paare(s);
+  R4<R>* bR = static_cast<R4<R>*>(s.pr_bR);
+  R4<R>* wR = static_cast<R4<R>*>(s.pr_wR);
+  R* g5R = static_cast<R*>(s.pr_g5R);
+  const double h2 = s.h * s.h;
+  SC_FOR(i, n) {
+    // spring P + i; a pinched region's springs stay in the list with zero
+    // weights (no entries, no force), so the list keeps the reference's order
+    const uint32_t q = P + uint32_t(i);
+    if (q >= s.cap_pairs) continue;
+    const bool aus = s.klemm[s.sn_wurzel[i]] != 0;
+    const uint2 et = s.sn_ke[i];
+    const uint32_t e = et.x, t = et.y;
+    const double k = 2.0 * s.steifigkeit * (s.e_kante[e] + s.e_dreieck[t]) * (s.a_kante[e] + s.a_dreieck[t]) / 1e-6;
+    const double4 g4 = s.sn_g[i];
+    const D3 g = d3(g4.x, g4.y, g4.z);
+    const double f = k * double(s.folge[t] < 5u ? s.folge[t] : 5u) * 1e-3;
+    const double tk = s.sn_t[i];
+    const double4 w = s.sn_w[i];
+    const uint2 kp = s.k_idx[e];
+    const uint4 dp = s.d_idx[t];
+    const double on = aus ? 0.0 : 1.0;
+    s.pr_idx[q] = make_uint4(kp.x, kp.y, dp.x, dp.y);
+    s.pr_x5[q] = dp.z;
+    s.pr_w[q] = make_double4(on * (1.0 - tk), on * tk, -on * w.x, -on * w.y);
+    s.pr_g5[q] = -on * w.z;
+    s.pr_kf[q] = make_double4(g.x * f, g.y * f, g.z * f, k);
+    const double bxx = k * g.x * g.x, byy = k * g.y * g.y, bzz = k * g.z * g.z;
+    const double bxy = k * g.x * g.y, bxz = k * g.x * g.z, byz = k * g.y * g.z;
+    s.pr_b0[q] = make_double4(bxx, byy, bzz, bxy);
+    s.pr_b1[q] = make_double4(bxz, byz, 0.0, 0.0);
+    bR[2 * q] = {R(h2 * bxx), R(h2 * byy), R(h2 * bzz), R(h2 * bxy)};
+    bR[2 * q + 1] = {R(h2 * bxz), R(h2 * byz), R(0), R(0)};
+    wR[q] = {R(on * (1.0 - tk)), R(on * tk), R(-on * w.x), R(-on * w.y)};
+    g5R[q] = R(-on * w.z);
+  }
+}
+// per triangle: its intersections (for the impacts' filter)
+__global__ void __launch_bounds__(kT) t_count_kernel(const __grid_constant__ SelbstArgs s) {
+  const uint32_t n = s.zahl[SZ_SCHNITTE] < s.cap_s ? s.zahl[SZ_SCHNITTE] : s.cap_s;
+  SC_FOR(i, n) atomicAdd(&s.t_off[s.sn_ke[i].y], 1u);
+}
+__global__ void __launch_bounds__(kT) t_fill_kernel(const __grid_constant__ SelbstArgs s) {
+  const uint32_t n = s.zahl[SZ_SCHNITTE] < s.cap_s ? s.zahl[SZ_SCHNITTE] : s.cap_s;
+  SC_FOR(i, n) {
+    const uint32_t t = s.sn_ke[i].y;
+    s.t_ent[s.t_off[t] + atomicAdd(&s.t_cur[t], 1u)] = uint32_t(i);
+  }
+}
+
+// ============================================================ impacts
+// selbstkollision.rs:1063-1343 on the way x0 -> x1 (x1 = the step's x).
+constexpr double kStossAbstand = 1e-4;  // selbstkollision.rs:1090
+constexpr double kStossKanteMin = 1e-4;  // :1092
+
+// path boxes (selbstkollision.rs:1199-1203): points, edges, triangles
+__global__ void __launch_bounds__(kT) weg_boxen_kernel(const __grid_constant__ SelbstArgs s) {
+  SC_FOR(v, s.n) {
+    const D3 p[2] = {ld3(s.x0, uint32_t(v)), ld3(s.xs, uint32_t(v))};
+    const Box b = quader_punkte(p, 2, 1e-8);
+    s.hp2.lo[v] = make_double4(b.lo.x, b.lo.y, b.lo.z, 0.0);
+    s.hp2.hi[v] = make_double4(b.hi.x, b.hi.y, b.hi.z, 0.0);
+  }
+  SC_FOR(e, s.ne) {
+    const uint2 k = s.k_idx[e];
+    const D3 p[4] = {ld3(s.x0, k.x), ld3(s.x0, k.y), ld3(s.xs, k.x), ld3(s.xs, k.y)};
+    const Box b = quader_punkte(p, 4, 1e-8);
+    s.hk2.lo[e] = make_double4(b.lo.x, b.lo.y, b.lo.z, 0.0);
+    s.hk2.hi[e] = make_double4(b.hi.x, b.hi.y, b.hi.z, 0.0);
+  }
+  SC_FOR(t, s.nd) {
+    const uint4 d = s.d_idx[t];
+    const D3 p[6] = {ld3(s.x0, d.x), ld3(s.x0, d.y), ld3(s.x0, d.z), ld3(s.xs, d.x), ld3(s.xs, d.y), ld3(s.xs, d.z)};
+    const Box b = quader_punkte(p, 6, 1e-8);
+    s.qt2_lo[t] = make_double4(b.lo.x, b.lo.y, b.lo.z, 0.0);
+    s.qt2_hi[t] = make_double4(b.hi.x, b.hi.y, b.hi.z, 0.0);
+  }
+}
+
+__device__ __forceinline__ double ebenenabstand(D3 a, D3 b, D3 c, D3 p) { return dot(p - a, einheit(cross(b - a, c - a))); }
+// selbstkollision.rs:1128-1153 (regula falsi, 16 steps)
+__device__ bool koplanar_zeit(const D3 x0[4], const D3 x1[4], double tol, double& out) {
+  auto f = [&](double t) {
+    return ebenenabstand(lerp3(x0[0], x1[0], t), lerp3(x0[1], x1[1], t), lerp3(x0[2], x1[2], t),
+                         lerp3(x0[3], x1[3], t));
+  };
+  double t0 = 0.0, t1 = 1.0, d0 = f(0.0), d1 = f(1.0);
+  for (int it = 0; it < 16; ++it) {
+    if (d0 * d1 > 0.0) return false;
+    const double tau = t0 + (t1 - t0) * fabs(d0) / fmax(fabs(d0) + fabs(d1), DBL_MIN);
+    const double d = f(tau);
+    if (fabs(d) < tol || t1 - t0 < 1e-4) {
+      out = tau;
+      return true;
+    }
+    if (d0 * d > 0.0) {
+      t0 = tau;
+      d0 = d;
+    } else {
+      t1 = tau;
+      d1 = d;
+    }
+  }
+  return false;
+}
+// selbstkollision.rs:1173-1193
+__device__ bool kanten_kreuzen(D3 a, D3 b, D3 c, D3 d, double& so, double& wo) {
+  const D3 e1 = b - a, e2 = d - c;
+  const double l1 = norm(e1), l2 = norm(e2);
+  if (l1 < kStossKanteMin || l2 < kStossKanteMin) return false;
+  const D3 u1 = e1 * (1.0 / l1), u2 = e2 * (1.0 / l2);
+  const double g = dot(u1, u2);
+  if (fabs(g) > 0.99999) return false;
+  const D3 q = c - a;
+  const double nen = 1.0 - g * g;
+  const double sv = (dot(q, u1) - g * dot(q, u2)) / nen;
+  const double wv = (g * dot(q, u1) - dot(q, u2)) / nen;
+  if (sv <= 0.0 || sv >= l1 || wv <= 0.0 || wv >= l2) return false;
+  so = sv / l1;
+  wo = wv / l2;
+  return true;
+}
+
+// the earliest point through triangle t (selbstkollision.rs:1215-1251)
+__global__ void __launch_bounds__(kT) stoss_pd_kernel(const __grid_constant__ SelbstArgs s) {
+  const double z = zelle_aus(&s.lmax[1]);
+  SC_FOR(t, s.nd) {
+    s.st_art[t] = 0u;
+    const uint4 dq = s.d_idx[t];
+    const uint32_t d[3] = {dq.x, dq.y, dq.z};
+    if (d[0] == d[1] || d[1] == d[2] || d[0] == d[2]) continue;
+    const Box qt = box_of(s.qt2_lo, s.qt2_hi, t);
+    bool hat = false;
+    double bz = 0.0;
+    je_eintrag(qt, z, s.hp2.eimer, s.hp2.anf, s.hp2.ein, [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck) {
+      for (int k = 0; k < 3; ++k)
+        if (gleich_oder_partner(s, v, d[k])) return;
+      const Box qv = box_of(s.hp2.lo, s.hp2.hi, v);
+      if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, z, ci, cj, ck)) return;
+      const uint32_t idx[4] = {d[0], d[1], d[2], v};
+      if (s.w[idx[0]] <= 0.0 && s.w[idx[1]] <= 0.0 && s.w[idx[2]] <= 0.0 && s.w[idx[3]] <= 0.0) return;
+      D3 a0[4], a1[4];
+      for (int k = 0; k < 4; ++k) {
+        a0[k] = ld3(s.x0, idx[k]);
+        a1[k] = ld3(s.xs, idx[k]);
+      }
+      double zeit;
+      if (!koplanar_zeit(a0, a1, kStossAbstand * 0.1, zeit)) return;
+      if (hat && bz <= zeit) return;
+      D3 q[4];
+      for (int k = 0; k < 4; ++k) q[k] = lerp3(a0[k], a1[k], zeit);
+      double u, vv;
+      if (!im_dreieck(q[0], q[1], q[2], q[3], u, vv)) return;
+      const D3 n = einheit(cross(q[1] - q[0], q[2] - q[0]));
+      const double g[3] = {1.0 - u - vv, u, vv};
+      const D3 rel = (a1[3] - a0[3]) - (((a1[0] - a0[0]) * g[0] + (a1[1] - a0[1]) * g[1]) + (a1[2] - a0[2]) * g[2]);
+      const double seite = dot(rel, n) <= 0.0 ? 1.0 : -1.0;
+      hat = true;
+      bz = zeit;
+      s.st_idx[t] = make_uint4(v, d[0], d[1], d[2]);
+      s.st_lzs[t] = make_double4(u, vv, zeit, seite);
+      s.st_n[t] = make_double4(n.x * seite, n.y * seite, n.z * seite, 0.0);
+    });
+    if (hat) s.st_art[t] = 1u;
+  }
+}
+// the earliest partner edge of edge i (selbstkollision.rs:1253-1283)
+__global__ void __launch_bounds__(kT) stoss_kk_kernel(const __grid_constant__ SelbstArgs s) {
+  const double z = zelle_aus(&s.lmax[1]);
+  SC_FOR(i, s.ne) {
+    const uint32_t slot = uint32_t(s.nd + i);
+    s.st_art[slot] = 0u;
+    const uint2 ki = s.k_idx[i];
+    const uint32_t i0 = ki.x, i1 = ki.y;
+    if (i0 == i1) continue;
+    const Box qi = box_of(s.hk2.lo, s.hk2.hi, i);
+    bool hat = false;
+    double bz = 0.0;
+    je_eintrag(qi, z, s.hk2.eimer, s.hk2.anf, s.hk2.ein, [&](uint32_t j, int64_t ci, int64_t cj, int64_t ck) {
+      if (int64_t(j) <= i) return;
+      const Box qj = box_of(s.hk2.lo, s.hk2.hi, j);
+      if (!ueberlappt(qi, qj) || !erste_zelle(qi, qj, z, ci, cj, ck)) return;
+      const uint2 kj = s.k_idx[j];
+      if (gleich_oder_partner(s, kj.x, i0) || gleich_oder_partner(s, kj.x, i1) || gleich_oder_partner(s, kj.y, i0) ||
+          gleich_oder_partner(s, kj.y, i1))
+        return;
+      const uint32_t idx[4] = {i1, kj.x, kj.y, i0};
+      if (s.w[idx[0]] <= 0.0 && s.w[idx[1]] <= 0.0 && s.w[idx[2]] <= 0.0 && s.w[idx[3]] <= 0.0) return;
+      D3 a0[4], a1[4];
+      for (int k = 0; k < 4; ++k) {
+        a0[k] = ld3(s.x0, idx[k]);
+        a1[k] = ld3(s.xs, idx[k]);
+      }
+      double zeit;
+      if (!koplanar_zeit(a0, a1, kStossAbstand * 0.1, zeit)) return;
+      if (hat && bz <= zeit) return;
+      D3 q[4];
+      for (int k = 0; k < 4; ++k) q[k] = lerp3(a0[k], a1[k], zeit);
+      double sv, wv;
+      if (!kanten_kreuzen(q[3], q[0], q[1], q[2], sv, wv)) return;
+      const D3 n = einheit(cross(q[0] - q[3], q[2] - q[1]));
+      const D3 auf_i = (a1[3] - a0[3]) * (1.0 - sv) + (a1[0] - a0[0]) * sv;
+      const D3 auf_j = (a1[1] - a0[1]) * (1.0 - wv) + (a1[2] - a0[2]) * wv;
+      const double seite = dot(auf_i - auf_j, n) <= 0.0 ? 1.0 : -1.0;
+      hat = true;
+      bz = zeit;
+      s.st_idx[slot] = make_uint4(i0, i1, kj.x, kj.y);
+      s.st_lzs[slot] = make_double4(sv, wv, zeit, seite);
+      s.st_n[slot] = make_double4(n.x * seite, n.y * seite, n.z * seite, double(j));  // .w: the partner edge
+    });
+    if (hat) s.st_art[slot] = 2u;
+  }
+}
+// ohne_durchdrungene (selbstkollision.rs:1063-1084): keep flags per slot
+__device__ bool trifft(const SelbstArgs& s, uint32_t a, uint32_t b) {
+  const uint2 kd = s.k_dr[b];
+  const uint32_t ts[2] = {kd.x, kd.y};
+  for (int q = 0; q < 2; ++q) {
+    if (ts[q] == kKein) continue;
+    if (finde_schnitt(s, a, ts[q]) == kKein) continue;
+    const uint4 dk = s.d_kan[ts[q]];
+    if (dk.x == b || dk.y == b || dk.z == b) return true;
+  }
+  return false;
+}
+__global__ void __launch_bounds__(kT) stoss_filter_kernel(const __grid_constant__ SelbstArgs s) {
+  const int64_t m = s.nd + s.ne;
+  const uint32_t nsn = s.zahl[SZ_SCHNITTE] < s.cap_s ? s.zahl[SZ_SCHNITTE] : s.cap_s;
+  if (blockIdx.x == 0 && threadIdx.x == 0) s.st_off[m] = 0u;
+  SC_FOR(q, m) {
+    const uint32_t art = s.st_art[q];
+    bool keep = art != 0u;
+    if (keep && nsn > 0) {
+      const uint4 p = s.st_idx[q];
+      if (art == 1u) {
+        // dreieck_von(p1, p2, p3): the triangle of edge p1-p2 that holds p3 -
+        // the searching triangle's own edge 0
+        const uint32_t t = uint32_t(q);
+        const uint32_t ke = s.d_kan[t].x;
+        const uint2 kd = s.k_dr[ke];
+        uint32_t tt = 0;
+        const uint32_t cand[2] = {kd.x, kd.y};
+        for (int c = 0; c < 2; ++c) {
+          if (cand[c] == kKein) continue;
+          const uint4 d = s.d_idx[cand[c]];
+          if (d.x == p.w || d.y == p.w || d.z == p.w) {
+            tt = cand[c];
+            break;
+          }
+        }
+        for (uint32_t r = s.t_off[tt]; r < s.t_off[tt + 1] && keep; ++r) {
+          const uint2 k = s.k_idx[s.sn_ke[s.t_ent[r]].x];
+          if (k.x == p.x || k.y == p.x) keep = false;
+        }
+      } else {
+        // kante_von of both point pairs: the searching edge and its partner
+        const uint32_t i = uint32_t(q - s.nd), j = uint32_t(s.st_n[q].w);
+        keep = !(trifft(s, i, j) || trifft(s, j, i));
+      }
+    }
+    s.st_off[q] = keep ? 1u : 0u;
+  }
+}
+
+// the kept impacts in order: point-triangle by triangle, then edge-edge by edge
+__global__ void __launch_bounds__(kT) stoss_list_kernel(const __grid_constant__ SelbstArgs s) {
+  const int64_t m = s.nd + s.ne;
+  SC_FOR(q, m)
+  if (s.st_off[q + 1] != s.st_off[q]) s.im[s.st_off[q]] = uint32_t(q);
+}
+__device__ __forceinline__ uint32_t stoesse(const SelbstArgs& s) { return s.zahl[SZ_STOSS]; }
+// per point (w > 0) its impact slots (impact << 2 | slot), in impact order
+__global__ void __launch_bounds__(kT) im_count_kernel(const __grid_constant__ SelbstArgs s) {
+  SC_FOR(j, stoesse(s)) {
+    const uint4 p = s.st_idx[s.im[j]];
+    const uint32_t pts[4] = {p.x, p.y, p.z, p.w};
+    for (int k = 0; k < 4; ++k)
+      if (s.w[pts[k]] > 0.0) atomicAdd(&s.im_off[pts[k]], 1u);
+  }
+}
+__global__ void __launch_bounds__(kT) im_fill_kernel(const __grid_constant__ SelbstArgs s) {
+  SC_FOR(j, stoesse(s)) {
+    const uint4 p = s.st_idx[s.im[j]];
+    const uint32_t pts[4] = {p.x, p.y, p.z, p.w};
+    for (int k = 0; k < 4; ++k)
+      if (s.w[pts[k]] > 0.0)
+        s.im_ent[s.im_off[pts[k]] + atomicAdd(&s.im_cur[pts[k]], 1u)] = (uint32_t(j) << 2) | uint32_t(k);
+  }
+}
+__global__ void __launch_bounds__(kT) im_sort_kernel(const __grid_constant__ SelbstArgs s) {
+  SC_FOR(i, s.n) sort_range(s.im_ent, s.im_off[i], s.im_off[i + 1]);
+}
+// one response pass, per impact (selbstkollision.rs:1292-1328): the
+// correction of each of its points with w > 0 into im_c
+__global__ void __launch_bounds__(kT) antwort_a_kernel(const __grid_constant__ SelbstArgs s) {
+  if (s.zahl[SZ_HALT]) return;
+  uint32_t zahl = 0;
+  SC_FOR(j, stoesse(s)) {
+    const uint32_t q = s.im[j];
+    const uint4 p = s.st_idx[q];
+    const uint32_t pts[4] = {p.x, p.y, p.z, p.w};
+    const double4 lzs = s.st_lzs[q];
+    D3 n;
+    double d, g[4];
+    bool erste[4];
+    if (s.st_art[q] == 1u) {
+      const D3 x1 = ld3(s.xs, p.y), x2 = ld3(s.xs, p.z), x3 = ld3(s.xs, p.w);
+      n = einheit(cross(x2 - x1, x3 - x1)) * lzs.w;
+      g[0] = 1.0;
+      g[1] = 1.0 - lzs.x - lzs.y;
+      g[2] = lzs.x;
+      g[3] = lzs.y;
+      erste[0] = true;
+      erste[1] = erste[2] = erste[3] = false;
+      d = dot(n, ld3(s.xs, p.x) - x1);
+    } else {
+      const double4 n4 = s.st_n[q];
+      n = d3(n4.x, n4.y, n4.z);
+      const D3 a = lerp3(ld3(s.xs, p.x), ld3(s.xs, p.y), lzs.x), b = lerp3(ld3(s.xs, p.z), ld3(s.xs, p.w), lzs.y);
+      g[0] = 1.0 - lzs.x;
+      g[1] = lzs.x;
+      g[2] = 1.0 - lzs.y;
+      g[3] = lzs.y;
+      erste[0] = erste[1] = true;
+      erste[2] = erste[3] = false;
+      d = dot(n, a - b);
+    }
+    const double tief = kStossAbstand - d;
+    if (tief <= 0.0) {
+      for (int k = 0; k < 4; ++k) s.im_c[4 * j + k] = make_double4(0, 0, 0, 0);
+      continue;
+    }
+    double m1 = 0.0, m2 = 0.0;
+    bool fest1 = true, fest2 = true;
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t i = pts[k];
+      const double4 nf = make_double4(s.nrm_fest[3 * i], s.nrm_fest[3 * i + 1], s.nrm_fest[3 * i + 2], 0.0);
+      const double me = (nf.x != 0.0 || nf.y != 0.0 || nf.z != 0.0) ? s.masse[i] * 1e9 : s.masse[i];
+      if (erste[k]) {
+        m1 += g[k] * me;
+        fest1 = fest1 && s.w[i] <= 0.0;
+      } else {
+        m2 += g[k] * me;
+        fest2 = fest2 && s.w[i] <= 0.0;
+      }
+    }
+    const double alpha = fest2 ? 1.0 : (fest1 ? 0.0 : m2 / (m1 + m2));
+    for (int k = 0; k < 4; ++k) {
+      if (!(s.w[pts[k]] > 0.0)) {
+        s.im_c[4 * j + k] = make_double4(0, 0, 0, 0);
+        continue;
+      }
+      const D3 c = erste[k] ? n * (tief * alpha) : n * (-(tief * (1.0 - alpha)));
+      s.im_c[4 * j + k] = make_double4(c.x, c.y, c.z, 1.0);
+    }
+    ++zahl;
+  }
+  if (zahl) atomicAdd(&s.zahl[SZ_ANTWORT], zahl);
+}
+// per point: the mean of its corrections (selbstkollision.rs:1329-1336)
+__global__ void __launch_bounds__(kT) antwort_b_kernel(const __grid_constant__ SelbstArgs s) {
+  if (s.zahl[SZ_HALT]) return;
+  uint32_t bewegt = 0;
+  SC_FOR(i, s.n) {
+    D3 dx = d3(0, 0, 0);
+    uint32_t cnt = 0;
+    for (uint32_t e = s.im_off[i]; e < s.im_off[i + 1]; ++e) {
+      const double4 c = s.im_c[s.im_ent[e]];
+      if (c.w == 0.0) continue;
+      dx = dx + d3(c.x, c.y, c.z);
+      ++cnt;
+    }
+    if (cnt) {
+      st3(s.xs, uint32_t(i), ld3(s.xs, uint32_t(i)) + dx * (1.0 / double(cnt)));
+      ++bewegt;
+    }
+  }
+  if (bewegt) atomicAdd(&s.zahl[SZ_BEWEGT], bewegt);
+}
+__global__ void antwort_c_kernel(const __grid_constant__ SelbstArgs s) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    if (s.zahl[SZ_BEWEGT] == 0u) s.zahl[SZ_HALT] = 1u;
+    s.zahl[SZ_BEWEGT] = 0u;
+  }
+}
+// running sums of the statistics (impact corrections, intersections, regions)
+__global__ void stat_kernel(const __grid_constant__ SelbstArgs s, unsigned long long* acc) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    acc[0] += s.zahl[SZ_ANTWORT];
+    acc[1] += s.zahl[SZ_SCHNITTE];
+    acc[2] += s.zahl[SZ_GEBIETE];
+  }
+}
 }  // namespace
 
 size_t selbst_scan_tmp_words(int64_t n) { return size_t((n + kScanChunk - 1) / kScanChunk) + 1; }
 // normals, boxes; 2 scans, fill, sort, count, 2 scans; fill, springs, damping,
 // count, scan, fill, sort
-int selbst_launches_per_run() { return 2 + (6 + 3 + 6) + (4 + 3 + 3); }
+int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3); }
+int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1; }
+
+// Impacts, part 1 (selbstkollision.rs:1196-1203): the longest edge at x1, the
+// path boxes, the bucket counts of the point and edge path hashes. The host
+// has zeroed lmax[1] and both hashes' bucket arrays.
+cudaError_t selbst_stoss_zaehlen(const SelbstArgs& s, cudaStream_t st) {
+  cudaError_t e;
+  kante_max_kernel<<<grid_for(s.ne), kT, 0, st>>>(s, s.xs, &s.lmax[1]);
+  weg_boxen_kernel<<<grid_for(s.n > s.ne ? (s.n > s.nd ? s.n : s.nd) : (s.ne > s.nd ? s.ne : s.nd)), kT, 0, st>>>(s);
+  hg_count_kernel<<<grid_for(s.n), kT, 0, st>>>(s.hp2, &s.lmax[1], &s.zahl[SZ_HASH_P2]);
+  hg_count_kernel<<<grid_for(s.ne), kT, 0, st>>>(s.hk2, &s.lmax[1], &s.zahl[SZ_HASH_K2]);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = scan(s.hp2.anf, int64_t(s.hp2.eimer) + 1, s.scan_tmp, nullptr, st)) != cudaSuccess) return e;
+  return scan(s.hk2.anf, int64_t(s.hk2.eimer) + 1, s.scan_tmp, nullptr, st);
+}
+
+// Impacts, part 2: the hashes filled, the earliest impact per triangle and
+// per edge, those between parts that already interpenetrate dropped, the
+// response passes (selbstkollision.rs:1063-1343), and the statistics' sums.
+// The host has checked the hash capacities and zeroed im_off and im_cur.
+cudaError_t selbst_stoss_antwort(const SelbstArgs& s, int iterationen, unsigned long long* acc, cudaStream_t st) {
+  cudaError_t e;
+  hg_fill_kernel<<<grid_for(s.n), kT, 0, st>>>(s.hp2, &s.lmax[1]);
+  hg_fill_kernel<<<grid_for(s.ne), kT, 0, st>>>(s.hk2, &s.lmax[1]);
+  hg_sort_kernel<<<grid_for(s.hp2.eimer), kT, 0, st>>>(s.hp2);
+  hg_sort_kernel<<<grid_for(s.hk2.eimer), kT, 0, st>>>(s.hk2);
+  stoss_pd_kernel<<<grid_for(s.nd), kT, 0, st>>>(s);
+  stoss_kk_kernel<<<grid_for(s.ne), kT, 0, st>>>(s);
+  stoss_filter_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = scan(s.st_off, s.nd + s.ne + 1, s.scan_tmp, &s.zahl[SZ_STOSS], st)) != cudaSuccess) return e;
+  stoss_list_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
+  im_count_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = scan(s.im_off, s.n + 1, s.scan_tmp, nullptr, st)) != cudaSuccess) return e;
+  im_fill_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
+  im_sort_kernel<<<grid_for(s.n), kT, 0, st>>>(s);
+  for (int it = 0; it < iterationen; ++it) {
+    antwort_a_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
+    antwort_b_kernel<<<grid_for(s.n), kT, 0, st>>>(s);
+    antwort_c_kernel<<<1, 32, 0, st>>>(s);
+  }
+  stat_kernel<<<1, 32, 0, st>>>(s, acc);
+  return cudaGetLastError();
+}
 
 // Part 1: normals, planes, boxes, bucket counts. The host has zeroed the
 // bucket-count arrays (anf_p, anf_k: eimer + 1 each) and the counters.
@@ -897,7 +1649,20 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   pairs_count_kernel<<<grid_for(s.nd > s.ne ? s.nd : s.ne), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = scan(s.off_t, s.nd + 1, s.scan_tmp, &s.zahl[SZ_PAARE_PT], st)) != cudaSuccess) return e;
-  return scan(s.off_e, s.ne + 1, s.scan_tmp, &s.zahl[SZ_PAARE_KK], st);
+  if ((e = scan(s.off_e, s.ne + 1, s.scan_tmp, &s.zahl[SZ_PAARE_KK], st)) != cudaSuccess) return e;
+  // edges through triangles (selbstkollision.rs:858-907): the longest edge,
+  // the triangle hash, the count per edge. The host has zeroed lmax and the
+  // triangle hash's bucket arrays.
+  kante_max_kernel<<<grid_for(s.ne), kT, 0, st>>>(s, s.x, &s.lmax[0]);
+  schnitt_boxen_kernel<<<grid_for(s.nd), kT, 0, st>>>(s);
+  hg_count_kernel<<<grid_for(s.nd), kT, 0, st>>>(s.hs, &s.lmax[0], &s.zahl[SZ_HASH_S]);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = scan(s.hs.anf, int64_t(s.hs.eimer) + 1, s.scan_tmp, nullptr, st)) != cudaSuccess) return e;
+  hg_fill_kernel<<<grid_for(s.nd), kT, 0, st>>>(s.hs, &s.lmax[0]);
+  hg_sort_kernel<<<grid_for(s.hs.eimer), kT, 0, st>>>(s.hs);
+  schnitt_count_kernel<<<grid_for(s.ne), kT, 0, st>>>(s);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return scan(s.off_s, s.ne + 1, s.scan_tmp, &s.zahl[SZ_SCHNITTE], st);
 }
 
 // Part 3: pairs, springs, damping, incidence lists. The host has checked the
@@ -918,6 +1683,21 @@ cudaError_t selbst_paare_und_federn(const SelbstArgs& s, cudaStream_t st) {
     smem_set = true;
   }
   daempfung_kernel<<<1, kDB, kDampSmem, st>>>(s);
+  // penetration regions and their push springs (selbstkollision.rs:858-1058);
+  // the host has zeroed hat, klemm, t_off and t_cur
+  const int64_t ns = int64_t(s.cap_s);
+  schnitt_fill_kernel<<<grid_for(s.ne), kT, 0, st>>>(s);
+  gebiete_kernel<<<1, 32, 0, st>>>(s);
+  klemm_kernel<<<grid_for(ns), kT, 0, st>>>(s);
+  folge_kernel<<<grid_for(s.nd), kT, 0, st>>>(s);
+  if (s.rsize == 4)
+    schub_kernel<float><<<grid_for(ns), kT, 0, st>>>(s);
+  else
+    schub_kernel<double><<<grid_for(ns), kT, 0, st>>>(s);
+  t_count_kernel<<<grid_for(ns), kT, 0, st>>>(s);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = scan(s.t_off, s.nd + 1, s.scan_tmp, nullptr, st)) != cudaSuccess) return e;
+  t_fill_kernel<<<grid_for(ns), kT, 0, st>>>(s);
   inc_count_kernel<<<grid_for(pmax), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = scan(s.inc_off, s.n + 1, s.scan_tmp, &s.zahl[SZ_INZIDENZ], st)) != cudaSuccess) return e;

@@ -7,6 +7,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "k3d_device.cuh"
+
 namespace k3d {
 
 constexpr uint32_t kKein = 0xffffffffu;  // no triangle / no part
@@ -18,7 +20,26 @@ enum SelbstZahl : int {
   SZ_PAARE_PT = 2,  // point-triangle pairs
   SZ_PAARE_KK = 3,  // edge-edge pairs
   SZ_INZIDENZ = 4,  // incidence entries
-  SZ_COUNT = 8
+  SZ_SCHUB = 5,     // push springs of the penetration regions, after the pairs
+  SZ_SCHNITTE = 6,  // edges through triangles
+  SZ_GEBIETE = 7,   // their regions
+  SZ_HASH_S = 8,    // entries of the triangle hash of the intersection search
+  SZ_HASH_P2 = 9,   // entries of the point-path hash of the impact search
+  SZ_HASH_K2 = 10,  // entries of the edge-path hash
+  SZ_STOSS = 11,    // impacts kept for the response
+  SZ_ANTWORT = 12,  // impact corrections applied (ImplizitStatistik::selbst_stoesse)
+  SZ_BEWEGT = 13,   // points moved by the last response pass
+  SZ_HALT = 14,     // set when a response pass moved no point (the passes stop)
+  SZ_COUNT = 16
+};
+
+// A spatial hash over boxes (Hashgitter, selbstkollision.rs:281-345): the
+// boxes, bucket starts (eimer + 1), entries (cap), fill cursors.
+struct HashG {
+  double4 *lo, *hi;
+  int64_t m;
+  uint32_t eimer, cap;
+  uint32_t *anf, *ein, *cur;
 };
 
 struct SelbstArgs {
@@ -65,13 +86,55 @@ struct SelbstArgs {
   double4* pr_ga;          // per slot g * (mass share of the other side), the damping's update factor
   void* pr_bR;             // h^2 * block in operator precision, 2 R4 per pair
   void* pr_wR;             // weights in operator precision, R4 per pair
-  uint32_t *inc_off, *inc_cur, *inc_ent;  // per point: (pair << 2 | slot)
+  // a fifth point per spring (the push springs of penetration regions join
+  // an edge to a triangle; kKein and weight 0 for the proximity pairs)
+  uint32_t* pr_x5;
+  double* pr_g5;
+  void* pr_g5R;                           // in operator precision
+  uint32_t *inc_off, *inc_cur, *inc_ent;  // per point: (spring << 3 | slot)
   uint32_t cap_inc;
-  uint32_t* inc_pos;  // per (pair << 2 | slot): its entry index, all ones for a zero weight
+  uint32_t* inc_pos;  // per (spring << 3 | slot): its entry index, all ones for a zero weight
   void* inc_out;      // per entry: the PCG's spring product of that slot, R4
   int32_t* slot_of;  // damping scratch per point: its shared-memory slot, -1 between batches
   uint32_t* zahl;    // SZ_COUNT counters
   uint32_t* scan_tmp;
+
+  // ---- penetration regions (selbstkollision.rs:810-1058)
+  int an_naehten;                 // ImplizitParameter::selbst_schnitte_an_naehten
+  unsigned long long* lmax;       // 2: the longest edge (as bits) at x and at the impact stage's x1
+  HashG hs;                       // triangle boxes
+  uint32_t* off_s;                // per edge: its intersections' count, then start (ne + 1)
+  uint32_t cap_s;
+  uint2* sn_ke;                   // per intersection: edge, triangle
+  double* sn_t;                   // position on the edge
+  double4* sn_w;                  // triangle weights
+  double4* sn_g;                  // direction (xyz) and weight
+  uint32_t *sn_wurzel, *sn_eltern, *sn_partner, *sn_sp;  // regions; push-spring slots (cap_s + 1)
+  uint2* sn_tausch;               // role swaps (6 per intersection at most)
+  double4* sn_summe;
+  uint32_t *t_off, *t_cur, *t_ent;  // per triangle: its intersections (nd + 1)
+  uint8_t *hat, *klemm;           // per triangle; per region root
+  uint32_t* folge;                // per triangle: steps in a row with an edge through it (kept)
+  const Body* bodies;             // for the pinch test (first body in contact)
+  int n_bodies;
+  const double* kabst;
+  double rand;
+  // ---- impacts (selbstkollision.rs:1063-1343)
+  const double* x0;               // the positions at the start of the substep
+  double* xs;                     // the positions the response moves (the step's x)
+  const double* nrm_fest;         // held points (nonzero normal) weigh 1e9 times their mass
+  int iterationen;
+  HashG hp2, hk2;                 // point paths, edge paths
+  double4 *qt2_lo, *qt2_hi;       // triangle paths
+  // the earliest impact per triangle (slots 0..nd) and per edge (nd..nd+ne)
+  uint32_t* st_art;               // 0 none, 1 point-triangle, 2 edge-edge
+  uint4* st_idx;
+  double4* st_lzs;                // lage (2), zeit, seite
+  double4* st_n;                  // normal (edge-edge)
+  uint32_t* st_off;               // kept impacts: count, then start (nd + ne + 1)
+  uint32_t* im;                   // the kept impacts' slots in order
+  uint32_t *im_off, *im_cur, *im_ent;  // per point: (impact << 2 | slot) (n + 1)
+  double4* im_c;                  // per (impact, slot): the correction, w = 1 if it applies
 };
 
 // The stage in three parts with host reads of the counters between them
@@ -80,6 +143,11 @@ cudaError_t selbst_hash_zaehlen(const SelbstArgs& s, cudaStream_t st);
 cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStream_t st);
 cudaError_t selbst_paare_und_federn(const SelbstArgs& s, cudaStream_t st);
 int selbst_launches_per_run();
+// Impacts after the step's integration, in two parts with a host read of the
+// path hashes' entry counts between them.
+cudaError_t selbst_stoss_zaehlen(const SelbstArgs& s, cudaStream_t st);
+cudaError_t selbst_stoss_antwort(const SelbstArgs& s, int iterationen, unsigned long long* acc, cudaStream_t st);
+int selbst_stoss_launches(int iterationen);
 size_t selbst_scan_tmp_words(int64_t n);
 
 }  // namespace k3d

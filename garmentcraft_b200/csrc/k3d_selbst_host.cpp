@@ -46,6 +46,8 @@ void selbst_free(SelbstHost& H) {
   free_all(H.fest);
   free_all(H.pairs);
   free_all(H.hashk);
+  free_all(H.schn);
+  free_all(H.wege);
   H.on = false;
   H.ran = false;
 }
@@ -263,8 +265,70 @@ cudaError_t selbst_upload(SelbstHost& H, const k3d_scene* sc, double zusatzdicke
   if ((e = alloc(s.slot_of, size_t(n), H.fest)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(s.slot_of, 0xff, sizeof(int32_t) * std::max<size_t>(size_t(n), 1), st)) != cudaSuccess)
     return e;
-  const int64_t longest = std::max({int64_t(s.eimer_p) + 1, int64_t(s.eimer_k) + 1, nd + 1, ne + 1, n + 1});
+  // penetration regions: the triangle hash (a triangle box spans at most
+  // three cells per axis: its extent is at most the cell, the longest edge,
+  // plus the margin), per edge and per triangle lists, the fold counts
+  s.hs.m = nd;
+  s.hs.eimer = uint32_t(std::max<int64_t>(2 * nd, 64));
+  s.hs.cap = uint32_t(std::min<int64_t>(27 * std::max<int64_t>(nd, 1), int64_t(0xffffffffu)));
+  if ((e = alloc(s.hs.lo, size_t(nd), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hs.hi, size_t(nd), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hs.anf, size_t(s.hs.eimer) + 1, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hs.cur, size_t(s.hs.eimer), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hs.ein, size_t(s.hs.cap), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.lmax, 2, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.off_s, size_t(ne) + 1, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.t_off, size_t(nd) + 1, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.t_cur, size_t(nd), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hat, size_t(nd), H.fest)) != cudaSuccess) return e;
+  {
+    std::vector<uint32_t> eins(size_t(std::max<int64_t>(nd, 1)), 1u);
+    if ((e = up(s.folge, eins, H.fest, st)) != cudaSuccess) return e;
+  }
+  // impacts: path hashes (entries sized per run), per triangle and edge slots
+  s.hp2.m = n;
+  s.hp2.eimer = uint32_t(std::max<int64_t>(2 * n, 64));
+  s.hk2.m = ne;
+  s.hk2.eimer = uint32_t(std::max<int64_t>(2 * ne, 64));
+  if ((e = alloc(s.hp2.lo, size_t(n), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hp2.hi, size_t(n), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hp2.anf, size_t(s.hp2.eimer) + 1, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hp2.cur, size_t(s.hp2.eimer), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hk2.lo, size_t(ne), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hk2.hi, size_t(ne), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hk2.anf, size_t(s.hk2.eimer) + 1, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hk2.cur, size_t(s.hk2.eimer), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.qt2_lo, size_t(nd), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.qt2_hi, size_t(nd), H.fest)) != cudaSuccess) return e;
+  const size_t slots = size_t(nd + ne);
+  if ((e = alloc(s.st_art, slots, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.st_idx, slots, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.st_lzs, slots, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.st_n, slots, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.st_off, slots + 1, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.im, slots, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.im_off, size_t(n) + 1, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.im_cur, size_t(n), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.im_ent, 4 * slots, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.im_c, 4 * slots, H.fest)) != cudaSuccess) return e;
+  double* x0 = nullptr;
+  if ((e = alloc(x0, 3 * size_t(n), H.fest)) != cudaSuccess) return e;
+  s.x0 = x0;
+  H.x0 = x0;
+  Body* bd = nullptr;
+  if ((e = alloc(bd, size_t(kMaxBodies), H.fest)) != cudaSuccess) return e;
+  s.bodies = bd;
+  H.bodies_dev = bd;
+  if ((e = alloc(H.acc, 3, H.fest)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(H.acc, 0, 3 * sizeof(unsigned long long), st)) != cudaSuccess) return e;
+  const int64_t longest = std::max({int64_t(s.eimer_p) + 1, int64_t(s.eimer_k) + 1, nd + 1, ne + 1, n + 1,
+                                    int64_t(s.hs.eimer) + 1, int64_t(s.hp2.eimer) + 1, int64_t(s.hk2.eimer) + 1,
+                                    nd + ne + 1});
   if ((e = alloc(s.scan_tmp, selbst_scan_tmp_words(longest), H.fest)) != cudaSuccess) return e;
+  if ((e = selbst_grow_schnitte(H, 1024)) != cudaSuccess) return e;
+  if ((e = selbst_grow_wege(H, uint32_t(std::min<int64_t>(8 * std::max<int64_t>(n, 1), 0x7fffffff)),
+                            uint32_t(std::min<int64_t>(8 * std::max<int64_t>(ne, 1), 0x7fffffff)))) != cudaSuccess)
+    return e;
   if ((e = selbst_grow_edge_hash(H, uint32_t(std::min<int64_t>(27 * std::max<int64_t>(ne, 1), 0x7fffffff)))) !=
       cudaSuccess)
     return e;
@@ -273,6 +337,34 @@ cudaError_t selbst_upload(SelbstHost& H, const k3d_scene* sc, double zusatzdicke
     return e;
   H.on = true;
   return cudaStreamSynchronize(st);
+}
+
+cudaError_t selbst_grow_schnitte(SelbstHost& H, uint32_t cap) {
+  free_all(H.schn);
+  SelbstArgs& s = H.s;
+  s.cap_s = cap;
+  cudaError_t e;
+  if ((e = alloc(s.sn_ke, cap, H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.sn_t, cap, H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.sn_w, cap, H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.sn_g, cap, H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.sn_wurzel, cap, H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.sn_eltern, cap, H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.sn_partner, cap, H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.sn_sp, size_t(cap) + 1, H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.sn_tausch, 6 * size_t(cap), H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.sn_summe, cap, H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.klemm, cap, H.schn)) != cudaSuccess) return e;
+  return alloc(s.t_ent, cap, H.schn);
+}
+
+cudaError_t selbst_grow_wege(SelbstHost& H, uint32_t cap_p, uint32_t cap_k) {
+  free_all(H.wege);
+  cudaError_t e;
+  H.s.hp2.cap = cap_p;
+  H.s.hk2.cap = cap_k;
+  if ((e = alloc(H.s.hp2.ein, size_t(cap_p), H.wege)) != cudaSuccess) return e;
+  return alloc(H.s.hk2.ein, size_t(cap_k), H.wege);
 }
 
 cudaError_t selbst_grow_edge_hash(SelbstHost& H, uint32_t cap) {
@@ -285,7 +377,7 @@ cudaError_t selbst_grow_pairs(SelbstHost& H, uint32_t cap) {
   free_all(H.pairs);
   SelbstArgs& s = H.s;
   s.cap_pairs = cap;
-  s.cap_inc = 4u * cap;
+  s.cap_inc = 5u * cap;
   cudaError_t e;
   if ((e = alloc(s.pr_idx, cap, H.pairs)) != cudaSuccess) return e;
   if ((e = alloc(s.pr_src, cap, H.pairs)) != cudaSuccess) return e;
@@ -302,7 +394,12 @@ cudaError_t selbst_grow_pairs(SelbstHost& H, uint32_t cap) {
   char* wR = nullptr;
   if ((e = alloc(wR, size_t(cap) * 4 * size_t(s.rsize), H.pairs)) != cudaSuccess) return e;
   s.pr_wR = wR;
-  if ((e = alloc(s.inc_pos, size_t(s.cap_inc), H.pairs)) != cudaSuccess) return e;
+  if ((e = alloc(s.pr_x5, cap, H.pairs)) != cudaSuccess) return e;
+  if ((e = alloc(s.pr_g5, cap, H.pairs)) != cudaSuccess) return e;
+  char* g5R = nullptr;
+  if ((e = alloc(g5R, size_t(cap) * size_t(s.rsize), H.pairs)) != cudaSuccess) return e;
+  s.pr_g5R = g5R;
+  if ((e = alloc(s.inc_pos, size_t(8) * cap, H.pairs)) != cudaSuccess) return e;
   char* out = nullptr;
   if ((e = alloc(out, size_t(s.cap_inc) * 4 * size_t(s.rsize), H.pairs)) != cudaSuccess) return e;
   s.inc_out = out;
@@ -335,26 +432,72 @@ cudaError_t selbst_run(SelbstHost& H, double h, cudaStream_t st, int& launches) 
     const uint64_t want = uint64_t(z[SZ_HASH_K]) + z[SZ_HASH_K] / 2 + 1024;
     if ((e = selbst_grow_edge_hash(H, uint32_t(std::min<uint64_t>(want, 0xffffffffu)))) != cudaSuccess) return e;
   }
+  if ((e = cudaMemsetAsync(s.lmax, 0, 2 * sizeof(unsigned long long), st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(s.hs.anf, 0, sizeof(uint32_t) * (size_t(s.hs.eimer) + 1), st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(s.hs.cur, 0, sizeof(uint32_t) * size_t(s.hs.eimer), st)) != cudaSuccess) return e;
   if ((e = selbst_hash_fuellen_und_paare_zaehlen(s, st)) != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(z, s.zahl, sizeof(z), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-  const uint64_t paare = uint64_t(z[SZ_PAARE_PT]) + z[SZ_PAARE_KK];
-  if (paare > s.cap_pairs) {
-    const uint64_t want = paare + paare / 2 + 1024;
-    if (want > 0x3fffffffu) return cudaErrorMemoryAllocation;
+  if (z[SZ_HASH_S] > s.hs.cap) return cudaErrorInvalidValue;  // cannot happen: 27 buckets per triangle box
+  const uint32_t n_s = z[SZ_SCHNITTE];
+  if (n_s > s.cap_s) {
+    const uint64_t want = uint64_t(n_s) + n_s / 2 + 1024;
+    if (want > 0x0fffffffu) return cudaErrorMemoryAllocation;
+    if ((e = selbst_grow_schnitte(H, uint32_t(want))) != cudaSuccess) return e;
+  }
+  // the proximity pairs, then one push spring per intersection
+  const uint64_t paare = uint64_t(z[SZ_PAARE_PT]) + z[SZ_PAARE_KK], federn = paare + n_s;
+  if (federn > s.cap_pairs) {
+    const uint64_t want = federn + federn / 2 + 1024;
+    if (want > 0x1fffffffu) return cudaErrorMemoryAllocation;
     if ((e = selbst_grow_pairs(H, uint32_t(want))) != cudaSuccess) return e;
   }
   if ((e = cudaMemsetAsync(s.inc_off, 0, sizeof(uint32_t) * (size_t(s.n) + 1), st)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(s.inc_cur, 0, sizeof(uint32_t) * size_t(s.n), st)) != cudaSuccess) return e;
-  if (paare > 0 && (e = cudaMemsetAsync(s.inc_pos, 0xff, sizeof(uint32_t) * 4 * size_t(paare), st)) != cudaSuccess)
+  if (federn > 0 && (e = cudaMemsetAsync(s.inc_pos, 0xff, sizeof(uint32_t) * 8 * size_t(federn), st)) != cudaSuccess)
+    return e;
+  if ((e = cudaMemsetAsync(s.hat, 0, size_t(std::max<int64_t>(s.nd, 1)), st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(s.klemm, 0, size_t(s.cap_s), st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(s.t_off, 0, sizeof(uint32_t) * (size_t(s.nd) + 1), st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(s.t_cur, 0, sizeof(uint32_t) * size_t(std::max<int64_t>(s.nd, 1)), st)) != cudaSuccess)
     return e;
   if ((e = selbst_paare_und_federn(s, st)) != cudaSuccess) return e;
   H.n_pt = z[SZ_PAARE_PT];
   H.n_kk = z[SZ_PAARE_KK];
+  H.n_s = n_s;
   H.naehe_pt += z[SZ_PAARE_PT];
   H.naehe_kk += z[SZ_PAARE_KK];
   H.ran = true;
   launches += selbst_launches_per_run();
+  return cudaSuccess;
+}
+
+cudaError_t selbst_stoss_run(SelbstHost& H, double* x, const double* nrm_fest, int iterationen, cudaStream_t st,
+                            int& launches) {
+  if (!H.on) return cudaSuccess;
+  SelbstArgs& s = H.s;
+  s.xs = x;
+  s.nrm_fest = nrm_fest;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(&s.lmax[1], 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
+  for (HashG* g : {&s.hp2, &s.hk2}) {
+    if ((e = cudaMemsetAsync(g->anf, 0, sizeof(uint32_t) * (size_t(g->eimer) + 1), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(g->cur, 0, sizeof(uint32_t) * size_t(g->eimer), st)) != cudaSuccess) return e;
+  }
+  if ((e = selbst_stoss_zaehlen(s, st)) != cudaSuccess) return e;
+  uint32_t z[SZ_COUNT];
+  if ((e = cudaMemcpyAsync(z, s.zahl, sizeof(z), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  if (z[SZ_HASH_P2] > s.hp2.cap || z[SZ_HASH_K2] > s.hk2.cap) {
+    const uint64_t wp = std::max<uint64_t>(s.hp2.cap, uint64_t(z[SZ_HASH_P2]) + z[SZ_HASH_P2] / 2 + 1024);
+    const uint64_t wk = std::max<uint64_t>(s.hk2.cap, uint64_t(z[SZ_HASH_K2]) + z[SZ_HASH_K2] / 2 + 1024);
+    if (wp > 0x7fffffffu || wk > 0x7fffffffu) return cudaErrorMemoryAllocation;
+    if ((e = selbst_grow_wege(H, uint32_t(wp), uint32_t(wk))) != cudaSuccess) return e;
+  }
+  if ((e = cudaMemsetAsync(s.im_off, 0, sizeof(uint32_t) * (size_t(s.n) + 1), st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(s.im_cur, 0, sizeof(uint32_t) * size_t(s.n), st)) != cudaSuccess) return e;
+  if ((e = selbst_stoss_antwort(s, iterationen, H.acc, st)) != cudaSuccess) return e;
+  launches += selbst_stoss_launches(iterationen);
   return cudaSuccess;
 }
 
@@ -366,6 +509,9 @@ void selbst_step_args(const SelbstHost& H, StepArgs& a) {
     a.sc_bR = a.sc_wR = nullptr;
     a.sc_out = nullptr;
     a.sc_np = 0;
+    a.sc_x5 = nullptr;
+    a.sc_g5 = nullptr;
+    a.sc_g5R = nullptr;
     return;
   }
   const SelbstArgs& s = H.s;
@@ -380,7 +526,10 @@ void selbst_step_args(const SelbstHost& H, StepArgs& a) {
   a.sc_wR = s.pr_wR;
   a.sc_pos = s.inc_pos;
   a.sc_out = s.inc_out;
-  a.sc_np = std::min<uint32_t>(H.n_pt + H.n_kk, s.cap_pairs);
+  a.sc_x5 = s.pr_x5;
+  a.sc_g5 = s.pr_g5;
+  a.sc_g5R = s.pr_g5R;
+  a.sc_np = std::min<uint32_t>(H.n_pt + H.n_kk + H.n_s, s.cap_pairs);
 }
 
 }  // namespace k3d

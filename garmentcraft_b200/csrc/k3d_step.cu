@@ -286,20 +286,21 @@ __device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<R>* buf, int
     y += bm[3 * P + sid] * pj.x + bm[4 * P + sid] * pj.y + bm[5 * P + sid] * pj.z;
     z += bm[6 * P + sid] * pj.x + bm[7 * P + sid] * pj.y + bm[8 * P + sid] * pj.z;
   }
-  if (SC) {  // proximity springs, matrix-free (h^2 is in their blocks)
+  if (SC) {  // self-collision springs, matrix-free (h^2 is in their blocks)
     const R4<R>* bR = static_cast<const R4<R>*>(a.sc_bR);
     const R4<R>* wR = static_cast<const R4<R>*>(a.sc_wR);
+    const R* g5R = static_cast<const R*>(a.sc_g5R);
     const R4<R> pi = next_dir<R>(buf[i], beta);
     for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
-      const uint32_t ent = a.sc_ent[e], q = ent >> 2, k = ent & 3u;
+      const uint32_t ent = a.sc_ent[e], q = ent >> 3, k = ent & 7u;
       const uint4 id = a.sc_idx[q];
       const R4<R> w4 = wR[q];
-      const R g[4] = {w4.x, w4.y, w4.z, w4.w};
-      const uint32_t ix[4] = {id.x, id.y, id.z, id.w};
+      const R g[5] = {w4.x, w4.y, w4.z, w4.w, g5R[q]};
+      const uint32_t ix[5] = {id.x, id.y, id.z, id.w, a.sc_x5[q]};
       const R gk = g[k];
       R sx = 0, sy = 0, sz = 0;
 #pragma unroll
-      for (int r = 0; r < 4; ++r)
+      for (int r = 0; r < 5; ++r)
         if ((gk > R(0) && g[r] < R(0)) || (gk < R(0) && g[r] > R(0))) {
           const R om = -gk * g[r];
           const R4<R> pr = next_dir<R>(buf[ix[r]], beta);
@@ -434,24 +435,27 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       // slot's share of c.A c is c_k.t_k.
       const R4<R>* bR = static_cast<const R4<R>*>(a.sc_bR);
       const R4<R>* wR = static_cast<const R4<R>*>(a.sc_wR);
+      const R* g5R = static_cast<const R*>(a.sc_g5R);
       R4<R>* out = static_cast<R4<R>*>(a.sc_out);
       const int64_t nth = int64_t(sh.g.nblk) * blockDim.x;
       for (int64_t q = int64_t(sh.bidx) * blockDim.x + threadIdx.x; q < int64_t(a.sc_np); q += nth) {
         const uint4 id = a.sc_idx[q];
         const R4<R> w4 = wR[q];
-        const R g[4] = {w4.x, w4.y, w4.z, w4.w};
-        const uint32_t ix[4] = {id.x, id.y, id.z, id.w};
-        R4<R> c[4];
+        const R g[5] = {w4.x, w4.y, w4.z, w4.w, g5R[q]};
+        const uint32_t x5 = a.sc_x5[q];
+        const uint32_t ix[5] = {id.x, id.y, id.z, id.w, x5};
+        R4<R> c[5];
 #pragma unroll
         for (int r = 0; r < 4; ++r) c[r] = next_dir<R>(cur[ix[r]], rb);
+        c[4] = x5 != 0xffffffffu ? next_dir<R>(cur[x5], rb) : R4<R>{R(0), R(0), R(0), R(0)};
         const R4<R> b0 = bR[2 * q], b1 = bR[2 * q + 1];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const uint32_t e = a.sc_pos[4 * q + k];
+        for (int k = 0; k < 5; ++k) {
+          const uint32_t e = a.sc_pos[8 * q + k];
           if (e == 0xffffffffu) continue;
           R sx = 0, sy = 0, sz = 0;
 #pragma unroll
-          for (int r = 0; r < 4; ++r)
+          for (int r = 0; r < 5; ++r)
             if ((g[k] > R(0) && g[r] < R(0)) || (g[k] < R(0) && g[r] > R(0))) {
               const R om = -g[k] * g[r];
               sx += om * (c[k].x - c[r].x);

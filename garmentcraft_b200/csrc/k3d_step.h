@@ -104,9 +104,14 @@ struct StepArgs {
   const uint4* sc_idx;
   const double4 *sc_w, *sc_kf, *sc_b0, *sc_b1;
   const void *sc_bR, *sc_wR;
-  // the PCG iteration's spring product pair by pair: each nonzero slot's
-  // entry index (sc_pos, per pair << 2 | slot) and the per-entry products
-  // (sc_out, R4), summed per point in list order; sc_np pairs
+  // the fifth point and weight of each spring (kKein / 0 for proximity pairs;
+  // the push springs of penetration regions join an edge to a triangle)
+  const uint32_t* sc_x5;
+  const double* sc_g5;
+  const void* sc_g5R;
+  // the PCG iteration's spring product spring by spring: each nonzero slot's
+  // entry index (sc_pos, per spring << 3 | slot) and the per-entry products
+  // (sc_out, R4), summed per point in list order; sc_np springs
   const uint32_t* sc_pos;
   void* sc_out;
   uint32_t sc_np;

@@ -108,7 +108,9 @@ __device__ __forceinline__ void pmul(const R* P, int64_t i, R x, R y, R z, R& ox
 
 // w = (R) dv, c = 0: the next element pass with beta = 0 applies A to dv.
 
-// Proximity springs at point i in FP64 (implizit.rs:214-220, 267-276): over
+// Springs of self-collision (proximity pairs, then the push springs of
+// penetration regions; up to five points each) at point i in FP64
+// (implizit.rs:214-220, 267-276): over
 // the point's incidence entries, B times the sum over the pair's other side
 // of om (p_i - p_r) with om = -g_q g_r > 0. `dg` (if given) receives
 // sum om B, the springs' part of the diagonal block (xx, yy, zz, xy, xz, yz).
@@ -117,16 +119,16 @@ __device__ __forceinline__ D3 feder_hp64(const StepArgs& a, int64_t i, P&& p, do
   D3 out = d3(0.0, 0.0, 0.0);
   const D3 pi = p(uint32_t(i));
   for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
-    const uint32_t ent = a.sc_ent[e], q = ent >> 2, k = ent & 3u;
+    const uint32_t ent = a.sc_ent[e], q = ent >> 3, k = ent & 7u;
     const uint4 id = a.sc_idx[q];
     const double4 g4 = a.sc_w[q];
-    const double g[4] = {g4.x, g4.y, g4.z, g4.w};
-    const uint32_t ix[4] = {id.x, id.y, id.z, id.w};
+    const double g[5] = {g4.x, g4.y, g4.z, g4.w, a.sc_g5[q]};
+    const uint32_t ix[5] = {id.x, id.y, id.z, id.w, a.sc_x5[q]};
     const double gk = g[k];
     D3 sm = d3(0.0, 0.0, 0.0);
     double so = 0.0;
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+    for (int r = 0; r < 5; ++r)
       if ((gk > 0.0 && g[r] < 0.0) || (gk < 0.0 && g[r] > 0.0)) {
         const double om = -gk * g[r];
         sm = sm + (pi - p(ix[r])) * om;
