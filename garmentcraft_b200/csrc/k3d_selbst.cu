@@ -332,16 +332,25 @@ __global__ void __launch_bounds__(kT) hash_fill_kernel(const __grid_constant__ S
 }
 
 // Ascending entries inside each bucket: the reference fills its buckets in
-// entry order (selbstkollision.rs:316-322).
+// entry order (selbstkollision.rs:316-322). The keys of a range are distinct,
+// so any sort gives the same result; Shell sort with Ciura's gaps keeps a
+// crowded bucket (hundreds of entries) from stalling its thread.
 __device__ __forceinline__ void sort_range(uint32_t* a, uint32_t lo, uint32_t hi) {
-  for (uint32_t i = lo + 1; i < hi; ++i) {
-    const uint32_t key = a[i];
-    uint32_t j = i;
-    while (j > lo && a[j - 1] > key) {
-      a[j] = a[j - 1];
-      --j;
+  const uint32_t n = hi - lo;
+  if (n < 2) return;
+  const uint32_t gaps[8] = {701u, 301u, 132u, 57u, 23u, 10u, 4u, 1u};
+  for (int g = 0; g < 8; ++g) {
+    const uint32_t gap = gaps[g];
+    if (gap >= n) continue;
+    for (uint32_t i = lo + gap; i < hi; ++i) {
+      const uint32_t key = a[i];
+      uint32_t j = i;
+      while (j >= lo + gap && a[j - gap] > key) {
+        a[j] = a[j - gap];
+        j -= gap;
+      }
+      a[j] = key;
     }
-    a[j] = key;
   }
 }
 __global__ void __launch_bounds__(kT) bucket_sort_kernel(const __grid_constant__ SelbstArgs s) {
