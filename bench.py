@@ -76,6 +76,9 @@ def args_():
     p.add_argument("--capture", type=int, default=0,
                    help="profiling case: run this many mixed-form steps of the drop on cuda:0 and exit")
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="form used by --capture")
+    p.add_argument("--workload", default="sheet", choices=["sheet", "garment", "adjoint"],
+                   help="case of --capture: the sheet drop, the garment with self-collision (frames), or the "
+                        "material-fit drop's adjoint (frames forward, then the backward)")
     p.add_argument("--no-batch", action="store_true", help="skip the batched-drape comparison")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (material-fit) leg")
     p.add_argument("--no-garment", action="store_true", help="skip the sewn-garment leg")
@@ -446,10 +449,37 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     if a.capture:
-        # a fixed case for ncu: the same drop, no timing, no flush
+        # a fixed case for ncu: no timing, no flush
         from garmentcraft_b200 import _abi
         from garmentcraft_b200.implizit import ImplizitCg
         prec = _abi.K3D_MIXED if a.precision == "mixed" else _abi.K3D_FP64
+        if a.workload == "adjoint":
+            import numpy as np
+            from garmentcraft_b200 import synth
+            from garmentcraft_b200.adjoint import Drapierung, Stoff
+            from garmentcraft_b200.params import ImplizitParameter
+            s, hid, start = synth.materialfit(n=ADJ_N)
+            par = ImplizitParameter(schritte_je_bild=1, cg_max=CG_MAX, cg_toleranz=1e-5, precision=_abi.K3D_FP64)
+            d = Drapierung(s, Stoff.von(hid), frames=a.capture, k=ADJ_K, param=par)
+            x, _ = d.vorwaerts(start)
+            g = d.rueckwaerts(2.0 * x)["roh"]
+            print(json.dumps({"capture_frames": a.capture, "forward_ms": g["ms_vorwaerts"],
+                              "backward_ms": g["ms_rueckwaerts"], "adjoint_cg_iterations": g["iterationen"]}))
+            return
+        if a.workload == "garment":
+            from garmentcraft_b200 import synth
+            from garmentcraft_b200.params import ImplizitParameter
+            s, _ = synth.garment_szene()
+            cg = ImplizitCg(ImplizitParameter(schritte_je_bild=1, cg_max=CG_MAX, cg_toleranz=1e-5, precision=prec,
+                                              selbstkollision=True))
+            cg.zustand_hochladen(s)
+            cg.bilder_auf_geraet(a.capture - 1)
+            st = cg.bilder_auf_geraet(1)
+            print(json.dumps({"capture_frames": a.capture, "last_frame_cg_iterations": st.cg_iterationen,
+                              "last_frame_ms": cg.letzte_bild_ms(), "last_frame_solve_ms": cg.letzte_loesung_ms(),
+                              "proximity_pairs": st.naehe_punkt_dreieck + st.naehe_kante_kante,
+                              "intersections": st.durchdringungen, "impacts": st.selbst_stoesse}))
+            return
         s = make_scene(a.n)
         cg = ImplizitCg(params(prec))
         cg.zustand_hochladen(s)
