@@ -153,6 +153,23 @@ class K3dAdjointStats(C.Structure):
     ]
 
 
+class K3dMeshInfo(C.Structure):
+    _fields_ = [
+        ("n_punkte", C.c_int64),
+        ("n_dreiecke", C.c_int64),
+        ("randkanten", C.c_int64),
+        ("volumen", C.c_double),
+        ("suchtiefe", C.c_double),
+        ("gitter_ursprung", C.c_double * 3),
+        ("gitter_zelle", C.c_double),
+        ("gitter_zahl", C.c_int64 * 3),
+        ("gitter_eintraege", C.c_int64),
+        ("ms_letzter_aufruf", C.c_double),
+        ("kernels_letzter_aufruf", C.c_int64),
+        ("ungeklaert", C.c_int64),
+    ]
+
+
 class K3dCgResult(C.Structure):
     _fields_ = [
         ("iterationen", C.c_int64),

@@ -13,7 +13,7 @@ from . import _abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_native", "libklon3d_b200.so")
 
-# every entry point include/klon3d_step.h declares
+# every entry point include/klon3d_step.h and include/klon3d_mesh.h declare
 EXPORTS = [
     "k3d_abi_version", "k3d_params_default", "k3d_simparams_default", "k3d_build_scene",
     "k3d_built_scene_view", "k3d_built_scene_free", "k3d_solver_create", "k3d_solver_destroy",
@@ -22,6 +22,8 @@ EXPORTS = [
     "k3d_residual", "k3d_read_load", "k3d_last_frame_ms", "k3d_last_solve_ms", "k3d_kernel_launches",
     "k3d_operator_noalloc", "k3d_selfcollision_pairs", "k3d_selfcollision_hash", "k3d_selfcollision_springs",
     "k3d_adjoint_forward", "k3d_adjoint_backward",
+    "k3d_mesh_create", "k3d_mesh_destroy", "k3d_mesh_last_error", "k3d_mesh_update", "k3d_mesh_get_info",
+    "k3d_mesh_tables", "k3d_mesh_nearest", "k3d_mesh_penetration", "k3d_mesh_sdf",
 ]
 
 _lib = None
@@ -98,6 +100,25 @@ def lib():
     L.k3d_selfcollision_hash.restype = C.c_int64
     L.k3d_selfcollision_springs.argtypes = [P, C.c_int64, dp, dp]
     L.k3d_selfcollision_springs.restype = C.c_int64
+    i32p = C.POINTER(C.c_int32)
+    L.k3d_mesh_create.argtypes = [dp, C.c_int64, u32p, C.c_int64, C.c_double, C.c_int32, C.POINTER(P), C.c_char_p,
+                                  C.c_int64]
+    L.k3d_mesh_create.restype = st
+    L.k3d_mesh_destroy.argtypes = [P]
+    L.k3d_mesh_last_error.argtypes = [P]
+    L.k3d_mesh_last_error.restype = C.c_char_p
+    L.k3d_mesh_update.argtypes = [P, dp]
+    L.k3d_mesh_update.restype = st
+    L.k3d_mesh_get_info.argtypes = [P, C.POINTER(_abi.K3dMeshInfo)]
+    L.k3d_mesh_get_info.restype = st
+    L.k3d_mesh_tables.argtypes = [P, dp, dp, u32p, dp]
+    L.k3d_mesh_tables.restype = st
+    L.k3d_mesh_nearest.argtypes = [P, dp, C.c_int64, C.c_double, dp, dp, dp, i32p, i32p]
+    L.k3d_mesh_nearest.restype = st
+    L.k3d_mesh_penetration.argtypes = [P, dp, dp, C.c_int64, i32p, dp, dp]
+    L.k3d_mesh_penetration.restype = st
+    L.k3d_mesh_sdf.argtypes = [P, i32p, dp, C.c_double, C.c_double, C.POINTER(C.c_float)]
+    L.k3d_mesh_sdf.restype = st
     if L.k3d_abi_version() != _abi.K3D_ABI_VERSION:
         raise RuntimeError("libklon3d_b200.so ABI version mismatch")
     _lib = L

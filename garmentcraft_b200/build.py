@@ -13,15 +13,17 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_native")
 LIB = os.path.join(OUT_DIR, "libklon3d_b200.so")
 SOURCES = ["k3d_step.cu", "k3d_build.cu", "k3d_host.cpp", "scene_build.cpp", "k3d_noalloc.cu", "k3d_selbst.cu",
-           "k3d_selbst_host.cpp", "k3d_adjoint.cu"]
+           "k3d_selbst_host.cpp", "k3d_adjoint.cu", "k3d_netz.cu"]
 HEADERS = ["k3d_step.h", "k3d_device.cuh", "k3d_step_common.cuh", "scene_build.h", "k3d_selbst.h",
            "k3d_selbst_host.h", "k3d_adjoint.h"]
 # Per-file flags. The build of the system and the self-collision stage round
 # every product and sum on their own (no fused multiply-add), as the
 # reference's arithmetic does: the element term of k3d_build.cu needs it, and
 # the self-collision cell indices, buckets and pairs come out bit-exact. The
-# adjoint replays the forward's contact queries and rounds the same way.
-EXTRA = {"k3d_build.cu": ["-fmad=false"], "k3d_selbst.cu": ["-fmad=false"], "k3d_adjoint.cu": ["-fmad=false"]}
+# adjoint replays the forward's contact queries and rounds the same way; the
+# body mesh's nearest-point regions and distances round as the reference's.
+EXTRA = {"k3d_build.cu": ["-fmad=false"], "k3d_selbst.cu": ["-fmad=false"], "k3d_adjoint.cu": ["-fmad=false"],
+         "k3d_netz.cu": ["-fmad=false"]}
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
@@ -37,6 +39,7 @@ def _stale() -> bool:
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
     deps.append(os.path.join(HERE, "..", "include", "klon3d_step.h"))
+    deps.append(os.path.join(HERE, "..", "include", "klon3d_mesh.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 

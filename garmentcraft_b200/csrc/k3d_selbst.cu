@@ -1589,6 +1589,9 @@ __global__ void stat_kernel(const __grid_constant__ SelbstArgs s, unsigned long 
 }  // namespace
 
 size_t selbst_scan_tmp_words(int64_t n) { return size_t((n + kScanChunk - 1) / kScanChunk) + 1; }
+cudaError_t exclusive_scan_u32(uint32_t* data, int64_t n, uint32_t* tmp, uint32_t* total, cudaStream_t st) {
+  return scan(data, n, tmp, total, st);
+}
 // normals, boxes; 2 scans, fill, sort, count, 2 scans; fill, springs, damping,
 // count, scan, fill, sort
 int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3); }

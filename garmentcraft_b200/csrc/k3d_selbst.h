@@ -149,5 +149,8 @@ cudaError_t selbst_stoss_zaehlen(const SelbstArgs& s, cudaStream_t st);
 cudaError_t selbst_stoss_antwort(const SelbstArgs& s, int iterationen, unsigned long long* acc, cudaStream_t st);
 int selbst_stoss_launches(int iterationen);
 size_t selbst_scan_tmp_words(int64_t n);
+// Exclusive prefix sum of n uint32 in place (3 launches); tmp holds
+// selbst_scan_tmp_words(n) words; `total` (device, may be null) gets the sum.
+cudaError_t exclusive_scan_u32(uint32_t* data, int64_t n, uint32_t* tmp, uint32_t* total, cudaStream_t st);
 
 }  // namespace k3d

@@ -511,3 +511,92 @@ def body_to_c(body: dict) -> _abi.K3dBody:
     sdf = body.get("sdf")
     kb.sdf = _abi.ptr(sdf, C.c_float) if sdf is not None else None
     return kb
+
+
+# ------------------------------------------------------------------ body meshes
+def wuerfel_netz(h: float = 1.0):
+    """The cube [-h, h]^3 as 12 triangles, counter-clockwise from outside.
+    Corner i has the signs of its bits (x: 1, y: 2, z: 4); each face splits
+    along its diagonal from the (-, -) to the (+, +) corner of its two
+    in-plane axes. Returns (points (8, 3), triangles (12, 3))."""
+    p = np.array([[h if i & 1 else -h, h if i & 2 else -h, h if i & 4 else -h] for i in range(8)], dtype=np.float64)
+    d = []
+    for a in range(3):
+        b, c = (a + 1) % 3, (a + 2) % 3
+        for s in (-1, 1):
+            def ecke(u, v):
+                bits = {a: s > 0, b: u > 0, c: v > 0}
+                return sum(1 << k for k in range(3) if bits[k])
+            q = [ecke(-1, -1), ecke(1, -1), ecke(1, 1), ecke(-1, 1)]  # counter-clockwise about +e_a
+            if s < 0:
+                q = [q[0], q[3], q[2], q[1]]
+            d += [[q[0], q[1], q[2]], [q[0], q[2], q[3]]]
+    return p, np.asarray(d, dtype=np.uint32)
+
+
+def zylinder_netz(radius: float, z_unten: float, z_oben: float, segmente: int, ringe: int):
+    """A closed cylinder about the z axis (netzkoerper.rs:934-962): `segmente`
+    points per ring, `ringe` bands between z_unten and z_oben, each cap a fan
+    about its centre point, outward normals."""
+    s, r = max(segmente, 3), max(ringe, 1)
+    w = 2.0 * math.pi * np.arange(s) / s
+    z = z_unten + (z_oben - z_unten) * np.arange(r + 1) / r
+    ring = np.stack([radius * np.cos(w), radius * np.sin(w)], axis=1)
+    p = np.concatenate([np.column_stack([ring, np.full(s, zi)]) for zi in z]
+                       + [np.array([[0.0, 0.0, z_unten], [0.0, 0.0, z_oben]])])
+    unten, oben = (r + 1) * s, (r + 1) * s + 1
+
+    def idx(i, j):
+        return i * s + j % s
+    d = []
+    for i in range(r):
+        for j in range(s):
+            a, b, c, e = idx(i, j), idx(i, j + 1), idx(i + 1, j + 1), idx(i + 1, j)
+            d += [[a, b, c], [a, c, e]]
+    for j in range(s):
+        d.append([unten, idx(0, j + 1), idx(0, j)])
+        d.append([oben, idx(r, j), idx(r, j + 1)])
+    return p, np.asarray(d, dtype=np.uint32)
+
+
+def koerper_netz(segmente: int = 256, ringe: int = 73, halbachsen=(0.18, 0.12, 0.85), mitte=(0.0, 0.0, 0.9),
+                 seed: int = 0):
+    """A closed, star-shaped body surface standing in for a scanned body
+    mesh: a latitude-longitude ellipsoid with the given half axes whose radius
+    is modulated by low-order waves (amplitudes from the seed, radius factor
+    in [0.7, 1.3]), `ringe - 1` rings of `segmente` points plus two poles,
+    2 * segmente * (ringe - 1) triangles (36,864 at the defaults, the size of
+    a human base mesh split into triangles). Outward normals."""
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(-0.05, 0.05, size=(4, 4))
+    th = math.pi * np.arange(1, ringe) / ringe
+    ph = 2.0 * math.pi * np.arange(segmente) / segmente
+    T, Ph = np.meshgrid(th, ph, indexing="ij")
+    f = np.ones_like(T)
+    for m in range(4):
+        for k in range(4):
+            f += amp[m, k] * np.sin((m + 1) * T) * np.cos(k * Ph + m)
+    f = np.clip(f, 0.7, 1.3)
+    x = halbachsen[0] * f * np.sin(T) * np.cos(Ph)
+    y = halbachsen[1] * f * np.sin(T) * np.sin(Ph)
+    z = halbachsen[2] * f * np.cos(T)
+    p = np.column_stack([x.ravel(), y.ravel(), z.ravel()])
+    p = np.concatenate([p, [[0.0, 0.0, halbachsen[2]], [0.0, 0.0, -halbachsen[2]]]]) + np.asarray(mitte)
+    nord, sued = p.shape[0] - 2, p.shape[0] - 1
+    s = segmente
+
+    def idx(i, j):
+        return i * s + j % s
+    d = []
+    for i in range(ringe - 2):
+        for j in range(s):
+            a, b, c, e = idx(i, j), idx(i, j + 1), idx(i + 1, j + 1), idx(i + 1, j)
+            d += [[a, c, b], [a, e, c]]
+    for j in range(s):
+        d.append([nord, idx(0, j), idx(0, j + 1)])
+        d.append([sued, idx(ringe - 2, j + 1), idx(ringe - 2, j)])
+    d = np.asarray(d, dtype=np.uint32)
+    q = p[d.astype(np.int64)]
+    if np.einsum("ij,ij->i", q[:, 0], np.cross(q[:, 1], q[:, 2])).sum() < 0.0:
+        d = d[:, [0, 2, 1]]
+    return p, np.ascontiguousarray(d)

@@ -20,6 +20,7 @@
 #include <map>
 #include <optional>
 #include <set>
+#include <string>
 #include <utility>
 #include <vector>
 
@@ -112,6 +113,53 @@ struct Koerper {
   double spacing = 1;
   std::optional<Kontakt> kontakt(V3 x, double abstand) const;
   Koerper verschoben(double t) const;
+};
+
+// ---------------------------------------------------------------- body mesh
+// sim/src/netzkoerper.rs:49-175 (Region, Naechster, Gitter, Koerpernetz).
+// Regions: 0-2 corner k, 3-5 edge k (corner k to k+1), 6 face.
+struct Naechster {
+  double abstand = 0;  // outside positive
+  V3 punkt{}, normale{};
+  uint32_t dreieck = 0;
+  int region = 6;
+};
+struct Durchstoss {
+  V3 punkt{}, normale{};
+  uint32_t dreieck = 0;
+};
+struct NetzGitter {
+  V3 ursprung{};
+  double zelle = 0;
+  std::array<size_t, 3> zahl{};
+  std::vector<uint32_t> anfang, eintraege;
+  std::array<int64_t, 3> index(V3 x) const;
+  size_t zellnummer(size_t kx, size_t ky, size_t kz) const;
+  bool bereich(V3 lo, V3 hi, std::array<std::pair<size_t, size_t>, 3>& r) const;
+};
+std::pair<V3, int> naechster_auf_dreieck(V3 p, V3 a, V3 b, V3 c);
+struct Koerpernetz {
+  std::vector<V3> punkte;
+  std::vector<std::array<uint32_t, 3>> dreiecke;
+  std::vector<V3> flaechennormale;
+  std::vector<std::array<uint32_t, 3>> nachbar;
+  std::vector<V3> punktnormale;
+  std::vector<std::pair<V3, double>> kugel;
+  double suchtiefe = 0;
+  NetzGitter gitter;
+  size_t randkanten = 0;
+  double volumen = 0;
+  static std::optional<std::string> neu(std::vector<V3> p, std::vector<std::array<uint32_t, 3>> d, double suchtiefe,
+                                        Koerpernetz& out);
+  std::optional<std::string> nachfuehren(const std::vector<V3>& p);
+  V3 kantennormale(size_t t, int k) const;
+  V3 pseudonormale(size_t t, int r) const;
+  Naechster ergebnis(V3 x, size_t t, V3 c, int r) const;
+  std::optional<Naechster> naechster(V3 x, double radius) const;
+  Naechster naechster_alle(V3 x) const;
+  std::optional<Durchstoss> durchstoss(V3 a, V3 b) const;
+  void sdf(const int32_t dims[3], V3 ursprung, double spacing, double band, float* out) const;
+  void gitter_bauen();
 };
 
 // ---------------------------------------------------------------- scene

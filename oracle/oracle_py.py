@@ -109,6 +109,17 @@ def lib():
     L.orc_selbst_hash.restype = C.c_int64
     L.orc_selbst_federn.argtypes = [P, dp, dp, C.c_int64, u32p, dp, dp, dp]
     L.orc_selbst_federn.restype = C.c_int64
+    cp = C.c_char_p
+    L.orc_netz_neu.argtypes = [dp, C.c_int64, u32p, C.c_int64, C.c_double, cp, C.c_int64]
+    L.orc_netz_neu.restype = P
+    L.orc_netz_free.argtypes = [P]
+    L.orc_netz_nachfuehren.argtypes = [P, dp, cp, C.c_int64]
+    L.orc_netz_nachfuehren.restype = C.c_int32
+    L.orc_netz_info.argtypes = [P, i64p, dp, dp, dp, i64p, i64p]
+    L.orc_netz_tabellen.argtypes = [P, dp, dp, u32p, dp]
+    L.orc_netz_naechster.argtypes = [P, dp, C.c_int64, C.c_double, dp, dp, dp, i32p, i32p]
+    L.orc_netz_durchstoss.argtypes = [P, dp, dp, C.c_int64, i32p, dp, dp]
+    L.orc_netz_sdf.argtypes = [P, i32p, dp, C.c_double, C.c_double, C.POINTER(C.c_float)]
     _lib = L
     return L
 
@@ -350,3 +361,75 @@ def stoesse(x0, x1, w, masse, dreiecke=None, kanten=None, pd=True, kk=True, iter
     n = L.orc_stoesse(x0.shape[0], _d(x0), _d(x1), _d(w), _d(m), tri.shape[0], tri.ctypes.data_as(up),
                       ka.shape[0], ka.ctypes.data_as(up), int(pd), int(kk), iterationen, _d(out), 64, C.byref(z))
     return out[:n], int(z.value), x1
+
+
+class Koerpernetz:
+    """The body mesh as a signed-distance collider (netzkoerper.rs:145-800),
+    oracle side. Raises ValueError with the reference's reason where
+    Koerpernetz::neu refuses the mesh."""
+
+    def __init__(self, punkte, dreiecke, suchtiefe: float = 0.01):
+        self.L = lib()
+        p = f64(punkte).reshape(-1, 3)
+        d = np.ascontiguousarray(dreiecke, dtype=np.uint32).reshape(-1, 3)
+        self.n, self.nd = p.shape[0], d.shape[0]
+        err = C.create_string_buffer(256)
+        self.h = self.L.orc_netz_neu(_d(p), self.n, d.ctypes.data_as(C.POINTER(C.c_uint32)), self.nd, suchtiefe,
+                                     err, 256)
+        if not self.h:
+            raise ValueError(err.value.decode())
+        self.suchtiefe = suchtiefe
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.orc_netz_free(self.h)
+            self.h = None
+
+    def nachfuehren(self, punkte):
+        p = f64(punkte).reshape(-1, 3)
+        err = C.create_string_buffer(256)
+        if self.L.orc_netz_nachfuehren(self.h, _d(p), err, 256):
+            raise ValueError(err.value.decode())
+
+    def info(self) -> dict:
+        rk, zahl, ein = C.c_int64(), np.zeros(3, dtype=np.int64), C.c_int64()
+        vol, urs, zelle = C.c_double(), np.zeros(3), C.c_double()
+        self.L.orc_netz_info(self.h, C.byref(rk), C.byref(vol), _d(urs), C.byref(zelle),
+                             zahl.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(ein))
+        return dict(randkanten=rk.value, volumen=vol.value, ursprung=urs, zelle=zelle.value, zahl=zahl,
+                    eintraege=ein.value)
+
+    def tabellen(self) -> dict:
+        fn, pn = np.zeros((self.nd, 3)), np.zeros((self.n, 3))
+        nb, kg = np.zeros((self.nd, 3), dtype=np.uint32), np.zeros((self.nd, 4))
+        self.L.orc_netz_tabellen(self.h, _d(fn), _d(pn), nb.ctypes.data_as(C.POINTER(C.c_uint32)), _d(kg))
+        return dict(flaechennormale=fn, punktnormale=pn, nachbar=nb, kugel=kg)
+
+    def naechster(self, x, radius: float = 0.0) -> dict:
+        """radius > 0: naechster (:503-539), dreieck -1 where nothing is
+        closer; otherwise naechster_alle (:770-782)."""
+        x = f64(x).reshape(-1, 3)
+        m = x.shape[0]
+        ab, pu, no = np.zeros(m), np.zeros((m, 3)), np.zeros((m, 3))
+        dr, rg = np.zeros(m, dtype=np.int32), np.zeros(m, dtype=np.int32)
+        i32 = C.POINTER(C.c_int32)
+        self.L.orc_netz_naechster(self.h, _d(x), m, radius, _d(ab), _d(pu), _d(no), dr.ctypes.data_as(i32),
+                                  rg.ctypes.data_as(i32))
+        return dict(abstand=ab, punkt=pu, normale=no, dreieck=dr, region=rg)
+
+    def durchstoss(self, a, b) -> dict:
+        a, b = f64(a).reshape(-1, 3), f64(b).reshape(-1, 3)
+        m = a.shape[0]
+        dr, pu, no = np.zeros(m, dtype=np.int32), np.zeros((m, 3)), np.zeros((m, 3))
+        self.L.orc_netz_durchstoss(self.h, _d(a), _d(b), m, dr.ctypes.data_as(C.POINTER(C.c_int32)), _d(pu),
+                                   _d(no))
+        return dict(dreieck=dr, punkt=pu, normale=no)
+
+    def sdf(self, dims, ursprung, spacing: float, band: float = 0.0):
+        """naechster_alle at every node, clamped to +-band when band > 0;
+        float32 array of shape (dims[2], dims[1], dims[0])."""
+        dm = np.ascontiguousarray(dims, dtype=np.int32)
+        out = np.zeros((dims[2], dims[1], dims[0]), dtype=np.float32)
+        self.L.orc_netz_sdf(self.h, dm.ctypes.data_as(C.POINTER(C.c_int32)), _d(f64(ursprung)), spacing, band,
+                            out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out

@@ -225,31 +225,6 @@ bool erste_zelle(const Quader& a, const Quader& b, double zelle, std::array<int6
     if (zellindex(std::fmax(a.first[k], b.first[k]), zelle) != c[k]) return false;
   return true;
 }
-// netzkoerper.rs:185-218 (Ericson's closest point on a triangle)
-V3 naechster_auf_dreieck(V3 p, V3 a, V3 b, V3 c) {
-  auto quot = [](double z, double n) { return n > 0.0 ? z / n : 0.0; };
-  V3 ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
-  double d1 = dot(ab, ap), d2 = dot(ac, ap);
-  if (d1 <= 0.0 && d2 <= 0.0) return a;
-  V3 bp = sub(p, b);
-  double d3 = dot(ab, bp), d4 = dot(ac, bp);
-  if (d3 >= 0.0 && d4 <= d3) return b;
-  double vc = d1 * d4 - d3 * d2;
-  if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) return add(a, mul(ab, quot(d1, d1 - d3)));
-  V3 cp = sub(p, c);
-  double d5 = dot(ab, cp), d6 = dot(ac, cp);
-  if (d6 >= 0.0 && d5 <= d6) return c;
-  double vb = d5 * d2 - d1 * d6;
-  if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) return add(a, mul(ac, quot(d2, d2 - d6)));
-  double va = d3 * d6 - d5 * d4;
-  if (va <= 0.0 && d4 - d3 >= 0.0 && d5 - d6 >= 0.0) {
-    double w = quot(d4 - d3, (d4 - d3) + (d5 - d6));
-    return add(b, mul(sub(c, b), w));
-  }
-  double s = va + vb + vc;
-  double v = quot(vb, s), w = quot(vc, s);
-  return add(a, add(mul(ab, v), mul(ac, w)));
-}
 }  // namespace
 
 // selbstkollision.rs:347-357
@@ -265,7 +240,7 @@ Quader quader_punkte(const V3* p, int n, double m) {
 
 // selbstkollision.rs:370-384
 std::array<double, 3> naechster_dreieck(V3 p0, V3 p1, V3 p2, V3 x) {
-  V3 a = naechster_auf_dreieck(x, p0, p1, p2);
+  V3 a = naechster_auf_dreieck(x, p0, p1, p2).first;
   V3 e1 = sub(p1, p0), e2 = sub(p2, p0), r = sub(a, p0);
   double d11 = dot(e1, e1), d12 = dot(e1, e2), d22 = dot(e2, e2);
   double det = d11 * d22 - d12 * d12;

@@ -12,12 +12,17 @@ from garmentcraft_b200._lib import EXPORTS, LIB_PATH, lib
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "klon3d_step.h")
+MESH_HEADER = os.path.join(ROOT, "include", "klon3d_mesh.h")
 
 
 def header_functions():
-    txt = open(HEADER).read()
-    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(k3d_[a-z0-9_]+)\s*\(", txt)))
+    names = set()
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if h.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", h)).read()
+            txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+            names.update(re.findall(r"\b(k3d_[a-z0-9_]+)\s*\(", txt))
+    return sorted(names)
 
 
 def test_header_names_every_export():
@@ -38,13 +43,14 @@ STRUCTS = {
     "k3d_scene": _abi.K3dScene, "k3d_stats": _abi.K3dStats, "k3d_cg_result": _abi.K3dCgResult,
     "k3d_system_readback": _abi.K3dSystemReadback, "k3d_material": _abi.K3dMaterial,
     "k3d_piece": _abi.K3dPiece, "k3d_seam_part": _abi.K3dSeamPart, "k3d_seam": _abi.K3dSeam,
-    "k3d_pattern": _abi.K3dPattern,
+    "k3d_pattern": _abi.K3dPattern, "k3d_mesh_info": _abi.K3dMeshInfo,
 }
 
 
 def test_struct_layouts_match(tmp_path):
     src = tmp_path / "sizes.c"
-    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', f'#include "{MESH_HEADER}"',
+             "int main(void){"]
     for name, cls in STRUCTS.items():
         lines.append(f'printf("{name} %zu\\n", sizeof({name}));')
         for f, _ in cls._fields_:

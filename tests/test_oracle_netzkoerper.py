@@ -1,0 +1,171 @@
+"""The oracle's restatement of the body mesh (sim/src/netzkoerper.rs) pinned
+by the reference's own tests (netzkoerper.rs:1001-1079): the cube's exact
+distance at faces, edges and corners, the grid query equal to the
+all-triangle query on a closed cylinder, the segment penetration from
+outside, and the refusals of Koerpernetz::neu. CPU only."""
+import math
+
+import numpy as np
+import pytest
+
+from garmentcraft_b200 import synth
+import oracle_py as O
+
+MASKE = (1 << 64) - 1
+
+
+class Xorshift:
+    """The reference tests' dependency-free generator (netzkoerper.rs:994-999)."""
+
+    def __init__(self, s):
+        self.s = s
+
+    def __call__(self):
+        s = self.s
+        s ^= (s << 13) & MASKE
+        s ^= s >> 7
+        s ^= (s << 17) & MASKE
+        self.s = s
+        return (s >> 11) / float(1 << 53)
+
+
+def abstand_wuerfel(x, h):
+    q = np.abs(x) - h
+    aussen = np.linalg.norm(np.maximum(q, 0.0), axis=-1)
+    return aussen + np.minimum(q.max(axis=-1), 0.0)
+
+
+def wuerfel():
+    p, d = synth.wuerfel_netz(1.0)
+    return O.Koerpernetz(p, d, 0.5)
+
+
+def wuerfel_punkte(n=20_000):
+    z = Xorshift(0x1234_5678_9ABC_DEF1)
+    return np.array([[3.0 * z() - 1.5 for _ in range(3)] for _ in range(n)])
+
+
+def test_wuerfel_abstand_exakt_auch_an_kanten_und_ecken():
+    # netzkoerper.rs:1001-1028
+    w = wuerfel()
+    i = w.info()
+    assert i["randkanten"] == 0 and abs(i["volumen"] - 8.0) < 1e-12
+    x = wuerfel_punkte()
+    r = w.naechster(x)
+    soll = abstand_wuerfel(x, 1.0)
+    assert np.max(np.abs(r["abstand"] - soll)) < 1e-12
+    zurueck = x - r["normale"] * r["abstand"][:, None]
+    assert np.max(np.linalg.norm(zurueck - r["punkt"], axis=1)) < 1e-9
+    r = w.naechster(np.array([[2.0, 2.0, 2.0], [1.5, 0.3, 1.5], [0.9, 0.95, 0.0]]))
+    assert r["region"][0] in (0, 1, 2) and abs(r["abstand"][0] - math.sqrt(3.0)) < 1e-12
+    assert r["region"][1] in (3, 4, 5) and abs(r["abstand"][1] - math.sqrt(0.5)) < 1e-12
+    assert abs(r["abstand"][2] + 0.05) < 1e-12
+
+
+def zylinder_punkte(n=20_000):
+    z = Xorshift(0xFEED_BEEF_DEAD_CAFE)
+    out = np.empty((n, 3))
+    for q in range(n):
+        r = 0.07 + 0.04 * z()
+        w = 2.0 * math.pi * z()
+        out[q] = (r * math.cos(w), r * math.sin(w), -0.32 + 0.44 * z())
+    return out
+
+
+def test_gitter_wie_alle_dreiecke():
+    # netzkoerper.rs:1032-1059
+    p, d = synth.zylinder_netz(0.09, -0.3, 0.1, 96, 20)
+    k = O.Koerpernetz(p, d, 0.01)
+    assert k.info()["randkanten"] == 0
+    x = zylinder_punkte()
+    alle = k.naechster(x)
+    g = k.naechster(x, 0.01)
+    hit = g["dreieck"] >= 0
+    assert np.max(np.abs(g["abstand"][hit] - alle["abstand"][hit])) < 1e-12
+    assert np.max(np.linalg.norm(g["punkt"][hit] - alle["punkt"][hit], axis=1)) < 1e-12
+    assert np.all(np.abs(alle["abstand"][~hit]) >= 0.01)
+    innen, aussen, weit = int(np.sum(g["abstand"][hit] < 0)), int(np.sum(g["abstand"][hit] >= 0)), int(np.sum(~hit))
+    assert innen > 1000 and aussen > 1000 and weit > 1000, (innen, aussen, weit)
+
+
+def test_durchstoss_von_aussen():
+    # netzkoerper.rs:1063-1079
+    w = wuerfel()
+    a = np.array([[0.2, 0.3, 3.0], [0.2, 0.3, 0.0], [0.2, 0.3, 3.0], [0.5, 0.5, 2.0]])
+    b = np.array([[0.2, 0.3, -3.0], [0.2, 0.3, -3.0], [0.2, 0.3, 1.5], [0.5, 0.5, 0.0]])
+    r = w.durchstoss(a, b)
+    assert r["dreieck"][0] >= 0 and np.linalg.norm(r["punkt"][0] - [0.2, 0.3, 1.0]) < 1e-12
+    assert abs(r["normale"][0][2] - 1.0) < 1e-12
+    assert r["dreieck"][1] < 0 and r["dreieck"][2] < 0
+    assert r["dreieck"][3] >= 0 and abs(r["punkt"][3][2] - 1.0) < 1e-12
+    q, dd = synth.zylinder_netz(0.05, -0.001, 0.001, 64, 1)
+    platte = O.Koerpernetz(q, dd, 0.01)
+    r = platte.durchstoss([[0.01, 0.0, 0.05]], [[0.01, 0.0, -0.05]])
+    assert r["dreieck"][0] >= 0 and abs(r["punkt"][0][2] - 0.001) < 1e-12 and r["normale"][0][2] > 0.999
+
+
+def test_neu_weist_ab():
+    # Koerpernetz::neu (:297-367): what it refuses
+    p, d = synth.wuerfel_netz(1.0)
+    with pytest.raises(ValueError, match="without triangles"):
+        O.Koerpernetz(p, d[:0], 0.5)
+    with pytest.raises(ValueError, match="search depth"):
+        O.Koerpernetz(p, d, 0.0)
+    bad = d.copy()
+    bad[3, 1] = 8
+    with pytest.raises(ValueError, match="out of range"):
+        O.Koerpernetz(p, bad, 0.5)
+    flip = d.copy()
+    flip[0] = flip[0][[0, 2, 1]]
+    with pytest.raises(ValueError, match="inconsistent"):
+        O.Koerpernetz(p, flip, 0.5)
+    with pytest.raises(ValueError, match="volume"):
+        O.Koerpernetz(p, d[:, [0, 2, 1]], 0.5)
+    with pytest.raises(ValueError, match="more than two"):
+        O.Koerpernetz(p, np.concatenate([d, d[:1]]), 0.5)
+
+
+def test_offene_kanten_werden_gezaehlt():
+    p, d = synth.wuerfel_netz(1.0)
+    k = O.Koerpernetz(p, d[:-1], 0.5)  # one triangle missing: three open edges
+    assert k.info()["randkanten"] == 3
+
+
+def test_nachfuehren_und_gitter_waechst():
+    p, d = synth.wuerfel_netz(1.0)
+    k = O.Koerpernetz(p, d, 0.25)
+    g0 = k.info()
+    k.nachfuehren(p * 0.5)  # shrinks: the grid keeps its box
+    g1 = k.info()
+    assert np.array_equal(g0["zahl"], g1["zahl"]) and np.array_equal(g0["ursprung"], g1["ursprung"])
+    assert abs(g1["volumen"] - 1.0) < 1e-12
+    x = wuerfel_punkte(2000)
+    assert np.max(np.abs(k.naechster(x)["abstand"] - abstand_wuerfel(x, 0.5))) < 1e-12
+    k.nachfuehren(p + [2.0, 0.0, 0.0])  # moves beyond the box: the grid grows
+    g2 = k.info()
+    assert g2["zahl"][0] > g1["zahl"][0] and g2["ursprung"][0] == g1["ursprung"][0]
+    with pytest.raises(ValueError, match="volume"):
+        k.nachfuehren(p * np.array([-1.0, 1.0, 1.0]))  # mirrored: turned inside out
+
+
+def test_punktnormalen_winkelgewichtet():
+    # punktabhaengig (:257-290): at a cube corner the three faces meet at
+    # right angles; the corner normal is the diagonal whatever the split
+    w = wuerfel()
+    t = w.tabellen()
+    p, _ = synth.wuerfel_netz(1.0)
+    soll = p / np.linalg.norm(p, axis=1, keepdims=True)
+    assert np.max(np.abs(t["punktnormale"] - soll)) < 1e-15
+    fn = t["flaechennormale"]
+    assert np.allclose(np.abs(fn).sum(axis=1), 1.0)
+
+
+def test_sdf_definition_am_wuerfel():
+    w = wuerfel()
+    dims, o, s = (13, 11, 9), np.array([-1.6, -1.4, -1.2]), 0.27
+    g = w.sdf(dims, o, s)
+    k, j, i = np.meshgrid(np.arange(dims[2]), np.arange(dims[1]), np.arange(dims[0]), indexing="ij")
+    x = np.stack([o[0] + s * i, o[1] + s * j, o[2] + s * k], axis=-1)
+    assert np.max(np.abs(g - abstand_wuerfel(x, 1.0))) < 1e-6
+    gb = w.sdf(dims, o, s, band=0.4)
+    assert np.array_equal(gb, np.clip(g, -0.4, 0.4))
