@@ -10,7 +10,7 @@ c_u32_p = C.POINTER(C.c_uint32)
 c_u8_p = C.POINTER(C.c_uint8)
 c_f32_p = C.POINTER(C.c_float)
 
-K3D_ABI_VERSION = 3
+K3D_ABI_VERSION = 4
 
 K3D_OK = 0
 K3D_NOT_CONVERGED = 1
@@ -25,6 +25,7 @@ K3D_MIXED = 1
 
 K3D_BODY_CYLINDER = 0
 K3D_BODY_SDF_GRID = 1
+K3D_BODY_MESH = 2
 
 STATUS_NAMES = {
     0: "K3D_OK", 1: "K3D_NOT_CONVERGED", 2: "K3D_BREAKDOWN", 3: "K3D_NON_FINITE",
@@ -72,6 +73,7 @@ class K3dBody(C.Structure):
         ("sdf", c_f32_p),
         ("instanz", C.c_int32),
         ("pad", C.c_int32),
+        ("netz", C.c_void_p),
     ]
 
 

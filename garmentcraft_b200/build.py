@@ -15,7 +15,7 @@ LIB = os.path.join(OUT_DIR, "libklon3d_b200.so")
 SOURCES = ["k3d_step.cu", "k3d_build.cu", "k3d_host.cpp", "scene_build.cpp", "k3d_noalloc.cu", "k3d_selbst.cu",
            "k3d_selbst_host.cpp", "k3d_adjoint.cu", "k3d_netz.cu"]
 HEADERS = ["k3d_step.h", "k3d_device.cuh", "k3d_step_common.cuh", "scene_build.h", "k3d_selbst.h",
-           "k3d_selbst_host.h", "k3d_adjoint.h"]
+           "k3d_selbst_host.h", "k3d_adjoint.h", "k3d_vec.cuh", "k3d_netz.cuh", "k3d_netz.h"]
 # Per-file flags. The build of the system and the self-collision stage round
 # every product and sum on their own (no fused multiply-add), as the
 # reference's arithmetic does: the element term of k3d_build.cu needs it, and

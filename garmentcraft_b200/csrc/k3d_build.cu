@@ -408,8 +408,10 @@ __global__ void __launch_bounds__(kBlock) assemble_kernel(const __grid_constant_
 // (A p)_i = sum over the row's blocks of B p_col, p = w + beta c from `buf`.
 
 // ------------------------------------------------------------ friction + integration
-// implizit.rs:957-1013 (no mesh bodies: the segment check does not apply).
-__device__ void integrate(const StepArgs& a, double (&cnt)[3]) {
+// implizit.rs:957-1013: friction, the new position, the segment check against
+// mesh bodies (entry point pushed out by the collision distance, the impact's
+// normal velocity removed and Coulomb on the impact), the push-out.
+__device__ void integrate(const StepArgs& a, double (&cnt)[4]) {
   const double h = a.h;
   K3D_FOR(i, a.n) {
     if (!a.frei[i]) {
@@ -437,8 +439,32 @@ __device__ void integrate(const StepArgs& a, double (&cnt)[3]) {
         fl |= 4u;
       }
     }
-    D3 x = ld3(a.x, uint32_t(i)) + v * h;
+    const D3 alt = ld3(a.x, uint32_t(i));
+    D3 x = alt + v * h;
     const int inst = a.pinst ? int(a.pinst[i]) : 0;
+    if (a.durchstoss_pruefen) {
+      for (int kb = 0; kb < a.n_bodies; ++kb) {
+        const Body& k = a.bodies[kb];
+        if (k.art != 2 || (k.inst >= 0 && k.inst != inst)) continue;
+        const D3 vers = d3(k.punkt[0], k.punkt[1], k.punkt[2]);
+        D3 pl, nk;
+        uint32_t t;
+        if (netz::durchstoss(*k.netz, alt - vers, x - vers, pl, nk, t)) {
+          cnt[3] += 1.0;
+          x = (pl + vers) + nk * a.kabst[i];
+          const D3 vk = d3(k.vel[0], k.vel[1], k.vel[2]);
+          const D3 rel = v - vk;
+          const double vn = dot(rel, nk);
+          if (vn < 0.0) {
+            D3 tt = rel - nk * vn;
+            const double lt = norm(tt);
+            const double grenze = a.reib[i] * -vn;
+            tt = lt <= grenze ? d3(0.0, 0.0, 0.0) : tt * (1.0 - grenze / lt);
+            v = vk + tt;
+          }
+        }
+      }
+    }
     for (int kb = 0; kb < a.n_bodies; ++kb) {
       if (a.bodies[kb].inst >= 0 && a.bodies[kb].inst != inst) continue;
       D3 nn;
@@ -493,11 +519,11 @@ __global__ void __launch_bounds__(kBlock) build_points_kernel(const __grid_const
 // 128 registers a thread gets at this shape keep the FP32 form free of spills.
 
 __global__ void __launch_bounds__(kBlock) integrate_kernel(const __grid_constant__ StepArgs a) {
-  __shared__ double red[3][32];
-  double cnt[3] = {0.0, 0.0, 0.0};
+  __shared__ double red[4][32];
+  double cnt[4] = {0.0, 0.0, 0.0, 0.0};
   integrate(a, cnt);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 0; k < 4; ++k) {
     double x = cnt[k];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
@@ -505,8 +531,8 @@ __global__ void __launch_bounds__(kBlock) integrate_kernel(const __grid_constant
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    const int slot[3] = {ST_CONTACTS, ST_STICKING, ST_NONFINITE};
-    for (int k = 0; k < 3; ++k) {
+    const int slot[4] = {ST_CONTACTS, ST_STICKING, ST_NONFINITE, ST_PENETRATIONS};
+    for (int k = 0; k < 4; ++k) {
       double t = 0.0;
       for (int w = 0; w < int(blockDim.x >> 5); ++w) t += red[k][w];
       if (t > 0.0) atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[slot[k]]), (unsigned long long)t);

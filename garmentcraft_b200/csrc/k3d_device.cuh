@@ -16,31 +16,10 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "k3d_netz.cuh"
+#include "k3d_vec.cuh"
+
 namespace k3d {
-
-template <typename R>
-struct alignas(4 * sizeof(R)) R4 {
-  R x, y, z, w;
-};
-
-struct D3 {
-  double x, y, z;
-};
-__device__ __forceinline__ D3 d3(double x, double y, double z) { return {x, y, z}; }
-__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-__device__ __forceinline__ D3 operator*(D3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
-__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ D3 cross(D3 a, D3 b) {
-  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
-}
-__device__ __forceinline__ double norm(D3 a) { return sqrt(dot(a, a)); }
-__device__ __forceinline__ D3 ld3(const double* p, uint32_t i) { return {p[3 * i], p[3 * i + 1], p[3 * i + 2]}; }
-__device__ __forceinline__ void st3(double* p, uint32_t i, D3 v) {
-  p[3 * i] = v.x;
-  p[3 * i + 1] = v.y;
-  p[3 * i + 2] = v.z;
-}
 
 // Body descriptor as the kernel reads it (k3d_body, plus the substep offset).
 struct Body {
@@ -49,13 +28,24 @@ struct Body {
   double punkt[3], achse[3], radius, vel[3], ursprung[3], spacing;
   const float* sdf;  // device copy of the grid
   int inst;          // the instance (independent drape) it acts on, -1 = every instance
+  const netz::Dev* netz;  // mesh body: the mesh's tables (device)
 };
 constexpr int kMaxBodies = 64;
 
-// Contact query, sim/src/koerper.rs:69-91 for the cylinder; the SDF grid is a
-// trilinear interpolant of node values (value and gradient), no contact
-// outside the grid.
+// Contact query, sim/src/koerper.rs:69-91 for the cylinder and the mesh (the
+// exact nearest point within max(search depth, distance), koerper.rs:80-87);
+// the SDF grid is a trilinear interpolant of node values (value and
+// gradient), no contact outside the grid.
 __device__ inline bool kontakt(const Body& k, D3 x, double abstand, D3& normale, double& tiefe) {
+  if (k.art == 2) {
+    netz::Treffer t;
+    const D3 xl = x - d3(k.punkt[0], k.punkt[1], k.punkt[2]);
+    if (!netz::naechster(*k.netz, xl, fmax(k.netz->suchtiefe, abstand), t)) return false;
+    tiefe = abstand - t.abstand;
+    if (!(tiefe > 0.0)) return false;
+    normale = t.normale;
+    return true;
+  }
   if (k.art == 0) {
     D3 ax = d3(k.achse[0], k.achse[1], k.achse[2]);
     D3 a = ax * (1.0 / norm(ax));

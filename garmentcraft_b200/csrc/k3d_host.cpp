@@ -12,6 +12,7 @@
 
 #include "../../include/klon3d_step.h"
 #include "k3d_adjoint.h"
+#include "k3d_netz.h"
 #include "k3d_selbst_host.h"
 #include "k3d_step.h"
 #include "scene_build.h"
@@ -51,6 +52,7 @@ struct k3d_solver {
   k3d_simparams sim{};
   std::vector<k3d_body> bodies;         // frame-start bodies as last given
   std::vector<void*> sdf_dev;           // device copies of SDF grids
+  std::vector<const netz::Dev*> netz_dev;  // mesh bodies' tables (owned by their k3d_mesh)
   std::vector<int64_t> seam_slot;       // spring index of each seam, -1 if not streamed
   std::vector<double2> s_kl_host;
   int64_t launches = 0;
@@ -349,6 +351,7 @@ static void release_device(k3d_solver* h) {
   h->arena = Arena{};
   for (void* p : h->sdf_dev) cudaFree(p);
   h->sdf_dev.clear();
+  h->netz_dev.clear();
   h->uploaded = false;
 }
 
@@ -429,6 +432,8 @@ static k3d_status validate(const k3d_scene* s) {
     if (k.instanz < -1 || (s->n_instanzen > 1 && k.instanz >= s->n_instanzen)) return K3D_BAD_ARGUMENT;
     if (k.art == K3D_BODY_SDF_GRID) {
       if (!k.sdf || k.dims[0] < 2 || k.dims[1] < 2 || k.dims[2] < 2 || !(k.spacing > 0.0)) return K3D_BAD_ARGUMENT;
+    } else if (k.art == K3D_BODY_MESH) {
+      if (!k.netz) return K3D_BAD_ARGUMENT;
     } else if (k.art != K3D_BODY_CYLINDER) {
       return K3D_BAD_ARGUMENT;
     }
@@ -745,6 +750,13 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
       K3D_CUDA(h, up(d, k.sdf, 4 * cnt));
     }
     h->sdf_dev.push_back(d);
+    const netz::Dev* nv = nullptr;
+    if (k.art == K3D_BODY_MESH) {
+      int dev = -1;
+      nv = mesh_device_view(k.netz, &dev);
+      if (!nv || dev != h->device) return fail(h, K3D_BAD_ARGUMENT, "a mesh body lives on another device");
+    }
+    h->netz_dev.push_back(nv);
   }
   K3D_CUDA(h, cudaStreamSynchronize(st));
   if (h->p.selbstkollision) {
@@ -789,6 +801,7 @@ static void step_args(k3d_solver* h, int mode, double t_bodies, bool need_load) 
   a.need_load = (need_load || h->p.normalkraft_aus_last) ? 1 : 0;
   a.first_step = (mode == MODE_STEP && h->first_step) ? 1 : 0;
   a.n_bodies = int(h->bodies.size());
+  a.durchstoss_pruefen = h->p.durchstoss_pruefen ? 1 : 0;
   for (int b = 0; b < a.n_bodies; ++b) {
     const k3d_body& k = h->bodies[b];
     Body& d = a.bodies[b];
@@ -803,6 +816,7 @@ static void step_args(k3d_solver* h, int mode, double t_bodies, bool need_load) 
     d.radius = k.radius;
     d.spacing = k.spacing;
     d.sdf = static_cast<const float*>(h->sdf_dev[b]);
+    d.netz = h->netz_dev[b];
     d.inst = h->n_grp > 1 ? k.instanz : -1;
   }
 }
@@ -873,6 +887,7 @@ static k3d_status read_stats(k3d_solver* h, k3d_stats* out) {
     out->kontakte = st[ST_CONTACTS];
     out->haftend = st[ST_STICKING];
     out->freigegeben = st[ST_RELEASED];
+    out->durchstoesse = st[ST_PENETRATIONS];
     out->rest_max = rm[0];
     out->zusammenbrueche = st[ST_BREAKDOWNS];
     out->dv_max = rm[1];
@@ -1218,6 +1233,8 @@ static k3d_status adj_check(k3d_solver* h) {
   if (h->p.normalkraft_aus_last) return fail(h, K3D_BAD_ARGUMENT, "the adjoint needs normalkraft_aus_last off");
   if (h->bodies.size() > size_t(kMaxAdjointBodies))
     return fail(h, K3D_BAD_ARGUMENT, "the adjoint takes at most 14 bodies");
+  for (const k3d_body& k : h->bodies)
+    if (k.art == K3D_BODY_MESH) return fail(h, K3D_BAD_ARGUMENT, "the adjoint takes cylinder and grid bodies only");
   return K3D_OK;
 }
 

@@ -39,175 +39,6 @@ namespace netz {
 constexpr int kT = 256;
 constexpr int kTile = 128;  // triangles per shared-memory tile of the all-triangle query
 
-struct Dev {
-  int64_t n, nd;
-  const double* p;  // 3 per point
-  const uint4* d;   // triangle points (w unused)
-  double4* fn;      // face normal
-  const uint4* nb;  // neighbour across edge k (the triangle itself at an open edge)
-  double4* pn;      // angle-weighted point normal
-  double4* kg;      // bounding sphere: centre, radius
-  double* wk;       // corner angles, 3 per triangle
-  double* vt;       // volume term per triangle
-  const uint32_t *pi_off, *pi_ent;
-  // grid
-  double u0, u1, u2, zelle;
-  int32_t zx, zy, zz;
-  uint32_t *anf, *ein, *cur;
-  uint32_t cap;
-};
-
-__device__ __forceinline__ D3 ld4(const double4& v) { return d3(v.x, v.y, v.z); }
-__device__ __forceinline__ D3 punkt(const Dev& g, uint32_t i) { return ld3(g.p, i); }
-
-// netzkoerper.rs:220-227
-__device__ __forceinline__ D3 normiert(D3 a) {
-  const double l = norm(a);
-  if (l > 0.0) return a * (1.0 / l);
-  return d3(0.0, 0.0, 0.0);
-}
-
-// `f64 as i64` (saturating, NaN to 0), then the cell index of netzkoerper.rs:87-92
-__device__ __forceinline__ int64_t als_i64(double v) {
-  if (isnan(v)) return 0;
-  if (v >= 9.2233720368547758e18) return INT64_MAX;
-  if (v <= -9.2233720368547758e18) return INT64_MIN;
-  return int64_t(v);
-}
-__device__ __forceinline__ void zell_index(const Dev& g, D3 x, int64_t k[3]) {
-  k[0] = als_i64(floor((x.x - g.u0) / g.zelle));
-  k[1] = als_i64(floor((x.y - g.u1) / g.zelle));
-  k[2] = als_i64(floor((x.z - g.u2) / g.zelle));
-}
-// netzkoerper.rs:117-128: the clamped cell range of the box [lo, hi]
-__device__ __forceinline__ bool bereich(const Dev& g, D3 lo, D3 hi, int r0[3], int r1[3]) {
-  int64_t a[3], b[3];
-  zell_index(g, lo, a);
-  zell_index(g, hi, b);
-  const int64_t z[3] = {g.zx, g.zy, g.zz};
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    if (b[q] < 0 || a[q] >= z[q]) return false;
-    r0[q] = int(a[q] < 0 ? 0 : a[q]);
-    r1[q] = int(b[q] > z[q] - 1 ? z[q] - 1 : b[q]);
-  }
-  return true;
-}
-
-// netzkoerper.rs:185-216 (Ericson 2005, 5.1.5); regions 0-2 corner, 3-5 edge, 6 face
-__device__ __forceinline__ D3 naechster_auf_dreieck(D3 p, D3 a, D3 b, D3 c, int& reg) {
-  auto quot = [](double z, double n) { return n > 0.0 ? z / n : 0.0; };
-  const D3 ab = b - a, ac = c - a, ap = p - a;
-  const double d1 = dot(ab, ap), d2 = dot(ac, ap);
-  if (d1 <= 0.0 && d2 <= 0.0) {
-    reg = 0;
-    return a;
-  }
-  const D3 bp = p - b;
-  const double d3_ = dot(ab, bp), d4 = dot(ac, bp);
-  if (d3_ >= 0.0 && d4 <= d3_) {
-    reg = 1;
-    return b;
-  }
-  const double vc = d1 * d4 - d3_ * d2;
-  if (vc <= 0.0 && d1 >= 0.0 && d3_ <= 0.0) {
-    reg = 3;
-    return a + ab * quot(d1, d1 - d3_);
-  }
-  const D3 cp = p - c;
-  const double d5 = dot(ab, cp), d6 = dot(ac, cp);
-  if (d6 >= 0.0 && d5 <= d6) {
-    reg = 2;
-    return c;
-  }
-  const double vb = d5 * d2 - d1 * d6;
-  if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
-    reg = 5;
-    return a + ac * quot(d2, d2 - d6);
-  }
-  const double va = d3_ * d6 - d5 * d4;
-  if (va <= 0.0 && d4 - d3_ >= 0.0 && d5 - d6 >= 0.0) {
-    const double w = quot(d4 - d3_, (d4 - d3_) + (d5 - d6));
-    reg = 4;
-    return b + (c - b) * w;
-  }
-  const double s = va + vb + vc;
-  const double v = quot(vb, s), w = quot(vc, s);
-  reg = 6;
-  return a + (ab * v + ac * w);
-}
-
-// netzkoerper.rs:431-447
-__device__ __forceinline__ D3 pseudonormale(const Dev& g, uint32_t t, int r) {
-  if (r == 6) return ld4(g.fn[t]);
-  if (r >= 3) {
-    const uint4 o4 = g.nb[t];
-    const uint32_t o = (r == 3) ? o4.x : (r == 4 ? o4.y : o4.z);
-    if (o == t) return ld4(g.fn[t]);
-    return normiert(ld4(g.fn[t]) + ld4(g.fn[o]));
-  }
-  const uint4 d = g.d[t];
-  return ld4(g.pn[r == 0 ? d.x : (r == 1 ? d.y : d.z)]);
-}
-
-struct Treffer {
-  double abstand;
-  D3 punkt, normale;
-  uint32_t dreieck;
-  int region;
-};
-// netzkoerper.rs:492-499
-__device__ __forceinline__ Treffer ergebnis(const Dev& g, D3 x, uint32_t t, D3 c, int r) {
-  const D3 pn = pseudonormale(g, t, r);
-  const D3 d = x - c;
-  const double l = norm(d);
-  const bool aussen = dot(d, pn) >= 0.0;
-  const D3 nrm = l > 1e-12 ? d * (aussen ? 1.0 / l : -1.0 / l) : pn;
-  return Treffer{aussen ? l : -l, c, nrm, t, r};
-}
-
-// A conservative sphere test: the triangle may hold a point no farther than
-// `best` (the slack keeps ties and rounding on the safe side).
-__device__ __forceinline__ bool kugel_nah(D3 x, double4 k, double best) {
-  const double b = norm(x - d3(k.x, k.y, k.z)) - k.w;
-  return !(b > best + 1e-12 * (fabs(best) + fabs(b)) + 1e-300);
-}
-
-// netzkoerper.rs:503-539 over the grid, ties to the smallest triangle index
-__device__ bool naechster(const Dev& g, D3 x, double radius, Treffer& out) {
-  int r0[3], r1[3];
-  if (!bereich(g, x - d3(radius, radius, radius), x + d3(radius, radius, radius), r0, r1)) return false;
-  double best = radius;
-  bool hit = false;
-  uint32_t bt = 0xffffffffu;
-  D3 bq = d3(0, 0, 0);
-  int br = 6;
-  for (int kz = r0[2]; kz <= r1[2]; ++kz)
-    for (int ky = r0[1]; ky <= r1[1]; ++ky)
-      for (int kx = r0[0]; kx <= r1[0]; ++kx) {
-        const int64_t z = (int64_t(kz) * g.zy + ky) * g.zx + kx;
-        const uint32_t e1 = g.anf[z + 1];
-        for (uint32_t e = g.anf[z]; e < e1; ++e) {
-          const uint32_t t = g.ein[e];
-          if (!kugel_nah(x, g.kg[t], best)) continue;
-          const uint4 d = g.d[t];
-          int reg;
-          const D3 q = naechster_auf_dreieck(x, punkt(g, d.x), punkt(g, d.y), punkt(g, d.z), reg);
-          const double l = norm(x - q);
-          if (l < best || (hit && l == best && t < bt)) {
-            best = l;
-            hit = true;
-            bt = t;
-            bq = q;
-            br = reg;
-          }
-        }
-      }
-  if (!hit) return false;
-  out = ergebnis(g, x, bt, bq, br);
-  return true;
-}
-
 // ---------------------------------------------------------------- point-dependent tables
 // netzkoerper.rs:257-290, per triangle: face normal, corner angles, sphere, volume term
 __global__ void __launch_bounds__(kT) flaechen_kernel(const __grid_constant__ Dev g) {
@@ -452,53 +283,17 @@ __global__ void __launch_bounds__(kTile) alle_kernel(const __grid_constant__ Dev
   }
 }
 
-// netzkoerper.rs:541-593, ties in the segment parameter to the smallest triangle
+// netzkoerper.rs:541-593 per segment
 __global__ void __launch_bounds__(kT) durchstoss_kernel(const __grid_constant__ Dev g, const double* pa,
                                                         const double* pb, int64_t n, int32_t* dr, double* pu,
                                                         double* no) {
   for (int64_t q = int64_t(blockIdx.x) * kT + threadIdx.x; q < n; q += int64_t(gridDim.x) * kT) {
-    const D3 a = ld3(pa, uint32_t(q)), b = ld3(pb, uint32_t(q));
-    const D3 d = b - a;
-    bool hit = false;
-    double sb = 0.0;
-    uint32_t tb = 0;
-    int r0[3], r1[3];
-    if (dot(d, d) >= 1e-24 &&
-        bereich(g, d3(fmin(a.x, b.x), fmin(a.y, b.y), fmin(a.z, b.z)), d3(fmax(a.x, b.x), fmax(a.y, b.y), fmax(a.z, b.z)),
-                r0, r1)) {
-      const double eps = 1e-12;
-      for (int kz = r0[2]; kz <= r1[2]; ++kz)
-        for (int ky = r0[1]; ky <= r1[1]; ++ky)
-          for (int kx = r0[0]; kx <= r1[0]; ++kx) {
-            const int64_t z = (int64_t(kz) * g.zy + ky) * g.zx + kx;
-            for (uint32_t e = g.anf[z]; e < g.anf[z + 1]; ++e) {
-              const uint32_t t = g.ein[e];
-              if (dot(d, ld4(g.fn[t])) >= 0.0) continue;
-              const uint4 tri = g.d[t];
-              const D3 p0 = punkt(g, tri.x), p1 = punkt(g, tri.y), p2 = punkt(g, tri.z);
-              const D3 e1 = p1 - p0, e2 = p2 - p0;
-              const D3 pv = cross(d, e2);
-              const double det = dot(e1, pv);
-              if (fabs(det) < 1e-30) continue;
-              const D3 tv = a - p0;
-              const double u = dot(tv, pv) / det;
-              if (u < -eps || u > 1.0 + eps) continue;
-              const D3 qv = cross(tv, e1);
-              const double v = dot(d, qv) / det;
-              if (v < -eps || u + v > 1.0 + eps) continue;
-              const double s = dot(e2, qv) / det;
-              if (s >= -eps && s <= 1.0 + eps && (!hit || s < sb || (s == sb && t < tb))) {
-                hit = true;
-                sb = s;
-                tb = t;
-              }
-            }
-          }
-    }
-    if (hit) {
-      dr[q] = int32_t(tb);
-      st3(pu, uint32_t(q), a + d * fmin(fmax(sb, 0.0), 1.0));
-      st3(no, uint32_t(q), ld4(g.fn[tb]));
+    D3 p, nn;
+    uint32_t t = 0;
+    if (durchstoss(g, ld3(pa, uint32_t(q)), ld3(pb, uint32_t(q)), p, nn, t)) {
+      dr[q] = int32_t(t);
+      st3(pu, uint32_t(q), p);
+      st3(no, uint32_t(q), nn);
     } else {
       dr[q] = -1;
       st3(pu, uint32_t(q), d3(0, 0, 0));
@@ -575,6 +370,7 @@ struct k3d_mesh {
   double u[3] = {0, 0, 0}, zelle = 0;
   int64_t zahl[3] = {0, 0, 0};
   Dev g{};
+  Dev* g_dev = nullptr;              // device copy of g, read by the step's contact query
   std::vector<double> punkte;        // host copy of the current positions
   std::vector<void*> fest;           // allocations of fixed size
   uint32_t *anf = nullptr, *cur = nullptr;  // cell starts and fill cursors (Z + 1)
@@ -687,6 +483,7 @@ k3d_status gitter(k3d_mesh* m, const double h[6]) {
   zellen_fuellen_kernel<<<blocks_for(g.nd), kT, 0, st>>>(g);
   zellen_sortieren_kernel<<<blocks_for(nz), kT, 0, st>>>(g, nz);
   NCK(cudaGetLastError(), "grid fill");
+  NCK(cudaMemcpyAsync(m->g_dev, &m->g, sizeof(Dev), cudaMemcpyHostToDevice, st), "grid view");
   m->kernels += 1 + 3 + 2;
   return K3D_OK;
 }
@@ -836,6 +633,8 @@ k3d_status k3d_mesh_create(const double* punkte, int64_t n, const uint32_t* drei
     Dev& g = m->g;
     g.n = n;
     g.nd = nd;
+    g.suchtiefe = suchtiefe;
+    NCK(alloc(m, m->g_dev, 1), "alloc");
     double* p = nullptr;
     uint4 *d = nullptr, *nb = nullptr;
     uint32_t *po = nullptr, *pe = nullptr;
@@ -1060,3 +859,11 @@ k3d_status k3d_mesh_sdf(k3d_mesh* m, const int32_t dims[3], const double ursprun
 }
 
 }  // extern "C"
+
+namespace k3d {
+const netz::Dev* mesh_device_view(const k3d_mesh* m, int* device) {
+  if (!m) return nullptr;
+  if (device) *device = m->device;
+  return m->g_dev;
+}
+}  // namespace k3d

@@ -24,6 +24,7 @@ enum StatSlot : int {
   ST_NONFINITE = 7,
   ST_LAST_ITERATIONS = 8,
   ST_HELD = 9,
+  ST_PENETRATIONS = 10,  // segment entries through a mesh body (ImplizitStatistik::durchstoesse)
   ST_COUNT = 16
 };
 
@@ -52,6 +53,7 @@ struct StepArgs {
   int64_t n, nt, nb, ns;
   int mode, first_step, need_load, normal_aus_last;
   int cg_max, n_bodies;
+  int durchstoss_pruefen, pad0;  // segment check against mesh bodies (implizit.rs:988-1002)
   double h, daempf, g[3], tol, kontakt_rand, boden;
   Body bodies[kMaxBodies];
   // points (double)

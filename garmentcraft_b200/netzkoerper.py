@@ -149,6 +149,17 @@ class Koerpernetz:
                     geschwindigkeit=tuple(float(v) for v in geschwindigkeit), sdf=np.ascontiguousarray(g.ravel()))
 
     @property
+    def c_handle(self):
+        """The k3d_mesh pointer for k3d_body.netz."""
+        return self._h.value if self._h is not None else None
+
+    def body(self, versatz=(0.0, 0.0, 0.0), geschwindigkeit=(0.0, 0.0, 0.0), instanz: int = -1) -> dict:
+        """Koerper::Netz (koerper.rs:20-24) as a body dict for a scene; the
+        dict holds this mesh, which must outlive the solver's use of it."""
+        return dict(art=_abi.K3D_BODY_MESH, punkt=tuple(float(v) for v in versatz),
+                    geschwindigkeit=tuple(float(v) for v in geschwindigkeit), instanz=int(instanz), netz=self)
+
+    @property
     def letzte_ms(self) -> float:
         """Device time of the last call's kernels (CUDA events), ms."""
         return float(self.info().ms_letzter_aufruf)

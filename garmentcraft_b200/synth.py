@@ -510,6 +510,8 @@ def body_to_c(body: dict) -> _abi.K3dBody:
     kb.instanz = int(body.get("instanz", -1))
     sdf = body.get("sdf")
     kb.sdf = _abi.ptr(sdf, C.c_float) if sdf is not None else None
+    netz = body.get("netz")
+    kb.netz = netz.c_handle if netz is not None else None
     return kb
 
 
@@ -600,3 +602,33 @@ def koerper_netz(segmente: int = 256, ringe: int = 73, halbachsen=(0.18, 0.12, 0
     if np.einsum("ij,ij->i", q[:, 0], np.cross(q[:, 1], q[:, 2])).sum() < 0.0:
         d = d[:, [0, 2, 1]]
     return p, np.ascontiguousarray(d)
+
+
+def punkteregen(netz_punkte, kante_m: float = 0.01, hoehe_m: float = 0.05, rand_m: float = 0.02):
+    """Loose points raining onto a body mesh: a grid at `kante_m` spacing
+    over the mesh's footprint grown by `rand_m`, `hoehe_m` above its top, at
+    rest; mass 1e-5 kg, collision distance 0.2 mm, friction 0.6, gravity
+    only (the point rain of the reference's mesh-body tests,
+    sim/tests/band/mod.rs:279-315, over a synthetic body). No body is
+    attached; add one to the scene's koerper."""
+    from .szene import Szene
+    p = np.asarray(netz_punkte, dtype=np.float64)
+    lo, hi = p.min(axis=0) - rand_m, p.max(axis=0) + rand_m
+    xs = np.arange(lo[0], hi[0] + 0.5 * kante_m, kante_m)
+    ys = np.arange(lo[1], hi[1] + 0.5 * kante_m, kante_m)
+    gx, gy = np.meshgrid(xs, ys, indexing="ij")
+    x = np.column_stack([gx.ravel(), gy.ravel(), np.full(gx.size, hi[2] - rand_m + hoehe_m)])
+    n = x.shape[0]
+    m = 1e-5
+
+    def leer(cols, dt=np.float64):
+        return np.zeros((0, cols) if cols else 0, dtype=dt)
+    return Szene(x=x, v=np.zeros((n, 3)), masse=np.full(n, m), w=np.full(n, 1.0 / m),
+                 kollisionsabstand=np.full(n, 0.2e-3), reibung=np.full(n, 0.6),
+                 abstand_punkte=leer(2, np.uint32), abstand_ruhe=leer(0), abstand_nachgiebigkeit=leer(0),
+                 membran_kante=leer(0, np.uint8), naht_punkte=leer(2, np.uint32), naht_ruhe=leer(0),
+                 biegung_punkte=leer(4, np.uint32), biegung_ruhe=leer(0), biegung_nachgiebigkeit=leer(0),
+                 membran_punkte=leer(3, np.uint32), membran_flaeche=leer(0), membran_ruhe_inv=leer(4),
+                 membran_kette=leer(2), membran_schuss=leer(2), membran_steif=leer(3),
+                 dreiecke=leer(3, np.uint32), ruhe_inv=leer(4),
+                 param=Simparameter(bild_dt=1.0 / 60.0, schwerkraft=(0.0, 0.0, -9.81), daempfung=0.0))

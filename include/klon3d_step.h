@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define K3D_ABI_VERSION 3
+#define K3D_ABI_VERSION 4
 
 /* Status of a call. Unconverged CG is data (k3d_cg_result), not an error,
  * as in CgLauf (sim/src/implizit.rs:294-299). */
@@ -70,9 +70,17 @@ typedef struct k3d_simparams {
 
 /* Body kinds. K3D_BODY_CYLINDER is Koerper::Zylinder (sim/src/koerper.rs:19).
  * K3D_BODY_SDF_GRID is a sampled signed-distance grid with trilinear value
- * and gradient; the reference's mesh body answers the same query exactly
- * (sim/src/netzkoerper.rs:503-539) and has no sampled form. */
-enum { K3D_BODY_CYLINDER = 0, K3D_BODY_SDF_GRID = 1 };
+ * and gradient (k3d_mesh_sdf in klon3d_mesh.h samples a body mesh into one).
+ * K3D_BODY_MESH is Koerper::Netz (koerper.rs:20-24): a k3d_mesh (klon3d_mesh.h)
+ * on the solver's device at offset `punkt`, moving rigidly with
+ * `geschwindigkeit`; its contact is the exact nearest query within
+ * max(search depth, distance) (koerper.rs:80-87), and the step's segment
+ * check (k3d_params.durchstoss_pruefen, implizit.rs:988-1002) tests the
+ * points' paths against it. The mesh must outlive the solver's use of it;
+ * k3d_mesh_update between frames moves it. */
+enum { K3D_BODY_CYLINDER = 0, K3D_BODY_SDF_GRID = 1, K3D_BODY_MESH = 2 };
+
+struct k3d_mesh;
 
 typedef struct k3d_body {
   int32_t art;              /* K3D_BODY_* */
@@ -86,6 +94,7 @@ typedef struct k3d_body {
   const float* sdf;         /* grid: dims[0]*dims[1]*dims[2] values, x fastest (host) */
   int32_t instanz;          /* the instance it acts on in a batch scene, -1 = every instance */
   int32_t pad;
+  const struct k3d_mesh* netz; /* K3D_BODY_MESH: the mesh (null otherwise) */
 } k3d_body;
 
 /* Szene (sim/src/szene.rs:198-269): the arrays the implicit step reads or

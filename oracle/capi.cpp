@@ -49,6 +49,8 @@ Koerperdaten koerper_aus(const k3d_body* kb, int32_t n) {
     }
     k.radius = s.radius;
     k.spacing = s.spacing;
+    // the oracle's mesh bodies carry an oracle Koerpernetz (orc_netz_neu) in `netz`
+    if (s.art == K3D_BODY_MESH) k.netz = reinterpret_cast<const Koerpernetz*>(s.netz);
     if (s.art == K3D_BODY_SDF_GRID && s.sdf) {
       size_t nn = size_t(s.dims[0]) * size_t(s.dims[1]) * size_t(s.dims[2]);
       out.gitter[b].assign(s.sdf, s.sdf + nn);
@@ -421,6 +423,7 @@ void orc_sim_frames(void* h, int32_t n, k3d_stats* st) {
     summe.kontakte += b.kontakte;
     summe.haftend += b.haftend;
     summe.freigegeben += b.freigegeben;
+    summe.durchstoesse += b.durchstoesse;
     summe.rest_max = std::max(summe.rest_max, b.rest_max);
     summe.naehe_punkt_dreieck += b.naehe_punkt_dreieck;
     summe.naehe_kante_kante += b.naehe_kante_kante;

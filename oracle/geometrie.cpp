@@ -122,8 +122,15 @@ std::pair<std::vector<size_t>, std::vector<std::pair<size_t, size_t>>> ordnung(c
 }
 
 // ------------------------------------------------------------ bodies
-// koerper.rs:69-91 (Zylinder); art 1 is the sampled signed-distance grid.
+// koerper.rs:69-91 (Zylinder, Netz); art 1 is the sampled signed-distance grid.
 std::optional<Kontakt> Koerper::kontakt(V3 x, double abstand) const {
+  if (art == 2) {
+    auto n = netz->naechster(sub(x, punkt), std::max(netz->suchtiefe, abstand));
+    if (!n) return std::nullopt;
+    const double tiefe = abstand - n->abstand;
+    if (!(tiefe > 0.0)) return std::nullopt;
+    return Kontakt{n->normale, tiefe, geschwindigkeit};
+  }
   if (art == 0) {
     V3 a = mul(achse, 1.0 / norm(achse));
     V3 d = sub(x, punkt);
@@ -171,6 +178,14 @@ std::optional<Kontakt> Koerper::kontakt(V3 x, double abstand) const {
   return Kontakt{mul(g, 1.0 / gl), tiefe, geschwindigkeit};
 }
 // koerper.rs:122-133
+// koerper.rs:99-107 (only the mesh has a skin to pass through)
+std::optional<std::array<V3, 3>> Koerper::durchstoss(V3 von, V3 nach) const {
+  if (art != 2) return std::nullopt;
+  auto r = netz->durchstoss(sub(von, punkt), sub(nach, punkt));
+  if (!r) return std::nullopt;
+  return std::array<V3, 3>{add(r->punkt, punkt), r->normale, geschwindigkeit};
+}
+
 Koerper Koerper::verschoben(double t) const {
   Koerper k = *this;
   k.punkt = add(punkt, mul(geschwindigkeit, t));

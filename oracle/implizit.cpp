@@ -329,8 +329,7 @@ System ImplizitCg::system_bauen(Szene& s, double h, std::vector<std::optional<Fe
   return sys;
 }
 
-// implizit.rs:899-1038 (no self-collision, no body-point passes; durchstoss
-// only applies to mesh bodies, which this restatement does not carry)
+// implizit.rs:899-1038 (no body-point passes)
 void ImplizitCg::schritt(Szene& s, double h, Aufnahme* auf) {
   const size_t n = s.x.size();
   const V3 g = s.param.schwerkraft;
@@ -402,7 +401,28 @@ void ImplizitCg::schritt(Szene& s, double h, Aufnahme* auf) {
       }
     }
     s.v[i] = v;
-    s.x[i] = add(s.x[i], mul(v, h));
+    const V3 alt = s.x[i];
+    s.x[i] = add(alt, mul(v, h));
+    // implizit.rs:988-1002: a path through a mesh body's skin sets down at
+    // the entry; the impact removes the normal velocity relative to the body
+    // and Coulomb on the impact takes up to mu |vn| of the tangential
+    if (param.durchstoss_pruefen)
+      for (const Koerper& kb : s.koerper) {
+        auto d = kb.durchstoss(alt, s.x[i]);
+        if (!d) continue;
+        const V3 p = (*d)[0], nk = (*d)[1], vk = (*d)[2];
+        statistik.durchstoesse += 1;
+        s.x[i] = add(p, mul(nk, s.kollisionsabstand[i]));
+        const V3 rel = sub(s.v[i], vk);
+        const double vn = dot(rel, nk);
+        if (vn < 0.0) {
+          V3 t = sub(rel, mul(nk, vn));
+          const double lt = norm(t);
+          const double grenze = s.reibung[i] * -vn;
+          t = lt <= grenze ? V3{0.0, 0.0, 0.0} : mul(t, 1.0 - grenze / lt);
+          s.v[i] = add(vk, t);
+        }
+      }
     for (size_t kb = 0; kb < s.koerper.size(); ++kb) {
       auto kt = s.koerper[kb].kontakt(s.x[i], s.kollisionsabstand[i]);
       if (kt) {

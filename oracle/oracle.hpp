@@ -93,16 +93,16 @@ std::pair<std::vector<size_t>, std::vector<std::pair<size_t, size_t>>> ordnung(
     const std::vector<uint32_t>& farbe, size_t zahl);
 
 // ---------------------------------------------------------------- bodies
-// sim/src/koerper.rs:16-35 (Zylinder) plus a sampled signed-distance grid,
-// which has no counterpart in the reference (its mesh body answers exact
-// nearest-triangle queries, sim/src/netzkoerper.rs:503-539).
+// sim/src/koerper.rs:16-35 (Zylinder, Netz) plus a sampled signed-distance
+// grid, which has no counterpart in the reference.
+struct Koerpernetz;
 struct Kontakt {
   V3 normale{};
   double tiefe = 0;
   V3 geschwindigkeit{};
 };
 struct Koerper {
-  int art = 0;  // 0 = Zylinder, 1 = SDF grid
+  int art = 0;  // 0 = Zylinder, 1 = SDF grid, 2 = Netz (punkt is its offset)
   V3 punkt{}, achse{0, 0, 1};
   double radius = 0;
   V3 geschwindigkeit{};
@@ -111,7 +111,10 @@ struct Koerper {
   std::array<int32_t, 3> dims{};
   V3 ursprung{};
   double spacing = 1;
+  const Koerpernetz* netz = nullptr;  // art 2; owned by the caller
   std::optional<Kontakt> kontakt(V3 x, double abstand) const;
+  // koerper.rs:99-107: entry point, face normal, body velocity at the entry
+  std::optional<std::array<V3, 3>> durchstoss(V3 von, V3 nach) const;
   Koerper verschoben(double t) const;
 };
 

@@ -385,6 +385,15 @@ class Koerpernetz:
             self.L.orc_netz_free(self.h)
             self.h = None
 
+    @property
+    def c_handle(self):
+        """The oracle mesh pointer, passed as k3d_body.netz to the oracle."""
+        return self.h
+
+    def body(self, versatz=(0.0, 0.0, 0.0), geschwindigkeit=(0.0, 0.0, 0.0), instanz: int = -1) -> dict:
+        return dict(art=_abi.K3D_BODY_MESH, punkt=tuple(float(v) for v in versatz),
+                    geschwindigkeit=tuple(float(v) for v in geschwindigkeit), instanz=int(instanz), netz=self)
+
     def nachfuehren(self, punkte):
         p = f64(punkte).reshape(-1, 3)
         err = C.create_string_buffer(256)

@@ -1,0 +1,122 @@
+"""Mesh bodies in the device step (K3D_BODY_MESH, Koerper::Netz): the contact
+set from the exact nearest query and the segment check at integration
+(implizit.rs:872-883, 988-1013) against the oracle, and the reference's
+point-rain acceptance (sim/tests/koerpernetz.rs:201-243) on a synthetic body."""
+import numpy as np
+import pytest
+
+import oracle_py as O
+from garmentcraft_b200 import _abi, synth
+from garmentcraft_b200.implizit import ImplizitCg, build_scene
+from garmentcraft_b200.netzkoerper import Koerpernetz
+from garmentcraft_b200.params import ImplizitParameter
+from test_oracle_netzkoerper import regen_koerper, regen_soll
+
+pytestmark = pytest.mark.gpu
+
+
+def mit_koerper(s, body):
+    t = s.copy()
+    t.koerper = [body]
+    return t
+
+
+@pytest.mark.parametrize("pruefen", [True, False])
+def test_punkteregen_wie_orakel(pruefen):
+    """Loose points on the mesh body, frame by frame: the same contact and
+    penetration counts as the oracle, positions to 1e-9 m."""
+    p, d = regen_koerper()
+    kg, ko = Koerpernetz(p, d, 0.01), O.Koerpernetz(p, d, 0.01)
+    s0 = synth.punkteregen(p, kante_m=0.02)
+    prm = ImplizitParameter(durchstoss_pruefen=pruefen)
+    s = mit_koerper(s0, kg.body())
+    o = O.OracleSim(mit_koerper(s0, ko.body()), prm.to_c())
+    cg = ImplizitCg(prm)
+    summe = 0
+    for f in range(45):
+        cg.bild(s)
+        st = o.frames(1)
+        a = cg.statistik
+        assert (a.kontakte, a.durchstoesse) == (st.kontakte, st.durchstoesse), f
+        summe += a.durchstoesse
+        xo, _ = o.state()
+        assert np.max(np.abs(s.x - xo)) <= 1e-9, f
+    assert (summe > 0) == pruefen
+
+
+def test_punkteregen_bleibt_draussen_geraet():
+    """sim/tests/koerpernetz.rs:201-243 on the device: with the check no point
+    in the skin after 90 frames and the flat hits at their first ray hit;
+    without it most fall through."""
+    p, d = regen_koerper()
+    kg, ko = Koerpernetz(p, d, 0.01), O.Koerpernetz(p, d, 0.01)
+    s0 = synth.punkteregen(p, kante_m=0.01)
+    soll, flach = regen_soll(ko, s0.x)
+    liegen = []
+    for pruefen in (True, False):
+        s = mit_koerper(s0, kg.body())
+        cg = ImplizitCg(ImplizitParameter(durchstoss_pruefen=pruefen))
+        n = 0
+        for _ in range(90):
+            cg.bild(s)
+            n += cg.statistik.durchstoesse
+        drin = int(np.sum(kg.naechster_alle(s.x)["abstand"] < -0.1e-3))
+        if pruefen:
+            assert drin == 0 and n > 0
+        liegen.append(int(np.sum(flach & (np.linalg.norm(s.x - soll, axis=1) < 0.005))))
+    assert flach.sum() > 60
+    assert liegen[0] >= flach.sum() - 4, (liegen, int(flach.sum()))
+    assert liegen[1] < flach.sum() / 2, liegen
+
+
+def tuch_ueber_koerper(n=33):
+    p, d = regen_koerper()
+    m, _ = synth.sheet_over_sphere(n=n, groesse_m=0.5, jitter_mm=1.0, seed=3)
+    s = build_scene(m)
+    s.x[:, 2] += p[:, 2].max() + 0.01 - s.x[:, 2].mean()
+    return p, d, s
+
+
+def test_tuch_auf_netz_wie_orakel():
+    """A sheet dropped onto the mesh body, FP64: the oracle's contact counts
+    per frame and positions to 1e-9 of the sheet's size."""
+    p, d, s0 = tuch_ueber_koerper()
+    kg, ko = Koerpernetz(p, d, 0.01), O.Koerpernetz(p, d, 0.01)
+    prm = ImplizitParameter(cg_max=100000, cg_toleranz=1e-12)
+    s = mit_koerper(s0, kg.body())
+    o = O.OracleSim(mit_koerper(s0, ko.body()), prm.to_c())
+    cg = ImplizitCg(prm)
+    for f in range(12):
+        cg.bild(s)
+        st = o.frames(1)
+        assert cg.statistik.kontakte == st.kontakte, f
+    xo, _ = o.state()
+    assert cg.statistik.kontakte > 100
+    assert np.max(np.abs(s.x - xo)) <= 1e-9 * 0.5
+
+
+@pytest.mark.parametrize("prec", [_abi.K3D_FP64, _abi.K3D_MIXED])
+def test_tuch_netz_gegen_gitter(prec):
+    """The same drape on the exact mesh and on its voxelised grid (2.5 mm,
+    3 cm band): the two bodies hold the sheet at the same place to within a
+    few grid spacings."""
+    p, d, s0 = tuch_ueber_koerper()
+    kg = Koerpernetz(p, d, 0.01)
+    gitter = kg.sdf_body(0.0025, 0.03)
+    a, b = mit_koerper(s0, kg.body()), mit_koerper(s0, gitter)
+    ca, cb = ImplizitCg(ImplizitParameter(precision=prec)), ImplizitCg(ImplizitParameter(precision=prec))
+    for _ in range(30):
+        ca.bild(a)
+        cb.bild(b)
+    assert ca.statistik.kontakte > 100 and cb.statistik.kontakte > 100
+    assert np.max(np.abs(a.x - b.x)) < 0.01
+    assert np.sum(kg.naechster_alle(a.x)["abstand"] < -1e-3) == 0
+
+
+def test_adjoint_weist_netz_ab():
+    p, d, s0 = tuch_ueber_koerper(n=9)
+    kg = Koerpernetz(p, d, 0.01)
+    cg = ImplizitCg(ImplizitParameter())
+    cg.hochladen(mit_koerper(s0, kg.body()))
+    with pytest.raises(Exception, match="cylinder and grid bodies"):
+        cg.adjoint_vorwaerts(1)

@@ -169,3 +169,45 @@ def test_sdf_definition_am_wuerfel():
     assert np.max(np.abs(g - abstand_wuerfel(x, 1.0))) < 1e-6
     gb = w.sdf(dims, o, s, band=0.4)
     assert np.array_equal(gb, np.clip(g, -0.4, 0.4))
+
+
+def regen_koerper():
+    """A squat body with broad, gently sloped shoulders for the rain."""
+    return synth.koerper_netz(segmente=128, ringe=49, halbachsen=(0.25, 0.18, 0.2), mitte=(0.0, 0.0, 1.0))
+
+
+def regen_soll(k, start):
+    """Expected rest: the first hit of the vertical ray where the surface is
+    flatter than 25 degrees (sim/tests/koerpernetz.rs:205-213)."""
+    tief = start.copy()
+    tief[:, 2] = -0.5
+    r = k.durchstoss(start, tief)
+    flach = (r["dreieck"] >= 0) & (r["normale"][:, 2] >= math.cos(math.radians(25.0)))
+    return r["punkt"], flach
+
+
+def test_punkteregen_bleibt_draussen():
+    """sim/tests/koerpernetz.rs:201-243 on a synthetic body: with the segment
+    check no point ends in the skin and the flat hits rest where their ray
+    first met the body; without it most fall through."""
+    from garmentcraft_b200.params import ImplizitParameter
+    p, d = regen_koerper()
+    k = O.Koerpernetz(p, d, 0.01)
+    s0 = synth.punkteregen(p, kante_m=0.02)
+    s0.koerper = [k.body()]
+    soll, flach = regen_soll(k, s0.x)
+    liegen, stoesse = [], []
+    for pruefen in (True, False):
+        sim = O.OracleSim(s0.copy(), ImplizitParameter(durchstoss_pruefen=pruefen).to_c())
+        n_stoss = sim.frames(90).durchstoesse
+        x, _ = sim.state()
+        drin = int(np.sum(k.naechster(x)["abstand"] < -0.1e-3))
+        da = int(np.sum(flach & (np.linalg.norm(x - soll, axis=1) < 0.005)))
+        if pruefen:
+            assert drin == 0
+        liegen.append(da)
+        stoesse.append(n_stoss)
+    assert flach.sum() > 60
+    assert liegen[0] >= flach.sum() - 4, (liegen, int(flach.sum()))
+    assert liegen[1] < flach.sum() / 2, liegen
+    assert stoesse[0] > 0 and stoesse[1] == 0
