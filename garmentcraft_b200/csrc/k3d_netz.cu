@@ -16,12 +16,12 @@
 // and one of the grid's entry count.
 //
 // Queries run one thread per point (or segment, or grid node). The nearest
-// query walks the cells the search box touches, skips triangles whose bounding
-// sphere is farther than the best so far, and keeps the smallest distance;
-// among equal distances the smallest triangle index, so that the result is
-// naechster_alle's whatever the cell order. Compiled without fused
-// multiply-add: the Ericson regions and distances round as the reference's
-// arithmetic does.
+// query walks the cells the search box touches in the reference's order,
+// skips triangles whose bounding sphere is no nearer than the best so far,
+// and keeps the first of the smallest distances, as the reference does; the
+// query over every triangle keeps the first in triangle order. Compiled
+// without fused multiply-add: the Ericson regions and distances round as the
+// reference's arithmetic does, so the step sees the same contact normals.
 #include <algorithm>
 #include <cmath>
 #include <cstring>

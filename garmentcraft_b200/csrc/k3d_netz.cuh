@@ -149,7 +149,10 @@ __device__ __forceinline__ bool kugel_nah(D3 x, double4 k, double best) {
   return !(b > best + 1e-12 * (fabs(best) + fabs(b)) + 1e-300);
 }
 
-// netzkoerper.rs:503-539 over the grid, ties to the smallest triangle index
+// netzkoerper.rs:503-539: cells in z, y, x order, each cell's triangles in
+// ascending order (the reference's fill order), the sphere test and the
+// strict comparison as there, so that among equal distances the same
+// triangle wins as in the reference
 __device__ inline bool naechster(const Dev& g, D3 x, double radius, Treffer& out) {
   int r0[3], r1[3];
   if (!bereich(g, x - d3(radius, radius, radius), x + d3(radius, radius, radius), r0, r1)) return false;
@@ -165,12 +168,13 @@ __device__ inline bool naechster(const Dev& g, D3 x, double radius, Treffer& out
         const uint32_t e1 = g.anf[z + 1];
         for (uint32_t e = g.anf[z]; e < e1; ++e) {
           const uint32_t t = g.ein[e];
-          if (!kugel_nah(x, g.kg[t], best)) continue;
+          const double4 k = g.kg[t];
+          if (norm(x - d3(k.x, k.y, k.z)) - k.w >= best) continue;
           const uint4 d = g.d[t];
           int reg;
           const D3 q = naechster_auf_dreieck(x, punkt(g, d.x), punkt(g, d.y), punkt(g, d.z), reg);
           const double l = norm(x - q);
-          if (l < best || (hit && l == best && t < bt)) {
+          if (l < best) {
             best = l;
             hit = true;
             bt = t;
@@ -185,7 +189,8 @@ __device__ inline bool naechster(const Dev& g, D3 x, double radius, Treffer& out
 }
 
 // netzkoerper.rs:541-593 for one segment a -> b: the first entry from
-// outside; among equal segment parameters the smallest triangle
+// outside; among equal segment parameters the first in the reference's cell
+// order
 __device__ inline bool durchstoss(const Dev& g, D3 a, D3 b, D3& p, D3& n, uint32_t& tb) {
   const D3 d = b - a;
   if (dot(d, d) < 1e-24) return false;
@@ -216,7 +221,7 @@ __device__ inline bool durchstoss(const Dev& g, D3 a, D3 b, D3& p, D3& n, uint32
           const double v = dot(d, qv) / det;
           if (v < -eps || u + v > 1.0 + eps) continue;
           const double s = dot(e2, qv) / det;
-          if (s >= -eps && s <= 1.0 + eps && (!hit || s < sb || (s == sb && t < tb))) {
+          if (s >= -eps && s <= 1.0 + eps && (!hit || s < sb)) {
             hit = true;
             sb = s;
             tb = t;

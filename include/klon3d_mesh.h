@@ -86,8 +86,9 @@ k3d_status k3d_mesh_tables(k3d_mesh* m, double* flaechennormale, double* punktno
  * radius <= 0: Koerpernetz::naechster_alle (:770-782), over every triangle.
  * abstand is signed (outside positive, the pseudonormal's side, :492-499),
  * normale points outwards (the pseudonormal where the point is on the
- * surface). Among triangles at exactly the same distance the smallest index
- * wins, as in naechster_alle. Any output pointer may be null. */
+ * surface). Among triangles at exactly the same distance the one the
+ * reference keeps wins: the first in its cell order (radius > 0) or the
+ * smallest index (radius <= 0). Any output pointer may be null. */
 k3d_status k3d_mesh_nearest(k3d_mesh* m, const double* x, int64_t n, double radius, double* abstand, double* punkt,
                             double* normale, int32_t* dreieck, int32_t* region);
 
@@ -95,7 +96,7 @@ k3d_status k3d_mesh_nearest(k3d_mesh* m, const double* x, int64_t n, double radi
  * the first entry through the surface from outside (triangles facing the
  * segment's direction are skipped); dreieck -1 where there is none; punkt on
  * the segment, normale the triangle's face normal. Among entries at exactly
- * the same segment parameter the smallest triangle index wins. The body
+ * the same segment parameter the first in the reference's cell order wins. The body
  * velocity at the hit (geschwindigkeit_an, :474-489) is the rigid body's own
  * and is not returned. */
 k3d_status k3d_mesh_penetration(k3d_mesh* m, const double* a, const double* b, int64_t n, int32_t* dreieck,

@@ -71,9 +71,10 @@ def test_gitter_wie_alle_dreiecke():
     alle = g.naechster_alle(x)
     gleich(alle, o.naechster(x))
     r = g.naechster(x, 0.01)
+    gleich(r, o.naechster(x, 0.01))
     hit = r["dreieck"] >= 0
-    for f in ("abstand", "punkt", "dreieck", "region"):
-        assert np.array_equal(r[f][hit], alle[f][hit]), f
+    assert np.max(np.abs(r["abstand"][hit] - alle["abstand"][hit])) < 1e-12
+    assert np.max(np.linalg.norm(r["punkt"][hit] - alle["punkt"][hit], axis=1)) < 1e-12
     assert np.all(np.abs(alle["abstand"][~hit]) >= 0.01)
     assert min(int(np.sum(r["abstand"][hit] < 0)), int(np.sum(r["abstand"][hit] >= 0)), int(np.sum(~hit))) > 1000
 
@@ -84,21 +85,15 @@ def koerper_proben(p, n, seed):
 
 
 def test_koerper_wie_orakel():
-    # The reference's grid query keeps the first of equal distances in its
-    # cell order; the device keeps the smallest triangle, as naechster_alle
-    # does. Distances agree with both, the chosen point with naechster_alle.
+    # both queries keep the reference's choice among equal distances: the
+    # grid query the first in its cell order, the other the smallest index
     p, d = synth.koerper_netz()
     g, o = beide(p, d, 0.01)
     x = koerper_proben(p, 4000, 1)
-    alle = o.naechster(x)
-    gleich(g.naechster_alle(x), alle)
-    rg, ro = g.naechster(x, 0.03), o.naechster(x, 0.03)
-    assert np.array_equal(rg["dreieck"] >= 0, ro["dreieck"] >= 0)
-    hit = rg["dreieck"] >= 0
-    assert hit.sum() > 1000
-    assert np.array_equal(rg["abstand"][hit], ro["abstand"][hit])
-    for f in ("abstand", "punkt", "dreieck", "region"):
-        assert np.array_equal(rg[f][hit], alle[f][hit]), f
+    gleich(g.naechster_alle(x), o.naechster(x))
+    rg = g.naechster(x, 0.03)
+    gleich(rg, o.naechster(x, 0.03))
+    assert (rg["dreieck"] >= 0).sum() > 1000
 
 
 def test_durchstoss_wie_referenz_und_orakel():
@@ -121,7 +116,7 @@ def test_durchstoss_wie_referenz_und_orakel():
     a = koerper_proben(p, 3000, 3)
     b = a + rng.normal(0.0, 0.03, a.shape)
     rg, ro = g.durchstoss(a, b), o.durchstoss(a, b)
-    assert np.array_equal(rg["dreieck"] >= 0, ro["dreieck"] >= 0)
+    assert np.array_equal(rg["dreieck"], ro["dreieck"])
     hit = rg["dreieck"] >= 0
     assert hit.sum() > 100
     assert np.array_equal(rg["punkt"][hit], ro["punkt"][hit])
