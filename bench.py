@@ -26,7 +26,9 @@ the device and back every step.
 ``adjoint`` is the backward/forward time of the step's adjoint on the
 material-fit workload (see adjoint_leg), with its gradient check.
 ``garment`` is the same step on the ~205k-point sewn garment with the
-self-collision proximity stage on and off (see garment_leg).
+self-collision proximity stage on and off (see garment_leg). ``mesh`` is the
+body mesh as a collider: voxelisation, nearest queries, segment tests and the
+sheet step on an exact mesh body (see mesh_leg).
 
 Multi-GPU: the step of one drape does not shard (a global Krylov solve), so
 ``--gpus N`` runs N independent replicas, one per rank, with no collective on
@@ -82,6 +84,7 @@ def args_():
     p.add_argument("--no-batch", action="store_true", help="skip the batched-drape comparison")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (material-fit) leg")
     p.add_argument("--no-garment", action="store_true", help="skip the sewn-garment leg")
+    p.add_argument("--no-mesh", action="store_true", help="skip the body-mesh leg")
     p.add_argument("--batch-steps", type=int, default=5)
     return p.parse_args()
 
@@ -201,6 +204,94 @@ def garment_leg(flush, torch):
                         "cg_iterations_per_step": its / GARMENT_STEPS, "proximity_pairs_per_step": pairs / GARMENT_STEPS}
     for tag in ("selfcollision", "no_selfcollision"):
         out[f"{tag}_mixed_vs_fp64"] = out[f"{tag}_mixed"]["value"] / out[f"{tag}_fp64"]["value"]
+    return out
+
+
+MESH_REPS = 5
+
+
+def mesh_leg(flush, torch):
+    """The body mesh as a collider (include/klon3d_mesh.h) on a synthetic
+    body of 36,864 triangles / 18,434 points (synth.koerper_netz, the size of
+    a human base mesh split into triangles): voxelisation into the SDF grid at
+    5 mm with a 3 cm and a 6 cm band, 200k nearest queries within the 1 cm
+    search depth, 200k segment tests, nachfuehren; then the 257x257 sheet
+    step on the mesh body against the same step on the 128^3 sphere grid.
+    Device times are the library's CUDA events around its kernels, L2
+    flushed before each; e2e is the C-ABI call with host arrays (copies
+    included), wall clock."""
+    import numpy as np
+    from garmentcraft_b200 import synth
+    from garmentcraft_b200.implizit import ImplizitCg
+    from garmentcraft_b200.netzkoerper import Koerpernetz
+    from garmentcraft_b200._abi import K3D_MIXED
+    dev = torch.cuda.current_device()
+    p, d = synth.koerper_netz()
+    k = Koerpernetz(p, d, 0.01, device=dev)
+    out = {"workload": f"synthetic body mesh, {d.shape[0]} triangles, {p.shape[0]} points, search depth 1 cm",
+           "create_ms_device": k.letzte_ms}
+
+    def timed(call):
+        dms, wms = [], []
+        call()
+        for r in range(MESH_REPS):
+            flush.fill_(float(r))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            call()
+            wms.append(1e3 * (time.perf_counter() - t0))
+            dms.append(k.letzte_ms)
+        return statistics.median(dms), statistics.median(wms)
+
+    for band in (0.03, 0.06):
+        body = {}
+
+        def vox():
+            body["b"] = k.sdf_body(0.005, band)
+        dm, wm = timed(vox)
+        nn = int(np.prod(body["b"]["dims"]))
+        out[f"sdf_band_{int(round(band * 100))}cm"] = {
+            "dims": list(body["b"]["dims"]), "nodes": nn, "ms_device": dm, "value": nn / (dm * 1e-3),
+            "unit": "nodes/s", "e2e": {"value": nn / (wm * 1e-3), "unit": "nodes/s", "ms": wm,
+                                       "d2h_bytes": 4 * nn}, "unresolved_nodes": int(k.info().ungeklaert)}
+    rng = np.random.default_rng(0)
+    q = 200_000
+    x = p[rng.integers(0, p.shape[0], q)] + rng.normal(0.0, 0.01, (q, 3))
+    y = x + rng.normal(0.0, 0.01, (q, 3))
+    dm, wm = timed(lambda: k.naechster(x, 0.01))
+    out["nearest"] = {"queries": q, "radius_m": 0.01, "ms_device": dm, "value": q / (dm * 1e-3), "unit": "queries/s",
+                      "e2e": {"value": q / (wm * 1e-3), "unit": "queries/s", "ms": wm}}
+    dm, wm = timed(lambda: k.durchstoss(x, y))
+    out["penetration"] = {"segments": q, "ms_device": dm, "value": q / (dm * 1e-3), "unit": "segments/s",
+                          "e2e": {"value": q / (wm * 1e-3), "unit": "segments/s", "ms": wm}}
+    flip = [p * 1.001, p]
+    state = {"i": 0}
+
+    def move():
+        state["i"] ^= 1
+        k.nachfuehren(flip[state["i"]])
+    dm, wm = timed(move)
+    out["nachfuehren"] = {"ms_device": dm, "ms_e2e": wm}
+    # the sheet step on the mesh body against the sphere grid
+    kugel_p, kugel_d = synth.koerper_netz(halbachsen=(0.3, 0.3, 0.3), mitte=(0.0, 0.0, 0.0))
+    kugel = Koerpernetz(kugel_p, kugel_d, 0.01, device=dev)
+    gitter = kugel.sdf_body(0.005, 0.03)
+    for name, body in (("step_mesh_body", kugel.body()), ("step_grid_body", gitter)):
+        s = make_scene(257)
+        s.koerper = [body]
+        cg = ImplizitCg(params(K3D_MIXED), device=dev)
+        cg.zustand_hochladen(s)
+        cg.bilder_auf_geraet(FREE_FALL + 6)
+        ms, its = [], 0
+        for r in range(MESH_REPS):
+            flush.fill_(float(r))
+            torch.cuda.synchronize()
+            its += cg.bilder_auf_geraet(1).cg_iterationen
+            ms.append(cg.letzte_bild_ms())
+        out[name] = {"ms_per_step": statistics.median(ms), "value": s.n / (statistics.median(ms) * 1e-3),
+                     "unit": UNIT, "cg_iterations_per_step": its / MESH_REPS}
+    out["step_mesh_body"]["body"] = f"bumpy sphere mesh r 0.3 m, {kugel_d.shape[0]} triangles, exact query"
+    out["step_grid_body"]["body"] = f"the same mesh voxelised, {'x'.join(map(str, gitter['dims']))} at 5 mm, trilinear"
     return out
 
 
@@ -392,10 +483,34 @@ def cpu_leg(n, warmup, seconds):
         el = time.perf_counter() - t0
         if el >= seconds:
             break
-    return {"value": s.n * steps / el, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"the first {steps} steps of the timed window (from step {sum(window(warmup))}) of the same "
-                      f"{n}x{n} drop, {el:.1f} s, FP64 C++ restatement of CpuLoeser/ImplizitCg, one thread",
-            "cg_iterations_per_step": its / steps}
+    out = {"value": s.n * steps / el, "unit": UNIT, "cores": 1, "kind": "port",
+           "sample": f"the first {steps} steps of the timed window (from step {sum(window(warmup))}) of the same "
+                     f"{n}x{n} drop, {el:.1f} s, FP64 C++ restatement of CpuLoeser/ImplizitCg, one thread",
+           "cg_iterations_per_step": its / steps}
+    out["mesh"] = cpu_mesh_leg(oracle_py)
+    return out
+
+
+def cpu_mesh_leg(oracle_py):
+    """The restated Koerpernetz queries (grid query within the search depth,
+    segment test; one thread) on 20k of the mesh leg's 200k points."""
+    import numpy as np
+    from garmentcraft_b200 import synth
+    p, d = synth.koerper_netz()
+    k = oracle_py.Koerpernetz(p, d, 0.01)
+    rng = np.random.default_rng(0)
+    q = 200_000
+    x = p[rng.integers(0, p.shape[0], q)] + rng.normal(0.0, 0.01, (q, 3))
+    y = x + rng.normal(0.0, 0.01, (q, 3))
+    m = 20_000
+    t0 = time.perf_counter()
+    k.naechster(x[:m], 0.01)
+    t1 = time.perf_counter()
+    k.durchstoss(x[:m], y[:m])
+    t2 = time.perf_counter()
+    return {"nearest": {"value": m / (t1 - t0), "unit": "queries/s"},
+            "penetration": {"value": m / (t2 - t1), "unit": "segments/s"}, "cores": 1, "kind": "port",
+            "sample": f"the first {m} of the mesh leg's 200k points, the same body mesh"}
 
 
 def dev_timed(n, prec, warmup, steps, flush, torch):
@@ -443,6 +558,7 @@ def e2e_timed(n, prec, warmup, steps, flush, torch):
 
 
 def main():
+    import numpy as np
     a = args_()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -454,7 +570,6 @@ def main():
         from garmentcraft_b200.implizit import ImplizitCg
         prec = _abi.K3D_MIXED if a.precision == "mixed" else _abi.K3D_FP64
         if a.workload == "adjoint":
-            import numpy as np
             from garmentcraft_b200 import synth
             from garmentcraft_b200.adjoint import Drapierung, Stoff
             from garmentcraft_b200.params import ImplizitParameter
@@ -587,6 +702,8 @@ def main():
         line["adjoint"] = adjoint_leg(torch)
     if world == 1 and not a.no_garment:
         line["garment"] = garment_leg(flush, torch)
+    if world == 1 and not a.no_mesh:
+        line["mesh"] = mesh_leg(flush, torch)
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_leg(a.n, a.warmup, a.cpu_seconds)
     if rank == 0:

@@ -163,10 +163,15 @@ __global__ void __launch_bounds__(kT) zellen_fuellen_kernel(const __grid_constan
         }
   }
 }
-// entries of a cell in ascending triangle order (insertion sort; cells are short)
+// Entries of a cell in ascending triangle order, the reference's fill order.
+// Short cells (up to kKurz entries) are sorted by one thread each; longer ones
+// (the cells round a pole of a latitude-longitude mesh hold hundreds) by a
+// block in shared memory (bitonic), the longest by a Shell sort of one thread.
+constexpr uint32_t kKurz = 32, kLang = 4096;
 __global__ void __launch_bounds__(kT) zellen_sortieren_kernel(const __grid_constant__ Dev g, int64_t nz) {
   for (int64_t z = int64_t(blockIdx.x) * kT + threadIdx.x; z < nz; z += int64_t(gridDim.x) * kT) {
     const uint32_t lo = g.anf[z], hi = g.anf[z + 1];
+    if (hi - lo > kKurz) continue;
     for (uint32_t i = lo + 1; i < hi; ++i) {
       const uint32_t v = g.ein[i];
       uint32_t j = i;
@@ -176,6 +181,50 @@ __global__ void __launch_bounds__(kT) zellen_sortieren_kernel(const __grid_const
       }
       g.ein[j] = v;
     }
+  }
+}
+__global__ void __launch_bounds__(kT) zellen_lang_kernel(const __grid_constant__ Dev g, int64_t nz) {
+  __shared__ uint32_t sh[kLang];
+  for (int64_t z = blockIdx.x; z < nz; z += gridDim.x) {
+    const uint32_t lo = g.anf[z], hi = g.anf[z + 1], n = hi - lo;
+    if (n <= kKurz) continue;
+    if (n > kLang) {  // Shell sort with Ciura's gaps, one thread
+      if (threadIdx.x == 0) {
+        const uint32_t gaps[8] = {701u, 301u, 132u, 57u, 23u, 10u, 4u, 1u};
+        for (int k = 0; k < 8; ++k) {
+          const uint32_t gap = gaps[k];
+          for (uint32_t i = lo + gap; i < hi; ++i) {
+            const uint32_t key = g.ein[i];
+            uint32_t j = i;
+            while (j >= lo + gap && g.ein[j - gap] > key) {
+              g.ein[j] = g.ein[j - gap];
+              j -= gap;
+            }
+            g.ein[j] = key;
+          }
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+    uint32_t m = 1;
+    while (m < n) m <<= 1;
+    for (uint32_t i = threadIdx.x; i < m; i += kT) sh[i] = i < n ? g.ein[lo + i] : 0xffffffffu;
+    __syncthreads();
+    for (uint32_t k = 2; k <= m; k <<= 1)
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        for (uint32_t i = threadIdx.x; i < m; i += kT) {
+          const uint32_t p = i ^ j;
+          if (p > i) {
+            const bool auf = (i & k) == 0;
+            const uint32_t a = sh[i], b = sh[p];
+            if ((a > b) == auf) sh[i] = b, sh[p] = a;
+          }
+        }
+        __syncthreads();
+      }
+    for (uint32_t i = threadIdx.x; i < n; i += kT) g.ein[lo + i] = sh[i];
+    __syncthreads();
   }
 }
 
@@ -303,14 +352,163 @@ __global__ void __launch_bounds__(kT) durchstoss_kernel(const __grid_constant__ 
 }
 
 // ---------------------------------------------------------------- voxelisation
-// nodes within the band: the exact signed distance; the rest NaN (open)
-__global__ void __launch_bounds__(kT) sdf_band_kernel(const __grid_constant__ Dev g, const __grid_constant__ Knoten kn) {
-  const int64_t n = int64_t(kn.nx) * kn.ny * kn.nz;
-  for (int64_t q = int64_t(blockIdx.x) * kT + threadIdx.x; q < n; q += int64_t(gridDim.x) * kT) {
-    Treffer r;
-    kn.sdf[q] = naechster(g, knoten_lage(kn, q), kn.band, r) ? float(r.abstand) : __int_as_float(0x7fc00000);
+// The nearest query for the voxeliser: the same result distance as
+// naechster (the value does not depend on the visiting order), found faster:
+// cells in shells of growing Chebyshev distance around x's cell, a cell
+// skipped when its box is no nearer than the best so far, the search ended
+// when a whole shell is farther. Ties go to the smallest triangle index.
+__device__ bool naechster_schalen(const Dev& g, D3 x, double radius, Treffer& out) {
+  int r0[3], r1[3];
+  if (!bereich(g, x - d3(radius, radius, radius), x + d3(radius, radius, radius), r0, r1)) return false;
+  int64_t k0[3];
+  zell_index(g, x, k0);
+  int64_t smax = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int64_t lo = k0[a] - r0[a], hi = r1[a] - k0[a];
+    smax = lo > smax ? lo : smax;
+    smax = hi > smax ? hi : smax;
+  }
+  const double xs[3] = {x.x, x.y, x.z}, us[3] = {g.u0, g.u1, g.u2};
+  double best = radius;
+  bool hit = false;
+  uint32_t bt = 0xffffffffu;
+  D3 bq = d3(0, 0, 0);
+  int br = 6;
+  for (int64_t s = 0; s <= smax; ++s) {
+    if (s >= 1 && double(s - 1) * g.zelle >= best) break;
+    for (int64_t dz = -s; dz <= s; ++dz) {
+      const int64_t kz = k0[2] + dz;
+      if (kz < r0[2] || kz > r1[2]) continue;
+      for (int64_t dy = -s; dy <= s; ++dy) {
+        const int64_t ky = k0[1] + dy;
+        if (ky < r0[1] || ky > r1[1]) continue;
+        const bool rand = (dz == -s || dz == s || dy == -s || dy == s);
+        const int64_t step = rand ? 1 : (s > 0 ? 2 * s : 1);
+        for (int64_t dx = -s; dx <= s; dx += step) {
+          const int64_t kx = k0[0] + dx;
+          if (kx < r0[0] || kx > r1[0]) continue;
+          const int64_t kk[3] = {kx, ky, kz};
+          double q2 = 0.0;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const double lo = us[a] + g.zelle * double(kk[a]), hi = lo + g.zelle;
+            const double e = xs[a] < lo ? lo - xs[a] : (xs[a] > hi ? xs[a] - hi : 0.0);
+            q2 += e * e;
+          }
+          if (q2 > best * best * (1.0 + 1e-9)) continue;
+          const int64_t z = (kz * g.zy + ky) * g.zx + kx;
+          const uint32_t e1 = g.anf[z + 1];
+          for (uint32_t e = g.anf[z]; e < e1; ++e) {
+            const uint32_t t = g.ein[e];
+            if (!kugel_nah(x, g.kg[t], best)) continue;
+            const uint4 d = g.d[t];
+            int reg;
+            const D3 q = naechster_auf_dreieck(x, punkt(g, d.x), punkt(g, d.y), punkt(g, d.z), reg);
+            const double l = norm(x - q);
+            if (l < best || (hit && l == best && t < bt)) {
+              best = l;
+              hit = true;
+              bt = t;
+              bq = q;
+              br = reg;
+            }
+          }
+        }
+      }
+    }
+  }
+  if (!hit) return false;
+  out = ergebnis(g, x, bt, bq, br);
+  return true;
+}
+
+// Bricks of 8 x 4 x 4 nodes, one block each. The block first gathers into
+// shared memory every triangle that may lie within the band of one of its
+// nodes: the triangles of the grid cells the brick's box grown by the band
+// touches, each taken once (from the first of its cells in that range), kept
+// when its bounding sphere comes within the band of the brick's box. Every
+// node then tests only those, with the same values as the nearest query
+// within the band (the set holds every triangle nearer than the band; ties go
+// to the smallest index). A brick whose list overflows queries cell by cell.
+constexpr int kZx = 8, kZy = 4, kZz = 4, kZiegel = kZx * kZy * kZz, kKand = 2048;
+__global__ void __launch_bounds__(kZiegel) sdf_ziegel_kernel(const __grid_constant__ Dev g,
+                                                             const __grid_constant__ Knoten kn) {
+  __shared__ uint32_t kand[kKand];
+  __shared__ uint32_t zahl;
+  const int64_t bx = (kn.nx + kZx - 1) / kZx, by = (kn.ny + kZy - 1) / kZy, bz = (kn.nz + kZz - 1) / kZz;
+  const float offen = __int_as_float(0x7fc00000);
+  const double band = kn.band;
+  for (int64_t zg = blockIdx.x; zg < bx * by * bz; zg += gridDim.x) {
+    const int64_t i0 = (zg % bx) * kZx, j0 = ((zg / bx) % by) * kZy, k0 = (zg / (bx * by)) * kZz;
+    const int64_t i1 = min(i0 + kZx, int64_t(kn.nx)), j1 = min(j0 + kZy, int64_t(kn.ny)),
+                  k1 = min(k0 + kZz, int64_t(kn.nz));
+    const D3 lo = d3(kn.o0 + kn.s * double(i0), kn.o1 + kn.s * double(j0), kn.o2 + kn.s * double(k0));
+    const D3 hi = d3(kn.o0 + kn.s * double(i1 - 1), kn.o1 + kn.s * double(j1 - 1), kn.o2 + kn.s * double(k1 - 1));
+    if (threadIdx.x == 0) zahl = 0;
+    __syncthreads();
+    int r0[3], r1[3];
+    const bool beruehrt = bereich(g, lo - d3(band, band, band), hi + d3(band, band, band), r0, r1);
+    if (beruehrt) {
+      const int64_t cx = r1[0] - r0[0] + 1, cy = r1[1] - r0[1] + 1, cz = r1[2] - r0[2] + 1;
+      for (int64_t c = threadIdx.x; c < cx * cy * cz; c += kZiegel) {
+        const int kx = r0[0] + int(c % cx), ky = r0[1] + int((c / cx) % cy), kz = r0[2] + int(c / (cx * cy));
+        const int64_t z = (int64_t(kz) * g.zy + ky) * g.zx + kx;
+        for (uint32_t e = g.anf[z]; e < g.anf[z + 1]; ++e) {
+          const uint32_t t = g.ein[e];
+          int t0[3], t1[3];
+          dreieck_zellen(g, t, t0, t1);
+          if (kx != max(t0[0], r0[0]) || ky != max(t0[1], r0[1]) || kz != max(t0[2], r0[2])) continue;
+          const double4 k = g.kg[t];
+          const double ex = fmax(fmax(lo.x - k.x, k.x - hi.x), 0.0), ey = fmax(fmax(lo.y - k.y, k.y - hi.y), 0.0),
+                       ez = fmax(fmax(lo.z - k.z, k.z - hi.z), 0.0);
+          const double dq = sqrt(ex * ex + ey * ey + ez * ez) - k.w;
+          if (dq > band * (1.0 + 1e-9) + 1e-12) continue;
+          const uint32_t pos = atomicAdd(&zahl, 1u);
+          if (pos < kKand) kand[pos] = t;
+        }
+      }
+    }
+    __syncthreads();
+    const uint32_t m = zahl;
+    const int li = threadIdx.x % kZx, lj = (threadIdx.x / kZx) % kZy, lk = threadIdx.x / (kZx * kZy);
+    const int64_t i = i0 + li, j = j0 + lj, kk = k0 + lk;
+    if (i < i1 && j < j1 && kk < k1) {
+      const int64_t q = (kk * kn.ny + j) * kn.nx + i;
+      const D3 x = d3(kn.o0 + kn.s * double(i), kn.o1 + kn.s * double(j), kn.o2 + kn.s * double(kk));
+      float v = offen;
+      if (m > kKand) {
+        Treffer t;
+        if (naechster_schalen(g, x, band, t)) v = float(t.abstand);
+      } else if (m > 0) {
+        double best = band;
+        bool hit = false;
+        uint32_t bt = 0xffffffffu;
+        D3 bq = d3(0, 0, 0);
+        int br = 6;
+        for (uint32_t c = 0; c < m; ++c) {
+          const uint32_t t = kand[c];
+          if (!kugel_nah(x, g.kg[t], best)) continue;
+          const uint4 dd = g.d[t];
+          int reg;
+          const D3 qq = naechster_auf_dreieck(x, punkt(g, dd.x), punkt(g, dd.y), punkt(g, dd.z), reg);
+          const double l = norm(x - qq);
+          if (l < best || (hit && l == best && t < bt)) {
+            best = l;
+            hit = true;
+            bt = t;
+            bq = qq;
+            br = reg;
+          }
+        }
+        if (hit) v = float(ergebnis(g, x, bt, bq, br).abstand);
+      }
+      kn.sdf[q] = v;
+    }
+    __syncthreads();
   }
 }
+
 // One thread per grid line along axis `achse`: an open run next to a set
 // node takes that node's sign (band > spacing: no surface lies between two
 // neighbouring nodes when one of them is at least band from it). Counts the
@@ -482,9 +680,10 @@ k3d_status gitter(k3d_mesh* m, const double h[6]) {
   NCK(cudaMemcpyAsync(m->cur, m->anf, size_t(nz) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st), "grid fill");
   zellen_fuellen_kernel<<<blocks_for(g.nd), kT, 0, st>>>(g);
   zellen_sortieren_kernel<<<blocks_for(nz), kT, 0, st>>>(g, nz);
+  zellen_lang_kernel<<<unsigned(std::min<int64_t>(nz, 148 * 4)), kT, 0, st>>>(g, nz);
   NCK(cudaGetLastError(), "grid fill");
   NCK(cudaMemcpyAsync(m->g_dev, &m->g, sizeof(Dev), cudaMemcpyHostToDevice, st), "grid view");
-  m->kernels += 1 + 3 + 2;
+  m->kernels += 1 + 3 + 3;
   return K3D_OK;
 }
 
@@ -824,7 +1023,8 @@ k3d_status k3d_mesh_sdf(k3d_mesh* m, const int32_t dims[3], const double ursprun
   Uhr uhr(m);
   m->ungeklaert = 0;
   if (band > 0.0) {
-    sdf_band_kernel<<<blocks_for(nn), kT, 0, st>>>(m->g, kn);
+    const int64_t ziegel = ((dims[0] + kZx - 1) / kZx) * int64_t((dims[1] + kZy - 1) / kZy) * ((dims[2] + kZz - 1) / kZz);
+    sdf_ziegel_kernel<<<unsigned(std::min<int64_t>(ziegel, 148 * 64)), kZiegel, 0, st>>>(m->g, kn);
     NCK(cudaGetLastError(), "sdf band");
     for (int achse = 0; achse < 3; ++achse) {
       NCK(cudaMemsetAsync(m->offen, 0, sizeof(unsigned long long), st), "sdf lines");

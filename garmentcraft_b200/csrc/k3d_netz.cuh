@@ -145,8 +145,9 @@ __device__ __forceinline__ Treffer ergebnis(const Dev& g, D3 x, uint32_t t, D3 c
 // A conservative sphere test: the triangle may hold a point no farther than
 // `best` (the slack keeps ties and rounding on the safe side).
 __device__ __forceinline__ bool kugel_nah(D3 x, double4 k, double best) {
-  const double b = norm(x - d3(k.x, k.y, k.z)) - k.w;
-  return !(b > best + 1e-12 * (fabs(best) + fabs(b)) + 1e-300);
+  const D3 d = x - d3(k.x, k.y, k.z);
+  const double b = best + k.w;  // |x - m| <= best + r, squared (no square root)
+  return dot(d, d) <= b * b * (1.0 + 1e-9) + 1e-300;
 }
 
 // netzkoerper.rs:503-539: cells in z, y, x order, each cell's triangles in
