@@ -78,9 +78,10 @@ def args_():
     p.add_argument("--capture", type=int, default=0,
                    help="profiling case: run this many mixed-form steps of the drop on cuda:0 and exit")
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="form used by --capture")
-    p.add_argument("--workload", default="sheet", choices=["sheet", "garment", "adjoint"],
-                   help="case of --capture: the sheet drop, the garment with self-collision (frames), or the "
-                        "material-fit drop's adjoint (frames forward, then the backward)")
+    p.add_argument("--workload", default="sheet", choices=["sheet", "garment", "adjoint", "mesh"],
+                   help="case of --capture: the sheet drop, the garment with self-collision (frames), the "
+                        "material-fit drop's adjoint (frames forward, then the backward), or the body mesh "
+                        "(rounds of voxelisation at a 3 and a 6 cm band)")
     p.add_argument("--no-batch", action="store_true", help="skip the batched-drape comparison")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (material-fit) leg")
     p.add_argument("--no-garment", action="store_true", help="skip the sewn-garment leg")
@@ -580,6 +581,18 @@ def main():
             g = d.rueckwaerts(2.0 * x)["roh"]
             print(json.dumps({"capture_frames": a.capture, "forward_ms": g["ms_vorwaerts"],
                               "backward_ms": g["ms_rueckwaerts"], "adjoint_cg_iterations": g["iterationen"]}))
+            return
+        if a.workload == "mesh":
+            from garmentcraft_b200 import synth
+            from garmentcraft_b200.netzkoerper import Koerpernetz
+            p, d = synth.koerper_netz()
+            k = Koerpernetz(p, d, 0.01)
+            ms = {"create": k.letzte_ms}
+            for r in range(a.capture):
+                for band in (0.03, 0.06):
+                    k.sdf_body(0.005, band)
+                    ms[f"sdf_{band}"] = k.letzte_ms
+            print(json.dumps({"capture_rounds": a.capture, "ms_device": ms}))
             return
         if a.workload == "garment":
             from garmentcraft_b200 import synth
