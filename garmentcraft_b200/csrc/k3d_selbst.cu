@@ -504,21 +504,38 @@ __device__ uint32_t kante_kante(const SelbstArgs& s, int64_t e, uint32_t pos) {
   return cnt;
 }
 
-// count pass: pair count per triangle and per edge (off_t[t], off_e[e])
+// count pass: pair count per triangle and per edge (off_t[t], off_e[e]);
+// the triangles and edges that have pairs go to a list for the fill pass
 __global__ void __launch_bounds__(kT) pairs_count_kernel(const __grid_constant__ SelbstArgs s) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {  // the scans run over n + 1 values
     s.off_t[s.nd] = 0u;
     s.off_e[s.ne] = 0u;
   }
-  SC_FOR(t, s.nd) s.off_t[t] = punkt_dreieck<false>(s, t, 0);
-  SC_FOR(e, s.ne) s.off_e[e] = kante_kante<false>(s, e, 0);
+  SC_FOR(t, s.nd) {
+    const uint32_t c = punkt_dreieck<false>(s, t, 0);
+    s.off_t[t] = c;
+    if (c) s.aktiv_p[atomicAdd(&s.zahl[SZ_AKTIV_P], 1u)] = uint32_t(t);
+  }
+  SC_FOR(e, s.ne) {
+    const uint32_t c = kante_kante<false>(s, e, 0);
+    s.off_e[e] = c;
+    if (c) s.aktiv_p[atomicAdd(&s.zahl[SZ_AKTIV_P], 1u)] = uint32_t(s.nd + e);
+  }
 }
 
-// fill pass: point-triangle pairs first (triangle order), then edge-edge
-__global__ void __launch_bounds__(kT) pairs_fill_kernel(const __grid_constant__ SelbstArgs s) {
+// fill pass over the listed triangles and edges only: each writes its pairs
+// from its scanned start, so the buffer holds the point-triangle pairs in
+// triangle order, then the edge-edge pairs in edge order, whatever the list's
+// order
+__global__ void __launch_bounds__(kT) pairs_fill_kernel(const __grid_constant__ SelbstArgs s, uint32_t n_aktiv) {
   const uint32_t npt = s.zahl[SZ_PAARE_PT];
-  SC_FOR(t, s.nd) punkt_dreieck<true>(s, t, s.off_t[t]);
-  SC_FOR(e, s.ne) kante_kante<true>(s, e, npt + s.off_e[e]);
+  SC_FOR(q, n_aktiv) {
+    const uint32_t c = s.aktiv_p[q];
+    if (int64_t(c) < s.nd)
+      punkt_dreieck<true>(s, c, s.off_t[c]);
+    else
+      kante_kante<true>(s, int64_t(c) - s.nd, npt + s.off_e[c - s.nd]);
+  }
 }
 
 __device__ __forceinline__ uint32_t paare(const SelbstArgs& s) {
@@ -1044,11 +1061,19 @@ __device__ uint32_t kante_schnitte(const SelbstArgs& s, int64_t e, uint32_t pos,
 __global__ void __launch_bounds__(kT) schnitt_count_kernel(const __grid_constant__ SelbstArgs s) {
   const double z = zelle_aus(&s.lmax[0]);
   if (blockIdx.x == 0 && threadIdx.x == 0) s.off_s[s.ne] = 0u;
-  SC_FOR(e, s.ne) s.off_s[e] = kante_schnitte<false>(s, e, 0, z);
+  SC_FOR(e, s.ne) {
+    const uint32_t c = kante_schnitte<false>(s, e, 0, z);
+    s.off_s[e] = c;
+    if (c) s.aktiv_s[atomicAdd(&s.zahl[SZ_AKTIV_S], 1u)] = uint32_t(e);
+  }
 }
-__global__ void __launch_bounds__(kT) schnitt_fill_kernel(const __grid_constant__ SelbstArgs s) {
+// fill pass over the listed edges (their starts come from the scan)
+__global__ void __launch_bounds__(kT) schnitt_fill_kernel(const __grid_constant__ SelbstArgs s, uint32_t n_aktiv) {
   const double z = zelle_aus(&s.lmax[0]);
-  SC_FOR(e, s.ne) kante_schnitte<true>(s, e, s.off_s[e], z);
+  SC_FOR(q, n_aktiv) {
+    const uint32_t e = s.aktiv_s[q];
+    kante_schnitte<true>(s, e, s.off_s[e], z);
+  }
 }
 
 // finde(e, t): the intersection of edge e with triangle t (the list is edge by edge)
@@ -1679,9 +1704,9 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
 
 // Part 3: pairs, springs, damping, incidence lists. The host has checked the
 // pair capacity and zeroed inc_off (n + 1) and inc_cur (n).
-cudaError_t selbst_paare_und_federn(const SelbstArgs& s, cudaStream_t st) {
+cudaError_t selbst_paare_und_federn(const SelbstArgs& s, uint32_t n_aktiv_p, uint32_t n_aktiv_s, cudaStream_t st) {
   cudaError_t e;
-  pairs_fill_kernel<<<grid_for(s.nd > s.ne ? s.nd : s.ne), kT, 0, st>>>(s);
+  pairs_fill_kernel<<<grid_for(n_aktiv_p), kT, 0, st>>>(s, n_aktiv_p);
   const int64_t pmax = int64_t(s.cap_pairs);
   if (s.rsize == 4)
     federn_kernel<float><<<grid_for(pmax), kT, 0, st>>>(s);
@@ -1698,7 +1723,7 @@ cudaError_t selbst_paare_und_federn(const SelbstArgs& s, cudaStream_t st) {
   // penetration regions and their push springs (selbstkollision.rs:858-1058);
   // the host has zeroed hat, klemm, t_off and t_cur
   const int64_t ns = int64_t(s.cap_s);
-  schnitt_fill_kernel<<<grid_for(s.ne), kT, 0, st>>>(s);
+  schnitt_fill_kernel<<<grid_for(n_aktiv_s), kT, 0, st>>>(s, n_aktiv_s);
   gebiete_kernel<<<1, 32, 0, st>>>(s);
   klemm_kernel<<<grid_for(ns), kT, 0, st>>>(s);
   folge_kernel<<<grid_for(s.nd), kT, 0, st>>>(s);

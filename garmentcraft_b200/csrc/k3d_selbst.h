@@ -30,7 +30,9 @@ enum SelbstZahl : int {
   SZ_ANTWORT = 12,  // impact corrections applied (ImplizitStatistik::selbst_stoesse)
   SZ_BEWEGT = 13,   // points moved by the last response pass
   SZ_HALT = 14,     // set when a response pass moved no point (the passes stop)
-  SZ_COUNT = 16
+  SZ_AKTIV_P = 15,  // triangles and edges with proximity pairs (the fill pass's list)
+  SZ_AKTIV_S = 16,  // edges through a triangle (the intersection fill pass's list)
+  SZ_COUNT = 18
 };
 
 // A spatial hash over boxes (Hashgitter, selbstkollision.rs:281-345): the
@@ -75,6 +77,7 @@ struct SelbstArgs {
   uint32_t *anf_k, *ein_k, *cur_k;         // edge hash
   uint32_t cap_ep, cap_ek;
   uint32_t *off_t, *off_e;  // pair counts -> starts per triangle / edge (n + 1)
+  uint32_t* aktiv_p;        // triangles (t) and edges (nd + e) with pairs, in no order (nd + ne)
   uint32_t cap_pairs;
   uint4* pr_idx;           // 4 points
   uint2* pr_src;           // triangle (point-triangle) or the two edges (edge-edge)
@@ -104,6 +107,7 @@ struct SelbstArgs {
   unsigned long long* lmax;       // 2: the longest edge (as bits) at x and at the impact stage's x1
   HashG hs;                       // triangle boxes
   uint32_t* off_s;                // per edge: its intersections' count, then start (ne + 1)
+  uint32_t* aktiv_s;              // edges with intersections, in no order (ne)
   uint32_t cap_s;
   uint2* sn_ke;                   // per intersection: edge, triangle
   double* sn_t;                   // position on the edge
@@ -141,7 +145,8 @@ struct SelbstArgs {
 // (the host sizes the hash and pair buffers from the counts).
 cudaError_t selbst_hash_zaehlen(const SelbstArgs& s, cudaStream_t st);
 cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStream_t st);
-cudaError_t selbst_paare_und_federn(const SelbstArgs& s, cudaStream_t st);
+// n_aktiv_p, n_aktiv_s: the fill lists' lengths (counters SZ_AKTIV_P, SZ_AKTIV_S)
+cudaError_t selbst_paare_und_federn(const SelbstArgs& s, uint32_t n_aktiv_p, uint32_t n_aktiv_s, cudaStream_t st);
 int selbst_launches_per_run();
 // Impacts after the step's integration, in two parts with a host read of the
 // path hashes' entry counts between them.

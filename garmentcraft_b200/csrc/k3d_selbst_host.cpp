@@ -259,6 +259,7 @@ cudaError_t selbst_upload(SelbstHost& H, const k3d_scene* sc, double zusatzdicke
   if ((e = alloc(s.ein_p, size_t(s.cap_ep), H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.off_t, size_t(nd) + 1, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.off_e, size_t(ne) + 1, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.aktiv_p, size_t(nd) + size_t(ne) + 1, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.inc_off, size_t(n) + 1, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.inc_cur, size_t(n), H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.zahl, size_t(SZ_COUNT), H.fest)) != cudaSuccess) return e;
@@ -278,6 +279,7 @@ cudaError_t selbst_upload(SelbstHost& H, const k3d_scene* sc, double zusatzdicke
   if ((e = alloc(s.hs.ein, size_t(s.hs.cap), H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.lmax, 2, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.off_s, size_t(ne) + 1, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.aktiv_s, size_t(ne) + 1, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.t_off, size_t(nd) + 1, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.t_cur, size_t(nd), H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.hat, size_t(nd), H.fest)) != cudaSuccess) return e;
@@ -461,7 +463,7 @@ cudaError_t selbst_run(SelbstHost& H, double h, cudaStream_t st, int& launches) 
   if ((e = cudaMemsetAsync(s.t_off, 0, sizeof(uint32_t) * (size_t(s.nd) + 1), st)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(s.t_cur, 0, sizeof(uint32_t) * size_t(std::max<int64_t>(s.nd, 1)), st)) != cudaSuccess)
     return e;
-  if ((e = selbst_paare_und_federn(s, st)) != cudaSuccess) return e;
+  if ((e = selbst_paare_und_federn(s, z[SZ_AKTIV_P], z[SZ_AKTIV_S], st)) != cudaSuccess) return e;
   H.n_pt = z[SZ_PAARE_PT];
   H.n_kk = z[SZ_PAARE_KK];
   H.n_s = n_s;
