@@ -1094,92 +1094,182 @@ __device__ __forceinline__ void vereinige(uint32_t* el, uint32_t a, uint32_t b) 
   const uint32_t ra = wurzel(el, a), rb = wurzel(el, b);
   if (ra != rb) el[ra > rb ? ra : rb] = ra < rb ? ra : rb;
 }
-// gebiete (selbstkollision.rs:931-1009) as the reference runs it, on one
-// thread: the unions depend on their order.
-__global__ void gebiete_kernel(const __grid_constant__ SelbstArgs s) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  const uint32_t n = s.zahl[SZ_SCHNITTE] < s.cap_s ? s.zahl[SZ_SCHNITTE] : s.cap_s;
-  uint32_t* el = s.sn_eltern;
-  for (uint32_t i = 0; i < n; ++i) el[i] = i;
-  uint32_t nt = 0;
-  const uint32_t cap_t = 6u * s.cap_s;
-  for (uint32_t i = 0; i < n; ++i) {
-    const uint2 et = s.sn_ke[i];
-    const uint32_t e = et.x, t = et.y;
-    const uint2 kd2 = s.k_dr[e];
-    uint32_t kde[2], nk = 0;
-    if (kd2.x != kKein) kde[nk++] = kd2.x;
-    if (kd2.y != kKein) kde[nk++] = kd2.y;
-    uint32_t andere[6], na = 0;
-    for (uint32_t q = 0; q < nk; ++q) {
-      const uint4 dk = s.d_kan[kde[q]];
-      const uint32_t f3[3] = {dk.x, dk.y, dk.z};
-      for (int a = 0; a < 3; ++a)
-        if (f3[a] != e) andere[na++] = f3[a];
-    }
-    uint32_t tn[6], ntn = 0;  // nachbardreiecke(t)
-    {
-      const uint4 dk = s.d_kan[t];
-      const uint32_t f3[3] = {dk.x, dk.y, dk.z};
-      for (int a = 0; a < 3; ++a) {
-        const uint2 u2 = s.k_dr[f3[a]];
-        if (u2.x != kKein && u2.x != t) tn[ntn++] = u2.x;
-        if (u2.y != kKein && u2.y != t) tn[ntn++] = u2.y;
-      }
-    }
-    for (uint32_t a = 0; a < na; ++a) {
-      const uint32_t j = finde_schnitt(s, andere[a], t);
-      if (j != kKein) vereinige(el, i, j);
-    }
-    for (uint32_t u = 0; u < ntn; ++u) {
-      uint32_t j = finde_schnitt(s, e, tn[u]);
-      if (j != kKein) vereinige(el, i, j);
-      for (uint32_t a = 0; a < na; ++a) {
-        j = finde_schnitt(s, andere[a], tn[u]);
-        if (j != kKein) vereinige(el, i, j);
-      }
-    }
-    const uint4 dt = s.d_kan[t];
-    const uint32_t ft[3] = {dt.x, dt.y, dt.z};
+// gebiete (selbstkollision.rs:931-1009). Linking the larger root under the
+// smaller one makes every root the smallest member of its set, so the
+// partition and the roots after the unions of the first loop do not depend
+// on their order: those run in parallel (lock-free union-find). The role
+// swaps are listed per intersection in the reference's order (counted,
+// scanned, filled); the two swap rounds, whose unions do depend on the
+// order, and the direction sums (in intersection order) run on one thread of
+// one block, in shared memory when the intersections fit.
+
+// the intersections of i's region (gleich) and its role swaps (tausch), in
+// the reference's order (selbstkollision.rs:947-981)
+template <class F, class G>
+__device__ __forceinline__ void gebiet_nachbarn(const SelbstArgs& s, uint32_t i, F&& gleich, G&& tausch) {
+  const uint2 et = s.sn_ke[i];
+  const uint32_t e = et.x, t = et.y;
+  const uint2 kd2 = s.k_dr[e];
+  uint32_t kde[2], nk = 0;
+  if (kd2.x != kKein) kde[nk++] = kd2.x;
+  if (kd2.y != kKein) kde[nk++] = kd2.y;
+  uint32_t andere[6], na = 0;
+  for (uint32_t q = 0; q < nk; ++q) {
+    const uint4 dk = s.d_kan[kde[q]];
+    const uint32_t f3[3] = {dk.x, dk.y, dk.z};
     for (int a = 0; a < 3; ++a)
-      for (uint32_t q = 0; q < nk; ++q) {
-        const uint32_t j = finde_schnitt(s, ft[a], kde[q]);
-        if (j != kKein && nt < cap_t) s.sn_tausch[nt++] = make_uint2(i, j);
+      if (f3[a] != e) andere[na++] = f3[a];
+  }
+  uint32_t tn[6], ntn = 0;  // nachbardreiecke(t)
+  {
+    const uint4 dk = s.d_kan[t];
+    const uint32_t f3[3] = {dk.x, dk.y, dk.z};
+    for (int a = 0; a < 3; ++a) {
+      const uint2 u2 = s.k_dr[f3[a]];
+      if (u2.x != kKein && u2.x != t) tn[ntn++] = u2.x;
+      if (u2.y != kKein && u2.y != t) tn[ntn++] = u2.y;
+    }
+  }
+  for (uint32_t a = 0; a < na; ++a) {
+    const uint32_t j = finde_schnitt(s, andere[a], t);
+    if (j != kKein) gleich(j);
+  }
+  for (uint32_t u = 0; u < ntn; ++u) {
+    uint32_t j = finde_schnitt(s, e, tn[u]);
+    if (j != kKein) gleich(j);
+    for (uint32_t a = 0; a < na; ++a) {
+      j = finde_schnitt(s, andere[a], tn[u]);
+      if (j != kKein) gleich(j);
+    }
+  }
+  const uint4 dt = s.d_kan[t];
+  const uint32_t ft[3] = {dt.x, dt.y, dt.z};
+  for (int a = 0; a < 3; ++a)
+    for (uint32_t q = 0; q < nk; ++q) {
+      const uint32_t j = finde_schnitt(s, ft[a], kde[q]);
+      if (j != kKein) tausch(j);
+    }
+}
+__device__ __forceinline__ uint32_t anzahl_schnitte(const SelbstArgs& s) {
+  return s.zahl[SZ_SCHNITTE] < s.cap_s ? s.zahl[SZ_SCHNITTE] : s.cap_s;
+}
+// the root of x while other threads link roots (reads only)
+__device__ __forceinline__ uint32_t wurzel_lesen(const volatile uint32_t* el, uint32_t x) {
+  uint32_t p = el[x];
+  while (p != x) {
+    x = p;
+    p = el[x];
+  }
+  return x;
+}
+__device__ __forceinline__ void vereinige_parallel(uint32_t* el, uint32_t a, uint32_t b) {
+  for (;;) {
+    a = wurzel_lesen(el, a);
+    b = wurzel_lesen(el, b);
+    if (a == b) return;
+    if (a > b) {
+      const uint32_t c = a;
+      a = b;
+      b = c;
+    }
+    if (atomicCAS(&el[b], b, a) == b) return;  // else b was linked meanwhile: again from the new roots
+  }
+}
+__global__ void __launch_bounds__(kT) gebiete_init_kernel(const __grid_constant__ SelbstArgs s) {
+  const uint32_t n = anzahl_schnitte(s);
+  SC_FOR(i, n) s.sn_eltern[i] = uint32_t(i);
+  if (blockIdx.x == 0 && threadIdx.x == 0) s.sn_toff[n] = 0u;
+}
+// the first loop's unions; the role swaps per intersection counted
+__global__ void __launch_bounds__(kT) gebiete_vereinigen_kernel(const __grid_constant__ SelbstArgs s) {
+  const uint32_t n = anzahl_schnitte(s);
+  SC_FOR(i, n) {
+    uint32_t nt = 0;
+    gebiet_nachbarn(s, uint32_t(i), [&](uint32_t j) { vereinige_parallel(s.sn_eltern, uint32_t(i), j); },
+                    [&](uint32_t) { ++nt; });
+    s.sn_toff[i] = nt;
+  }
+}
+__global__ void __launch_bounds__(kT) gebiete_tausch_kernel(const __grid_constant__ SelbstArgs s) {
+  const uint32_t n = anzahl_schnitte(s);
+  SC_FOR(i, n) {
+    uint32_t q = s.sn_toff[i];
+    gebiet_nachbarn(s, uint32_t(i), [&](uint32_t) {},
+                    [&](uint32_t j) { s.sn_tausch[q++] = make_uint2(uint32_t(i), j); });
+  }
+}
+constexpr uint32_t kGebietSmem = 2048;
+constexpr size_t kGebietSmemBytes = size_t(kGebietSmem) * (2 * sizeof(uint32_t) + 3 * sizeof(double) + sizeof(double4));
+// the two swap rounds, the roots, the direction sums (one block)
+__global__ void __launch_bounds__(1024) gebiete_runden_kernel(const __grid_constant__ SelbstArgs s) {
+  extern __shared__ double gsh[];
+  __shared__ uint32_t gebiete;
+  const uint32_t n = anzahl_schnitte(s), nt = s.sn_toff[n];
+  const bool sm = n <= kGebietSmem;
+  double4* g = reinterpret_cast<double4*>(gsh);
+  double* summe = gsh + 4 * kGebietSmem;
+  uint32_t* el = sm ? reinterpret_cast<uint32_t*>(summe + 3 * kGebietSmem) : s.sn_eltern;
+  uint32_t* partner = sm ? el + kGebietSmem : s.sn_partner;
+  if (threadIdx.x == 0) gebiete = 0;
+  if (sm)
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+      el[i] = s.sn_eltern[i];
+      g[i] = s.sn_g[i];
+      summe[3 * i] = summe[3 * i + 1] = summe[3 * i + 2] = 0.0;
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int runde = 0; runde < 2; ++runde) {
+      for (uint32_t i = 0; i < n; ++i) partner[i] = kKein;
+      for (uint32_t q = 0; q < nt; ++q) {
+        const uint2 ij = s.sn_tausch[q];
+        const uint32_t ri = wurzel(el, ij.x), rj = wurzel(el, ij.y);
+        if (rj < partner[ri]) partner[ri] = rj;
+        if (ri < partner[rj]) partner[rj] = ri;
       }
-  }
-  for (int runde = 0; runde < 2; ++runde) {
-    for (uint32_t i = 0; i < n; ++i) s.sn_partner[i] = kKein;
-    for (uint32_t q = 0; q < nt; ++q) {
-      const uint2 ij = s.sn_tausch[q];
-      const uint32_t ri = wurzel(el, ij.x), rj = wurzel(el, ij.y);
-      if (rj < s.sn_partner[ri]) s.sn_partner[ri] = rj;
-      if (ri < s.sn_partner[rj]) s.sn_partner[rj] = ri;
-    }
-    for (uint32_t q = 0; q < nt; ++q) {
-      const uint2 ij = s.sn_tausch[q];
-      const uint32_t rj = wurzel(el, ij.y);
-      if (s.sn_partner[rj] != kKein) vereinige(el, ij.x, s.sn_partner[rj]);
+      for (uint32_t q = 0; q < nt; ++q) {
+        const uint2 ij = s.sn_tausch[q];
+        const uint32_t rj = wurzel(el, ij.y);
+        if (partner[rj] != kKein) vereinige(el, ij.x, partner[rj]);
+      }
     }
   }
-  uint32_t gebiete = 0;
-  for (uint32_t i = 0; i < n; ++i) {
-    s.sn_wurzel[i] = wurzel(el, i);
-    s.sn_summe[i] = make_double4(0, 0, 0, 0);
-    if (s.sn_wurzel[i] == i) ++gebiete;
+  __syncthreads();
+  uint32_t eigene = 0;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t r = wurzel_lesen(el, i);
+    s.sn_wurzel[i] = r;
+    if (r == i) ++eigene;
+    if (!sm) s.sn_summe[i] = make_double4(0, 0, 0, 0);
   }
-  for (uint32_t i = 0; i < n; ++i) {
-    const double4 g = s.sn_g[i];
-    double4& m = s.sn_summe[s.sn_wurzel[i]];
-    m.x += g.x * g.w;
-    m.y += g.y * g.w;
-    m.z += g.z * g.w;
+  if (eigene) atomicAdd(&gebiete, eigene);
+  __syncthreads();
+  if (threadIdx.x == 0) {  // the sums in intersection order, as the reference adds them
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t r = s.sn_wurzel[i];
+      if (sm) {
+        const double4 gi = g[i];
+        summe[3 * r] += gi.x * gi.w;
+        summe[3 * r + 1] += gi.y * gi.w;
+        summe[3 * r + 2] += gi.z * gi.w;
+      } else {
+        const double4 gi = s.sn_g[i];
+        double4& m = s.sn_summe[r];
+        m.x += gi.x * gi.w;
+        m.y += gi.y * gi.w;
+        m.z += gi.z * gi.w;
+      }
+    }
+    s.zahl[SZ_GEBIETE] = gebiete;
   }
-  for (uint32_t i = 0; i < n; ++i) {
-    const double4 m = s.sn_summe[s.sn_wurzel[i]];
-    const D3 r = einheit(d3(m.x, m.y, m.z));
-    s.sn_g[i] = make_double4(r.x, r.y, r.z, s.sn_g[i].w);
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t r = s.sn_wurzel[i];
+    const D3 m = sm ? d3(summe[3 * r], summe[3 * r + 1], summe[3 * r + 2])
+                    : d3(s.sn_summe[r].x, s.sn_summe[r].y, s.sn_summe[r].z);
+    const D3 u = einheit(m);
+    s.sn_g[i] = make_double4(u.x, u.y, u.z, s.sn_g[i].w);
   }
-  s.zahl[SZ_GEBIETE] = gebiete;
 }
 
 // the first body in contact at point i (implizit.rs:700)
@@ -1619,7 +1709,7 @@ cudaError_t exclusive_scan_u32(uint32_t* data, int64_t n, uint32_t* tmp, uint32_
 }
 // normals, boxes; 2 scans, fill, sort, count, 2 scans; fill, springs, damping,
 // count, scan, fill, sort
-int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3); }
+int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3) + 6; }
 int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1; }
 
 // Impacts, part 1 (selbstkollision.rs:1196-1203): the longest edge at x1, the
@@ -1704,7 +1794,8 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
 
 // Part 3: pairs, springs, damping, incidence lists. The host has checked the
 // pair capacity and zeroed inc_off (n + 1) and inc_cur (n).
-cudaError_t selbst_paare_und_federn(const SelbstArgs& s, uint32_t n_aktiv_p, uint32_t n_aktiv_s, cudaStream_t st) {
+cudaError_t selbst_paare_und_federn(const SelbstArgs& s, uint32_t n_aktiv_p, uint32_t n_aktiv_s, uint32_t n_s,
+                                    cudaStream_t st) {
   cudaError_t e;
   pairs_fill_kernel<<<grid_for(n_aktiv_p), kT, 0, st>>>(s, n_aktiv_p);
   const int64_t pmax = int64_t(s.cap_pairs);
@@ -1724,7 +1815,21 @@ cudaError_t selbst_paare_und_federn(const SelbstArgs& s, uint32_t n_aktiv_p, uin
   // the host has zeroed hat, klemm, t_off and t_cur
   const int64_t ns = int64_t(s.cap_s);
   schnitt_fill_kernel<<<grid_for(n_aktiv_s), kT, 0, st>>>(s, n_aktiv_s);
-  gebiete_kernel<<<1, 32, 0, st>>>(s);
+  {
+    static bool gebiete_smem = false;
+    if (!gebiete_smem) {
+      if ((e = cudaFuncSetAttribute(gebiete_runden_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(kGebietSmemBytes))) != cudaSuccess)
+        return e;
+      gebiete_smem = true;
+    }
+  }
+  gebiete_init_kernel<<<grid_for(n_s), kT, 0, st>>>(s);
+  gebiete_vereinigen_kernel<<<grid_for(n_s), kT, 0, st>>>(s);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = scan(s.sn_toff, int64_t(n_s) + 1, s.sn_scan_tmp, nullptr, st)) != cudaSuccess) return e;
+  gebiete_tausch_kernel<<<grid_for(n_s), kT, 0, st>>>(s);
+  gebiete_runden_kernel<<<1, 1024, kGebietSmemBytes, st>>>(s);
   klemm_kernel<<<grid_for(ns), kT, 0, st>>>(s);
   folge_kernel<<<grid_for(s.nd), kT, 0, st>>>(s);
   if (s.rsize == 4)

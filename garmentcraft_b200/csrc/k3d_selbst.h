@@ -115,6 +115,8 @@ struct SelbstArgs {
   double4* sn_g;                  // direction (xyz) and weight
   uint32_t *sn_wurzel, *sn_eltern, *sn_partner, *sn_sp;  // regions; push-spring slots (cap_s + 1)
   uint2* sn_tausch;               // role swaps (6 per intersection at most)
+  uint32_t* sn_toff;              // role swaps per intersection, then their starts (cap_s + 1)
+  uint32_t* sn_scan_tmp;          // scan scratch for sn_toff
   double4* sn_summe;
   uint32_t *t_off, *t_cur, *t_ent;  // per triangle: its intersections (nd + 1)
   uint8_t *hat, *klemm;           // per triangle; per region root
@@ -146,7 +148,9 @@ struct SelbstArgs {
 cudaError_t selbst_hash_zaehlen(const SelbstArgs& s, cudaStream_t st);
 cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStream_t st);
 // n_aktiv_p, n_aktiv_s: the fill lists' lengths (counters SZ_AKTIV_P, SZ_AKTIV_S)
-cudaError_t selbst_paare_und_federn(const SelbstArgs& s, uint32_t n_aktiv_p, uint32_t n_aktiv_s, cudaStream_t st);
+// n_s: the intersections (counter SZ_SCHNITTE, at most cap_s)
+cudaError_t selbst_paare_und_federn(const SelbstArgs& s, uint32_t n_aktiv_p, uint32_t n_aktiv_s, uint32_t n_s,
+                                    cudaStream_t st);
 int selbst_launches_per_run();
 // Impacts after the step's integration, in two parts with a host read of the
 // path hashes' entry counts between them.

@@ -355,6 +355,8 @@ cudaError_t selbst_grow_schnitte(SelbstHost& H, uint32_t cap) {
   if ((e = alloc(s.sn_partner, cap, H.schn)) != cudaSuccess) return e;
   if ((e = alloc(s.sn_sp, size_t(cap) + 1, H.schn)) != cudaSuccess) return e;
   if ((e = alloc(s.sn_tausch, 6 * size_t(cap), H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.sn_toff, size_t(cap) + 1, H.schn)) != cudaSuccess) return e;
+  if ((e = alloc(s.sn_scan_tmp, selbst_scan_tmp_words(int64_t(cap) + 1), H.schn)) != cudaSuccess) return e;
   if ((e = alloc(s.sn_summe, cap, H.schn)) != cudaSuccess) return e;
   if ((e = alloc(s.klemm, cap, H.schn)) != cudaSuccess) return e;
   return alloc(s.t_ent, cap, H.schn);
@@ -463,7 +465,7 @@ cudaError_t selbst_run(SelbstHost& H, double h, cudaStream_t st, int& launches) 
   if ((e = cudaMemsetAsync(s.t_off, 0, sizeof(uint32_t) * (size_t(s.nd) + 1), st)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(s.t_cur, 0, sizeof(uint32_t) * size_t(std::max<int64_t>(s.nd, 1)), st)) != cudaSuccess)
     return e;
-  if ((e = selbst_paare_und_federn(s, z[SZ_AKTIV_P], z[SZ_AKTIV_S], st)) != cudaSuccess) return e;
+  if ((e = selbst_paare_und_federn(s, z[SZ_AKTIV_P], z[SZ_AKTIV_S], n_s, st)) != cudaSuccess) return e;
   H.n_pt = z[SZ_PAARE_PT];
   H.n_kk = z[SZ_PAARE_KK];
   H.n_s = n_s;
