@@ -333,26 +333,69 @@ __global__ void __launch_bounds__(kT) hash_fill_kernel(const __grid_constant__ S
 
 // Ascending entries inside each bucket: the reference fills its buckets in
 // entry order (selbstkollision.rs:316-322). The keys of a range are distinct,
-// so any sort gives the same result; Shell sort with Ciura's gaps keeps a
-// crowded bucket (hundreds of entries) from stalling its thread.
+// so any sort gives the same result. Ranges of up to kKurzSort entries are
+// sorted by one thread each (insertion sort); longer ones by a block each
+// (lang_sort_kernel), so that a crowded bucket does not stall its thread.
+constexpr uint32_t kKurzSort = 32, kLangSort = 4096;
 __device__ __forceinline__ void sort_range(uint32_t* a, uint32_t lo, uint32_t hi) {
-  const uint32_t n = hi - lo;
-  if (n < 2) return;
-  const uint32_t gaps[8] = {701u, 301u, 132u, 57u, 23u, 10u, 4u, 1u};
-  for (int g = 0; g < 8; ++g) {
-    const uint32_t gap = gaps[g];
-    if (gap >= n) continue;
-    for (uint32_t i = lo + gap; i < hi; ++i) {
-      const uint32_t key = a[i];
-      uint32_t j = i;
-      while (j >= lo + gap && a[j - gap] > key) {
-        a[j] = a[j - gap];
-        j -= gap;
-      }
-      a[j] = key;
+  if (hi - lo < 2 || hi - lo > kKurzSort) return;
+  for (uint32_t i = lo + 1; i < hi; ++i) {
+    const uint32_t key = a[i];
+    uint32_t j = i;
+    while (j > lo && a[j - 1] > key) {
+      a[j] = a[j - 1];
+      --j;
     }
+    a[j] = key;
   }
 }
+// ranges [off[b], off[b + 1]) longer than kKurzSort: bitonic in shared memory
+// up to kLangSort entries, Shell sort (Ciura's gaps) on one thread beyond
+__global__ void __launch_bounds__(kT) lang_sort_kernel(const uint32_t* off, uint32_t* a, int64_t nb) {
+  __shared__ uint32_t sh[kLangSort];
+  for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
+    const uint32_t lo = off[b], hi = off[b + 1], n = hi - lo;
+    if (n <= kKurzSort) continue;
+    if (n > kLangSort) {
+      if (threadIdx.x == 0) {
+        const uint32_t gaps[8] = {701u, 301u, 132u, 57u, 23u, 10u, 4u, 1u};
+        for (int g = 0; g < 8; ++g) {
+          const uint32_t gap = gaps[g];
+          for (uint32_t i = lo + gap; i < hi; ++i) {
+            const uint32_t key = a[i];
+            uint32_t j = i;
+            while (j >= lo + gap && a[j - gap] > key) {
+              a[j] = a[j - gap];
+              j -= gap;
+            }
+            a[j] = key;
+          }
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+    uint32_t m = 1;
+    while (m < n) m <<= 1;
+    for (uint32_t i = threadIdx.x; i < m; i += kT) sh[i] = i < n ? a[lo + i] : 0xffffffffu;
+    __syncthreads();
+    for (uint32_t k = 2; k <= m; k <<= 1)
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        for (uint32_t i = threadIdx.x; i < m; i += kT) {
+          const uint32_t p = i ^ j;
+          if (p > i) {
+            const bool auf = (i & k) == 0;
+            const uint32_t x = sh[i], y = sh[p];
+            if ((x > y) == auf) sh[i] = y, sh[p] = x;
+          }
+        }
+        __syncthreads();
+      }
+    for (uint32_t i = threadIdx.x; i < n; i += kT) a[lo + i] = sh[i];
+    __syncthreads();
+  }
+}
+unsigned grid_lang(int64_t nb) { return unsigned(nb < 148 * 4 ? (nb < 1 ? 1 : nb) : 148 * 4); }
 __global__ void __launch_bounds__(kT) bucket_sort_kernel(const __grid_constant__ SelbstArgs s) {
   SC_FOR(b, s.eimer_p) sort_range(s.ein_p, s.anf_p[b], s.anf_p[b + 1]);
   SC_FOR(b, s.eimer_k) sort_range(s.ein_k, s.anf_k[b], s.anf_k[b + 1]);
@@ -1709,8 +1752,8 @@ cudaError_t exclusive_scan_u32(uint32_t* data, int64_t n, uint32_t* tmp, uint32_
 }
 // normals, boxes; 2 scans, fill, sort, count, 2 scans; fill, springs, damping,
 // count, scan, fill, sort
-int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3) + 6; }
-int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1; }
+int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3) + 6 + 4; }
+int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1 + 3; }
 
 // Impacts, part 1 (selbstkollision.rs:1196-1203): the longest edge at x1, the
 // path boxes, the bucket counts of the point and edge path hashes. The host
@@ -1735,7 +1778,9 @@ cudaError_t selbst_stoss_antwort(const SelbstArgs& s, int iterationen, unsigned 
   hg_fill_kernel<<<grid_for(s.n), kT, 0, st>>>(s.hp2, &s.lmax[1]);
   hg_fill_kernel<<<grid_for(s.ne), kT, 0, st>>>(s.hk2, &s.lmax[1]);
   hg_sort_kernel<<<grid_for(s.hp2.eimer), kT, 0, st>>>(s.hp2);
+  lang_sort_kernel<<<grid_lang(s.hp2.eimer), kT, 0, st>>>(s.hp2.anf, s.hp2.ein, s.hp2.eimer);
   hg_sort_kernel<<<grid_for(s.hk2.eimer), kT, 0, st>>>(s.hk2);
+  lang_sort_kernel<<<grid_lang(s.hk2.eimer), kT, 0, st>>>(s.hk2.anf, s.hk2.ein, s.hk2.eimer);
   stoss_pd_kernel<<<grid_for(s.nd), kT, 0, st>>>(s);
   stoss_kk_kernel<<<grid_for(s.ne), kT, 0, st>>>(s);
   stoss_filter_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
@@ -1747,6 +1792,7 @@ cudaError_t selbst_stoss_antwort(const SelbstArgs& s, int iterationen, unsigned 
   if ((e = scan(s.im_off, s.n + 1, s.scan_tmp, nullptr, st)) != cudaSuccess) return e;
   im_fill_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
   im_sort_kernel<<<grid_for(s.n), kT, 0, st>>>(s);
+  lang_sort_kernel<<<grid_lang(s.n), kT, 0, st>>>(s.im_off, s.im_ent, s.n);
   for (int it = 0; it < iterationen; ++it) {
     antwort_a_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
     antwort_b_kernel<<<grid_for(s.n), kT, 0, st>>>(s);
@@ -1773,6 +1819,8 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   if ((e = scan(s.anf_k, int64_t(s.eimer_k) + 1, s.scan_tmp, nullptr, st)) != cudaSuccess) return e;
   hash_fill_kernel<<<grid_for(s.n > s.ne ? s.n : s.ne), kT, 0, st>>>(s);
   bucket_sort_kernel<<<grid_for(s.eimer_p > s.eimer_k ? s.eimer_p : s.eimer_k), kT, 0, st>>>(s);
+  lang_sort_kernel<<<grid_lang(s.eimer_p), kT, 0, st>>>(s.anf_p, s.ein_p, s.eimer_p);
+  lang_sort_kernel<<<grid_lang(s.eimer_k), kT, 0, st>>>(s.anf_k, s.ein_k, s.eimer_k);
   pairs_count_kernel<<<grid_for(s.nd > s.ne ? s.nd : s.ne), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = scan(s.off_t, s.nd + 1, s.scan_tmp, &s.zahl[SZ_PAARE_PT], st)) != cudaSuccess) return e;
@@ -1787,6 +1835,7 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   if ((e = scan(s.hs.anf, int64_t(s.hs.eimer) + 1, s.scan_tmp, nullptr, st)) != cudaSuccess) return e;
   hg_fill_kernel<<<grid_for(s.nd), kT, 0, st>>>(s.hs, &s.lmax[0]);
   hg_sort_kernel<<<grid_for(s.hs.eimer), kT, 0, st>>>(s.hs);
+  lang_sort_kernel<<<grid_lang(s.hs.eimer), kT, 0, st>>>(s.hs.anf, s.hs.ein, s.hs.eimer);
   schnitt_count_kernel<<<grid_for(s.ne), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return scan(s.off_s, s.ne + 1, s.scan_tmp, &s.zahl[SZ_SCHNITTE], st);
@@ -1845,6 +1894,7 @@ cudaError_t selbst_paare_und_federn(const SelbstArgs& s, uint32_t n_aktiv_p, uin
   if ((e = scan(s.inc_off, s.n + 1, s.scan_tmp, &s.zahl[SZ_INZIDENZ], st)) != cudaSuccess) return e;
   inc_fill_kernel<<<grid_for(pmax), kT, 0, st>>>(s);
   inc_sort_kernel<<<grid_for(s.n), kT, 0, st>>>(s);
+  lang_sort_kernel<<<grid_lang(s.n), kT, 0, st>>>(s.inc_off, s.inc_ent, s.n);
   inc_pos_kernel<<<grid_for(int64_t(s.cap_inc)), kT, 0, st>>>(s);
   return cudaGetLastError();
 }
