@@ -549,7 +549,7 @@ __device__ uint32_t kante_kante(const SelbstArgs& s, int64_t e, uint32_t pos) {
 
 // count pass: pair count per triangle and per edge (off_t[t], off_e[e]);
 // the triangles and edges that have pairs go to a list for the fill pass
-__global__ void __launch_bounds__(kT) pairs_count_kernel(const __grid_constant__ SelbstArgs s) {
+__global__ void __launch_bounds__(kT, 4) pairs_count_kernel(const __grid_constant__ SelbstArgs s) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {  // the scans run over n + 1 values
     s.off_t[s.nd] = 0u;
     s.off_e[s.ne] = 0u;
@@ -570,7 +570,7 @@ __global__ void __launch_bounds__(kT) pairs_count_kernel(const __grid_constant__
 // from its scanned start, so the buffer holds the point-triangle pairs in
 // triangle order, then the edge-edge pairs in edge order, whatever the list's
 // order
-__global__ void __launch_bounds__(kT) pairs_fill_kernel(const __grid_constant__ SelbstArgs s, uint32_t n_aktiv) {
+__global__ void __launch_bounds__(kT, 4) pairs_fill_kernel(const __grid_constant__ SelbstArgs s, uint32_t n_aktiv) {
   const uint32_t npt = s.zahl[SZ_PAARE_PT];
   SC_FOR(q, n_aktiv) {
     const uint32_t c = s.aktiv_p[q];
@@ -1101,7 +1101,7 @@ __device__ uint32_t kante_schnitte(const SelbstArgs& s, int64_t e, uint32_t pos,
   });
   return cnt;
 }
-__global__ void __launch_bounds__(kT) schnitt_count_kernel(const __grid_constant__ SelbstArgs s) {
+__global__ void __launch_bounds__(kT, 4) schnitt_count_kernel(const __grid_constant__ SelbstArgs s) {
   const double z = zelle_aus(&s.lmax[0]);
   if (blockIdx.x == 0 && threadIdx.x == 0) s.off_s[s.ne] = 0u;
   SC_FOR(e, s.ne) {
@@ -1111,7 +1111,7 @@ __global__ void __launch_bounds__(kT) schnitt_count_kernel(const __grid_constant
   }
 }
 // fill pass over the listed edges (their starts come from the scan)
-__global__ void __launch_bounds__(kT) schnitt_fill_kernel(const __grid_constant__ SelbstArgs s, uint32_t n_aktiv) {
+__global__ void __launch_bounds__(kT, 4) schnitt_fill_kernel(const __grid_constant__ SelbstArgs s, uint32_t n_aktiv) {
   const double z = zelle_aus(&s.lmax[0]);
   SC_FOR(q, n_aktiv) {
     const uint32_t e = s.aktiv_s[q];
@@ -1475,7 +1475,7 @@ __device__ bool kanten_kreuzen(D3 a, D3 b, D3 c, D3 d, double& so, double& wo) {
 }
 
 // the earliest point through triangle t (selbstkollision.rs:1215-1251)
-__global__ void __launch_bounds__(kT) stoss_pd_kernel(const __grid_constant__ SelbstArgs s) {
+__global__ void __launch_bounds__(kT, 4) stoss_pd_kernel(const __grid_constant__ SelbstArgs s) {
   const double z = zelle_aus(&s.lmax[1]);
   SC_FOR(t, s.nd) {
     s.st_art[t] = 0u;
@@ -1518,7 +1518,7 @@ __global__ void __launch_bounds__(kT) stoss_pd_kernel(const __grid_constant__ Se
   }
 }
 // the earliest partner edge of edge i (selbstkollision.rs:1253-1283)
-__global__ void __launch_bounds__(kT) stoss_kk_kernel(const __grid_constant__ SelbstArgs s) {
+__global__ void __launch_bounds__(kT, 4) stoss_kk_kernel(const __grid_constant__ SelbstArgs s) {
   const double z = zelle_aus(&s.lmax[1]);
   SC_FOR(i, s.ne) {
     const uint32_t slot = uint32_t(s.nd + i);

@@ -142,7 +142,10 @@ __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV
     atom_add_release(sh.g.count, 1u);
     const uint64_t t0 = globaltimer();
     int err = 0;
-    while (int(ld_acquire_u32(sh.g.count) - target) < 0) {
+    // poll the counter alone; the error flag and the time limit every 16th
+    // poll (each check is another round trip behind the acquiring load)
+    for (unsigned poll = 1; int(ld_acquire_u32(sh.g.count) - target) < 0; ++poll) {
+      if ((poll & 15u) != 0u) continue;
       if ((err = ld_relaxed_i32(&s->error)) != 0) break;
       if (globaltimer() - t0 > kBarrierLimitNs) {
         atomicCAS(&s->error, 0, K3D_STATUS_TIMEOUT);
