@@ -350,52 +350,71 @@ __device__ __forceinline__ void sort_range(uint32_t* a, uint32_t lo, uint32_t hi
   }
 }
 // ranges [off[b], off[b + 1]) longer than kKurzSort: bitonic in shared memory
-// up to kLangSort entries, Shell sort (Ciura's gaps) on one thread beyond
-__global__ void __launch_bounds__(kT) lang_sort_kernel(const uint32_t* off, uint32_t* a, int64_t nb) {
-  __shared__ uint32_t sh[kLangSort];
-  for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
-    const uint32_t lo = off[b], hi = off[b + 1], n = hi - lo;
-    if (n <= kKurzSort) continue;
-    if (n > kLangSort) {
-      if (threadIdx.x == 0) {
-        const uint32_t gaps[8] = {701u, 301u, 132u, 57u, 23u, 10u, 4u, 1u};
-        for (int g = 0; g < 8; ++g) {
-          const uint32_t gap = gaps[g];
-          for (uint32_t i = lo + gap; i < hi; ++i) {
-            const uint32_t key = a[i];
-            uint32_t j = i;
-            while (j >= lo + gap && a[j - gap] > key) {
-              a[j] = a[j - gap];
-              j -= gap;
-            }
-            a[j] = key;
+// up to kLangSort entries, Shell sort (Ciura's gaps) on one thread beyond. The
+// block checks kT ranges at a time for length and sorts the long ones of that
+// chunk one after another.
+__device__ __forceinline__ void lang_sortieren(uint32_t* a, uint32_t lo, uint32_t hi, uint32_t* sh) {
+  const uint32_t n = hi - lo;
+  if (n > kLangSort) {
+    if (threadIdx.x == 0) {
+      const uint32_t gaps[8] = {701u, 301u, 132u, 57u, 23u, 10u, 4u, 1u};
+      for (int g = 0; g < 8; ++g) {
+        const uint32_t gap = gaps[g];
+        for (uint32_t i = lo + gap; i < hi; ++i) {
+          const uint32_t key = a[i];
+          uint32_t j = i;
+          while (j >= lo + gap && a[j - gap] > key) {
+            a[j] = a[j - gap];
+            j -= gap;
           }
+          a[j] = key;
+        }
+      }
+    }
+    __syncthreads();
+    return;
+  }
+  uint32_t m = 1;
+  while (m < n) m <<= 1;
+  for (uint32_t i = threadIdx.x; i < m; i += kT) sh[i] = i < n ? a[lo + i] : 0xffffffffu;
+  __syncthreads();
+  for (uint32_t k = 2; k <= m; k <<= 1)
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < m; i += kT) {
+        const uint32_t p = i ^ j;
+        if (p > i) {
+          const bool auf = (i & k) == 0;
+          const uint32_t x = sh[i], y = sh[p];
+          if ((x > y) == auf) sh[i] = y, sh[p] = x;
         }
       }
       __syncthreads();
-      continue;
     }
-    uint32_t m = 1;
-    while (m < n) m <<= 1;
-    for (uint32_t i = threadIdx.x; i < m; i += kT) sh[i] = i < n ? a[lo + i] : 0xffffffffu;
+  for (uint32_t i = threadIdx.x; i < n; i += kT) a[lo + i] = sh[i];
+  __syncthreads();
+}
+__global__ void __launch_bounds__(kT) lang_sort_kernel(const uint32_t* off, uint32_t* a, int64_t nb) {
+  __shared__ uint32_t sh[kLangSort];
+  __shared__ uint32_t lang[kT];
+  __shared__ uint32_t zahl;
+  for (int64_t base = int64_t(blockIdx.x) * kT; base < nb; base += int64_t(gridDim.x) * kT) {
+    if (threadIdx.x == 0) zahl = 0;
     __syncthreads();
-    for (uint32_t k = 2; k <= m; k <<= 1)
-      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-        for (uint32_t i = threadIdx.x; i < m; i += kT) {
-          const uint32_t p = i ^ j;
-          if (p > i) {
-            const bool auf = (i & k) == 0;
-            const uint32_t x = sh[i], y = sh[p];
-            if ((x > y) == auf) sh[i] = y, sh[p] = x;
-          }
-        }
-        __syncthreads();
-      }
-    for (uint32_t i = threadIdx.x; i < n; i += kT) a[lo + i] = sh[i];
+    const int64_t b = base + threadIdx.x;
+    if (b < nb && off[b + 1] - off[b] > kKurzSort) lang[atomicAdd(&zahl, 1u)] = threadIdx.x;
+    __syncthreads();
+    const uint32_t m = zahl;
+    for (uint32_t q = 0; q < m; ++q) {
+      const int64_t bq = base + lang[q];
+      lang_sortieren(a, off[bq], off[bq + 1], sh);
+    }
     __syncthreads();
   }
 }
-unsigned grid_lang(int64_t nb) { return unsigned(nb < 148 * 4 ? (nb < 1 ? 1 : nb) : 148 * 4); }
+unsigned grid_lang(int64_t nb) {
+  const int64_t b = (nb + kT - 1) / kT;
+  return unsigned(b < 1 ? 1 : (b > 148 * 4 ? 148 * 4 : b));
+}
 __global__ void __launch_bounds__(kT) bucket_sort_kernel(const __grid_constant__ SelbstArgs s) {
   SC_FOR(b, s.eimer_p) sort_range(s.ein_p, s.anf_p[b], s.anf_p[b + 1]);
   SC_FOR(b, s.eimer_k) sort_range(s.ein_k, s.anf_k[b], s.anf_k[b + 1]);
