@@ -297,7 +297,8 @@ __global__ void __launch_bounds__(kBlock) adj_final_set_kernel(const __grid_cons
 // y = A x on the assembled FP64 blocks
 __global__ void __launch_bounds__(kBlock) adj_spmv_kernel(const __grid_constant__ StepArgs a, const double* x,
                                                            double* y) {
-  const double* bm = static_cast<const double*>(a.bmat);
+  const R4<double>* b4 = static_cast<const R4<double>*>(a.bmat);
+  const double* b1 = static_cast<const double*>(a.bmat) + 8 * a.bplane;
   const int64_t P = a.bplane;
   K3D_FOR(i, a.n) {
     double sx = 0.0, sy = 0.0, sz = 0.0;
@@ -305,9 +306,10 @@ __global__ void __launch_bounds__(kBlock) adj_spmv_kernel(const __grid_constant_
     for (uint32_t k = 0; k < cnt; ++k) {
       const int64_t sid = int64_t(k) * a.np + i;
       const D3 p = ld3(x, a.col[sid]);
-      sx += bm[sid] * p.x + bm[P + sid] * p.y + bm[2 * P + sid] * p.z;
-      sy += bm[3 * P + sid] * p.x + bm[4 * P + sid] * p.y + bm[5 * P + sid] * p.z;
-      sz += bm[6 * P + sid] * p.x + bm[7 * P + sid] * p.y + bm[8 * P + sid] * p.z;
+      const R4<double> u = b4[sid], v = b4[P + sid];
+      sx += u.x * p.x + u.y * p.y + u.z * p.z;
+      sy += u.w * p.x + v.x * p.y + v.y * p.z;
+      sz += v.z * p.x + v.w * p.y + b1[sid] * p.z;
     }
     st3(y, uint32_t(i), d3(sx, sy, sz));
   }

@@ -400,8 +400,11 @@ __global__ void __launch_bounds__(kBlock) assemble_kernel(const __grid_constant_
       B[4] += md;
       B[8] += md;
     }
-#pragma unroll
-    for (int q = 0; q < 9; ++q) bm[q * a.bplane + sid] = R(B[q]);
+    // the block as two 4-vectors (m00 m01 m02 m10), (m11 m12 m20 m21) and m22
+    R4<R>* b4 = reinterpret_cast<R4<R>*>(bm);
+    b4[sid] = R4<R>{R(B[0]), R(B[1]), R(B[2]), R(B[3])};
+    b4[a.bplane + sid] = R4<R>{R(B[4]), R(B[5]), R(B[6]), R(B[7])};
+    bm[8 * a.bplane + sid] = R(B[8]);
   }
 }
 

@@ -276,7 +276,9 @@ __device__ void dv_to_w(const StepArgs& a, const View<R>& vw, const Shared& sh) 
 template <typename R, bool SC>
 __device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<R>* buf, int64_t i, R beta, R& ox, R& oy,
                                         R& oz) {
-  const R* bm = static_cast<const R*>(a.bmat);
+  // blocks as (m00 m01 m02 m10), (m11 m12 m20 m21), m22: three loads a block
+  const R4<R>* b4 = static_cast<const R4<R>*>(a.bmat);
+  const R* b1 = static_cast<const R*>(a.bmat) + 8 * a.bplane;
   const int64_t P = a.bplane;
   R x = 0, y = 0, z = 0;
   const uint32_t cnt = __ldg(&a.row_cnt[i]);
@@ -285,9 +287,11 @@ __device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<R>* buf, int
     const int64_t sid = int64_t(k) * a.np + i;
     const uint32_t j = __ldg(&a.col[sid]);
     const R4<R> pj = next_dir<R>(buf[j], beta);
-    x += bm[sid] * pj.x + bm[P + sid] * pj.y + bm[2 * P + sid] * pj.z;
-    y += bm[3 * P + sid] * pj.x + bm[4 * P + sid] * pj.y + bm[5 * P + sid] * pj.z;
-    z += bm[6 * P + sid] * pj.x + bm[7 * P + sid] * pj.y + bm[8 * P + sid] * pj.z;
+    const R4<R> u = b4[sid], v = b4[P + sid];
+    const R w = b1[sid];
+    x += u.x * pj.x + u.y * pj.y + u.z * pj.z;
+    y += u.w * pj.x + v.x * pj.y + v.y * pj.z;
+    z += v.z * pj.x + v.w * pj.y + w * pj.z;
   }
   if (SC) {  // self-collision springs, matrix-free (h^2 is in their blocks)
     const R4<R>* bR = static_cast<const R4<R>*>(a.sc_bR);
