@@ -142,6 +142,45 @@ __device__ void je_eintrag(const Box& q, double zelle, uint32_t eimer, const uin
   }
 }
 
+// je_eintrag for a group of kG lanes working on one item: the lanes take
+// consecutive entries of each cell's bucket, in the reference's order; `pruefe`
+// tests one entry (filling the payload), `schreibe` writes a hit at its
+// position. The hits keep the order of the one-thread loop: within a chunk of
+// kG entries a hit's rank is the number of hits on lower lanes. Returns the
+// number of hits (the same on every lane of the group).
+constexpr int kG = 8;
+struct Gruppe {
+  unsigned maske;  // the group's lanes within the warp
+  int lane;        // this lane's index in the group
+};
+__device__ __forceinline__ Gruppe gruppe() {
+  const int l = threadIdx.x & 31;
+  return Gruppe{((1u << kG) - 1u) << (l & ~(kG - 1)), l & (kG - 1)};
+}
+template <bool FILL, typename Payload, typename T, typename W>
+__device__ uint32_t je_eintrag_gruppe(const Gruppe& gr, const Box& q, double zelle, uint32_t eimer,
+                                      const uint32_t* anf, const uint32_t* ein, uint32_t pos, T&& pruefe, W&& schreibe) {
+  if (!zellbereich_ok(q, zelle)) return 0;
+  const Cells c = cells_of(q, zelle);
+  const unsigned unter = gr.maske & ((1u << (threadIdx.x & 31)) - 1u);
+  uint32_t cnt = 0;
+  for (uint32_t a = 0; a < c.total; ++a) {
+    int64_t i, j, k;
+    cell_at(c, a, i, j, k);
+    const uint32_t h = streue(i, j, k, eimer);
+    const uint32_t lo = anf[h], hi = anf[h + 1];
+    for (uint32_t b0 = lo; b0 < hi; b0 += kG) {
+      const uint32_t e = b0 + uint32_t(gr.lane);
+      Payload pl;
+      const bool hit = e < hi && pruefe(ein[e], i, j, k, pl);
+      const unsigned b = __ballot_sync(gr.maske, hit);
+      if (FILL && hit) schreibe(pl, pos + cnt + uint32_t(__popc(b & unter)));
+      cnt += uint32_t(__popc(b));
+    }
+  }
+  return cnt;
+}
+
 // selbstkollision.rs:347-357, on p[0..n) with margin m
 __device__ __forceinline__ Box quader_punkte(const D3* p, int n, double m) {
   Box b{d3(INFINITY, INFINITY, INFINITY), d3(-INFINITY, -INFINITY, -INFINITY)};
@@ -420,66 +459,9 @@ __global__ void __launch_bounds__(kT) bucket_sort_kernel(const __grid_constant__
   SC_FOR(b, s.eimer_k) sort_range(s.ein_k, s.anf_k[b], s.anf_k[b + 1]);
 }
 
-// Point-triangle search for triangle t (selbstkollision.rs:400-466): counts,
-// or writes its pairs from `pos` on, in the reference's order.
-template <bool FILL>
-__device__ uint32_t punkt_dreieck(const SelbstArgs& s, int64_t t, uint32_t pos) {
-  const uint4 dq = s.d_idx[t];
-  const uint32_t i0 = dq.x, i1 = dq.y, i2 = dq.z;
-  if (i0 == i1 || i1 == i2 || i0 == i2) return 0;
-  const uint32_t d[3] = {i0, i1, i2};
-  const D3 p[3] = {ld3(s.x, i0), ld3(s.x, i1), ld3(s.x, i2)};
-  const double rt = s.r_dreieck[t];
-  const Box qt = quader_punkte(p, 3, rt + kZuschlagQuader);
-  const double4 n4 = s.nrm_t[t];
-  const D3 nt = d3(n4.x, n4.y, n4.z);
-  const uint4 dk = s.d_kan[t];
-  const uint32_t ek[3] = {dk.x, dk.y, dk.z};
-  D3 en[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const double4 q = s.keb[ek[k]];
-    en[k] = d3(q.x, q.y, q.z);
-  }
-  const double sg[3] = {dot(p[2] - p[0], en[0]), dot(p[0] - p[1], en[1]), dot(p[1] - p[2], en[2])};
-  const bool alle_fest = s.w[i0] <= 0.0 && s.w[i1] <= 0.0 && s.w[i2] <= 0.0;
-  uint32_t cnt = 0;
-  je_eintrag(qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck) {
-    for (int k = 0; k < 3; ++k)
-      if (gleich_oder_partner(s, v, d[k])) return;
-    if (s.w[v] <= 0.0 && alle_fest) return;
-    const Box qv = box_of(s.qp_lo, s.qp_hi, v);
-    if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, s.zelle, ci, cj, ck)) return;
-    const D3 xv = ld3(s.x, v);
-    double ruhe = rt + s.r_punkt[v];
-    double eine;
-    if (band_abstand(s, v, d, 3, eine)) ruhe = eine;
-    const double soll = ruhe + kZuschlagPaar;
-    const double sd = dot(nt, xv - p[0]);
-    if (fabs(sd) > soll) return;
-    for (int k = 0; k < 3; ++k)
-      if (dot(xv - p[k], en[k]) * sg[k] < 0.0) return;
-    double g[3];
-    naechster_dreieck(p[0], p[1], p[2], xv, g);
-    const D3 cp = (p[0] * g[0] + p[1] * g[1]) + p[2] * g[2];
-    const D3 r = xv - cp;
-    const double abstand = norm(r);
-    if (abstand > soll) return;
-    if (FILL) {
-      const uint32_t q = pos + cnt;
-      if (q < s.cap_pairs) {
-        const D3 n = abstand > 1e-12 ? r * (1.0 / abstand) : nt;
-        s.pr_idx[q] = make_uint4(v, i0, i1, i2);
-        s.pr_src[q] = make_uint2(uint32_t(t), kKein);
-        s.pr_w[q] = make_double4(1.0, -g[0], -g[1], -g[2]);
-        s.pr_nab[q] = make_double4(n.x, n.y, n.z, abstand);
-        s.pr_ruhe[q] = ruhe;
-      }
-    }
-    ++cnt;
-  });
-  return cnt;
-}
+// Point-triangle search for triangle t (selbstkollision.rs:400-466) and
+// edge-edge search for edge e (:506-598): see punkt_dreieck_gruppe and
+// kante_kante_gruppe below (a group of lanes per triangle or edge).
 
 // selbstkollision.rs:489-503
 __device__ bool ist_kuerzeste(const SelbstArgs& s, uint32_t e, D3 u, D3 m) {
@@ -506,65 +488,147 @@ __device__ bool ist_kuerzeste(const SelbstArgs& s, uint32_t e, D3 u, D3 m) {
   return true;
 }
 
-// Edge-edge search for edge e (selbstkollision.rs:506-598).
+// The searches, one group of kG lanes per triangle or edge: the tests of
+// selbstkollision.rs:400-466 (point-triangle) and :506-598 (edge-edge) per
+// candidate, the hits written in the reference's order.
+struct PaarPT {
+  uint32_t v;
+  double g0, g1, g2, ab, ruhe;
+  D3 n;
+};
 template <bool FILL>
-__device__ uint32_t kante_kante(const SelbstArgs& s, int64_t e, uint32_t pos) {
+__device__ uint32_t punkt_dreieck_gruppe(const SelbstArgs& s, const Gruppe& gr, int64_t t, uint32_t pos) {
+  const uint4 dq = s.d_idx[t];
+  const uint32_t i0 = dq.x, i1 = dq.y, i2 = dq.z;
+  if (i0 == i1 || i1 == i2 || i0 == i2) return 0;
+  const uint32_t d[3] = {i0, i1, i2};
+  const D3 p[3] = {ld3(s.x, i0), ld3(s.x, i1), ld3(s.x, i2)};
+  const double rt = s.r_dreieck[t];
+  const Box qt = quader_punkte(p, 3, rt + kZuschlagQuader);
+  const double4 n4 = s.nrm_t[t];
+  const D3 nt = d3(n4.x, n4.y, n4.z);
+  const uint4 dk = s.d_kan[t];
+  const uint32_t ek[3] = {dk.x, dk.y, dk.z};
+  D3 en[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double4 q = s.keb[ek[k]];
+    en[k] = d3(q.x, q.y, q.z);
+  }
+  const double sg[3] = {dot(p[2] - p[0], en[0]), dot(p[0] - p[1], en[1]), dot(p[1] - p[2], en[2])};
+  const bool alle_fest = s.w[i0] <= 0.0 && s.w[i1] <= 0.0 && s.w[i2] <= 0.0;
+  return je_eintrag_gruppe<FILL, PaarPT>(
+      gr, qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, pos,
+      [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck, PaarPT& o) -> bool {
+        for (int k = 0; k < 3; ++k)
+          if (gleich_oder_partner(s, v, d[k])) return false;
+        if (s.w[v] <= 0.0 && alle_fest) return false;
+        const Box qv = box_of(s.qp_lo, s.qp_hi, v);
+        if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, s.zelle, ci, cj, ck)) return false;
+        const D3 xv = ld3(s.x, v);
+        double ruhe = rt + s.r_punkt[v];
+        double eine;
+        if (band_abstand(s, v, d, 3, eine)) ruhe = eine;
+        const double soll = ruhe + kZuschlagPaar;
+        const double sd = dot(nt, xv - p[0]);
+        if (fabs(sd) > soll) return false;
+        for (int k = 0; k < 3; ++k)
+          if (dot(xv - p[k], en[k]) * sg[k] < 0.0) return false;
+        double g[3];
+        naechster_dreieck(p[0], p[1], p[2], xv, g);
+        const D3 cp = (p[0] * g[0] + p[1] * g[1]) + p[2] * g[2];
+        const D3 r = xv - cp;
+        const double abstand = norm(r);
+        if (abstand > soll) return false;
+        if (FILL) {
+          o.v = v;
+          o.g0 = g[0], o.g1 = g[1], o.g2 = g[2];
+          o.ab = abstand;
+          o.ruhe = ruhe;
+          o.n = abstand > 1e-12 ? r * (1.0 / abstand) : nt;
+        }
+        return true;
+      },
+      [&](const PaarPT& o, uint32_t q) {
+        if (q < s.cap_pairs) {
+          s.pr_idx[q] = make_uint4(o.v, i0, i1, i2);
+          s.pr_src[q] = make_uint2(uint32_t(t), kKein);
+          s.pr_w[q] = make_double4(1.0, -o.g0, -o.g1, -o.g2);
+          s.pr_nab[q] = make_double4(o.n.x, o.n.y, o.n.z, o.ab);
+          s.pr_ruhe[q] = o.ruhe;
+        }
+      });
+}
+struct PaarKK {
+  uint32_t f, b0, b1;
+  double sp, tp, ab, ruhe;
+  D3 n;
+};
+template <bool FILL>
+__device__ uint32_t kante_kante_gruppe(const SelbstArgs& s, const Gruppe& gr, int64_t e, uint32_t pos) {
   const uint2 ka = s.k_idx[e];
   const uint32_t a0 = ka.x, a1 = ka.y;
   if (a0 == a1) return 0;
   const D3 pa0 = ld3(s.x, a0), pa1 = ld3(s.x, a1);
   const Box qe = box_of(s.qk_lo, s.qk_hi, e);
-  uint32_t cnt = 0;
-  je_eintrag(qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, [&](uint32_t f, int64_t ci, int64_t cj, int64_t ck) {
-    if (int64_t(f) <= e) return;
-    const Box qf = box_of(s.qk_lo, s.qk_hi, f);
-    if (!ueberlappt(qe, qf) || !erste_zelle(qe, qf, s.zelle, ci, cj, ck)) return;
-    const uint2 kb = s.k_idx[f];
-    const uint32_t b0 = kb.x, b1 = kb.y;
-    if (gleich_oder_partner(s, a0, b0) || gleich_oder_partner(s, a1, b0) || gleich_oder_partner(s, a0, b1) ||
-        gleich_oder_partner(s, a1, b1))
-      return;
-    const uint32_t bb[2] = {b0, b1}, aa[2] = {a0, a1};
-    double band = 0.0;
-    const bool hat_band = band_abstand(s, a0, bb, 2, band) || band_abstand(s, a1, bb, 2, band) ||
-                          band_abstand(s, b0, aa, 2, band) || band_abstand(s, b1, aa, 2, band);
-    if (s.w[a0] <= 0.0 && s.w[a1] <= 0.0 && s.w[b0] <= 0.0 && s.w[b1] <= 0.0) return;
-    const D3 pb0 = ld3(s.x, b0), pb1 = ld3(s.x, b1);
-    const D3 da = pa1 - pa0, db = pb1 - pb0;
-    const double la = norm(da), lb = norm(db);
-    if (la < kKanteMin || lb < kKanteMin) return;
-    const D3 ua = da * (1.0 / la), ub = db * (1.0 / lb);
-    const double cw = dot(ua, ub);
-    if (fabs(cw) > 0.99999) return;
-    const D3 r = pb0 - pa0;
-    const double p = dot(r, ua), q = -dot(r, ub);
-    const double nen = 1.0 - cw * cw;
-    const double sa = (p + cw * q) / nen;
-    const double sb = (q + cw * p) / nen;
-    if (!(0.0 <= sa && sa <= la) || !(0.0 <= sb && sb <= lb)) return;
-    const D3 pa = pa0 + ua * sa;
-    const D3 pb = pb0 + ub * sb;
-    const D3 dv = pa - pb;
-    const double abstand = norm(dv);
-    const double ruhe = hat_band ? band : s.r_kante[e] + s.r_kante[f];
-    if (abstand > ruhe + kZuschlagPaar) return;
-    const D3 n = einheit(dv);
-    if (!ist_kuerzeste(s, f, ub, n) || !ist_kuerzeste(s, uint32_t(e), ua, n * -1.0)) return;
-    if (FILL) {
-      const uint32_t w = pos + cnt;
-      if (w < s.cap_pairs) {
-        const double sp = sa / la, tp = sb / lb;
-        s.pr_idx[w] = make_uint4(a0, a1, b0, b1);
-        s.pr_src[w] = make_uint2(uint32_t(e), f);
-        s.pr_w[w] = make_double4(1.0 - sp, sp, -(1.0 - tp), -tp);
-        s.pr_nab[w] = make_double4(n.x, n.y, n.z, abstand);
-        s.pr_ruhe[w] = ruhe;
-      }
-    }
-    ++cnt;
-  });
-  return cnt;
+  return je_eintrag_gruppe<FILL, PaarKK>(
+      gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, pos,
+      [&](uint32_t f, int64_t ci, int64_t cj, int64_t ck, PaarKK& o) -> bool {
+        if (int64_t(f) <= e) return false;
+        const Box qf = box_of(s.qk_lo, s.qk_hi, f);
+        if (!ueberlappt(qe, qf) || !erste_zelle(qe, qf, s.zelle, ci, cj, ck)) return false;
+        const uint2 kb = s.k_idx[f];
+        const uint32_t b0 = kb.x, b1 = kb.y;
+        if (gleich_oder_partner(s, a0, b0) || gleich_oder_partner(s, a1, b0) || gleich_oder_partner(s, a0, b1) ||
+            gleich_oder_partner(s, a1, b1))
+          return false;
+        const uint32_t bb[2] = {b0, b1}, aa[2] = {a0, a1};
+        double band = 0.0;
+        const bool hat_band = band_abstand(s, a0, bb, 2, band) || band_abstand(s, a1, bb, 2, band) ||
+                              band_abstand(s, b0, aa, 2, band) || band_abstand(s, b1, aa, 2, band);
+        if (s.w[a0] <= 0.0 && s.w[a1] <= 0.0 && s.w[b0] <= 0.0 && s.w[b1] <= 0.0) return false;
+        const D3 pb0 = ld3(s.x, b0), pb1 = ld3(s.x, b1);
+        const D3 da = pa1 - pa0, db = pb1 - pb0;
+        const double la = norm(da), lb = norm(db);
+        if (la < kKanteMin || lb < kKanteMin) return false;
+        const D3 ua = da * (1.0 / la), ub = db * (1.0 / lb);
+        const double cw = dot(ua, ub);
+        if (fabs(cw) > 0.99999) return false;
+        const D3 r = pb0 - pa0;
+        const double p = dot(r, ua), q = -dot(r, ub);
+        const double nen = 1.0 - cw * cw;
+        const double sa = (p + cw * q) / nen;
+        const double sb = (q + cw * p) / nen;
+        if (!(0.0 <= sa && sa <= la) || !(0.0 <= sb && sb <= lb)) return false;
+        const D3 pa = pa0 + ua * sa;
+        const D3 pb = pb0 + ub * sb;
+        const D3 dv = pa - pb;
+        const double abstand = norm(dv);
+        const double ruhe = hat_band ? band : s.r_kante[e] + s.r_kante[f];
+        if (abstand > ruhe + kZuschlagPaar) return false;
+        const D3 n = einheit(dv);
+        if (!ist_kuerzeste(s, f, ub, n) || !ist_kuerzeste(s, uint32_t(e), ua, n * -1.0)) return false;
+        if (FILL) {
+          o.f = f, o.b0 = b0, o.b1 = b1;
+          o.sp = sa / la, o.tp = sb / lb;
+          o.ab = abstand, o.ruhe = ruhe, o.n = n;
+        }
+        return true;
+      },
+      [&](const PaarKK& o, uint32_t w) {
+        if (w < s.cap_pairs) {
+          s.pr_idx[w] = make_uint4(a0, a1, o.b0, o.b1);
+          s.pr_src[w] = make_uint2(uint32_t(e), o.f);
+          s.pr_w[w] = make_double4(1.0 - o.sp, o.sp, -(1.0 - o.tp), -o.tp);
+          s.pr_nab[w] = make_double4(o.n.x, o.n.y, o.n.z, o.ab);
+          s.pr_ruhe[w] = o.ruhe;
+        }
+      });
 }
+// one group of kG lanes per item: the items of a grid-stride loop
+#define GR_FOR(i, n)                                                                                   \
+  for (int64_t i = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / kG; i < int64_t(n);                \
+       i += int64_t(gridDim.x) * blockDim.x / kG)
 
 // count pass: pair count per triangle and per edge (off_t[t], off_e[e]);
 // the triangles and edges that have pairs go to a list for the fill pass
@@ -573,15 +637,20 @@ __global__ void __launch_bounds__(kT, 4) pairs_count_kernel(const __grid_constan
     s.off_t[s.nd] = 0u;
     s.off_e[s.ne] = 0u;
   }
-  SC_FOR(t, s.nd) {
-    const uint32_t c = punkt_dreieck<false>(s, t, 0);
-    s.off_t[t] = c;
-    if (c) s.aktiv_p[atomicAdd(&s.zahl[SZ_AKTIV_P], 1u)] = uint32_t(t);
+  const Gruppe gr = gruppe();
+  GR_FOR(t, s.nd) {
+    const uint32_t c = punkt_dreieck_gruppe<false>(s, gr, t, 0);
+    if (gr.lane == 0) {
+      s.off_t[t] = c;
+      if (c) s.aktiv_p[atomicAdd(&s.zahl[SZ_AKTIV_P], 1u)] = uint32_t(t);
+    }
   }
-  SC_FOR(e, s.ne) {
-    const uint32_t c = kante_kante<false>(s, e, 0);
-    s.off_e[e] = c;
-    if (c) s.aktiv_p[atomicAdd(&s.zahl[SZ_AKTIV_P], 1u)] = uint32_t(s.nd + e);
+  GR_FOR(e, s.ne) {
+    const uint32_t c = kante_kante_gruppe<false>(s, gr, e, 0);
+    if (gr.lane == 0) {
+      s.off_e[e] = c;
+      if (c) s.aktiv_p[atomicAdd(&s.zahl[SZ_AKTIV_P], 1u)] = uint32_t(s.nd + e);
+    }
   }
 }
 
@@ -591,12 +660,13 @@ __global__ void __launch_bounds__(kT, 4) pairs_count_kernel(const __grid_constan
 // order
 __global__ void __launch_bounds__(kT, 4) pairs_fill_kernel(const __grid_constant__ SelbstArgs s, uint32_t n_aktiv) {
   const uint32_t npt = s.zahl[SZ_PAARE_PT];
-  SC_FOR(q, n_aktiv) {
+  const Gruppe gr = gruppe();
+  GR_FOR(q, n_aktiv) {
     const uint32_t c = s.aktiv_p[q];
     if (int64_t(c) < s.nd)
-      punkt_dreieck<true>(s, c, s.off_t[c]);
+      punkt_dreieck_gruppe<true>(s, gr, c, s.off_t[c]);
     else
-      kante_kante<true>(s, int64_t(c) - s.nd, npt + s.off_e[c - s.nd]);
+      kante_kante_gruppe<true>(s, gr, int64_t(c) - s.nd, npt + s.off_e[c - s.nd]);
   }
 }
 
@@ -1840,7 +1910,7 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   bucket_sort_kernel<<<grid_for(s.eimer_p > s.eimer_k ? s.eimer_p : s.eimer_k), kT, 0, st>>>(s);
   lang_sort_kernel<<<grid_lang(s.eimer_p), kT, 0, st>>>(s.anf_p, s.ein_p, s.eimer_p);
   lang_sort_kernel<<<grid_lang(s.eimer_k), kT, 0, st>>>(s.anf_k, s.ein_k, s.eimer_k);
-  pairs_count_kernel<<<grid_for(s.nd > s.ne ? s.nd : s.ne), kT, 0, st>>>(s);
+  pairs_count_kernel<<<grid_for(kG * (s.nd > s.ne ? s.nd : s.ne)), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = scan(s.off_t, s.nd + 1, s.scan_tmp, &s.zahl[SZ_PAARE_PT], st)) != cudaSuccess) return e;
   if ((e = scan(s.off_e, s.ne + 1, s.scan_tmp, &s.zahl[SZ_PAARE_KK], st)) != cudaSuccess) return e;
@@ -1865,7 +1935,7 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
 cudaError_t selbst_paare_und_federn(const SelbstArgs& s, uint32_t n_aktiv_p, uint32_t n_aktiv_s, uint32_t n_s,
                                     cudaStream_t st) {
   cudaError_t e;
-  pairs_fill_kernel<<<grid_for(n_aktiv_p), kT, 0, st>>>(s, n_aktiv_p);
+  pairs_fill_kernel<<<grid_for(kG * int64_t(n_aktiv_p)), kT, 0, st>>>(s, n_aktiv_p);
   const int64_t pmax = int64_t(s.cap_pairs);
   if (s.rsize == 4)
     federn_kernel<float><<<grid_for(pmax), kT, 0, st>>>(s);
