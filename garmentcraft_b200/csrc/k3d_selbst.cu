@@ -1128,8 +1128,14 @@ __device__ bool kante_durch_dreieck(D3 a, D3 b, D3 v0, D3 v1, D3 v2, D3 n, doubl
 
 // The intersections of edge e (selbstkollision.rs:866-903), counted or
 // written from `pos` on in the reference's order.
+struct SchnittT {
+  uint32_t t;
+  double tk, w0, w1, w2;
+  D3 n;
+  double cn;
+};
 template <bool FILL>
-__device__ uint32_t kante_schnitte(const SelbstArgs& s, int64_t e, uint32_t pos, double zelle) {
+__device__ uint32_t kante_schnitte(const SelbstArgs& s, const Gruppe& gr, int64_t e, uint32_t pos, double zelle) {
   const uint2 ka = s.k_idx[e];
   const uint2 kd = s.k_dr[e];
   const uint32_t a0 = ka.x, a1 = ka.y;
@@ -1138,73 +1144,83 @@ __device__ uint32_t kante_schnitte(const SelbstArgs& s, int64_t e, uint32_t pos,
   const D3 pe[2] = {pa, pb};
   const Box qe = quader_punkte(pe, 2, kZuschlagQuader);
   const D3 ehat = einheit(pb - pa);
-  uint32_t cnt = 0;
-  je_eintrag(qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, [&](uint32_t t, int64_t ci, int64_t cj, int64_t ck) {
-    const uint4 d = s.d_idx[t];
-    const uint32_t dd[3] = {d.x, d.y, d.z};
-    bool nachbar = false;
-    for (int k = 0; k < 3; ++k)
-      nachbar = nachbar || (s.an_naehten ? (dd[k] == a0 || dd[k] == a1)
-                                         : (gleich_oder_partner(s, a0, dd[k]) || gleich_oder_partner(s, a1, dd[k])));
-    const Box qt = box_of(s.hs.lo, s.hs.hi, t);
-    if (nachbar || !ueberlappt(qt, qe) || !erste_zelle(qe, qt, zelle, ci, cj, ck)) return;
-    const double4 n4 = s.nrm_t[t];
-    const D3 n = d3(n4.x, n4.y, n4.z);
-    double tk, w[3];
-    if (!kante_durch_dreieck(pa, pb, ld3(s.x, d.x), ld3(s.x, d.y), ld3(s.x, d.z), n, tk, w)) return;
-    const double cn = dot(n, ehat);
-    if (fabs(cn) < 1e-6) return;
-    if (FILL) {
-      const D3 p = lerp3(pa, pb, tk);
-      D3 g = d3(0, 0, 0);
-      const uint32_t kk[2] = {kd.x, kd.y};
-      for (int q = 0; q < 2; ++q) {
-        if (kk[q] == kKein) continue;
-        const uint4 dk = s.d_idx[kk[q]];
-        const uint32_t dkk[3] = {dk.x, dk.y, dk.z};
-        uint32_t o = kKein;
-        for (int a = 0; a < 3; ++a)
-          if (dkk[a] != a0 && dkk[a] != a1) {
-            o = dkk[a];
-            break;
-          }
-        if (o == kKein) continue;
-        const double4 m4 = s.nrm_t[kk[q]];
-        D3 m = einheit(cross(n, d3(m4.x, m4.y, m4.z)));
-        const D3 r = ld3(s.x, o) - p;
-        const D3 r_quer = r - ehat * dot(ehat, r);
-        if (dot(m, r_quer) < 0.0) m = m * -1.0;
-        g = g + (m - n * (dot(ehat, m) / cn));
-      }
-      const double lg = norm(g);
-      const uint32_t q = pos + cnt;
-      if (q < s.cap_s) {
-        const D3 gh = einheit(g);
-        s.sn_ke[q] = make_uint2(uint32_t(e), t);
-        s.sn_t[q] = tk;
-        s.sn_w[q] = make_double4(w[0], w[1], w[2], 0.0);
-        s.sn_g[q] = make_double4(gh.x, gh.y, gh.z, lg / sqrt(lg * lg + 2.25));
-      }
-    }
-    ++cnt;
-  });
-  return cnt;
+  return je_eintrag_gruppe<FILL, SchnittT>(
+      gr, qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, pos,
+      [&](uint32_t t, int64_t ci, int64_t cj, int64_t ck, SchnittT& o) -> bool {
+        const uint4 d = s.d_idx[t];
+        const uint32_t dd[3] = {d.x, d.y, d.z};
+        bool nachbar = false;
+        for (int k = 0; k < 3; ++k)
+          nachbar = nachbar || (s.an_naehten ? (dd[k] == a0 || dd[k] == a1)
+                                             : (gleich_oder_partner(s, a0, dd[k]) || gleich_oder_partner(s, a1, dd[k])));
+        const Box qt = box_of(s.hs.lo, s.hs.hi, t);
+        if (nachbar || !ueberlappt(qt, qe) || !erste_zelle(qe, qt, zelle, ci, cj, ck)) return false;
+        const double4 n4 = s.nrm_t[t];
+        const D3 n = d3(n4.x, n4.y, n4.z);
+        double tk, w[3];
+        if (!kante_durch_dreieck(pa, pb, ld3(s.x, d.x), ld3(s.x, d.y), ld3(s.x, d.z), n, tk, w)) return false;
+        const double cn = dot(n, ehat);
+        if (fabs(cn) < 1e-6) return false;
+        if (FILL) {
+          o.t = t;
+          o.tk = tk;
+          o.w0 = w[0], o.w1 = w[1], o.w2 = w[2];
+          o.n = n;
+          o.cn = cn;
+        }
+        return true;
+      },
+      [&](const SchnittT& o, uint32_t q) {
+        const D3 p = lerp3(pa, pb, o.tk);
+        D3 g = d3(0, 0, 0);
+        const uint32_t kk[2] = {kd.x, kd.y};
+        for (int r = 0; r < 2; ++r) {
+          if (kk[r] == kKein) continue;
+          const uint4 dk = s.d_idx[kk[r]];
+          const uint32_t dkk[3] = {dk.x, dk.y, dk.z};
+          uint32_t ot = kKein;
+          for (int a = 0; a < 3; ++a)
+            if (dkk[a] != a0 && dkk[a] != a1) {
+              ot = dkk[a];
+              break;
+            }
+          if (ot == kKein) continue;
+          const double4 m4 = s.nrm_t[kk[r]];
+          D3 m = einheit(cross(o.n, d3(m4.x, m4.y, m4.z)));
+          const D3 rr = ld3(s.x, ot) - p;
+          const D3 r_quer = rr - ehat * dot(ehat, rr);
+          if (dot(m, r_quer) < 0.0) m = m * -1.0;
+          g = g + (m - o.n * (dot(ehat, m) / o.cn));
+        }
+        const double lg = norm(g);
+        if (q < s.cap_s) {
+          const D3 gh = einheit(g);
+          s.sn_ke[q] = make_uint2(uint32_t(e), o.t);
+          s.sn_t[q] = o.tk;
+          s.sn_w[q] = make_double4(o.w0, o.w1, o.w2, 0.0);
+          s.sn_g[q] = make_double4(gh.x, gh.y, gh.z, lg / sqrt(lg * lg + 2.25));
+        }
+      });
 }
 __global__ void __launch_bounds__(kT, 4) schnitt_count_kernel(const __grid_constant__ SelbstArgs s) {
   const double z = zelle_aus(&s.lmax[0]);
   if (blockIdx.x == 0 && threadIdx.x == 0) s.off_s[s.ne] = 0u;
-  SC_FOR(e, s.ne) {
-    const uint32_t c = kante_schnitte<false>(s, e, 0, z);
-    s.off_s[e] = c;
-    if (c) s.aktiv_s[atomicAdd(&s.zahl[SZ_AKTIV_S], 1u)] = uint32_t(e);
+  const Gruppe gr = gruppe();
+  GR_FOR(e, s.ne) {
+    const uint32_t c = kante_schnitte<false>(s, gr, e, 0, z);
+    if (gr.lane == 0) {
+      s.off_s[e] = c;
+      if (c) s.aktiv_s[atomicAdd(&s.zahl[SZ_AKTIV_S], 1u)] = uint32_t(e);
+    }
   }
 }
 // fill pass over the listed edges (their starts come from the scan)
 __global__ void __launch_bounds__(kT, 4) schnitt_fill_kernel(const __grid_constant__ SelbstArgs s, uint32_t n_aktiv) {
   const double z = zelle_aus(&s.lmax[0]);
-  SC_FOR(q, n_aktiv) {
+  const Gruppe gr = gruppe();
+  GR_FOR(q, n_aktiv) {
     const uint32_t e = s.aktiv_s[q];
-    kante_schnitte<true>(s, e, s.off_s[e], z);
+    kante_schnitte<true>(s, gr, e, s.off_s[e], z);
   }
 }
 
@@ -1925,7 +1941,7 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   hg_fill_kernel<<<grid_for(s.nd), kT, 0, st>>>(s.hs, &s.lmax[0]);
   hg_sort_kernel<<<grid_for(s.hs.eimer), kT, 0, st>>>(s.hs);
   lang_sort_kernel<<<grid_lang(s.hs.eimer), kT, 0, st>>>(s.hs.anf, s.hs.ein, s.hs.eimer);
-  schnitt_count_kernel<<<grid_for(s.ne), kT, 0, st>>>(s);
+  schnitt_count_kernel<<<grid_for(kG * s.ne), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return scan(s.off_s, s.ne + 1, s.scan_tmp, &s.zahl[SZ_SCHNITTE], st);
 }
@@ -1952,7 +1968,7 @@ cudaError_t selbst_paare_und_federn(const SelbstArgs& s, uint32_t n_aktiv_p, uin
   // penetration regions and their push springs (selbstkollision.rs:858-1058);
   // the host has zeroed hat, klemm, t_off and t_cur
   const int64_t ns = int64_t(s.cap_s);
-  schnitt_fill_kernel<<<grid_for(n_aktiv_s), kT, 0, st>>>(s, n_aktiv_s);
+  schnitt_fill_kernel<<<grid_for(kG * int64_t(n_aktiv_s)), kT, 0, st>>>(s, n_aktiv_s);
   {
     static bool gebiete_smem = false;
     if (!gebiete_smem) {
