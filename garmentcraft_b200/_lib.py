@@ -23,7 +23,8 @@ EXPORTS = [
     "k3d_operator_noalloc", "k3d_selfcollision_pairs", "k3d_selfcollision_hash", "k3d_selfcollision_springs",
     "k3d_adjoint_forward", "k3d_adjoint_backward",
     "k3d_mesh_create", "k3d_mesh_destroy", "k3d_mesh_last_error", "k3d_mesh_update", "k3d_mesh_get_info",
-    "k3d_mesh_tables", "k3d_mesh_nearest", "k3d_mesh_penetration", "k3d_mesh_sdf",
+    "k3d_mesh_tables", "k3d_mesh_nearest", "k3d_mesh_penetration", "k3d_mesh_sdf", "k3d_mesh_set_velocity",
+    "k3d_mesh_velocity_at",
 ]
 
 _lib = None
@@ -119,6 +120,10 @@ def lib():
     L.k3d_mesh_penetration.restype = st
     L.k3d_mesh_sdf.argtypes = [P, i32p, dp, C.c_double, C.c_double, C.POINTER(C.c_float)]
     L.k3d_mesh_sdf.restype = st
+    L.k3d_mesh_set_velocity.argtypes = [P, dp]
+    L.k3d_mesh_set_velocity.restype = st
+    L.k3d_mesh_velocity_at.argtypes = [P, i32p, dp, C.c_int64, dp, dp]
+    L.k3d_mesh_velocity_at.restype = st
     if L.k3d_abi_version() != _abi.K3D_ABI_VERSION:
         raise RuntimeError("libklon3d_b200.so ABI version mismatch")
     _lib = L

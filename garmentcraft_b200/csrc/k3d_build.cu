@@ -244,10 +244,9 @@ __device__ void build_points(const StepArgs& a, const View<R>& vw, double& held)
       const int inst = a.pinst ? int(a.pinst[i]) : 0;
       for (int kb = 0; kb < a.n_bodies; ++kb) {
         if (a.bodies[kb].inst >= 0 && a.bodies[kb].inst != inst) continue;
-        D3 nn;
+        D3 nn, bv;
         double tiefe;
-        if (kontakt(a.bodies[kb], xi, a.kabst[i] + a.kontakt_rand, nn, tiefe)) {
-          const D3 bv = d3(a.bodies[kb].vel[0], a.bodies[kb].vel[1], a.bodies[kb].vel[2]);
+        if (kontakt_v(a.bodies[kb], xi, a.kabst[i] + a.kontakt_rand, nn, tiefe, bv)) {
           nrm = nn;
           vn_soll = (tiefe - a.kontakt_rand) / h + dot(bv, nn);
           vb = bv;
@@ -455,7 +454,7 @@ __device__ void integrate(const StepArgs& a, double (&cnt)[4]) {
         if (netz::durchstoss(*k.netz, alt - vers, x - vers, pl, nk, t)) {
           cnt[3] += 1.0;
           x = (pl + vers) + nk * a.kabst[i];
-          const D3 vk = d3(k.vel[0], k.vel[1], k.vel[2]);
+          const D3 vk = netz::geschwindigkeit_an(*k.netz, t, pl, d3(k.vel[0], k.vel[1], k.vel[2]));
           const D3 rel = v - vk;
           const double vn = dot(rel, nk);
           if (vn < 0.0) {
@@ -470,11 +469,10 @@ __device__ void integrate(const StepArgs& a, double (&cnt)[4]) {
     }
     for (int kb = 0; kb < a.n_bodies; ++kb) {
       if (a.bodies[kb].inst >= 0 && a.bodies[kb].inst != inst) continue;
-      D3 nn;
+      D3 nn, bv;
       double tiefe;
-      if (kontakt(a.bodies[kb], x, a.kabst[i], nn, tiefe)) {
+      if (kontakt_v(a.bodies[kb], x, a.kabst[i], nn, tiefe, bv)) {
         x = x + nn * tiefe;
-        const D3 bv = d3(a.bodies[kb].vel[0], a.bodies[kb].vel[1], a.bodies[kb].vel[2]);
         const double vn = dot(v - bv, nn);
         if (vn < 0.0) v = v - nn * vn;
         if (kb < kMaxAdjointBodies) fl |= (1u << (4 + 2 * kb)) | (vn < 0.0 ? 1u << (5 + 2 * kb) : 0u);

@@ -35,8 +35,11 @@ constexpr int kMaxBodies = 64;
 // Contact query, sim/src/koerper.rs:69-91 for the cylinder and the mesh (the
 // exact nearest point within max(search depth, distance), koerper.rs:80-87);
 // the SDF grid is a trilinear interpolant of node values (value and
-// gradient), no contact outside the grid.
-__device__ inline bool kontakt(const Body& k, D3 x, double abstand, D3& normale, double& tiefe) {
+// gradient), no contact outside the grid. vk: the body's velocity at the
+// contact (a mesh with a velocity field: at the nearest point).
+__device__ inline bool kontakt(const Body& k, D3 x, double abstand, D3& normale, double& tiefe);
+__device__ inline bool kontakt_v(const Body& k, D3 x, double abstand, D3& normale, double& tiefe, D3& vk) {
+  vk = d3(k.vel[0], k.vel[1], k.vel[2]);
   if (k.art == 2) {
     netz::Treffer t;
     const D3 xl = x - d3(k.punkt[0], k.punkt[1], k.punkt[2]);
@@ -44,7 +47,15 @@ __device__ inline bool kontakt(const Body& k, D3 x, double abstand, D3& normale,
     tiefe = abstand - t.abstand;
     if (!(tiefe > 0.0)) return false;
     normale = t.normale;
+    vk = netz::geschwindigkeit_an(*k.netz, t.dreieck, t.punkt, vk);
     return true;
+  }
+  return kontakt(k, x, abstand, normale, tiefe);
+}
+__device__ inline bool kontakt(const Body& k, D3 x, double abstand, D3& normale, double& tiefe) {
+  if (k.art == 2) {
+    D3 vk;
+    return kontakt_v(k, x, abstand, normale, tiefe, vk);
   }
   if (k.art == 0) {
     D3 ax = d3(k.achse[0], k.achse[1], k.achse[2]);

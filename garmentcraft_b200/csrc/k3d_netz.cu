@@ -351,6 +351,14 @@ __global__ void __launch_bounds__(kT) durchstoss_kernel(const __grid_constant__ 
   }
 }
 
+// the surface velocity at given (triangle, point) pairs
+__global__ void __launch_bounds__(kT) geschwindigkeit_kernel(const __grid_constant__ Dev g, const int32_t* dr,
+                                                             const double* p, int64_t n, double sx, double sy,
+                                                             double sz, double* out) {
+  for (int64_t q = int64_t(blockIdx.x) * kT + threadIdx.x; q < n; q += int64_t(gridDim.x) * kT)
+    st3(out, uint32_t(q), geschwindigkeit_an(g, uint32_t(dr[q]), ld3(p, uint32_t(q)), d3(sx, sy, sz)));
+}
+
 // ---------------------------------------------------------------- voxelisation
 // The nearest query for the voxeliser: the same result distance as
 // naechster (the value does not depend on the visiting order), found faster:
@@ -569,6 +577,7 @@ struct k3d_mesh {
   int64_t zahl[3] = {0, 0, 0};
   Dev g{};
   Dev* g_dev = nullptr;              // device copy of g, read by the step's contact query
+  double* pv_buf = nullptr;          // velocity field storage (3 per point); g.pv points here when set
   std::vector<double> punkte;        // host copy of the current positions
   std::vector<void*> fest;           // allocations of fixed size
   uint32_t *anf = nullptr, *cur = nullptr;  // cell starts and fill cursors (Z + 1)
@@ -834,6 +843,8 @@ k3d_status k3d_mesh_create(const double* punkte, int64_t n, const uint32_t* drei
     g.nd = nd;
     g.suchtiefe = suchtiefe;
     NCK(alloc(m, m->g_dev, 1), "alloc");
+    NCK(alloc(m, m->pv_buf, size_t(3 * n)), "alloc");
+    g.pv = nullptr;
     double* p = nullptr;
     uint4 *d = nullptr, *nb = nullptr;
     uint32_t *po = nullptr, *pe = nullptr;
@@ -880,8 +891,11 @@ k3d_status k3d_mesh_update(k3d_mesh* m, const double* punkte) {
   double* p = const_cast<double*>(m->g.p);
   Uhr uhr(m);
   NCK(cudaMemcpyAsync(p, punkte, size_t(3 * m->n) * sizeof(double), cudaMemcpyHostToDevice, st), "upload");
+  const double* pv_alt = m->g.pv;
+  m->g.pv = nullptr;  // the velocity field belonged to the old positions (netzkoerper.rs:409)
   k3d_status r = punktabhaengig_und_gitter(m);
   if (r == K3D_BAD_ARGUMENT) {
+    m->g.pv = pv_alt;  // refused: the mesh keeps its positions and its field
     // keep the previous positions and everything that hangs on them
     const std::string why = !(m->volumen > 0.0) ? "volume <= 0 after deforming: the mesh turned inside out" : m->err;
     NCK(cudaMemcpyAsync(p, m->punkte.data(), size_t(3 * m->n) * sizeof(double), cudaMemcpyHostToDevice, st),
@@ -894,6 +908,18 @@ k3d_status k3d_mesh_update(k3d_mesh* m, const double* punkte) {
   if (r != K3D_OK) return r;
   NCK(uhr.stopp(), "update");
   m->punkte.assign(punkte, punkte + 3 * m->n);
+  return K3D_OK;
+}
+
+k3d_status k3d_mesh_set_velocity(k3d_mesh* m, const double* v) {
+  if (!m) return K3D_BAD_ARGUMENT;
+  if (v && !endlich(v, 3 * m->n)) return fail(m, K3D_BAD_ARGUMENT, "a velocity is not finite");
+  NCK(cudaSetDevice(m->device), "device");
+  cudaStream_t st = m->stream;
+  if (v) NCK(cudaMemcpyAsync(m->pv_buf, v, size_t(3 * m->n) * sizeof(double), cudaMemcpyHostToDevice, st), "upload");
+  m->g.pv = v ? m->pv_buf : nullptr;
+  NCK(cudaMemcpyAsync(m->g_dev, &m->g, sizeof(Dev), cudaMemcpyHostToDevice, st), "view");
+  NCK(cudaStreamSynchronize(st), "velocity");
   return K3D_OK;
 }
 
@@ -976,6 +1002,32 @@ k3d_status k3d_mesh_nearest(k3d_mesh* m, const double* x, int64_t n, double radi
   if (normale) NCK(cudaMemcpyAsync(normale, dno, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, st), "read");
   if (dreieck) NCK(cudaMemcpyAsync(dreieck, ddr, N * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read");
   if (region) NCK(cudaMemcpyAsync(region, drg, N * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read");
+  NCK(cudaStreamSynchronize(st), "read");
+  return K3D_OK;
+}
+
+k3d_status k3d_mesh_velocity_at(k3d_mesh* m, const int32_t* dreieck, const double* punkt, int64_t n,
+                                const double starr[3], double* out) {
+  if (!m || n < 0 || (n > 0 && (!dreieck || !punkt || !out)) || !starr) return fail(m, K3D_BAD_ARGUMENT, "null argument");
+  if (n >= (int64_t(1) << 30)) return fail(m, K3D_BAD_ARGUMENT, "over 2^30 points");
+  for (int64_t q = 0; q < n; ++q)
+    if (dreieck[q] < 0 || int64_t(dreieck[q]) >= m->nd) return fail(m, K3D_BAD_ARGUMENT, "triangle out of range");
+  if (n == 0) return K3D_OK;
+  NCK(cudaSetDevice(m->device), "device");
+  cudaStream_t st = m->stream;
+  const size_t N = size_t(n);
+  NCK(io_grow(m, N * 6 * sizeof(double) + N * sizeof(int32_t)), "alloc");
+  double* dp = static_cast<double*>(m->io);
+  double* dout = dp + 3 * N;
+  int32_t* ddr = reinterpret_cast<int32_t*>(dout + 3 * N);
+  NCK(cudaMemcpyAsync(dp, punkt, 3 * N * sizeof(double), cudaMemcpyHostToDevice, st), "upload");
+  NCK(cudaMemcpyAsync(ddr, dreieck, N * sizeof(int32_t), cudaMemcpyHostToDevice, st), "upload");
+  Uhr uhr(m);
+  geschwindigkeit_kernel<<<blocks_for(n), kT, 0, st>>>(m->g, ddr, dp, n, starr[0], starr[1], starr[2], dout);
+  NCK(cudaGetLastError(), "velocity");
+  NCK(uhr.stopp(), "velocity");
+  m->kernels = 1;
+  NCK(cudaMemcpyAsync(out, dout, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, st), "read");
   NCK(cudaStreamSynchronize(st), "read");
   return K3D_OK;
 }

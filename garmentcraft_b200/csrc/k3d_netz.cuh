@@ -26,6 +26,7 @@ struct Dev {
   double* wk;       // corner angles, 3 per triangle
   double* vt;       // volume term per triangle
   const uint32_t *pi_off, *pi_ent;
+  const double* pv;  // velocity per point (3 per point), null: the body moves rigidly
   // grid
   double u0, u1, u2, zelle;
   int32_t zx, zy, zz;
@@ -187,6 +188,34 @@ __device__ inline bool naechster(const Dev& g, D3 x, double radius, Treffer& out
   if (!hit) return false;
   out = ergebnis(g, x, bt, bq, br);
   return true;
+}
+
+// netzkoerper.rs:474-489 with the barycentric weights of :229-243: the
+// surface velocity at p on triangle t, the rigid one without a field
+__device__ inline D3 geschwindigkeit_an(const Dev& g, uint32_t t, D3 p, D3 starr) {
+  if (!g.pv) return starr;
+  const uint4 d = g.d[t];
+  const D3 a = punkt(g, d.x), b = punkt(g, d.y), c = punkt(g, d.z);
+  const D3 e1 = b - a, e2 = c - a, e3 = p - a;
+  const double d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2);
+  const double d20 = dot(e3, e1), d21 = dot(e3, e2);
+  const double nenner = d00 * d11 - d01 * d01;
+  double w[3] = {1.0, 0.0, 0.0};
+  if (nenner != 0.0) {
+    const double u = (d11 * d20 - d01 * d21) / nenner;
+    const double v = (d00 * d21 - d01 * d20) / nenner;
+    w[0] = 1.0 - u - v, w[1] = u, w[2] = v;
+  }
+  const uint32_t ix[3] = {d.x, d.y, d.z};
+  D3 q = d3(0.0, 0.0, 0.0);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const D3 vj = ld3(g.pv, ix[j]);
+    q.x += w[j] * vj.x;
+    q.y += w[j] * vj.y;
+    q.z += w[j] * vj.z;
+  }
+  return q;
 }
 
 // netzkoerper.rs:541-593 for one segment a -> b: the first entry from

@@ -90,6 +90,26 @@ class Koerpernetz:
                                             _d(kg)))
         return dict(flaechennormale=fn, punktnormale=pn, nachbar=nb, kugel=kg)
 
+    def setze_punktgeschwindigkeit(self, v=None) -> None:
+        """Koerpernetz::setze_punktgeschwindigkeit (:454-463): the velocity
+        per point of a deforming body; None clears it (rigid again)."""
+        if v is None or len(v) == 0:
+            self._check(self._L.k3d_mesh_set_velocity(self._h, None))
+            return
+        a = _f64(v)
+        if a.shape[0] != self.n_punkte:
+            raise K3dError(_abi.K3D_BAD_ARGUMENT, f"velocity for {a.shape[0]} points, the mesh has {self.n_punkte}")
+        self._check(self._L.k3d_mesh_set_velocity(self._h, _d(a)))
+
+    def geschwindigkeit_an(self, dreieck, punkt, starr=(0.0, 0.0, 0.0)) -> np.ndarray:
+        """Koerpernetz::geschwindigkeit_an (:474-489) per (triangle, point)."""
+        dr = np.ascontiguousarray(dreieck, dtype=np.int32).reshape(-1)
+        p = _f64(punkt)
+        out = np.zeros((dr.shape[0], 3))
+        self._check(self._L.k3d_mesh_velocity_at(self._h, dr.ctypes.data_as(_ip), _d(p), dr.shape[0],
+                                                 _d(_f64(starr, (3,))), _d(out)))
+        return out
+
     # ------------------------------------------------------------------ queries
     def _nearest(self, x, radius: float) -> dict:
         x = _f64(x)

@@ -72,6 +72,19 @@ typedef struct k3d_mesh_info {
 } k3d_mesh_info;
 k3d_status k3d_mesh_get_info(const k3d_mesh* m, k3d_mesh_info* out);
 
+/* setze_punktgeschwindigkeit (:454-463): v 3 per point (m/s), the velocity
+ * field of a deforming body, or null to clear it (the body moves rigidly
+ * again). Contacts and the step's segment check then take the body's
+ * velocity at the hit from the field (geschwindigkeit_an, :474-489, the
+ * barycentric mix of the hit triangle's point velocities); k3d_mesh_update
+ * clears the field, as nachfuehren does (:409). */
+k3d_status k3d_mesh_set_velocity(k3d_mesh* m, const double* v);
+
+/* geschwindigkeit_an (:474-489) per (triangle, point on it): out 3 per
+ * point, starr (3) where no field is set. */
+k3d_status k3d_mesh_velocity_at(k3d_mesh* m, const int32_t* dreieck, const double* punkt, int64_t n,
+                                const double starr[3], double* out);
+
 /* The point-dependent tables (punktabhaengig, :257-290) and the edge
  * neighbours (:319-337); any pointer may be null. flaechennormale 3 per
  * triangle, punktnormale 3 per point (angle-weighted, summed in triangle
@@ -92,13 +105,13 @@ k3d_status k3d_mesh_tables(k3d_mesh* m, double* flaechennormale, double* punktno
 k3d_status k3d_mesh_nearest(k3d_mesh* m, const double* x, int64_t n, double radius, double* abstand, double* punkt,
                             double* normale, int32_t* dreieck, int32_t* region);
 
-/* Koerpernetz::durchstoss (:541-593) per segment a -> b (3 per segment):
+/* Koerpernetz::durchstoss (:541-593) per segment a -> b (3 per segment), in
+ * the mesh's frame:
  * the first entry through the surface from outside (triangles facing the
  * segment's direction are skipped); dreieck -1 where there is none; punkt on
  * the segment, normale the triangle's face normal. Among entries at exactly
  * the same segment parameter the first in the reference's cell order wins. The body
- * velocity at the hit (geschwindigkeit_an, :474-489) is the rigid body's own
- * and is not returned. */
+ * velocity at the hit is k3d_mesh_velocity_at of (dreieck, punkt). */
 k3d_status k3d_mesh_penetration(k3d_mesh* m, const double* a, const double* b, int64_t n, int32_t* dreieck,
                                 double* punkt, double* normale);
 

@@ -129,7 +129,7 @@ std::optional<Kontakt> Koerper::kontakt(V3 x, double abstand) const {
     if (!n) return std::nullopt;
     const double tiefe = abstand - n->abstand;
     if (!(tiefe > 0.0)) return std::nullopt;
-    return Kontakt{n->normale, tiefe, geschwindigkeit};
+    return Kontakt{n->normale, tiefe, netz->geschwindigkeit_an(n->dreieck, n->punkt, geschwindigkeit)};
   }
   if (art == 0) {
     V3 a = mul(achse, 1.0 / norm(achse));
@@ -183,7 +183,7 @@ std::optional<std::array<V3, 3>> Koerper::durchstoss(V3 von, V3 nach) const {
   if (art != 2) return std::nullopt;
   auto r = netz->durchstoss(sub(von, punkt), sub(nach, punkt));
   if (!r) return std::nullopt;
-  return std::array<V3, 3>{add(r->punkt, punkt), r->normale, geschwindigkeit};
+  return std::array<V3, 3>{add(r->punkt, punkt), r->normale, netz->geschwindigkeit_an(r->dreieck, r->punkt, geschwindigkeit)};
 }
 
 Koerper Koerper::verschoben(double t) const {

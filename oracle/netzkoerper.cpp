@@ -70,6 +70,18 @@ double punktabhaengig(const std::vector<V3>& p, const std::vector<std::array<uin
   return volumen;
 }
 
+// netzkoerper.rs:232-243: barycentric weights of p's projection
+std::array<double, 3> schwerpunktgewichte(V3 p, V3 a, V3 b, V3 c) {
+  const V3 e1 = sub(b, a), e2 = sub(c, a), e3 = sub(p, a);
+  const double d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2);
+  const double d20 = dot(e3, e1), d21 = dot(e3, e2);
+  const double nenner = d00 * d11 - d01 * d01;
+  if (nenner == 0.0) return {1.0, 0.0, 0.0};
+  const double u = (d11 * d20 - d01 * d21) / nenner;
+  const double w = (d00 * d21 - d01 * d20) / nenner;
+  return {1.0 - u - w, u, w};
+}
+
 // netzkoerper.rs:785-797
 void huelle(const std::vector<V3>& p, V3& lo, V3& hi) {
   lo = {INFINITY, INFINITY, INFINITY};
@@ -237,8 +249,28 @@ std::optional<std::string> Koerpernetz::nachfuehren(const std::vector<V3>& p) {
   if (v <= 0.0) return std::string("volume <= 0 after deforming: the mesh turned inside out");
   punkte = p;
   volumen = v;
+  punktgeschwindigkeit.clear();  // the field belonged to the old positions
   gitter_bauen();
   return std::nullopt;
+}
+
+// netzkoerper.rs:454-463
+std::optional<std::string> Koerpernetz::setze_punktgeschwindigkeit(const std::vector<V3>& v) {
+  if (!v.empty() && v.size() != punkte.size()) return std::string("velocity field size differs from the points");
+  punktgeschwindigkeit = v;
+  return std::nullopt;
+}
+// netzkoerper.rs:474-489
+V3 Koerpernetz::geschwindigkeit_an(size_t t, V3 p, V3 starr) const {
+  if (punktgeschwindigkeit.empty()) return starr;
+  const auto& d = dreiecke[t];
+  const auto g = schwerpunktgewichte(p, punkte[d[0]], punkte[d[1]], punkte[d[2]]);
+  V3 q{0.0, 0.0, 0.0};
+  for (int j = 0; j < 3; ++j) {
+    const V3 v = punktgeschwindigkeit[d[j]];
+    for (int k = 0; k < 3; ++k) q[k] += g[j] * v[k];
+  }
+  return q;
 }
 
 // netzkoerper.rs:431-438
@@ -485,6 +517,26 @@ void orc_netz_durchstoss(void* h, const double* a, const double* b, int64_t n, i
       if (punkt) punkt[3 * q + c] = r ? r->punkt[c] : 0.0;
       if (normale) normale[3 * q + c] = r ? r->normale[c] : 0.0;
     }
+  }
+}
+// setze_punktgeschwindigkeit: v 3 per point, or null to clear
+int32_t orc_netz_setze_geschwindigkeit(void* h, const double* v, int64_t n, char* err, int64_t err_cap) {
+  auto* k = static_cast<Koerpernetz*>(h);
+  std::vector<V3> f;
+  if (v) f = punkte_aus(v, n);
+  if (auto e = k->setze_punktgeschwindigkeit(f)) {
+    fehler_setzen(*e, err, err_cap);
+    return 1;
+  }
+  return 0;
+}
+void orc_netz_geschwindigkeit_an(void* h, const int32_t* dreieck, const double* punkt, int64_t n,
+                                 const double* starr3, double* out) {
+  const auto* k = static_cast<const Koerpernetz*>(h);
+  const V3 starr = {starr3[0], starr3[1], starr3[2]};
+  for (int64_t q = 0; q < n; ++q) {
+    const V3 v = k->geschwindigkeit_an(size_t(dreieck[q]), {punkt[3 * q], punkt[3 * q + 1], punkt[3 * q + 2]}, starr);
+    for (int a = 0; a < 3; ++a) out[3 * q + a] = v[a];
   }
 }
 void orc_netz_sdf(void* h, const int32_t* dims3, const double* ursprung3, double spacing, double band, float* out) {

@@ -152,6 +152,9 @@ struct Koerpernetz {
   NetzGitter gitter;
   size_t randkanten = 0;
   double volumen = 0;
+  std::vector<V3> punktgeschwindigkeit;  // empty: the body moves rigidly
+  std::optional<std::string> setze_punktgeschwindigkeit(const std::vector<V3>& v);
+  V3 geschwindigkeit_an(size_t t, V3 p, V3 starr) const;
   static std::optional<std::string> neu(std::vector<V3> p, std::vector<std::array<uint32_t, 3>> d, double suchtiefe,
                                         Koerpernetz& out);
   std::optional<std::string> nachfuehren(const std::vector<V3>& p);

@@ -120,6 +120,9 @@ def lib():
     L.orc_netz_naechster.argtypes = [P, dp, C.c_int64, C.c_double, dp, dp, dp, i32p, i32p]
     L.orc_netz_durchstoss.argtypes = [P, dp, dp, C.c_int64, i32p, dp, dp]
     L.orc_netz_sdf.argtypes = [P, i32p, dp, C.c_double, C.c_double, C.POINTER(C.c_float)]
+    L.orc_netz_setze_geschwindigkeit.argtypes = [P, dp, C.c_int64, cp, C.c_int64]
+    L.orc_netz_setze_geschwindigkeit.restype = C.c_int32
+    L.orc_netz_geschwindigkeit_an.argtypes = [P, i32p, dp, C.c_int64, dp, dp]
     _lib = L
     return L
 
@@ -433,6 +436,26 @@ class Koerpernetz:
         self.L.orc_netz_durchstoss(self.h, _d(a), _d(b), m, dr.ctypes.data_as(C.POINTER(C.c_int32)), _d(pu),
                                    _d(no))
         return dict(dreieck=dr, punkt=pu, normale=no)
+
+    def setze_punktgeschwindigkeit(self, v=None):
+        """netzkoerper.rs:454-463; None or empty clears the field."""
+        err = C.create_string_buffer(256)
+        if v is None or len(v) == 0:
+            rc = self.L.orc_netz_setze_geschwindigkeit(self.h, None, 0, err, 256)
+        else:
+            a = f64(v).reshape(-1, 3)
+            rc = self.L.orc_netz_setze_geschwindigkeit(self.h, _d(a), a.shape[0], err, 256)
+        if rc:
+            raise ValueError(err.value.decode())
+
+    def geschwindigkeit_an(self, dreieck, punkt, starr=(0.0, 0.0, 0.0)):
+        """netzkoerper.rs:474-489 per (triangle, point)."""
+        dr = np.ascontiguousarray(dreieck, dtype=np.int32).reshape(-1)
+        p = f64(punkt).reshape(-1, 3)
+        out = np.zeros((dr.shape[0], 3))
+        self.L.orc_netz_geschwindigkeit_an(self.h, dr.ctypes.data_as(C.POINTER(C.c_int32)), _d(p), dr.shape[0],
+                                           _d(f64(starr)), _d(out))
+        return out
 
     def sdf(self, dims, ursprung, spacing: float, band: float = 0.0):
         """naechster_alle at every node, clamped to +-band when band > 0;

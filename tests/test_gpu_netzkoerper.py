@@ -196,3 +196,30 @@ def test_sdf_koerper_voll_gegen_stichprobe():
     assert np.array_equal(np.sign(got[~nah]), np.sign(soll[~nah]))
     assert np.all(np.abs(got[~nah]) == np.float32(0.03))
     assert (sdf < 0).sum() > 0.05 * sdf.size
+
+
+def test_geschwindigkeitsfeld_wie_orakel():
+    # netzkoerper.rs:1116-1215 on the device, and a random field against the oracle
+    p, d = synth.wuerfel_netz(1.0)
+    g, o = beide(p, d, 0.5)
+    feld = np.zeros((8, 3))
+    feld[7] = (0.0, 0.0, -1.0)
+    g.setze_punktgeschwindigkeit(feld)
+    r = g.naechster(np.array([[1.02, 1.0, 1.0], [1.02, 0.0, 1.0], [-1.02, 0.5, 0.5]]), 0.05)
+    v = g.geschwindigkeit_an(r["dreieck"], r["punkt"])
+    assert np.array_equal(v[0], [0.0, 0.0, -1.0]) and abs(v[1][2] + 0.5) < 1e-12
+    assert np.array_equal(v[2], [0.0, 0.0, 0.0])
+    g.setze_punktgeschwindigkeit(None)
+    assert np.array_equal(g.geschwindigkeit_an(r["dreieck"], r["punkt"], (0.3, -0.2, 0.1)), np.tile([0.3, -0.2, 0.1], (3, 1)))
+    p, d = synth.koerper_netz(segmente=96, ringe=33)
+    g, o = beide(p, d, 0.01)
+    rng = np.random.default_rng(8)
+    feld = rng.normal(0.0, 1.0, p.shape)
+    g.setze_punktgeschwindigkeit(feld)
+    o.setze_punktgeschwindigkeit(feld)
+    x = koerper_proben(p, 3000, 9)
+    r = o.naechster(x)
+    assert np.array_equal(g.geschwindigkeit_an(r["dreieck"], r["punkt"]), o.geschwindigkeit_an(r["dreieck"], r["punkt"]))
+    g.nachfuehren(p)  # clears the field, as nachfuehren does
+    assert np.array_equal(g.geschwindigkeit_an(r["dreieck"][:5], r["punkt"][:5], (1.0, 2.0, 3.0)),
+                          np.tile([1.0, 2.0, 3.0], (5, 1)))

@@ -213,3 +213,60 @@ def test_punkteregen_bleibt_draussen():
     assert liegen[0] >= 0.95 * flach.sum(), (liegen, int(flach.sum()))
     assert liegen[1] < flach.sum() / 2, liegen
     assert stoesse[0] > 0 and stoesse[1] == 0
+
+
+# ---------------------------------------------------------------- velocity field
+# netzkoerper.rs:1116-1215 (the per-point body velocity of a deforming body)
+
+def test_geschwindigkeit_wird_gemischt():
+    # a field linear in z comes out exactly at every hit (barycentric weights)
+    p, d = synth.wuerfel_netz(1.0)
+    k = O.Koerpernetz(p, d, 0.5)
+    k.setze_punktgeschwindigkeit(np.stack([p[:, 2], 0 * p[:, 2], 0 * p[:, 2]], axis=1))
+    for t in range(d.shape[0]):
+        a, b, c = p[d[t, 0]], p[d[t, 1]], p[d[t, 2]]
+        for q in (a, b, c, (a + b + c) * (1.0 / 3.0), a + (b - a) * 0.25):
+            v = k.geschwindigkeit_an([t], [q], (9.0, 9.0, 9.0))[0]
+            assert abs(v[0] - q[2]) < 1e-12 and v[1] == 0.0 and v[2] == 0.0
+    k.setze_punktgeschwindigkeit(np.tile([0.25, -0.5, 1.5], (8, 1)))
+    for t in range(d.shape[0]):
+        v = k.geschwindigkeit_an([t], [p[d[t, 0]]], (9.0, 9.0, 9.0))[0]
+        assert np.max(np.abs(v - [0.25, -0.5, 1.5])) < 1e-15
+
+
+def test_ohne_feld_gilt_die_eine_geschwindigkeit():
+    starr = (0.3, -0.2, 0.1)
+    k = wuerfel()
+    r = k.naechster([[1.02, 0.2, 0.5], [0.2, 1.02, 0.3]], 0.05)
+    v = k.geschwindigkeit_an(r["dreieck"], r["punkt"], starr)
+    assert np.array_equal(v, np.tile(starr, (2, 1)))
+
+
+def test_geschwindigkeit_je_stelle_verschieden():
+    p, d = synth.wuerfel_netz(1.0)
+    k = O.Koerpernetz(p, d, 0.5)
+    feld = np.zeros((8, 3))
+    feld[7] = (0.0, 0.0, -1.0)  # corner (1, 1, 1) moves down, the rest stand
+    k.setze_punktgeschwindigkeit(feld)
+    r = k.naechster([[1.02, 1.0, 1.0], [1.02, 0.0, 1.0], [-1.02, 0.5, 0.5]], 0.05)
+    v = k.geschwindigkeit_an(r["dreieck"], r["punkt"])
+    assert np.array_equal(v[0], [0.0, 0.0, -1.0])
+    assert abs(v[1][2] + 0.5) < 1e-12
+    assert np.array_equal(v[2], [0.0, 0.0, 0.0])
+
+
+def test_punktgeschwindigkeit_laenge_geprueft_und_nachfuehren_raeumt_ab():
+    k = wuerfel()
+    with pytest.raises(ValueError, match="size"):
+        k.setze_punktgeschwindigkeit(np.zeros((3, 3)))
+    k.setze_punktgeschwindigkeit(np.tile([1.0, 0.0, 0.0], (8, 1)))
+    r = k.naechster([[1.02, 0.2, 0.5]], 0.05)
+    assert np.array_equal(k.geschwindigkeit_an(r["dreieck"], r["punkt"])[0], [1.0, 0.0, 0.0])
+    k.setze_punktgeschwindigkeit(None)
+    assert np.array_equal(k.geschwindigkeit_an(r["dreieck"], r["punkt"], (7.0, 7.0, 7.0))[0], [7.0, 7.0, 7.0])
+    p, d = synth.zylinder_netz(0.15, -0.4, 0.4, 24, 8)
+    z = O.Koerpernetz(p, d, 0.01)
+    z.setze_punktgeschwindigkeit(np.tile([1.0, 0.0, 0.0], (p.shape[0], 1)))
+    z.nachfuehren(p)
+    r = z.naechster([[0.16, 0.0, 0.0]], 0.05)
+    assert np.array_equal(z.geschwindigkeit_an(r["dreieck"], r["punkt"], (0.5, 0.5, 0.5))[0], [0.5, 0.5, 0.5])
