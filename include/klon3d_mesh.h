@@ -14,7 +14,8 @@
  * `crates/klon3d-sim/`. Plain pointers and sizes; every array is a host
  * array owned by the caller; the handle owns its device buffers and one CUDA
  * stream, and each call returns when its results are in the caller's arrays.
- * One handle is used by one thread at a time.
+ * One handle is used by one thread at a time; each call makes the handle's
+ * device current on the calling thread (as the solver's calls do).
  */
 #ifndef KLON3D_MESH_H
 #define KLON3D_MESH_H
