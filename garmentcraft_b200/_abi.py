@@ -48,7 +48,10 @@ class K3dParams(C.Structure):
         ("selbst_steifigkeit", C.c_double),
         ("selbst_stoss_iterationen", C.c_int32),
         ("selbst_schnitte_an_naehten", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("koerperpunkt_durchgaenge", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("koerperpunkt_tiefe", C.c_double),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

@@ -487,6 +487,162 @@ __device__ void integrate(const StepArgs& a, double (&cnt)[4]) {
 }
 
 
+// ------------------------------------------------------------ body points against cloth triangles
+// netzkoerper.rs:612-735 for mesh body kb: per cloth triangle the deepest
+// stab of a body point (its line p + t n through the triangle at
+// -tief < t < -1e-9; the first of equal depth in the point grid's order),
+// then the triangles with a stab lifted in triangle order on one thread.
+__global__ void __launch_bounds__(kBlock) kp_such_kernel(const __grid_constant__ StepArgs a, int kb) {
+  if (a.kp_ctl[2]) return;
+  const Body& k = a.bodies[kb];
+  const netz::Dev& g = *k.netz;
+  const double tief = a.kp_tief, band = -1e-9, rand = fmax(tief, band);
+  const D3 vers = d3(k.punkt[0], k.punkt[1], k.punkt[2]);
+  K3D_FOR(t, a.kp_nt) {
+    const uint4 tr = a.kp_tri[t];
+    if (k.inst >= 0 && a.pinst && int(a.pinst[tr.x]) != k.inst) continue;
+    const D3 p0 = ld3(a.x, tr.x), p1 = ld3(a.x, tr.y), p2 = ld3(a.x, tr.z);
+    D3 lo = d3(fmin(fmin(p0.x, p1.x), p2.x), fmin(fmin(p0.y, p1.y), p2.y), fmin(fmin(p0.z, p1.z), p2.z));
+    D3 hi = d3(fmax(fmax(p0.x, p1.x), p2.x), fmax(fmax(p0.y, p1.y), p2.y), fmax(fmax(p0.z, p1.z), p2.z));
+    lo = (lo - vers) - d3(rand, rand, rand);
+    hi = (hi - vers) + d3(rand, rand, rand);
+    const D3 e1 = p1 - p0, e2 = p2 - p0;
+    int r0[3], r1[3];
+    if (!netz::bereich(g, lo, hi, r0, r1)) continue;
+    bool hat = false;
+    double dbest = 0.0;
+    D3 nb = d3(0, 0, 0), bb = d3(0, 0, 0);
+    uint32_t kir = 0;
+    for (int kz = r0[2]; kz <= r1[2]; ++kz)
+      for (int ky = r0[1]; ky <= r1[1]; ++ky)
+        for (int kx = r0[0]; kx <= r1[0]; ++kx) {
+          const int64_t z = (int64_t(kz) * g.zy + ky) * g.zx + kx;
+          for (uint32_t e = g.pg_anf[z]; e < g.pg_anf[z + 1]; ++e) {
+            const uint32_t q = g.pg_ein[e];
+            const D3 p = netz::punkt(g, q) + vers;
+            const D3 n = netz::ld4(g.pn[q]);
+            const D3 pv = cross(n, e2);
+            const double det = dot(e1, pv);
+            if (fabs(det) < 1e-18) continue;
+            const D3 tv = p - p0;
+            const double bu = dot(tv, pv) / det;
+            if (!(bu >= 0.0 && bu <= 1.0)) continue;
+            const D3 qv = cross(tv, e1);
+            const double bv = dot(n, qv) / det;
+            if (bv < 0.0 || bu + bv > 1.0) continue;
+            const double tt = dot(e2, qv) / det;
+            if (tt > -tief && tt < band && (!hat || -tt > dbest)) {
+              hat = true;
+              dbest = -tt;
+              nb = n;
+              bb = d3(1.0 - bu - bv, bu, bv);
+              kir = q;
+            }
+          }
+        }
+    if (hat) {
+      a.kp_a[t] = make_double4(dbest, nb.x, nb.y, nb.z);
+      a.kp_b[t] = make_double4(bb.x, bb.y, bb.z, double(kir));
+      a.kp_list[atomicAdd(&a.kp_ctl[0], 1u)] = uint32_t(t);
+    }
+  }
+}
+constexpr uint32_t kKpSort = 4096;
+__global__ void __launch_bounds__(1024) kp_anwenden_kernel(const __grid_constant__ StepArgs a, int kb) {
+  __shared__ uint32_t sh[kKpSort];
+  if (a.kp_ctl[2]) return;
+  const uint32_t m = a.kp_ctl[0] < a.kp_nt ? a.kp_ctl[0] : uint32_t(a.kp_nt);
+  uint32_t* list = a.kp_list;
+  // the listed triangles in ascending order
+  if (m > 1 && m <= kKpSort) {
+    uint32_t p2 = 1;
+    while (p2 < m) p2 <<= 1;
+    for (uint32_t i = threadIdx.x; i < p2; i += blockDim.x) sh[i] = i < m ? list[i] : 0xffffffffu;
+    __syncthreads();
+    for (uint32_t s = 2; s <= p2; s <<= 1)
+      for (uint32_t j = s >> 1; j > 0; j >>= 1) {
+        for (uint32_t i = threadIdx.x; i < p2; i += blockDim.x) {
+          const uint32_t o = i ^ j;
+          if (o > i) {
+            const bool auf = (i & s) == 0;
+            const uint32_t x = sh[i], y = sh[o];
+            if ((x > y) == auf) sh[i] = y, sh[o] = x;
+          }
+        }
+        __syncthreads();
+      }
+    list = sh;
+  } else if (m > kKpSort && threadIdx.x == 0) {  // insertion by Ciura's gaps on one thread
+    const uint32_t gaps[8] = {701u, 301u, 132u, 57u, 23u, 10u, 4u, 1u};
+    for (int gi = 0; gi < 8; ++gi)
+      for (uint32_t i = gaps[gi]; i < m; ++i) {
+        const uint32_t key = list[i];
+        uint32_t j = i;
+        while (j >= gaps[gi] && list[j - gaps[gi]] > key) {
+          list[j] = list[j - gaps[gi]];
+          j -= gaps[gi];
+        }
+        list[j] = key;
+      }
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const Body& k = a.bodies[kb];
+  const netz::Dev& g = *k.netz;
+  const D3 starr = d3(k.vel[0], k.vel[1], k.vel[2]);
+  unsigned zahl = 0;
+  for (uint32_t q = 0; q < m; ++q) {
+    const uint32_t t = list[q];
+    const double4 A = a.kp_a[t], B = a.kp_b[t];
+    const uint4 tr = a.kp_tri[t];
+    const uint32_t idx[3] = {tr.x, tr.y, tr.z};
+    const double bary[3] = {B.x, B.y, B.z}, gew[3] = {a.w[tr.x], a.w[tr.y], a.w[tr.z]};
+    double nenner = -0.0;
+    for (int j = 0; j < 3; ++j) nenner += bary[j] * bary[j] * gew[j];
+    if (nenner <= 0.0) continue;
+    const D3 n = d3(A.y, A.z, A.w);
+    const D3 vk = g.pv ? ld3(g.pv, uint32_t(B.w)) : starr;
+    D3 vq = d3(0.0, 0.0, 0.0);
+    for (int j = 0; j < 3; ++j) vq = vq + ld3(a.v, idx[j]) * bary[j];
+    vq = vq - vk;
+    const double vn = fmin(dot(vq, n), 0.0);
+    for (int j = 0; j < 3; ++j) {
+      const double f = bary[j] * gew[j] / nenner;
+      st3(a.x, idx[j], ld3(a.x, idx[j]) + n * (f * A.x));
+      st3(a.v, idx[j], ld3(a.v, idx[j]) - n * (f * vn));
+    }
+    ++zahl;
+  }
+  a.kp_ctl[1] += zahl;
+  a.kp_ctl[0] = 0u;
+  if (zahl) atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[ST_BODY_POINTS]), (unsigned long long)zahl);
+}
+// end of a pass: stop when it corrected nothing (implizit.rs:1023-1025)
+__global__ void kp_ende_kernel(const __grid_constant__ StepArgs a) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  if (!a.kp_ctl[2] && a.kp_ctl[1] == 0u) a.kp_ctl[2] = 1u;
+  a.kp_ctl[1] = 0u;
+}
+
+cudaError_t launch_koerperpunkte(const StepArgs& a, cudaStream_t st, int& launched) {
+  if (a.kp_passes <= 0 || a.kp_nt <= 0) return cudaSuccess;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(a.kp_ctl, 0, 4 * sizeof(unsigned), st)) != cudaSuccess) return e;
+  int64_t b = (a.kp_nt + kBlock - 1) / kBlock;
+  const unsigned grid = unsigned(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
+  for (int pass = 0; pass < a.kp_passes; ++pass) {
+    for (int kb = 0; kb < a.n_bodies; ++kb) {
+      if (a.bodies[kb].art != 2) continue;
+      kp_such_kernel<<<grid, kBlock, 0, st>>>(a, kb);
+      kp_anwenden_kernel<<<1, 1024, 0, st>>>(a, kb);
+      launched += 2;
+    }
+    kp_ende_kernel<<<1, 32, 0, st>>>(a);
+    launched += 1;
+  }
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------ kernels
 // Build (elements): an ordinary grid-stride launch at full occupancy.
 template <typename R>

@@ -53,6 +53,7 @@ struct k3d_solver {
   std::vector<k3d_body> bodies;         // frame-start bodies as last given
   std::vector<void*> sdf_dev;           // device copies of SDF grids
   std::vector<const netz::Dev*> netz_dev;  // mesh bodies' tables (owned by their k3d_mesh)
+  std::vector<void*> kp_mem;            // body-point pass: cloth triangles and per-triangle stabs
   std::vector<int64_t> seam_slot;       // spring index of each seam, -1 if not streamed
   std::vector<double2> s_kl_host;
   int64_t launches = 0;
@@ -285,6 +286,8 @@ void k3d_params_default(k3d_params* o) {
   o->kontakt_rand = 1e-4;
   o->normalkraft_aus_last = 0;
   o->durchstoss_pruefen = 1;
+  o->koerperpunkt_durchgaenge = 0;
+  o->koerperpunkt_tiefe = 0.01;
   o->selbstkollision = 0;
   o->precision = K3D_FP64;
   o->selbst_zusatzdicke = 2.5e-3;
@@ -352,6 +355,8 @@ static void release_device(k3d_solver* h) {
   for (void* p : h->sdf_dev) cudaFree(p);
   h->sdf_dev.clear();
   h->netz_dev.clear();
+  for (void* p : h->kp_mem) cudaFree(p);
+  h->kp_mem.clear();
   h->uploaded = false;
 }
 
@@ -758,6 +763,39 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
     }
     h->netz_dev.push_back(nv);
   }
+  // body points against cloth triangles (implizit.rs:1015-1025): the cloth
+  // triangles on the device whenever a mesh body is present, so that the
+  // pass count can change between frames
+  {
+    bool netz = false;
+    for (const k3d_body& k : h->bodies) netz = netz || k.art == K3D_BODY_MESH;
+    a.kp_passes = 0;
+    a.kp_nt = 0;
+    if (netz && s->n_dreiecke > 0) {
+      const int64_t nt = s->n_dreiecke;
+      std::vector<uint4> tri(static_cast<size_t>(nt));
+      for (int64_t t = 0; t < nt; ++t)
+        tri[size_t(t)] = make_uint4(s->dreiecke[3 * t], s->dreiecke[3 * t + 1], s->dreiecke[3 * t + 2], 0u);
+      void *pt = nullptr, *pa = nullptr, *pb = nullptr, *pl = nullptr, *pc = nullptr;
+      K3D_CUDA(h, cudaMalloc(&pt, size_t(nt) * sizeof(uint4)));
+      h->kp_mem.push_back(pt);
+      K3D_CUDA(h, cudaMalloc(&pa, size_t(nt) * sizeof(double4)));
+      h->kp_mem.push_back(pa);
+      K3D_CUDA(h, cudaMalloc(&pb, size_t(nt) * sizeof(double4)));
+      h->kp_mem.push_back(pb);
+      K3D_CUDA(h, cudaMalloc(&pl, size_t(nt) * sizeof(uint32_t)));
+      h->kp_mem.push_back(pl);
+      K3D_CUDA(h, cudaMalloc(&pc, 4 * sizeof(unsigned)));
+      h->kp_mem.push_back(pc);
+      K3D_CUDA(h, up(pt, tri.data(), tri.size() * sizeof(uint4)));
+      a.kp_tri = static_cast<const uint4*>(pt);
+      a.kp_a = static_cast<double4*>(pa);
+      a.kp_b = static_cast<double4*>(pb);
+      a.kp_list = static_cast<uint32_t*>(pl);
+      a.kp_ctl = static_cast<unsigned*>(pc);
+      a.kp_nt = nt;
+    }
+  }
   K3D_CUDA(h, cudaStreamSynchronize(st));
   if (h->p.selbstkollision) {
     if (n >= (int64_t(1) << 30) || s->n_dreiecke >= (int64_t(1) << 31))
@@ -802,6 +840,8 @@ static void step_args(k3d_solver* h, int mode, double t_bodies, bool need_load) 
   a.first_step = (mode == MODE_STEP && h->first_step) ? 1 : 0;
   a.n_bodies = int(h->bodies.size());
   a.durchstoss_pruefen = h->p.durchstoss_pruefen ? 1 : 0;
+  a.kp_passes = a.kp_nt > 0 ? std::max(h->p.koerperpunkt_durchgaenge, 0) : 0;
+  a.kp_tief = h->p.koerperpunkt_tiefe;
   for (int b = 0; b < a.n_bodies; ++b) {
     const k3d_body& k = h->bodies[b];
     Body& d = a.bodies[b];
@@ -888,6 +928,7 @@ static k3d_status read_stats(k3d_solver* h, k3d_stats* out) {
     out->haftend = st[ST_STICKING];
     out->freigegeben = st[ST_RELEASED];
     out->durchstoesse = st[ST_PENETRATIONS];
+    out->koerperpunkte = st[ST_BODY_POINTS];
     out->rest_max = rm[0];
     out->zusammenbrueche = st[ST_BREAKDOWNS];
     out->dv_max = rm[1];

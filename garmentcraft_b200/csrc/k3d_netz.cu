@@ -142,6 +142,23 @@ __device__ __forceinline__ void dreieck_zellen(const Dev& g, int64_t t, int r0[3
     r1[q] = int(b[q] > z[q] - 1 ? z[q] - 1 : (b[q] < -1 ? -1 : b[q]));
   }
 }
+// the point grid (gitter_punkte, :863-879): each point in its clamped cell
+__device__ __forceinline__ int64_t punkt_zelle(const Dev& g, uint32_t i) {
+  int64_t k[3];
+  zell_index(g, punkt(g, i), k);
+  const int64_t z[3] = {g.zx, g.zy, g.zz};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) k[q] = k[q] < 0 ? 0 : (k[q] > z[q] - 1 ? z[q] - 1 : k[q]);
+  return (k[2] * g.zy + k[1]) * g.zx + k[0];
+}
+__global__ void __launch_bounds__(kT) punkte_zaehlen_kernel(const __grid_constant__ Dev g) {
+  for (int64_t i = int64_t(blockIdx.x) * kT + threadIdx.x; i < g.n; i += int64_t(gridDim.x) * kT)
+    atomicAdd(&g.pg_anf[punkt_zelle(g, uint32_t(i))], 1u);
+}
+__global__ void __launch_bounds__(kT) punkte_fuellen_kernel(const __grid_constant__ Dev g, uint32_t* cur) {
+  for (int64_t i = int64_t(blockIdx.x) * kT + threadIdx.x; i < g.n; i += int64_t(gridDim.x) * kT)
+    g.pg_ein[atomicAdd(&cur[punkt_zelle(g, uint32_t(i))], 1u)] = uint32_t(i);
+}
 __global__ void __launch_bounds__(kT) zellen_zaehlen_kernel(const __grid_constant__ Dev g) {
   for (int64_t t = int64_t(blockIdx.x) * kT + threadIdx.x; t < g.nd; t += int64_t(gridDim.x) * kT) {
     int r0[3], r1[3];
@@ -168,25 +185,25 @@ __global__ void __launch_bounds__(kT) zellen_fuellen_kernel(const __grid_constan
 // (the cells round a pole of a latitude-longitude mesh hold hundreds) by a
 // block in shared memory (bitonic), the longest by a Shell sort of one thread.
 constexpr uint32_t kKurz = 32, kLang = 4096;
-__global__ void __launch_bounds__(kT) zellen_sortieren_kernel(const __grid_constant__ Dev g, int64_t nz) {
+__global__ void __launch_bounds__(kT) zellen_sortieren_kernel(const uint32_t* anf, uint32_t* ein, int64_t nz) {
   for (int64_t z = int64_t(blockIdx.x) * kT + threadIdx.x; z < nz; z += int64_t(gridDim.x) * kT) {
-    const uint32_t lo = g.anf[z], hi = g.anf[z + 1];
+    const uint32_t lo = anf[z], hi = anf[z + 1];
     if (hi - lo > kKurz) continue;
     for (uint32_t i = lo + 1; i < hi; ++i) {
-      const uint32_t v = g.ein[i];
+      const uint32_t v = ein[i];
       uint32_t j = i;
-      while (j > lo && g.ein[j - 1] > v) {
-        g.ein[j] = g.ein[j - 1];
+      while (j > lo && ein[j - 1] > v) {
+        ein[j] = ein[j - 1];
         --j;
       }
-      g.ein[j] = v;
+      ein[j] = v;
     }
   }
 }
-__global__ void __launch_bounds__(kT) zellen_lang_kernel(const __grid_constant__ Dev g, int64_t nz) {
+__global__ void __launch_bounds__(kT) zellen_lang_kernel(const uint32_t* anf, uint32_t* ein, int64_t nz) {
   __shared__ uint32_t sh[kLang];
   for (int64_t z = blockIdx.x; z < nz; z += gridDim.x) {
-    const uint32_t lo = g.anf[z], hi = g.anf[z + 1], n = hi - lo;
+    const uint32_t lo = anf[z], hi = anf[z + 1], n = hi - lo;
     if (n <= kKurz) continue;
     if (n > kLang) {  // Shell sort with Ciura's gaps, one thread
       if (threadIdx.x == 0) {
@@ -194,13 +211,13 @@ __global__ void __launch_bounds__(kT) zellen_lang_kernel(const __grid_constant__
         for (int k = 0; k < 8; ++k) {
           const uint32_t gap = gaps[k];
           for (uint32_t i = lo + gap; i < hi; ++i) {
-            const uint32_t key = g.ein[i];
+            const uint32_t key = ein[i];
             uint32_t j = i;
-            while (j >= lo + gap && g.ein[j - gap] > key) {
-              g.ein[j] = g.ein[j - gap];
+            while (j >= lo + gap && ein[j - gap] > key) {
+              ein[j] = ein[j - gap];
               j -= gap;
             }
-            g.ein[j] = key;
+            ein[j] = key;
           }
         }
       }
@@ -209,7 +226,7 @@ __global__ void __launch_bounds__(kT) zellen_lang_kernel(const __grid_constant__
     }
     uint32_t m = 1;
     while (m < n) m <<= 1;
-    for (uint32_t i = threadIdx.x; i < m; i += kT) sh[i] = i < n ? g.ein[lo + i] : 0xffffffffu;
+    for (uint32_t i = threadIdx.x; i < m; i += kT) sh[i] = i < n ? ein[lo + i] : 0xffffffffu;
     __syncthreads();
     for (uint32_t k = 2; k <= m; k <<= 1)
       for (uint32_t j = k >> 1; j > 0; j >>= 1) {
@@ -223,7 +240,7 @@ __global__ void __launch_bounds__(kT) zellen_lang_kernel(const __grid_constant__
         }
         __syncthreads();
       }
-    for (uint32_t i = threadIdx.x; i < n; i += kT) g.ein[lo + i] = sh[i];
+    for (uint32_t i = threadIdx.x; i < n; i += kT) ein[lo + i] = sh[i];
     __syncthreads();
   }
 }
@@ -586,6 +603,9 @@ struct k3d_mesh {
   int64_t ein_cap = 0;
   uint32_t* scan_tmp = nullptr;
   int64_t scan_cap = 0;
+  uint32_t* pg_anf = nullptr;        // point grid starts (Z + 1)
+  int64_t pg_cap = 0;
+  uint32_t* pg_ein = nullptr;        // point grid entries (N)
   double* hull = nullptr;            // 7 doubles
   uint32_t* total = nullptr;         // the scan's sum
   unsigned long long* offen = nullptr;
@@ -688,11 +708,23 @@ k3d_status gitter(k3d_mesh* m, const double h[6]) {
   g.cap = uint32_t(std::min<int64_t>(m->ein_cap, 0xffffffffll));
   NCK(cudaMemcpyAsync(m->cur, m->anf, size_t(nz) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st), "grid fill");
   zellen_fuellen_kernel<<<blocks_for(g.nd), kT, 0, st>>>(g);
-  zellen_sortieren_kernel<<<blocks_for(nz), kT, 0, st>>>(g, nz);
-  zellen_lang_kernel<<<unsigned(std::min<int64_t>(nz, 148 * 4)), kT, 0, st>>>(g, nz);
+  zellen_sortieren_kernel<<<blocks_for(nz), kT, 0, st>>>(g.anf, g.ein, nz);
+  zellen_lang_kernel<<<unsigned(std::min<int64_t>(nz, 148 * 4)), kT, 0, st>>>(g.anf, g.ein, nz);
   NCK(cudaGetLastError(), "grid fill");
+  // the point grid on the same cells (its fill cursors reuse the triangle grid's)
+  NCK(grow(m->pg_anf, m->pg_cap, nz + 1), "grid alloc");
+  g.pg_anf = m->pg_anf;
+  g.pg_ein = m->pg_ein;
+  NCK(cudaMemsetAsync(g.pg_anf, 0, size_t(nz + 1) * sizeof(uint32_t), st), "point grid");
+  punkte_zaehlen_kernel<<<blocks_for(g.n), kT, 0, st>>>(g);
+  NCK(exclusive_scan_u32(g.pg_anf, nz + 1, m->scan_tmp, nullptr, st), "point grid");
+  NCK(cudaMemcpyAsync(m->cur, g.pg_anf, size_t(nz) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st), "point grid");
+  punkte_fuellen_kernel<<<blocks_for(g.n), kT, 0, st>>>(g, m->cur);
+  zellen_sortieren_kernel<<<blocks_for(nz), kT, 0, st>>>(g.pg_anf, g.pg_ein, nz);
+  zellen_lang_kernel<<<unsigned(std::min<int64_t>(nz, 148 * 4)), kT, 0, st>>>(g.pg_anf, g.pg_ein, nz);
+  NCK(cudaGetLastError(), "point grid");
   NCK(cudaMemcpyAsync(m->g_dev, &m->g, sizeof(Dev), cudaMemcpyHostToDevice, st), "grid view");
-  m->kernels += 1 + 3 + 3;
+  m->kernels += 1 + 3 + 3 + 1 + 3 + 1 + 2;
   return K3D_OK;
 }
 
@@ -734,7 +766,7 @@ void freigeben(k3d_mesh* m) {
   cudaSetDevice(m->device);
   for (void* p : m->fest) cudaFree(p);
   for (void* p : {static_cast<void*>(m->anf), static_cast<void*>(m->cur), static_cast<void*>(m->ein),
-                  static_cast<void*>(m->scan_tmp), m->io})
+                  static_cast<void*>(m->scan_tmp), static_cast<void*>(m->pg_anf), m->io})
     if (p) cudaFree(p);
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
@@ -844,6 +876,7 @@ k3d_status k3d_mesh_create(const double* punkte, int64_t n, const uint32_t* drei
     g.suchtiefe = suchtiefe;
     NCK(alloc(m, m->g_dev, 1), "alloc");
     NCK(alloc(m, m->pv_buf, size_t(3 * n)), "alloc");
+    NCK(alloc(m, m->pg_ein, size_t(n)), "alloc");
     g.pv = nullptr;
     double* p = nullptr;
     uint4 *d = nullptr, *nb = nullptr;

@@ -32,6 +32,7 @@ struct Dev {
   int32_t zx, zy, zz;
   uint32_t *anf, *ein, *cur;
   uint32_t cap;
+  uint32_t *pg_anf, *pg_ein;  // point grid on the same cells (Z + 1 starts; N entries, ascending per cell)
 };
 
 __device__ __forceinline__ D3 ld4(const double4& v) { return d3(v.x, v.y, v.z); }

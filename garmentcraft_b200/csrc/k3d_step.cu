@@ -750,6 +750,7 @@ static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int&
   if (a.mode == MODE_STEP) {
     if ((e = plain(K.integrate, a, a.n, st)) != cudaSuccess) return e;
     launched += 1;
+    if ((e = launch_koerperpunkte(a, st, launched)) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }

@@ -25,6 +25,7 @@ enum StatSlot : int {
   ST_LAST_ITERATIONS = 8,
   ST_HELD = 9,
   ST_PENETRATIONS = 10,  // segment entries through a mesh body (ImplizitStatistik::durchstoesse)
+  ST_BODY_POINTS = 11,   // triangles lifted over a body point (ImplizitStatistik::koerperpunkte)
   ST_COUNT = 16
 };
 
@@ -54,6 +55,14 @@ struct StepArgs {
   int mode, first_step, need_load, normal_aus_last;
   int cg_max, n_bodies;
   int durchstoss_pruefen, pad0;  // segment check against mesh bodies (implizit.rs:988-1002)
+  // body points against cloth triangles after integration (implizit.rs:1015-1025)
+  int kp_passes, kp_pad;
+  double kp_tief;
+  int64_t kp_nt;            // cloth triangles
+  const uint4* kp_tri;      // their points
+  double4 *kp_a, *kp_b;     // per triangle its deepest stab: (depth, normal), (weights, body point)
+  uint32_t* kp_list;        // triangles with a stab
+  unsigned* kp_ctl;         // listed stabs, corrections in this pass, stop
   double h, daempf, g[3], tol, kontakt_rand, boden;
   Body bodies[kMaxBodies];
   // points (double)
@@ -155,6 +164,8 @@ cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream
 // The FP64 PCG launch alone on the system built before (one pass, no release
 // test): dv (start and result), b, normals and the assembled A as in `a`.
 cudaError_t launch_pcg64(const StepArgs& a, int blocks, cudaStream_t stream);
+// The body-point passes after integration (none when kp_passes or kp_nt is 0).
+cudaError_t launch_koerperpunkte(const StepArgs& a, cudaStream_t stream, int& launched);
 constexpr int kMaxAdjointBodies = 14;  // bodies whose push-outs fit in rec_flags
 
 }  // namespace k3d

@@ -23,6 +23,8 @@ class ImplizitParameter:
     selbst_steifigkeit: float = 1e-3
     selbst_stoss_iterationen: int = 1
     selbst_schnitte_an_naehten: bool = False
+    koerperpunkt_durchgaenge: int = 0
+    koerperpunkt_tiefe: float = 0.01
     precision: int = _abi.K3D_FP64
 
     def to_c(self) -> _abi.K3dParams:
@@ -40,6 +42,8 @@ class ImplizitParameter:
         p.selbst_steifigkeit = self.selbst_steifigkeit
         p.selbst_stoss_iterationen = self.selbst_stoss_iterationen
         p.selbst_schnitte_an_naehten = int(self.selbst_schnitte_an_naehten)
+        p.koerperpunkt_durchgaenge = self.koerperpunkt_durchgaenge
+        p.koerperpunkt_tiefe = self.koerperpunkt_tiefe
         return p
 
 

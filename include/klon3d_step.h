@@ -58,7 +58,10 @@ typedef struct k3d_params {
   double selbst_steifigkeit;    /* default 1e-3 */
   int32_t selbst_stoss_iterationen;   /* impact response passes (implizit.rs:491), default 1 */
   int32_t selbst_schnitte_an_naehten; /* edges through their seam partners' triangles count (:494), default 0 */
-  int32_t reserved[6];
+  int32_t koerperpunkt_durchgaenge;   /* body points against cloth triangles: passes per step (implizit.rs:479), default 0 = off */
+  int32_t reserved0;
+  double koerperpunkt_tiefe;          /* m below a body point a triangle is still lifted (implizit.rs:481), default 0.01 */
+  int32_t reserved[2];
 } k3d_params;
 
 /* Simparameter (sim/src/szene.rs:96-126), the part the implicit step reads. */

@@ -196,6 +196,8 @@ ImplizitParameter param_aus(const k3d_params* p) {
   o.selbst_steifigkeit = p->selbst_steifigkeit;
   o.selbst_stoss_iterationen = size_t(std::max(p->selbst_stoss_iterationen, 0));
   o.selbst_schnitte_an_naehten = p->selbst_schnitte_an_naehten != 0;
+  o.koerperpunkt_durchgaenge = size_t(std::max(p->koerperpunkt_durchgaenge, 0));
+  o.koerperpunkt_tiefe = p->koerperpunkt_tiefe;
   return o;
 }
 
@@ -424,6 +426,7 @@ void orc_sim_frames(void* h, int32_t n, k3d_stats* st) {
     summe.haftend += b.haftend;
     summe.freigegeben += b.freigegeben;
     summe.durchstoesse += b.durchstoesse;
+    summe.koerperpunkte += b.koerperpunkte;
     summe.rest_max = std::max(summe.rest_max, b.rest_max);
     summe.naehe_punkt_dreieck += b.naehe_punkt_dreieck;
     summe.naehe_kante_kante += b.naehe_kante_kante;

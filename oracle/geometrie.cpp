@@ -186,6 +186,12 @@ std::optional<std::array<V3, 3>> Koerper::durchstoss(V3 von, V3 nach) const {
   return std::array<V3, 3>{add(r->punkt, punkt), r->normale, netz->geschwindigkeit_an(r->dreieck, r->punkt, geschwindigkeit)};
 }
 
+size_t Koerper::punkte_gegen_dreiecke(double tief, const std::vector<std::array<uint32_t, 3>>& dreiecke,
+                                      const std::vector<double>& w, std::vector<V3>& x, std::vector<V3>& v) const {
+  if (art != 2) return 0;
+  return netz->punkte_gegen_dreiecke(tief, punkt, geschwindigkeit, dreiecke, w, x, v);
+}
+
 Koerper Koerper::verschoben(double t) const {
   Koerper k = *this;
   k.punkt = add(punkt, mul(geschwindigkeit, t));

@@ -329,7 +329,7 @@ System ImplizitCg::system_bauen(Szene& s, double h, std::vector<std::optional<Fe
   return sys;
 }
 
-// implizit.rs:899-1038 (no body-point passes)
+// implizit.rs:899-1038
 void ImplizitCg::schritt(Szene& s, double h, Aufnahme* auf) {
   const size_t n = s.x.size();
   const V3 g = s.param.schwerkraft;
@@ -432,6 +432,13 @@ void ImplizitCg::schritt(Szene& s, double h, Aufnahme* auf) {
         if (auf) auf->stoss[i] |= (1u << (2 * kb)) | (vn < 0.0 ? 1u << (2 * kb + 1) : 0u);
       }
     }
+  }
+  // implizit.rs:1015-1025: body points against cloth triangles
+  for (size_t pass = 0; pass < param.koerperpunkt_durchgaenge; ++pass) {
+    size_t k = 0;
+    for (const Koerper& kb : s.koerper) k += kb.punkte_gegen_dreiecke(param.koerperpunkt_tiefe, s.dreiecke, s.w, s.x, s.v);
+    statistik.koerperpunkte += k;
+    if (k == 0) break;
   }
   // implizit.rs:1027-1037: the way x_anfang -> x, impacts between parts that
   // do not already interpenetrate, position response; held points count as

@@ -180,6 +180,25 @@ void Koerpernetz::gitter_bauen() {
       r[q] = {size_t(std::max<int64_t>(a[q], 0)), size_t(std::min<int64_t>(b[q], n - 1))};
     }
   };
+  // the point grid on the same cells (gitter_punkte, :863-879): each point in
+  // its own cell, in point order
+  punktgitter.ursprung = u;
+  punktgitter.zelle = z;
+  punktgitter.zahl = zahl;
+  punktgitter.anfang.assign(nz + 1, 0);
+  auto zelle_von = [&](size_t i) {
+    std::array<size_t, 3> k{};
+    for (int q = 0; q < 3; ++q)
+      k[q] = size_t(std::min<int64_t>(std::max<int64_t>(zellen[i][q], 0), int64_t(zahl[q]) - 1));
+    return gitter.zellnummer(k[0], k[1], k[2]);
+  };
+  for (size_t i = 0; i < punkte.size(); ++i) punktgitter.anfang[zelle_von(i) + 1] += 1;
+  for (size_t q = 0; q < nz; ++q) punktgitter.anfang[q + 1] += punktgitter.anfang[q];
+  punktgitter.eintraege.assign(punktgitter.anfang[nz], 0);
+  {
+    std::vector<uint32_t> frei(punktgitter.anfang.begin(), punktgitter.anfang.end());
+    for (size_t i = 0; i < punkte.size(); ++i) punktgitter.eintraege[frei[zelle_von(i)]++] = uint32_t(i);
+  }
   std::array<std::pair<size_t, size_t>, 3> r{};
   for (const auto& d : dreiecke) {
     spanne(d, r);
@@ -394,6 +413,86 @@ std::optional<Durchstoss> Koerpernetz::durchstoss(V3 a, V3 b) const {
   return Durchstoss{p, flaechennormale[tb], uint32_t(tb)};
 }
 
+// netzkoerper.rs:612-665 (punkte_gegen_dreiecke) with stiche (:677-735):
+// every body point whose line p + t n (n its point normal) meets a cloth
+// triangle at -tief < t < -1e-9 stabs it; per triangle the deepest stab (the
+// first of equal depth in the point grid's order) lifts the triangle, in
+// triangle order, by barycentric weight and inverse mass, and takes the
+// triangle's velocity into the body point's away.
+size_t Koerpernetz::punkte_gegen_dreiecke(double tief, V3 versatz, V3 geschwindigkeit,
+                                          const std::vector<std::array<uint32_t, 3>>& dreiecke,
+                                          const std::vector<double>& w, std::vector<V3>& x,
+                                          std::vector<V3>& v) const {
+  struct Stich {
+    bool hat = false;
+    double d = 0;
+    V3 n{}, bary{};
+    uint32_t kir = 0;
+  };
+  std::vector<Stich> tiefster(dreiecke.size());
+  const double band = -1e-9, rand = std::max(tief, band);
+  for (size_t di = 0; di < dreiecke.size(); ++di) {
+    const V3 a = x[dreiecke[di][0]], b = x[dreiecke[di][1]], c = x[dreiecke[di][2]];
+    V3 lo = a, hi = a;
+    for (const V3& q : {b, c})
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], q[k]);
+        hi[k] = std::max(hi[k], q[k]);
+      }
+    lo = sub(sub(lo, versatz), V3{rand, rand, rand});
+    hi = add(sub(hi, versatz), V3{rand, rand, rand});
+    const V3 e1 = sub(b, a), e2 = sub(c, a);
+    std::array<std::pair<size_t, size_t>, 3> r{};
+    if (!punktgitter.bereich(lo, hi, r)) continue;
+    for (size_t kz = r[2].first; kz <= r[2].second; ++kz)
+      for (size_t ky = r[1].first; ky <= r[1].second; ++ky)
+        for (size_t kx = r[0].first; kx <= r[0].second; ++kx) {
+          const size_t z = punktgitter.zellnummer(kx, ky, kz);
+          for (uint32_t e = punktgitter.anfang[z]; e < punktgitter.anfang[z + 1]; ++e) {
+            const uint32_t k = punktgitter.eintraege[e];
+            const V3 p = add(punkte[k], versatz);
+            const V3 n = punktnormale[k];
+            const V3 pv = cross(n, e2);
+            const double det = dot(e1, pv);
+            if (std::fabs(det) < 1e-18) continue;
+            const V3 tv = sub(p, a);
+            const double bu = dot(tv, pv) / det;
+            if (!(bu >= 0.0 && bu <= 1.0)) continue;
+            const V3 qv = cross(tv, e1);
+            const double bv = dot(n, qv) / det;
+            if (bv < 0.0 || bu + bv > 1.0) continue;
+            const double t = dot(e2, qv) / det;
+            if (t > -tief && t < band) {
+              Stich& s = tiefster[di];
+              if (!s.hat || -t > s.d) s = Stich{true, -t, n, V3{1.0 - bu - bv, bu, bv}, k};
+            }
+          }
+        }
+  }
+  size_t zahl = 0;
+  for (size_t di = 0; di < dreiecke.size(); ++di) {
+    const Stich& s = tiefster[di];
+    if (!s.hat) continue;
+    const auto& idx = dreiecke[di];
+    const double gew[3] = {w[idx[0]], w[idx[1]], w[idx[2]]};
+    double nenner = -0.0;
+    for (int j = 0; j < 3; ++j) nenner += s.bary[j] * s.bary[j] * gew[j];
+    if (nenner <= 0.0) continue;
+    const V3 vk = punktgeschwindigkeit.empty() ? geschwindigkeit : punktgeschwindigkeit[s.kir];
+    V3 vq{0.0, 0.0, 0.0};
+    for (int j = 0; j < 3; ++j) vq = add(vq, mul(v[idx[j]], s.bary[j]));
+    vq = sub(vq, vk);
+    const double vn = std::min(dot(vq, s.n), 0.0);
+    for (int j = 0; j < 3; ++j) {
+      const double f = s.bary[j] * gew[j] / nenner;
+      x[idx[j]] = add(x[idx[j]], mul(s.n, f * s.d));
+      v[idx[j]] = sub(v[idx[j]], mul(s.n, f * vn));
+    }
+    ++zahl;
+  }
+  return zahl;
+}
+
 // The sampled grid: node (i, j, k) at ursprung + spacing * (i, j, k); its
 // value is the signed distance of naechster_alle, clamped to [-band, band]
 // when band > 0.
@@ -518,6 +617,21 @@ void orc_netz_durchstoss(void* h, const double* a, const double* b, int64_t n, i
       if (normale) normale[3 * q + c] = r ? r->normale[c] : 0.0;
     }
   }
+}
+// punkte_gegen_dreiecke on raw cloth arrays (x, v changed in place)
+int64_t orc_netz_punkte_gegen_dreiecke(void* h, double tief, const double* versatz3, const double* geschw3,
+                                       const uint32_t* dreiecke, int64_t nd, const double* w, double* x, double* v,
+                                       int64_t n) {
+  const auto* k = static_cast<const Koerpernetz*>(h);
+  std::vector<std::array<uint32_t, 3>> d(static_cast<size_t>(nd));
+  for (int64_t t = 0; t < nd; ++t) d[size_t(t)] = {dreiecke[3 * t], dreiecke[3 * t + 1], dreiecke[3 * t + 2]};
+  std::vector<V3> xs = punkte_aus(x, n), vs = punkte_aus(v, n);
+  const std::vector<double> ws(w, w + n);
+  const size_t z = k->punkte_gegen_dreiecke(tief, {versatz3[0], versatz3[1], versatz3[2]},
+                                            {geschw3[0], geschw3[1], geschw3[2]}, d, ws, xs, vs);
+  for (int64_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) x[3 * i + a] = xs[size_t(i)][a], v[3 * i + a] = vs[size_t(i)][a];
+  return int64_t(z);
 }
 // setze_punktgeschwindigkeit: v 3 per point, or null to clear
 int32_t orc_netz_setze_geschwindigkeit(void* h, const double* v, int64_t n, char* err, int64_t err_cap) {

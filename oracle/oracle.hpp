@@ -115,6 +115,9 @@ struct Koerper {
   std::optional<Kontakt> kontakt(V3 x, double abstand) const;
   // koerper.rs:99-107: entry point, face normal, body velocity at the entry
   std::optional<std::array<V3, 3>> durchstoss(V3 von, V3 nach) const;
+  // koerper.rs:113-118: body points against cloth triangles (mesh only)
+  size_t punkte_gegen_dreiecke(double tief, const std::vector<std::array<uint32_t, 3>>& dreiecke,
+                               const std::vector<double>& w, std::vector<V3>& x, std::vector<V3>& v) const;
   Koerper verschoben(double t) const;
 };
 
@@ -150,6 +153,7 @@ struct Koerpernetz {
   std::vector<std::pair<V3, double>> kugel;
   double suchtiefe = 0;
   NetzGitter gitter;
+  NetzGitter punktgitter;  // the same cells, entries the body points (netzkoerper.rs:863-879)
   size_t randkanten = 0;
   double volumen = 0;
   std::vector<V3> punktgeschwindigkeit;  // empty: the body moves rigidly
@@ -165,6 +169,10 @@ struct Koerpernetz {
   Naechster naechster_alle(V3 x) const;
   std::optional<Durchstoss> durchstoss(V3 a, V3 b) const;
   void sdf(const int32_t dims[3], V3 ursprung, double spacing, double band, float* out) const;
+  // netzkoerper.rs:612-690
+  size_t punkte_gegen_dreiecke(double tief, V3 versatz, V3 geschwindigkeit,
+                               const std::vector<std::array<uint32_t, 3>>& dreiecke, const std::vector<double>& w,
+                               std::vector<V3>& x, std::vector<V3>& v) const;
   void gitter_bauen();
 };
 
@@ -391,6 +399,8 @@ struct ImplizitParameter {
   double selbst_steifigkeit = 1e-3;
   size_t selbst_stoss_iterationen = 1;      // implizit.rs:491, 525
   bool selbst_schnitte_an_naehten = false;  // implizit.rs:494, 526
+  size_t koerperpunkt_durchgaenge = 0;      // implizit.rs:479, 520
+  double koerperpunkt_tiefe = 0.01;         // implizit.rs:481, 521
 };
 // sim/src/implizit.rs:535-561
 struct ImplizitStatistik {

@@ -123,6 +123,8 @@ def lib():
     L.orc_netz_setze_geschwindigkeit.argtypes = [P, dp, C.c_int64, cp, C.c_int64]
     L.orc_netz_setze_geschwindigkeit.restype = C.c_int32
     L.orc_netz_geschwindigkeit_an.argtypes = [P, i32p, dp, C.c_int64, dp, dp]
+    L.orc_netz_punkte_gegen_dreiecke.argtypes = [P, C.c_double, dp, dp, u32p, C.c_int64, dp, dp, dp, C.c_int64]
+    L.orc_netz_punkte_gegen_dreiecke.restype = C.c_int64
     _lib = L
     return L
 
@@ -456,6 +458,15 @@ class Koerpernetz:
         self.L.orc_netz_geschwindigkeit_an(self.h, dr.ctypes.data_as(C.POINTER(C.c_int32)), _d(p), dr.shape[0],
                                            _d(f64(starr)), _d(out))
         return out
+
+    def punkte_gegen_dreiecke(self, tief, dreiecke, w, x, v, versatz=(0.0, 0.0, 0.0), geschwindigkeit=(0.0, 0.0, 0.0)):
+        """netzkoerper.rs:612-665 on raw cloth arrays: returns (count, x, v)."""
+        d = np.ascontiguousarray(dreiecke, dtype=np.uint32).reshape(-1, 3)
+        xs, vs = f64(x).reshape(-1, 3).copy(), f64(v).reshape(-1, 3).copy()
+        n = self.L.orc_netz_punkte_gegen_dreiecke(self.h, tief, _d(f64(versatz)), _d(f64(geschwindigkeit)),
+                                                  d.ctypes.data_as(C.POINTER(C.c_uint32)), d.shape[0],
+                                                  _d(f64(w)), _d(xs), _d(vs), xs.shape[0])
+        return int(n), xs, vs
 
     def sdf(self, dims, ursprung, spacing: float, band: float = 0.0):
         """naechster_alle at every node, clamped to +-band when band > 0;

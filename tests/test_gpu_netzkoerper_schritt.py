@@ -203,3 +203,46 @@ def test_punkteregen_auf_bewegtem_koerper(pruefen):
     for _ in range(38):
         cr.bild(r)
     assert np.max(np.linalg.norm(s.x - r.x, axis=1)) > 1e-3
+
+
+def tuch_ueber_spitze():
+    """A coarse frictionless sheet (8 x 8 points, 7 cm apart) 1 cm over the
+    reference's tetrahedron (netzkoerper.rs:1085-1090), doubled in size and
+    moved off the sheet's centre so that its tip meets a triangle's inside."""
+    from test_oracle_netzkoerper import spitze
+    p, d = spitze()
+    p = p * 2.0 + [0.01, 0.02, 0.0]
+    m, _ = synth.sheet_over_sphere(n=8, groesse_m=0.5, jitter_mm=0.0, seed=3)
+    s = build_scene(m)
+    s.x[:, 2] += 0.03 - s.x[:, 2].mean()
+    s.reibung[:] = 0.0
+    return p, d, s
+
+
+def test_koerperpunkte_wie_orakel():
+    """The body-point passes after integration (implizit.rs:1015-1025,
+    netzkoerper.rs:612-735) on the device: frame by frame from the device's
+    state, the oracle's count of lifted triangles and every point to 1e-9 m.
+    The sheet hangs on the tip; without the passes it falls past it."""
+    p, d, s0 = tuch_ueber_spitze()
+    kg, ko = Koerpernetz(p, d, 0.01), O.Koerpernetz(p, d, 0.01)
+    prm = ImplizitParameter(cg_max=100000, cg_toleranz=1e-12, koerperpunkt_durchgaenge=2)
+    s = mit_koerper(s0, kg.body())
+    o = O.OracleSim(mit_koerper(s0, ko.body()), prm.to_c())
+    cg = ImplizitCg(prm)
+    gehoben = 0
+    for f in range(30):
+        o.set_state(s.x, s.v)
+        cg.bild(s)
+        st = o.frames(1)
+        assert cg.statistik.koerperpunkte == st.koerperpunkte, f
+        xo, _ = o.state()
+        assert np.max(np.abs(s.x - xo)) <= 1e-9, f
+        gehoben += cg.statistik.koerperpunkte
+    assert gehoben > 50 and s.x[:, 2].max() > p[3, 2]
+    ohne = mit_koerper(s0, kg.body())
+    cg0 = ImplizitCg(ImplizitParameter(cg_max=100000, cg_toleranz=1e-12))
+    for _ in range(30):
+        cg0.bild(ohne)
+        assert cg0.statistik.koerperpunkte == 0
+    assert ohne.x[:, 2].max() < p[:, 2].min()

@@ -270,3 +270,41 @@ def test_punktgeschwindigkeit_laenge_geprueft_und_nachfuehren_raeumt_ab():
     z.nachfuehren(p)
     r = z.naechster([[0.16, 0.0, 0.0]], 0.05)
     assert np.array_equal(z.geschwindigkeit_an(r["dreieck"], r["punkt"], (0.5, 0.5, 0.5))[0], [0.5, 0.5, 0.5])
+
+
+# ---------------------------------------------------------------- body points against cloth triangles
+
+def spitze():
+    """A tetrahedron whose tip stands 1 cm above the cloth plane z = 0
+    (the reference's test body, netzkoerper.rs:1085-1090)."""
+    p = np.array([[-0.02, -0.02, -0.03], [0.02, -0.02, -0.03], [0.0, 0.03, -0.03], [0.0, 0.0, 0.01]])
+    d = np.array([[0, 2, 1], [0, 1, 3], [1, 2, 3], [2, 0, 3]], dtype=np.uint32)
+    return p, d
+
+
+def test_spitze_sticht_nicht_durch():
+    # netzkoerper.rs:1081-1113: the tip lies between the cloth points; one pass
+    # lifts the triangle through the tip, a second finds nothing
+    p, d = spitze()
+    k = O.Koerpernetz(p, d, 0.02)
+    x = np.array([[-0.3, -0.3, 0.0], [0.3, -0.3, 0.0], [0.0, 0.4, 0.0]])
+    v = np.tile([0.0, 0.0, -1.0], (3, 1))
+    assert np.all(k.naechster(x)["abstand"] > 0.0)
+    n, x, v = k.punkte_gegen_dreiecke(0.02, [[0, 1, 2]], np.ones(3), x, v)
+    assert n == 1
+    a, b, c = x
+    nrm = np.cross(b - a, c - a)
+    nrm /= np.linalg.norm(nrm)
+    assert abs(np.dot(a - [0.0, 0.0, 0.01], nrm)) < 1e-12
+    assert np.all(x[:, 2] > 0.0)
+    ns = k.tabellen()["punktnormale"][3]
+    e1, e2 = b - a, c - a
+    pv = np.cross(ns, e2)
+    det = np.dot(e1, pv)
+    tv = np.array([0.0, 0.0, 0.01]) - a
+    bu = np.dot(tv, pv) / det
+    bv = np.dot(ns, np.cross(tv, e1)) / det
+    vq = v[0] * (1.0 - bu - bv) + v[1] * bu + v[2] * bv
+    assert np.dot(vq, ns) >= -1e-12
+    n2, _, _ = k.punkte_gegen_dreiecke(0.02, [[0, 1, 2]], np.ones(3), x, v)
+    assert n2 == 0
