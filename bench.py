@@ -86,6 +86,7 @@ def args_():
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (material-fit) leg")
     p.add_argument("--no-garment", action="store_true", help="skip the sewn-garment leg")
     p.add_argument("--no-mesh", action="store_true", help="skip the body-mesh leg")
+    p.add_argument("--no-shapes", action="store_true", help="skip the launch-shape (tuner, graph) leg")
     p.add_argument("--batch-steps", type=int, default=5)
     return p.parse_args()
 
@@ -293,6 +294,43 @@ def mesh_leg(flush, torch):
                      "unit": UNIT, "cg_iterations_per_step": its / MESH_REPS}
     out["step_mesh_body"]["body"] = f"bumpy sphere mesh r 0.3 m, {kugel_d.shape[0]} triangles, exact query"
     out["step_grid_body"]["body"] = f"the same mesh voxelised, {'x'.join(map(str, gitter['dims']))} at 5 mm, trilinear"
+    return out
+
+
+def shapes_leg():
+    """Launch shapes picked by the tuner (garmentcraft_b200.autotune): for a
+    small drape (33x33 sheet, 5 substeps per frame), the 64-drape batch and
+    the 257x257 sheet, every candidate (CTAs of the persistent PCG launch x
+    frame replayed as a CUDA graph or launched directly) timed on the same
+    frames from the drop's start, mixed form, device time per frame with CUDA
+    events. 'default' is the full grid with direct launches."""
+    import tempfile
+    from garmentcraft_b200 import _abi, autotune, synth
+    from garmentcraft_b200.implizit import build_scene
+    from garmentcraft_b200.params import ImplizitParameter
+    from garmentcraft_b200.szene import Szene
+    m, k = synth.sheet_over_sphere(n=33, seed=3, fall_m=0.02)
+    klein = build_scene(m, [k])
+    batch = Szene.verbinden([build_scene(mm, [b]) for mm, b in synth.drape_batch(64)])
+    gross = make_scene(257)
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        for name, s, sub in (("sheet_33x33_5_substeps", klein, 5), ("batch_64_drapes", batch, 1),
+                             ("sheet_257x257", gross, 1)):
+            par = ImplizitParameter(schritte_je_bild=sub, cg_max=CG_MAX, precision=_abi.K3D_MIXED)
+            q, rec = autotune.abstimmen(s, par, bilder=3, runden=2, cache=f"{d}/t.json", neu=True)
+            voll = max(z["pcg_bloecke"] for z in rec["kandidaten"])
+            dflt = next(z for z in rec["kandidaten"] if z["pcg_bloecke"] == voll and not z["graph"])
+            steps = 3 * sub
+            out[name] = {"vertices": s.n, "substeps_per_frame": sub,
+                         "default": {"pcg_blocks": voll, "graph": False, "ms_per_frame": dflt["ms_je_bild"],
+                                     "value": s.n * sub / (dflt["ms_je_bild"] * 1e-3)},
+                         "tuned": {"pcg_blocks": q.pcg_bloecke, "graph": bool(q.graph),
+                                   "ms_per_frame": rec["ms_je_bild"],
+                                   "value": s.n * sub / (rec["ms_je_bild"] * 1e-3)},
+                         "tuned_vs_default": dflt["ms_je_bild"] / rec["ms_je_bild"],
+                         "candidates": rec["kandidaten"], "frames_timed": 3, "steps_timed": steps}
+    out["unit"] = UNIT
     return out
 
 
@@ -711,6 +749,8 @@ def main():
     line.update(extra)
     if world == 1 and not a.no_batch:
         line["batched"] = batch_leg(a.batch_steps, flush, torch)
+    if world == 1 and not a.no_shapes:
+        line["launch_shapes"] = shapes_leg()
     if world == 1 and not a.no_adjoint:
         line["adjoint"] = adjoint_leg(torch)
     if world == 1 and not a.no_garment:

@@ -49,9 +49,10 @@ class K3dParams(C.Structure):
         ("selbst_stoss_iterationen", C.c_int32),
         ("selbst_schnitte_an_naehten", C.c_int32),
         ("koerperpunkt_durchgaenge", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("pcg_bloecke", C.c_int32),
         ("koerperpunkt_tiefe", C.c_double),
-        ("reserved", C.c_int32 * 2),
+        ("graph", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

@@ -20,6 +20,7 @@ EXPORTS = [
     "k3d_last_error", "k3d_solver_name", "k3d_upload_scene", "k3d_frame", "k3d_frames_resident",
     "k3d_upload_state", "k3d_download_state", "k3d_operator", "k3d_system_for", "k3d_solve",
     "k3d_residual", "k3d_read_load", "k3d_last_frame_ms", "k3d_last_solve_ms", "k3d_kernel_launches",
+    "k3d_pcg_blocks",
     "k3d_operator_noalloc", "k3d_selfcollision_pairs", "k3d_selfcollision_hash", "k3d_selfcollision_springs",
     "k3d_adjoint_forward", "k3d_adjoint_backward",
     "k3d_mesh_create", "k3d_mesh_destroy", "k3d_mesh_last_error", "k3d_mesh_update", "k3d_mesh_get_info",
@@ -91,6 +92,8 @@ def lib():
     L.k3d_last_solve_ms.restype = C.c_double
     L.k3d_kernel_launches.argtypes = [P]
     L.k3d_kernel_launches.restype = C.c_int64
+    L.k3d_pcg_blocks.argtypes = [P]
+    L.k3d_pcg_blocks.restype = C.c_int32
     L.k3d_operator_noalloc.argtypes = [C.POINTER(_abi.K3dParams), C.POINTER(_abi.K3dScene), C.c_void_p,
                                        C.c_void_p, C.c_void_p]
     L.k3d_operator_noalloc.restype = st

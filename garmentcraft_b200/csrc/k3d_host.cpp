@@ -59,6 +59,11 @@ struct k3d_solver {
   int64_t launches = 0;
   double last_ms = 0.0, solve_ms = 0.0;
   std::vector<cudaEvent_t> sev;  // one pair per substep of a frame
+  // a frame's launches as a CUDA graph (k3d_params.graph) and the launch
+  // arguments of each substep it was captured with
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<StepArgs> gkey;
+  int64_t glaunches = 0;
   Arena arena;
   StepArgs a{};  // device pointers and constants; per-launch fields are set before each launch
   double* d_pin = nullptr;  // probe input (3N)
@@ -342,6 +347,7 @@ k3d_solver* k3d_solver_create(const k3d_params* params, int32_t device) {
   }
   h->blocks = step_grid_blocks(h->p.precision == K3D_MIXED ? 1 : 0, device);
   if (h->blocks <= 0) h->err = "cannot size the cooperative grid";
+  else if (h->p.pcg_bloecke > 0) h->blocks = std::min(h->blocks, h->p.pcg_bloecke);
   return h;
 }
 
@@ -357,6 +363,9 @@ static void release_device(k3d_solver* h) {
   h->netz_dev.clear();
   for (void* p : h->kp_mem) cudaFree(p);
   h->kp_mem.clear();
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  h->gexec = nullptr;
+  h->gkey.clear();
   h->uploaded = false;
 }
 
@@ -378,6 +387,7 @@ const char* k3d_solver_name(const k3d_solver* h) { return h ? h->name.c_str() : 
 double k3d_last_frame_ms(const k3d_solver* h) { return h ? h->last_ms : 0.0; }
 double k3d_last_solve_ms(const k3d_solver* h) { return h ? h->solve_ms : 0.0; }
 int64_t k3d_kernel_launches(const k3d_solver* h) { return h ? h->launches : 0; }
+int32_t k3d_pcg_blocks(const k3d_solver* h) { return h && h->blocks > 0 ? h->blocks : 0; }
 
 // kg = d2U/dg2 (kontinuum.rs:391-406), symmetric (00, 11, 22, 01, 02, 12)
 static void kg_host(const double* ri, double fl, double kx, double ky, double sx, double sy, double ek, double es,
@@ -961,10 +971,76 @@ static k3d_status ready(k3d_solver* h) {
   return K3D_OK;
 }
 
+// One frame of substeps as one CUDA graph: the substeps' launch arguments
+// are formed first (step_args writes host fields only); when they equal
+// those of the captured graph it is replayed, else the frame is captured
+// again and the executable graph updated (or instantiated anew).
+static k3d_status frame_graph(k3d_solver* h) {
+  const int sub = std::max(h->p.schritte_je_bild, 1);
+  const double hs = h->sim.bild_dt / double(sub);
+  const bool first0 = h->first_step;
+  std::vector<StepArgs> key(static_cast<size_t>(sub));
+  h->a.ev_solve0 = h->a.ev_solve1 = nullptr;
+  for (int k = 0; k < sub; ++k) {
+    step_args(h, MODE_STEP, double(k + 1) * hs, false);
+    key[size_t(k)] = h->a;
+    h->first_step = false;
+  }
+  h->first_step = first0;
+  bool same = h->gexec && h->gkey.size() == key.size();
+  for (size_t k = 0; same && k < key.size(); ++k)
+    same = std::memcmp(&key[k], &h->gkey[k], sizeof(StepArgs)) == 0;
+  if (!same) {
+    K3D_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t l0 = h->launches;
+    k3d_status st = K3D_OK;
+    for (int k = 0; k < sub && st == K3D_OK; ++k) st = launch(h, MODE_STEP, double(k + 1) * hs, false);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+    if (st != K3D_OK || ec != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      h->first_step = first0;
+      h->launches = l0;
+      if (st != K3D_OK) return st;
+      return cuda_fail(h, ec, "frame capture");
+    }
+    h->glaunches = h->launches - l0;
+    h->launches = l0;
+    if (h->gexec) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(h->gexec, g, &info) != cudaSuccess) {
+        (void)cudaGetLastError();
+        cudaGraphExecDestroy(h->gexec);
+        h->gexec = nullptr;
+      }
+    }
+    cudaError_t ei = cudaSuccess;
+    if (!h->gexec) ei = cudaGraphInstantiate(&h->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      h->gexec = nullptr;
+      h->gkey.clear();
+      return cuda_fail(h, ei, "frame graph instantiate");
+    }
+    h->gkey = std::move(key);
+  }
+  K3D_CUDA(h, cudaGraphLaunch(h->gexec, h->stream));
+  h->launches += h->glaunches;
+  h->first_step = false;
+  return K3D_OK;
+}
+
 // One frame of substeps on the resident state.
 static k3d_status frame_device(k3d_solver* h, size_t& ev_used) {
   const int sub = std::max(h->p.schritte_je_bild, 1);
   const double hs = h->sim.bild_dt / double(sub);
+  if (h->p.graph && !h->sc.on) {
+    k3d_status st = frame_graph(h);
+    if (st != K3D_OK) return st;
+    for (auto& b : h->bodies)
+      for (int q = 0; q < 3; ++q) b.punkt[q] += b.geschwindigkeit[q] * h->sim.bild_dt;
+    return K3D_OK;
+  }
   for (int k = 0; k < sub; ++k) {
     while (h->sev.size() < ev_used + 2) {
       cudaEvent_t e;

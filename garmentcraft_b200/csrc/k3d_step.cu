@@ -718,9 +718,21 @@ static cudaError_t plain(const void* fn, const StepArgs& a, int64_t work, cudaSt
   return cudaLaunchKernel(fn, dim3(unsigned(blocks)), dim3(kBlock), args, 0, st);
 }
 
+// The persistent launch: cooperative (every block resident at once), also
+// inside a stream capture, where it becomes a cooperative kernel node.
 static cudaError_t cooperative(const void* fn, const StepArgs& a, int blocks, cudaStream_t st) {
   void* args[] = {(void*)&a};
-  return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kSolveBlock), args, 0, st);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(blocks));
+  cfg.blockDim = dim3(kSolveBlock);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 template <typename R>

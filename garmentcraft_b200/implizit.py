@@ -269,3 +269,8 @@ class ImplizitCg:
 
     def kernel_starts(self) -> int:
         return self._L.k3d_kernel_launches(self._h)
+
+    def pcg_bloecke(self) -> int:
+        """CTAs of the persistent PCG launch (``ImplizitParameter.pcg_bloecke``,
+        capped at the most that can be resident at once)."""
+        return self._L.k3d_pcg_blocks(self._h)

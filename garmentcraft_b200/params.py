@@ -26,6 +26,8 @@ class ImplizitParameter:
     koerperpunkt_durchgaenge: int = 0
     koerperpunkt_tiefe: float = 0.01
     precision: int = _abi.K3D_FP64
+    pcg_bloecke: int = 0
+    graph: bool = False
 
     def to_c(self) -> _abi.K3dParams:
         p = _abi.K3dParams()
@@ -44,6 +46,8 @@ class ImplizitParameter:
         p.selbst_schnitte_an_naehten = int(self.selbst_schnitte_an_naehten)
         p.koerperpunkt_durchgaenge = self.koerperpunkt_durchgaenge
         p.koerperpunkt_tiefe = self.koerperpunkt_tiefe
+        p.pcg_bloecke = self.pcg_bloecke
+        p.graph = int(self.graph)
         return p
 
 

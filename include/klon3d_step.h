@@ -59,9 +59,16 @@ typedef struct k3d_params {
   int32_t selbst_stoss_iterationen;   /* impact response passes (implizit.rs:491), default 1 */
   int32_t selbst_schnitte_an_naehten; /* edges through their seam partners' triangles count (:494), default 0 */
   int32_t koerperpunkt_durchgaenge;   /* body points against cloth triangles: passes per step (implizit.rs:479), default 0 = off */
-  int32_t reserved0;
+  int32_t pcg_bloecke;                /* no reference counterpart: CTAs of the persistent PCG launch, at most one
+                                         per SM times the CTAs that fit; 0 (default) = that maximum. Fewer CTAs
+                                         make each grid barrier cheaper, which pays on small drapes */
   double koerperpunkt_tiefe;          /* m below a body point a triangle is still lifted (implizit.rs:481), default 0.01 */
-  int32_t reserved[2];
+  int32_t graph;                      /* no reference counterpart: 1 = each frame's launches are captured once as a
+                                         CUDA graph and replayed while their arguments stay the same (recaptured
+                                         when they change, e.g. a moving body); not with self-collision, whose
+                                         stage reads counts back between launches. The per-frame PCG time of
+                                         k3d_last_solve_ms stays 0 then. Default 0 */
+  int32_t reserved;
 } k3d_params;
 
 /* Simparameter (sim/src/szene.rs:96-126), the part the implicit step reads. */
@@ -313,6 +320,11 @@ double k3d_last_solve_ms(const k3d_solver* h);
 
 /* Number of device kernels the handle launched since creation. */
 int64_t k3d_kernel_launches(const k3d_solver* h);
+
+/* No reference counterpart: CTAs of the handle's persistent PCG launch
+ * (k3d_params.pcg_bloecke, capped at the most that can be resident at once);
+ * 0 when the handle has no device. */
+int32_t k3d_pcg_blocks(const k3d_solver* h);
 
 /* ---------------------------------------------------------------- adjoint
  * The reference has no differentiation; these have no counterpart in it.
