@@ -205,6 +205,7 @@ struct Sim {
   Szene s;
   Koerperdaten kd;
   ImplizitCg cg;
+  CpuReferenz xpbd;  // the XPBD cross-check on the same scene (cpu.rs)
 };
 
 void stats_aus(const ImplizitStatistik& st, k3d_stats* out) {
@@ -437,6 +438,37 @@ void orc_sim_frames(void* h, int32_t n, k3d_stats* st) {
   stats_aus(summe, st);
 }
 
+// n frames of the XPBD cross-check (CpuReferenz::bild, cpu.rs:222-245) with
+// `unterschritte` substeps each; out4 = contacts, sticking, depth sum and
+// tangential sum of the last frame (Kontaktstatistik).
+void orc_sim_xpbd_frames(void* h, int32_t n, int32_t unterschritte, double* out4) {
+  auto* sim = static_cast<Sim*>(h);
+  for (int32_t f = 0; f < n; ++f) sim->xpbd.bild(sim->s, size_t(std::max(unterschritte, 1)));
+  if (out4) {
+    out4[0] = double(sim->xpbd.statistik.kontakte);
+    out4[1] = double(sim->xpbd.statistik.haftend);
+    out4[2] = sim->xpbd.statistik.tiefe;
+    out4[3] = sim->xpbd.statistik.tangential;
+  }
+}
+
+// One distance constraint on two points (cpu.rs:251-270): korr6 is updated.
+void orc_xpbd_abstand(const double* x6, const double* delta6, double* korr6, const double* w2, double ruhe,
+                      double alpha_h2) {
+  std::vector<V3> x = {{x6[0], x6[1], x6[2]}, {x6[3], x6[4], x6[5]}};
+  std::vector<V3> d = {{delta6[0], delta6[1], delta6[2]}, {delta6[3], delta6[4], delta6[5]}};
+  std::vector<V3> k = {{korr6[0], korr6[1], korr6[2]}, {korr6[3], korr6[4], korr6[5]}};
+  std::vector<double> w = {w2[0], w2[1]};
+  xpbd_abstand(x, d, k, w, {0u, 1u}, ruhe, alpha_h2);
+  for (int i = 0; i < 2; ++i)
+    for (int c = 0; c < 3; ++c) korr6[3 * i + c] = k[size_t(i)][size_t(c)];
+}
+
+// The membrane's three XPBD constraints (kontinuum.rs:526-551) for the
+// element m12 (orc_membran_eval's layout) at p9: c3, grad27 (constraint,
+// point, axis), alpha3.
+void orc_membran_zuege(const double* m12, const double* p9, double* c3, double* grad27, double* alpha3);
+
 void orc_sim_get_state(void* h, double* x, double* v) {
   auto* sim = static_cast<Sim*>(h);
   for (size_t i = 0; i < sim->s.x.size(); ++i)
@@ -594,6 +626,15 @@ void orc_membran_eval(const double* m12, const double* p9, double* dehnung3, dou
     hessen9[a] = hs.f1[a];
     hessen9[3 + a] = hs.f2[a];
     hessen9[6 + a] = hs.w[a];
+  }
+}
+void orc_membran_zuege(const double* m12, const double* p9, double* c3, double* grad27, double* alpha3) {
+  const auto z = membran_zuege(membran_aus(m12), p3_aus(p9));
+  for (int q = 0; q < 3; ++q) {
+    c3[q] = z[size_t(q)].c;
+    alpha3[q] = z[size_t(q)].alpha;
+    for (int k = 0; k < 3; ++k)
+      for (int a = 0; a < 3; ++a) grad27[9 * q + 3 * k + a] = z[size_t(q)].grad[size_t(k)][size_t(a)];
   }
 }
 void orc_membran_mal_h(const double* m12, const double* p9, const double* d9, double* out9) {

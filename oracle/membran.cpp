@@ -1,5 +1,6 @@
 // ORACLE (test infrastructure). Restatement of the orthotropic StVK membrane
 // of sim/src/kontinuum.rs in FP64, same operation order as the reference.
+#include <limits>
 #include "oracle.hpp"
 
 namespace orc {
@@ -263,6 +264,33 @@ std::array<M3, 3> membran_diag_bloecke_aus(const Membran& m, const Hessen& h) {
     for (int c = 0; c < 3; ++c) out[k][c][c] += s;
   }
   return out;
+}
+
+// kontinuum.rs:526-551: warp strain, weft strain and the engineering shear
+// angle 2*e_ks, each with its gradient per point and its compliance
+// 1 / (k * area) (infinite when the stiffness or the area is not positive).
+std::array<Zug, 3> membran_zuege(const Membran& m, const std::array<V3, 3>& p) {
+  V3 f1, f2;
+  membran_f(m, p, f1, f2);
+  const V3 e = membran_dehnung(m, p);
+  const J3 j = jacobi_aus(m, f1, f2);
+  const Basis B = basis(m);
+  auto grad = [&](const V3& v, bool halb) {
+    std::array<V3, 3> g{};
+    for (int k = 0; k < 3; ++k)
+      for (int col = 0; col < 3; ++col) {
+        double s = 0.0;
+        for (int i = 0; i < 3; ++i) s += j[k][i][col] * v[i];
+        g[k][col] = halb ? 0.5 * s : s;
+      }
+    return g;
+  };
+  const double fl = m.flaeche;
+  auto alpha = [&](double k) {
+    return (k > 0.0 && fl > 0.0) ? 1.0 / (k * fl) : std::numeric_limits<double>::infinity();
+  };
+  return {Zug{e[0], grad(B.a, true), alpha(m.kette_n_m)}, Zug{e[1], grad(B.b, true), alpha(m.dehnung_n_m)},
+          Zug{2.0 * e[2], grad(B.c, false), alpha(m.schub_n_m)}};
 }
 
 }  // namespace orc

@@ -72,6 +72,13 @@ double membran_energie(const Membran& m, const std::array<V3, 3>& p);
 std::array<V3, 3> membran_krafte(const Membran& m, const std::array<V3, 3>& p);
 std::array<V3, 3> membran_krafte_zug(const Membran& m, const std::array<V3, 3>& p);
 Hessen membran_hessen(const Membran& m, const std::array<V3, 3>& p);
+// kontinuum.rs:526-551 (Zug): one scalar XPBD constraint of a membrane
+struct Zug {
+  double c = 0;
+  std::array<V3, 3> grad{};
+  double alpha = 0;
+};
+std::array<Zug, 3> membran_zuege(const Membran& m, const std::array<V3, 3>& p);
 std::array<V3, 3> membran_mal_h_aus(const Membran& m, const Hessen& h, const std::array<V3, 3>& d);
 std::array<M3, 3> membran_diag_bloecke_aus(const Membran& m, const Hessen& h);
 V3 psd2(double a, double b, double c);
@@ -459,5 +466,22 @@ std::vector<std::pair<double, double>> dehnung_je_dreieck(const Szene& s);
 double nahtspalt(const Szene& s);
 double mittlere_geschwindigkeit(const Szene& s);
 V3 schwerpunkt(const Szene& s);
+
+// ---------------------------------------------------------------- XPBD cross-check
+// sim/src/cpu.rs:62-245 (CpuReferenz); the device step has no XPBD form
+struct Kontaktstatistik {
+  size_t kontakte = 0, haftend = 0;
+  double tiefe = 0, tangential = 0;
+};
+void xpbd_abstand(const std::vector<V3>& x, const std::vector<V3>& delta, std::vector<V3>& korr,
+                  const std::vector<double>& w, std::array<uint32_t, 2> p, double ruhe, double alpha_h2);
+void xpbd_biegung(const std::vector<V3>& x, const std::vector<V3>& delta, std::vector<V3>& korr,
+                  const std::vector<double>& w, std::array<uint32_t, 4> p, double ruhe, double alpha_h2);
+struct CpuReferenz {
+  std::vector<V3> delta, korr, last;
+  Kontaktstatistik statistik;
+  void unterschritt(Szene& s, double h);
+  void bild(Szene& s, size_t unterschritte);
+};
 
 }  // namespace orc

@@ -74,6 +74,9 @@ def lib():
     L.orc_membran_bauen.argtypes = [dp, dp, dp, dp, dp]
     L.orc_membran_bauen.restype = C.c_int32
     L.orc_membran_eval.argtypes = [dp, dp, dp, dp, dp, dp, dp, dp]
+    L.orc_membran_zuege.argtypes = [dp, dp, dp, dp, dp]
+    L.orc_sim_xpbd_frames.argtypes = [P, C.c_int32, C.c_int32, dp]
+    L.orc_xpbd_abstand.argtypes = [dp, dp, dp, dp, C.c_double, C.c_double]
     L.orc_membran_mal_h.argtypes = [dp, dp, dp, dp]
     L.orc_membran_diag.argtypes = [dp, dp, dp]
     L.orc_psd2.argtypes = [C.c_double, C.c_double, C.c_double, dp]
@@ -179,6 +182,13 @@ class OracleSim:
         st = _abi.K3dStats()
         self.L.orc_sim_frames(self.h, n, C.byref(st))
         return st
+
+    def xpbd_frames(self, n: int = 1, unterschritte: int = 20) -> dict:
+        """n frames of the XPBD cross-check (CpuReferenz, cpu.rs:222-245) on
+        this scene; the last frame's Kontaktstatistik."""
+        out = np.zeros(4)
+        self.L.orc_sim_xpbd_frames(self.h, n, unterschritte, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return dict(kontakte=int(out[0]), haftend=int(out[1]), tiefe=out[2], tangential=out[3])
 
     def adjoint(self, n: int, gx, gv, toleranz: float = 1e-12) -> dict:
         """``n`` frames from the current state, then the adjoint back through

@@ -1,0 +1,94 @@
+"""The XPBD cross-check solver (CpuReferenz, sim/src/cpu.rs:62-245) in the
+oracle: the reference's known answers for its distance constraint
+(cpu.rs:405-413) and properties of the membrane constraints and the substep
+(free fall is exact at the rest shape; the tube rests on its cylinder)."""
+import ctypes as C
+
+import numpy as np
+
+import oracle_py as O
+from garmentcraft_b200 import synth
+from garmentcraft_b200.implizit import build_scene
+from garmentcraft_b200.params import ImplizitParameter
+from test_oracle_golden import einheit, meval
+
+D = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(C.POINTER(C.c_double))
+
+
+def test_abstand_starr():
+    # cpu.rs:405-413: alpha = 0 restores the rest length in one projection
+    x = np.array([0.0, 0.0, 0.0, 2.0, 0.0, 0.0])
+    k = np.zeros(6)
+    O.lib().orc_xpbd_abstand(D(x), D(np.zeros(6)), k.ctypes.data_as(C.POINTER(C.c_double)), D([1.0, 1.0]), 1.0, 0.0)
+    p = (x + k).reshape(2, 3)
+    assert abs(np.linalg.norm(p[1] - p[0]) - 1.0) < 1e-12
+    assert abs(p[0, 0] - 0.5) < 1e-12
+
+
+def zuege(m, p):
+    c3, g27, a3 = np.zeros(3), np.zeros(27), np.zeros(3)
+    O.lib().orc_membran_zuege(D(m), D(np.asarray(p, float).ravel()), c3.ctypes.data_as(C.POINTER(C.c_double)),
+                              g27.ctypes.data_as(C.POINTER(C.c_double)), a3.ctypes.data_as(C.POINTER(C.c_double)))
+    return c3, g27.reshape(3, 3, 3), a3
+
+
+def test_membran_zuege_gradient_und_nachgiebigkeit():
+    """kontinuum.rs:526-551: the constraints are the warp strain, the weft
+    strain and 2x the shear strain; their gradients match central
+    differences, and alpha = 1 / (k * area)."""
+    e = np.array([300.0, 120.0, 40.0])
+    m = einheit(e, [np.cos(0.3), np.sin(0.3)])
+    p = np.array([[0.01, -0.02, 0.03], [1.1, 0.05, -0.02], [0.07, 0.93, 0.1]])
+    c, g, a = zuege(m, p)
+    d = meval(m, p)["dehnung"]
+    assert np.allclose(c, [d[0], d[1], 2.0 * d[2]], rtol=0, atol=1e-15)
+    assert np.allclose(a, 1.0 / (e * 0.5), rtol=1e-12)
+    eps = 1e-7
+    for k in range(3):
+        for ax in range(3):
+            pp, pm = p.copy(), p.copy()
+            pp[k, ax] += eps
+            pm[k, ax] -= eps
+            fd = (zuege(m, pp)[0] - zuege(m, pm)[0]) / (2 * eps)
+            assert np.allclose(g[:, k, ax], fd, atol=1e-6), (k, ax)
+
+
+def test_freier_fall_exakt():
+    """At the rest shape every constraint is zero, so a sheet away from its
+    body falls as the substep's prediction alone: after N substeps of
+    length h from rest, g h^2 N (N + 1) / 2 and v = g N h."""
+    m, kugel = synth.sheet_over_sphere(n=9, seed=1, jitter_mm=0.0)
+    s = build_scene(m)
+    n = 12
+    o = O.OracleSim(s, ImplizitParameter().to_c())
+    x0, _ = o.state()
+    st = o.xpbd_frames(1, n)
+    x, v = o.state()
+    h = s.param.bild_dt / n
+    gz = s.param.schwerkraft[2]
+    assert st["kontakte"] == 0
+    assert np.allclose(x[:, 2] - x0[:, 2], gz * h * h * n * (n + 1) / 2, rtol=1e-9, atol=0)
+    assert np.allclose(x[:, :2], x0[:, :2], atol=1e-15)
+    assert np.allclose(v[:, 2], gz * n * h, rtol=1e-12)
+
+
+def test_roehre_haelt_auf_dem_zylinder():
+    """The tube on its cylinder under XPBD: contacts every substep, most of
+    them sticking, and no point inside the cylinder by more than its
+    collision distance after 10 frames."""
+    m, body = synth.tube()
+    s = build_scene(m, [body])
+    o = O.OracleSim(s, ImplizitParameter().to_c())
+    oi = O.OracleSim(s, ImplizitParameter().to_c())
+    for _ in range(10):
+        st = o.xpbd_frames(1, 20)
+        oi.frames(1)
+    x, _ = o.state()
+    xi, _ = oi.state()
+    r = np.linalg.norm(x[:, :2] - np.asarray(body["punkt"])[:2], axis=1)
+    ri = np.linalg.norm(xi[:, :2] - np.asarray(body["punkt"])[:2], axis=1)
+    assert st["kontakte"] > 0 and st["haftend"] > 0.5 * st["kontakte"]
+    assert r.min() > body["radius"] - s.kollisionsabstand.max() - 1e-4
+    # the cross-check of the implicit step (examples/vergleich.rs): both hold
+    # the tube at the cylinder's radius plus the collision distance
+    assert np.max(np.abs(r - ri)) < 1e-4
