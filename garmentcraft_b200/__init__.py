@@ -5,12 +5,12 @@ C ABI in include/klon3d_step.h; this package is the host-side mirror of the
 reference's solver API for Python callers and the tests.
 """
 from . import _abi, synth
-from ._abi import K3D_FP64, K3D_MIXED
+from ._abi import K3D_FP64, K3D_MIXED, K3D_MIXED_STORAGE
 from .params import ImplizitParameter, ImplizitStatistik
 from .szene import Szene
 
 __all__ = ["ImplizitCg", "ImplizitParameter", "ImplizitStatistik", "Szene", "build_scene", "synth",
-           "K3D_FP64", "K3D_MIXED", "CgLauf"]
+           "K3D_FP64", "K3D_MIXED", "K3D_MIXED_STORAGE", "CgLauf"]
 
 
 def __getattr__(name):

@@ -22,6 +22,7 @@ K3D_TIMEOUT = 6
 
 K3D_FP64 = 0
 K3D_MIXED = 1
+K3D_MIXED_STORAGE = 2
 
 K3D_BODY_CYLINDER = 0
 K3D_BODY_SDF_GRID = 1

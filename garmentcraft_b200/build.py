@@ -21,9 +21,10 @@ HEADERS = ["k3d_step.h", "k3d_device.cuh", "k3d_step_common.cuh", "scene_build.h
 # reference's arithmetic does: the element term of k3d_build.cu needs it, and
 # the self-collision cell indices, buckets and pairs come out bit-exact. The
 # adjoint replays the forward's contact queries and rounds the same way; the
-# body mesh's nearest-point regions and distances round as the reference's.
+# body mesh's nearest-point regions and distances round as the reference's;
+# the allocation-free operator evaluates the same element products as the build.
 EXTRA = {"k3d_build.cu": ["-fmad=false"], "k3d_selbst.cu": ["-fmad=false"], "k3d_adjoint.cu": ["-fmad=false"],
-         "k3d_netz.cu": ["-fmad=false"]}
+         "k3d_netz.cu": ["-fmad=false"], "k3d_noalloc.cu": ["-fmad=false"]}
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [

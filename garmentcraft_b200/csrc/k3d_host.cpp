@@ -45,7 +45,8 @@ struct k3d_solver {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::string err, name;
   int blocks = 0;
-  size_t rsize = 8;
+  size_t rsize = 8;  // operator records, assembled blocks, preconditioner
+  size_t vsize = 8;  // the PCG's vectors
   bool uploaded = false, first_step = true;
   int64_t n = 0, nt = 0, nb = 0, ns = 0;
   double boden = 0.0;
@@ -204,10 +205,11 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.kabst = cv.kabst = A.take<double>(N);
   a.reib = cv.reib = A.take<double>(N);
   a.frei = cv.frei = A.take<uint8_t>(N);
-  a.c = A.take<char>(8 * N * R);  // c and w per point
-  a.r = A.take<char>(3 * N * R);
-  a.z = A.take<char>(3 * N * R);
-  a.ap = A.take<char>(3 * N * R);
+  const size_t V = h->vsize;
+  a.c = A.take<char>(8 * N * V);  // c and w per point
+  a.r = A.take<char>(3 * N * V);
+  a.z = A.take<char>(3 * N * V);
+  a.ap = A.take<char>(3 * N * V);
   a.nrm = A.take<char>(3 * N * R);
   a.pinv = A.take<char>(6 * N * R);
   a.md = A.take<char>(N * R);
@@ -246,7 +248,7 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.s_dq = A.take<char>(4 * S * R);
   a.s_k = A.take<char>(S * R);
   a.sync = A.take<SyncState>(1);
-  a.partials = A.take<double>(size_t(8) * h->blocks);  // two buffers of 4 sums per block
+  a.partials = A.take<double>(size_t(kPartialsPerBlock) * h->blocks);  // reduction slots
   a.n_grp = h->n_grp;
   a.grp = cv.grp = A.take<Grp>(size_t(h->n_grp));
   a.blk_grp = cv.blk_grp = A.take<uint32_t>(size_t(h->blocks));
@@ -262,9 +264,9 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.bmat = A.take<char>(9 * nbs * R);
   a.ctr_off = cv.ctr_off = A.take<uint32_t>(nbs + 1);
   a.ctr = cv.ctr = A.take<uint32_t>(P.ctr.size());
-  a.cw2 = A.take<char>(8 * N * R);  // the second buffer of (c, w)
+  a.cw2 = A.take<char>(8 * N * V);  // the second buffer of (c, w)
   cv.m_rin64 = cv.m_kgA64 = nullptr;
-  if (R == 4) {  // FP64 operator copies for the residuals of the mixed form
+  if (V == 4) {  // FP64 operator copies for the residuals of the mixed form
     a.m_f1w64 = A.take<double4>(T);
     a.m_f2w64 = A.take<double4>(T);
     a.m_kgB64 = A.take<double4>(T);
@@ -338,14 +340,21 @@ k3d_solver* k3d_solver_create(const k3d_params* params, int32_t device) {
   else
     k3d_params_default(&h->p);
   h->device = device;
-  h->rsize = h->p.precision == K3D_MIXED ? 4 : 8;
-  h->name = h->p.precision == K3D_MIXED ? "B200 (f32/f64)" : "B200 (f64)";
+  if (h->p.precision < K3D_FP64 || h->p.precision > K3D_MIXED_STORAGE) {
+    h->err = "unknown precision";
+    return h;  // every later call reports K3D_DEVICE_ERROR
+  }
+  h->rsize = h->p.precision == K3D_FP64 ? 8 : 4;
+  h->vsize = h->p.precision == K3D_MIXED ? 4 : 8;
+  h->name = h->p.precision == K3D_MIXED           ? "B200 (f32/f64)"
+            : h->p.precision == K3D_MIXED_STORAGE ? "B200 (f32 operator/f64)"
+                                                  : "B200 (f64)";
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
     h->err = "no CUDA device available";
     return h;  // every later call reports K3D_DEVICE_ERROR
   }
-  h->blocks = step_grid_blocks(h->p.precision == K3D_MIXED ? 1 : 0, device);
+  h->blocks = step_grid_blocks(h->p.precision, device);
   if (h->blocks <= 0) h->err = "cannot size the cooperative grid";
   else if (h->p.pcg_bloecke > 0) h->blocks = std::min(h->blocks, h->p.pcg_bloecke);
   return h;
@@ -744,7 +753,7 @@ k3d_status k3d_upload_scene(k3d_solver* h, const k3d_scene* s) {
       for (int64_t i = io[k]; i < io[k + 1]; ++i) msum += s->masse[i];
       g.boden = msum * 1e-18;
       g.count = a.grp_cnt + 32 * size_t(k);
-      g.partials = a.partials + 8 * size_t(first);
+      g.partials = a.partials + size_t(kPartialsPerBlock) * size_t(first);
       for (int q = 0; q < nbk[k]; ++q) blk[first + q] = uint32_t(k);
       first += unsigned(nbk[k]);
     }
@@ -890,7 +899,7 @@ static k3d_status launch(k3d_solver* h, int mode, double t_bodies, bool need_loa
     if (es != cudaSuccess) return cuda_fail(h, es, "self-collision stage");
   }
   selbst_step_args(h->sc, a);
-  cudaError_t e = launch_step(a, h->p.precision == K3D_MIXED ? 1 : 0, h->blocks, h->stream, launched);
+  cudaError_t e = launch_step(a, h->p.precision, h->blocks, h->stream, launched);
   h->launches += launched;
   if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
   if (h->sc.on && mode == MODE_STEP) {  // cloth against cloth on the way (implizit.rs:1027-1037)

@@ -10,9 +10,15 @@
 // fixed-point accumulators with integer atomics: the total does not depend on
 // the order the corners arrive in, so the result is deterministic without the
 // per-point corner lists a handle builds at upload (those would need memory).
-// Pass 0 finds the largest corner product component M; pass 1 adds every
-// component scaled by 2^(50 - exponent(M)) (exact power-of-two scaling), so
-// the resolution is M * 2^-50 and up to 2^13 corners per point cannot overflow.
+// Pass 0 finds the largest corner product component M and counts each
+// point's corners (in the accumulators, zero then); a middle pass takes the
+// largest count K and clears the accumulators; pass 1 adds every component
+// scaled by 2^(62 - ceil(log2 K) - exponent(M)) (exact power-of-two scaling),
+// so a point's sum of at most K terms below 2^(62 - ceil(log2 K)) each cannot
+// overflow, and the resolution is M * 2^-(62 - ceil(log2 K)).
+//
+// The element products round as the handle's build kernels do (this file is
+// compiled without fused multiply-add, like k3d_build.cu).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,10 +36,14 @@ constexpr int64_t kMaxPoints = 131072;
 constexpr int kMaxDevices = 64;
 constexpr int kBlock = 256;
 // [0, 3 kMaxPoints): accumulators; [3 kMaxPoints]: bits of max |product|;
-// [3 kMaxPoints + 1]: set to 1 when an element names a point out of range.
+// [3 kMaxPoints + 1]: set to 1 when an element names a point out of range;
+// [3 kMaxPoints + 2]: set to 1 when a product or an input is not finite;
+// [3 kMaxPoints + 3]: the largest number of corners at one point.
 static __device__ __align__(256) unsigned long long g_scratch[3 * kMaxPoints + 32];
 constexpr int64_t kMaxSlot = 3 * kMaxPoints;
 constexpr int64_t kErrSlot = 3 * kMaxPoints + 1;
+constexpr int64_t kNanSlot = 3 * kMaxPoints + 2;
+constexpr int64_t kCntSlot = 3 * kMaxPoints + 3;
 
 struct Args {
   int64_t n, ne, nn, nb, nt;
@@ -55,21 +65,32 @@ struct Args {
 
 __device__ __forceinline__ D3 ldp(const double* p, uint32_t i) { return ld3(p, i); }
 
+// 2^ex scales the largest component M below 2^(62 - ceil(log2 K)), K the
+// largest corner count at one point.
 __device__ __forceinline__ int scale_exp(const unsigned long long* scratch) {
   const double m = __longlong_as_double((long long)scratch[kMaxSlot]);
   if (!(m > 0.0)) return 0;
   int ex = 0;
-  frexp(m, &ex);
-  return 50 - ex;
+  frexp(m, &ex);  // m < 2^ex
+  int lk = 0;
+  while ((1ull << lk) < scratch[kCntSlot] && lk < 62) ++lk;
+  return 62 - lk - ex;
 }
 
-// pass 0: record max |component|; pass 1: add the fixed-point component.
+// pass 0: record max |component|, count the point's corners, flag a
+// non-finite component; pass 1: add the fixed-point component.
 __device__ __forceinline__ void emit(const Args& a, int pass, int ex, uint32_t i, double vx, double vy, double vz) {
   if (pass == 0) {
+    if (!isfinite(vx) || !isfinite(vy) || !isfinite(vz)) {
+      a.scratch[kNanSlot] = 1ull;
+      return;
+    }
     const double m = fmax(fabs(vx), fmax(fabs(vy), fabs(vz)));
     if (m > 0.0) atomicMax(&a.scratch[kMaxSlot], (unsigned long long)__double_as_longlong(m));
+    atomicAdd(&a.scratch[3 * size_t(i)], 1ull);
     return;
   }
+  if (a.scratch[kNanSlot] != 0ull) return;
   atomicAdd(&a.scratch[3 * size_t(i)], (unsigned long long)llrint(ldexp(vx, ex)));
   atomicAdd(&a.scratch[3 * size_t(i) + 1], (unsigned long long)llrint(ldexp(vy, ex)));
   atomicAdd(&a.scratch[3 * size_t(i) + 2], (unsigned long long)llrint(ldexp(vz, ex)));
@@ -90,6 +111,22 @@ __global__ void zero_kernel(Args a) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.scratch[kMaxSlot] = 0ull;
     a.scratch[kErrSlot] = 0ull;
+    a.scratch[kNanSlot] = 0ull;
+    a.scratch[kCntSlot] = 0ull;
+  }
+}
+
+// Between the passes: the largest corner count, and the accumulators back to
+// zero. A non-finite p or mass is flagged here (a non-finite position makes
+// its element products non-finite, flagged in pass 0).
+__global__ void middle_kernel(Args a) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n; i += int64_t(gridDim.x) * blockDim.x) {
+    atomicMax(&a.scratch[kCntSlot], a.scratch[3 * i]);
+    a.scratch[3 * i] = 0ull;
+    a.scratch[3 * i + 1] = 0ull;
+    a.scratch[3 * i + 2] = 0ull;
+    const D3 pi = ld3(a.p, uint32_t(i));
+    if (!isfinite(pi.x) || !isfinite(pi.y) || !isfinite(pi.z) || !isfinite(a.masse[i])) a.scratch[kNanSlot] = 1ull;
   }
 }
 
@@ -187,7 +224,12 @@ __global__ void elements_kernel(Args a, int pass) {
 __global__ void finish_kernel(Args a) {
   const int ex = scale_exp(a.scratch);
   const double h2 = a.h * a.h;
+  const bool nan = a.scratch[kNanSlot] != 0ull;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n; i += int64_t(gridDim.x) * blockDim.x) {
+    if (nan) {  // as k3d_operator, whose sums carry the NaN through
+      a.out[3 * i] = a.out[3 * i + 1] = a.out[3 * i + 2] = __longlong_as_double(0x7FF8000000000000ll);
+      continue;
+    }
     const double md = a.masse[i] * (1.0 + a.h * a.c);
     const D3 pi = ld3(a.p, uint32_t(i));
     double hs[3];
@@ -222,6 +264,8 @@ extern "C" k3d_status k3d_operator_noalloc(const k3d_params* params, const k3d_s
                                            void* stream) {
   using namespace k3d::noalloc;
   if (!params || !s || !p || !out) return K3D_BAD_ARGUMENT;
+  // the proximity springs of self-collision belong to a handle's stage
+  if (params->selbstkollision != 0) return K3D_BAD_ARGUMENT;
   if (s->n_punkte < 0 || s->n_punkte > kMaxPoints) return K3D_BAD_ARGUMENT;  // scratch holds 131072 points
   if (s->n_abstand < 0 || s->n_naht < 0 || s->n_biegung < 0 || s->n_membran < 0) return K3D_BAD_ARGUMENT;
   if (s->n_punkte > 0 && (!s->x || !s->masse)) return K3D_BAD_ARGUMENT;
@@ -266,14 +310,20 @@ extern "C" k3d_status k3d_operator_noalloc(const k3d_params* params, const k3d_s
   const int64_t work = std::max<int64_t>({a.nt, a.nb, a.ne + a.nn, 1});
   const unsigned eb = unsigned(std::min<int64_t>((work + kBlock - 1) / kBlock, 148 * 16));
   const unsigned pb = unsigned(std::min<int64_t>((3 * std::max<int64_t>(a.n, 1) + kBlock - 1) / kBlock, 148 * 16));
+  // launch errors left on this thread by earlier, unrelated work are not this
+  // call's: clear them before launching
+  (void)cudaGetLastError();
   zero_kernel<<<pb, kBlock, 0, st>>>(a);
   elements_kernel<<<eb, kBlock, 0, st>>>(a, 0);
+  middle_kernel<<<pb, kBlock, 0, st>>>(a);
   elements_kernel<<<eb, kBlock, 0, st>>>(a, 1);
   finish_kernel<<<pb, kBlock, 0, st>>>(a);
   if (cudaGetLastError() != cudaSuccess) return K3D_DEVICE_ERROR;
   if (cudaStreamSynchronize(st) != cudaSuccess) return K3D_DEVICE_ERROR;
-  unsigned long long err = 0;
-  if (cudaMemcpy(&err, a.scratch + kErrSlot, sizeof(err), cudaMemcpyDeviceToHost) != cudaSuccess)
+  unsigned long long flags[2] = {0, 0};  // out of range, not finite
+  if (cudaMemcpy(flags, a.scratch + kErrSlot, sizeof(flags), cudaMemcpyDeviceToHost) != cudaSuccess)
     return K3D_DEVICE_ERROR;
-  return err ? K3D_BAD_ARGUMENT : K3D_OK;
+  if (flags[0]) return K3D_BAD_ARGUMENT;
+  if (flags[1]) return K3D_NON_FINITE;
+  return K3D_OK;
 }

@@ -404,8 +404,10 @@ cudaError_t selbst_grow_pairs(SelbstHost& H, uint32_t cap) {
   if ((e = alloc(g5R, size_t(cap) * size_t(s.rsize), H.pairs)) != cudaSuccess) return e;
   s.pr_g5R = g5R;
   if ((e = alloc(s.inc_pos, size_t(8) * cap, H.pairs)) != cudaSuccess) return e;
+  // the per-entry products are in the PCG's vector precision, which is FP64
+  // also where the operator copies are FP32 (K3D_MIXED_STORAGE)
   char* out = nullptr;
-  if ((e = alloc(out, size_t(s.cap_inc) * 4 * size_t(s.rsize), H.pairs)) != cudaSuccess) return e;
+  if ((e = alloc(out, size_t(s.cap_inc) * 4 * sizeof(double), H.pairs)) != cudaSuccess) return e;
   s.inc_out = out;
   return alloc(s.inc_ent, size_t(s.cap_inc), H.pairs);
 }

@@ -20,18 +20,10 @@
 namespace k3d {
 
 // ------------------------------------------------------------ barrier + reductions
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
 __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
   int v;
   asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
-}
-__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ uint64_t globaltimer() {
@@ -50,13 +42,12 @@ constexpr double kMixedTolFloor = 1e-6;
 // grown by kGrow (then the direction restarts).
 constexpr double kReliable = 1e-2;
 constexpr double kGrow = 1e2;
-constexpr int kMaxRed = 4;
+constexpr int kMaxRed = kRedMax;
 
 struct Shared {
   double red[kMaxRed][32];
   double res[kMaxRed];
-  unsigned epoch;  // barriers passed in this launch
-  unsigned rbuf;   // reductions done in this launch (partials buffer parity)
+  unsigned epoch;  // grid barriers passed in this launch
   int err;
   Grp g;           // this block's group (instance)
   unsigned bidx;   // this block's index within the group
@@ -68,16 +59,41 @@ struct Shared {
   for (int64_t i = (lo) + int64_t(sh.bidx) * blockDim.x + threadIdx.x; i < (hi); \
        i += int64_t(sh.g.nblk) * blockDim.x)
 
-__device__ __forceinline__ unsigned atom_add_release(unsigned* p, unsigned v) {
-  unsigned old;
-  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-  return old;
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const double* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(double* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_u64(double* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Block sum of NV values in a fixed order (warp xor tree, then the warps in
-// order); the result is in v in every thread.
+// Grid barrier with a sum of NV doubles over the group's blocks, in one
+// round trip. Each block owns one slot per value in a ring of kRing
+// generations; an empty slot holds kLeer (every bit set, written by the host
+// before the launch). Barrier e: the block writes its partials into
+// generation e % kRing (the last one with release semantics, after its other
+// writes) and empties its own slots of generation (e + 1) % kRing. Warp 0 then
+// polls every block's slots of generation e until none is empty and adds them
+// in block order (fixed per lane, then a fixed xor tree), so every block
+// holds the same bits. Emptying generation e + 1 at barrier e is safe: every
+// block read its generation-(e - 2) values before it wrote those of barrier
+// e - 1, which this block has seen. A partial that happens to carry the kLeer
+// bits (a NaN) is written as another NaN. The wait gives up after
+// kBarrierLimitNs or when another block has recorded an error; the return
+// value is false then and the caller leaves the kernel.
+constexpr unsigned long long kLeer = 0xFFFFFFFFFFFFFFFFull;
 template <int NV>
-__device__ __forceinline__ void block_sum(Shared& sh, double (&v)[NV]) {
+__device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV]) {
+  static_assert(NV >= 1 && NV <= kMaxRed, "values per barrier");
+  SyncState* s = a.sync;
+  const unsigned nb = sh.g.nblk;
+  const unsigned e = sh.epoch;
+  double* gen = sh.g.partials + size_t(e % kRing) * kMaxRed * nb;
+  double* gnext = sh.g.partials + size_t((e + 1) % kRing) * kMaxRed * nb;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < NV; ++k) {
@@ -87,100 +103,73 @@ __device__ __forceinline__ void block_sum(Shared& sh, double (&v)[NV]) {
     if (lane == 0) sh.red[k][warp] = x;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    const int nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      double t = 0.0;
-      for (int w = 0; w < nw; ++w) t += sh.red[k][w];
-      sh.res[k] = t;
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < NV; ++k) v[k] = sh.res[k];
-  __syncthreads();
-}
-
-// Grid barrier: every block adds one to a counter that starts at zero in
-// each launch; barrier k of the launch is passed when the counter reaches
-// k * gridDim.x. With NV > 0 it also sums NV doubles over the grid: each
-// block writes its partials before arriving and, once through, adds all
-// blocks' partials in block order itself, so every block holds the same
-// bits. Partials alternate between two buffers (a block can only reuse a
-// buffer after every block has passed the barrier that follows the reads).
-// The wait gives up after kBarrierLimitNs or when another block has recorded
-// an error; the return value is false then and the caller leaves the kernel.
-template <int NV>
-__device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV : 1]) {
-  SyncState* s = a.sync;
-  const unsigned buf = sh.rbuf & 1u;
-  const unsigned nb = sh.g.nblk;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if constexpr (NV > 0) {
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      double x = v[k];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-      if (lane == 0) sh.red[k][warp] = x;
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if constexpr (NV > 0) {
+  if (warp == 0) {
+    if (lane == 0) {
       const int nw = (blockDim.x + 31) >> 5;
+      unsigned long long bits[NV];
 #pragma unroll
       for (int k = 0; k < NV; ++k) {
         double t = 0.0;
         for (int w = 0; w < nw; ++w) t += sh.red[k][w];
-        sh.g.partials[(buf * kMaxRed + k) * nb + sh.bidx] = t;
+        bits[k] = (unsigned long long)__double_as_longlong(t);
+        if (bits[k] == kLeer) bits[k] = 0x7FF8000000000000ull;
+        st_relaxed_u64(gnext + size_t(k) * nb + sh.bidx, kLeer);
       }
-      sh.rbuf += 1;  // every thread read the parity at entry, before the barrier above
+#pragma unroll
+      for (int k = 0; k < NV - 1; ++k) st_relaxed_u64(gen + size_t(k) * nb + sh.bidx, bits[k]);
+      st_release_u64(gen + size_t(NV - 1) * nb + sh.bidx, bits[NV - 1]);
     }
-    const unsigned target = (sh.epoch + 1) * nb;
-    atom_add_release(sh.g.count, 1u);
+    __syncwarp();
+    double acc[NV];
     const uint64_t t0 = globaltimer();
     int err = 0;
-    // poll the counter alone; the error flag and the time limit every 16th
-    // poll (each check is another round trip behind the acquiring load)
-    for (unsigned poll = 1; int(ld_acquire_u32(sh.g.count) - target) < 0; ++poll) {
-      if ((poll & 15u) != 0u) continue;
-      if ((err = ld_relaxed_i32(&s->error)) != 0) break;
-      if (globaltimer() - t0 > kBarrierLimitNs) {
-        atomicCAS(&s->error, 0, K3D_STATUS_TIMEOUT);
-        err = K3D_STATUS_TIMEOUT;
-        break;
+    for (unsigned poll = 1;; ++poll) {
+      bool full = true;
+#pragma unroll
+      for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+      for (unsigned b = lane; b < nb; b += 32) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+          const unsigned long long u = ld_relaxed_u64(gen + size_t(k) * nb + b);
+          full = full && u != kLeer;
+          acc[k] += __longlong_as_double((long long)u);
+        }
       }
+      if (__all_sync(0xffffffffu, full)) break;
+      if ((poll & 15u) != 0u) continue;
+      // the error flag and the time limit every 16th poll
+      if (lane == 0) {
+        if ((err = ld_relaxed_i32(&s->error)) == 0 && globaltimer() - t0 > kBarrierLimitNs) {
+          atomicCAS(&s->error, 0, K3D_STATUS_TIMEOUT);
+          err = K3D_STATUS_TIMEOUT;
+        }
+      }
+      err = __shfl_sync(0xffffffffu, err, 0);
+      if (err != 0) break;
     }
-    sh.err = err;
-    sh.epoch += 1;
+    fence_acq_rel();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double x = acc[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if (lane == 0) sh.res[k] = x;
+    }
+    if (lane == 0) {
+      sh.err = err;
+      sh.epoch = e + 1;
+    }
   }
   __syncthreads();
   if (sh.err != 0) return false;
-  if constexpr (NV > 0) {
-    // warp 0 adds the block partials in block order (fixed per lane, then a
-    // fixed xor tree): every block gets the same bits
-    if (warp == 0) {
 #pragma unroll
-      for (int k = 0; k < NV; ++k) {
-        double x = 0.0;
-        for (unsigned b = lane; b < nb; b += 32) x += __ldcg(&sh.g.partials[(buf * kMaxRed + k) * nb + b]);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if (lane == 0) sh.res[k] = x;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = sh.res[k];
-  }
+  for (int k = 0; k < NV; ++k) v[k] = sh.res[k];
   return true;
 }
 
 __device__ __forceinline__ bool barrier(const StepArgs& a, Shared& sh) {
   double none[1] = {0.0};
-  return grid_sync<0>(a, sh, none);
+  return grid_sync<1>(a, sh, none);
 }
 
 
@@ -260,79 +249,117 @@ __device__ __noinline__ D3 a_dv64(const StepArgs& a, int64_t i) {
   return d3(md * d.x + h2 * x, md * d.y + h2 * y, md * d.z + h2 * z);
 }
 
-// H p at point i: the sum of its corner slots, rank by rank (coalesced over
-// consecutive points).
+// ------------------------------------------------------------ PCG vectors
+// The PCG's vectors in precision V: the (c, w) buffers, r and ap; the
+// preconditioner (symmetric 3x3 per point) and the mass term in R, the
+// operator precision. FP64 vectors filter with the FP64 contact normal.
+template <typename R, typename V>
+struct Vec {
+  CW<V>* cw;
+  V *r, *ap;
+  const R* pinv;
+  const V* nrm;
+  R* nrm_r;  // the operator-precision normal, cleared with the FP64 one on release
+  const R* md;
+  __device__ explicit Vec(const StepArgs& a)
+      : cw((CW<V>*)a.c), r((V*)a.r), ap((V*)a.ap), pinv((const R*)a.pinv),
+        nrm(sizeof(V) == 8 ? (const V*)(const void*)a.nrm_d : (const V*)a.nrm), nrm_r((R*)a.nrm),
+        md((const R*)a.md) {}
+};
 
-template <typename R>
-__device__ void dv_to_w(const StepArgs& a, const View<R>& vw, const Shared& sh) {
-  GRP_FOR(i, sh.g.r0, sh.g.r1) {
-    const D3 d = ld3(a.dv, uint32_t(i));
-    vw.cw[i].w = {R(d.x), R(d.y), R(d.z), R(0)};
-    vw.cw[i].c = {R(0), R(0), R(0), R(0)};
-  }
+template <typename R, typename V>
+__device__ __forceinline__ void pmulv(const R* P, int64_t i, V x, V y, V z, V& ox, V& oy, V& oz) {
+  const V p0 = V(P[6 * i]), p1 = V(P[6 * i + 1]), p2 = V(P[6 * i + 2]), p3 = V(P[6 * i + 3]),
+          p4 = V(P[6 * i + 4]), p5 = V(P[6 * i + 5]);
+  ox = p0 * x + p3 * y + p4 * z;
+  oy = p3 * x + p1 * y + p5 * z;
+  oz = p4 * x + p5 * y + p2 * z;
 }
 
+// w = (V) dv, c = 0: the next row product with beta = 0 applies A to dv.
+template <typename V>
+__device__ void dv_to_w(const StepArgs& a, CW<V>* cw, const Shared& sh) {
+  GRP_FOR(i, sh.g.r0, sh.g.r1) {
+    const D3 d = ld3(a.dv, uint32_t(i));
+    cw[i].w = {V(d.x), V(d.y), V(d.z), V(0)};
+    cw[i].c = {V(0), V(0), V(0), V(0)};
+  }
+}
 
 // a 4-wide record through the read-only data path
 __device__ __forceinline__ R4<float> ldg_r4(const R4<float>* p) {
   const float4 v = __ldg(reinterpret_cast<const float4*>(p));
   return R4<float>{v.x, v.y, v.z, v.w};
 }
-template <typename R, bool SC>
-__device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<R>* buf, int64_t i, R beta, R& ox, R& oy,
-                                        R& oz) {
+
+// Column indices fetched per batch of a row's blocks: the batch's indices
+// are independent loads, then the batch's gathers and blocks, so a row of 13
+// blocks waits on two chains of two loads instead of thirteen.
+constexpr int kColBatch = 8;
+
+// (A c)_i over row i of the assembled A, c = w + beta c formed at each
+// neighbour from buf. Blocks in R, vectors and sums in V.
+template <typename R, typename V, bool SC>
+__device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<V>* buf, int64_t i, V beta, V& ox, V& oy,
+                                        V& oz) {
   // blocks as (m00 m01 m02 m10), (m11 m12 m20 m21), m22: three loads a block;
   // the FP32 ones through the read-only path (the assembled A is not written
   // during a solve launch), so that they may move ahead of this loop's stores
   const R4<R>* b4 = static_cast<const R4<R>*>(a.bmat);
   const R* b1 = static_cast<const R*>(a.bmat) + 8 * a.bplane;
   const int64_t P = a.bplane;
-  R x = 0, y = 0, z = 0;
+  V x = 0, y = 0, z = 0;
   const uint32_t cnt = __ldg(&a.row_cnt[i]);
-#pragma unroll 2
-  for (uint32_t k = 0; k < cnt; ++k) {
-    const int64_t sid = int64_t(k) * a.np + i;
-    const uint32_t j = __ldg(&a.col[sid]);
-    const R4<R> pj = next_dir<R>(buf[j], beta);
-    R4<R> u, v;
-    R w;
-    if constexpr (sizeof(R) == 4) {  // measured: faster for the FP32 blocks, slower for the FP64 ones
-      u = ldg_r4(&b4[sid]), v = ldg_r4(&b4[P + sid]);
-      w = __ldg(&b1[sid]);
-    } else {
-      u = b4[sid], v = b4[P + sid];
-      w = b1[sid];
+  for (uint32_t k0 = 0; k0 < cnt; k0 += kColBatch) {
+    uint32_t js[kColBatch];
+#pragma unroll
+    for (int q = 0; q < kColBatch; ++q) js[q] = k0 + q < cnt ? __ldg(&a.col[int64_t(k0 + q) * a.np + i]) : 0u;
+#pragma unroll
+    for (int q = 0; q < kColBatch; ++q) {
+      if (k0 + q < cnt) {
+        const int64_t sid = int64_t(k0 + q) * a.np + i;
+        const R4<V> pj = next_dir<V>(buf[js[q]], beta);
+        R4<R> u, v;
+        R w;
+        if constexpr (sizeof(R) == 4) {  // measured: faster for the FP32 blocks, slower for the FP64 ones
+          u = ldg_r4(&b4[sid]), v = ldg_r4(&b4[P + sid]);
+          w = __ldg(&b1[sid]);
+        } else {
+          u = b4[sid], v = b4[P + sid];
+          w = b1[sid];
+        }
+        x += V(u.x) * pj.x + V(u.y) * pj.y + V(u.z) * pj.z;
+        y += V(u.w) * pj.x + V(v.x) * pj.y + V(v.y) * pj.z;
+        z += V(v.z) * pj.x + V(v.w) * pj.y + V(w) * pj.z;
+      }
     }
-    x += u.x * pj.x + u.y * pj.y + u.z * pj.z;
-    y += u.w * pj.x + v.x * pj.y + v.y * pj.z;
-    z += v.z * pj.x + v.w * pj.y + w * pj.z;
   }
   if (SC) {  // self-collision springs, matrix-free (h^2 is in their blocks)
     const R4<R>* bR = static_cast<const R4<R>*>(a.sc_bR);
     const R4<R>* wR = static_cast<const R4<R>*>(a.sc_wR);
     const R* g5R = static_cast<const R*>(a.sc_g5R);
-    const R4<R> pi = next_dir<R>(buf[i], beta);
+    const R4<V> pi = next_dir<V>(buf[i], beta);
     for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
       const uint32_t ent = a.sc_ent[e], q = ent >> 3, k = ent & 7u;
       const uint4 id = a.sc_idx[q];
       const R4<R> w4 = wR[q];
-      const R g[5] = {w4.x, w4.y, w4.z, w4.w, g5R[q]};
+      const V g[5] = {V(w4.x), V(w4.y), V(w4.z), V(w4.w), V(g5R[q])};
       const uint32_t ix[5] = {id.x, id.y, id.z, id.w, a.sc_x5[q]};
-      const R gk = g[k];
-      R sx = 0, sy = 0, sz = 0;
+      const V gk = g[k];
+      V sx = 0, sy = 0, sz = 0;
 #pragma unroll
       for (int r = 0; r < 5; ++r)
-        if ((gk > R(0) && g[r] < R(0)) || (gk < R(0) && g[r] > R(0))) {
-          const R om = -gk * g[r];
-          const R4<R> pr = next_dir<R>(buf[ix[r]], beta);
+        if ((gk > V(0) && g[r] < V(0)) || (gk < V(0) && g[r] > V(0))) {
+          const V om = -gk * g[r];
+          const R4<V> pr = next_dir<V>(buf[ix[r]], beta);
           sx += om * (pi.x - pr.x);
           sy += om * (pi.y - pr.y);
           sz += om * (pi.z - pr.z);
         }
       const R4<R> b0 = bR[2 * q], b1 = bR[2 * q + 1];
-      x += b0.x * sx + b0.w * sy + b1.x * sz;
-      y += b0.w * sx + b0.y * sy + b1.y * sz;
-      z += b1.x * sx + b1.y * sy + b0.z * sz;
+      x += V(b0.x) * sx + V(b0.w) * sy + V(b1.x) * sz;
+      y += V(b0.w) * sx + V(b0.y) * sy + V(b1.y) * sz;
+      z += V(b1.x) * sx + V(b1.y) * sy + V(b0.z) * sz;
     }
   }
   ox = x;
@@ -345,14 +372,15 @@ __device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<R>* buf, int
 //   points: c = w + beta c (neighbours' from one (c, w) buffer, own written to
 //           the other), ap = S A c, c.ap                            -> sum
 //   points: dv += alpha c, r -= alpha ap, z = P r, w = S z, r.z       -> sum
-// The mixed form takes its residuals (start, reliable updates) from the FP64
-// operator. Returns false on a barrier error.
-template <typename R, bool SC>
-__device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& iters, bool& unconverged,
+// The mixed form (FP32 vectors) takes its residuals (start, reliable
+// updates) from the FP64 operator. Returns false on a barrier error.
+template <typename R, typename V, bool SC>
+__device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t& iters, bool& unconverged,
                     bool& breakdown, double& rest) {
-  CW<R>* cur = static_cast<CW<R>*>(a.c);
-  CW<R>* nxt = static_cast<CW<R>*>(a.cw2);
-  const bool hi = a.m_f1w64 != nullptr;
+  constexpr bool kLow = sizeof(V) == 4;  // FP32 vectors: the recursion needs reliable updates
+  CW<V>* cur = static_cast<CW<V>*>(a.c);
+  CW<V>* nxt = static_cast<CW<V>*>(a.cw2);
+  const bool hi = kLow && a.m_f1w64 != nullptr;
   // start: pinned points 0, held points get their normal target
   GRP_FOR(i, sh.g.r0, sh.g.r1) {
     D3 d = ld3(a.dv, uint32_t(i));
@@ -366,8 +394,8 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       }
     }
     st3(a.dv, uint32_t(i), d);
-    cur[i].w = {R(d.x), R(d.y), R(d.z), R(0)};
-    cur[i].c = {R(0), R(0), R(0), R(0)};
+    cur[i].w = {V(d.x), V(d.y), V(d.z), V(0)};
+    cur[i].c = {V(0), V(0), V(0), V(0)};
   }
   if (!barrier(a, sh)) return false;
   if (hi) {
@@ -376,70 +404,70 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
   }
   double red[2] = {0.0, 0.0};
   GRP_FOR(i, sh.g.r0, sh.g.r1) {
-    R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, cx = 0, cy = 0, cz = 0;
+    V rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, cx = 0, cy = 0, cz = 0;
     if (a.frei[i]) {
       const D3 b = ld3(a.b, uint32_t(i));
       D3 ad;
       if (hi) {
         ad = a_dv64<SC>(a, i);
       } else {
-        R hx, hy, hz;
-        bsr_row<R, SC>(a, cur, i, R(0), hx, hy, hz);
+        V hx, hy, hz;
+        bsr_row<R, V, SC>(a, cur, i, V(0), hx, hy, hz);
         ad = d3(double(hx), double(hy), double(hz));
       }
       const D3 n = ld3(a.nrm_d, uint32_t(i));
       D3 rd = b - ad;
       rd = rd - n * dot(rd, n);
-      rx = R(rd.x);
-      ry = R(rd.y);
-      rz = R(rd.z);
-      R fx = R(b.x), fy = R(b.y), fz = R(b.z);
-      filt<R>(vw.nrm, i, fx, fy, fz);
-      R px, py, pz;
-      pmul<R>(vw.pinv, i, fx, fy, fz, px, py, pz);
+      rx = V(rd.x);
+      ry = V(rd.y);
+      rz = V(rd.z);
+      V fx = V(b.x), fy = V(b.y), fz = V(b.z);
+      filt<V>(vw.nrm, i, fx, fy, fz);
+      V px, py, pz;
+      pmulv<R, V>(vw.pinv, i, fx, fy, fz, px, py, pz);
       red[1] += double(fx) * double(px) + double(fy) * double(py) + double(fz) * double(pz);
-      pmul<R>(vw.pinv, i, rx, ry, rz, zx, zy, zz);
+      pmulv<R, V>(vw.pinv, i, rx, ry, rz, zx, zy, zz);
       cx = zx;
       cy = zy;
       cz = zz;
-      filt<R>(vw.nrm, i, cx, cy, cz);
+      filt<V>(vw.nrm, i, cx, cy, cz);
       red[0] += double(rx) * double(cx) + double(ry) * double(cy) + double(rz) * double(cz);
     }
     vw.r[3 * i] = rx;
     vw.r[3 * i + 1] = ry;
     vw.r[3 * i + 2] = rz;
-    nxt[i].w = {cx, cy, cz, R(0)};  // the first direction: w + 0 c
-    nxt[i].c = {R(0), R(0), R(0), R(0)};
+    nxt[i].w = {cx, cy, cz, V(0)};  // the first direction: w + 0 c
+    nxt[i].c = {V(0), V(0), V(0), V(0)};
   }
   if (!grid_sync<2>(a, sh, red)) return false;
   {
-    CW<R>* t = cur;
+    CW<V>* t = cur;
     cur = nxt;
     nxt = t;
   }
   double delta = red[0];
   const double bb = red[1];
-  const double tol = sizeof(R) == 4 ? fmax(a.tol, kMixedTolFloor) : a.tol;
+  const double tol = kLow ? fmax(a.tol, kMixedTolFloor) : a.tol;
   const double ziel = fmax(tol * tol * fmax(bb, delta), sh.g.boden);
   int64_t it = 0;
   double beta = 0.0, delta_ref = delta;
   breakdown = false;
   while (delta > ziel && it < a.cg_max) {
-    const R rb = R(beta);
-    // ca = c.Ac and, for the FP32 operator, cm = c.M(1+hc)c: the Hessian part
-    // is positive semi-definite, so c.Ac >= cm holds exactly; an FP32 product
+    const V rb = V(beta);
+    // ca = c.Ac and, for FP32 vectors, cm = c.M(1+hc)c: the Hessian part is
+    // positive semi-definite, so c.Ac >= cm holds exactly; an FP32 product
     // that falls far below it has lost the direction and the solve stops
-    // there as at a breakdown (the FP64 form keeps the reference's test only).
+    // there as at a breakdown (the other forms keep the reference's test only).
     double ca[2] = {0.0, 0.0};
 #pragma unroll 2
     GRP_FOR(i, sh.g.r0, sh.g.r1) {
-      const R4<R> ci = next_dir<R>(cur[i], rb);
+      const R4<V> ci = next_dir<V>(cur[i], rb);
       nxt[i].c = ci;
-      R ax = 0, ay = 0, az = 0;
+      V ax = 0, ay = 0, az = 0;
       if (a.frei[i]) {
-        bsr_row<R, false>(a, cur, i, rb, ax, ay, az);
-        filt<R>(vw.nrm, i, ax, ay, az);
-        if (sizeof(R) == 4) {
+        bsr_row<R, V, false>(a, cur, i, rb, ax, ay, az);
+        filt<V>(vw.nrm, i, ax, ay, az);
+        if (kLow) {
           const double m = double(vw.md[i]);
           ca[1] += m * (double(ci.x) * double(ci.x) + double(ci.y) * double(ci.y) + double(ci.z) * double(ci.z));
         }
@@ -457,48 +485,48 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       const R4<R>* bR = static_cast<const R4<R>*>(a.sc_bR);
       const R4<R>* wR = static_cast<const R4<R>*>(a.sc_wR);
       const R* g5R = static_cast<const R*>(a.sc_g5R);
-      R4<R>* out = static_cast<R4<R>*>(a.sc_out);
+      R4<V>* out = static_cast<R4<V>*>(a.sc_out);
       const int64_t nth = int64_t(sh.g.nblk) * blockDim.x;
       for (int64_t q = int64_t(sh.bidx) * blockDim.x + threadIdx.x; q < int64_t(a.sc_np); q += nth) {
         const uint4 id = a.sc_idx[q];
         const R4<R> w4 = wR[q];
-        const R g[5] = {w4.x, w4.y, w4.z, w4.w, g5R[q]};
+        const V g[5] = {V(w4.x), V(w4.y), V(w4.z), V(w4.w), V(g5R[q])};
         const uint32_t x5 = a.sc_x5[q];
         const uint32_t ix[5] = {id.x, id.y, id.z, id.w, x5};
-        R4<R> c[5];
+        R4<V> c[5];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) c[r] = next_dir<R>(cur[ix[r]], rb);
-        c[4] = x5 != 0xffffffffu ? next_dir<R>(cur[x5], rb) : R4<R>{R(0), R(0), R(0), R(0)};
+        for (int r = 0; r < 4; ++r) c[r] = next_dir<V>(cur[ix[r]], rb);
+        c[4] = x5 != 0xffffffffu ? next_dir<V>(cur[x5], rb) : R4<V>{V(0), V(0), V(0), V(0)};
         const R4<R> b0 = bR[2 * q], b1 = bR[2 * q + 1];
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
           const uint32_t e = a.sc_pos[8 * q + k];
           if (e == 0xffffffffu) continue;
-          R sx = 0, sy = 0, sz = 0;
+          V sx = 0, sy = 0, sz = 0;
 #pragma unroll
           for (int r = 0; r < 5; ++r)
-            if ((g[k] > R(0) && g[r] < R(0)) || (g[k] < R(0) && g[r] > R(0))) {
-              const R om = -g[k] * g[r];
+            if ((g[k] > V(0) && g[r] < V(0)) || (g[k] < V(0) && g[r] > V(0))) {
+              const V om = -g[k] * g[r];
               sx += om * (c[k].x - c[r].x);
               sy += om * (c[k].y - c[r].y);
               sz += om * (c[k].z - c[r].z);
             }
-          const R tx = b0.x * sx + b0.w * sy + b1.x * sz;
-          const R ty = b0.w * sx + b0.y * sy + b1.y * sz;
-          const R tz = b1.x * sx + b1.y * sy + b0.z * sz;
-          out[e] = {tx, ty, tz, R(0)};
+          const V tx = V(b0.x) * sx + V(b0.w) * sy + V(b1.x) * sz;
+          const V ty = V(b0.w) * sx + V(b0.y) * sy + V(b1.y) * sz;
+          const V tz = V(b1.x) * sx + V(b1.y) * sy + V(b0.z) * sz;
+          out[e] = {tx, ty, tz, V(0)};
           ca[0] += double(c[k].x) * double(tx) + double(c[k].y) * double(ty) + double(c[k].z) * double(tz);
         }
       }
     }
-    if (sizeof(R) == 4) {
+    if (kLow) {
       if (!grid_sync<2>(a, sh, ca)) return false;
     } else {
       double c1[1] = {ca[0]};
       if (!grid_sync<1>(a, sh, c1)) return false;
       ca[0] = c1[0];
     }
-    if (ca[0] <= DBL_MIN || !isfinite(ca[0]) || (sizeof(R) == 4 && ca[0] < 0.5 * ca[1])) {
+    if (ca[0] <= DBL_MIN || !isfinite(ca[0]) || (kLow && ca[0] < 0.5 * ca[1])) {
       breakdown = true;
       break;
     }
@@ -506,37 +534,37 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     double rzs[1] = {0.0};
 #pragma unroll 2
     GRP_FOR(i, sh.g.r0, sh.g.r1) {
-      const R4<R> ci = nxt[i].c;
+      const R4<V> ci = nxt[i].c;
       D3 d = ld3(a.dv, uint32_t(i));
       d = d + d3(double(ci.x), double(ci.y), double(ci.z)) * alpha;
       st3(a.dv, uint32_t(i), d);
-      R apx = vw.ap[3 * i], apy = vw.ap[3 * i + 1], apz = vw.ap[3 * i + 2];
+      V apx = vw.ap[3 * i], apy = vw.ap[3 * i + 1], apz = vw.ap[3 * i + 2];
       if (SC && a.frei[i]) {  // the point's proximity-spring entries, in list order
-        const R4<R>* out = static_cast<const R4<R>*>(a.sc_out);
-        R sx = 0, sy = 0, sz = 0;
+        const R4<V>* out = static_cast<const R4<V>*>(a.sc_out);
+        V sx = 0, sy = 0, sz = 0;
         for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
-          const R4<R> t = out[e];
+          const R4<V> t = out[e];
           sx += t.x;
           sy += t.y;
           sz += t.z;
         }
-        filt<R>(vw.nrm, i, sx, sy, sz);
+        filt<V>(vw.nrm, i, sx, sy, sz);
         apx += sx;
         apy += sy;
         apz += sz;
       }
-      const R rx = R(double(vw.r[3 * i]) - alpha * double(apx));
-      const R ry = R(double(vw.r[3 * i + 1]) - alpha * double(apy));
-      const R rzz = R(double(vw.r[3 * i + 2]) - alpha * double(apz));
+      const V rx = V(double(vw.r[3 * i]) - alpha * double(apx));
+      const V ry = V(double(vw.r[3 * i + 1]) - alpha * double(apy));
+      const V rzz = V(double(vw.r[3 * i + 2]) - alpha * double(apz));
       vw.r[3 * i] = rx;
       vw.r[3 * i + 1] = ry;
       vw.r[3 * i + 2] = rzz;
-      R zx, zy, zz;
-      pmul<R>(vw.pinv, i, rx, ry, rzz, zx, zy, zz);
+      V zx, zy, zz;
+      pmulv<R, V>(vw.pinv, i, rx, ry, rzz, zx, zy, zz);
       if (!a.frei[i]) zx = zy = zz = 0;
-      R wx = zx, wy = zy, wz = zz;
-      filt<R>(vw.nrm, i, wx, wy, wz);
-      nxt[i].w = {wx, wy, wz, R(0)};
+      V wx = zx, wy = zy, wz = zz;
+      filt<V>(vw.nrm, i, wx, wy, wz);
+      nxt[i].w = {wx, wy, wz, V(0)};
       rzs[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rzz) * double(zz);
     }
     if (!grid_sync<1>(a, sh, rzs)) return false;
@@ -552,25 +580,25 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
       if (!barrier(a, sh)) return false;
       double rz2[1] = {0.0};
       GRP_FOR(i, sh.g.r0, sh.g.r1) {
-        R rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, wx = 0, wy = 0, wz = 0;
+        V rx = 0, ry = 0, rz = 0, zx = 0, zy = 0, zz = 0, wx = 0, wy = 0, wz = 0;
         if (a.frei[i]) {
           const D3 n = ld3(a.nrm_d, uint32_t(i));
           D3 rd = ld3(a.b, uint32_t(i)) - a_dv64<SC>(a, i);
           rd = rd - n * dot(rd, n);
-          rx = R(rd.x);
-          ry = R(rd.y);
-          rz = R(rd.z);
-          pmul<R>(vw.pinv, i, rx, ry, rz, zx, zy, zz);
+          rx = V(rd.x);
+          ry = V(rd.y);
+          rz = V(rd.z);
+          pmulv<R, V>(vw.pinv, i, rx, ry, rz, zx, zy, zz);
           wx = zx;
           wy = zy;
           wz = zz;
-          filt<R>(vw.nrm, i, wx, wy, wz);
+          filt<V>(vw.nrm, i, wx, wy, wz);
           rz2[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rz) * double(zz);
         }
         vw.r[3 * i] = rx;
         vw.r[3 * i + 1] = ry;
         vw.r[3 * i + 2] = rz;
-        nxt[i].w = {wx, wy, wz, R(0)};
+        nxt[i].w = {wx, wy, wz, V(0)};
       }
       if (!grid_sync<1>(a, sh, rz2)) return false;
       delta = rz2[0];
@@ -579,7 +607,7 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
     }
     beta = beta_next;
     {
-      CW<R>* t = cur;
+      CW<V>* t = cur;
       cur = nxt;
       nxt = t;
     }
@@ -594,13 +622,13 @@ __device__ bool pcg(const StepArgs& a, const View<R>& vw, Shared& sh, int64_t& i
 // ------------------------------------------------------------ release pass
 // implizit.rs:924-942: normal force from the residual A dv - b along the
 // contact normal; a held point that pulls on the body is released.
-template <typename R, bool SC>
-__device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double& released, bool last) {
-  const bool hi = a.m_f1w64 != nullptr;
+template <typename R, typename V, bool SC>
+__device__ bool release(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, double& released, bool last) {
+  const bool hi = sizeof(V) == 4 && a.m_f1w64 != nullptr;
   if (hi)
     apply_dv64(a, sh);
   else
-    dv_to_w<R>(a, vw, sh);
+    dv_to_w<V>(a, vw.cw, sh);
   if (!barrier(a, sh)) return false;
   double cnt[1] = {0.0};
   GRP_FOR(i, sh.g.r0, sh.g.r1) {
@@ -611,14 +639,14 @@ __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double
     if (hi) {
       rest = a_dv64<SC>(a, i) - b;
     } else {
-      R hx, hy, hz;
-      bsr_row<R, SC>(a, vw.cw, i, R(0), hx, hy, hz);
+      V hx, hy, hz;
+      bsr_row<R, V, SC>(a, vw.cw, i, V(0), hx, hy, hz);
       rest = d3(double(hx), double(hy), double(hz)) - b;
     }
     const double fn = dot(rest, n) / a.h;
     if (fn < 0.0) {
       st3(a.nrm_d, uint32_t(i), d3(0, 0, 0));
-      vw.nrm[3 * i] = vw.nrm[3 * i + 1] = vw.nrm[3 * i + 2] = R(0);
+      vw.nrm_r[3 * i] = vw.nrm_r[3 * i + 1] = vw.nrm_r[3 * i + 2] = R(0);
       cnt[0] += 1.0;
       // released after the last solve: held in dv's constraint, free in friction
       if (last && a.rec_flags) a.rec_flags[i] |= 8u;
@@ -632,25 +660,24 @@ __device__ bool release(const StepArgs& a, const View<R>& vw, Shared& sh, double
 }
 
 
-template <typename R, bool SC>
+template <typename R, typename V, bool SC>
 __global__ void __launch_bounds__(kSolveBlock, 1) solve_kernel(const __grid_constant__ StepArgs a) {
   __shared__ Shared sh;
   if (threadIdx.x == 0) {
     sh.epoch = 0;
-    sh.rbuf = 0;
     sh.err = 0;
     sh.g = a.grp[a.blk_grp[blockIdx.x]];
     sh.bidx = blockIdx.x - sh.g.first_blk;
   }
   __syncthreads();
-  const View<R> vw(a);
+  const Vec<R, V> vw(a);
   const bool lead = sh.bidx == 0 && threadIdx.x == 0;  // one thread per group
   const bool any_held = a.stats[ST_HELD] > 0;
   int64_t iters = 0;
   bool unconv = false, brk = false;
   double rest = 0.0;
   for (int pass = 0; pass < 2; ++pass) {
-    if (!pcg<R, SC>(a, vw, sh, iters, unconv, brk, rest)) return;
+    if (!pcg<R, V, SC>(a, vw, sh, iters, unconv, brk, rest)) return;
     double dvm[1] = {0.0};
     GRP_FOR(i, sh.g.r0, sh.g.r1) {
       const D3 d = ld3(a.dv, uint32_t(i));
@@ -676,34 +703,39 @@ __global__ void __launch_bounds__(kSolveBlock, 1) solve_kernel(const __grid_cons
     if (a.mode == MODE_SOLVE) return;
     if (!any_held) break;
     double rel = 0.0;
-    if (!release<R, SC>(a, vw, sh, rel, pass == 1)) return;
+    if (!release<R, V, SC>(a, vw, sh, rel, pass == 1)) return;
     if (lead && rel > 0.0)
       atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[ST_RELEASED]), (unsigned long long)rel);
     if (rel == 0.0) break;
   }
 }
 
-// Friction and integration; counts contacts, sticking and non-finite points.
-
 // ------------------------------------------------------------ launch
-template <typename R>
+// Precision forms: 0 FP64 (R = V = double), 1 mixed (R = V = float),
+// 2 FP32 storage (R = float blocks and preconditioner, V = double vectors).
+template <typename R, typename V>
 struct Kernels {
-  static void* sv() { return (void*)solve_kernel<R, false>; }
-  static void* svf() { return (void*)solve_kernel<R, true>; }
+  static void* sv() { return (void*)solve_kernel<R, V, false>; }
+  static void* svf() { return (void*)solve_kernel<R, V, true>; }
 };
 
-static int g_solve_blocks[2] = {0, 0};
+static int g_solve_blocks[3] = {0, 0, 0};
 static int g_sms = 0;
 
+static const void* solve_fn(int precision) {
+  return precision == 0 ? Kernels<double, double>::sv()
+                        : precision == 1 ? Kernels<float, float>::sv() : Kernels<float, double>::sv();
+}
+
 int step_grid_blocks(int precision, int device) {
-  const int idx = precision == 0 ? 0 : 1;
+  const int idx = precision < 0 || precision > 2 ? 0 : precision;
   if (g_solve_blocks[idx] > 0) return g_solve_blocks[idx];
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return -1;
   g_sms = prop.multiProcessorCount;
   int per_sm = 0;
-  const void* fn = idx == 0 ? Kernels<double>::sv() : Kernels<float>::sv();
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolveBlock, 0) != cudaSuccess || per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solve_fn(idx), kSolveBlock, 0) != cudaSuccess ||
+      per_sm < 1)
     return -1;
   g_solve_blocks[idx] = prop.multiProcessorCount * per_sm;
   return g_solve_blocks[idx];
@@ -719,8 +751,11 @@ static cudaError_t plain(const void* fn, const StepArgs& a, int64_t work, cudaSt
 }
 
 // The persistent launch: cooperative (every block resident at once), also
-// inside a stream capture, where it becomes a cooperative kernel node.
+// inside a stream capture, where it becomes a cooperative kernel node. The
+// reduction slots start empty (every bit set) in each launch.
 static cudaError_t cooperative(const void* fn, const StepArgs& a, int blocks, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(a.partials, 0xFF, sizeof(double) * kPartialsPerBlock * size_t(blocks), st);
+  if (e != cudaSuccess) return e;
   void* args[] = {(void*)&a};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -735,12 +770,11 @@ static cudaError_t cooperative(const void* fn, const StepArgs& a, int blocks, cu
   return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
-template <typename R>
+template <typename R, typename V>
 static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int& launched) {
   cudaError_t e;
   const BuildKernels K = build_kernels(sizeof(R) == 8 ? 0 : 1);
   const int64_t elems = a.nt > a.nb ? (a.nt > a.ns ? a.nt : a.ns) : (a.nb > a.ns ? a.nb : a.ns);
-  if ((e = cudaMemsetAsync(a.grp_cnt, 0, sizeof(unsigned) * 32 * size_t(a.n_grp), st)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(&a.stats[ST_HELD], 0, sizeof(long long), st)) != cudaSuccess) return e;
   if ((e = plain(K.elements, a, elems, st)) != cudaSuccess) return e;
   if ((e = plain(K.points, a, a.n, st)) != cudaSuccess) return e;
@@ -756,7 +790,8 @@ static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int&
   if (a.ev_solve0 && (e = cudaEventRecord(a.ev_solve0, st)) != cudaSuccess) return e;
   if ((e = plain(K.assemble, a, a.bplane, st)) != cudaSuccess) return e;
   launched += 1;
-  if ((e = cooperative(a.sc_off ? Kernels<R>::svf() : Kernels<R>::sv(), a, blocks, st)) != cudaSuccess) return e;
+  if ((e = cooperative(a.sc_off ? Kernels<R, V>::svf() : Kernels<R, V>::sv(), a, blocks, st)) != cudaSuccess)
+    return e;
   if (a.ev_solve1 && (e = cudaEventRecord(a.ev_solve1, st)) != cudaSuccess) return e;
   launched += 1;
   if (a.mode == MODE_STEP) {
@@ -770,15 +805,16 @@ static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int&
 cudaError_t launch_pcg64(const StepArgs& a, int blocks, cudaStream_t stream) {
   StepArgs s = a;
   s.mode = MODE_SOLVE;
-  cudaError_t e = cudaMemsetAsync(s.grp_cnt, 0, sizeof(unsigned) * 32 * size_t(s.n_grp), stream);
-  if (e != cudaSuccess) return e;
-  return cooperative(Kernels<double>::sv(), s, blocks, stream);
+  return cooperative(Kernels<double, double>::sv(), s, blocks, stream);
 }
 
 cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream_t stream, int& launched) {
   launched = 0;
-  return precision == 0 ? launch_t<double>(a, blocks, stream, launched) : launch_t<float>(a, blocks, stream, launched);
+  switch (precision) {
+    case 0: return launch_t<double, double>(a, blocks, stream, launched);
+    case 1: return launch_t<float, float>(a, blocks, stream, launched);
+    default: return launch_t<float, double>(a, blocks, stream, launched);
+  }
 }
 
 }  // namespace k3d
-

@@ -31,6 +31,12 @@ enum StatSlot : int {
 
 constexpr int K3D_STATUS_TIMEOUT = 6;
 
+// Grid reductions of the PCG launch: up to kRedMax doubles per barrier, one
+// slot per value and block in a ring of kRing generations (k3d_step.cu).
+constexpr int kRedMax = 4;
+constexpr int kRing = 3;
+constexpr int kPartialsPerBlock = kRedMax * kRing;
+
 struct SyncState {
   unsigned count;  // barrier arrivals in this launch (zeroed before each launch)
   unsigned pad0[31];
@@ -46,8 +52,9 @@ struct Grp {
   int64_t t0, t1, b0, b1, s0, s1;  // membranes, bends, springs
   unsigned first_blk, nblk;
   double boden;       // convergence floor: 1e-18 of the instance's mass (implizit.rs:390-391)
-  unsigned* count;    // barrier arrivals (zeroed before each launch)
-  double* partials;   // 2 * kMaxRed per block of the group
+  unsigned* count;    // unused by the PCG launch (kept for the layout)
+  double* partials;   // kPartialsPerBlock per block of the group: [kRing][kRedMax][nblk],
+                      // every bit set before each PCG launch
 };
 
 struct StepArgs {
@@ -147,7 +154,7 @@ struct StepArgs {
   // bookkeeping
   cudaEvent_t ev_solve0, ev_solve1;  // around the PCG launch (host-side handles)
   SyncState* sync;
-  double* partials;  // kMaxRed * blocks
+  double* partials;  // kPartialsPerBlock * blocks
   long long* stats;
   double* stat_rest_max;
 };

@@ -10,7 +10,9 @@ from . import _abi
 class ImplizitParameter:
     """Settings of the implicit path, same meaning and defaults as the
     reference (implizit.rs:505-531). ``precision`` picks the device form:
-    K3D_FP64 mirrors the reference, K3D_MIXED is the FP32/FP64 form."""
+    K3D_FP64 mirrors the reference, K3D_MIXED is the FP32/FP64 form,
+    K3D_MIXED_STORAGE stores the operator and preconditioner in FP32 and runs
+    the CG vectors in FP64."""
     schritte_je_bild: int = 5
     cg_max: int = 50
     cg_toleranz: float = 1e-5

@@ -39,8 +39,12 @@ typedef enum k3d_status {
 
 /* Arithmetic of the device step. FP64 mirrors the reference CPU solver;
  * MIXED evaluates forces, Hessian products and the preconditioner in FP32 and
- * keeps dot products, CG scalars, convergence test, dv and x/v in FP64. */
-typedef enum k3d_precision { K3D_FP64 = 0, K3D_MIXED = 1 } k3d_precision;
+ * keeps dot products, CG scalars, convergence test, dv and x/v in FP64.
+ * MIXED_STORAGE stores the assembled operator blocks and the preconditioner in
+ * FP32 (half the bytes the CG streams per iteration) and keeps the CG vectors
+ * and their arithmetic in FP64: the CG then runs in FP64 on the FP32-rounded
+ * operator, with the FP64 form's iteration counts. */
+typedef enum k3d_precision { K3D_FP64 = 0, K3D_MIXED = 1, K3D_MIXED_STORAGE = 2 } k3d_precision;
 
 /* ImplizitParameter (sim/src/implizit.rs:457-531), same meaning and defaults
  * (k3d_params_default). */
@@ -361,22 +365,24 @@ k3d_status k3d_adjoint_backward(k3d_solver* h, const double* gx, const double* g
 /* ---------------------------------------------------------------- no allocation
  * k3d_operator_noalloc has no counterpart in the reference. It is A p as
  * k3d_operator computes it (FP64, the scene's positions s->x), for a caller
- * that must not allocate device memory: code that runs while a CUDA graph is
- * being captured, a host application or framework that owns the whole device
- * memory budget through its own pool and forbids cudaMalloc/cudaFree behind
- * its back, or a real-time loop that must never block in the driver's
- * allocator. No handle is needed and nothing is allocated: every pointer in
- * `s` (x, masse and the constraint arrays; v, w, bodies are not read) and `p`,
- * `out` (3 doubles per point) are DEVICE pointers owned by the caller, and the
- * only scratch is a static array of 3 MiB inside the library, present on every
- * GPU that loads it until the process exits. Limits: s->n_punkte <= 131072
- * (K3D_BAD_ARGUMENT beyond), at most 8192 element corners per point. The
- * first call on a device looks the scratch up for that device; make that
- * first call before any stream capture. Calls share the scratch, so calls
- * that overlap on the GPU (other streams, other host threads) race; the call
- * clears what it needs and synchronises `stream` (a cudaStream_t, null = the
- * legacy default stream) before it returns. An element that names a point
- * out of range is skipped and reported as K3D_BAD_ARGUMENT. */
+ * that must not allocate device memory: a host application or framework that
+ * owns the whole device memory budget through its own pool and forbids
+ * cudaMalloc/cudaFree behind its back, or a real-time loop that must never
+ * block in the driver's allocator. No handle is needed and nothing is
+ * allocated: every pointer in `s` (x, masse and the constraint arrays; v, w,
+ * bodies are not read) and `p`, `out` (3 doubles per point) are DEVICE
+ * pointers owned by the caller, and the only scratch is a static array of
+ * 3 MiB inside the library, present on every GPU that loads it until the
+ * process exits. Limits: s->n_punkte <= 131072 (K3D_BAD_ARGUMENT beyond);
+ * params->selbstkollision must be 0 (the proximity springs belong to a
+ * handle's self-collision stage; K3D_BAD_ARGUMENT otherwise). A non-finite
+ * position, mass or p gives NaN in `out` and K3D_NON_FINITE. The first call
+ * on a device looks the scratch up for that device; make that first call
+ * before any stream capture. Calls share the scratch, so calls that overlap
+ * on the GPU (other streams, other host threads) race; the call clears what
+ * it needs and synchronises `stream` (a cudaStream_t, null = the legacy
+ * default stream) before it returns. An element that names a point out of
+ * range is skipped and reported as K3D_BAD_ARGUMENT. */
 k3d_status k3d_operator_noalloc(const k3d_params* params, const k3d_scene* s, const double* p, double* out,
                                 void* stream);
 
