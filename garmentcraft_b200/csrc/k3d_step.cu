@@ -74,17 +74,17 @@ __device__ __forceinline__ void st_relaxed_u64(double* p, unsigned long long v) 
 // Grid barrier with a sum of NV doubles over the group's blocks, in one
 // round trip. Each block owns one slot per value in a ring of kRing
 // generations; an empty slot holds kLeer (every bit set, written by the host
-// before the launch). Barrier e: the block writes its partials into
-// generation e % kRing (the last one with release semantics, after its other
-// writes) and empties its own slots of generation (e + 1) % kRing. Warp 0 then
+// before the launch). Barrier e: the block empties all its kMaxRed slots of
+// generation (e + 1) % kRing and writes its partials into generation e % kRing
+// (the last one with release semantics, after its other writes). Warp 0 then
 // polls every block's slots of generation e until none is empty and adds them
-// in block order (fixed per lane, then a fixed xor tree), so every block
-// holds the same bits. Emptying generation e + 1 at barrier e is safe: every
-// block read its generation-(e - 2) values before it wrote those of barrier
-// e - 1, which this block has seen. A partial that happens to carry the kLeer
-// bits (a NaN) is written as another NaN. The wait gives up after
-// kBarrierLimitNs or when another block has recorded an error; the return
-// value is false then and the caller leaves the kernel.
+// in block order (fixed per lane, then a fixed xor tree), so every block holds
+// the same bits. Emptying generation e + 1 at barrier e is safe: every block
+// read its generation-(e - 2) values before it wrote those of barrier e - 1,
+// which this block has seen. A partial that happens to carry the kLeer bits
+// (a NaN) is written as another NaN. The wait gives up after kBarrierLimitNs
+// or when another block has recorded an error; the return value is false then
+// and the caller leaves the kernel.
 constexpr unsigned long long kLeer = 0xFFFFFFFFFFFFFFFFull;
 template <int NV>
 __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV]) {
@@ -113,8 +113,11 @@ __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV]) {
         for (int w = 0; w < nw; ++w) t += sh.red[k][w];
         bits[k] = (unsigned long long)__double_as_longlong(t);
         if (bits[k] == kLeer) bits[k] = 0x7FF8000000000000ull;
-        st_relaxed_u64(gnext + size_t(k) * nb + sh.bidx, kLeer);
       }
+      // every slot of the next generation, whatever the next barrier's NV:
+      // a slot left full would hand a stale value to a later, wider barrier
+#pragma unroll
+      for (int k = 0; k < kMaxRed; ++k) st_relaxed_u64(gnext + size_t(k) * nb + sh.bidx, kLeer);
 #pragma unroll
       for (int k = 0; k < NV - 1; ++k) st_relaxed_u64(gen + size_t(k) * nb + sh.bidx, bits[k]);
       st_release_u64(gen + size_t(NV - 1) * nb + sh.bidx, bits[NV - 1]);
