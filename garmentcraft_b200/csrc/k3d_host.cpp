@@ -266,7 +266,7 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.ctr = cv.ctr = A.take<uint32_t>(P.ctr.size());
   a.cw2 = A.take<char>(8 * N * V);  // the second buffer of (c, w)
   cv.m_rin64 = cv.m_kgA64 = nullptr;
-  if (V == 4) {  // FP64 operator copies for the residuals of the mixed form
+  if (R == 4) {  // FP64 operator records: the assembly of the FP32 blocks reads them
     a.m_f1w64 = A.take<double4>(T);
     a.m_f2w64 = A.take<double4>(T);
     a.m_kgB64 = A.take<double4>(T);
@@ -275,8 +275,8 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
     a.b_grad64 = A.take<double4>(4 * B);
     a.s_dq64 = A.take<double4>(S);
     a.s_k64 = A.take<double>(S);
-    a.slot64 = A.take<double4>(nslots);
   }
+  if (V == 4) a.slot64 = A.take<double4>(nslots);  // the FP64 residuals of the FP32-vector form
 }
 
 extern "C" {
