@@ -20,10 +20,18 @@
 namespace k3d {
 
 // ------------------------------------------------------------ barrier + reductions
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
   int v;
   asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ uint64_t globaltimer() {
@@ -47,7 +55,8 @@ constexpr int kMaxRed = kRedMax;
 struct Shared {
   double red[kMaxRed][32];
   double res[kMaxRed];
-  unsigned epoch;  // grid barriers passed in this launch
+  unsigned epoch;  // barriers passed in this launch
+  unsigned rbuf;   // reductions done in this launch (partials buffer parity)
   int err;
   Grp g;           // this block's group (instance)
   unsigned bidx;   // this block's index within the group
@@ -59,41 +68,16 @@ struct Shared {
   for (int64_t i = (lo) + int64_t(sh.bidx) * blockDim.x + threadIdx.x; i < (hi); \
        i += int64_t(sh.g.nblk) * blockDim.x)
 
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const double* p) {
-  unsigned long long v;
-  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_u64(double* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ void st_relaxed_u64(double* p, unsigned long long v) {
-  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__device__ __forceinline__ unsigned atom_add_release(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
 }
 
-// Grid barrier with a sum of NV doubles over the group's blocks, in one
-// round trip. Each block owns one slot per value in a ring of kRing
-// generations; an empty slot holds kLeer (every bit set, written by the host
-// before the launch). Barrier e: the block empties all its kMaxRed slots of
-// generation (e + 1) % kRing and writes its partials into generation e % kRing
-// (the last one with release semantics, after its other writes). Warp 0 then
-// polls every block's slots of generation e until none is empty and adds them
-// in block order (fixed per lane, then a fixed xor tree), so every block holds
-// the same bits. Emptying generation e + 1 at barrier e is safe: every block
-// read its generation-(e - 2) values before it wrote those of barrier e - 1,
-// which this block has seen. A partial that happens to carry the kLeer bits
-// (a NaN) is written as another NaN. The wait gives up after kBarrierLimitNs
-// or when another block has recorded an error; the return value is false then
-// and the caller leaves the kernel.
-constexpr unsigned long long kLeer = 0xFFFFFFFFFFFFFFFFull;
+// Block sum of NV values in a fixed order (warp xor tree, then the warps in
+// order); the result is in v in every thread.
 template <int NV>
-__device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV]) {
-  static_assert(NV >= 1 && NV <= kMaxRed, "values per barrier");
-  SyncState* s = a.sync;
-  const unsigned nb = sh.g.nblk;
-  const unsigned e = sh.epoch;
-  double* gen = sh.g.partials + size_t(e % kRing) * kMaxRed * nb;
-  double* gnext = sh.g.partials + size_t((e + 1) % kRing) * kMaxRed * nb;
+__device__ __forceinline__ void block_sum(Shared& sh, double (&v)[NV]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < NV; ++k) {
@@ -103,76 +87,100 @@ __device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV]) {
     if (lane == 0) sh.red[k][warp] = x;
   }
   __syncthreads();
-  if (warp == 0) {
-    if (lane == 0) {
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double t = 0.0;
+      for (int w = 0; w < nw; ++w) t += sh.red[k][w];
+      sh.res[k] = t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = sh.res[k];
+  __syncthreads();
+}
+
+// Grid barrier: every block adds one to a counter that starts at zero in
+// each launch; barrier k of the launch is passed when the counter reaches
+// k * gridDim.x. With NV > 0 it also sums NV doubles over the grid: each
+// block writes its partials before arriving and, once through, adds all
+// blocks' partials in block order itself, so every block holds the same
+// bits. Partials alternate between two buffers (a block can only reuse a
+// buffer after every block has passed the barrier that follows the reads).
+// The wait gives up after kBarrierLimitNs or when another block has recorded
+// an error; the return value is false then and the caller leaves the kernel.
+template <int NV>
+__device__ bool grid_sync(const StepArgs& a, Shared& sh, double (&v)[NV > 0 ? NV : 1]) {
+  SyncState* s = a.sync;
+  const unsigned buf = sh.rbuf & 1u;
+  const unsigned nb = sh.g.nblk;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if constexpr (NV > 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double x = v[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if (lane == 0) sh.red[k][warp] = x;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if constexpr (NV > 0) {
       const int nw = (blockDim.x + 31) >> 5;
-      unsigned long long bits[NV];
 #pragma unroll
       for (int k = 0; k < NV; ++k) {
         double t = 0.0;
         for (int w = 0; w < nw; ++w) t += sh.red[k][w];
-        bits[k] = (unsigned long long)__double_as_longlong(t);
-        if (bits[k] == kLeer) bits[k] = 0x7FF8000000000000ull;
+        sh.g.partials[(buf * kMaxRed + k) * nb + sh.bidx] = t;
       }
-      // every slot of the next generation, whatever the next barrier's NV:
-      // a slot left full would hand a stale value to a later, wider barrier
-#pragma unroll
-      for (int k = 0; k < kMaxRed; ++k) st_relaxed_u64(gnext + size_t(k) * nb + sh.bidx, kLeer);
-#pragma unroll
-      for (int k = 0; k < NV - 1; ++k) st_relaxed_u64(gen + size_t(k) * nb + sh.bidx, bits[k]);
-      st_release_u64(gen + size_t(NV - 1) * nb + sh.bidx, bits[NV - 1]);
+      sh.rbuf += 1;  // every thread read the parity at entry, before the barrier above
     }
-    __syncwarp();
-    double acc[NV];
+    const unsigned target = (sh.epoch + 1) * nb;
+    atom_add_release(sh.g.count, 1u);
     const uint64_t t0 = globaltimer();
     int err = 0;
-    for (unsigned poll = 1;; ++poll) {
-      bool full = true;
-#pragma unroll
-      for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-      for (unsigned b = lane; b < nb; b += 32) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-          const unsigned long long u = ld_relaxed_u64(gen + size_t(k) * nb + b);
-          full = full && u != kLeer;
-          acc[k] += __longlong_as_double((long long)u);
-        }
-      }
-      if (__all_sync(0xffffffffu, full)) break;
+    // poll the counter alone; the error flag and the time limit every 16th
+    // poll (each check is another round trip behind the acquiring load)
+    for (unsigned poll = 1; int(ld_acquire_u32(sh.g.count) - target) < 0; ++poll) {
       if ((poll & 15u) != 0u) continue;
-      // the error flag and the time limit every 16th poll
-      if (lane == 0) {
-        if ((err = ld_relaxed_i32(&s->error)) == 0 && globaltimer() - t0 > kBarrierLimitNs) {
-          atomicCAS(&s->error, 0, K3D_STATUS_TIMEOUT);
-          err = K3D_STATUS_TIMEOUT;
-        }
+      if ((err = ld_relaxed_i32(&s->error)) != 0) break;
+      if (globaltimer() - t0 > kBarrierLimitNs) {
+        atomicCAS(&s->error, 0, K3D_STATUS_TIMEOUT);
+        err = K3D_STATUS_TIMEOUT;
+        break;
       }
-      err = __shfl_sync(0xffffffffu, err, 0);
-      if (err != 0) break;
     }
-    fence_acq_rel();
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      double x = acc[k];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-      if (lane == 0) sh.res[k] = x;
-    }
-    if (lane == 0) {
-      sh.err = err;
-      sh.epoch = e + 1;
-    }
+    sh.err = err;
+    sh.epoch += 1;
   }
   __syncthreads();
   if (sh.err != 0) return false;
+  if constexpr (NV > 0) {
+    // warp 0 adds the block partials in block order (fixed per lane, then a
+    // fixed xor tree): every block gets the same bits
+    if (warp == 0) {
 #pragma unroll
-  for (int k = 0; k < NV; ++k) v[k] = sh.res[k];
+      for (int k = 0; k < NV; ++k) {
+        double x = 0.0;
+        for (unsigned b = lane; b < nb; b += 32) x += __ldcg(&sh.g.partials[(buf * kMaxRed + k) * nb + b]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sh.res[k] = x;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = sh.res[k];
+  }
   return true;
 }
 
 __device__ __forceinline__ bool barrier(const StepArgs& a, Shared& sh) {
   double none[1] = {0.0};
-  return grid_sync<1>(a, sh, none);
+  return grid_sync<0>(a, sh, none);
 }
 
 
@@ -256,16 +264,33 @@ __device__ __noinline__ D3 a_dv64(const StepArgs& a, int64_t i) {
 // The PCG's vectors in precision V: the (c, w) buffers, r and ap; the
 // preconditioner (symmetric 3x3 per point) and the mass term in R, the
 // operator precision. FP64 vectors filter with the FP64 contact normal.
+// A (c, w) buffer of the PCG: the direction c and the filtered
+// preconditioned residual w = S P^-1 r as two arrays of the points (c at the
+// buffer's start, w after it), so a gather of w alone touches w's sectors only.
+template <typename V>
+struct Dir {
+  R4<V>* c;
+  R4<V>* w;
+  __device__ Dir(void* base, int64_t n) : c(static_cast<R4<V>*>(base)), w(static_cast<R4<V>*>(base) + n) {}
+};
+// c' = w + beta c at point j (implizit.rs:421), the same helper everywhere so
+// every reader holds the same bits
+template <typename V>
+__device__ __forceinline__ R4<V> next_dir(const Dir<V>& d, int64_t j, V beta) {
+  const R4<V> c = d.c[j], w = d.w[j];
+  return {fmar(beta, c.x, w.x), fmar(beta, c.y, w.y), fmar(beta, c.z, w.z), V(0)};
+}
+
 template <typename R, typename V>
 struct Vec {
-  CW<V>* cw;
+  Dir<V> cw;
   V *r, *ap;
   const R* pinv;
   const V* nrm;
   R* nrm_r;  // the operator-precision normal, cleared with the FP64 one on release
   const R* md;
   __device__ explicit Vec(const StepArgs& a)
-      : cw((CW<V>*)a.c), r((V*)a.r), ap((V*)a.ap), pinv((const R*)a.pinv),
+      : cw(a.c, a.n), r((V*)a.r), ap((V*)a.ap), pinv((const R*)a.pinv),
         nrm(sizeof(V) == 8 ? (const V*)(const void*)a.nrm_d : (const V*)a.nrm), nrm_r((R*)a.nrm),
         md((const R*)a.md) {}
 };
@@ -281,11 +306,11 @@ __device__ __forceinline__ void pmulv(const R* P, int64_t i, V x, V y, V z, V& o
 
 // w = (V) dv, c = 0: the next row product with beta = 0 applies A to dv.
 template <typename V>
-__device__ void dv_to_w(const StepArgs& a, CW<V>* cw, const Shared& sh) {
+__device__ void dv_to_w(const StepArgs& a, const Dir<V>& cw, const Shared& sh) {
   GRP_FOR(i, sh.g.r0, sh.g.r1) {
     const D3 d = ld3(a.dv, uint32_t(i));
-    cw[i].w = {V(d.x), V(d.y), V(d.z), V(0)};
-    cw[i].c = {V(0), V(0), V(0), V(0)};
+    cw.w[i] = {V(d.x), V(d.y), V(d.z), V(0)};
+    cw.c[i] = {V(0), V(0), V(0), V(0)};
   }
 }
 
@@ -295,15 +320,11 @@ __device__ __forceinline__ R4<float> ldg_r4(const R4<float>* p) {
   return R4<float>{v.x, v.y, v.z, v.w};
 }
 
-// Column indices fetched per batch of a row's blocks: the batch's indices
-// are independent loads, then the batch's gathers and blocks, so a row of 13
-// blocks waits on two chains of two loads instead of thirteen.
-constexpr int kColBatch = 8;
-
 // (A c)_i over row i of the assembled A, c = w + beta c formed at each
-// neighbour from buf. Blocks in R, vectors and sums in V.
-template <typename R, typename V, bool SC>
-__device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<V>* buf, int64_t i, V beta, V& ox, V& oy,
+// neighbour from buf; with WONLY, (A w)_i (beta is not read). Blocks in R,
+// vectors and sums in V.
+template <typename R, typename V, bool SC, bool WONLY = false>
+__device__ __forceinline__ void bsr_row(const StepArgs& a, const Dir<V>& buf, int64_t i, V beta, V& ox, V& oy,
                                         V& oz) {
   // blocks as (m00 m01 m02 m10), (m11 m12 m20 m21), m22: three loads a block;
   // the FP32 ones through the read-only path (the assembled A is not written
@@ -313,35 +334,29 @@ __device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<V>* buf, int
   const int64_t P = a.bplane;
   V x = 0, y = 0, z = 0;
   const uint32_t cnt = __ldg(&a.row_cnt[i]);
-  for (uint32_t k0 = 0; k0 < cnt; k0 += kColBatch) {
-    uint32_t js[kColBatch];
-#pragma unroll
-    for (int q = 0; q < kColBatch; ++q) js[q] = k0 + q < cnt ? __ldg(&a.col[int64_t(k0 + q) * a.np + i]) : 0u;
-#pragma unroll
-    for (int q = 0; q < kColBatch; ++q) {
-      if (k0 + q < cnt) {
-        const int64_t sid = int64_t(k0 + q) * a.np + i;
-        const R4<V> pj = next_dir<V>(buf[js[q]], beta);
-        R4<R> u, v;
-        R w;
-        if constexpr (sizeof(R) == 4) {  // measured: faster for the FP32 blocks, slower for the FP64 ones
-          u = ldg_r4(&b4[sid]), v = ldg_r4(&b4[P + sid]);
-          w = __ldg(&b1[sid]);
-        } else {
-          u = b4[sid], v = b4[P + sid];
-          w = b1[sid];
-        }
-        x += V(u.x) * pj.x + V(u.y) * pj.y + V(u.z) * pj.z;
-        y += V(u.w) * pj.x + V(v.x) * pj.y + V(v.y) * pj.z;
-        z += V(v.z) * pj.x + V(v.w) * pj.y + V(w) * pj.z;
-      }
+#pragma unroll 2
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const int64_t sid = int64_t(k) * a.np + i;
+    const uint32_t j = __ldg(&a.col[sid]);
+    const R4<V> pj = WONLY ? buf.w[j] : next_dir<V>(buf, j, beta);
+    R4<R> u, v;
+    R w;
+    if constexpr (sizeof(R) == 4) {  // measured: faster for the FP32 blocks, slower for the FP64 ones
+      u = ldg_r4(&b4[sid]), v = ldg_r4(&b4[P + sid]);
+      w = __ldg(&b1[sid]);
+    } else {
+      u = b4[sid], v = b4[P + sid];
+      w = b1[sid];
     }
+    x += V(u.x) * pj.x + V(u.y) * pj.y + V(u.z) * pj.z;
+    y += V(u.w) * pj.x + V(v.x) * pj.y + V(v.y) * pj.z;
+    z += V(v.z) * pj.x + V(v.w) * pj.y + V(w) * pj.z;
   }
   if (SC) {  // self-collision springs, matrix-free (h^2 is in their blocks)
     const R4<R>* bR = static_cast<const R4<R>*>(a.sc_bR);
     const R4<R>* wR = static_cast<const R4<R>*>(a.sc_wR);
     const R* g5R = static_cast<const R*>(a.sc_g5R);
-    const R4<V> pi = next_dir<V>(buf[i], beta);
+    const R4<V> pi = next_dir<V>(buf, i, beta);
     for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
       const uint32_t ent = a.sc_ent[e], q = ent >> 3, k = ent & 7u;
       const uint4 id = a.sc_idx[q];
@@ -354,7 +369,7 @@ __device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<V>* buf, int
       for (int r = 0; r < 5; ++r)
         if ((gk > V(0) && g[r] < V(0)) || (gk < V(0) && g[r] > V(0))) {
           const V om = -gk * g[r];
-          const R4<V> pr = next_dir<V>(buf[ix[r]], beta);
+          const R4<V> pr = next_dir<V>(buf, ix[r], beta);
           sx += om * (pi.x - pr.x);
           sy += om * (pi.y - pr.y);
           sz += om * (pi.z - pr.z);
@@ -376,13 +391,18 @@ __device__ __forceinline__ void bsr_row(const StepArgs& a, const CW<V>* buf, int
 //           the other), ap = S A c, c.ap                            -> sum
 //   points: dv += alpha c, r -= alpha ap, z = P r, w = S z, r.z       -> sum
 // The mixed form (FP32 vectors) takes its residuals (start, reliable
-// updates) from the FP64 operator. Returns false on a barrier error.
+// updates) from the FP64 operator. With the FP32 operator the block part of
+// A c follows A c = A w + beta A c_prev: the row product gathers w alone (half
+// the bytes of c and w), and ap keeps S A c_prev between iterations. The FP64
+// form applies A to c directly, as the reference does. Returns false on a
+// barrier error.
 template <typename R, typename V, bool SC>
 __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t& iters, bool& unconverged,
                     bool& breakdown, double& rest) {
   constexpr bool kLow = sizeof(V) == 4;  // FP32 vectors: the recursion needs reliable updates
-  CW<V>* cur = static_cast<CW<V>*>(a.c);
-  CW<V>* nxt = static_cast<CW<V>*>(a.cw2);
+  constexpr bool kRec = sizeof(R) == 4;  // A c from A w and the previous A c
+  Dir<V> cur(a.c, a.n);
+  Dir<V> nxt(a.cw2, a.n);
   const bool hi = kLow && a.m_f1w64 != nullptr;
   // start: pinned points 0, held points get their normal target
   GRP_FOR(i, sh.g.r0, sh.g.r1) {
@@ -397,8 +417,8 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
       }
     }
     st3(a.dv, uint32_t(i), d);
-    cur[i].w = {V(d.x), V(d.y), V(d.z), V(0)};
-    cur[i].c = {V(0), V(0), V(0), V(0)};
+    cur.w[i] = {V(d.x), V(d.y), V(d.z), V(0)};
+    cur.c[i] = {V(0), V(0), V(0), V(0)};
   }
   if (!barrier(a, sh)) return false;
   if (hi) {
@@ -415,7 +435,7 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
         ad = a_dv64<SC>(a, i);
       } else {
         V hx, hy, hz;
-        bsr_row<R, V, SC>(a, cur, i, V(0), hx, hy, hz);
+        bsr_row<R, V, SC, true>(a, cur, i, V(0), hx, hy, hz);
         ad = d3(double(hx), double(hy), double(hz));
       }
       const D3 n = ld3(a.nrm_d, uint32_t(i));
@@ -439,12 +459,12 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
     vw.r[3 * i] = rx;
     vw.r[3 * i + 1] = ry;
     vw.r[3 * i + 2] = rz;
-    nxt[i].w = {cx, cy, cz, V(0)};  // the first direction: w + 0 c
-    nxt[i].c = {V(0), V(0), V(0), V(0)};
+    nxt.w[i] = {cx, cy, cz, V(0)};  // the first direction: w + 0 c
+    nxt.c[i] = {V(0), V(0), V(0), V(0)};
   }
   if (!grid_sync<2>(a, sh, red)) return false;
   {
-    CW<V>* t = cur;
+    const Dir<V> t = cur;
     cur = nxt;
     nxt = t;
   }
@@ -464,12 +484,22 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
     double ca[2] = {0.0, 0.0};
 #pragma unroll 2
     GRP_FOR(i, sh.g.r0, sh.g.r1) {
-      const R4<V> ci = next_dir<V>(cur[i], rb);
-      nxt[i].c = ci;
+      const R4<V> ci = next_dir<V>(cur, i, rb);
+      nxt.c[i] = ci;
       V ax = 0, ay = 0, az = 0;
       if (a.frei[i]) {
-        bsr_row<R, V, false>(a, cur, i, rb, ax, ay, az);
-        filt<V>(vw.nrm, i, ax, ay, az);
+        if (kRec) {
+          bsr_row<R, V, false, true>(a, cur, i, rb, ax, ay, az);
+          filt<V>(vw.nrm, i, ax, ay, az);
+          if (beta != 0.0) {  // + beta S A c_prev (the first direction has none)
+            ax = fmar(rb, vw.ap[3 * i], ax);
+            ay = fmar(rb, vw.ap[3 * i + 1], ay);
+            az = fmar(rb, vw.ap[3 * i + 2], az);
+          }
+        } else {
+          bsr_row<R, V, false>(a, cur, i, rb, ax, ay, az);
+          filt<V>(vw.nrm, i, ax, ay, az);
+        }
         if (kLow) {
           const double m = double(vw.md[i]);
           ca[1] += m * (double(ci.x) * double(ci.x) + double(ci.y) * double(ci.y) + double(ci.z) * double(ci.z));
@@ -498,8 +528,8 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
         const uint32_t ix[5] = {id.x, id.y, id.z, id.w, x5};
         R4<V> c[5];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) c[r] = next_dir<V>(cur[ix[r]], rb);
-        c[4] = x5 != 0xffffffffu ? next_dir<V>(cur[x5], rb) : R4<V>{V(0), V(0), V(0), V(0)};
+        for (int r = 0; r < 4; ++r) c[r] = next_dir<V>(cur, ix[r], rb);
+        c[4] = x5 != 0xffffffffu ? next_dir<V>(cur, x5, rb) : R4<V>{V(0), V(0), V(0), V(0)};
         const R4<R> b0 = bR[2 * q], b1 = bR[2 * q + 1];
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
@@ -537,7 +567,7 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
     double rzs[1] = {0.0};
 #pragma unroll 2
     GRP_FOR(i, sh.g.r0, sh.g.r1) {
-      const R4<V> ci = nxt[i].c;
+      const R4<V> ci = nxt.c[i];
       D3 d = ld3(a.dv, uint32_t(i));
       d = d + d3(double(ci.x), double(ci.y), double(ci.z)) * alpha;
       st3(a.dv, uint32_t(i), d);
@@ -567,7 +597,7 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
       if (!a.frei[i]) zx = zy = zz = 0;
       V wx = zx, wy = zy, wz = zz;
       filt<V>(vw.nrm, i, wx, wy, wz);
-      nxt[i].w = {wx, wy, wz, V(0)};
+      nxt.w[i] = {wx, wy, wz, V(0)};
       rzs[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rzz) * double(zz);
     }
     if (!grid_sync<1>(a, sh, rzs)) return false;
@@ -601,7 +631,7 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
         vw.r[3 * i] = rx;
         vw.r[3 * i + 1] = ry;
         vw.r[3 * i + 2] = rz;
-        nxt[i].w = {wx, wy, wz, V(0)};
+        nxt.w[i] = {wx, wy, wz, V(0)};
       }
       if (!grid_sync<1>(a, sh, rz2)) return false;
       delta = rz2[0];
@@ -610,7 +640,7 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
     }
     beta = beta_next;
     {
-      CW<V>* t = cur;
+      const Dir<V> t = cur;
       cur = nxt;
       nxt = t;
     }
@@ -643,7 +673,7 @@ __device__ bool release(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, doub
       rest = a_dv64<SC>(a, i) - b;
     } else {
       V hx, hy, hz;
-      bsr_row<R, V, SC>(a, vw.cw, i, V(0), hx, hy, hz);
+      bsr_row<R, V, SC, true>(a, vw.cw, i, V(0), hx, hy, hz);
       rest = d3(double(hx), double(hy), double(hz)) - b;
     }
     const double fn = dot(rest, n) / a.h;
@@ -668,6 +698,7 @@ __global__ void __launch_bounds__(kSolveBlock, 1) solve_kernel(const __grid_cons
   __shared__ Shared sh;
   if (threadIdx.x == 0) {
     sh.epoch = 0;
+    sh.rbuf = 0;
     sh.err = 0;
     sh.g = a.grp[a.blk_grp[blockIdx.x]];
     sh.bidx = blockIdx.x - sh.g.first_blk;
@@ -755,9 +786,9 @@ static cudaError_t plain(const void* fn, const StepArgs& a, int64_t work, cudaSt
 
 // The persistent launch: cooperative (every block resident at once), also
 // inside a stream capture, where it becomes a cooperative kernel node. The
-// reduction slots start empty (every bit set) in each launch.
+// groups' barrier counters start at zero in each launch.
 static cudaError_t cooperative(const void* fn, const StepArgs& a, int blocks, cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(a.partials, 0xFF, sizeof(double) * kPartialsPerBlock * size_t(blocks), st);
+  cudaError_t e = cudaMemsetAsync(a.grp_cnt, 0, sizeof(unsigned) * 32 * size_t(a.n_grp), st);
   if (e != cudaSuccess) return e;
   void* args[] = {(void*)&a};
   cudaLaunchAttribute attr[1];

@@ -31,11 +31,10 @@ enum StatSlot : int {
 
 constexpr int K3D_STATUS_TIMEOUT = 6;
 
-// Grid reductions of the PCG launch: up to kRedMax doubles per barrier, one
-// slot per value and block in a ring of kRing generations (k3d_step.cu).
+// Grid reductions of the PCG launch: up to kRedMax doubles per barrier, the
+// block partials double-buffered (k3d_step.cu).
 constexpr int kRedMax = 4;
-constexpr int kRing = 3;
-constexpr int kPartialsPerBlock = kRedMax * kRing;
+constexpr int kPartialsPerBlock = 2 * kRedMax;
 
 struct SyncState {
   unsigned count;  // barrier arrivals in this launch (zeroed before each launch)
@@ -52,9 +51,8 @@ struct Grp {
   int64_t t0, t1, b0, b1, s0, s1;  // membranes, bends, springs
   unsigned first_blk, nblk;
   double boden;       // convergence floor: 1e-18 of the instance's mass (implizit.rs:390-391)
-  unsigned* count;    // unused by the PCG launch (kept for the layout)
-  double* partials;   // kPartialsPerBlock per block of the group: [kRing][kRedMax][nblk],
-                      // every bit set before each PCG launch
+  unsigned* count;    // barrier arrivals (zeroed before each launch)
+  double* partials;   // kPartialsPerBlock per block of the group
 };
 
 struct StepArgs {
