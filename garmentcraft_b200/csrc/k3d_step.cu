@@ -385,6 +385,63 @@ __device__ __forceinline__ void bsr_row(const StepArgs& a, const Dir<V>& buf, in
   oz = z;
 }
 
+// Rows a thread takes together in the CG iteration's two point passes. A
+// thread with more than one row (the grid has fewer threads than points)
+// issues the rows' loads before any of their stores: its stores may alias
+// the next row's loads as far as the compiler knows, so a row at a time
+// would wait for each row's chain of loads in turn.
+constexpr int kRows = 2;
+
+// (A c)_i (or (A w)_i with WONLY) for the rows ii[q] with on[q], in one loop
+// over the block ranks; the result is zero where !on[q].
+template <typename R, typename V, bool WONLY, int RW>
+__device__ __forceinline__ void bsr_rows(const StepArgs& a, const Dir<V>& buf, const int64_t (&ii)[RW],
+                                         const bool (&on)[RW], V beta, V (&ox)[RW], V (&oy)[RW], V (&oz)[RW]) {
+  const R4<R>* b4 = static_cast<const R4<R>*>(a.bmat);
+  const R* b1 = static_cast<const R*>(a.bmat) + 8 * a.bplane;
+  const int64_t P = a.bplane;
+  uint32_t cnt[RW];
+  uint32_t cmax = 0;
+#pragma unroll
+  for (int q = 0; q < RW; ++q) {
+    cnt[q] = on[q] ? __ldg(&a.row_cnt[ii[q]]) : 0u;
+    cmax = cnt[q] > cmax ? cnt[q] : cmax;
+    ox[q] = oy[q] = oz[q] = V(0);
+  }
+#pragma unroll 2
+  for (uint32_t k = 0; k < cmax; ++k) {
+#pragma unroll
+    for (int q = 0; q < RW; ++q) {
+      if (k < cnt[q]) {
+        const int64_t sid = int64_t(k) * a.np + ii[q];
+        const uint32_t j = __ldg(&a.col[sid]);
+        const R4<V> pj = WONLY ? buf.w[j] : next_dir<V>(buf, j, beta);
+        R4<R> u, v;
+        R w;
+        if constexpr (sizeof(R) == 4) {
+          u = ldg_r4(&b4[sid]), v = ldg_r4(&b4[P + sid]);
+          w = __ldg(&b1[sid]);
+        } else {
+          u = b4[sid], v = b4[P + sid];
+          w = b1[sid];
+        }
+        ox[q] += V(u.x) * pj.x + V(u.y) * pj.y + V(u.z) * pj.z;
+        oy[q] += V(u.w) * pj.x + V(v.x) * pj.y + V(v.y) * pj.z;
+        oz[q] += V(v.z) * pj.x + V(v.w) * pj.y + V(w) * pj.z;
+      }
+    }
+  }
+}
+
+// x -= n (n.x): the contact filter S with the normal given by value
+template <typename V>
+__device__ __forceinline__ void filt3(const V (&n)[3], V& x, V& y, V& z) {
+  const V d = x * n[0] + y * n[1] + z * n[2];
+  x -= n[0] * d;
+  y -= n[1] * d;
+  z -= n[2] * d;
+}
+
 // ------------------------------------------------------------ PCG
 // implizit.rs:370-426 with the assembled A, two grid syncs per iteration:
 //   points: c = w + beta c (neighbours' from one (c, w) buffer, own written to
@@ -482,33 +539,49 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
     // that falls far below it has lost the direction and the solve stops
     // there as at a breakdown (the other forms keep the reference's test only).
     double ca[2] = {0.0, 0.0};
-#pragma unroll 2
-    GRP_FOR(i, sh.g.r0, sh.g.r1) {
-      const R4<V> ci = next_dir<V>(cur, i, rb);
-      nxt.c[i] = ci;
-      V ax = 0, ay = 0, az = 0;
-      if (a.frei[i]) {
-        if (kRec) {
-          bsr_row<R, V, false, true>(a, cur, i, rb, ax, ay, az);
-          filt<V>(vw.nrm, i, ax, ay, az);
-          if (beta != 0.0) {  // + beta S A c_prev (the first direction has none)
-            ax = fmar(rb, vw.ap[3 * i], ax);
-            ay = fmar(rb, vw.ap[3 * i + 1], ay);
-            az = fmar(rb, vw.ap[3 * i + 2], az);
-          }
-        } else {
-          bsr_row<R, V, false>(a, cur, i, rb, ax, ay, az);
-          filt<V>(vw.nrm, i, ax, ay, az);
+    const int64_t gstride = int64_t(sh.g.nblk) * blockDim.x;
+    for (int64_t i0 = sh.g.r0 + int64_t(sh.bidx) * blockDim.x + threadIdx.x; i0 < sh.g.r1; i0 += kRows * gstride) {
+      int64_t ii[kRows];
+      bool on[kRows], fr[kRows];
+      R4<V> ci[kRows];
+      V nr[kRows][3], pp[kRows][3], md[kRows];
+#pragma unroll
+      for (int q = 0; q < kRows; ++q) {
+        ii[q] = i0 + q * gstride;
+        on[q] = ii[q] < sh.g.r1;
+        const int64_t i = on[q] ? ii[q] : i0;
+        ci[q] = next_dir<V>(cur, i, rb);
+        fr[q] = on[q] && a.frei[i];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          nr[q][c] = vw.nrm[3 * i + c];
+          pp[q][c] = kRec ? vw.ap[3 * i + c] : V(0);
         }
-        if (kLow) {
-          const double m = double(vw.md[i]);
-          ca[1] += m * (double(ci.x) * double(ci.x) + double(ci.y) * double(ci.y) + double(ci.z) * double(ci.z));
-        }
+        md[q] = kLow ? V(vw.md[i]) : V(0);
       }
-      vw.ap[3 * i] = ax;
-      vw.ap[3 * i + 1] = ay;
-      vw.ap[3 * i + 2] = az;
-      ca[0] += double(ci.x) * double(ax) + double(ci.y) * double(ay) + double(ci.z) * double(az);
+      V ax[kRows], ay[kRows], az[kRows];
+      bsr_rows<R, V, kRec, kRows>(a, cur, ii, fr, rb, ax, ay, az);
+#pragma unroll
+      for (int q = 0; q < kRows; ++q) {
+        if (!on[q]) continue;
+        const int64_t i = ii[q];
+        nxt.c[i] = ci[q];
+        if (fr[q]) {
+          filt3<V>(nr[q], ax[q], ay[q], az[q]);
+          if (kRec && beta != 0.0) {  // + beta S A c_prev (the first direction has none)
+            ax[q] = fmar(rb, pp[q][0], ax[q]);
+            ay[q] = fmar(rb, pp[q][1], ay[q]);
+            az[q] = fmar(rb, pp[q][2], az[q]);
+          }
+          if (kLow)
+            ca[1] += double(md[q]) * (double(ci[q].x) * double(ci[q].x) + double(ci[q].y) * double(ci[q].y) +
+                                      double(ci[q].z) * double(ci[q].z));
+        }
+        vw.ap[3 * i] = ax[q];
+        vw.ap[3 * i + 1] = ay[q];
+        vw.ap[3 * i + 2] = az[q];
+        ca[0] += double(ci[q].x) * double(ax[q]) + double(ci[q].y) * double(ay[q]) + double(ci[q].z) * double(az[q]);
+      }
     }
     if (SC) {
       // proximity springs pair by pair (implizit.rs:214-220): each nonzero
@@ -565,40 +638,65 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
     }
     const double alpha = delta / ca[0];
     double rzs[1] = {0.0};
-#pragma unroll 2
-    GRP_FOR(i, sh.g.r0, sh.g.r1) {
-      const R4<V> ci = nxt.c[i];
-      D3 d = ld3(a.dv, uint32_t(i));
-      d = d + d3(double(ci.x), double(ci.y), double(ci.z)) * alpha;
-      st3(a.dv, uint32_t(i), d);
-      V apx = vw.ap[3 * i], apy = vw.ap[3 * i + 1], apz = vw.ap[3 * i + 2];
-      if (SC && a.frei[i]) {  // the point's proximity-spring entries, in list order
-        const R4<V>* out = static_cast<const R4<V>*>(a.sc_out);
-        V sx = 0, sy = 0, sz = 0;
-        for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
-          const R4<V> t = out[e];
-          sx += t.x;
-          sy += t.y;
-          sz += t.z;
+    for (int64_t i0 = sh.g.r0 + int64_t(sh.bidx) * blockDim.x + threadIdx.x; i0 < sh.g.r1; i0 += kRows * gstride) {
+      int64_t ii[kRows];
+      bool on[kRows], fr[kRows];
+      R4<V> ci[kRows];
+      D3 d[kRows];
+      V ap[kRows][3], r[kRows][3], nr[kRows][3], pv[kRows][6];
+#pragma unroll
+      for (int q = 0; q < kRows; ++q) {  // every load first
+        ii[q] = i0 + q * gstride;
+        on[q] = ii[q] < sh.g.r1;
+        const int64_t i = on[q] ? ii[q] : i0;
+        ci[q] = nxt.c[i];
+        d[q] = ld3(a.dv, uint32_t(i));
+        fr[q] = a.frei[i];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          ap[q][c] = vw.ap[3 * i + c];
+          r[q][c] = vw.r[3 * i + c];
+          nr[q][c] = vw.nrm[3 * i + c];
         }
-        filt<V>(vw.nrm, i, sx, sy, sz);
-        apx += sx;
-        apy += sy;
-        apz += sz;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) pv[q][c] = V(vw.pinv[6 * i + c]);
       }
-      const V rx = V(double(vw.r[3 * i]) - alpha * double(apx));
-      const V ry = V(double(vw.r[3 * i + 1]) - alpha * double(apy));
-      const V rzz = V(double(vw.r[3 * i + 2]) - alpha * double(apz));
-      vw.r[3 * i] = rx;
-      vw.r[3 * i + 1] = ry;
-      vw.r[3 * i + 2] = rzz;
-      V zx, zy, zz;
-      pmulv<R, V>(vw.pinv, i, rx, ry, rzz, zx, zy, zz);
-      if (!a.frei[i]) zx = zy = zz = 0;
-      V wx = zx, wy = zy, wz = zz;
-      filt<V>(vw.nrm, i, wx, wy, wz);
-      nxt.w[i] = {wx, wy, wz, V(0)};
-      rzs[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rzz) * double(zz);
+#pragma unroll
+      for (int q = 0; q < kRows; ++q) {
+        if (!on[q]) continue;
+        const int64_t i = ii[q];
+        st3(a.dv, uint32_t(i), d[q] + d3(double(ci[q].x), double(ci[q].y), double(ci[q].z)) * alpha);
+        V apx = ap[q][0], apy = ap[q][1], apz = ap[q][2];
+        if (SC && fr[q]) {  // the point's proximity-spring entries, in list order
+          const R4<V>* out = static_cast<const R4<V>*>(a.sc_out);
+          V sx = 0, sy = 0, sz = 0;
+          for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
+            const R4<V> t = out[e];
+            sx += t.x;
+            sy += t.y;
+            sz += t.z;
+          }
+          filt3<V>(nr[q], sx, sy, sz);
+          apx += sx;
+          apy += sy;
+          apz += sz;
+        }
+        const V rx = V(double(r[q][0]) - alpha * double(apx));
+        const V ry = V(double(r[q][1]) - alpha * double(apy));
+        const V rzz = V(double(r[q][2]) - alpha * double(apz));
+        vw.r[3 * i] = rx;
+        vw.r[3 * i + 1] = ry;
+        vw.r[3 * i + 2] = rzz;
+        const V* P = pv[q];
+        V zx = P[0] * rx + P[3] * ry + P[4] * rzz;
+        V zy = P[3] * rx + P[1] * ry + P[5] * rzz;
+        V zz = P[4] * rx + P[5] * ry + P[2] * rzz;
+        if (!fr[q]) zx = zy = zz = 0;
+        V wx = zx, wy = zy, wz = zz;
+        filt3<V>(nr[q], wx, wy, wz);
+        nxt.w[i] = {wx, wy, wz, V(0)};
+        rzs[0] += double(rx) * double(zx) + double(ry) * double(zy) + double(rzz) * double(zz);
+      }
     }
     if (!grid_sync<1>(a, sh, rzs)) return false;
     double beta_next = rzs[0] / delta;
