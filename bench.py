@@ -17,11 +17,23 @@ start), the steps before them are an untimed pre-roll. Both arms time the same
 window from the same state.
 
 A step is one implicit backward-Euler step (build, PCG with release pass,
-friction, integration) of the whole sheet. ``value`` is measured on the
-device-resident state with CUDA events around the step kernels, L2 flushed
-(256 MiB write) before every timed step; ``e2e`` is the same step through the
-public API (ImplizitCg.bild) with x and v copied from pinned host memory to
-the device and back every step.
+friction, integration) of the whole sheet. ``value`` is the chosen form,
+K3D_MIXED_STORAGE (operator blocks and preconditioner stored in FP32, CG
+vectors and sums in FP64), measured on the device-resident state with CUDA
+events around the step kernels, L2 flushed (256 MiB write) before every timed
+step; ``e2e`` is the same step through the public API (ImplizitCg.bild) with x
+and v copied from pinned host memory to the device and back every step.
+``fp64`` (the drop-in form) and ``mixed_fp32_vectors`` (K3D_MIXED) are timed
+on the same window; ``mixed_vs_fp64`` gives the speed ratios and the
+position error of each form against FP64 after one step from the same state
+and after 100 steps of the drop.
+
+``cpu_baseline`` is the FP64 oracle (the reference's CPU step restated, one
+thread) on steps sampled across the timed window, each started from the FP64
+device state at that step with its CG warm start, so it sees the window's
+iteration counts. ``--impl reference`` runs the oracle alone over exactly the
+K timed steps of the window, with the scene built by the oracle's own scene
+builder; it loads no part of the device library.
 
 ``adjoint`` is the backward/forward time of the step's adjoint on the
 material-fit workload (see adjoint_leg), with its gradient check.
@@ -40,7 +52,6 @@ import argparse
 import json
 import math
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -68,7 +79,7 @@ UNIT = "vertex-steps/s"
 def args_():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=40)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--n", type=int, default=257, help="vertices per side of the sheet")
@@ -77,7 +88,8 @@ def args_():
     p.add_argument("--no-compare", action="store_true")
     p.add_argument("--capture", type=int, default=0,
                    help="profiling case: run this many mixed-form steps of the drop on cuda:0 and exit")
-    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="form used by --capture")
+    p.add_argument("--precision", default="storage", choices=["storage", "mixed", "fp64"],
+                   help="form used by --capture: storage (K3D_MIXED_STORAGE), mixed (K3D_MIXED) or fp64")
     p.add_argument("--workload", default="sheet", choices=["sheet", "garment", "adjoint", "mesh"],
                    help="case of --capture: the sheet drop, the garment with self-collision (frames), the "
                         "material-fit drop's adjoint (frames forward, then the backward), or the body mesh "
@@ -170,13 +182,18 @@ GARMENT_PRE = 10    # untimed frames of the garment before its window
 GARMENT_STEPS = 5
 
 
-def garment_leg(flush, torch):
+def garment_leg(flush, torch, peaks, cpu=True):
     """The sewn-garment workload (synth.garment_szene: 28 panels, ~205k
     points, 15-capsule body SDF 256x256x384 at 5 mm, latex, 2 mm collision
     thickness, dt 1/120): frames GARMENT_PRE .. GARMENT_PRE + GARMENT_STEPS of
-    the drop, device-resident, L2 flushed before every timed frame, mixed
-    and FP64, with the self-collision proximity stage on (the workload) and
-    off (the step alone)."""
+    the drop, device-resident, L2 flushed before every timed frame, in the
+    three forms, with the self-collision stage on (the workload) and off (the
+    step alone). For the chosen form with self-collision on: the PCG
+    roofline, e2e through ImplizitCg.bild with host buffers (pinned, copied
+    in and out every frame), and a cpu_baseline of one oracle step (FP64, one
+    thread) from the FP64 device state at the window's first frame, warm
+    start included. One-step position error of each form against FP64 from
+    that state."""
     import numpy as np
     from garmentcraft_b200 import _abi, synth
     from garmentcraft_b200.implizit import ImplizitCg
@@ -184,28 +201,96 @@ def garment_leg(flush, torch):
     s0, _ = synth.garment_szene()
     out = {"workload": f"sewn garment: 28 panels, {s0.n} points, {s0.membran_punkte.shape[0]} membranes, "
                        f"{s0.naht_punkte.shape[0]} seam pairs, 15-capsule SDF 256x256x384 at 5 mm",
-           "window": f"frames {GARMENT_PRE}-{GARMENT_PRE + GARMENT_STEPS}", "unit": UNIT}
+           "window": f"frames {GARMENT_PRE}-{GARMENT_PRE + GARMENT_STEPS - 1}", "unit": UNIT}
+
+    def par(prec, selbst):
+        return ImplizitParameter(schritte_je_bild=1, cg_max=CG_MAX, cg_toleranz=1e-5, precision=prec,
+                                 selbstkollision=selbst)
     for selbst in (True, False):
-        for prec, name in ((_abi.K3D_MIXED, "mixed"), (_abi.K3D_FP64, "fp64")):
+        for prec in (HEADLINE, 0, 1):
+            name = FORMS[prec][0]
             s = s0.copy()
-            par = ImplizitParameter(schritte_je_bild=1, cg_max=CG_MAX, cg_toleranz=1e-5, precision=prec,
-                                    selbstkollision=selbst)
-            cg = ImplizitCg(par, device=torch.cuda.current_device())
+            cg = ImplizitCg(par(prec, selbst), device=torch.cuda.current_device())
             cg.zustand_hochladen(s)
             cg.bilder_auf_geraet(GARMENT_PRE)
-            ms, its, pairs = [], 0, 0
+            ms, sms, its, solves, pairs = [], 0.0, 0, 0, 0
             for k in range(GARMENT_STEPS):
                 flush.fill_(float(k))
                 torch.cuda.synchronize()
                 st = cg.bilder_auf_geraet(1)
                 ms.append(cg.letzte_bild_ms())
+                sms += cg.letzte_loesung_ms()
                 its += st.cg_iterationen
+                solves += st.loesungen
                 pairs += st.naehe_punkt_dreieck + st.naehe_kante_kante
             key = f"{'selfcollision' if selbst else 'no_selfcollision'}_{name}"
             out[key] = {"value": s.n * GARMENT_STEPS / (sum(ms) * 1e-3), "ms_per_step": float(np.mean(ms)),
-                        "cg_iterations_per_step": its / GARMENT_STEPS, "proximity_pairs_per_step": pairs / GARMENT_STEPS}
+                        "cg_iterations_per_step": its / GARMENT_STEPS, "proximity_pairs_per_step": pairs / GARMENT_STEPS,
+                        "pcg_ms_per_step": sms / GARMENT_STEPS}
+            if selbst and prec == HEADLINE:
+                out["roofline"] = roofline_of(s, prec, its, solves, sms, sum(ms), GARMENT_STEPS, peaks,
+                                              "k3d::solve_kernel<float, double, true>")
+            del cg
     for tag in ("selfcollision", "no_selfcollision"):
-        out[f"{tag}_mixed_vs_fp64"] = out[f"{tag}_mixed"]["value"] / out[f"{tag}_fp64"]["value"]
+        for prec in (HEADLINE, 1):
+            out[f"{tag}_{FORMS[prec][0]}_vs_fp64"] = out[f"{tag}_{FORMS[prec][0]}"]["value"] / out[f"{tag}_fp64"]["value"]
+    # e2e: the public call with host buffers
+    s = s0.copy()
+    for nm in ("x", "v"):
+        t = torch.empty(getattr(s, nm).shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = getattr(s, nm)
+        setattr(s, nm, t.numpy())
+    cg = ImplizitCg(par(HEADLINE, True), device=torch.cuda.current_device())
+    cg.bilder_resident(s, GARMENT_PRE)
+    tot = 0.0
+    for k in range(GARMENT_STEPS):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cg.bild(s)
+        tot += time.perf_counter() - t0
+    out["e2e"] = {"value": s.n * GARMENT_STEPS / tot, "unit": UNIT, "h2d_bytes_per_step": 48 * s.n,
+                  "d2h_bytes_per_step": 48 * s.n + 144, "form": FORMS[HEADLINE][0], "selfcollision": True}
+    del cg
+    # one step of each form from the FP64 state at the window's start; the CPU sample from it
+    s = s0.copy()
+    cg = ImplizitCg(par(0, True), device=torch.cuda.current_device())
+    cg.zustand_hochladen(s)
+    cg.bilder_auf_geraet(GARMENT_PRE)
+    cg.zustand_lesen(s)
+    warm = cg.warmstart_lesen()
+    ref = s.copy()
+    cg.bilder_auf_geraet(1)
+    cg.zustand_lesen(ref)
+    d = float(np.linalg.norm(ref.x.max(0) - ref.x.min(0)))
+    err = {}
+    for prec in (HEADLINE, 1):
+        t = s.copy()
+        c = ImplizitCg(par(prec, True), device=torch.cuda.current_device())
+        c.zustand_hochladen(t)
+        c.bilder_auf_geraet(1)
+        c.zustand_lesen(t)
+        dx = np.linalg.norm(t.x - ref.x, axis=1)
+        err[FORMS[prec][0]] = {"max": float(dx.max() / d), "rms": float(np.sqrt(np.mean(dx ** 2)) / d)}
+        del c
+    out["one_step_error_vs_fp64"] = {"from": f"the FP64 state at frame {GARMENT_PRE}", "errors": err,
+                                     "definition": "|x_form - x_fp64| / bbox diagonal after one step "
+                                                   "(the FP64 step with its warm start, the forms without)"}
+    if cpu:
+        O = oracle_mod()
+        m, body = synth.garment(ziel_punkte=200_000)
+        so = O.build_scene(m, [body])
+        so.kollisionsabstand[:] = 2e-3  # as synth.garment_szene
+        sim = O.OracleSim(so, par(0, True).to_c())
+        sim.set_state(s.x, s.v)
+        sim.set_dv_warm(warm)
+        t0 = time.perf_counter()
+        st = sim.frames(1)
+        el = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": s.n / el, "unit": UNIT, "cores": 1, "kind": "port",
+                               "sample": f"one step (frame {GARMENT_PRE}) from the FP64 device state with its warm "
+                                         f"start, self-collision on, {el:.1f} s, FP64 C++ restatement, one thread",
+                               "cg_iterations_per_step": st.cg_iterationen}
     return out
 
 
@@ -415,35 +500,70 @@ def make_scene(n, pinned=False, jitter_mm=1.0):
     return s
 
 
+def oracle_mod():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    return oracle_py
+
+
+def make_scene_oracle(n, jitter_mm=1.0):
+    """The same sheet built by the oracle's own scene builder (oracle/szene.cpp,
+    Szene::aus_netz restated): no part of the device library is loaded."""
+    from garmentcraft_b200 import synth
+    m, body = synth.sheet_over_sphere(n=n, jitter_mm=jitter_mm)
+    return oracle_mod().build_scene(m, [body])
+
+
+HEADLINE = 2  # K3D_MIXED_STORAGE: the chosen form
+FORMS = {0: ("fp64", 8, 8), 1: ("mixed_fp32_vectors", 4, 4), 2: ("mixed_storage", 4, 8)}
+
+
 def params(prec):
     from garmentcraft_b200.params import ImplizitParameter
     return ImplizitParameter(schritte_je_bild=1, cg_max=CG_MAX, cg_toleranz=1e-5, precision=prec)
 
 
-def algorithmic_solve_bytes(s, sw, iters, solves):
-    """Algorithmic bytes of the PCG launches alone (the dominant kernel):
-    operator applications (CG iterations + 2 per solve) and the per-iteration
-    vector update, with the per-unit figures of algorithmic_bytes."""
+def element_counts(s):
     N, T, B = s.n, s.membran_punkte.shape[0], s.biegung_punkte.shape[0]
     S = s.naht_punkte.shape[0] + int(np.sum(s.membran_kante == 0))
-    per_app = N * 10 * sw + T * (12 + 21 * sw) + B * (16 + 13 * sw) + S * (8 + 5 * sw)
-    return (iters + 2 * solves) * per_app + iters * N * 31 * sw
+    return N, T, B, S
 
 
-def algorithmic_bytes(s, sw, steps, iters, solves):
+def algorithmic_solve_bytes(s, s_op, s_vec, iters, solves):
+    """Algorithmic bytes of the PCG launches alone (the dominant kernel), with
+    the per-unit figures of algorithmic_bytes: operator records at s_op bytes
+    per value, vectors at s_vec (FP64 form 8/8, mixed 4/4, storage form 4/8;
+    the preconditioner is an operator value)."""
+    N, T, B, S = element_counts(s)
+    per_app = N * 10 * s_vec + T * (12 + 21 * s_op) + B * (16 + 13 * s_op) + S * (8 + 5 * s_op)
+    per_it = N * (25 * s_vec + 6 * s_op)
+    return (iters + 2 * solves) * per_app + iters * per_it
+
+
+def algorithmic_bytes(s, s_op, s_vec, steps, iters, solves):
     """Minimal streamed bytes of the step (each datum once per pass), per
     unit: per operator application N*10s + T*(12+21s) + B*(16+13s) +
-    S*(8+5s); per CG iteration the vector update N*31s; per step the build
-    and integration 48N + T*(12+21s) + B*(16+13s) + S*(8+5s) + 18s*N + 96N +
-    32N. Operator applications per step = CG iterations + 2 per solve (the
-    start residual and the release test)."""
-    N, T, B = s.n, s.membran_punkte.shape[0], s.biegung_punkte.shape[0]
-    S = s.naht_punkte.shape[0] + int(np.sum(s.membran_kante == 0))
-    elem = T * (12 + 21 * sw) + B * (16 + 13 * sw) + S * (8 + 5 * sw)
-    per_app = N * 10 * sw + elem
-    per_it = N * 31 * sw
-    build = 48 * N + elem + 18 * sw * N + 96 * N + 32 * N
-    return (iters + 2 * solves) * per_app + iters * per_it + steps * build
+    S*(8+5s); per CG iteration the vector update N*31s (of which the
+    preconditioner 6s); per step the build and integration 48N + T*(12+21s) +
+    B*(16+13s) + S*(8+5s) + 18s*N + 96N + 32N. Operator applications per step =
+    CG iterations + 2 per solve (the start residual and the release test)."""
+    N, T, B, S = element_counts(s)
+    elem = T * (12 + 21 * s_op) + B * (16 + 13 * s_op) + S * (8 + 5 * s_op)
+    build = 48 * N + elem + 18 * s_op * N + 96 * N + 32 * N
+    return algorithmic_solve_bytes(s, s_op, s_vec, iters, solves) + steps * build
+
+
+def roofline_of(s, prec, iters, solves, solve_ms, step_ms, steps, peaks, kernel):
+    _, s_op, s_vec = FORMS[prec]
+    alg = algorithmic_solve_bytes(s, s_op, s_vec, iters, solves)
+    achieved = alg / (solve_ms / 1e3) / 1e9
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "peak_source": "measured" if peaks else "fallback", "kernel": kernel,
+            "algorithmic_bytes_per_launch": alg / steps, "kernel_share_of_step": solve_ms / step_ms,
+            "cg_iterations_per_launch": iters / steps,
+            "note": "achieved = algorithmic PCG bytes / PCG launch time (CUDA events on the launching stream); "
+                    "traffic (ncu DRAM bytes) is not measured in this run"}
 
 
 class Clocks:
@@ -492,41 +612,66 @@ def read_peaks():
         return None
 
 
-def read_traffic():
-    """DRAM bytes per CG iteration of solve_kernel<float>, from the committed
-    ncu summary (dram__bytes_read.sum + dram__bytes_write.sum of one captured
-    launch divided by its iterations)."""
-    try:
-        txt = open(os.path.join(ROOT, "profiles", "solve_kernel_sheet257.md")).read()
-        m = re.search(r"traffic_bytes_per_iteration:\s*([0-9.eE+]+)", txt)
-        return float(m.group(1)) if m else None
-    except Exception:
-        return None
-
-
-def cpu_leg(n, warmup, seconds):
-    """The FP64 oracle (single thread, the reference's CPU path restated) on
-    the same workload: `warmup` steps, then steps until `seconds` pass."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle_py
+def reference_leg(n, warmup, steps):
+    """The FP64 oracle (single thread, the reference's CPU step restated) over
+    exactly the timed window: the untimed steps up to the window, then the K
+    window steps timed. The scene comes from the oracle's scene builder."""
+    O = oracle_mod()
     from garmentcraft_b200 import _abi
-    s = make_scene(n)
-    sim = oracle_py.OracleSim(s, params(_abi.K3D_FP64).to_c())
+    s = make_scene_oracle(n)
+    sim = O.OracleSim(s, params(_abi.K3D_FP64).to_c())
     pre, wu = window(warmup)
     sim.frames(pre + wu)
-    steps, t0 = 0, time.perf_counter()
-    its = 0
-    while True:
+    its, t0 = 0, time.perf_counter()
+    for _ in range(steps):
         its += sim.frames(1).cg_iterationen
-        steps += 1
-        el = time.perf_counter() - t0
-        if el >= seconds:
-            break
+    el = time.perf_counter() - t0
     out = {"value": s.n * steps / el, "unit": UNIT, "cores": 1, "kind": "port",
-           "sample": f"the first {steps} steps of the timed window (from step {sum(window(warmup))}) of the same "
-                     f"{n}x{n} drop, {el:.1f} s, FP64 C++ restatement of CpuLoeser/ImplizitCg, one thread",
+           "sample": f"all {steps} timed steps (steps {pre + wu}-{pre + wu + steps - 1}) of the {n}x{n} drop, "
+                     f"{el:.1f} s, FP64 C++ restatement of CpuLoeser/ImplizitCg, one thread",
            "cg_iterations_per_step": its / steps}
-    out["mesh"] = cpu_mesh_leg(oracle_py)
+    out["mesh"] = cpu_mesh_leg(O)
+    return s, out
+
+
+def cpu_sample(n, warmup, steps, seconds, torch):
+    """cpu_baseline of the device arm: the oracle on steps spread over the
+    timed window. The FP64 device form runs the window; before each sampled
+    step its state (x, v and the CG warm start) goes to the oracle, which
+    takes that one step, timed. Reported beside the device FP64 form's
+    iterations on the same steps."""
+    O = oracle_mod()
+    from garmentcraft_b200 import _abi
+    from garmentcraft_b200.implizit import ImplizitCg
+    s = make_scene(n)
+    so = make_scene_oracle(n)
+    cg = ImplizitCg(params(_abi.K3D_FP64), device=torch.cuda.current_device())
+    cg.zustand_hochladen(s)
+    pre, wu = window(warmup)
+    cg.bilder_auf_geraet(pre + wu)
+    picks = sorted({int(round(q * (steps - 1) / 3.0)) for q in range(4)})
+    sim = O.OracleSim(so, params(_abi.K3D_FP64).to_c())
+    cpu_s, cpu_its, dev_its, done = 0.0, 0, 0, []
+    for k in range(steps):
+        if k in picks and cpu_s < seconds:
+            cg.zustand_lesen(s)
+            sim.set_state(s.x, s.v)
+            sim.set_dv_warm(cg.warmstart_lesen())
+            t0 = time.perf_counter()
+            cpu_its += sim.frames(1).cg_iterationen
+            cpu_s += time.perf_counter() - t0
+            dev_its += cg.bilder_auf_geraet(1).cg_iterationen
+            done.append(k)
+        else:
+            cg.bilder_auf_geraet(1)
+    start = pre + wu
+    out = {"value": s.n * len(done) / cpu_s, "unit": UNIT, "cores": 1, "kind": "port",
+           "sample": f"steps {[start + k for k in done]} of the timed window ({start}-{start + steps - 1}) of the "
+                     f"same {n}x{n} drop, each from the FP64 device state at that step (x, v, CG warm start), "
+                     f"{cpu_s:.1f} s, FP64 C++ restatement of CpuLoeser/ImplizitCg, one thread",
+           "cg_iterations_per_step": cpu_its / len(done),
+           "device_fp64_cg_iterations_per_step_same_states": dev_its / len(done)}
+    out["mesh"] = cpu_mesh_leg(O)
     return out
 
 
@@ -607,7 +752,7 @@ def main():
         # a fixed case for ncu: no timing, no flush
         from garmentcraft_b200 import _abi
         from garmentcraft_b200.implizit import ImplizitCg
-        prec = _abi.K3D_MIXED if a.precision == "mixed" else _abi.K3D_FP64
+        prec = {"mixed": _abi.K3D_MIXED, "fp64": _abi.K3D_FP64, "storage": _abi.K3D_MIXED_STORAGE}[a.precision]
         if a.workload == "adjoint":
             from garmentcraft_b200 import synth
             from garmentcraft_b200.adjoint import Drapierung, Stoff
@@ -658,8 +803,7 @@ def main():
     if a.impl == "reference":
         if rank != 0:
             return
-        s = make_scene(a.n)
-        cpu = cpu_leg(a.n, a.warmup, max(10.0, min(150.0, a.cpu_seconds * 6)))
+        s, cpu = reference_leg(a.n, a.warmup, a.steps)
         line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": a.gpus,
                 "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -691,7 +835,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(bus)
-    ms, its, solves, launches, s_mix, cg = dev_timed(a.n, _abi.K3D_MIXED, a.warmup, a.steps, flush, torch)
+    ms, its, solves, launches, s_h, cg = dev_timed(a.n, HEADLINE, a.warmup, a.steps, flush, torch)
     torch.cuda.synchronize()
     clk = clocks.stop()
     t_dev = sum(ms) / 1e3
@@ -699,11 +843,11 @@ def main():
         t = torch.tensor([t_dev], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_dev = float(t.item())
-    nv = s_mix.n
+    nv = s_h.n
     value = world * nv * a.steps / t_dev
 
     # the same steps through the public API with host buffers
-    t_e2e, _ = e2e_timed(a.n, _abi.K3D_MIXED, a.warmup, a.steps, flush, torch)
+    t_e2e, _ = e2e_timed(a.n, HEADLINE, a.warmup, a.steps, flush, torch)
     if world > 1:
         t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -713,39 +857,70 @@ def main():
 
     extra = {}
     if not a.no_compare:
-        ms64, its64, solves64, _, s64, _ = dev_timed(a.n, _abi.K3D_FP64, a.warmup, a.steps, flush, torch)
-        t64 = sum(ms64) / 1e3
-        extra["fp64"] = {"value": nv * a.steps / t64, "ms_per_step": 1e3 * t64 / a.steps,
-                         "cg_iterations_per_step": its64 / a.steps}
-        # position error of the mixed form after 100 steps of the same drop
         from garmentcraft_b200.implizit import ImplizitCg
-        sa, sb = make_scene(a.n), make_scene(a.n)
-        ImplizitCg(params(_abi.K3D_FP64)).bilder_resident(sa, 100)
-        ImplizitCg(params(_abi.K3D_MIXED)).bilder_resident(sb, 100)
-        d = float(np.linalg.norm(sa.x.max(0) - sa.x.min(0)))
-        err = float(np.max(np.linalg.norm(sa.x - sb.x, axis=1)) / d)
-        extra["mixed_vs_fp64"] = {"speedup": t64 / t_dev if world == 1 else None,
-                                  "rel_pos_err_after_100_steps": err,
-                                  "definition": "max_i |x_mixed - x_fp64| / bbox diagonal"}
+        t_form = {HEADLINE: t_dev}
+        for prec in (0, 1):
+            msf, itsf, solvesf, _, _, cgf = dev_timed(a.n, prec, a.warmup, a.steps, flush, torch)
+            t_form[prec] = sum(msf) / 1e3
+            extra[FORMS[prec][0]] = {"value": nv * a.steps / t_form[prec], "ms_per_step": 1e3 * t_form[prec] / a.steps,
+                                     "cg_iterations_per_step": itsf / a.steps,
+                                     "pcg_us_per_iteration": 1e3 * cgf.solve_ms_total / max(itsf, 1)}
+            del cgf
+        # one step of each form from the FP64 state at steps of the window, and 100 steps of the drop
+        pre, wu = window(a.warmup)
+        s0 = make_scene(a.n)
+        c64 = ImplizitCg(params(0))
+        c64.zustand_hochladen(s0)
+        c64.bilder_auf_geraet(pre + wu)
+        one = {FORMS[p][0]: [] for p in (HEADLINE, 1)}
+        at = []
+        for k in range(0, a.steps, max(1, a.steps // 4)):
+            st0 = s0.copy()
+            c64.zustand_lesen(st0)
+            ref = st0.copy()
+            c64.bilder_auf_geraet(1)
+            c64.zustand_lesen(ref)
+            d = float(np.linalg.norm(ref.x.max(0) - ref.x.min(0)))
+            for prec in (HEADLINE, 1):
+                t = st0.copy()
+                cf = ImplizitCg(params(prec))
+                cf.zustand_hochladen(t)
+                cf.bilder_auf_geraet(1)
+                cf.zustand_lesen(t)
+                dx = np.linalg.norm(t.x - ref.x, axis=1)
+                one[FORMS[prec][0]].append({"max": float(dx.max() / d), "rms": float(np.sqrt(np.mean(dx ** 2)) / d)})
+                del cf
+            at.append(pre + wu + k)
+            c64.bilder_auf_geraet(max(1, a.steps // 4) - 1)
+        del c64
+        sa = make_scene(a.n)
+        ImplizitCg(params(0)).bilder_resident(sa, 100)
+        err100 = {}
+        for prec in (HEADLINE, 1):
+            sb = make_scene(a.n)
+            ImplizitCg(params(prec)).bilder_resident(sb, 100)
+            d = float(np.linalg.norm(sa.x.max(0) - sa.x.min(0)))
+            err100[FORMS[prec][0]] = float(np.max(np.linalg.norm(sa.x - sb.x, axis=1)) / d)
+        extra["mixed_vs_fp64"] = {
+            "speedup": {FORMS[p][0]: t_form[0] / t_form[p] for p in (HEADLINE, 1)} if world == 1 else None,
+            "one_step_error": {"at_steps": at, "errors": one,
+                               "definition": "|x_form - x_fp64| / bbox diagonal after one step from the same FP64 "
+                                             "state (the FP64 step with its warm start, the forms without)"},
+            "rel_pos_err_after_100_steps": err100,
+            "definition": "max_i |x_form - x_fp64| / bbox diagonal"}
 
     peaks = read_peaks()
-    alg = algorithmic_solve_bytes(s_mix, 4, its, solves)
-    achieved = alg / (cg.solve_ms_total / 1e3) / 1e9
-    peak = peaks["hbm_gbs"] if peaks else 6650.0
-    tpi = read_traffic()
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": tpi * its / a.steps if tpi else None,
-                "peak_source": "measured" if peaks else "fallback", "kernel": "k3d::solve_kernel<float>",
-                "algorithmic_bytes_per_launch": alg / a.steps,
-                "kernel_share_of_step": cg.solve_ms_total / sum(ms),
-                "note": "working set is L2-resident; traffic = ncu DRAM bytes per iteration x iterations per launch"}
+    roofline = roofline_of(s_h, HEADLINE, its, solves, cg.solve_ms_total, sum(ms), a.steps, peaks,
+                           "k3d::solve_kernel<float, double, false>")
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1e3 * t_dev / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": workload_config(a.n, s_mix, {"precision": "mixed (FP32 operator, FP64 dots/scalars/state)"}),
+            "config": workload_config(a.n, s_h, {"precision": "mixed storage (FP32 operator blocks and "
+                                                              "preconditioner, FP64 CG vectors, sums and state)"}),
             "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
-            "cg_iterations_per_step": its / a.steps, "clocks": clk}
+            "cg_iterations_per_step": its / a.steps,
+            "pcg_us_per_iteration": 1e3 * cg.solve_ms_total / max(its, 1), "clocks": clk}
     line.update(extra)
     if world == 1 and not a.no_batch:
         line["batched"] = batch_leg(a.batch_steps, flush, torch)
@@ -754,11 +929,11 @@ def main():
     if world == 1 and not a.no_adjoint:
         line["adjoint"] = adjoint_leg(torch)
     if world == 1 and not a.no_garment:
-        line["garment"] = garment_leg(flush, torch)
+        line["garment"] = garment_leg(flush, torch, peaks, cpu=not a.no_cpu)
     if world == 1 and not a.no_mesh:
         line["mesh"] = mesh_leg(flush, torch)
     if rank == 0 and world == 1 and not a.no_cpu:
-        line["cpu_baseline"] = cpu_leg(a.n, a.warmup, a.cpu_seconds)
+        line["cpu_baseline"] = cpu_sample(a.n, a.warmup, a.steps, a.cpu_seconds, torch)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

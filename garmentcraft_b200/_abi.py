@@ -177,6 +177,14 @@ class K3dMeshInfo(C.Structure):
     ]
 
 
+class K3dContactSet(C.Structure):
+    _fields_ = [
+        ("fest", C.POINTER(C.c_uint8)),
+        ("normale", C.POINTER(C.c_double)),
+        ("vn_soll", C.POINTER(C.c_double)),
+    ]
+
+
 class K3dCgResult(C.Structure):
     _fields_ = [
         ("iterationen", C.c_int64),

@@ -18,8 +18,8 @@ EXPORTS = [
     "k3d_abi_version", "k3d_params_default", "k3d_simparams_default", "k3d_build_scene",
     "k3d_built_scene_view", "k3d_built_scene_free", "k3d_solver_create", "k3d_solver_destroy",
     "k3d_last_error", "k3d_solver_name", "k3d_upload_scene", "k3d_frame", "k3d_frames_resident",
-    "k3d_upload_state", "k3d_download_state", "k3d_operator", "k3d_system_for", "k3d_solve",
-    "k3d_residual", "k3d_read_load", "k3d_last_frame_ms", "k3d_last_solve_ms", "k3d_kernel_launches",
+    "k3d_upload_state", "k3d_download_state", "k3d_operator", "k3d_system_for", "k3d_solve", "k3d_solve_contacts",
+    "k3d_residual", "k3d_read_load", "k3d_read_warm_start", "k3d_last_frame_ms", "k3d_last_solve_ms", "k3d_kernel_launches",
     "k3d_pcg_blocks",
     "k3d_operator_noalloc", "k3d_selfcollision_pairs", "k3d_selfcollision_hash", "k3d_selfcollision_springs",
     "k3d_adjoint_forward", "k3d_adjoint_backward",
@@ -82,10 +82,14 @@ def lib():
     L.k3d_system_for.restype = st
     L.k3d_solve.argtypes = [P, dp, C.POINTER(_abi.K3dCgResult)]
     L.k3d_solve.restype = st
+    L.k3d_solve_contacts.argtypes = [P, C.POINTER(_abi.K3dContactSet), dp, C.POINTER(_abi.K3dCgResult)]
+    L.k3d_solve_contacts.restype = st
     L.k3d_residual.argtypes = [P, dp, dp]
     L.k3d_residual.restype = st
     L.k3d_read_load.argtypes = [P, dp]
     L.k3d_read_load.restype = st
+    L.k3d_read_warm_start.argtypes = [P, dp]
+    L.k3d_read_warm_start.restype = st
     L.k3d_last_frame_ms.argtypes = [P]
     L.k3d_last_frame_ms.restype = C.c_double
     L.k3d_last_solve_ms.argtypes = [P]

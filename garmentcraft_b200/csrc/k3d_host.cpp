@@ -47,6 +47,8 @@ struct k3d_solver {
   int blocks = 0;
   size_t rsize = 8;  // operator records, assembled blocks, preconditioner
   size_t vsize = 8;  // the PCG's vectors
+  uint8_t* d_fest = nullptr;  // device copy of a caller's contact set
+  double *d_fest_n = nullptr, *d_fest_soll = nullptr;
   bool uploaded = false, first_step = true;
   int64_t n = 0, nt = 0, nb = 0, ns = 0;
   double boden = 0.0;
@@ -200,6 +202,9 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   h->d_pout = A.take<double>(3 * N);
   a.fnk = A.take<double>(N);
   a.vn_soll = A.take<double>(N);
+  h->d_fest = A.take<uint8_t>(N);  // a caller's contact set (k3d_solve_contacts)
+  h->d_fest_n = A.take<double>(3 * N);
+  h->d_fest_soll = A.take<double>(N);
   a.masse = cv.masse = A.take<double>(N);
   a.w = cv.w = A.take<double>(N);
   a.kabst = cv.kabst = A.take<double>(N);
@@ -1234,6 +1239,24 @@ k3d_status k3d_solve(k3d_solver* h, double* dv_inout, k3d_cg_result* out) {
   return sv[ST_UNCONVERGED] ? K3D_NOT_CONVERGED : K3D_OK;
 }
 
+k3d_status k3d_solve_contacts(k3d_solver* h, const k3d_contact_set* fest, double* dv_inout, k3d_cg_result* out) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if (!fest || !fest->fest || !fest->normale || !fest->vn_soll) return fail(h, K3D_BAD_ARGUMENT, "null contact set");
+  if (h->sc.on) return fail(h, K3D_BAD_ARGUMENT, "a caller's contact set with self-collision on");
+  const size_t N = size_t(h->n);
+  K3D_CUDA(h, cudaMemcpyAsync(h->d_fest, fest->fest, N, cudaMemcpyHostToDevice, h->stream));
+  K3D_CUDA(h, cudaMemcpyAsync(h->d_fest_n, fest->normale, 24 * N, cudaMemcpyHostToDevice, h->stream));
+  K3D_CUDA(h, cudaMemcpyAsync(h->d_fest_soll, fest->vn_soll, 8 * N, cudaMemcpyHostToDevice, h->stream));
+  h->a.fest_in = h->d_fest;
+  h->a.fest_n = h->d_fest_n;
+  h->a.fest_soll = h->d_fest_soll;
+  st = k3d_solve(h, dv_inout, out);
+  h->a.fest_in = nullptr;
+  h->a.fest_n = h->a.fest_soll = nullptr;
+  return st;
+}
+
 k3d_status k3d_residual(k3d_solver* h, const double* dv, double* out) {
   k3d_status st = ready(h);
   if (st != K3D_OK) return st;
@@ -1245,6 +1268,15 @@ k3d_status k3d_residual(k3d_solver* h, const double* dv, double* out) {
   if (st != K3D_OK) return st;
   K3D_CUDA(h, cudaMemcpyAsync(out, h->d_pout, 24 * size_t(h->n), cudaMemcpyDeviceToHost, h->stream));
   return check_sync(h);
+}
+
+k3d_status k3d_read_warm_start(k3d_solver* h, double* dv) {
+  k3d_status st = ready(h);
+  if (st != K3D_OK) return st;
+  if (!dv) return fail(h, K3D_BAD_ARGUMENT, "null vector");
+  K3D_CUDA(h, cudaStreamSynchronize(h->stream));
+  K3D_CUDA(h, cudaMemcpy(dv, h->a.dv, 24 * size_t(h->n), cudaMemcpyDeviceToHost));
+  return K3D_OK;
 }
 
 k3d_status k3d_read_load(k3d_solver* h, double* out) {

@@ -902,6 +902,22 @@ static cudaError_t cooperative(const void* fn, const StepArgs& a, int blocks, cu
   return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
+// The caller's contact set in place of the one the build found (held points
+// get the given normal and normal velocity, the others none).
+template <typename R>
+__global__ void __launch_bounds__(kBlock) contacts_kernel(const __grid_constant__ StepArgs a) {
+  R* nrm = static_cast<R*>(a.nrm);
+  K3D_FOR(i, a.n) {
+    const bool on = a.fest_in[i] != 0;
+    const D3 n = on ? ld3(a.fest_n, uint32_t(i)) : d3(0, 0, 0);
+    st3(a.nrm_d, uint32_t(i), n);
+    nrm[3 * i] = R(n.x);
+    nrm[3 * i + 1] = R(n.y);
+    nrm[3 * i + 2] = R(n.z);
+    a.vn_soll[i] = on ? a.fest_soll[i] : 0.0;
+  }
+}
+
 template <typename R, typename V>
 static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int& launched) {
   cudaError_t e;
@@ -911,6 +927,10 @@ static cudaError_t launch_t(const StepArgs& a, int blocks, cudaStream_t st, int&
   if ((e = plain(K.elements, a, elems, st)) != cudaSuccess) return e;
   if ((e = plain(K.points, a, a.n, st)) != cudaSuccess) return e;
   launched = 2;
+  if (a.fest_in) {
+    if ((e = plain((const void*)contacts_kernel<R>, a, a.n, st)) != cudaSuccess) return e;
+    launched += 1;
+  }
   if (a.mode == MODE_SYSTEM && !a.p_out) return cudaSuccess;
   if (a.mode == MODE_OPERATOR || a.mode == MODE_RESIDUAL || a.mode == MODE_SYSTEM) {
     if ((e = plain(K.probe_load, a, a.n, st)) != cudaSuccess) return e;

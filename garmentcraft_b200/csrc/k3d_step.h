@@ -134,6 +134,11 @@ struct StepArgs {
   // probes
   const double* p_in;
   double* p_out;
+  // the caller's contact set of a solve (k3d_solve_contacts), null otherwise:
+  // held flag, unit normal (3 per point) and required normal velocity; it
+  // replaces the set the build found against the bodies
+  const uint8_t* fest_in;
+  const double *fest_n, *fest_soll;
   // instances (independent drapes): per point its instance (null for one),
   // the groups of the PCG launch and each block's group
   const uint32_t* pinst;

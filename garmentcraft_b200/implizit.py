@@ -161,12 +161,26 @@ class ImplizitCg:
         self._check(self._L.k3d_system_for(self._h, C.byref(rb)), "system")
         return out
 
-    def loese(self, s: Szene, dv: np.ndarray):
-        """Loeser::loese (implizit.rs:370-426) on the system of the scene's state."""
+    def loese(self, s: Szene, dv: np.ndarray, fest: dict | None = None):
+        """Loeser::loese (implizit.rs:308, 370-426) on the system of the
+        scene's state. ``fest`` is the contact set the reference hands every
+        backend (implizit.rs:870-883): a dict of ``fest`` (held flag per
+        point), ``normale`` (unit normal, 3 per point) and ``vn_soll``
+        (required normal velocity); None solves with the contact set the
+        device finds against the bodies."""
         self._sync_state(s)
         dv = np.ascontiguousarray(dv, dtype=np.float64).copy()
         res = _abi.K3dCgResult()
-        self._check(self._L.k3d_solve(self._h, _d(dv), C.byref(res)), "solve")
+        if fest is None:
+            self._check(self._L.k3d_solve(self._h, _d(dv), C.byref(res)), "solve")
+        else:
+            on = np.ascontiguousarray(fest["fest"], dtype=np.uint8)
+            nrm = np.ascontiguousarray(fest["normale"], dtype=np.float64)
+            soll = np.ascontiguousarray(fest["vn_soll"], dtype=np.float64)
+            if on.shape != (s.n,) or nrm.shape != (s.n, 3) or soll.shape != (s.n,):
+                raise ValueError("contact set does not match the scene's points")
+            cs = _abi.K3dContactSet(on.ctypes.data_as(C.POINTER(C.c_uint8)), _d(nrm), _d(soll))
+            self._check(self._L.k3d_solve_contacts(self._h, C.byref(cs), _d(dv), C.byref(res)), "solve")
         return dv, CgLauf(res.iterationen, bool(res.nicht_konvergiert), res.rest, bool(res.breakdown))
 
     def rest_geloest(self, s: Szene, dv: np.ndarray) -> np.ndarray:
@@ -181,6 +195,13 @@ class ImplizitCg:
         """Loeser::last_lesen (implizit.rs:348-350)."""
         out = np.zeros((self._szene.n, 3))
         self._check(self._L.k3d_read_load(self._h, _d(out)), "load")
+        return out
+
+    def warmstart_lesen(self) -> np.ndarray:
+        """The CG warm start of the next substep (ImplizitCg's dv_vorher,
+        implizit.rs:906, 945), 3 per point."""
+        out = np.zeros((self._szene.n, 3))
+        self._check(self._L.k3d_read_warm_start(self._h, _d(out)), "warm start")
         return out
 
     # ---- self-collision probes: the proximity stage's last run

@@ -308,11 +308,37 @@ k3d_status k3d_system_for(k3d_solver* h, k3d_system_readback* out);
  * start in and the solution out (3 per point). */
 k3d_status k3d_solve(k3d_solver* h, double* dv_inout, k3d_cg_result* out);
 
+/* The contact set Loeser::loese receives (`fest: &[Option<Fest>]`,
+ * implizit.rs:308; Fest at :594-599) as arrays over the points: fest[i] = 1
+ * holds point i (Some) with the unit normal normale[3i..3i+2] and the normal
+ * velocity vn_soll[i] it must have after the step; fest[i] = 0 leaves it
+ * free (None). Fest::v_koerper is not read by a solve. Host pointers. */
+typedef struct k3d_contact_set {
+  const uint8_t* fest;
+  const double* normale;
+  const double* vn_soll;
+} k3d_contact_set;
+
+/* Loeser::loese (implizit.rs:308) with the caller's contact set, as
+ * ImplizitCg::schritt hands its host-built set to every backend
+ * (implizit.rs:870-883), one that builds the system itself included
+ * (GpuLoeser::loese, gpu.rs:1808-1817): the device builds the system of the
+ * current state and solves it with `fest` in place of the contact set it
+ * would find against the bodies. dv_inout as in k3d_solve. */
+k3d_status k3d_solve_contacts(k3d_solver* h, const k3d_contact_set* fest, double* dv_inout, k3d_cg_result* out);
+
 /* Loeser::rest_geloest (implizit.rs:337-342): A dv - b without the filter. */
 k3d_status k3d_residual(k3d_solver* h, const double* dv, double* out);
 
 /* Loeser::last_lesen (implizit.rs:348-350): the load of the last built system. */
 k3d_status k3d_read_load(k3d_solver* h, double* out);
+
+/* The CG warm start the next substep starts from (ImplizitCg's private
+ * dv_vorher, implizit.rs:578, 906, 945): the last solve's dv, 3 per point,
+ * which k3d_frame and k3d_frames_resident carry from substep to substep. The
+ * reference has no accessor for it; with it a caller can hand the device's
+ * state, warm start included, to another solver (e.g. a CPU cross-check). */
+k3d_status k3d_read_warm_start(k3d_solver* h, double* dv);
 
 /* Time of the last device frame in ms, measured with CUDA events on the
  * handle's stream (the figure GpuLoeser::zeiten reports, gpu.rs:1225-1227). */

@@ -498,6 +498,12 @@ void orc_sim_naht_offen(void* h) { naht_offen(static_cast<Sim*>(h)->s); }
 void orc_sim_set_reibung(void* h, double mu) {
   for (double& r : static_cast<Sim*>(h)->s.reibung) r = mu;
 }
+void orc_sim_set_dv_warm(void* h, const double* dv) {
+  auto* sim = static_cast<Sim*>(h);
+  sim->cg.dv_vorher.resize(sim->s.x.size());
+  for (size_t i = 0; i < sim->cg.dv_vorher.size(); ++i)
+    for (int a = 0; a < 3; ++a) sim->cg.dv_vorher[i][a] = dv[3 * i + a];
+}
 void orc_sim_get_dv_warm(void* h, double* dv) {
   auto* sim = static_cast<Sim*>(h);
   for (size_t i = 0; i < sim->cg.dv_vorher.size(); ++i)
@@ -543,6 +549,35 @@ void orc_sim_solve(void* h, double* dv, k3d_cg_result* out) {
   std::vector<std::optional<Fest>> fest;
   System sys = sim->cg.system_bauen(sim->s, substep_h(sim), fest);
   size_t n = sim->s.x.size();
+  std::vector<V3> d(n);
+  for (size_t i = 0; i < n; ++i) d[i] = {dv[3 * i], dv[3 * i + 1], dv[3 * i + 2]};
+  CgLauf l = cpu_loese(sys, fest, d);
+  for (size_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) dv[3 * i + a] = d[i][a];
+  out->iterationen = int64_t(l.iterationen);
+  out->nicht_konvergiert = l.nicht_konvergiert ? 1 : 0;
+  out->breakdown = 0;
+  out->rest = l.rest;
+}
+
+// Loeser::loese with a given contact set (implizit.rs:308): the system of the
+// current state, the caller's Fest in place of the one system_bauen found.
+void orc_sim_solve_contacts(void* h, const uint8_t* on, const double* nrm, const double* soll, double* dv,
+                            k3d_cg_result* out) {
+  auto* sim = static_cast<Sim*>(h);
+  std::vector<std::optional<Fest>> fest;
+  System sys = sim->cg.system_bauen(sim->s, substep_h(sim), fest);
+  size_t n = sim->s.x.size();
+  for (size_t i = 0; i < n; ++i) {
+    if (!on[i]) {
+      fest[i].reset();
+      continue;
+    }
+    Fest f;
+    f.normale = {nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]};
+    f.vn_soll = soll[i];
+    fest[i] = f;
+  }
   std::vector<V3> d(n);
   for (size_t i = 0; i < n; ++i) d[i] = {dv[3 * i], dv[3 * i + 1], dv[3 * i + 2]};
   CgLauf l = cpu_loese(sys, fest, d);

@@ -60,9 +60,11 @@ def lib():
     L.orc_sim_naht_offen.argtypes = [P]
     L.orc_sim_set_reibung.argtypes = [P, C.c_double]
     L.orc_sim_get_dv_warm.argtypes = [P, dp]
+    L.orc_sim_set_dv_warm.argtypes = [P, dp]
     L.orc_sim_operator.argtypes = [P, dp, dp]
     L.orc_sim_system.argtypes = [P, C.POINTER(_abi.K3dSystemReadback)]
     L.orc_sim_solve.argtypes = [P, dp, C.POINTER(_abi.K3dCgResult)]
+    L.orc_sim_solve_contacts.argtypes = [P, C.POINTER(C.c_uint8), dp, dp, dp, C.POINTER(_abi.K3dCgResult)]
     L.orc_sim_umfang.argtypes = [P, dp, dp]
     L.orc_sim_umfang.restype = C.c_double
     L.orc_sim_nahtspalt.argtypes = [P]
@@ -249,6 +251,11 @@ class OracleSim:
         self.L.orc_sim_get_dv_warm(self.h, _d(dv))
         return dv
 
+    def set_dv_warm(self, dv):
+        """Sets the warm start of the next substep (dv_vorher)."""
+        dv = f64(dv)
+        self.L.orc_sim_set_dv_warm(self.h, _d(dv))
+
     def operator(self, p):
         p = f64(p)
         out = np.zeros((self.n, 3))
@@ -265,6 +272,17 @@ class OracleSim:
                                     out["fest"].ctypes.data_as(C.POINTER(C.c_uint8)))
         self.L.orc_sim_system(self.h, C.byref(rb))
         return out
+
+    def solve_contacts(self, dv, fest):
+        """Loeser::loese with the given contact set (dict of fest, normale,
+        vn_soll as ImplizitCg.loese takes it)."""
+        dv = f64(dv).copy()
+        on = np.ascontiguousarray(fest["fest"], dtype=np.uint8)
+        nrm, soll = f64(fest["normale"]), f64(fest["vn_soll"])
+        res = _abi.K3dCgResult()
+        self.L.orc_sim_solve_contacts(self.h, on.ctypes.data_as(C.POINTER(C.c_uint8)), _d(nrm), _d(soll), _d(dv),
+                                      C.byref(res))
+        return dv, res
 
     def solve(self, dv):
         dv = f64(dv).copy()

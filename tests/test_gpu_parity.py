@@ -117,6 +117,39 @@ def test_loese_wie_cpu():
     assert rel(ImplizitCg(par).rest_geloest(s, a), r_o.operator(a) - r_o.system()["rhs"]) <= 1e-10
 
 
+def test_loese_mit_vorgegebenem_kontaktsatz():
+    # Loeser::loese takes the contact set from its caller (implizit.rs:308,
+    # 870-883). The tube's own set gives the device's own solve; a changed set
+    # (every third held point released, the others' normal velocity shifted)
+    # is honoured, and both match the oracle's solve with the same set to 1e-9.
+    s = tube_scene()
+    par = ImplizitParameter(schritte_je_bild=1, cg_max=4000, cg_toleranz=1e-12)
+    orc = O.OracleSim(s, par.to_c())
+    orc.frames(3)
+    x, v = orc.state()
+    s.x[:], s.v[:] = x, v
+    dv0 = orc.dv_warm()
+    sysr = orc.system()
+    eigen = {"fest": sysr["fest"], "normale": sysr["normale"], "vn_soll": sysr["vn_soll"]}
+    assert eigen["fest"].sum() > 10
+    cg = ImplizitCg(par)
+    a, _ = cg.loese(s, dv0, fest=eigen)
+    b, _ = cg.loese(s, dv0)
+    assert rel(a, b) <= 1e-12
+    ao, _ = orc.solve_contacts(dv0, eigen)
+    assert rel(a, ao) <= 1e-9
+    held = np.flatnonzero(eigen["fest"])
+    anders = {k: v.copy() for k, v in eigen.items()}
+    anders["fest"][held[::3]] = 0
+    anders["normale"][held[::3]] = 0.0
+    anders["vn_soll"][held[1::3]] += 0.01
+    c, lc = cg.loese(s, dv0, fest=anders)
+    co, lo = orc.solve_contacts(dv0, anders)
+    assert abs(lc.iterationen - lo.iterationen) <= 2
+    assert rel(c, co) <= 1e-9
+    assert rel(c, a) > 1e-6  # the set is honoured
+
+
 def test_loese_sheet_innerhalb_der_toleranz():
     # ill conditioned (sheet on the sphere, tol 1e-8): the solutions differ by
     # rounding amplified by the condition number; both meet the tolerance and
