@@ -385,12 +385,11 @@ __device__ __forceinline__ void bsr_row(const StepArgs& a, const Dir<V>& buf, in
   oz = z;
 }
 
-// Rows a thread takes together in the CG iteration's two point passes. A
-// thread with more than one row (the grid has fewer threads than points)
-// issues the rows' loads before any of their stores: its stores may alias
-// the next row's loads as far as the compiler knows, so a row at a time
-// would wait for each row's chain of loads in turn.
-constexpr int kRows = 2;
+// Rows a thread takes together in the CG iteration's two point passes; each
+// round issues its rows' loads before any of their stores. Measured on the
+// 66k- and 201k-point sheets: one row per round is fastest (two cost 15-25 %
+// more per iteration, three more still).
+constexpr int kRows = 1;
 
 // (A c)_i (or (A w)_i with WONLY) for the rows ii[q] with on[q], in one loop
 // over the block ranks; the result is zero where !on[q].
