@@ -404,13 +404,15 @@ def shapes_leg():
                              ("sheet_257x257", gross, 1)):
             par = ImplizitParameter(schritte_je_bild=sub, cg_max=CG_MAX, precision=_abi.K3D_MIXED)
             q, rec = autotune.abstimmen(s, par, bilder=3, runden=2, cache=f"{d}/t.json", neu=True)
-            voll = max(z["pcg_bloecke"] for z in rec["kandidaten"])
-            dflt = next(z for z in rec["kandidaten"] if z["pcg_bloecke"] == voll and not z["graph"])
+            voll = max(z["pcg_bloecke"] for z in rec["kandidaten"] if z["pcg_threads"] == 512)
+            dflt = next(z for z in rec["kandidaten"]
+                        if z["pcg_threads"] == 512 and z["pcg_bloecke"] == voll and not z["graph"])
             steps = 3 * sub
             out[name] = {"vertices": s.n, "substeps_per_frame": sub,
-                         "default": {"pcg_blocks": voll, "graph": False, "ms_per_frame": dflt["ms_je_bild"],
+                         "default": {"pcg_threads": 512, "pcg_blocks": voll, "graph": False,
+                                     "ms_per_frame": dflt["ms_je_bild"],
                                      "value": s.n * sub / (dflt["ms_je_bild"] * 1e-3)},
-                         "tuned": {"pcg_blocks": q.pcg_bloecke, "graph": bool(q.graph),
+                         "tuned": {"pcg_threads": q.pcg_threads, "pcg_blocks": q.pcg_bloecke, "graph": bool(q.graph),
                                    "ms_per_frame": rec["ms_je_bild"],
                                    "value": s.n * sub / (rec["ms_je_bild"] * 1e-3)},
                          "tuned_vs_default": dflt["ms_je_bild"] / rec["ms_je_bild"],

@@ -53,7 +53,7 @@ class K3dParams(C.Structure):
         ("pcg_bloecke", C.c_int32),
         ("koerperpunkt_tiefe", C.c_double),
         ("graph", C.c_int32),
-        ("reserved", C.c_int32),
+        ("pcg_threads", C.c_int32),
     ]
 
 

@@ -1,9 +1,14 @@
 """Launch-shape tuner for the device step (no counterpart in the reference,
 whose solver has a single CPU form).
 
-The step has two launch choices that change its speed but not its
+The step has three launch choices that change its speed but not its
 arithmetic beyond the summation order of the grid reductions:
 
+* ``pcg_threads`` -- the CTA size of the persistent PCG launch: 512 threads
+  (one CTA per SM, 128 registers a thread), 256 (two CTAs per SM, the same
+  registers; twice the CTAs at every grid barrier) or 1024 (one CTA per SM,
+  64 registers a thread, so the kernel spills; twice the warps to hide the
+  row products' load latency).
 * ``pcg_bloecke`` -- CTAs of the persistent PCG launch. Every PCG iteration
   passes two grid barriers whose cost grows with the CTAs that arrive; a
   small drape has too little work per iteration to hide it, so fewer CTAs
@@ -12,7 +17,8 @@ arithmetic beyond the summation order of the grid reductions:
   the host launch cost between the short kernels of a substep (not with
   self-collision, whose stage reads counts back between launches).
 
-``abstimmen`` times every candidate on the caller's own scene (the same
+``abstimmen`` times every candidate (CTA size x CTA count x graph) on the
+caller's own scene (the same
 frames from the same state, device time from CUDA events), keeps the fastest
 and caches it in a JSON file keyed by the device, the precision and the
 scene's size, so the sweep runs once per shape.
@@ -28,6 +34,7 @@ from .params import ImplizitParameter
 from .szene import Szene
 
 CACHE_ENV = "GARMENTCRAFT_B200_TUNE"
+THREADS = (512, 256, 1024)  # CTA sizes the library is built for
 
 
 def cache_pfad() -> str:
@@ -78,30 +85,41 @@ def _schreiben(pfad: str, daten: dict) -> None:
     os.replace(tmp, pfad)
 
 
+def _gewaehlt(param: ImplizitParameter, rec: dict) -> ImplizitParameter:
+    return replace(param, pcg_bloecke=rec["pcg_bloecke"], graph=rec["graph"],
+                   pcg_threads=rec.get("pcg_threads", 0))
+
+
 def abstimmen(s: Szene, param: ImplizitParameter | None = None, bilder: int = 3, runden: int = 2,
-              cache: str | None = None, device: int = 0, neu: bool = False) -> tuple[ImplizitParameter, dict]:
+              cache: str | None = None, device: int = 0, neu: bool = False,
+              threads: tuple[int, ...] = THREADS) -> tuple[ImplizitParameter, dict]:
     """The fastest launch shape for ``s`` under ``param``: returns the
-    parameters with ``pcg_bloecke`` and ``graph`` set, and the record (the
-    time per frame of every candidate). ``s`` is not changed. A cached
-    record for the same key is used unless ``neu``."""
+    parameters with ``pcg_threads``, ``pcg_bloecke`` and ``graph`` set, and
+    the record (the time per frame of every candidate). ``s`` is not changed.
+    A cached record for the same key is used unless ``neu``."""
     param = param or ImplizitParameter()
     pfad = cache or cache_pfad()
     probe = ImplizitCg(param, device)
     geraet = probe.loeser_name()
-    probe.hochladen(s.copy())
-    voll = probe.pcg_bloecke()
     del probe
     key = schluessel(geraet, param, s)
     daten = _lesen(pfad)
     if not neu and key in daten:
         rec = daten[key]
-        return replace(param, pcg_bloecke=rec["pcg_bloecke"], graph=rec["graph"]), rec
+        return _gewaehlt(param, rec), rec
     inst = _instanzen(s)
     graphen = (False,) if param.selbstkollision else (False, True)
+    formen = []
+    for nt in threads:
+        probe = ImplizitCg(replace(param, pcg_threads=nt), device)
+        probe.hochladen(s.copy())
+        voll = probe.pcg_bloecke()
+        del probe
+        formen += [(nt, b) for b in kandidaten(voll, inst)]
     zeiten = []
-    for b in kandidaten(voll, inst):
+    for nt, b in formen:
         for g in graphen:
-            p = replace(param, pcg_bloecke=b, graph=g)
+            p = replace(param, pcg_bloecke=b, graph=g, pcg_threads=nt)
             cg = ImplizitCg(p, device)
             t = s.copy()
             cg.hochladen(t)
@@ -111,11 +129,11 @@ def abstimmen(s: Szene, param: ImplizitParameter | None = None, bilder: int = 3,
                 cg.zustand_hochladen(s)
                 cg.bilder_auf_geraet(bilder)
                 best = min(best, cg.letzte_bild_ms() / bilder)
-            zeiten.append({"pcg_bloecke": b, "graph": g, "ms_je_bild": best})
+            zeiten.append({"pcg_threads": nt, "pcg_bloecke": b, "graph": g, "ms_je_bild": best})
             del cg
     sieger = min(zeiten, key=lambda z: z["ms_je_bild"])
-    rec = {"pcg_bloecke": sieger["pcg_bloecke"], "graph": sieger["graph"], "ms_je_bild": sieger["ms_je_bild"],
-           "kandidaten": zeiten, "bilder": bilder}
+    rec = {"pcg_threads": sieger["pcg_threads"], "pcg_bloecke": sieger["pcg_bloecke"], "graph": sieger["graph"],
+           "ms_je_bild": sieger["ms_je_bild"], "kandidaten": zeiten, "bilder": bilder}
     daten[key] = rec
     _schreiben(pfad, daten)
-    return replace(param, pcg_bloecke=rec["pcg_bloecke"], graph=rec["graph"]), rec
+    return _gewaehlt(param, rec), rec

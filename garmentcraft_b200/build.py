@@ -12,18 +12,21 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_native")
 LIB = os.path.join(OUT_DIR, "libklon3d_b200.so")
-SOURCES = ["k3d_step.cu", "k3d_build.cu", "k3d_host.cpp", "scene_build.cpp", "k3d_noalloc.cu", "k3d_selbst.cu",
+SOURCES = ["k3d_step.cu", "k3d_step_f32.cu", "k3d_build.cu", "k3d_host.cpp", "scene_build.cpp", "k3d_noalloc.cu", "k3d_selbst.cu",
            "k3d_selbst_host.cpp", "k3d_adjoint.cu", "k3d_netz.cu"]
-HEADERS = ["k3d_step.h", "k3d_device.cuh", "k3d_step_common.cuh", "scene_build.h", "k3d_selbst.h",
+HEADERS = ["k3d_step.h", "k3d_device.cuh", "k3d_step_common.cuh", "k3d_solve.cuh", "scene_build.h", "k3d_selbst.h",
            "k3d_selbst_host.h", "k3d_adjoint.h", "k3d_vec.cuh", "k3d_netz.cuh", "k3d_netz.h"]
 # Per-file flags. The build of the system and the self-collision stage round
 # every product and sum on their own (no fused multiply-add), as the
 # reference's arithmetic does: the element term of k3d_build.cu needs it, and
-# the self-collision cell indices, buckets and pairs come out bit-exact. The
+# the self-collision cell indices, buckets and pairs come out bit-exact. So
+# does the PCG with FP64 vectors (k3d_step.cu): its bits then do not depend on
+# the compiler's choice of which products to fuse, and the mesh-body parity
+# tests hold; the FP32-vector PCG (k3d_step_f32.cu) keeps fused products. The
 # adjoint replays the forward's contact queries and rounds the same way; the
 # body mesh's nearest-point regions and distances round as the reference's;
 # the allocation-free operator evaluates the same element products as the build.
-EXTRA = {"k3d_build.cu": ["-fmad=false"], "k3d_selbst.cu": ["-fmad=false"], "k3d_adjoint.cu": ["-fmad=false"],
+EXTRA = {"k3d_step.cu": ["-fmad=false"], "k3d_build.cu": ["-fmad=false"], "k3d_selbst.cu": ["-fmad=false"], "k3d_adjoint.cu": ["-fmad=false"],
          "k3d_netz.cu": ["-fmad=false"], "k3d_noalloc.cu": ["-fmad=false"]}
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -255,6 +255,7 @@ static void carve(k3d_solver* h, Arena& A, size_t N, size_t T, size_t B, size_t 
   a.sync = A.take<SyncState>(1);
   a.partials = A.take<double>(size_t(kPartialsPerBlock) * h->blocks);  // reduction slots
   a.n_grp = h->n_grp;
+  a.solve_threads = h->p.pcg_threads;
   a.grp = cv.grp = A.take<Grp>(size_t(h->n_grp));
   a.blk_grp = cv.blk_grp = A.take<uint32_t>(size_t(h->blocks));
   a.grp_cnt = A.take<unsigned>(size_t(32) * size_t(h->n_grp));
@@ -359,7 +360,12 @@ k3d_solver* k3d_solver_create(const k3d_params* params, int32_t device) {
     h->err = "no CUDA device available";
     return h;  // every later call reports K3D_DEVICE_ERROR
   }
-  h->blocks = step_grid_blocks(h->p.precision, device);
+  if (h->p.pcg_threads == 0) h->p.pcg_threads = kSolveBlock;
+  if (h->p.pcg_threads != 256 && h->p.pcg_threads != 512 && h->p.pcg_threads != 1024) {
+    h->err = "pcg_threads must be 256, 512 or 1024";
+    return h;  // every later call reports K3D_DEVICE_ERROR
+  }
+  h->blocks = step_grid_blocks(h->p.precision, h->p.pcg_threads, device);
   if (h->blocks <= 0) h->err = "cannot size the cooperative grid";
   else if (h->p.pcg_bloecke > 0) h->blocks = std::min(h->blocks, h->p.pcg_bloecke);
   return h;

@@ -8,7 +8,7 @@
 namespace k3d {
 
 constexpr int kBlock = 256;       // ordinary launches
-constexpr int kSolveBlock = 512;  // the persistent PCG launch
+constexpr int kSolveBlock = 512;  // the persistent PCG launch's default CTA size (256 and 1024 also built)
 
 enum Mode : int { MODE_STEP = 0, MODE_SYSTEM = 1, MODE_OPERATOR = 2, MODE_SOLVE = 3, MODE_RESIDUAL = 4 };
 
@@ -154,6 +154,8 @@ struct StepArgs {
   // normal velocity removed
   int adjoint;
   uint32_t* rec_flags;
+  int solve_threads;  // threads per CTA of the persistent PCG launch (256, 512 or 1024)
+  int pad_st;
   // bookkeeping
   cudaEvent_t ev_solve0, ev_solve1;  // around the PCG launch (host-side handles)
   SyncState* sync;
@@ -168,7 +170,9 @@ struct BuildKernels {
 };
 BuildKernels build_kernels(int precision);
 
-int step_grid_blocks(int precision, int device);
+// CTAs of the persistent PCG launch that fit at once (SMs x CTAs per SM) for
+// the form and CTA size (256, 512 or 1024 threads); -1 on error.
+int step_grid_blocks(int precision, int threads, int device);
 // Enqueues one substep (or probe) on `stream`; `launched` = kernels enqueued.
 cudaError_t launch_step(const StepArgs& a, int precision, int blocks, cudaStream_t stream, int& launched);
 // The FP64 PCG launch alone on the system built before (one pass, no release

@@ -30,6 +30,7 @@ class ImplizitParameter:
     precision: int = _abi.K3D_FP64
     pcg_bloecke: int = 0
     graph: bool = False
+    pcg_threads: int = 0
 
     def to_c(self) -> _abi.K3dParams:
         p = _abi.K3dParams()
@@ -50,6 +51,7 @@ class ImplizitParameter:
         p.koerperpunkt_tiefe = self.koerperpunkt_tiefe
         p.pcg_bloecke = self.pcg_bloecke
         p.graph = int(self.graph)
+        p.pcg_threads = self.pcg_threads
         return p
 
 

@@ -72,7 +72,8 @@ typedef struct k3d_params {
                                          when they change, e.g. a moving body); not with self-collision, whose
                                          stage reads counts back between launches. The per-frame PCG time of
                                          k3d_last_solve_ms stays 0 then. Default 0 */
-  int32_t reserved;
+  int32_t pcg_threads;                /* no reference counterpart: threads per CTA of the persistent PCG launch,
+                                         256 (two CTAs per SM), 512 or 1024 (one per SM); 0 (default) = 512 */
 } k3d_params;
 
 /* Simparameter (sim/src/szene.rs:96-126), the part the implicit step reads. */

@@ -1,0 +1,82 @@
+"""Device against oracle at the workloads' full sizes (slow: the oracle is a
+single CPU thread; about two minutes for the sheet and two for the garment).
+
+* The sheet over the sphere, 257 x 257 points (66,049): the device's FP64
+  drop runs to step 36, just after first contact; from that state two steps,
+  each from the device's state, on the device and in the oracle at PCG
+  tolerance 1e-12: equal contact and release counts, positions within 1e-9
+  of the bounding-box diagonal. The chosen form (FP32 operator storage) from
+  the same states stays within 1e-5.
+* The sewn garment, 205,284 points with the self-collision stage on: from
+  the FP64 device state at frame 10, one step on the device and in the
+  oracle at tolerance 1e-10: equal proximity pair, intersection, region and
+  impact counts, positions within 1e-8 of the diagonal.
+
+The step followed is implizit.rs:899-1038 (with selbstkollision.rs for the
+garment's stage); both sides start each compared step without a warm start
+(a new solver), so only the state is shared.
+"""
+import numpy as np
+import pytest
+
+import oracle_py as O
+from garmentcraft_b200 import _abi, synth
+from garmentcraft_b200.implizit import ImplizitCg, build_scene
+from garmentcraft_b200.params import ImplizitParameter
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+
+def diag(x):
+    return float(np.linalg.norm(x.max(0) - x.min(0)))
+
+
+def test_sheet_257_nach_dem_aufprall_wie_orakel():
+    m, body = synth.sheet_over_sphere(n=257, jitter_mm=1.0)
+    s = build_scene(m, [body])
+    vor = ImplizitParameter(schritte_je_bild=1, cg_max=4000, cg_toleranz=1e-5)
+    ImplizitCg(vor).bilder_resident(s, 36)
+    eng = ImplizitParameter(schritte_je_bild=1, cg_max=40000, cg_toleranz=1e-12)
+    o = O.OracleSim(s.copy(), eng.to_c())
+    cg = ImplizitCg(eng)
+    kontakte = 0
+    for k in range(2):
+        o.set_state(s.x, s.v)
+        start = s.copy()
+        cg.bild(s)
+        st = o.frames(1)
+        a = cg.statistik
+        assert (a.kontakte, a.freigegeben) == (st.kontakte, st.freigegeben), k
+        assert not a.nicht_konvergiert and not st.nicht_konvergiert
+        xo, _ = o.state()
+        assert np.max(np.abs(s.x - xo)) <= 1e-9 * diag(xo), k
+        kontakte += a.kontakte
+        # the chosen form from the same state, one step
+        t = start.copy()
+        ImplizitCg(ImplizitParameter(schritte_je_bild=1, cg_max=40000, cg_toleranz=1e-8,
+                                     precision=_abi.K3D_MIXED_STORAGE)).bild(t)
+        assert np.max(np.abs(t.x - xo)) <= 1e-5 * diag(xo), k
+    assert kontakte > 1000  # the sheet is on the sphere
+
+
+def test_garment_205k_mit_selbstkollision_wie_orakel():
+    s, _ = synth.garment_szene()
+    assert s.n > 200_000
+    vor = ImplizitParameter(schritte_je_bild=1, cg_max=4000, cg_toleranz=1e-5, selbstkollision=True)
+    cg0 = ImplizitCg(vor)
+    cg0.zustand_hochladen(s)
+    cg0.bilder_auf_geraet(10)
+    cg0.zustand_lesen(s)
+    eng = ImplizitParameter(schritte_je_bild=1, cg_max=40000, cg_toleranz=1e-10, selbstkollision=True)
+    o = O.OracleSim(s.copy(), eng.to_c())
+    o.set_state(s.x, s.v)
+    cg = ImplizitCg(eng)
+    cg.bild(s)
+    st = o.frames(1)
+    a = cg.statistik
+    for f in ("naehe_punkt_dreieck", "naehe_kante_kante", "durchdringungen", "durchdringungsgebiete",
+              "selbst_stoesse", "kontakte"):
+        assert getattr(a, f) == getattr(st, f), f
+    assert a.naehe_punkt_dreieck + a.naehe_kante_kante > 1000
+    xo, _ = o.state()
+    assert np.max(np.abs(s.x - xo)) <= 1e-8 * diag(xo)
