@@ -260,8 +260,11 @@ def garment_leg(flush, torch, peaks, cpu=True):
     cg.zustand_lesen(s)
     warm = cg.warmstart_lesen()
     ref = s.copy()
-    cg.bilder_auf_geraet(1)
-    cg.zustand_lesen(ref)
+    cr = ImplizitCg(par(0, True), device=torch.cuda.current_device())
+    cr.zustand_hochladen(ref)
+    cr.bilder_auf_geraet(1)
+    cr.zustand_lesen(ref)
+    del cr
     d = float(np.linalg.norm(ref.x.max(0) - ref.x.min(0)))
     err = {}
     for prec in (HEADLINE, 1):
@@ -274,8 +277,8 @@ def garment_leg(flush, torch, peaks, cpu=True):
         err[FORMS[prec][0]] = {"max": float(dx.max() / d), "rms": float(np.sqrt(np.mean(dx ** 2)) / d)}
         del c
     out["one_step_error_vs_fp64"] = {"from": f"the FP64 state at frame {GARMENT_PRE}", "errors": err,
-                                     "definition": "|x_form - x_fp64| / bbox diagonal after one step "
-                                                   "(the FP64 step with its warm start, the forms without)"}
+                                     "definition": "|x_form - x_fp64| / bbox diagonal after one step from the "
+                                                   "same state, every form on a new solver (no warm start)"}
     if cpu:
         O = oracle_mod()
         m, body = synth.garment(ziel_punkte=200_000)
@@ -880,8 +883,12 @@ def main():
             st0 = s0.copy()
             c64.zustand_lesen(st0)
             ref = st0.copy()
+            cr = ImplizitCg(params(0))
+            cr.zustand_hochladen(ref)
+            cr.bilder_auf_geraet(1)
+            cr.zustand_lesen(ref)
+            del cr
             c64.bilder_auf_geraet(1)
-            c64.zustand_lesen(ref)
             d = float(np.linalg.norm(ref.x.max(0) - ref.x.min(0)))
             for prec in (HEADLINE, 1):
                 t = st0.copy()
@@ -907,7 +914,7 @@ def main():
             "speedup": {FORMS[p][0]: t_form[0] / t_form[p] for p in (HEADLINE, 1)} if world == 1 else None,
             "one_step_error": {"at_steps": at, "errors": one,
                                "definition": "|x_form - x_fp64| / bbox diagonal after one step from the same FP64 "
-                                             "state (the FP64 step with its warm start, the forms without)"},
+                                             "state, every form on a new solver (no warm start)"},
             "rel_pos_err_after_100_steps": err100,
             "definition": "max_i |x_form - x_fp64| / bbox diagonal"}
 
