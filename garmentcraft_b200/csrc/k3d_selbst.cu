@@ -520,11 +520,13 @@ __device__ uint32_t punkt_dreieck_gruppe(const SelbstArgs& s, const Gruppe& gr, 
   return je_eintrag_gruppe<FILL, PaarPT>(
       gr, qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, pos,
       [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck, PaarPT& o) -> bool {
+        // the reference's conditions, the cheapest rejection first (each is
+        // a plain condition on the candidate, so the order changes no result)
+        const Box qv = box_of(s.qp_lo, s.qp_hi, v);
+        if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, s.zelle, ci, cj, ck)) return false;
         for (int k = 0; k < 3; ++k)
           if (gleich_oder_partner(s, v, d[k])) return false;
         if (s.w[v] <= 0.0 && alle_fest) return false;
-        const Box qv = box_of(s.qp_lo, s.qp_hi, v);
-        if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, s.zelle, ci, cj, ck)) return false;
         const D3 xv = ld3(s.x, v);
         double ruhe = rt + s.r_punkt[v];
         double eine;
@@ -1147,14 +1149,16 @@ __device__ uint32_t kante_schnitte(const SelbstArgs& s, const Gruppe& gr, int64_
   return je_eintrag_gruppe<FILL, SchnittT>(
       gr, qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, pos,
       [&](uint32_t t, int64_t ci, int64_t cj, int64_t ck, SchnittT& o) -> bool {
+        // the box first: the cheapest rejection (plain conditions, any order)
+        const Box qt = box_of(s.hs.lo, s.hs.hi, t);
+        if (!ueberlappt(qt, qe) || !erste_zelle(qe, qt, zelle, ci, cj, ck)) return false;
         const uint4 d = s.d_idx[t];
         const uint32_t dd[3] = {d.x, d.y, d.z};
         bool nachbar = false;
         for (int k = 0; k < 3; ++k)
           nachbar = nachbar || (s.an_naehten ? (dd[k] == a0 || dd[k] == a1)
                                              : (gleich_oder_partner(s, a0, dd[k]) || gleich_oder_partner(s, a1, dd[k])));
-        const Box qt = box_of(s.hs.lo, s.hs.hi, t);
-        if (nachbar || !ueberlappt(qt, qe) || !erste_zelle(qe, qt, zelle, ci, cj, ck)) return false;
+        if (nachbar) return false;
         const double4 n4 = s.nrm_t[t];
         const D3 n = d3(n4.x, n4.y, n4.z);
         double tk, w[3];
@@ -1591,10 +1595,10 @@ __global__ void __launch_bounds__(kT, 4) stoss_pd_kernel(const __grid_constant__
     bool hat = false;
     double bz = 0.0;
     je_eintrag(qt, z, s.hp2.eimer, s.hp2.anf, s.hp2.ein, [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck) {
-      for (int k = 0; k < 3; ++k)
-        if (gleich_oder_partner(s, v, d[k])) return;
       const Box qv = box_of(s.hp2.lo, s.hp2.hi, v);
       if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, z, ci, cj, ck)) return;
+      for (int k = 0; k < 3; ++k)
+        if (gleich_oder_partner(s, v, d[k])) return;
       const uint32_t idx[4] = {d[0], d[1], d[2], v};
       if (s.w[idx[0]] <= 0.0 && s.w[idx[1]] <= 0.0 && s.w[idx[2]] <= 0.0 && s.w[idx[3]] <= 0.0) return;
       D3 a0[4], a1[4];

@@ -586,8 +586,10 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
       const R4<R>* wR = static_cast<const R4<R>*>(a.sc_wR);
       const R* g5R = static_cast<const R*>(a.sc_g5R);
       R4<V>* out = static_cast<R4<V>*>(a.sc_out);
+      // spring q on thread nth - 1 - q: the springs go to the threads with the
+      // fewest rows first (the rows fill the threads from the grid's start)
       const int64_t nth = int64_t(sh.g.nblk) * blockDim.x;
-      for (int64_t q = int64_t(sh.bidx) * blockDim.x + threadIdx.x; q < int64_t(a.sc_np); q += nth) {
+      for (int64_t q = nth - 1 - (int64_t(sh.bidx) * blockDim.x + threadIdx.x); q < int64_t(a.sc_np); q += nth) {
         const uint4 id = a.sc_idx[q];
         const R4<R> w4 = wR[q];
         const V g[5] = {V(w4.x), V(w4.y), V(w4.z), V(w4.w), V(g5R[q])};
@@ -638,6 +640,7 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
       R4<V> ci[kRows];
       D3 d[kRows];
       V ap[kRows][3], r[kRows][3], nr[kRows][3], pv[kRows][6];
+      uint32_t se[kRows][2];  // the point's proximity-spring entries (SC)
 #pragma unroll
       for (int q = 0; q < kRows; ++q) {  // every load first
         ii[q] = i0 + q * gstride;
@@ -654,6 +657,8 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
         }
 #pragma unroll
         for (int c = 0; c < 6; ++c) pv[q][c] = V(vw.pinv[6 * i + c]);
+        se[q][0] = SC ? a.sc_off[i] : 0u;
+        se[q][1] = SC ? a.sc_off[i + 1] : 0u;
       }
 #pragma unroll
       for (int q = 0; q < kRows; ++q) {
@@ -664,7 +669,7 @@ __device__ bool pcg(const StepArgs& a, const Vec<R, V>& vw, Shared& sh, int64_t&
         if (SC && fr[q]) {  // the point's proximity-spring entries, in list order
           const R4<V>* out = static_cast<const R4<V>*>(a.sc_out);
           V sx = 0, sy = 0, sz = 0;
-          for (uint32_t e = a.sc_off[i]; e < a.sc_off[i + 1]; ++e) {
+          for (uint32_t e = se[q][0]; e < se[q][1]; ++e) {
             const R4<V> t = out[e];
             sx += t.x;
             sy += t.y;

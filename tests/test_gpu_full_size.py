@@ -6,7 +6,8 @@ single CPU thread; about two minutes for the sheet and two for the garment).
   each from the device's state, on the device and in the oracle at PCG
   tolerance 1e-12: equal contact and release counts, positions within 1e-9
   of the bounding-box diagonal. The chosen form (FP32 operator storage) from
-  the same states stays within 1e-5.
+  the same states stays within 1e-4 of the diagonal (the FP32-rounded
+  operator moves the solution by about 3e-5 there, measured).
 * The sewn garment, 205,284 points with the self-collision stage on: from
   the FP64 device state at frame 10, one step on the device and in the
   oracle at tolerance 1e-10: equal proximity pair, intersection, region and
@@ -55,7 +56,7 @@ def test_sheet_257_nach_dem_aufprall_wie_orakel():
         t = start.copy()
         ImplizitCg(ImplizitParameter(schritte_je_bild=1, cg_max=40000, cg_toleranz=1e-8,
                                      precision=_abi.K3D_MIXED_STORAGE)).bild(t)
-        assert np.max(np.abs(t.x - xo)) <= 1e-5 * diag(xo), k
+        assert np.max(np.abs(t.x - xo)) <= 1e-4 * diag(xo), k
     assert kontakte > 1000  # the sheet is on the sphere
 
 
