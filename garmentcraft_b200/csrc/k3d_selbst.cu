@@ -127,18 +127,37 @@ __device__ void je_eimer(const Box& q, double zelle, uint32_t eimer, F&& f) {
   }
 }
 
-// selbstkollision.rs:328-344: f(entry, i, j, k) over the entries of the box's cells
+// A box in FP32 rounded outward (lo down, hi up). Every search below tests
+// ueberlappt(query, entry) in FP64 among its conditions; if the outward FP32
+// boxes do not overlap, the FP64 ones do not either (lo32 <= lo and hi <= hi32),
+// so a candidate that fails the FP32 test is skipped without loading its FP64
+// box, and no result changes.
+struct Box32 {
+  float lx, ly, lz, hx, hy, hz;
+};
+__device__ __forceinline__ Box32 box32(const Box& b) {
+  return {__double2float_rd(b.lo.x), __double2float_rd(b.lo.y), __double2float_rd(b.lo.z),
+          __double2float_ru(b.hi.x), __double2float_ru(b.hi.y), __double2float_ru(b.hi.z)};
+}
+__device__ __forceinline__ bool ueberlappt32(const Box32& q, const float4& l, const float4& h) {
+  return q.lx <= h.x && l.x <= q.hx && q.ly <= h.y && l.y <= q.hy && q.lz <= h.z && l.z <= q.hz;
+}
+
+// selbstkollision.rs:328-344: f(entry, i, j, k) over the entries of the box's
+// cells; entries whose FP32 box (elo, ehi, entry order) misses q are skipped
 template <typename F>
 __device__ void je_eintrag(const Box& q, double zelle, uint32_t eimer, const uint32_t* anf, const uint32_t* ein,
-                           F&& f) {
+                           const float4* elo, const float4* ehi, F&& f) {
   if (!zellbereich_ok(q, zelle)) return;
   const Cells c = cells_of(q, zelle);
+  const Box32 q32 = box32(q);
   for (uint32_t a = 0; a < c.total; ++a) {
     int64_t i, j, k;
     cell_at(c, a, i, j, k);
     const uint32_t h = streue(i, j, k, eimer);
     const uint32_t e1 = anf[h + 1];
-    for (uint32_t s = anf[h]; s < e1; ++s) f(ein[s], i, j, k);
+    for (uint32_t s = anf[h]; s < e1; ++s)
+      if (ueberlappt32(q32, elo[s], ehi[s])) f(ein[s], i, j, k);
   }
 }
 
@@ -159,9 +178,11 @@ __device__ __forceinline__ Gruppe gruppe() {
 }
 template <bool FILL, typename Payload, typename T, typename W>
 __device__ uint32_t je_eintrag_gruppe(const Gruppe& gr, const Box& q, double zelle, uint32_t eimer,
-                                      const uint32_t* anf, const uint32_t* ein, uint32_t pos, T&& pruefe, W&& schreibe) {
+                                      const uint32_t* anf, const uint32_t* ein, const float4* elo, const float4* ehi,
+                                      uint32_t pos, T&& pruefe, W&& schreibe) {
   if (!zellbereich_ok(q, zelle)) return 0;
   const Cells c = cells_of(q, zelle);
+  const Box32 q32 = box32(q);
   const unsigned unter = gr.maske & ((1u << (threadIdx.x & 31)) - 1u);
   uint32_t cnt = 0;
   for (uint32_t a = 0; a < c.total; ++a) {
@@ -172,7 +193,7 @@ __device__ uint32_t je_eintrag_gruppe(const Gruppe& gr, const Box& q, double zel
     for (uint32_t b0 = lo; b0 < hi; b0 += kG) {
       const uint32_t e = b0 + uint32_t(gr.lane);
       Payload pl;
-      const bool hit = e < hi && pruefe(ein[e], i, j, k, pl);
+      const bool hit = e < hi && ueberlappt32(q32, elo[e], ehi[e]) && pruefe(ein[e], i, j, k, pl);
       const unsigned b = __ballot_sync(gr.maske, hit);
       if (FILL && hit) schreibe(pl, pos + cnt + uint32_t(__popc(b & unter)));
       cnt += uint32_t(__popc(b));
@@ -450,6 +471,21 @@ __global__ void __launch_bounds__(kT) lang_sort_kernel(const uint32_t* off, uint
     __syncthreads();
   }
 }
+// The FP32 boxes of a hash's entries, in entry order (after the per-bucket
+// sort), rounded outward: the searches' pre-test (see Box32).
+__global__ void __launch_bounds__(kT) eintrag_boxen_kernel(const uint32_t* anf, uint32_t eimer, uint32_t cap,
+                                                           const uint32_t* ein, const double4* lo, const double4* hi,
+                                                           float4* elo, float4* ehi) {
+  const uint32_t n = anf[eimer] < cap ? anf[eimer] : cap;
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const uint32_t b = ein[q];
+    const double4 l = lo[b], h = hi[b];
+    elo[q] = make_float4(__double2float_rd(l.x), __double2float_rd(l.y), __double2float_rd(l.z), 0.f);
+    ehi[q] = make_float4(__double2float_ru(h.x), __double2float_ru(h.y), __double2float_ru(h.z), 0.f);
+  }
+}
+constexpr unsigned kEintragGrid = 148 * 8;
+
 unsigned grid_lang(int64_t nb) {
   const int64_t b = (nb + kT - 1) / kT;
   return unsigned(b < 1 ? 1 : (b > 148 * 4 ? 148 * 4 : b));
@@ -518,7 +554,7 @@ __device__ uint32_t punkt_dreieck_gruppe(const SelbstArgs& s, const Gruppe& gr, 
   const double sg[3] = {dot(p[2] - p[0], en[0]), dot(p[0] - p[1], en[1]), dot(p[1] - p[2], en[2])};
   const bool alle_fest = s.w[i0] <= 0.0 && s.w[i1] <= 0.0 && s.w[i2] <= 0.0;
   return je_eintrag_gruppe<FILL, PaarPT>(
-      gr, qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, pos,
+      gr, qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, s.ebp_lo, s.ebp_hi, pos,
       [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck, PaarPT& o) -> bool {
         // the reference's conditions, the cheapest rejection first (each is
         // a plain condition on the candidate, so the order changes no result)
@@ -574,7 +610,7 @@ __device__ uint32_t kante_kante_gruppe(const SelbstArgs& s, const Gruppe& gr, in
   const D3 pa0 = ld3(s.x, a0), pa1 = ld3(s.x, a1);
   const Box qe = box_of(s.qk_lo, s.qk_hi, e);
   return je_eintrag_gruppe<FILL, PaarKK>(
-      gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, pos,
+      gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, s.ebk_lo, s.ebk_hi, pos,
       [&](uint32_t f, int64_t ci, int64_t cj, int64_t ck, PaarKK& o) -> bool {
         if (int64_t(f) <= e) return false;
         const Box qf = box_of(s.qk_lo, s.qk_hi, f);
@@ -1147,7 +1183,7 @@ __device__ uint32_t kante_schnitte(const SelbstArgs& s, const Gruppe& gr, int64_
   const Box qe = quader_punkte(pe, 2, kZuschlagQuader);
   const D3 ehat = einheit(pb - pa);
   return je_eintrag_gruppe<FILL, SchnittT>(
-      gr, qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, pos,
+      gr, qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, s.hs.elo, s.hs.ehi, pos,
       [&](uint32_t t, int64_t ci, int64_t cj, int64_t ck, SchnittT& o) -> bool {
         // the box first: the cheapest rejection (plain conditions, any order)
         const Box qt = box_of(s.hs.lo, s.hs.hi, t);
@@ -1594,7 +1630,8 @@ __global__ void __launch_bounds__(kT, 4) stoss_pd_kernel(const __grid_constant__
     const Box qt = box_of(s.qt2_lo, s.qt2_hi, t);
     bool hat = false;
     double bz = 0.0;
-    je_eintrag(qt, z, s.hp2.eimer, s.hp2.anf, s.hp2.ein, [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck) {
+    je_eintrag(qt, z, s.hp2.eimer, s.hp2.anf, s.hp2.ein, s.hp2.elo, s.hp2.ehi,
+               [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck) {
       const Box qv = box_of(s.hp2.lo, s.hp2.hi, v);
       if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, z, ci, cj, ck)) return;
       for (int k = 0; k < 3; ++k)
@@ -1638,7 +1675,8 @@ __global__ void __launch_bounds__(kT, 4) stoss_kk_kernel(const __grid_constant__
     const Box qi = box_of(s.hk2.lo, s.hk2.hi, i);
     bool hat = false;
     double bz = 0.0;
-    je_eintrag(qi, z, s.hk2.eimer, s.hk2.anf, s.hk2.ein, [&](uint32_t j, int64_t ci, int64_t cj, int64_t ck) {
+    je_eintrag(qi, z, s.hk2.eimer, s.hk2.anf, s.hk2.ein, s.hk2.elo, s.hk2.ehi,
+               [&](uint32_t j, int64_t ci, int64_t cj, int64_t ck) {
       if (int64_t(j) <= i) return;
       const Box qj = box_of(s.hk2.lo, s.hk2.hi, j);
       if (!ueberlappt(qi, qj) || !erste_zelle(qi, qj, z, ci, cj, ck)) return;
@@ -1861,8 +1899,10 @@ cudaError_t exclusive_scan_u32(uint32_t* data, int64_t n, uint32_t* tmp, uint32_
 }
 // normals, boxes; 2 scans, fill, sort, count, 2 scans; fill, springs, damping,
 // count, scan, fill, sort
-int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3) + 6 + 4; }
-int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1 + 3; }
+// (+3 and +2: the entry boxes of the point, edge and triangle hashes and of
+// the two path hashes)
+int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3) + 6 + 4 + 3; }
+int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1 + 3 + 2; }
 
 // Impacts, part 1 (selbstkollision.rs:1196-1203): the longest edge at x1, the
 // path boxes, the bucket counts of the point and edge path hashes. The host
@@ -1890,6 +1930,10 @@ cudaError_t selbst_stoss_antwort(const SelbstArgs& s, int iterationen, unsigned 
   lang_sort_kernel<<<grid_lang(s.hp2.eimer), kT, 0, st>>>(s.hp2.anf, s.hp2.ein, s.hp2.eimer);
   hg_sort_kernel<<<grid_for(s.hk2.eimer), kT, 0, st>>>(s.hk2);
   lang_sort_kernel<<<grid_lang(s.hk2.eimer), kT, 0, st>>>(s.hk2.anf, s.hk2.ein, s.hk2.eimer);
+  eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.hp2.anf, s.hp2.eimer, s.hp2.cap, s.hp2.ein, s.hp2.lo, s.hp2.hi,
+                                                    s.hp2.elo, s.hp2.ehi);
+  eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.hk2.anf, s.hk2.eimer, s.hk2.cap, s.hk2.ein, s.hk2.lo, s.hk2.hi,
+                                                    s.hk2.elo, s.hk2.ehi);
   stoss_pd_kernel<<<grid_for(s.nd), kT, 0, st>>>(s);
   stoss_kk_kernel<<<grid_for(s.ne), kT, 0, st>>>(s);
   stoss_filter_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
@@ -1930,6 +1974,10 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   bucket_sort_kernel<<<grid_for(s.eimer_p > s.eimer_k ? s.eimer_p : s.eimer_k), kT, 0, st>>>(s);
   lang_sort_kernel<<<grid_lang(s.eimer_p), kT, 0, st>>>(s.anf_p, s.ein_p, s.eimer_p);
   lang_sort_kernel<<<grid_lang(s.eimer_k), kT, 0, st>>>(s.anf_k, s.ein_k, s.eimer_k);
+  eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.anf_p, s.eimer_p, s.cap_ep, s.ein_p, s.qp_lo, s.qp_hi, s.ebp_lo,
+                                                    s.ebp_hi);
+  eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.anf_k, s.eimer_k, s.cap_ek, s.ein_k, s.qk_lo, s.qk_hi, s.ebk_lo,
+                                                    s.ebk_hi);
   pairs_count_kernel<<<grid_for(kG * (s.nd > s.ne ? s.nd : s.ne)), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = scan(s.off_t, s.nd + 1, s.scan_tmp, &s.zahl[SZ_PAARE_PT], st)) != cudaSuccess) return e;
@@ -1945,6 +1993,8 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   hg_fill_kernel<<<grid_for(s.nd), kT, 0, st>>>(s.hs, &s.lmax[0]);
   hg_sort_kernel<<<grid_for(s.hs.eimer), kT, 0, st>>>(s.hs);
   lang_sort_kernel<<<grid_lang(s.hs.eimer), kT, 0, st>>>(s.hs.anf, s.hs.ein, s.hs.eimer);
+  eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.hs.anf, s.hs.eimer, s.hs.cap, s.hs.ein, s.hs.lo, s.hs.hi, s.hs.elo,
+                                                    s.hs.ehi);
   schnitt_count_kernel<<<grid_for(kG * s.ne), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return scan(s.off_s, s.ne + 1, s.scan_tmp, &s.zahl[SZ_SCHNITTE], st);

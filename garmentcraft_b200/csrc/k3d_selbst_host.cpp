@@ -257,6 +257,8 @@ cudaError_t selbst_upload(SelbstHost& H, const k3d_scene* sc, double zusatzdicke
   // a cell), so 8 buckets per point bound the point hash
   s.cap_ep = uint32_t(std::min<int64_t>(8 * std::max<int64_t>(n, 1), int64_t(0xffffffffu)));
   if ((e = alloc(s.ein_p, size_t(s.cap_ep), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.ebp_lo, size_t(s.cap_ep), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.ebp_hi, size_t(s.cap_ep), H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.off_t, size_t(nd) + 1, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.off_e, size_t(ne) + 1, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.aktiv_p, size_t(nd) + size_t(ne) + 1, H.fest)) != cudaSuccess) return e;
@@ -277,6 +279,8 @@ cudaError_t selbst_upload(SelbstHost& H, const k3d_scene* sc, double zusatzdicke
   if ((e = alloc(s.hs.anf, size_t(s.hs.eimer) + 1, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.hs.cur, size_t(s.hs.eimer), H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.hs.ein, size_t(s.hs.cap), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hs.elo, size_t(s.hs.cap), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.hs.ehi, size_t(s.hs.cap), H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.lmax, 2, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.off_s, size_t(ne) + 1, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.aktiv_s, size_t(ne) + 1, H.fest)) != cudaSuccess) return e;
@@ -368,12 +372,19 @@ cudaError_t selbst_grow_wege(SelbstHost& H, uint32_t cap_p, uint32_t cap_k) {
   H.s.hp2.cap = cap_p;
   H.s.hk2.cap = cap_k;
   if ((e = alloc(H.s.hp2.ein, size_t(cap_p), H.wege)) != cudaSuccess) return e;
+  if ((e = alloc(H.s.hp2.elo, size_t(cap_p), H.wege)) != cudaSuccess) return e;
+  if ((e = alloc(H.s.hp2.ehi, size_t(cap_p), H.wege)) != cudaSuccess) return e;
+  if ((e = alloc(H.s.hk2.elo, size_t(cap_k), H.wege)) != cudaSuccess) return e;
+  if ((e = alloc(H.s.hk2.ehi, size_t(cap_k), H.wege)) != cudaSuccess) return e;
   return alloc(H.s.hk2.ein, size_t(cap_k), H.wege);
 }
 
 cudaError_t selbst_grow_edge_hash(SelbstHost& H, uint32_t cap) {
   free_all(H.hashk);
   H.s.cap_ek = cap;
+  cudaError_t e;
+  if ((e = alloc(H.s.ebk_lo, size_t(cap), H.hashk)) != cudaSuccess) return e;
+  if ((e = alloc(H.s.ebk_hi, size_t(cap), H.hashk)) != cudaSuccess) return e;
   return alloc(H.s.ein_k, size_t(cap), H.hashk);
 }
 
