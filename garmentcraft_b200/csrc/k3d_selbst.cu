@@ -144,7 +144,11 @@ __device__ __forceinline__ bool ueberlappt32(const Box32& q, const float4& l, co
 }
 
 // selbstkollision.rs:328-344: f(entry, i, j, k) over the entries of the box's
-// cells; entries whose FP32 box (elo, ehi, entry order) misses q are skipped
+// cells. With entry boxes (elo, ehi: FP32, entry order) an entry whose box
+// misses q is skipped; without (null), every entry goes to f. The pre-test
+// pays where the box test is the search's first condition; where a cheaper
+// test on the entry's index comes first (edge against later edge) it costs
+// more than it saves (measured), and those searches pass null.
 template <typename F>
 __device__ void je_eintrag(const Box& q, double zelle, uint32_t eimer, const uint32_t* anf, const uint32_t* ein,
                            const float4* elo, const float4* ehi, F&& f) {
@@ -157,7 +161,7 @@ __device__ void je_eintrag(const Box& q, double zelle, uint32_t eimer, const uin
     const uint32_t h = streue(i, j, k, eimer);
     const uint32_t e1 = anf[h + 1];
     for (uint32_t s = anf[h]; s < e1; ++s)
-      if (ueberlappt32(q32, elo[s], ehi[s])) f(ein[s], i, j, k);
+      if (!elo || ueberlappt32(q32, elo[s], ehi[s])) f(ein[s], i, j, k);
   }
 }
 
@@ -193,7 +197,7 @@ __device__ uint32_t je_eintrag_gruppe(const Gruppe& gr, const Box& q, double zel
     for (uint32_t b0 = lo; b0 < hi; b0 += kG) {
       const uint32_t e = b0 + uint32_t(gr.lane);
       Payload pl;
-      const bool hit = e < hi && ueberlappt32(q32, elo[e], ehi[e]) && pruefe(ein[e], i, j, k, pl);
+      const bool hit = e < hi && (!elo || ueberlappt32(q32, elo[e], ehi[e])) && pruefe(ein[e], i, j, k, pl);
       const unsigned b = __ballot_sync(gr.maske, hit);
       if (FILL && hit) schreibe(pl, pos + cnt + uint32_t(__popc(b & unter)));
       cnt += uint32_t(__popc(b));
@@ -453,19 +457,55 @@ __device__ __forceinline__ void lang_sortieren(uint32_t* a, uint32_t lo, uint32_
   for (uint32_t i = threadIdx.x; i < n; i += kT) a[lo + i] = sh[i];
   __syncthreads();
 }
+// a range of up to kWarpSort entries by one warp: bitonic in the warp's part
+// of shared memory
+constexpr uint32_t kWarpSort = 256;
+__device__ __forceinline__ void warp_sortieren(uint32_t* a, uint32_t lo, uint32_t hi, uint32_t* sh) {
+  const uint32_t n = hi - lo, lane = threadIdx.x & 31;
+  uint32_t m = 1;
+  while (m < n) m <<= 1;
+  for (uint32_t i = lane; i < m; i += 32) sh[i] = i < n ? a[lo + i] : 0xffffffffu;
+  __syncwarp();
+  for (uint32_t k = 2; k <= m; k <<= 1)
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = lane; i < m; i += 32) {
+        const uint32_t p = i ^ j;
+        if (p > i) {
+          const bool auf = (i & k) == 0;
+          const uint32_t x = sh[i], y = sh[p];
+          if ((x > y) == auf) sh[i] = y, sh[p] = x;
+        }
+      }
+      __syncwarp();
+    }
+  for (uint32_t i = lane; i < n; i += 32) a[lo + i] = sh[i];
+  __syncwarp();
+}
+// The ranges longer than kKurzSort of kT buckets at a time: those up to
+// kWarpSort entries one per warp, side by side; the longer ones by the whole
+// block, one after another.
 __global__ void __launch_bounds__(kT) lang_sort_kernel(const uint32_t* off, uint32_t* a, int64_t nb) {
   __shared__ uint32_t sh[kLangSort];
   __shared__ uint32_t lang[kT];
-  __shared__ uint32_t zahl;
+  __shared__ uint32_t zahl, gross;
+  uint32_t* wsh = sh + (threadIdx.x >> 5) * kWarpSort;  // kT / 32 warps x kWarpSort <= kLangSort
   for (int64_t base = int64_t(blockIdx.x) * kT; base < nb; base += int64_t(gridDim.x) * kT) {
-    if (threadIdx.x == 0) zahl = 0;
+    if (threadIdx.x == 0) zahl = gross = 0;
     __syncthreads();
     const int64_t b = base + threadIdx.x;
-    if (b < nb && off[b + 1] - off[b] > kKurzSort) lang[atomicAdd(&zahl, 1u)] = threadIdx.x;
+    const uint32_t len = b < nb ? off[b + 1] - off[b] : 0u;
+    if (len > kKurzSort && len <= kWarpSort) lang[atomicAdd(&zahl, 1u)] = threadIdx.x;
     __syncthreads();
     const uint32_t m = zahl;
-    for (uint32_t q = 0; q < m; ++q) {
+    if (len > kWarpSort) lang[kT - 1 - atomicAdd(&gross, 1u)] = threadIdx.x;  // from the list's other end
+    for (uint32_t q = threadIdx.x >> 5; q < m; q += kT / 32) {
       const int64_t bq = base + lang[q];
+      warp_sortieren(a, off[bq], off[bq + 1], wsh);
+    }
+    __syncthreads();
+    const uint32_t g = gross;
+    for (uint32_t q = 0; q < g; ++q) {
+      const int64_t bq = base + lang[kT - 1 - q];
       lang_sortieren(a, off[bq], off[bq + 1], sh);
     }
     __syncthreads();
@@ -610,7 +650,7 @@ __device__ uint32_t kante_kante_gruppe(const SelbstArgs& s, const Gruppe& gr, in
   const D3 pa0 = ld3(s.x, a0), pa1 = ld3(s.x, a1);
   const Box qe = box_of(s.qk_lo, s.qk_hi, e);
   return je_eintrag_gruppe<FILL, PaarKK>(
-      gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, s.ebk_lo, s.ebk_hi, pos,
+      gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, nullptr, nullptr, pos,
       [&](uint32_t f, int64_t ci, int64_t cj, int64_t ck, PaarKK& o) -> bool {
         if (int64_t(f) <= e) return false;
         const Box qf = box_of(s.qk_lo, s.qk_hi, f);
@@ -1675,7 +1715,7 @@ __global__ void __launch_bounds__(kT, 4) stoss_kk_kernel(const __grid_constant__
     const Box qi = box_of(s.hk2.lo, s.hk2.hi, i);
     bool hat = false;
     double bz = 0.0;
-    je_eintrag(qi, z, s.hk2.eimer, s.hk2.anf, s.hk2.ein, s.hk2.elo, s.hk2.ehi,
+    je_eintrag(qi, z, s.hk2.eimer, s.hk2.anf, s.hk2.ein, nullptr, nullptr,
                [&](uint32_t j, int64_t ci, int64_t cj, int64_t ck) {
       if (int64_t(j) <= i) return;
       const Box qj = box_of(s.hk2.lo, s.hk2.hi, j);
@@ -1899,10 +1939,10 @@ cudaError_t exclusive_scan_u32(uint32_t* data, int64_t n, uint32_t* tmp, uint32_
 }
 // normals, boxes; 2 scans, fill, sort, count, 2 scans; fill, springs, damping,
 // count, scan, fill, sort
-// (+3 and +2: the entry boxes of the point, edge and triangle hashes and of
-// the two path hashes)
-int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3) + 6 + 4 + 3; }
-int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1 + 3 + 2; }
+// (+2 and +1: the entry boxes of the point and triangle hashes and of the
+// point path hash)
+int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3) + 6 + 4 + 2; }
+int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1 + 3 + 1; }
 
 // Impacts, part 1 (selbstkollision.rs:1196-1203): the longest edge at x1, the
 // path boxes, the bucket counts of the point and edge path hashes. The host
@@ -1932,8 +1972,6 @@ cudaError_t selbst_stoss_antwort(const SelbstArgs& s, int iterationen, unsigned 
   lang_sort_kernel<<<grid_lang(s.hk2.eimer), kT, 0, st>>>(s.hk2.anf, s.hk2.ein, s.hk2.eimer);
   eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.hp2.anf, s.hp2.eimer, s.hp2.cap, s.hp2.ein, s.hp2.lo, s.hp2.hi,
                                                     s.hp2.elo, s.hp2.ehi);
-  eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.hk2.anf, s.hk2.eimer, s.hk2.cap, s.hk2.ein, s.hk2.lo, s.hk2.hi,
-                                                    s.hk2.elo, s.hk2.ehi);
   stoss_pd_kernel<<<grid_for(s.nd), kT, 0, st>>>(s);
   stoss_kk_kernel<<<grid_for(s.ne), kT, 0, st>>>(s);
   stoss_filter_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
@@ -1976,8 +2014,6 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   lang_sort_kernel<<<grid_lang(s.eimer_k), kT, 0, st>>>(s.anf_k, s.ein_k, s.eimer_k);
   eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.anf_p, s.eimer_p, s.cap_ep, s.ein_p, s.qp_lo, s.qp_hi, s.ebp_lo,
                                                     s.ebp_hi);
-  eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.anf_k, s.eimer_k, s.cap_ek, s.ein_k, s.qk_lo, s.qk_hi, s.ebk_lo,
-                                                    s.ebk_hi);
   pairs_count_kernel<<<grid_for(kG * (s.nd > s.ne ? s.nd : s.ne)), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = scan(s.off_t, s.nd + 1, s.scan_tmp, &s.zahl[SZ_PAARE_PT], st)) != cudaSuccess) return e;
