@@ -1616,8 +1616,31 @@ __global__ void __launch_bounds__(kT) weg_boxen_kernel(const __grid_constant__ S
 }
 
 __device__ __forceinline__ double ebenenabstand(D3 a, D3 b, D3 c, D3 p) { return dot(p - a, einheit(cross(b - a, c - a))); }
+// Whether the unnormalised triple product (p - a).((b - a) x (c - a)) has the
+// same strict sign at the step's start and end, far enough from zero that the
+// reference's ebenenabstand (the same product divided by |(b - a) x (c - a)|,
+// which then exceeds its 1e-12 floor) has that sign too. The margin 1e-12 of
+// the product of the operands' L1 norms is far above the rounding of either
+// form. True means f(0) f(1) > 0, so koplanar_zeit returns false at once; it
+// saves the two square roots and divisions of that test.
+__device__ __forceinline__ double tripel(const D3 q[4], double& grenze, double& n2) {
+  const D3 u = q[1] - q[0], v = q[2] - q[0], w = q[3] - q[0];
+  const D3 c = cross(u, v);
+  n2 = dot(c, c);
+  auto l1 = [](D3 a) { return fabs(a.x) + fabs(a.y) + fabs(a.z); };
+  grenze = 1e-12 * l1(w) * l1(u) * l1(v);
+  return dot(w, c);
+}
+__device__ __forceinline__ bool gleiche_seite(const D3 x0[4], const D3 x1[4]) {
+  double g0, g1, n0, n1;
+  const double t0 = tripel(x0, g0, n0), t1 = tripel(x1, g1, n1);
+  const double n_min = 1.0000001e-24;  // |cross| clearly above einheit's 1e-12 floor
+  return n0 > n_min && n1 > n_min && fabs(t0) > g0 && fabs(t1) > g1 && ((t0 > 0.0) == (t1 > 0.0));
+}
+
 // selbstkollision.rs:1128-1153 (regula falsi, 16 steps)
 __device__ bool koplanar_zeit(const D3 x0[4], const D3 x1[4], double tol, double& out) {
+  if (gleiche_seite(x0, x1)) return false;
   auto f = [&](double t) {
     return ebenenabstand(lerp3(x0[0], x1[0], t), lerp3(x0[1], x1[1], t), lerp3(x0[2], x1[2], t),
                          lerp3(x0[3], x1[3], t));
