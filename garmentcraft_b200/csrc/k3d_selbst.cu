@@ -143,12 +143,12 @@ __device__ __forceinline__ bool ueberlappt32(const Box32& q, const float4& l, co
   return q.lx <= h.x && l.x <= q.hx && q.ly <= h.y && l.y <= q.hy && q.lz <= h.z && l.z <= q.hz;
 }
 
-// selbstkollision.rs:328-344: f(entry, i, j, k) over the entries of the box's
-// cells. With entry boxes (elo, ehi: FP32, entry order) an entry whose box
-// misses q is skipped; without (null), every entry goes to f. The pre-test
-// pays where the box test is the search's first condition; where a cheaper
-// test on the entry's index comes first (edge against later edge) it costs
-// more than it saves (measured), and those searches pass null.
+// selbstkollision.rs:328-344: f(entry, i, j, k, position) over the entries of
+// the box's cells. With entry boxes (elo, ehi: FP32, entry order) an entry
+// whose box misses q is skipped; without (null), every entry goes to f. The
+// pre-test pays where the box test is the search's first condition; where a
+// cheaper test on the entry's index comes first (edge against later edge), f
+// makes the pre-test itself after that test, from the entry's position.
 template <typename F>
 __device__ void je_eintrag(const Box& q, double zelle, uint32_t eimer, const uint32_t* anf, const uint32_t* ein,
                            const float4* elo, const float4* ehi, F&& f) {
@@ -161,7 +161,7 @@ __device__ void je_eintrag(const Box& q, double zelle, uint32_t eimer, const uin
     const uint32_t h = streue(i, j, k, eimer);
     const uint32_t e1 = anf[h + 1];
     for (uint32_t s = anf[h]; s < e1; ++s)
-      if (!elo || ueberlappt32(q32, elo[s], ehi[s])) f(ein[s], i, j, k);
+      if (!elo || ueberlappt32(q32, elo[s], ehi[s])) f(ein[s], i, j, k, s);
   }
 }
 
@@ -400,7 +400,8 @@ __global__ void __launch_bounds__(kT) hash_fill_kernel(const __grid_constant__ S
 // so any sort gives the same result. Ranges of up to kKurzSort entries are
 // sorted by one thread each (insertion sort); longer ones by a block each
 // (lang_sort_kernel), so that a crowded bucket does not stall its thread.
-constexpr uint32_t kKurzSort = 32, kLangSort = 4096;
+constexpr uint32_t kKurzSort = 32, kLangSort = 16384;
+constexpr size_t kLangSortSmem = sizeof(uint32_t) * kLangSort;  // dynamic shared memory of lang_sort_kernel
 __device__ __forceinline__ void sort_range(uint32_t* a, uint32_t lo, uint32_t hi) {
   if (hi - lo < 2 || hi - lo > kKurzSort) return;
   for (uint32_t i = lo + 1; i < hi; ++i) {
@@ -413,10 +414,9 @@ __device__ __forceinline__ void sort_range(uint32_t* a, uint32_t lo, uint32_t hi
     a[j] = key;
   }
 }
-// ranges [off[b], off[b + 1]) longer than kKurzSort: bitonic in shared memory
-// up to kLangSort entries, Shell sort (Ciura's gaps) on one thread beyond. The
-// block checks kT ranges at a time for length and sorts the long ones of that
-// chunk one after another.
+// ranges [off[b], off[b + 1]) longer than kWarpSort: bitonic in the block's
+// dynamic shared memory up to kLangSort entries (a path hash of the garment
+// has buckets of 5-6k entries), Shell sort (Ciura's gaps) on one thread beyond.
 __device__ __forceinline__ void lang_sortieren(uint32_t* a, uint32_t lo, uint32_t hi, uint32_t* sh) {
   const uint32_t n = hi - lo;
   if (n > kLangSort) {
@@ -485,7 +485,7 @@ __device__ __forceinline__ void warp_sortieren(uint32_t* a, uint32_t lo, uint32_
 // kWarpSort entries one per warp, side by side; the longer ones by the whole
 // block, one after another.
 __global__ void __launch_bounds__(kT) lang_sort_kernel(const uint32_t* off, uint32_t* a, int64_t nb) {
-  __shared__ uint32_t sh[kLangSort];
+  extern __shared__ uint32_t sh[];  // kLangSort entries
   __shared__ uint32_t lang[kT];
   __shared__ uint32_t zahl, gross;
   uint32_t* wsh = sh + (threadIdx.x >> 5) * kWarpSort;  // kT / 32 warps x kWarpSort <= kLangSort
@@ -526,6 +526,19 @@ __global__ void __launch_bounds__(kT) eintrag_boxen_kernel(const uint32_t* anf, 
 }
 constexpr unsigned kEintragGrid = 148 * 8;
 
+unsigned grid_lang(int64_t nb);
+// lang_sort_kernel over nb ranges with its shared memory (set once per process)
+cudaError_t lang_sort(const uint32_t* off, uint32_t* a, int64_t nb, cudaStream_t st) {
+  static bool gesetzt = false;
+  if (!gesetzt) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(lang_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kLangSortSmem));
+    if (e != cudaSuccess) return e;
+    gesetzt = true;
+  }
+  lang_sort_kernel<<<grid_lang(nb), kT, kLangSortSmem, st>>>(off, a, nb);
+  return cudaSuccess;
+}
 unsigned grid_lang(int64_t nb) {
   const int64_t b = (nb + kT - 1) / kT;
   return unsigned(b < 1 ? 1 : (b > 148 * 4 ? 148 * 4 : b));
@@ -1694,7 +1707,7 @@ __global__ void __launch_bounds__(kT, 4) stoss_pd_kernel(const __grid_constant__
     bool hat = false;
     double bz = 0.0;
     je_eintrag(qt, z, s.hp2.eimer, s.hp2.anf, s.hp2.ein, s.hp2.elo, s.hp2.ehi,
-               [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck) {
+               [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck, uint32_t) {
       const Box qv = box_of(s.hp2.lo, s.hp2.hi, v);
       if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, z, ci, cj, ck)) return;
       for (int k = 0; k < 3; ++k)
@@ -1738,9 +1751,11 @@ __global__ void __launch_bounds__(kT, 4) stoss_kk_kernel(const __grid_constant__
     const Box qi = box_of(s.hk2.lo, s.hk2.hi, i);
     bool hat = false;
     double bz = 0.0;
+    const Box32 qi32 = box32(qi);
     je_eintrag(qi, z, s.hk2.eimer, s.hk2.anf, s.hk2.ein, nullptr, nullptr,
-               [&](uint32_t j, int64_t ci, int64_t cj, int64_t ck) {
+               [&](uint32_t j, int64_t ci, int64_t cj, int64_t ck, uint32_t sq) {
       if (int64_t(j) <= i) return;
+      if (!ueberlappt32(qi32, s.hk2.elo[sq], s.hk2.ehi[sq])) return;
       const Box qj = box_of(s.hk2.lo, s.hk2.hi, j);
       if (!ueberlappt(qi, qj) || !erste_zelle(qi, qj, z, ci, cj, ck)) return;
       const uint2 kj = s.k_idx[j];
@@ -1962,10 +1977,10 @@ cudaError_t exclusive_scan_u32(uint32_t* data, int64_t n, uint32_t* tmp, uint32_
 }
 // normals, boxes; 2 scans, fill, sort, count, 2 scans; fill, springs, damping,
 // count, scan, fill, sort
-// (+2 and +1: the entry boxes of the point and triangle hashes and of the
-// point path hash)
+// (+2 and +2: the entry boxes of the point and triangle hashes and of the
+// two path hashes)
 int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3) + 6 + 4 + 2; }
-int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1 + 3 + 1; }
+int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1 + 3 + 2; }
 
 // Impacts, part 1 (selbstkollision.rs:1196-1203): the longest edge at x1, the
 // path boxes, the bucket counts of the point and edge path hashes. The host
@@ -1990,11 +2005,13 @@ cudaError_t selbst_stoss_antwort(const SelbstArgs& s, int iterationen, unsigned 
   hg_fill_kernel<<<grid_for(s.n), kT, 0, st>>>(s.hp2, &s.lmax[1]);
   hg_fill_kernel<<<grid_for(s.ne), kT, 0, st>>>(s.hk2, &s.lmax[1]);
   hg_sort_kernel<<<grid_for(s.hp2.eimer), kT, 0, st>>>(s.hp2);
-  lang_sort_kernel<<<grid_lang(s.hp2.eimer), kT, 0, st>>>(s.hp2.anf, s.hp2.ein, s.hp2.eimer);
+  if ((e = lang_sort(s.hp2.anf, s.hp2.ein, s.hp2.eimer, st)) != cudaSuccess) return e;
   hg_sort_kernel<<<grid_for(s.hk2.eimer), kT, 0, st>>>(s.hk2);
-  lang_sort_kernel<<<grid_lang(s.hk2.eimer), kT, 0, st>>>(s.hk2.anf, s.hk2.ein, s.hk2.eimer);
+  if ((e = lang_sort(s.hk2.anf, s.hk2.ein, s.hk2.eimer, st)) != cudaSuccess) return e;
   eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.hp2.anf, s.hp2.eimer, s.hp2.cap, s.hp2.ein, s.hp2.lo, s.hp2.hi,
                                                     s.hp2.elo, s.hp2.ehi);
+  eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.hk2.anf, s.hk2.eimer, s.hk2.cap, s.hk2.ein, s.hk2.lo, s.hk2.hi,
+                                                    s.hk2.elo, s.hk2.ehi);
   stoss_pd_kernel<<<grid_for(s.nd), kT, 0, st>>>(s);
   stoss_kk_kernel<<<grid_for(s.ne), kT, 0, st>>>(s);
   stoss_filter_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
@@ -2006,7 +2023,7 @@ cudaError_t selbst_stoss_antwort(const SelbstArgs& s, int iterationen, unsigned 
   if ((e = scan(s.im_off, s.n + 1, s.scan_tmp, nullptr, st)) != cudaSuccess) return e;
   im_fill_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
   im_sort_kernel<<<grid_for(s.n), kT, 0, st>>>(s);
-  lang_sort_kernel<<<grid_lang(s.n), kT, 0, st>>>(s.im_off, s.im_ent, s.n);
+  if ((e = lang_sort(s.im_off, s.im_ent, s.n, st)) != cudaSuccess) return e;
   for (int it = 0; it < iterationen; ++it) {
     antwort_a_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
     antwort_b_kernel<<<grid_for(s.n), kT, 0, st>>>(s);
@@ -2033,8 +2050,8 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   if ((e = scan(s.anf_k, int64_t(s.eimer_k) + 1, s.scan_tmp, nullptr, st)) != cudaSuccess) return e;
   hash_fill_kernel<<<grid_for(s.n > s.ne ? s.n : s.ne), kT, 0, st>>>(s);
   bucket_sort_kernel<<<grid_for(s.eimer_p > s.eimer_k ? s.eimer_p : s.eimer_k), kT, 0, st>>>(s);
-  lang_sort_kernel<<<grid_lang(s.eimer_p), kT, 0, st>>>(s.anf_p, s.ein_p, s.eimer_p);
-  lang_sort_kernel<<<grid_lang(s.eimer_k), kT, 0, st>>>(s.anf_k, s.ein_k, s.eimer_k);
+  if ((e = lang_sort(s.anf_p, s.ein_p, s.eimer_p, st)) != cudaSuccess) return e;
+  if ((e = lang_sort(s.anf_k, s.ein_k, s.eimer_k, st)) != cudaSuccess) return e;
   eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.anf_p, s.eimer_p, s.cap_ep, s.ein_p, s.qp_lo, s.qp_hi, s.ebp_lo,
                                                     s.ebp_hi);
   pairs_count_kernel<<<grid_for(kG * (s.nd > s.ne ? s.nd : s.ne)), kT, 0, st>>>(s);
@@ -2051,7 +2068,7 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   if ((e = scan(s.hs.anf, int64_t(s.hs.eimer) + 1, s.scan_tmp, nullptr, st)) != cudaSuccess) return e;
   hg_fill_kernel<<<grid_for(s.nd), kT, 0, st>>>(s.hs, &s.lmax[0]);
   hg_sort_kernel<<<grid_for(s.hs.eimer), kT, 0, st>>>(s.hs);
-  lang_sort_kernel<<<grid_lang(s.hs.eimer), kT, 0, st>>>(s.hs.anf, s.hs.ein, s.hs.eimer);
+  if ((e = lang_sort(s.hs.anf, s.hs.ein, s.hs.eimer, st)) != cudaSuccess) return e;
   eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.hs.anf, s.hs.eimer, s.hs.cap, s.hs.ein, s.hs.lo, s.hs.hi, s.hs.elo,
                                                     s.hs.ehi);
   schnitt_count_kernel<<<grid_for(kG * s.ne), kT, 0, st>>>(s);
@@ -2112,7 +2129,7 @@ cudaError_t selbst_paare_und_federn(const SelbstArgs& s, uint32_t n_aktiv_p, uin
   if ((e = scan(s.inc_off, s.n + 1, s.scan_tmp, &s.zahl[SZ_INZIDENZ], st)) != cudaSuccess) return e;
   inc_fill_kernel<<<grid_for(pmax), kT, 0, st>>>(s);
   inc_sort_kernel<<<grid_for(s.n), kT, 0, st>>>(s);
-  lang_sort_kernel<<<grid_lang(s.n), kT, 0, st>>>(s.inc_off, s.inc_ent, s.n);
+  if ((e = lang_sort(s.inc_off, s.inc_ent, s.n, st)) != cudaSuccess) return e;
   inc_pos_kernel<<<grid_for(int64_t(s.cap_inc)), kT, 0, st>>>(s);
   return cudaGetLastError();
 }

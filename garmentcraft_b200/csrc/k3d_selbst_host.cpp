@@ -374,6 +374,8 @@ cudaError_t selbst_grow_wege(SelbstHost& H, uint32_t cap_p, uint32_t cap_k) {
   if ((e = alloc(H.s.hp2.ein, size_t(cap_p), H.wege)) != cudaSuccess) return e;
   if ((e = alloc(H.s.hp2.elo, size_t(cap_p), H.wege)) != cudaSuccess) return e;
   if ((e = alloc(H.s.hp2.ehi, size_t(cap_p), H.wege)) != cudaSuccess) return e;
+  if ((e = alloc(H.s.hk2.elo, size_t(cap_k), H.wege)) != cudaSuccess) return e;
+  if ((e = alloc(H.s.hk2.ehi, size_t(cap_k), H.wege)) != cudaSuccess) return e;
   return alloc(H.s.hk2.ein, size_t(cap_k), H.wege);
 }
 
