@@ -197,7 +197,7 @@ __device__ uint32_t je_eintrag_gruppe(const Gruppe& gr, const Box& q, double zel
     for (uint32_t b0 = lo; b0 < hi; b0 += kG) {
       const uint32_t e = b0 + uint32_t(gr.lane);
       Payload pl;
-      const bool hit = e < hi && (!elo || ueberlappt32(q32, elo[e], ehi[e])) && pruefe(ein[e], i, j, k, pl);
+      const bool hit = e < hi && (!elo || ueberlappt32(q32, elo[e], ehi[e])) && pruefe(ein[e], i, j, k, e, pl);
       const unsigned b = __ballot_sync(gr.maske, hit);
       if (FILL && hit) schreibe(pl, pos + cnt + uint32_t(__popc(b & unter)));
       cnt += uint32_t(__popc(b));
@@ -608,7 +608,7 @@ __device__ uint32_t punkt_dreieck_gruppe(const SelbstArgs& s, const Gruppe& gr, 
   const bool alle_fest = s.w[i0] <= 0.0 && s.w[i1] <= 0.0 && s.w[i2] <= 0.0;
   return je_eintrag_gruppe<FILL, PaarPT>(
       gr, qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, s.ebp_lo, s.ebp_hi, pos,
-      [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck, PaarPT& o) -> bool {
+      [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck, uint32_t, PaarPT& o) -> bool {
         // the reference's conditions, the cheapest rejection first (each is
         // a plain condition on the candidate, so the order changes no result)
         const Box qv = box_of(s.qp_lo, s.qp_hi, v);
@@ -662,10 +662,12 @@ __device__ uint32_t kante_kante_gruppe(const SelbstArgs& s, const Gruppe& gr, in
   if (a0 == a1) return 0;
   const D3 pa0 = ld3(s.x, a0), pa1 = ld3(s.x, a1);
   const Box qe = box_of(s.qk_lo, s.qk_hi, e);
+  const Box32 qe32 = box32(qe);
   return je_eintrag_gruppe<FILL, PaarKK>(
       gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, nullptr, nullptr, pos,
-      [&](uint32_t f, int64_t ci, int64_t cj, int64_t ck, PaarKK& o) -> bool {
+      [&](uint32_t f, int64_t ci, int64_t cj, int64_t ck, uint32_t sq, PaarKK& o) -> bool {
         if (int64_t(f) <= e) return false;
+        if (!ueberlappt32(qe32, s.ebk_lo[sq], s.ebk_hi[sq])) return false;
         const Box qf = box_of(s.qk_lo, s.qk_hi, f);
         if (!ueberlappt(qe, qf) || !erste_zelle(qe, qf, s.zelle, ci, cj, ck)) return false;
         const uint2 kb = s.k_idx[f];
@@ -1237,7 +1239,7 @@ __device__ uint32_t kante_schnitte(const SelbstArgs& s, const Gruppe& gr, int64_
   const D3 ehat = einheit(pb - pa);
   return je_eintrag_gruppe<FILL, SchnittT>(
       gr, qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, s.hs.elo, s.hs.ehi, pos,
-      [&](uint32_t t, int64_t ci, int64_t cj, int64_t ck, SchnittT& o) -> bool {
+      [&](uint32_t t, int64_t ci, int64_t cj, int64_t ck, uint32_t, SchnittT& o) -> bool {
         // the box first: the cheapest rejection (plain conditions, any order)
         const Box qt = box_of(s.hs.lo, s.hs.hi, t);
         if (!ueberlappt(qt, qe) || !erste_zelle(qe, qt, zelle, ci, cj, ck)) return false;
@@ -1977,9 +1979,9 @@ cudaError_t exclusive_scan_u32(uint32_t* data, int64_t n, uint32_t* tmp, uint32_
 }
 // normals, boxes; 2 scans, fill, sort, count, 2 scans; fill, springs, damping,
 // count, scan, fill, sort
-// (+2 and +2: the entry boxes of the point and triangle hashes and of the
-// two path hashes)
-int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3) + 6 + 4 + 2; }
+// (+3 and +2: the entry boxes of the point, edge and triangle hashes and of
+// the two path hashes)
+int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3) + 6 + 4 + 3; }
 int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1 + 3 + 2; }
 
 // Impacts, part 1 (selbstkollision.rs:1196-1203): the longest edge at x1, the
@@ -2054,6 +2056,8 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   if ((e = lang_sort(s.anf_k, s.ein_k, s.eimer_k, st)) != cudaSuccess) return e;
   eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.anf_p, s.eimer_p, s.cap_ep, s.ein_p, s.qp_lo, s.qp_hi, s.ebp_lo,
                                                     s.ebp_hi);
+  eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.anf_k, s.eimer_k, s.cap_ek, s.ein_k, s.qk_lo, s.qk_hi, s.ebk_lo,
+                                                    s.ebk_hi);
   pairs_count_kernel<<<grid_for(kG * (s.nd > s.ne ? s.nd : s.ne)), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = scan(s.off_t, s.nd + 1, s.scan_tmp, &s.zahl[SZ_PAARE_PT], st)) != cudaSuccess) return e;

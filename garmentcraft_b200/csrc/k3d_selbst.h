@@ -76,7 +76,7 @@ struct SelbstArgs {
   double4 *qp_lo, *qp_hi, *qk_lo, *qk_hi;  // point and edge boxes
   uint32_t *anf_p, *ein_p, *cur_p;         // point hash: starts (eimer+1), entries, fill cursors
   uint32_t *anf_k, *ein_k, *cur_k;         // edge hash
-  float4 *ebp_lo, *ebp_hi;                 // per entry of the point hash its box in FP32, rounded outward
+  float4 *ebp_lo, *ebp_hi, *ebk_lo, *ebk_hi;  // per entry of the point / edge hash its box in FP32, rounded outward
   uint32_t cap_ep, cap_ek;
   uint32_t *off_t, *off_e;  // pair counts -> starts per triangle / edge (n + 1)
   uint32_t* aktiv_p;        // triangles (t) and edges (nd + e) with pairs, in no order (nd + ne)

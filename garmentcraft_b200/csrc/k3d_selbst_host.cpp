@@ -382,6 +382,9 @@ cudaError_t selbst_grow_wege(SelbstHost& H, uint32_t cap_p, uint32_t cap_k) {
 cudaError_t selbst_grow_edge_hash(SelbstHost& H, uint32_t cap) {
   free_all(H.hashk);
   H.s.cap_ek = cap;
+  cudaError_t e;
+  if ((e = alloc(H.s.ebk_lo, size_t(cap), H.hashk)) != cudaSuccess) return e;
+  if ((e = alloc(H.s.ebk_hi, size_t(cap), H.hashk)) != cudaSuccess) return e;
   return alloc(H.s.ein_k, size_t(cap), H.hashk);
 }
 
