@@ -94,6 +94,8 @@ def args_():
                    help="case of --capture: the sheet drop, the garment with self-collision (frames), the "
                         "material-fit drop's adjoint (frames forward, then the backward), or the body mesh "
                         "(rounds of voxelisation at a 3 and a 6 cm band)")
+    p.add_argument("--garment-points", type=int, default=200_000,
+                   help="points of the garment for --capture --workload garment (a smaller case for full captures)")
     p.add_argument("--no-batch", action="store_true", help="skip the batched-drape comparison")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (material-fit) leg")
     p.add_argument("--no-garment", action="store_true", help="skip the sewn-garment leg")
@@ -785,7 +787,7 @@ def main():
         if a.workload == "garment":
             from garmentcraft_b200 import synth
             from garmentcraft_b200.params import ImplizitParameter
-            s, _ = synth.garment_szene()
+            s, _ = synth.garment_szene(ziel_punkte=a.garment_points)
             cg = ImplizitCg(ImplizitParameter(schritte_je_bild=1, cg_max=CG_MAX, cg_toleranz=1e-5, precision=prec,
                                               selbstkollision=True))
             cg.zustand_hochladen(s)
