@@ -1697,6 +1697,145 @@ __device__ bool kanten_kreuzen(D3 a, D3 b, D3 c, D3 d, double& so, double& wo) {
   return true;
 }
 
+// One candidate of the impact searches: every condition of the reference's
+// loop body, the candidate's impact time and what the search writes for it.
+// `grenze`: with `hat`, a candidate at that time or later cannot win (the
+// search keeps the first of equal times) and is dropped before the expensive
+// part, as the reference's loop does.
+struct StossPD {
+  double zeit, u, v, seite;
+  D3 n;
+  uint32_t p;
+};
+__device__ __forceinline__ bool stoss_pd_kandidat(const SelbstArgs& s, const uint32_t (&d)[3], const Box& qt, double z,
+                                                  uint32_t v, int64_t ci, int64_t cj, int64_t ck, bool hat,
+                                                  double grenze, StossPD& o) {
+  const Box qv = box_of(s.hp2.lo, s.hp2.hi, v);
+  if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, z, ci, cj, ck)) return false;
+  for (int k = 0; k < 3; ++k)
+    if (gleich_oder_partner(s, v, d[k])) return false;
+  const uint32_t idx[4] = {d[0], d[1], d[2], v};
+  if (s.w[idx[0]] <= 0.0 && s.w[idx[1]] <= 0.0 && s.w[idx[2]] <= 0.0 && s.w[idx[3]] <= 0.0) return false;
+  D3 a0[4], a1[4];
+  for (int k = 0; k < 4; ++k) {
+    a0[k] = ld3(s.x0, idx[k]);
+    a1[k] = ld3(s.xs, idx[k]);
+  }
+  double zeit;
+  if (!koplanar_zeit(a0, a1, kStossAbstand * 0.1, zeit)) return false;
+  if (hat && grenze <= zeit) return false;
+  D3 q[4];
+  for (int k = 0; k < 4; ++k) q[k] = lerp3(a0[k], a1[k], zeit);
+  double u, vv;
+  if (!im_dreieck(q[0], q[1], q[2], q[3], u, vv)) return false;
+  const D3 n = einheit(cross(q[1] - q[0], q[2] - q[0]));
+  const double g[3] = {1.0 - u - vv, u, vv};
+  const D3 rel = (a1[3] - a0[3]) - (((a1[0] - a0[0]) * g[0] + (a1[1] - a0[1]) * g[1]) + (a1[2] - a0[2]) * g[2]);
+  o.zeit = zeit;
+  o.u = u;
+  o.v = vv;
+  o.seite = dot(rel, n) <= 0.0 ? 1.0 : -1.0;
+  o.n = n;
+  o.p = v;
+  return true;
+}
+__device__ __forceinline__ void stoss_pd_schreiben(const SelbstArgs& s, int64_t t, const uint32_t (&d)[3],
+                                                   const StossPD& o) {
+  s.st_idx[t] = make_uint4(o.p, d[0], d[1], d[2]);
+  s.st_lzs[t] = make_double4(o.u, o.v, o.zeit, o.seite);
+  s.st_n[t] = make_double4(o.n.x * o.seite, o.n.y * o.seite, o.n.z * o.seite, 0.0);
+  s.st_art[t] = 1u;
+}
+struct StossKK {
+  double zeit, sv, wv, seite;
+  D3 n;
+  uint32_t j, b0, b1;
+};
+__device__ __forceinline__ bool stoss_kk_kandidat(const SelbstArgs& s, int64_t i, uint32_t i0, uint32_t i1,
+                                                  const Box& qi, const Box32& qi32, double z, uint32_t j, int64_t ci,
+                                                  int64_t cj, int64_t ck, uint32_t sq, bool hat, double grenze,
+                                                  StossKK& o) {
+  if (int64_t(j) <= i) return false;
+  if (!ueberlappt32(qi32, s.hk2.elo[sq], s.hk2.ehi[sq])) return false;
+  const Box qj = box_of(s.hk2.lo, s.hk2.hi, j);
+  if (!ueberlappt(qi, qj) || !erste_zelle(qi, qj, z, ci, cj, ck)) return false;
+  const uint2 kj = s.k_idx[j];
+  if (gleich_oder_partner(s, kj.x, i0) || gleich_oder_partner(s, kj.x, i1) || gleich_oder_partner(s, kj.y, i0) ||
+      gleich_oder_partner(s, kj.y, i1))
+    return false;
+  const uint32_t idx[4] = {i1, kj.x, kj.y, i0};
+  if (s.w[idx[0]] <= 0.0 && s.w[idx[1]] <= 0.0 && s.w[idx[2]] <= 0.0 && s.w[idx[3]] <= 0.0) return false;
+  D3 a0[4], a1[4];
+  for (int k = 0; k < 4; ++k) {
+    a0[k] = ld3(s.x0, idx[k]);
+    a1[k] = ld3(s.xs, idx[k]);
+  }
+  double zeit;
+  if (!koplanar_zeit(a0, a1, kStossAbstand * 0.1, zeit)) return false;
+  if (hat && grenze <= zeit) return false;
+  D3 q[4];
+  for (int k = 0; k < 4; ++k) q[k] = lerp3(a0[k], a1[k], zeit);
+  double sv, wv;
+  if (!kanten_kreuzen(q[3], q[0], q[1], q[2], sv, wv)) return false;
+  const D3 n = einheit(cross(q[0] - q[3], q[2] - q[1]));
+  const D3 auf_i = (a1[3] - a0[3]) * (1.0 - sv) + (a1[0] - a0[0]) * sv;
+  const D3 auf_j = (a1[1] - a0[1]) * (1.0 - wv) + (a1[2] - a0[2]) * wv;
+  o.zeit = zeit;
+  o.sv = sv;
+  o.wv = wv;
+  o.seite = dot(auf_i - auf_j, n) <= 0.0 ? 1.0 : -1.0;
+  o.n = n;
+  o.j = j;
+  o.b0 = kj.x;
+  o.b1 = kj.y;
+  return true;
+}
+__device__ __forceinline__ void stoss_kk_schreiben(const SelbstArgs& s, uint32_t slot, uint32_t i0, uint32_t i1,
+                                                   const StossKK& o) {
+  s.st_idx[slot] = make_uint4(i0, i1, o.b0, o.b1);
+  s.st_lzs[slot] = make_double4(o.sv, o.wv, o.zeit, o.seite);
+  s.st_n[slot] = make_double4(o.n.x * o.seite, o.n.y * o.seite, o.n.z * o.seite, double(o.j));  // .w: the partner edge
+  s.st_art[slot] = 2u;
+}
+
+// The candidates a query visits: the entries of its cells' buckets (cells
+// counted with repeats, as the search walks them), saturating.
+__device__ __forceinline__ uint32_t kandidaten(const Box& q, double z, const HashG& g) {
+  if (!zellbereich_ok(q, z)) return 0;
+  const Cells c = cells_of(q, z);
+  uint32_t n = 0;
+  for (uint32_t a = 0; a < c.total && n < 0x80000000u; ++a) {
+    int64_t i, j, k;
+    cell_at(c, a, i, j, k);
+    const uint32_t h = streue(i, j, k, g.eimer);
+    n += g.anf[h + 1] - g.anf[h];
+  }
+  return n;
+}
+// A query with more candidates than this goes to the cooperative pass: one
+// warp takes it, so a few queries on crowded buckets (the path boxes may span
+// up to 64 cells an axis, and buckets of several thousand entries occur) do
+// not hold their warps for the whole search.
+constexpr uint32_t kSchwer = 256;
+
+// The warp's first hit by (time, visit ordinal): the reference's loop keeps
+// the earliest time and, among equal times, the first candidate it visits.
+// Lane `beste` holds it; -1 when no lane has one.
+__device__ __forceinline__ int warp_erster(bool hat, double zeit, uint64_t ord) {
+  const unsigned voll = 0xffffffffu;
+  double zm = hat ? zeit : INFINITY;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) zm = fmin(zm, __shfl_xor_sync(voll, zm, o));
+  uint64_t om = hat && zeit == zm ? ord : ~0ull;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t x = __shfl_xor_sync(voll, om, o);
+    om = x < om ? x : om;
+  }
+  const unsigned wer = __ballot_sync(voll, hat && zeit == zm && ord == om);
+  return wer ? __ffs(wer) - 1 : -1;
+}
+
 // the earliest point through triangle t (selbstkollision.rs:1215-1251)
 __global__ void __launch_bounds__(kT, 4) stoss_pd_kernel(const __grid_constant__ SelbstArgs s) {
   const double z = zelle_aus(&s.lmax[1]);
@@ -1706,39 +1845,21 @@ __global__ void __launch_bounds__(kT, 4) stoss_pd_kernel(const __grid_constant__
     const uint32_t d[3] = {dq.x, dq.y, dq.z};
     if (d[0] == d[1] || d[1] == d[2] || d[0] == d[2]) continue;
     const Box qt = box_of(s.qt2_lo, s.qt2_hi, t);
+    if (kandidaten(qt, z, s.hp2) > kSchwer) {
+      s.schwer_pd[atomicAdd(&s.zahl[SZ_SCHWER_PD], 1u)] = uint32_t(t);
+      continue;
+    }
     bool hat = false;
-    double bz = 0.0;
+    StossPD best{};
     je_eintrag(qt, z, s.hp2.eimer, s.hp2.anf, s.hp2.ein, s.hp2.elo, s.hp2.ehi,
                [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck, uint32_t) {
-      const Box qv = box_of(s.hp2.lo, s.hp2.hi, v);
-      if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, z, ci, cj, ck)) return;
-      for (int k = 0; k < 3; ++k)
-        if (gleich_oder_partner(s, v, d[k])) return;
-      const uint32_t idx[4] = {d[0], d[1], d[2], v};
-      if (s.w[idx[0]] <= 0.0 && s.w[idx[1]] <= 0.0 && s.w[idx[2]] <= 0.0 && s.w[idx[3]] <= 0.0) return;
-      D3 a0[4], a1[4];
-      for (int k = 0; k < 4; ++k) {
-        a0[k] = ld3(s.x0, idx[k]);
-        a1[k] = ld3(s.xs, idx[k]);
-      }
-      double zeit;
-      if (!koplanar_zeit(a0, a1, kStossAbstand * 0.1, zeit)) return;
-      if (hat && bz <= zeit) return;
-      D3 q[4];
-      for (int k = 0; k < 4; ++k) q[k] = lerp3(a0[k], a1[k], zeit);
-      double u, vv;
-      if (!im_dreieck(q[0], q[1], q[2], q[3], u, vv)) return;
-      const D3 n = einheit(cross(q[1] - q[0], q[2] - q[0]));
-      const double g[3] = {1.0 - u - vv, u, vv};
-      const D3 rel = (a1[3] - a0[3]) - (((a1[0] - a0[0]) * g[0] + (a1[1] - a0[1]) * g[1]) + (a1[2] - a0[2]) * g[2]);
-      const double seite = dot(rel, n) <= 0.0 ? 1.0 : -1.0;
-      hat = true;
-      bz = zeit;
-      s.st_idx[t] = make_uint4(v, d[0], d[1], d[2]);
-      s.st_lzs[t] = make_double4(u, vv, zeit, seite);
-      s.st_n[t] = make_double4(n.x * seite, n.y * seite, n.z * seite, 0.0);
-    });
-    if (hat) s.st_art[t] = 1u;
+                 StossPD o;
+                 if (stoss_pd_kandidat(s, d, qt, z, v, ci, cj, ck, hat, best.zeit, o)) {
+                   hat = true;
+                   best = o;
+                 }
+               });
+    if (hat) stoss_pd_schreiben(s, t, d, best);
   }
 }
 // the earliest partner edge of edge i (selbstkollision.rs:1253-1283)
@@ -1751,44 +1872,94 @@ __global__ void __launch_bounds__(kT, 4) stoss_kk_kernel(const __grid_constant__
     const uint32_t i0 = ki.x, i1 = ki.y;
     if (i0 == i1) continue;
     const Box qi = box_of(s.hk2.lo, s.hk2.hi, i);
+    if (kandidaten(qi, z, s.hk2) > kSchwer) {
+      s.schwer_kk[atomicAdd(&s.zahl[SZ_SCHWER_KK], 1u)] = uint32_t(i);
+      continue;
+    }
     bool hat = false;
-    double bz = 0.0;
+    StossKK best{};
     const Box32 qi32 = box32(qi);
     je_eintrag(qi, z, s.hk2.eimer, s.hk2.anf, s.hk2.ein, nullptr, nullptr,
                [&](uint32_t j, int64_t ci, int64_t cj, int64_t ck, uint32_t sq) {
-      if (int64_t(j) <= i) return;
-      if (!ueberlappt32(qi32, s.hk2.elo[sq], s.hk2.ehi[sq])) return;
-      const Box qj = box_of(s.hk2.lo, s.hk2.hi, j);
-      if (!ueberlappt(qi, qj) || !erste_zelle(qi, qj, z, ci, cj, ck)) return;
-      const uint2 kj = s.k_idx[j];
-      if (gleich_oder_partner(s, kj.x, i0) || gleich_oder_partner(s, kj.x, i1) || gleich_oder_partner(s, kj.y, i0) ||
-          gleich_oder_partner(s, kj.y, i1))
-        return;
-      const uint32_t idx[4] = {i1, kj.x, kj.y, i0};
-      if (s.w[idx[0]] <= 0.0 && s.w[idx[1]] <= 0.0 && s.w[idx[2]] <= 0.0 && s.w[idx[3]] <= 0.0) return;
-      D3 a0[4], a1[4];
-      for (int k = 0; k < 4; ++k) {
-        a0[k] = ld3(s.x0, idx[k]);
-        a1[k] = ld3(s.xs, idx[k]);
+                 StossKK o;
+                 if (stoss_kk_kandidat(s, i, i0, i1, qi, qi32, z, j, ci, cj, ck, sq, hat, best.zeit, o)) {
+                   hat = true;
+                   best = o;
+                 }
+               });
+    if (hat) stoss_kk_schreiben(s, slot, i0, i1, best);
+  }
+}
+// The listed heavy queries, one warp each: the lanes take a cell's entries in
+// turn (entry position lane, lane + 32, ...), each keeps its first hit by
+// time (its own visits are in the reference's order), and the warp's first
+// by (time, cell, position) writes the result.
+#define WARP_FOR(w, n)                                                                                       \
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < (n); w += (gridDim.x * blockDim.x) >> 5)
+__global__ void __launch_bounds__(kT, 4) stoss_pd_schwer_kernel(const __grid_constant__ SelbstArgs s) {
+  const double z = zelle_aus(&s.lmax[1]);
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t m = s.zahl[SZ_SCHWER_PD];
+  WARP_FOR(w, m) {
+    const uint32_t t = s.schwer_pd[w];
+    const uint4 dq = s.d_idx[t];
+    const uint32_t d[3] = {dq.x, dq.y, dq.z};
+    const Box qt = box_of(s.qt2_lo, s.qt2_hi, t);
+    const Cells c = cells_of(qt, z);  // zellbereich_ok held: the query had candidates
+    const Box32 q32 = box32(qt);
+    bool hat = false;
+    StossPD best{};
+    uint64_t ord = 0;
+    for (uint32_t a = 0; a < c.total; ++a) {
+      int64_t i, j, k;
+      cell_at(c, a, i, j, k);
+      const uint32_t h = streue(i, j, k, s.hp2.eimer);
+      const uint32_t lo = s.hp2.anf[h], hi = s.hp2.anf[h + 1];
+      for (uint32_t e = lo + lane; e < hi; e += 32) {
+        if (!ueberlappt32(q32, s.hp2.elo[e], s.hp2.ehi[e])) continue;
+        StossPD o;
+        if (stoss_pd_kandidat(s, d, qt, z, s.hp2.ein[e], i, j, k, hat, best.zeit, o)) {
+          hat = true;
+          best = o;
+          ord = (uint64_t(a) << 32) | e;
+        }
       }
-      double zeit;
-      if (!koplanar_zeit(a0, a1, kStossAbstand * 0.1, zeit)) return;
-      if (hat && bz <= zeit) return;
-      D3 q[4];
-      for (int k = 0; k < 4; ++k) q[k] = lerp3(a0[k], a1[k], zeit);
-      double sv, wv;
-      if (!kanten_kreuzen(q[3], q[0], q[1], q[2], sv, wv)) return;
-      const D3 n = einheit(cross(q[0] - q[3], q[2] - q[1]));
-      const D3 auf_i = (a1[3] - a0[3]) * (1.0 - sv) + (a1[0] - a0[0]) * sv;
-      const D3 auf_j = (a1[1] - a0[1]) * (1.0 - wv) + (a1[2] - a0[2]) * wv;
-      const double seite = dot(auf_i - auf_j, n) <= 0.0 ? 1.0 : -1.0;
-      hat = true;
-      bz = zeit;
-      s.st_idx[slot] = make_uint4(i0, i1, kj.x, kj.y);
-      s.st_lzs[slot] = make_double4(sv, wv, zeit, seite);
-      s.st_n[slot] = make_double4(n.x * seite, n.y * seite, n.z * seite, double(j));  // .w: the partner edge
-    });
-    if (hat) s.st_art[slot] = 2u;
+    }
+    const int wer = warp_erster(hat, best.zeit, ord);
+    if (wer >= 0 && int(lane) == wer) stoss_pd_schreiben(s, t, d, best);
+  }
+}
+__global__ void __launch_bounds__(kT, 4) stoss_kk_schwer_kernel(const __grid_constant__ SelbstArgs s) {
+  const double z = zelle_aus(&s.lmax[1]);
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t m = s.zahl[SZ_SCHWER_KK];
+  WARP_FOR(w, m) {
+    const int64_t ie = s.schwer_kk[w];
+    const uint32_t slot = uint32_t(s.nd + ie);
+    const uint2 ki = s.k_idx[ie];
+    const uint32_t i0 = ki.x, i1 = ki.y;
+    const Box qi = box_of(s.hk2.lo, s.hk2.hi, ie);
+    const Cells c = cells_of(qi, z);
+    const Box32 qi32 = box32(qi);
+    bool hat = false;
+    StossKK best{};
+    uint64_t ord = 0;
+    for (uint32_t a = 0; a < c.total; ++a) {
+      int64_t i, j, k;
+      cell_at(c, a, i, j, k);
+      const uint32_t h = streue(i, j, k, s.hk2.eimer);
+      const uint32_t lo = s.hk2.anf[h], hi = s.hk2.anf[h + 1];
+      for (uint32_t e = lo + lane; e < hi; e += 32) {
+        StossKK o;
+        if (stoss_kk_kandidat(s, ie, i0, i1, qi, qi32, z, s.hk2.ein[e], i, j, k, e, hat, best.zeit, o)) {
+          hat = true;
+          best = o;
+          ord = (uint64_t(a) << 32) | e;
+        }
+      }
+    }
+    const int wer = warp_erster(hat, best.zeit, ord);
+    if (wer >= 0 && int(lane) == wer) stoss_kk_schreiben(s, slot, i0, i1, best);
   }
 }
 // ohne_durchdrungene (selbstkollision.rs:1063-1084): keep flags per slot
@@ -1982,7 +2153,7 @@ cudaError_t exclusive_scan_u32(uint32_t* data, int64_t n, uint32_t* tmp, uint32_
 // (+3 and +2: the entry boxes of the point, edge and triangle hashes and of
 // the two path hashes)
 int selbst_launches_per_run() { return 2 + (6 + 3 + 6 + 10) + (4 + 12 + 3 + 3) + 6 + 4 + 3; }
-int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1 + 3 + 2; }
+int selbst_stoss_launches(int iterationen) { return 8 + 6 + 4 + 3 + 3 + 3 * iterationen + 1 + 3 + 2 + 2; }
 
 // Impacts, part 1 (selbstkollision.rs:1196-1203): the longest edge at x1, the
 // path boxes, the bucket counts of the point and edge path hashes. The host
@@ -2016,6 +2187,8 @@ cudaError_t selbst_stoss_antwort(const SelbstArgs& s, int iterationen, unsigned 
                                                     s.hk2.elo, s.hk2.ehi);
   stoss_pd_kernel<<<grid_for(s.nd), kT, 0, st>>>(s);
   stoss_kk_kernel<<<grid_for(s.ne), kT, 0, st>>>(s);
+  stoss_pd_schwer_kernel<<<148 * 4, kT, 0, st>>>(s);
+  stoss_kk_schwer_kernel<<<148 * 4, kT, 0, st>>>(s);
   stoss_filter_kernel<<<grid_for(s.nd + s.ne), kT, 0, st>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = scan(s.st_off, s.nd + s.ne + 1, s.scan_tmp, &s.zahl[SZ_STOSS], st)) != cudaSuccess) return e;

@@ -32,7 +32,9 @@ enum SelbstZahl : int {
   SZ_HALT = 14,     // set when a response pass moved no point (the passes stop)
   SZ_AKTIV_P = 15,  // triangles and edges with proximity pairs (the fill pass's list)
   SZ_AKTIV_S = 16,  // edges through a triangle (the intersection fill pass's list)
-  SZ_COUNT = 18
+  SZ_SCHWER_PD = 17,  // triangles whose impact search runs one warp each (many candidates)
+  SZ_SCHWER_KK = 18,  // edges likewise
+  SZ_COUNT = 20
 };
 
 // A spatial hash over boxes (Hashgitter, selbstkollision.rs:281-345): the
@@ -140,6 +142,7 @@ struct SelbstArgs {
   double4* st_lzs;                // lage (2), zeit, seite
   double4* st_n;                  // normal (edge-edge)
   uint32_t* st_off;               // kept impacts: count, then start (nd + ne + 1)
+  uint32_t *schwer_pd, *schwer_kk;  // triangles / edges with many candidates, in no order (nd / ne)
   uint32_t* im;                   // the kept impacts' slots in order
   uint32_t *im_off, *im_cur, *im_ent;  // per point: (impact << 2 | slot) (n + 1)
   double4* im_c;                  // per (impact, slot): the correction, w = 1 if it applies

@@ -312,6 +312,8 @@ cudaError_t selbst_upload(SelbstHost& H, const k3d_scene* sc, double zusatzdicke
   if ((e = alloc(s.st_lzs, slots, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.st_n, slots, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.st_off, slots + 1, H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.schwer_pd, size_t(std::max<int64_t>(nd, 1)), H.fest)) != cudaSuccess) return e;
+  if ((e = alloc(s.schwer_kk, size_t(std::max<int64_t>(ne, 1)), H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.im, slots, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.im_off, size_t(n) + 1, H.fest)) != cudaSuccess) return e;
   if ((e = alloc(s.im_cur, size_t(n), H.fest)) != cudaSuccess) return e;
