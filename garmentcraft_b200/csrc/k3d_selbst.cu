@@ -206,6 +206,53 @@ __device__ uint32_t je_eintrag_gruppe(const Gruppe& gr, const Box& q, double zel
   return cnt;
 }
 
+// The count of a query's hits for a count pass, the group's lanes over the
+// query's cells: lane l takes cells l, l + kG, ... and walks each one's
+// bucket itself, so a query whose box spans many cells is not walked cell by
+// cell; a bucket of more than kGross entries is walked by the whole group
+// (lanes over its entries) after its round. The same candidates as
+// je_eintrag_gruppe, tested by the same predicate: a count needs no order.
+constexpr uint32_t kGross = 32;
+template <typename Payload, typename T>
+__device__ uint32_t zaehle_gruppe(const Gruppe& gr, const Box& q, double zelle, uint32_t eimer, const uint32_t* anf,
+                                  const uint32_t* ein, const float4* elo, const float4* ehi, T&& pruefe) {
+  if (!zellbereich_ok(q, zelle)) return 0;
+  const Cells c = cells_of(q, zelle);
+  const Box32 q32 = box32(q);
+  uint32_t cnt = 0;
+  for (uint32_t a0 = 0; a0 < c.total; a0 += kG) {
+    const uint32_t a = a0 + uint32_t(gr.lane);
+    int64_t i = 0, j = 0, k = 0;
+    uint32_t lo = 0, hi = 0;
+    if (a < c.total) {
+      cell_at(c, a, i, j, k);
+      const uint32_t h = streue(i, j, k, eimer);
+      lo = anf[h];
+      hi = anf[h + 1];
+    }
+    const bool gross = hi - lo > kGross;
+    if (!gross) {
+      for (uint32_t e = lo; e < hi; ++e) {
+        Payload pl;
+        if ((!elo || ueberlappt32(q32, elo[e], ehi[e])) && pruefe(ein[e], i, j, k, e, pl)) ++cnt;
+      }
+    }
+    for (unsigned m = __ballot_sync(gr.maske, gross); m != 0u; m &= m - 1u) {
+      const int l = __ffs(m) - 1;  // the warp lane that holds the cell
+      const uint32_t glo = __shfl_sync(gr.maske, lo, l), ghi = __shfl_sync(gr.maske, hi, l);
+      const int64_t gi = __shfl_sync(gr.maske, (long long)i, l), gj = __shfl_sync(gr.maske, (long long)j, l),
+                    gk = __shfl_sync(gr.maske, (long long)k, l);
+      for (uint32_t e = glo + uint32_t(gr.lane); e < ghi; e += kG) {
+        Payload pl;
+        if ((!elo || ueberlappt32(q32, elo[e], ehi[e])) && pruefe(ein[e], gi, gj, gk, e, pl)) ++cnt;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = kG / 2; o > 0; o >>= 1) cnt += __shfl_xor_sync(gr.maske, cnt, o);
+  return cnt;
+}
+
 // selbstkollision.rs:347-357, on p[0..n) with margin m
 __device__ __forceinline__ Box quader_punkte(const D3* p, int n, double m) {
   Box b{d3(INFINITY, INFINITY, INFINITY), d3(-INFINITY, -INFINITY, -INFINITY)};
@@ -606,49 +653,53 @@ __device__ uint32_t punkt_dreieck_gruppe(const SelbstArgs& s, const Gruppe& gr, 
   }
   const double sg[3] = {dot(p[2] - p[0], en[0]), dot(p[0] - p[1], en[1]), dot(p[1] - p[2], en[2])};
   const bool alle_fest = s.w[i0] <= 0.0 && s.w[i1] <= 0.0 && s.w[i2] <= 0.0;
-  return je_eintrag_gruppe<FILL, PaarPT>(
-      gr, qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, s.ebp_lo, s.ebp_hi, pos,
-      [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck, uint32_t, PaarPT& o) -> bool {
-        // the reference's conditions, the cheapest rejection first (each is
-        // a plain condition on the candidate, so the order changes no result)
-        const Box qv = box_of(s.qp_lo, s.qp_hi, v);
-        if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, s.zelle, ci, cj, ck)) return false;
-        for (int k = 0; k < 3; ++k)
-          if (gleich_oder_partner(s, v, d[k])) return false;
-        if (s.w[v] <= 0.0 && alle_fest) return false;
-        const D3 xv = ld3(s.x, v);
-        double ruhe = rt + s.r_punkt[v];
-        double eine;
-        if (band_abstand(s, v, d, 3, eine)) ruhe = eine;
-        const double soll = ruhe + kZuschlagPaar;
-        const double sd = dot(nt, xv - p[0]);
-        if (fabs(sd) > soll) return false;
-        for (int k = 0; k < 3; ++k)
-          if (dot(xv - p[k], en[k]) * sg[k] < 0.0) return false;
-        double g[3];
-        naechster_dreieck(p[0], p[1], p[2], xv, g);
-        const D3 cp = (p[0] * g[0] + p[1] * g[1]) + p[2] * g[2];
-        const D3 r = xv - cp;
-        const double abstand = norm(r);
-        if (abstand > soll) return false;
-        if (FILL) {
-          o.v = v;
-          o.g0 = g[0], o.g1 = g[1], o.g2 = g[2];
-          o.ab = abstand;
-          o.ruhe = ruhe;
-          o.n = abstand > 1e-12 ? r * (1.0 / abstand) : nt;
-        }
-        return true;
-      },
-      [&](const PaarPT& o, uint32_t q) {
-        if (q < s.cap_pairs) {
-          s.pr_idx[q] = make_uint4(o.v, i0, i1, i2);
-          s.pr_src[q] = make_uint2(uint32_t(t), kKein);
-          s.pr_w[q] = make_double4(1.0, -o.g0, -o.g1, -o.g2);
-          s.pr_nab[q] = make_double4(o.n.x, o.n.y, o.n.z, o.ab);
-          s.pr_ruhe[q] = o.ruhe;
-        }
-      });
+  const auto pruefe = [&](uint32_t v, int64_t ci, int64_t cj, int64_t ck, uint32_t, PaarPT& o) -> bool {
+    // the reference's conditions, the cheapest rejection first (each is
+    // a plain condition on the candidate, so the order changes no result)
+    const Box qv = box_of(s.qp_lo, s.qp_hi, v);
+    if (!ueberlappt(qv, qt) || !erste_zelle(qt, qv, s.zelle, ci, cj, ck)) return false;
+    for (int k = 0; k < 3; ++k)
+      if (gleich_oder_partner(s, v, d[k])) return false;
+    if (s.w[v] <= 0.0 && alle_fest) return false;
+    const D3 xv = ld3(s.x, v);
+    double ruhe = rt + s.r_punkt[v];
+    double eine;
+    if (band_abstand(s, v, d, 3, eine)) ruhe = eine;
+    const double soll = ruhe + kZuschlagPaar;
+    const double sd = dot(nt, xv - p[0]);
+    if (fabs(sd) > soll) return false;
+    for (int k = 0; k < 3; ++k)
+      if (dot(xv - p[k], en[k]) * sg[k] < 0.0) return false;
+    double g[3];
+    naechster_dreieck(p[0], p[1], p[2], xv, g);
+    const D3 cp = (p[0] * g[0] + p[1] * g[1]) + p[2] * g[2];
+    const D3 r = xv - cp;
+    const double abstand = norm(r);
+    if (abstand > soll) return false;
+    if (FILL) {
+      o.v = v;
+      o.g0 = g[0], o.g1 = g[1], o.g2 = g[2];
+      o.ab = abstand;
+      o.ruhe = ruhe;
+      o.n = abstand > 1e-12 ? r * (1.0 / abstand) : nt;
+    }
+    return true;
+  };
+  const auto schreibe = [&](const PaarPT& o, uint32_t q) {
+    if (q < s.cap_pairs) {
+      s.pr_idx[q] = make_uint4(o.v, i0, i1, i2);
+      s.pr_src[q] = make_uint2(uint32_t(t), kKein);
+      s.pr_w[q] = make_double4(1.0, -o.g0, -o.g1, -o.g2);
+      s.pr_nab[q] = make_double4(o.n.x, o.n.y, o.n.z, o.ab);
+      s.pr_ruhe[q] = o.ruhe;
+    }
+  };
+  if constexpr (FILL) {
+    return je_eintrag_gruppe<true, PaarPT>(gr, qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, s.ebp_lo, s.ebp_hi,
+                                      pos, pruefe, schreibe);
+  } else {
+    return zaehle_gruppe<PaarPT>(gr, qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, s.ebp_lo, s.ebp_hi, pruefe);
+  }
 }
 struct PaarKK {
   uint32_t f, b0, b1;
@@ -663,60 +714,64 @@ __device__ uint32_t kante_kante_gruppe(const SelbstArgs& s, const Gruppe& gr, in
   const D3 pa0 = ld3(s.x, a0), pa1 = ld3(s.x, a1);
   const Box qe = box_of(s.qk_lo, s.qk_hi, e);
   const Box32 qe32 = box32(qe);
-  return je_eintrag_gruppe<FILL, PaarKK>(
-      gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, nullptr, nullptr, pos,
-      [&](uint32_t f, int64_t ci, int64_t cj, int64_t ck, uint32_t sq, PaarKK& o) -> bool {
-        if (int64_t(f) <= e) return false;
-        if (!ueberlappt32(qe32, s.ebk_lo[sq], s.ebk_hi[sq])) return false;
-        const Box qf = box_of(s.qk_lo, s.qk_hi, f);
-        if (!ueberlappt(qe, qf) || !erste_zelle(qe, qf, s.zelle, ci, cj, ck)) return false;
-        const uint2 kb = s.k_idx[f];
-        const uint32_t b0 = kb.x, b1 = kb.y;
-        if (gleich_oder_partner(s, a0, b0) || gleich_oder_partner(s, a1, b0) || gleich_oder_partner(s, a0, b1) ||
-            gleich_oder_partner(s, a1, b1))
-          return false;
-        const uint32_t bb[2] = {b0, b1}, aa[2] = {a0, a1};
-        double band = 0.0;
-        const bool hat_band = band_abstand(s, a0, bb, 2, band) || band_abstand(s, a1, bb, 2, band) ||
-                              band_abstand(s, b0, aa, 2, band) || band_abstand(s, b1, aa, 2, band);
-        if (s.w[a0] <= 0.0 && s.w[a1] <= 0.0 && s.w[b0] <= 0.0 && s.w[b1] <= 0.0) return false;
-        const D3 pb0 = ld3(s.x, b0), pb1 = ld3(s.x, b1);
-        const D3 da = pa1 - pa0, db = pb1 - pb0;
-        const double la = norm(da), lb = norm(db);
-        if (la < kKanteMin || lb < kKanteMin) return false;
-        const D3 ua = da * (1.0 / la), ub = db * (1.0 / lb);
-        const double cw = dot(ua, ub);
-        if (fabs(cw) > 0.99999) return false;
-        const D3 r = pb0 - pa0;
-        const double p = dot(r, ua), q = -dot(r, ub);
-        const double nen = 1.0 - cw * cw;
-        const double sa = (p + cw * q) / nen;
-        const double sb = (q + cw * p) / nen;
-        if (!(0.0 <= sa && sa <= la) || !(0.0 <= sb && sb <= lb)) return false;
-        const D3 pa = pa0 + ua * sa;
-        const D3 pb = pb0 + ub * sb;
-        const D3 dv = pa - pb;
-        const double abstand = norm(dv);
-        const double ruhe = hat_band ? band : s.r_kante[e] + s.r_kante[f];
-        if (abstand > ruhe + kZuschlagPaar) return false;
-        const D3 n = einheit(dv);
-        if (!ist_kuerzeste(s, f, ub, n) || !ist_kuerzeste(s, uint32_t(e), ua, n * -1.0)) return false;
-        if (FILL) {
-          o.f = f, o.b0 = b0, o.b1 = b1;
-          o.sp = sa / la, o.tp = sb / lb;
-          o.ab = abstand, o.ruhe = ruhe, o.n = n;
-        }
-        return true;
-      },
-      [&](const PaarKK& o, uint32_t w) {
-        if (w < s.cap_pairs) {
-          s.pr_idx[w] = make_uint4(a0, a1, o.b0, o.b1);
-          s.pr_src[w] = make_uint2(uint32_t(e), o.f);
-          s.pr_w[w] = make_double4(1.0 - o.sp, o.sp, -(1.0 - o.tp), -o.tp);
-          s.pr_nab[w] = make_double4(o.n.x, o.n.y, o.n.z, o.ab);
-          s.pr_ruhe[w] = o.ruhe;
-        }
-      });
+  const auto pruefe = [&](uint32_t f, int64_t ci, int64_t cj, int64_t ck, uint32_t sq, PaarKK& o) -> bool {
+    if (int64_t(f) <= e) return false;
+    if (!ueberlappt32(qe32, s.ebk_lo[sq], s.ebk_hi[sq])) return false;
+    const Box qf = box_of(s.qk_lo, s.qk_hi, f);
+    if (!ueberlappt(qe, qf) || !erste_zelle(qe, qf, s.zelle, ci, cj, ck)) return false;
+    const uint2 kb = s.k_idx[f];
+    const uint32_t b0 = kb.x, b1 = kb.y;
+    if (gleich_oder_partner(s, a0, b0) || gleich_oder_partner(s, a1, b0) || gleich_oder_partner(s, a0, b1) ||
+        gleich_oder_partner(s, a1, b1))
+      return false;
+    const uint32_t bb[2] = {b0, b1}, aa[2] = {a0, a1};
+    double band = 0.0;
+    const bool hat_band = band_abstand(s, a0, bb, 2, band) || band_abstand(s, a1, bb, 2, band) ||
+                          band_abstand(s, b0, aa, 2, band) || band_abstand(s, b1, aa, 2, band);
+    if (s.w[a0] <= 0.0 && s.w[a1] <= 0.0 && s.w[b0] <= 0.0 && s.w[b1] <= 0.0) return false;
+    const D3 pb0 = ld3(s.x, b0), pb1 = ld3(s.x, b1);
+    const D3 da = pa1 - pa0, db = pb1 - pb0;
+    const double la = norm(da), lb = norm(db);
+    if (la < kKanteMin || lb < kKanteMin) return false;
+    const D3 ua = da * (1.0 / la), ub = db * (1.0 / lb);
+    const double cw = dot(ua, ub);
+    if (fabs(cw) > 0.99999) return false;
+    const D3 r = pb0 - pa0;
+    const double p = dot(r, ua), q = -dot(r, ub);
+    const double nen = 1.0 - cw * cw;
+    const double sa = (p + cw * q) / nen;
+    const double sb = (q + cw * p) / nen;
+    if (!(0.0 <= sa && sa <= la) || !(0.0 <= sb && sb <= lb)) return false;
+    const D3 pa = pa0 + ua * sa;
+    const D3 pb = pb0 + ub * sb;
+    const D3 dv = pa - pb;
+    const double abstand = norm(dv);
+    const double ruhe = hat_band ? band : s.r_kante[e] + s.r_kante[f];
+    if (abstand > ruhe + kZuschlagPaar) return false;
+    const D3 n = einheit(dv);
+    if (!ist_kuerzeste(s, f, ub, n) || !ist_kuerzeste(s, uint32_t(e), ua, n * -1.0)) return false;
+    if (FILL) {
+      o.f = f, o.b0 = b0, o.b1 = b1;
+      o.sp = sa / la, o.tp = sb / lb;
+      o.ab = abstand, o.ruhe = ruhe, o.n = n;
+    }
+    return true;
+  };
+  const auto schreibe = [&](const PaarKK& o, uint32_t w) {
+    if (w < s.cap_pairs) {
+      s.pr_idx[w] = make_uint4(a0, a1, o.b0, o.b1);
+      s.pr_src[w] = make_uint2(uint32_t(e), o.f);
+      s.pr_w[w] = make_double4(1.0 - o.sp, o.sp, -(1.0 - o.tp), -o.tp);
+      s.pr_nab[w] = make_double4(o.n.x, o.n.y, o.n.z, o.ab);
+      s.pr_ruhe[w] = o.ruhe;
+    }
+  };
+  if constexpr (FILL) {
+    return je_eintrag_gruppe<true, PaarKK>(gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, nullptr, nullptr,
+                                      pos, pruefe, schreibe);
+  } else {
+    return zaehle_gruppe<PaarKK>(gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, nullptr, nullptr, pruefe);
+  }
 }
 // one group of kG lanes per item: the items of a grid-stride loop
 #define GR_FOR(i, n)                                                                                   \
@@ -1237,65 +1292,69 @@ __device__ uint32_t kante_schnitte(const SelbstArgs& s, const Gruppe& gr, int64_
   const D3 pe[2] = {pa, pb};
   const Box qe = quader_punkte(pe, 2, kZuschlagQuader);
   const D3 ehat = einheit(pb - pa);
-  return je_eintrag_gruppe<FILL, SchnittT>(
-      gr, qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, s.hs.elo, s.hs.ehi, pos,
-      [&](uint32_t t, int64_t ci, int64_t cj, int64_t ck, uint32_t, SchnittT& o) -> bool {
-        // the box first: the cheapest rejection (plain conditions, any order)
-        const Box qt = box_of(s.hs.lo, s.hs.hi, t);
-        if (!ueberlappt(qt, qe) || !erste_zelle(qe, qt, zelle, ci, cj, ck)) return false;
-        const uint4 d = s.d_idx[t];
-        const uint32_t dd[3] = {d.x, d.y, d.z};
-        bool nachbar = false;
-        for (int k = 0; k < 3; ++k)
-          nachbar = nachbar || (s.an_naehten ? (dd[k] == a0 || dd[k] == a1)
-                                             : (gleich_oder_partner(s, a0, dd[k]) || gleich_oder_partner(s, a1, dd[k])));
-        if (nachbar) return false;
-        const double4 n4 = s.nrm_t[t];
-        const D3 n = d3(n4.x, n4.y, n4.z);
-        double tk, w[3];
-        if (!kante_durch_dreieck(pa, pb, ld3(s.x, d.x), ld3(s.x, d.y), ld3(s.x, d.z), n, tk, w)) return false;
-        const double cn = dot(n, ehat);
-        if (fabs(cn) < 1e-6) return false;
-        if (FILL) {
-          o.t = t;
-          o.tk = tk;
-          o.w0 = w[0], o.w1 = w[1], o.w2 = w[2];
-          o.n = n;
-          o.cn = cn;
+  const auto pruefe = [&](uint32_t t, int64_t ci, int64_t cj, int64_t ck, uint32_t, SchnittT& o) -> bool {
+    // the box first: the cheapest rejection (plain conditions, any order)
+    const Box qt = box_of(s.hs.lo, s.hs.hi, t);
+    if (!ueberlappt(qt, qe) || !erste_zelle(qe, qt, zelle, ci, cj, ck)) return false;
+    const uint4 d = s.d_idx[t];
+    const uint32_t dd[3] = {d.x, d.y, d.z};
+    bool nachbar = false;
+    for (int k = 0; k < 3; ++k)
+      nachbar = nachbar || (s.an_naehten ? (dd[k] == a0 || dd[k] == a1)
+                                         : (gleich_oder_partner(s, a0, dd[k]) || gleich_oder_partner(s, a1, dd[k])));
+    if (nachbar) return false;
+    const double4 n4 = s.nrm_t[t];
+    const D3 n = d3(n4.x, n4.y, n4.z);
+    double tk, w[3];
+    if (!kante_durch_dreieck(pa, pb, ld3(s.x, d.x), ld3(s.x, d.y), ld3(s.x, d.z), n, tk, w)) return false;
+    const double cn = dot(n, ehat);
+    if (fabs(cn) < 1e-6) return false;
+    if (FILL) {
+      o.t = t;
+      o.tk = tk;
+      o.w0 = w[0], o.w1 = w[1], o.w2 = w[2];
+      o.n = n;
+      o.cn = cn;
+    }
+    return true;
+  };
+  const auto schreibe = [&](const SchnittT& o, uint32_t q) {
+    const D3 p = lerp3(pa, pb, o.tk);
+    D3 g = d3(0, 0, 0);
+    const uint32_t kk[2] = {kd.x, kd.y};
+    for (int r = 0; r < 2; ++r) {
+      if (kk[r] == kKein) continue;
+      const uint4 dk = s.d_idx[kk[r]];
+      const uint32_t dkk[3] = {dk.x, dk.y, dk.z};
+      uint32_t ot = kKein;
+      for (int a = 0; a < 3; ++a)
+        if (dkk[a] != a0 && dkk[a] != a1) {
+          ot = dkk[a];
+          break;
         }
-        return true;
-      },
-      [&](const SchnittT& o, uint32_t q) {
-        const D3 p = lerp3(pa, pb, o.tk);
-        D3 g = d3(0, 0, 0);
-        const uint32_t kk[2] = {kd.x, kd.y};
-        for (int r = 0; r < 2; ++r) {
-          if (kk[r] == kKein) continue;
-          const uint4 dk = s.d_idx[kk[r]];
-          const uint32_t dkk[3] = {dk.x, dk.y, dk.z};
-          uint32_t ot = kKein;
-          for (int a = 0; a < 3; ++a)
-            if (dkk[a] != a0 && dkk[a] != a1) {
-              ot = dkk[a];
-              break;
-            }
-          if (ot == kKein) continue;
-          const double4 m4 = s.nrm_t[kk[r]];
-          D3 m = einheit(cross(o.n, d3(m4.x, m4.y, m4.z)));
-          const D3 rr = ld3(s.x, ot) - p;
-          const D3 r_quer = rr - ehat * dot(ehat, rr);
-          if (dot(m, r_quer) < 0.0) m = m * -1.0;
-          g = g + (m - o.n * (dot(ehat, m) / o.cn));
-        }
-        const double lg = norm(g);
-        if (q < s.cap_s) {
-          const D3 gh = einheit(g);
-          s.sn_ke[q] = make_uint2(uint32_t(e), o.t);
-          s.sn_t[q] = o.tk;
-          s.sn_w[q] = make_double4(o.w0, o.w1, o.w2, 0.0);
-          s.sn_g[q] = make_double4(gh.x, gh.y, gh.z, lg / sqrt(lg * lg + 2.25));
-        }
-      });
+      if (ot == kKein) continue;
+      const double4 m4 = s.nrm_t[kk[r]];
+      D3 m = einheit(cross(o.n, d3(m4.x, m4.y, m4.z)));
+      const D3 rr = ld3(s.x, ot) - p;
+      const D3 r_quer = rr - ehat * dot(ehat, rr);
+      if (dot(m, r_quer) < 0.0) m = m * -1.0;
+      g = g + (m - o.n * (dot(ehat, m) / o.cn));
+    }
+    const double lg = norm(g);
+    if (q < s.cap_s) {
+      const D3 gh = einheit(g);
+      s.sn_ke[q] = make_uint2(uint32_t(e), o.t);
+      s.sn_t[q] = o.tk;
+      s.sn_w[q] = make_double4(o.w0, o.w1, o.w2, 0.0);
+      s.sn_g[q] = make_double4(gh.x, gh.y, gh.z, lg / sqrt(lg * lg + 2.25));
+    }
+  };
+  if constexpr (FILL) {
+    return je_eintrag_gruppe<true, SchnittT>(gr, qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, s.hs.elo, s.hs.ehi,
+                                      pos, pruefe, schreibe);
+  } else {
+    return zaehle_gruppe<SchnittT>(gr, qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, s.hs.elo, s.hs.ehi, pruefe);
+  }
 }
 __global__ void __launch_bounds__(kT, 4) schnitt_count_kernel(const __grid_constant__ SelbstArgs s) {
   const double z = zelle_aus(&s.lmax[0]);
