@@ -143,6 +143,39 @@ __device__ __forceinline__ bool ueberlappt32(const Box32& q, const float4& l, co
   return q.lx <= h.x && l.x <= q.hx && q.ly <= h.y && l.y <= q.hy && q.lz <= h.z && l.z <= q.hz;
 }
 
+// The entries s = a, a + st, ... < b of a bucket, in that order: f(ein[s], s)
+// for those whose index passes `vor` and whose FP32 box overlaps q32. The
+// indices of four entries are loaded, then the boxes of those that pass
+// `vor`, before any of them is tested: the impact searches are bound by load
+// latency, and several loads in flight per lane hide more of it than one.
+template <typename V, typename F>
+__device__ __forceinline__ void je_ueberlappend(uint32_t a, uint32_t b, uint32_t st, const Box32& q32,
+                                                const float4* elo, const float4* ehi, const uint32_t* ein, V&& vor,
+                                                F&& f) {
+  for (uint32_t s = a; s < b; s += 4u * st) {
+    uint32_t n[4];
+    bool ok[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t t = s + uint32_t(k) * st;
+      n[k] = t < b ? __ldg(&ein[t]) : 0u;
+      ok[k] = t < b && vor(n[k]);
+    }
+    unsigned m = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t t = s + uint32_t(k) * st;
+      if (ok[k] && ueberlappt32(q32, __ldg(&elo[t]), __ldg(&ehi[t]))) m |= 1u << k;
+    }
+    // the overlapping ones in order, through one call of f
+    while (m != 0u) {
+      const int k = __ffs(m) - 1;
+      m &= m - 1u;
+      f(k == 0 ? n[0] : (k == 1 ? n[1] : (k == 2 ? n[2] : n[3])), s + uint32_t(k) * st);
+    }
+  }
+}
+
 // selbstkollision.rs:328-344: f(entry, i, j, k, position) over the entries of
 // the box's cells. With entry boxes (elo, ehi: FP32, entry order) an entry
 // whose box misses q is skipped; without (null), every entry goes to f. The
@@ -1974,15 +2007,16 @@ __global__ void __launch_bounds__(kT, 4) stoss_pd_schwer_kernel(const __grid_con
       cell_at(c, a, i, j, k);
       const uint32_t h = streue(i, j, k, s.hp2.eimer);
       const uint32_t lo = s.hp2.anf[h], hi = s.hp2.anf[h + 1];
-      for (uint32_t e = lo + lane; e < hi; e += 32) {
-        if (!ueberlappt32(q32, s.hp2.elo[e], s.hp2.ehi[e])) continue;
+      const auto treffer = [&](uint32_t v, uint32_t e) {
         StossPD o;
-        if (stoss_pd_kandidat(s, d, qt, z, s.hp2.ein[e], i, j, k, hat, best.zeit, o)) {
+        if (stoss_pd_kandidat(s, d, qt, z, v, i, j, k, hat, best.zeit, o)) {
           hat = true;
           best = o;
           ord = (uint64_t(a) << 32) | e;
         }
-      }
+      };
+      je_ueberlappend(lo + lane, hi, 32u, q32, s.hp2.elo, s.hp2.ehi, s.hp2.ein, [](uint32_t) { return true; },
+                      treffer);
     }
     const int wer = warp_erster(hat, best.zeit, ord);
     if (wer >= 0 && int(lane) == wer) stoss_pd_schreiben(s, t, d, best);
@@ -2008,14 +2042,17 @@ __global__ void __launch_bounds__(kT, 4) stoss_kk_schwer_kernel(const __grid_con
       cell_at(c, a, i, j, k);
       const uint32_t h = streue(i, j, k, s.hk2.eimer);
       const uint32_t lo = s.hk2.anf[h], hi = s.hk2.anf[h + 1];
-      for (uint32_t e = lo + lane; e < hi; e += 32) {
+      const auto treffer = [&](uint32_t jj, uint32_t e) {
         StossKK o;
-        if (stoss_kk_kandidat(s, ie, i0, i1, qi, qi32, z, s.hk2.ein[e], i, j, k, e, hat, best.zeit, o)) {
+        if (stoss_kk_kandidat(s, ie, i0, i1, qi, qi32, z, jj, i, j, k, e, hat, best.zeit, o)) {
           hat = true;
           best = o;
           ord = (uint64_t(a) << 32) | e;
         }
-      }
+      };
+      // the index test (partner edges after this one) before the box loads
+      je_ueberlappend(lo + lane, hi, 32u, qi32, s.hk2.elo, s.hk2.ehi, s.hk2.ein,
+                      [&](uint32_t jj) { return int64_t(jj) > ie; }, treffer);
     }
     const int wer = warp_erster(hat, best.zeit, ord);
     if (wer >= 0 && int(lane) == wer) stoss_kk_schreiben(s, slot, i0, i1, best);
