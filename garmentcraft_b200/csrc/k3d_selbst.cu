@@ -145,25 +145,25 @@ __device__ __forceinline__ bool ueberlappt32(const Box32& q, const float4& l, co
 
 // The entries s = a, a + st, ... < b of a bucket, in that order: f(ein[s], s)
 // for those whose index passes `vor` and whose FP32 box overlaps q32. The
-// indices of four entries are loaded, then the boxes of those that pass
-// `vor`, before any of them is tested: the impact searches are bound by load
-// latency, and several loads in flight per lane hide more of it than one.
-template <typename V, typename F>
+// indices of D entries are loaded, then the boxes of those that pass `vor`,
+// before any of them is tested: the searches are bound by load latency, and
+// several loads in flight per lane hide more of it than one.
+template <int D, typename V, typename F>
 __device__ __forceinline__ void je_ueberlappend(uint32_t a, uint32_t b, uint32_t st, const Box32& q32,
                                                 const float4* elo, const float4* ehi, const uint32_t* ein, V&& vor,
                                                 F&& f) {
-  for (uint32_t s = a; s < b; s += 4u * st) {
-    uint32_t n[4];
-    bool ok[4];
+  for (uint32_t s = a; s < b; s += uint32_t(D) * st) {
+    uint32_t n[D];
+    bool ok[D];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < D; ++k) {
       const uint32_t t = s + uint32_t(k) * st;
       n[k] = t < b ? __ldg(&ein[t]) : 0u;
       ok[k] = t < b && vor(n[k]);
     }
     unsigned m = 0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < D; ++k) {
       const uint32_t t = s + uint32_t(k) * st;
       if (ok[k] && ueberlappt32(q32, __ldg(&elo[t]), __ldg(&ehi[t]))) m |= 1u << k;
     }
@@ -171,7 +171,11 @@ __device__ __forceinline__ void je_ueberlappend(uint32_t a, uint32_t b, uint32_t
     while (m != 0u) {
       const int k = __ffs(m) - 1;
       m &= m - 1u;
-      f(k == 0 ? n[0] : (k == 1 ? n[1] : (k == 2 ? n[2] : n[3])), s + uint32_t(k) * st);
+      uint32_t en = n[0];
+#pragma unroll
+      for (int q = 1; q < D; ++q)
+        if (q == k) en = n[q];
+      f(en, s + uint32_t(k) * st);
     }
   }
 }
@@ -245,10 +249,13 @@ __device__ uint32_t je_eintrag_gruppe(const Gruppe& gr, const Box& q, double zel
 // cell; a bucket of more than kGross entries is walked by the whole group
 // (lanes over its entries) after its round. The same candidates as
 // je_eintrag_gruppe, tested by the same predicate: a count needs no order.
+// With VOR, the walks test an entry's index with `vor` before its FP32 box
+// (elo, ehi) and keep several entries' loads in flight (je_ueberlappend).
 constexpr uint32_t kGross = 32;
-template <typename Payload, typename T>
+template <typename Payload, bool VOR = false, typename T, typename V = int>
 __device__ uint32_t zaehle_gruppe(const Gruppe& gr, const Box& q, double zelle, uint32_t eimer, const uint32_t* anf,
-                                  const uint32_t* ein, const float4* elo, const float4* ehi, T&& pruefe) {
+                                  const uint32_t* ein, const float4* elo, const float4* ehi, T&& pruefe,
+                                  V vor = V()) {
   if (!zellbereich_ok(q, zelle)) return 0;
   const Cells c = cells_of(q, zelle);
   const Box32 q32 = box32(q);
@@ -265,9 +272,16 @@ __device__ uint32_t zaehle_gruppe(const Gruppe& gr, const Box& q, double zelle, 
     }
     const bool gross = hi - lo > kGross;
     if (!gross) {
-      for (uint32_t e = lo; e < hi; ++e) {
-        Payload pl;
-        if ((!elo || ueberlappt32(q32, elo[e], ehi[e])) && pruefe(ein[e], i, j, k, e, pl)) ++cnt;
+      if constexpr (VOR) {
+        je_ueberlappend<4>(lo, hi, 1u, q32, elo, ehi, ein, vor, [&](uint32_t en, uint32_t e) {
+          Payload pl;
+          if (pruefe(en, i, j, k, e, pl)) ++cnt;
+        });
+      } else {
+        for (uint32_t e = lo; e < hi; ++e) {
+          Payload pl;
+          if ((!elo || ueberlappt32(q32, elo[e], ehi[e])) && pruefe(ein[e], i, j, k, e, pl)) ++cnt;
+        }
       }
     }
     for (unsigned m = __ballot_sync(gr.maske, gross); m != 0u; m &= m - 1u) {
@@ -275,9 +289,17 @@ __device__ uint32_t zaehle_gruppe(const Gruppe& gr, const Box& q, double zelle, 
       const uint32_t glo = __shfl_sync(gr.maske, lo, l), ghi = __shfl_sync(gr.maske, hi, l);
       const int64_t gi = __shfl_sync(gr.maske, (long long)i, l), gj = __shfl_sync(gr.maske, (long long)j, l),
                     gk = __shfl_sync(gr.maske, (long long)k, l);
-      for (uint32_t e = glo + uint32_t(gr.lane); e < ghi; e += kG) {
-        Payload pl;
-        if ((!elo || ueberlappt32(q32, elo[e], ehi[e])) && pruefe(ein[e], gi, gj, gk, e, pl)) ++cnt;
+      if constexpr (VOR) {
+        je_ueberlappend<4>(glo + uint32_t(gr.lane), ghi, uint32_t(kG), q32, elo, ehi, ein, vor,
+                           [&](uint32_t en, uint32_t e) {
+                             Payload pl;
+                             if (pruefe(en, gi, gj, gk, e, pl)) ++cnt;
+                           });
+      } else {
+        for (uint32_t e = glo + uint32_t(gr.lane); e < ghi; e += kG) {
+          Payload pl;
+          if ((!elo || ueberlappt32(q32, elo[e], ehi[e])) && pruefe(ein[e], gi, gj, gk, e, pl)) ++cnt;
+        }
       }
     }
   }
@@ -803,7 +825,9 @@ __device__ uint32_t kante_kante_gruppe(const SelbstArgs& s, const Gruppe& gr, in
     return je_eintrag_gruppe<true, PaarKK>(gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, nullptr, nullptr,
                                       pos, pruefe, schreibe);
   } else {
-    return zaehle_gruppe<PaarKK>(gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, nullptr, nullptr, pruefe);
+    // the index test (later edges only) before the box loads
+    return zaehle_gruppe<PaarKK, true>(gr, qe, s.zelle, s.eimer_k, s.anf_k, s.ein_k, s.ebk_lo, s.ebk_hi, pruefe,
+                                       [&](uint32_t f) { return int64_t(f) > e; });
   }
 }
 // one group of kG lanes per item: the items of a grid-stride loop
@@ -2015,7 +2039,7 @@ __global__ void __launch_bounds__(kT, 4) stoss_pd_schwer_kernel(const __grid_con
           ord = (uint64_t(a) << 32) | e;
         }
       };
-      je_ueberlappend(lo + lane, hi, 32u, q32, s.hp2.elo, s.hp2.ehi, s.hp2.ein, [](uint32_t) { return true; },
+      je_ueberlappend<8>(lo + lane, hi, 32u, q32, s.hp2.elo, s.hp2.ehi, s.hp2.ein, [](uint32_t) { return true; },
                       treffer);
     }
     const int wer = warp_erster(hat, best.zeit, ord);
@@ -2051,7 +2075,7 @@ __global__ void __launch_bounds__(kT, 4) stoss_kk_schwer_kernel(const __grid_con
         }
       };
       // the index test (partner edges after this one) before the box loads
-      je_ueberlappend(lo + lane, hi, 32u, qi32, s.hk2.elo, s.hk2.ehi, s.hk2.ein,
+      je_ueberlappend<8>(lo + lane, hi, 32u, qi32, s.hk2.elo, s.hk2.ehi, s.hk2.ein,
                       [&](uint32_t jj) { return int64_t(jj) > ie; }, treffer);
     }
     const int wer = warp_erster(hat, best.zeit, ord);
