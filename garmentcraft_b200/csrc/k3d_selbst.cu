@@ -753,7 +753,8 @@ __device__ uint32_t punkt_dreieck_gruppe(const SelbstArgs& s, const Gruppe& gr, 
     return je_eintrag_gruppe<true, PaarPT>(gr, qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, s.ebp_lo, s.ebp_hi,
                                       pos, pruefe, schreibe);
   } else {
-    return zaehle_gruppe<PaarPT>(gr, qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, s.ebp_lo, s.ebp_hi, pruefe);
+    return zaehle_gruppe<PaarPT, true>(gr, qt, s.zelle, s.eimer_p, s.anf_p, s.ein_p, s.ebp_lo, s.ebp_hi, pruefe,
+                                       [](uint32_t) { return true; });
   }
 }
 struct PaarKK {
@@ -1410,7 +1411,8 @@ __device__ uint32_t kante_schnitte(const SelbstArgs& s, const Gruppe& gr, int64_
     return je_eintrag_gruppe<true, SchnittT>(gr, qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, s.hs.elo, s.hs.ehi,
                                       pos, pruefe, schreibe);
   } else {
-    return zaehle_gruppe<SchnittT>(gr, qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, s.hs.elo, s.hs.ehi, pruefe);
+    return zaehle_gruppe<SchnittT, true>(gr, qe, zelle, s.hs.eimer, s.hs.anf, s.hs.ein, s.hs.elo, s.hs.ehi, pruefe,
+                                         [](uint32_t) { return true; });
   }
 }
 __global__ void __launch_bounds__(kT, 4) schnitt_count_kernel(const __grid_constant__ SelbstArgs s) {
