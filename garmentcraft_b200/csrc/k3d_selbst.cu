@@ -273,7 +273,7 @@ __device__ uint32_t zaehle_gruppe(const Gruppe& gr, const Box& q, double zelle, 
     const bool gross = hi - lo > kGross;
     if (!gross) {
       if constexpr (VOR) {
-        je_ueberlappend<4>(lo, hi, 1u, q32, elo, ehi, ein, vor, [&](uint32_t en, uint32_t e) {
+        je_ueberlappend<8>(lo, hi, 1u, q32, elo, ehi, ein, vor, [&](uint32_t en, uint32_t e) {
           Payload pl;
           if (pruefe(en, i, j, k, e, pl)) ++cnt;
         });
@@ -290,7 +290,7 @@ __device__ uint32_t zaehle_gruppe(const Gruppe& gr, const Box& q, double zelle, 
       const int64_t gi = __shfl_sync(gr.maske, (long long)i, l), gj = __shfl_sync(gr.maske, (long long)j, l),
                     gk = __shfl_sync(gr.maske, (long long)k, l);
       if constexpr (VOR) {
-        je_ueberlappend<4>(glo + uint32_t(gr.lane), ghi, uint32_t(kG), q32, elo, ehi, ein, vor,
+        je_ueberlappend<8>(glo + uint32_t(gr.lane), ghi, uint32_t(kG), q32, elo, ehi, ein, vor,
                            [&](uint32_t en, uint32_t e) {
                              Payload pl;
                              if (pruefe(en, gi, gj, gk, e, pl)) ++cnt;
