@@ -4,8 +4,10 @@ single CPU thread; about two minutes for the sheet and two for the garment).
 * The sheet over the sphere, 257 x 257 points (66,049): the device's FP64
   drop runs to step 42, after first contact (about step 38); from that state two steps,
   each from the device's state, on the device and in the oracle at PCG
-  tolerance 1e-12: equal contact and release counts, positions within 1e-9
-  of the bounding-box diagonal. The chosen form (FP32 operator storage) from
+  tolerance 1e-12: equal contact and release counts, positions within 1e-8
+  of the bounding-box diagonal (two solves stopped at 1e-12 on this stiff
+  contact system differ by up to 3.4e-9 of it, measured at the second step;
+  the same bound as the garment's). The chosen form (FP32 operator storage) from
   the same states stays within 1e-4 of the diagonal (the FP32-rounded
   operator moves the solution by about 3e-5 there, measured).
 * The sewn garment, 205,284 points with the self-collision stage on: from
@@ -50,7 +52,7 @@ def test_sheet_257_nach_dem_aufprall_wie_orakel():
         assert (a.kontakte, a.freigegeben) == (st.kontakte, st.freigegeben), k
         assert not a.nicht_konvergiert and not st.nicht_konvergiert
         xo, _ = o.state()
-        assert np.max(np.abs(s.x - xo)) <= 1e-9 * diag(xo), k
+        assert np.max(np.abs(s.x - xo)) <= 1e-8 * diag(xo), k
         kontakte += a.kontakte
         # the chosen form from the same state, one step
         t = start.copy()
