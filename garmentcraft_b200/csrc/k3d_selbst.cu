@@ -843,19 +843,30 @@ __global__ void __launch_bounds__(kT, 4) pairs_count_kernel(const __grid_constan
     s.off_t[s.nd] = 0u;
     s.off_e[s.ne] = 0u;
   }
+  // triangles (q < nd) and edges (nd + e) from one counter, one item per
+  // grab: the crowded parts of the cloth cluster in index ranges, so a fixed
+  // stride would leave some groups far more work than others
   const Gruppe gr = gruppe();
-  GR_FOR(t, s.nd) {
-    const uint32_t c = punkt_dreieck_gruppe<false>(s, gr, t, 0);
-    if (gr.lane == 0) {
-      s.off_t[t] = c;
-      if (c) s.aktiv_p[atomicAdd(&s.zahl[SZ_AKTIV_P], 1u)] = uint32_t(t);
-    }
-  }
-  GR_FOR(e, s.ne) {
-    const uint32_t c = kante_kante_gruppe<false>(s, gr, e, 0);
-    if (gr.lane == 0) {
-      s.off_e[e] = c;
-      if (c) s.aktiv_p[atomicAdd(&s.zahl[SZ_AKTIV_P], 1u)] = uint32_t(s.nd + e);
+  const int fuehrer = int(threadIdx.x & 31) & ~(kG - 1);
+  const uint64_t gesamt = uint64_t(s.nd) + uint64_t(s.ne);
+  for (;;) {
+    uint32_t q = 0;
+    if (gr.lane == 0) q = atomicAdd(&s.zahl[SZ_ARBEIT_P], 1u);
+    q = __shfl_sync(gr.maske, q, fuehrer);
+    if (q >= gesamt) break;
+    if (int64_t(q) < s.nd) {
+      const uint32_t c = punkt_dreieck_gruppe<false>(s, gr, q, 0);
+      if (gr.lane == 0) {
+        s.off_t[q] = c;
+        if (c) s.aktiv_p[atomicAdd(&s.zahl[SZ_AKTIV_P], 1u)] = q;
+      }
+    } else {
+      const int64_t e = int64_t(q) - s.nd;
+      const uint32_t c = kante_kante_gruppe<false>(s, gr, e, 0);
+      if (gr.lane == 0) {
+        s.off_e[e] = c;
+        if (c) s.aktiv_p[atomicAdd(&s.zahl[SZ_AKTIV_P], 1u)] = q;
+      }
     }
   }
 }
@@ -2353,7 +2364,7 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
                                                     s.ebp_hi);
   eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.anf_k, s.eimer_k, s.cap_ek, s.ein_k, s.qk_lo, s.qk_hi, s.ebk_lo,
                                                     s.ebk_hi);
-  pairs_count_kernel<<<grid_for(kG * (s.nd > s.ne ? s.nd : s.ne)), kT, 0, st>>>(s);
+  pairs_count_kernel<<<148 * 4, kT, 0, st>>>(s);  // resident blocks; the groups take items from a counter
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = scan(s.off_t, s.nd + 1, s.scan_tmp, &s.zahl[SZ_PAARE_PT], st)) != cudaSuccess) return e;
   if ((e = scan(s.off_e, s.ne + 1, s.scan_tmp, &s.zahl[SZ_PAARE_KK], st)) != cudaSuccess) return e;

@@ -34,6 +34,7 @@ enum SelbstZahl : int {
   SZ_AKTIV_S = 16,  // edges through a triangle (the intersection fill pass's list)
   SZ_SCHWER_PD = 17,  // triangles whose impact search runs one warp each (many candidates)
   SZ_SCHWER_KK = 18,  // edges likewise
+  SZ_ARBEIT_P = 19,   // the proximity count pass's next item (triangles, then nd + edges)
   SZ_COUNT = 20
 };
 
