@@ -836,6 +836,22 @@ __device__ uint32_t kante_kante_gruppe(const SelbstArgs& s, const Gruppe& gr, in
   for (int64_t i = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / kG; i < int64_t(n);                \
        i += int64_t(gridDim.x) * blockDim.x / kG)
 
+// Items 0 .. n-1 taken one at a time from a counter (zeroed with the stage's
+// counters) by a group of lanes: its first lane (`fuehrer`, a warp lane)
+// grabs, every lane of `maske` gets the item, f(item) runs on all of them.
+// Crowded parts of the cloth cluster in index ranges, so a fixed stride would
+// leave some groups far more work than others.
+template <typename F>
+__device__ __forceinline__ void je_gezogen(unsigned maske, int fuehrer, uint32_t* zaehler, uint64_t n, F&& f) {
+  for (;;) {
+    uint32_t q = 0;
+    if (int(threadIdx.x & 31) == fuehrer) q = atomicAdd(zaehler, 1u);
+    q = __shfl_sync(maske, q, fuehrer);
+    if (q >= n) break;
+    f(q);
+  }
+}
+
 // count pass: pair count per triangle and per edge (off_t[t], off_e[e]);
 // the triangles and edges that have pairs go to a list for the fill pass
 __global__ void __launch_bounds__(kT, 4) pairs_count_kernel(const __grid_constant__ SelbstArgs s) {
@@ -1430,13 +1446,13 @@ __global__ void __launch_bounds__(kT, 4) schnitt_count_kernel(const __grid_const
   const double z = zelle_aus(&s.lmax[0]);
   if (blockIdx.x == 0 && threadIdx.x == 0) s.off_s[s.ne] = 0u;
   const Gruppe gr = gruppe();
-  GR_FOR(e, s.ne) {
+  je_gezogen(gr.maske, int(threadIdx.x & 31) & ~(kG - 1), &s.zahl[SZ_ARBEIT_S], uint64_t(s.ne), [&](uint32_t e) {
     const uint32_t c = kante_schnitte<false>(s, gr, e, 0, z);
     if (gr.lane == 0) {
       s.off_s[e] = c;
-      if (c) s.aktiv_s[atomicAdd(&s.zahl[SZ_AKTIV_S], 1u)] = uint32_t(e);
+      if (c) s.aktiv_s[atomicAdd(&s.zahl[SZ_AKTIV_S], 1u)] = e;
     }
-  }
+  });
 }
 // fill pass over the listed edges (their starts come from the scan)
 __global__ void __launch_bounds__(kT, 4) schnitt_fill_kernel(const __grid_constant__ SelbstArgs s, uint32_t n_aktiv) {
@@ -2023,13 +2039,11 @@ __global__ void __launch_bounds__(kT, 4) stoss_kk_kernel(const __grid_constant__
 // turn (entry position lane, lane + 32, ...), each keeps its first hit by
 // time (its own visits are in the reference's order), and the warp's first
 // by (time, cell, position) writes the result.
-#define WARP_FOR(w, n)                                                                                       \
-  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < (n); w += (gridDim.x * blockDim.x) >> 5)
 __global__ void __launch_bounds__(kT, 4) stoss_pd_schwer_kernel(const __grid_constant__ SelbstArgs s) {
   const double z = zelle_aus(&s.lmax[1]);
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t m = s.zahl[SZ_SCHWER_PD];
-  WARP_FOR(w, m) {
+  je_gezogen(0xffffffffu, 0, &s.zahl[SZ_ARBEIT_PD], m, [&](uint32_t w) {
     const uint32_t t = s.schwer_pd[w];
     const uint4 dq = s.d_idx[t];
     const uint32_t d[3] = {dq.x, dq.y, dq.z};
@@ -2057,13 +2071,13 @@ __global__ void __launch_bounds__(kT, 4) stoss_pd_schwer_kernel(const __grid_con
     }
     const int wer = warp_erster(hat, best.zeit, ord);
     if (wer >= 0 && int(lane) == wer) stoss_pd_schreiben(s, t, d, best);
-  }
+  });
 }
 __global__ void __launch_bounds__(kT, 4) stoss_kk_schwer_kernel(const __grid_constant__ SelbstArgs s) {
   const double z = zelle_aus(&s.lmax[1]);
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t m = s.zahl[SZ_SCHWER_KK];
-  WARP_FOR(w, m) {
+  je_gezogen(0xffffffffu, 0, &s.zahl[SZ_ARBEIT_KK], m, [&](uint32_t w) {
     const int64_t ie = s.schwer_kk[w];
     const uint32_t slot = uint32_t(s.nd + ie);
     const uint2 ki = s.k_idx[ie];
@@ -2093,7 +2107,7 @@ __global__ void __launch_bounds__(kT, 4) stoss_kk_schwer_kernel(const __grid_con
     }
     const int wer = warp_erster(hat, best.zeit, ord);
     if (wer >= 0 && int(lane) == wer) stoss_kk_schreiben(s, slot, i0, i1, best);
-  }
+  });
 }
 // ohne_durchdrungene (selbstkollision.rs:1063-1084): keep flags per slot
 __device__ bool trifft(const SelbstArgs& s, uint32_t a, uint32_t b) {
@@ -2381,7 +2395,7 @@ cudaError_t selbst_hash_fuellen_und_paare_zaehlen(const SelbstArgs& s, cudaStrea
   if ((e = lang_sort(s.hs.anf, s.hs.ein, s.hs.eimer, st)) != cudaSuccess) return e;
   eintrag_boxen_kernel<<<kEintragGrid, kT, 0, st>>>(s.hs.anf, s.hs.eimer, s.hs.cap, s.hs.ein, s.hs.lo, s.hs.hi, s.hs.elo,
                                                     s.hs.ehi);
-  schnitt_count_kernel<<<grid_for(kG * s.ne), kT, 0, st>>>(s);
+  schnitt_count_kernel<<<148 * 4, kT, 0, st>>>(s);  // resident blocks; the groups take edges from a counter
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return scan(s.off_s, s.ne + 1, s.scan_tmp, &s.zahl[SZ_SCHNITTE], st);
 }

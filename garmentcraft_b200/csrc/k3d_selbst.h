@@ -35,7 +35,10 @@ enum SelbstZahl : int {
   SZ_SCHWER_PD = 17,  // triangles whose impact search runs one warp each (many candidates)
   SZ_SCHWER_KK = 18,  // edges likewise
   SZ_ARBEIT_P = 19,   // the proximity count pass's next item (triangles, then nd + edges)
-  SZ_COUNT = 20
+  SZ_ARBEIT_S = 20,   // the intersection count pass's next edge
+  SZ_ARBEIT_PD = 21,  // the heavy point-triangle impact search's next list entry
+  SZ_ARBEIT_KK = 22,  // the heavy edge-edge impact search's next list entry
+  SZ_COUNT = 24
 };
 
 // A spatial hash over boxes (Hashgitter, selbstkollision.rs:281-345): the
