@@ -398,3 +398,24 @@ def test_tube_hoop_strain_analytic():
     T = 600.0 * 0.5 * (lam * lam - 1.0)
     T_soll = 600.0 * 0.5 * ((1 + soll) ** 2 - 1.0)
     assert abs(T / T_soll - 1.0) < 0.02, (T, T_soll)
+
+
+# ---------------------------------------------------------------- sim/tests/implizit.rs:7-14, free fall
+def test_freier_fall_diskret():
+    """Backward Euler covers a*h^2*N(N+1)/2 in N steps under a constant
+    acceleration a (`weg_diskret`, sim/tests/implizit.rs:7-14). A free sheet
+    at its rest shape stays undeformed (a uniform move is in the stiffness'
+    null space), so every point falls exactly that far."""
+    muster, _ = synth.sheet_over_sphere(n=17, groesse_m=0.3, jitter_mm=1.0, seed=2)
+    s = O.build_scene(muster, [])
+    x0 = s.x.copy()
+    sim = O.OracleSim(s, ImplizitParameter(schritte_je_bild=1, cg_max=2000, cg_toleranz=1e-12).to_c())
+    n = 30
+    sim.frames(n)
+    x, v = sim.state()
+    h, g = muster.param.bild_dt, 9.81
+    soll = g * h * h * n * (n + 1) / 2.0
+    dz = x0[:, 2] - x[:, 2]
+    assert np.max(np.abs(dz / soll - 1.0)) < 1e-9
+    assert np.max(np.abs(x[:, :2] - x0[:, :2])) < 1e-12
+    assert np.max(np.abs(v[:, 2] + g * h * n)) < 1e-9 * g * h * n
