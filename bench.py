@@ -592,6 +592,7 @@ def params(prec):
 
 
 def element_counts(s):
+    import numpy as np
     N, T, B = s.n, s.membran_punkte.shape[0], s.biegung_punkte.shape[0]
     S = s.naht_punkte.shape[0] + int(np.sum(s.membran_kante == 0))
     return N, T, B, S
@@ -1019,5 +1020,4 @@ def main():
 
 
 if __name__ == "__main__":
-    import numpy as np  # noqa: F401  (used by algorithmic_bytes)
     main()
