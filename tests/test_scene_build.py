@@ -63,3 +63,14 @@ def test_two_pieces_with_seam_hinges():
     # 10 seam hinges on top of the interior edges of both pieces
     inner = 2 * (10 * 6 + 11 * 5 + 10 * 5 - (2 * 10 + 2 * 5))
     assert a.biegung_punkte.shape[0] == inner + 10
+
+
+def test_garment_205k_bitgleich():
+    # the sewn garment at full size: 28 panels, ~205k points, seams by length
+    # fraction (both builders, every field bit for bit)
+    m, body = synth.garment(ziel_punkte=200_000)
+    a, b = build_scene(m, [body]), O.build_scene(m, [body])
+    same(a, b)
+    assert a.n > 200_000 and a.teil_bereiche.shape[0] == 28
+    assert b.oracle_counts["membran_entartet"] == 0
+    assert a.membran_punkte.shape[0] == sum(t.dreiecke.shape[0] for t in m.teile)
