@@ -151,3 +151,24 @@ def test_ohne_reibung_dasselbe_gleichgewicht():
     assert abs(q(a, 0.95) - q(b, 0.95)) < 1e-3, (q(a, 0.95), q(b, 0.95))
     # both at the reduction's strain 1/(1 - r) - 1 = 5.82 % within 0.1 pp
     assert abs(q(a, 0.5) - (1 / (1 - 0.055) - 1)) < 1e-3
+
+
+def test_cg_bleibt_in_ruhe_stabil():
+    """sim/tests/implizit.rs:86-103: at rest the right-hand side is almost
+    zero, and the CG must not keep iterating on rounding noise (the absolute
+    floor of the stopping test, implizit.rs:392-398): the frictionless tube
+    (Roehre::default, Radical 0.4 at 5.5 % on a 9 cm cylinder) over 60 frames
+    of five substeps at tol 1e-8 keeps a finite mean speed below 1 m/s."""
+    R, mat = 0.09, synth.RADICAL_RUBBER_04
+    m, body = synth.tube(umfang_m=2 * math.pi * (R + mat.dicke_m / 2), hoehe_m=0.2, zylinder_radius_m=R,
+                         material=mat)
+    m.teile[0].reduktion = 0.055
+    s = O.build_scene(m, [body])
+    s.reibung[:] = 0.0
+    par = ImplizitParameter(cg_max=2000, cg_toleranz=1e-8)
+    assert par.schritte_je_bild == 5
+    sim = O.OracleSim(s, par.to_c())
+    for _ in range(60):
+        sim.frames(1)
+        v = sim.mittlere_geschwindigkeit()
+        assert np.isfinite(v) and v < 1.0, v
