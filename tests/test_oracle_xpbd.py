@@ -172,3 +172,19 @@ def test_cg_bleibt_in_ruhe_stabil():
         sim.frames(1)
         v = sim.mittlere_geschwindigkeit()
         assert np.isfinite(v) and v < 1.0, v
+
+
+def test_weichheitsbedingung():
+    """sim/tests/roehre.rs:110-128: the soft-substep rule asks Radical 0.4
+    for 2.5-4 times the substeps of Retifist 0.4 (about sqrt(10) at a similar
+    mass), more than 100; the scene's spring compliances and lumped masses
+    decide it."""
+    n = {}
+    for mat in (synth.RADICAL_RUBBER_04, synth.RETIFIST_NR_040):
+        m, body = synth.tube(umfang_m=2 * math.pi * (0.09 + mat.dicke_m / 2), hoehe_m=0.2, zylinder_radius_m=0.09,
+                             material=mat)
+        m.teile[0].reduktion = 0.055
+        n[mat.dehnung_n_m] = unterschritte_weich(O.build_scene(m, [body]))
+    rad, ret = n[synth.RADICAL_RUBBER_04.dehnung_n_m], n[synth.RETIFIST_NR_040.dehnung_n_m]
+    assert 2.5 <= rad / ret < 4.0, (rad, ret)
+    assert rad > 100
