@@ -114,8 +114,10 @@ def test_ohne_reibung_dasselbe_gleichgewicht():
     within 2e-4, 95th percentile within 1e-3. The implicit step runs until
     rest as in the reference (mean speed under 1e-5 m/s for 10 frames); the
     XPBD tube keeps its shape after 150 frames but turns about the frictionless
-    cylinder at a constant speed inversely proportional to the damping, so it
-    runs a fixed 150 frames of the soft substep count."""
+    cylinder at a constant speed inversely proportional to the damping (the
+    Gauss-Seidel sweep's handedness on this regular grid: reversing the
+    membranes' order reverses the turn), so it runs a fixed 150 frames of the
+    soft substep count."""
     R, mat = 0.09, synth.RETIFIST_NR_040
 
     def szene():
