@@ -876,7 +876,8 @@ def main():
         line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": a.gpus,
                 "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": workload_config(a.n, s, {"precision": "fp64 (CPU)"}),
+                "config": workload_config(a.n, s, {"precision": "fp64 (CPU)",
+                                                   "l2": "not applicable: one host thread, no device"}),
                 "cpu_baseline": cpu,
                 "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
